@@ -1,0 +1,131 @@
+"""ctypes binding of libadcgpu (include/adcgpu.h)."""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import pathlib
+
+_HERE = pathlib.Path(__file__).resolve().parent
+LIB_PATH = _HERE / "lib" / "libadcgpu.so"
+
+dp_ = C.POINTER(C.c_double)
+ip_ = C.POINTER(C.c_int)
+
+ADC_OK = 0
+ADC_ERR_DIAG = 1
+ADC_ERR_ARG = -1
+ADC_ERR_MESH = -2
+ADC_ERR_CUDA = -3
+ADC_ERR_NOMEM = -4
+ADC_ERR_TIMEOUT = -5
+ADC_ERR_UNSUPPORTED = -6
+ADC_PREC_FP64 = 0
+ADC_PREC_MIXED = 1
+
+
+class AdcParams(C.Structure):
+    _fields_ = [(n, C.c_double) for n in (
+        "dt", "g", "a00", "b00", "c00", "h0", "velmin", "slim", "hbreak", "ftheta",
+        "fgamma", "convcr", "prbckgrnd_mh2o")] + [(n, C.c_int) for n in (
+            "ifnlfa", "ifnlct", "ifnlcat", "nolifa", "iflinbf", "ifnlbf", "ifhybf", "itmax",
+            "nws", "ifwind", "isldia", "pad_")]
+
+
+ARRAY_FIELDS = [
+    ("x", dp_), ("y", dp_), ("dp", dp_), ("nm", ip_), ("nneigh", ip_), ("neitab", ip_),
+    ("fdxe", dp_), ("fdye", dp_), ("areas", dp_), ("csr_position", ip_),
+    ("tau0var", dp_), ("evm", dp_), ("fric", dp_), ("corif", dp_),
+    ("nbd", ip_), ("amig", dp_), ("per", dp_), ("face", dp_), ("ff", dp_),
+    ("emo", dp_), ("efa", dp_), ("nbv", ip_), ("lbcodei", ip_), ("csii", dp_), ("siii", dp_),
+    ("me2gw", ip_),
+    ("eta1", dp_), ("eta2", dp_), ("etas", dp_),
+    ("uu1", dp_), ("vv1", dp_), ("uu2", dp_), ("vv2", dp_), ("qx1", dp_), ("qy1", dp_),
+    ("qx2", dp_), ("qy2", dp_), ("h1", dp_), ("h2", dp_),
+    ("tk", dp_), ("tkm", dp_),
+    ("nodecode", ip_), ("nnodecode", ip_), ("noff", ip_), ("mju", ip_),
+    ("totalarea", dp_), ("alphal", dp_),
+    ("wsx1", dp_), ("wsy1", dp_), ("wsx2", dp_), ("wsy2", dp_), ("pr1", dp_), ("pr2", dp_),
+    ("coef", dp_), ("obccoef", dp_),
+    ("gwce_lv", dp_), ("mom_lv_x", dp_), ("mom_lv_y", dp_),
+]
+
+
+class AdcArrays(C.Structure):
+    _fields_ = [(n, C.c_int) for n in ("np", "ne", "mnei", "neta", "nbfr", "nvel", "nvelme",
+                                        "pad_")] + ARRAY_FIELDS
+
+
+class AdcStep(C.Structure):
+    _fields_ = [("it", C.c_int), ("pad_", C.c_int), ("timeloc", C.c_double),
+                ("timeh", C.c_double), ("rampelev", C.c_double), ("rampmete", C.c_double)]
+
+
+class AdcStepOut(C.Structure):
+    _fields_ = [("numitr", C.c_int), ("ier", C.c_int), ("ncchange", C.c_int),
+                ("status", C.c_int), ("ep", C.c_double), ("zeta", C.c_double),
+                ("cme", C.c_double), ("n_w1_events", C.c_int), ("pad_", C.c_int)]
+
+
+_lib = None
+
+
+def load():
+    """Load the in-tree libadcgpu.so; raise if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise RuntimeError(f"{LIB_PATH} is missing: run `python -m adcirc_b200.build` first")
+    lib = C.CDLL(str(LIB_PATH))
+    vp = C.c_void_p
+    sig = {
+        "adc_mesh_geometry": (C.c_int, [C.c_int, C.c_int, dp_, dp_, ip_, dp_, dp_, dp_]),
+        "adc_mesh_mnei": (C.c_int, [C.c_int, C.c_int, ip_]),
+        "adc_mesh_neighb": (C.c_int, [C.c_int, C.c_int, C.c_int, dp_, dp_, ip_, ip_, ip_, ip_]),
+        "adc_mesh_csr_positions": (C.c_int, [C.c_int, C.c_int, C.c_int, ip_, ip_, C.c_int, ip_]),
+        "adc_boundary_setup": (C.c_int, [C.c_int, dp_, dp_, C.c_int, ip_, ip_, ip_, C.c_double,
+                                          C.c_int, ip_, ip_, ip_, dp_, dp_, ip_, ip_]),
+        "adc_coldstart": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_double, dp_, ip_, dp_, dp_,
+                                     dp_, ip_, ip_, ip_, ip_, dp_]),
+        "adc_jcg": (None, [ip_, ip_, ip_, ip_, dp_, dp_, dp_, ip_, ip_, dp_, ip_, dp_, ip_]),
+        "adc_dfault": (None, [ip_, dp_]),
+        "adc_jcg_reset": (None, []),
+        "adc_gpu_bind": (C.c_int, [C.POINTER(AdcParams), C.POINTER(AdcArrays), C.c_int,
+                                    C.POINTER(vp)]),
+        "adc_gpu_free": (C.c_int, [vp]),
+        "adc_shift_friction": (C.c_int, [vp, C.POINTER(AdcStep)]),
+        "adc_gwce_new": (C.c_int, [vp, C.POINTER(AdcStep), C.POINTER(AdcStepOut)]),
+        "adc_wetdry": (C.c_int, [vp, C.POINTER(AdcStep), C.POINTER(AdcStepOut)]),
+        "adc_momentum": (C.c_int, [vp, C.POINTER(AdcStep)]),
+        "adc_timestep": (C.c_int, [vp, C.POINTER(AdcStep), C.POINTER(AdcStepOut)]),
+        "adc_run": (C.c_int, [vp, C.c_int, C.POINTER(AdcStep), ip_, C.POINTER(AdcStepOut)]),
+        "adc_sync_to_host": (C.c_int, [vp]),
+        "adc_sync_from_host": (C.c_int, [vp]),
+        "adc_set_met": (C.c_int, [vp, dp_, dp_, dp_]),
+        "adc_phase_times": (C.c_int, [vp, dp_, dp_, dp_, dp_, dp_]),
+        "adc_launch_count": (C.c_int64, [vp]),
+        "adc_last_run_ms": (C.c_double, [vp]),
+        "adc_last_error": (C.c_char_p, []),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = lib
+    return lib
+
+
+def exported_symbols():
+    """Names declared in include/adcgpu.h (used by the ABI test)."""
+    import re
+    hdr = (_HERE.parent / "include" / "adcgpu.h").read_text()
+    return sorted(set(re.findall(r"^\s*(?:[\w\s\*]+?)\b(adc_\w+)\s*\(", hdr, re.M)))
+
+
+def ptr(a, typ):
+    return a.ctypes.data_as(typ)
+
+
+def last_error() -> str:
+    s = load().adc_last_error()
+    return s.decode() if s else ""

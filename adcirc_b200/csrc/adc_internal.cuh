@@ -1,0 +1,159 @@
+// adc_internal.cuh -- device-side data layout shared by the libadcgpu kernels.
+//
+// HBM layout (one B200, state resident between calls):
+//   node arrays      double[NP]  (eta1, eta2, ..., SoA, 0-based node index)
+//   element arrays   nm[3*NE] (element-major, 0-based), fdx/fdy[3*NE], areas[NE]
+//   node->element    CSR n2e_ptr[NP+1], n2e[3*NE] = 3*e+k sorted by e, so
+//                    every per-node sum runs in the reference's element order
+//   GWCE matrix      diag[NP] + off-diagonals in sliced ELL (32-row slices,
+//                    column-major inside a slice, slot order = NeiTab order)
+//   scratch          element contribution buffers, JCG vectors, partials
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+
+#include "../../include/adcgpu.h"
+
+namespace adc {
+
+constexpr int kSlice = 32;            // rows per SELL slice (one warp)
+constexpr int kThreads = 256;
+constexpr long long kSpinCycles = 4000000000LL;  // ~2 s at 1.9 GHz
+
+// Device-visible scalar state of the step and of ITPACK.
+struct Flags {
+  int ncchange;       // NCCHANGE (wetdry.F / gwce.F:430)
+  int status;         // ADC_ERR_DIAG on a non-positive diagonal
+  int numitr;         // NUMITR of the last solve
+  int ier;            // JCG ier of the last solve
+  int n_w1_events;    // W1 events of the last wet/dry pass
+  int timeout;        // nonzero once a bounded wait expired
+  int cursor;         // index of the current step in the step table
+  int pad_;
+  double ep;          // EP (gwce.F:646-650), persists between rebuilds
+  double zeta;        // RPARM(1) after the last solve
+  double cme;         // RPARM(2) after the last solve
+};
+
+// ITPACK common blocks and saved locals (itpackv.F:/itcom1-3/, itjcg save,
+// chgcon save) for the device-side solver.  One thread of one block writes
+// them between grid barriers; every other thread reads them after.
+struct Itp {
+  int in, itmax, halt, adapt, q1, chg_ier, isym, pad_;
+  double zeta, cme, sme, gamma, rho, gamold, rhoold, delnnm, delsnm, udnm,
+      stptst, cmold, srelpr, rparm1;
+  double c1, c2, c3, c4;
+  double dtnrm, unorm;
+  int need_unorm, pad2_;
+};
+
+struct Bar {
+  unsigned int count;
+  unsigned int gen;
+};
+
+struct Ctx;
+
+}  // namespace adc
+
+struct adc_ctx {
+  // sizes
+  int np, ne, mnei, neta, nbfr, nvel, nvelme, prec;
+  int nslices, nnz_pad, n_obc, n_obc_rhs_nodes, n_me, itmax;
+  adc_params_t p;
+  adc_arrays_t host;     // bound host arrays (for sync)
+  cudaStream_t stream;
+  // node data
+  double *x, *y, *dp, *tau0, *evm, *fric, *corif;
+  int *nneigh;
+  // element data
+  int *nm;
+  double *fdx, *fdy, *areas;
+  int *n2e_ptr, *n2e;
+  // matrix structure (SELL)
+  int *sl_ptr, *sl_w, *col, *rlen;
+  int *lhs_src;          // 2 per padded slot: index 6*e+q of the element off-diagonal value, or -1
+  int *ell_of_sell;      // host-side sync helper: SELL slot -> (i + np*j) ELL index (device copy unused)
+  int *h_ell_of_sell;
+  // boundaries
+  int *nbd, *is_nbd;     // is_nbd[i] = I index (0-based) or -1
+  double *amig, *per, *face, *ff, *emo, *efa;
+  int *obc_slot, *obc_zero;   // per (I,J): SELL slot of Coef(nb,IJ) (-1 none), nb-is-NBD flag
+  int *obc_rhs_ptr, *obc_rhs_node, *obc_rhs_ent;  // per affected nb: entries I + neta*J, and b
+  int *obc_rhs_b;
+  int *me_of_node;       // momentum BC entry per node or -1
+  int *me_lbc;
+  double *me_csi, *me_sii;
+  // state
+  double *eta1, *eta2, *etas, *uu1, *vv1, *uu2, *vv2, *qx1, *qy1, *qx2, *qy2, *h1, *h2;
+  double *tk, *tkm, *totalarea, *alphal, *wsx1, *wsy1, *wsx2, *wsy2, *pr1, *pr2;
+  double *gwce_lv, *mom_x, *mom_y;
+  int *nodecode, *nnodecode, *noff, *noffold, *mju, *ncele;
+  double *diag, *offd, *obccoef;
+  // scratch
+  double *ebuf;          // element contributions, 9*NE doubles
+  double *ebuf2;         // 3*NE doubles (momentum y)
+  double *red;           // reduction partials
+  // W1 events
+  int *ev_cnt;           // per element-block event counts
+  int *ev_a, *ev_b;      // per element: NM123, partner (compacted per block)
+  double *ev_c;
+  int ev_blocks;
+  // JCG
+  double *ju1, *jd[3], *jdt[2], *jw, *soff;
+  double *jpart;         // partial dots per block (4 each)
+  double *jtri;          // tri(itmax,4)
+  adc::Itp *itp;
+  adc::Bar *bar;
+  int jcg_grid, jcg_rows_blocks;
+  // flags / steps
+  adc::Flags *flags;
+  adc_step_t *steps;     // device step table
+  int steps_cap;
+  int *numitr_log;
+  int numitr_cap;
+  // met forcing staging
+  double *met_wsx, *met_wsy, *met_pr;
+  int met_pending;
+  // timing
+  cudaEvent_t ev[6];
+  int64_t launches;
+  // graph
+  cudaGraphExec_t graph;
+  int graph_ok;
+  int graph_launches;    // kernel launches per replayed step
+  cudaEvent_t run_ev[2];
+  double last_run_ms;
+};
+
+namespace adc {
+
+// Error bookkeeping (thread-local message).
+void set_error(const char *fmt, ...);
+int cuda_fail(cudaError_t e, const char *what);
+
+#define ADC_CUDA(call)                                         \
+  do {                                                         \
+    cudaError_t e_ = (call);                                   \
+    if (e_ != cudaSuccess) return adc::cuda_fail(e_, #call);   \
+  } while (0)
+
+inline int nblk(long long n, int t = kThreads) { return (int)((n + t - 1) / t); }
+
+// Phase launchers (each returns ADC_OK or an error, records launches).
+int launch_shift_friction(adc_ctx *c);
+int launch_gwce_lhs(adc_ctx *c);
+int launch_gwce_rhs(adc_ctx *c);
+int launch_jcg(adc_ctx *c, int eta_update);
+int launch_wetdry(adc_ctx *c);
+int launch_momentum(adc_ctx *c);
+
+// Deterministic block reduction of one double (fixed tree).
+__device__ __forceinline__ double warp_sum(double v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+
+}  // namespace adc

@@ -1,0 +1,350 @@
+// gwce.cu -- GWCE_New (gwce.F:237-2111) for IM=0 (Kolar-Gray lateral
+// stress, non-conservative advection), consistent mass (ILump = 0),
+// Cartesian coordinates, plus the TIMESTEP glue that precedes it.
+//
+// Element terms are computed once per element into a scratch buffer and
+// gathered per node over the node->element CSR in increasing element order,
+// i.e. the order of the reference's scatter loops, starting from zero as
+// the reference does after zeroing.  No atomics touch floating point, so
+// the results are deterministic and, compiled without FMA contraction,
+// reproduce the serial arithmetic bit for bit.
+#include "adc_internal.cuh"
+
+namespace adc {
+
+// --------------------------------------------------------------- shift
+// timestep.F:231-237 (IT==1 H init), :375-416 (time-level shift, zeroing),
+// nodalattr.F:2399-2413 (quadratic/linear/hybrid friction), :2700-2704.
+__global__ void k_shift_friction(adc_ctx c, const adc_step_t *steps, const Flags *flags) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= c.np) return;
+  const adc_step_t st = steps[flags->cursor];
+  const adc_params_t &p = c.p;
+  if (st.it == 1) {
+    double h = c.dp[i] + p.ifnlfa * c.eta2[i];
+    c.h2[i] = h;
+    c.h1[i] = h;
+  }
+  c.qx1[i] = c.qx2[i];
+  c.qy1[i] = c.qy2[i];
+  double u1 = c.uu2[i], v1 = c.vv2[i];
+  c.uu1[i] = u1;
+  c.vv1[i] = v1;
+  c.gwce_lv[i] = 0.0;
+  c.mom_x[i] = 0.0;
+  c.mom_y[i] = 0.0;
+  if (p.nws != 0) {
+    c.wsx1[i] = c.wsx2[i];
+    c.wsx2[i] = 0.0;
+    c.wsy1[i] = c.wsy2[i];
+    c.wsy2[i] = 0.0;
+    c.pr1[i] = c.pr2[i];
+  }
+  c.pr2[i] = p.prbckgrnd_mh2o;
+  double uv1 = sqrt(u1 * u1 + v1 * v1);
+  double h1 = c.dp[i] + p.ifnlfa * c.eta2[i];
+  double hyb = 0.0;
+  if (p.ifhybf != 0) hyb = p.ifhybf * pow(1.0 + pow(p.hbreak / h1, p.ftheta), p.fgamma / p.ftheta);
+  double v = c.fric[i] * (p.iflinbf + (uv1 / h1) * (p.ifnlbf + hyb));
+  double cap = 2.0 / p.dt;
+  double tk = (v < cap) ? v : cap;
+  c.tk[i] = tk;
+  c.tkm[3 * i + 0] = tk;
+  c.tkm[3 * i + 1] = tk;
+  c.tkm[3 * i + 2] = 0.0;
+}
+
+// Met forcing supplied by the host for this step (WSX2, WSY2, PR2).
+__global__ void k_apply_met(adc_ctx c) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= c.np) return;
+  c.wsx2[i] = c.met_wsx[i];
+  c.wsy2[i] = c.met_wsy[i];
+  c.pr2[i] = c.met_pr[i];
+}
+
+// --------------------------------------------------------------- LHS
+// The rebuild runs only when NCChange > 0 (gwce.F:430-431).
+__global__ void k_lhs_begin(Flags *f, int *rebuild) {
+  int r = f->ncchange > 0;
+  *rebuild = r;
+  if (r) f->ncchange = 0;
+}
+
+// gwce.F:456-593: nine consistent-mass + gravity entries per element.
+__global__ void k_lhs_elem(adc_ctx c, const int *rebuild) {
+  if (!*rebuild) return;
+  int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= c.ne) return;
+  const adc_params_t &p = c.p;
+  const double DT = p.dt;
+  int n1 = c.nm[3 * e], n2 = c.nm[3 * e + 1], n3 = c.nm[3 * e + 2];
+  int NCEle = c.nodecode[n1] * c.nodecode[n2] * c.nodecode[n3] * c.noff[e];
+  double FDX1 = c.fdx[3 * e], FDX2 = c.fdx[3 * e + 1], FDX3 = c.fdx[3 * e + 2];
+  double FDY1 = c.fdy[3 * e], FDY2 = c.fdy[3 * e + 1], FDY3 = c.fdy[3 * e + 2];
+  double AreaIE2 = c.areas[e];
+  double AreaIE = AreaIE2 * 0.5;
+  double AreaIE4 = AreaIE2 * 2.0;
+  double DPAvg = (c.dp[n1] + c.dp[n2] + c.dp[n3]) / 3.0;
+  double GA = c.alphal[e] * p.a00 * p.g * DPAvg / AreaIE4;
+  double Tau0Avg = (c.tau0[n1] + c.tau0[n2] + c.tau0[n3]) / 3.0;
+  double MsOn = 2 * AreaIE * (1.0 / DT + Tau0Avg / 2.0) / DT / 12.0;
+  double MsOff = 1 * AreaIE * (1.0 / DT + Tau0Avg / 2.0) / DT / 12.0;
+  double nc = (double)NCEle;
+  double *o = c.ebuf + 9 * (size_t)e;
+  o[0] = (MsOn + GA * (FDX1 * FDX1 + FDY1 * FDY1)) * nc;
+  o[1] = (MsOn + GA * (FDX2 * FDX2 + FDY2 * FDY2)) * nc;
+  o[2] = (MsOn + GA * (FDX3 * FDX3 + FDY3 * FDY3)) * nc;
+  o[3] = (MsOff + GA * (FDX1 * FDX2 + FDY1 * FDY2)) * nc;  // (n1, J12)
+  o[4] = (MsOff + GA * (FDX1 * FDX3 + FDY1 * FDY3)) * nc;  // (n1, J13)
+  o[5] = (MsOff + GA * (FDX2 * FDX1 + FDY2 * FDY1)) * nc;  // (n2, J21)
+  o[6] = (MsOff + GA * (FDX2 * FDX3 + FDY2 * FDY3)) * nc;  // (n2, J23)
+  o[7] = (MsOff + GA * (FDX3 * FDX1 + FDY3 * FDY1)) * nc;  // (n3, J31)
+  o[8] = (MsOff + GA * (FDX3 * FDX2 + FDY3 * FDY2)) * nc;  // (n3, J32)
+}
+
+// Per-row gather of COEF in element order, and the per-block partial of
+// sum(diag^2) for EP (gwce.F:646-650).
+__global__ void k_lhs_gather(adc_ctx c, const int *rebuild) {
+  if (!*rebuild) return;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double d2 = 0.0;
+  if (i < c.np) {
+    double d = 0.0;
+    for (int q = c.n2e_ptr[i]; q < c.n2e_ptr[i + 1]; ++q) {
+      int ek = c.n2e[q];
+      int e = ek / 3, k = ek - 3 * e;
+      d = d + c.ebuf[9 * (size_t)e + k];
+    }
+    c.diag[i] = d;
+    d2 = d * d;
+    int s = i / kSlice, lane = i - s * kSlice;
+    int base = c.sl_ptr[s] + lane;
+    int len = c.rlen[i];
+    for (int k = 0; k < len; ++k) {
+      int idx = base + k * kSlice;
+      int a = c.lhs_src[2 * idx], b = c.lhs_src[2 * idx + 1];
+      double v = 0.0;
+      if (a >= 0) v = v + c.ebuf[a];
+      if (b >= 0) v = v + c.ebuf[b];
+      c.offd[idx] = v;
+    }
+  }
+  __shared__ double sh[32];
+  d2 = warp_sum(d2);
+  int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) sh[w] = d2;
+  __syncthreads();
+  if (w == 0) {
+    d2 = lane < (int)(blockDim.x >> 5) ? sh[lane] : 0.0;
+    d2 = warp_sum(d2);
+    if (lane == 0) c.red[blockIdx.x] = d2;
+  }
+}
+
+__global__ void k_lhs_ep(adc_ctx c, const int *rebuild, int nparts) {
+  if (!*rebuild) return;
+  __shared__ double sh[32];
+  double s = 0.0;
+  for (int b = threadIdx.x; b < nparts; b += blockDim.x) s += c.red[b];
+  s = warp_sum(s);
+  int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) sh[w] = s;
+  __syncthreads();
+  if (w == 0) {
+    s = lane < (int)(blockDim.x >> 5) ? sh[lane] : 0.0;
+    s = warp_sum(s);
+    if (lane == 0) c.flags->ep = sqrt(s / c.np);
+  }
+}
+
+// gwce.F:654-707: elevation-boundary rows and columns, OBCCoef, diagonal
+// checks.  Thread t < NP handles row t; thread NP + q handles the q-th
+// (I, J) column entry.
+__global__ void k_lhs_bc(adc_ctx c, const int *rebuild) {
+  if (!*rebuild) return;
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const double EP = c.flags->ep;
+  if (t < c.np) {
+    int i = t;
+    if (c.is_nbd[i] >= 0) {
+      c.diag[i] = EP;
+      int s = i / kSlice, lane = i - s * kSlice;
+      int base = c.sl_ptr[s] + lane;
+      int len = c.rlen[i];
+      for (int k = 0; k < len; ++k) c.offd[base + k * kSlice] = 0.0;
+    }
+    double d = c.diag[i];
+    if (d == 0.0) {
+      d = EP;
+      c.diag[i] = d;
+    }
+    if (d < 0.0) atomicExch(&c.flags->status, ADC_ERR_DIAG);
+    return;
+  }
+  int q = t - c.np;
+  if (q >= c.n_obc) return;
+  int slot = c.obc_slot[q];
+  double v = 0.0;
+  if (slot >= 0) {
+    if (!c.obc_zero[q]) v = c.offd[slot];
+    c.offd[slot] = 0.0;
+  }
+  c.obccoef[q] = v;
+}
+
+// --------------------------------------------------------------- RHS
+// gwce.F:1000-1617, one element, IM=0 branches.
+__global__ void k_rhs_elem(adc_ctx c) {
+  int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= c.ne) return;
+  const adc_params_t &p = c.p;
+  const double DT = p.dt, G = p.g, A00 = p.a00, B00 = p.b00, C00 = p.c00;
+  int n1 = c.nm[3 * e], n2 = c.nm[3 * e + 1], n3 = c.nm[3 * e + 2];
+  int NCEle = c.nodecode[n1] * c.nodecode[n2] * c.nodecode[n3] * c.noff[e];
+  double E0N1 = c.eta1[n1], E0N2 = c.eta1[n2], E0N3 = c.eta1[n3];
+  double E1N1 = c.eta2[n1], E1N2 = c.eta2[n2], E1N3 = c.eta2[n3];
+  double E1N1SQ = E1N1 * E1N1, E1N2SQ = E1N2 * E1N2, E1N3SQ = E1N3 * E1N3;
+  double ESN1 = c.etas[n1], ESN2 = c.etas[n2], ESN3 = c.etas[n3];
+  double U1N1 = c.uu1[n1], U1N2 = c.uu1[n2], U1N3 = c.uu1[n3];
+  double V1N1 = c.vv1[n1], V1N2 = c.vv1[n2], V1N3 = c.vv1[n3];
+  double QX1N1 = c.qx1[n1], QX1N2 = c.qx1[n2], QX1N3 = c.qx1[n3];
+  double QY1N1 = c.qy1[n1], QY1N2 = c.qy1[n2], QY1N3 = c.qy1[n3];
+  double H1N1 = c.h2[n1], H1N2 = c.h2[n2], H1N3 = c.h2[n3];
+  double EVMN1 = c.evm[n1], EVMN2 = c.evm[n2], EVMN3 = c.evm[n3];
+  double T0N1 = c.tau0[n1], T0N2 = c.tau0[n2], T0N3 = c.tau0[n3];
+  const bool met = p.nws != 0;
+  double Pr1N1 = 0.0, Pr1N2 = 0.0, Pr1N3 = 0.0;
+  if (met) { Pr1N1 = c.pr1[n1]; Pr1N2 = c.pr1[n2]; Pr1N3 = c.pr1[n3]; }
+  const double *tk1 = c.tkm + 3 * n1, *tk2 = c.tkm + 3 * n2, *tk3 = c.tkm + 3 * n3;
+  double BSXN1 = tk1[0] * QX1N1 + tk1[2] * QY1N1;
+  double BSYN1 = tk1[2] * QX1N1 + tk1[1] * QY1N1;
+  double BSXN2 = tk2[0] * QX1N2 + tk2[2] * QY1N2;
+  double BSYN2 = tk2[2] * QX1N2 + tk2[1] * QY1N2;
+  double BSXN3 = tk3[0] * QX1N3 + tk3[2] * QY1N3;
+  double BSYN3 = tk3[2] * QX1N3 + tk3[1] * QY1N3;
+  double AreaIE2 = c.areas[e];
+  double AreaIE = AreaIE2 / 2.0;
+  double AreaIE4 = 2.0 * AreaIE2;
+  double FDX1 = c.fdx[3 * e], FDX2 = c.fdx[3 * e + 1], FDX3 = c.fdx[3 * e + 2];
+  double FDY1 = c.fdy[3 * e], FDY2 = c.fdy[3 * e + 1], FDY3 = c.fdy[3 * e + 2];
+  double E0XGrad2A = E0N1 * FDX1 + E0N2 * FDX2 + E0N3 * FDX3;
+  double E0YGrad2A = E0N1 * FDY1 + E0N2 * FDY2 + E0N3 * FDY3;
+  double E1XGrad2A = E1N1 * FDX1 + E1N2 * FDX2 + E1N3 * FDX3;
+  double E1YGrad2A = E1N1 * FDY1 + E1N2 * FDY2 + E1N3 * FDY3;
+  double Tau0XGrad2A = T0N1 * FDX1 + T0N2 * FDX2 + T0N3 * FDX3;
+  double Tau0YGrad2A = T0N1 * FDY1 + T0N2 * FDY2 + T0N3 * FDY3;
+  double EVMXGrad = (EVMN1 * FDX1 + EVMN2 * FDX2 + EVMN3 * FDX3) / AreaIE2;
+  double EVMYGrad = (EVMN1 * FDY1 + EVMN2 * FDY2 + EVMN3 * FDY3) / AreaIE2;
+  double EVMAvgODT = ((EVMN1 + EVMN2 + EVMN3) / 3.0) / DT;
+  double MX = (EVMXGrad * (QX1N1 * FDX1 + QX1N2 * FDX2 + QX1N3 * FDX3) +
+               EVMYGrad * (QY1N1 * FDX1 + QY1N2 * FDX2 + QY1N3 * FDX3) -
+               EVMAvgODT * (ESN1 * FDX1 + ESN2 * FDX2 + ESN3 * FDX3)) / AreaIE2;
+  double MY = (EVMXGrad * (QX1N1 * FDY1 + QX1N2 * FDY2 + QX1N3 * FDY3) +
+               EVMYGrad * (QY1N1 * FDY1 + QY1N2 * FDY2 + QY1N3 * FDY3) -
+               EVMAvgODT * (ESN1 * FDY1 + ESN2 * FDY2 + ESN3 * FDY3)) / AreaIE2;
+  double CorifAvg = (c.corif[n1] + c.corif[n2] + c.corif[n3]) / 3.0;
+  double Tau0Avg = (T0N1 + T0N2 + T0N3) / 3.0;
+  double Tau0QXAvg = (T0N1 * QX1N1 + T0N2 * QX1N2 + T0N3 * QX1N3) / 3.0;
+  double Tau0QYAvg = (T0N1 * QY1N1 + T0N2 * QY1N2 + T0N3 * QY1N3) / 3.0;
+  double U1Avg = (U1N1 + U1N2 + U1N3) / 3.0;
+  double V1Avg = (V1N1 + V1N2 + V1N3) / 3.0;
+  double QX1Avg = (QX1N1 + QX1N2 + QX1N3) / 3.0;
+  double QY1Avg = (QY1N1 + QY1N2 + QY1N3) / 3.0;
+  double ESAvg = (ESN1 + ESN2 + ESN3) / 3.0;
+  double DPAvg = (c.dp[n1] + c.dp[n2] + c.dp[n3]) / 3.0;
+  double al = c.alphal[e];
+  double GDPAvgOAreaIE4 = al * G * DPAvg / AreaIE4;
+  double GDPAvgOAreaIE4_S0 = GDPAvgOAreaIE4;   // DPAvgS0 == DPAvg when IFNL_HDP = 0
+  double HAvg = (H1N1 + H1N2 + H1N3) / 3.0;
+  double GHAvg = al * G * HAvg;
+  double GHAvgOAreaIE2 = GHAvg / AreaIE2;
+  double BSXAvg = (BSXN1 + BSXN2 + BSXN3) / 3.0;
+  double BSYAvg = (BSYN1 + BSYN2 + BSYN3) / 3.0;
+  double WSXAvg = 0.0, WSYAvg = 0.0;
+  if (met) {
+    WSXAvg = (c.wsx1[n1] + c.wsx1[n2] + c.wsx1[n3]) / 3.0;
+    WSYAvg = (c.wsy1[n1] + c.wsy1[n2] + c.wsy1[n3]) / 3.0;
+  }
+  double MsFacR = AreaIE * (1.0 / DT - Tau0Avg / 2.0) / DT / 12.0;
+  double GOAreaIE4 = al * G / AreaIE4;
+  double Tau0SpaVar = (QX1Avg * Tau0XGrad2A + QY1Avg * Tau0YGrad2A) / 6.0;
+  double A00pB00 = A00 + B00;
+  double fa = p.ifnlfa * GOAreaIE4;
+  double JXAvg = CorifAvg * QY1Avg - fa * (E1N1SQ * FDX1 + E1N2SQ * FDX2 + E1N3SQ * FDX3) -
+                 GHAvgOAreaIE2 * (Pr1N1 * FDX1 + Pr1N2 * FDX2 + Pr1N3 * FDX3) + WSXAvg -
+                 BSXAvg + MX + Tau0QXAvg;
+  double JYAvg = -CorifAvg * QX1Avg - fa * (E1N1SQ * FDY1 + E1N2SQ * FDY2 + E1N3SQ * FDY3) -
+                 GHAvgOAreaIE2 * (Pr1N1 * FDY1 + Pr1N2 * FDY2 + Pr1N3 * FDY3) + WSYAvg -
+                 BSYAvg + MY + Tau0QYAvg;
+  JXAvg = JXAvg - p.ifnlct * (QX1Avg * (U1N1 * FDX1 + U1N2 * FDX2 + U1N3 * FDX3) +
+                              QY1Avg * (U1N1 * FDY1 + U1N2 * FDY2 + U1N3 * FDY3)) / AreaIE2 +
+          p.ifnlcat * U1Avg * ESAvg / DT;
+  JYAvg = JYAvg - p.ifnlct * (QX1Avg * (V1N1 * FDX1 + V1N2 * FDX2 + V1N3 * FDX3) +
+                              QY1Avg * (V1N1 * FDY1 + V1N2 * FDY2 + V1N3 * FDY3)) / AreaIE2 +
+          p.ifnlcat * V1Avg * ESAvg / DT;
+  double c0 = GDPAvgOAreaIE4_S0, c1 = GDPAvgOAreaIE4;
+  double T1 = (2 * ESN1 + 1 * (ESN2 + ESN3)) * MsFacR -
+              c0 * (C00 * (FDX1 * E0XGrad2A + FDY1 * E0YGrad2A)) -
+              c1 * (A00pB00 * (FDX1 * E1XGrad2A + FDY1 * E1YGrad2A)) +
+              (JXAvg * FDX1 + JYAvg * FDY1) * 0.5 + Tau0SpaVar;
+  double T2 = (2 * ESN2 + 1 * (ESN1 + ESN3)) * MsFacR -
+              c0 * (C00 * (FDX2 * E0XGrad2A + FDY2 * E0YGrad2A)) -
+              c1 * (A00pB00 * (FDX2 * E1XGrad2A + FDY2 * E1YGrad2A)) +
+              (JXAvg * FDX2 + JYAvg * FDY2) * 0.5 + Tau0SpaVar;
+  double T3 = (2 * ESN3 + 1 * (ESN1 + ESN2)) * MsFacR -
+              c0 * (C00 * (FDX3 * E0XGrad2A + FDY3 * E0YGrad2A)) -
+              c1 * (A00pB00 * (FDX3 * E1XGrad2A + FDY3 * E1YGrad2A)) +
+              (JXAvg * FDX3 + JYAvg * FDY3) * 0.5 + Tau0SpaVar;
+  double nc = (double)NCEle;
+  double *o = c.ebuf + 3 * (size_t)e;
+  o[0] = T1 * nc;
+  o[1] = T2 * nc;
+  o[2] = T3 * nc;
+}
+
+// GWCE_LV gather (element order) fused with gwce.F:1622-1631.
+__global__ void k_rhs_gather(adc_ctx c) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= c.np) return;
+  double v = 0.0;
+  for (int q = c.n2e_ptr[i]; q < c.n2e_ptr[i + 1]; ++q) v = v + c.ebuf[c.n2e[q]];
+  c.gwce_lv[i] = v;
+  c.eta1[i] = c.eta2[i];
+  c.h1[i] = c.h2[i];
+  c.eta2[i] = 0.0;
+}
+
+// gwce.F:1638-1651 periodic elevation BC and :1846-1850 load-vector rows.
+__global__ void k_eta_bc(adc_ctx c, const adc_step_t *steps, const Flags *flags) {
+  int I = blockIdx.x * blockDim.x + threadIdx.x;
+  if (I >= c.neta) return;
+  const adc_step_t st = steps[flags->cursor];
+  int b = c.nbd[I];
+  double e2 = 0.0;   // ETA2 was zeroed in k_rhs_gather
+  for (int J = 0; J < c.nbfr; ++J) {
+    int NCYC = 0;
+    if (c.per[J] != 0.0) NCYC = (int)(st.timeh / c.per[J]);
+    double ARGJ = c.amig[J] * (st.timeh - NCYC * c.per[J]) + c.face[J];
+    double RFF = c.ff[J] * st.rampelev;
+    double ARG = ARGJ - c.efa[J + (size_t)c.nbfr * I];
+    e2 = e2 + c.emo[J + (size_t)c.nbfr * I] * RFF * cos(ARG);
+  }
+  c.eta2[b] = e2;
+  double es = e2 - c.eta1[b];
+  c.etas[b] = es;
+  c.gwce_lv[b] = es * c.nodecode[b] * flags->ep;
+}
+
+// gwce.F:1851-1854 column correction, per affected neighbour in (I, J) order.
+__global__ void k_obc_rhs(adc_ctx c) {
+  int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= c.n_obc_rhs_nodes) return;
+  int nb = c.obc_rhs_node[r];
+  double v = c.gwce_lv[nb];
+  for (int q = c.obc_rhs_ptr[r]; q < c.obc_rhs_ptr[r + 1]; ++q)
+    v = v - c.etas[c.obc_rhs_b[q]] * c.obccoef[c.obc_rhs_ent[q]];
+  c.gwce_lv[nb] = v;
+}
+
+}  // namespace adc

@@ -1,0 +1,736 @@
+// step.cu -- libadcgpu host side: bind/upload, the TIMESTEP 2DDI sequence,
+// graph replay, host synchronisation and the ITPACK jcg drop-in.
+#include "adc_internal.cuh"
+
+#include <cfloat>
+#include <cmath>
+#include <cstdarg>
+#include <cstring>
+#include <string>
+#include <vector>
+#include <algorithm>
+
+namespace adc {
+
+thread_local std::string g_err;
+
+void set_error(const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_err = buf;
+}
+
+int cuda_fail(cudaError_t e, const char *what) {
+  set_error("%s: %s", what, cudaGetErrorString(e));
+  return ADC_ERR_CUDA;
+}
+
+int jcg_setup_grid(adc_ctx *c);
+
+// kernels defined in the other translation units
+__global__ void k_shift_friction(adc_ctx c, const adc_step_t *steps, const Flags *flags);
+__global__ void k_apply_met(adc_ctx c);
+__global__ void k_lhs_begin(Flags *f, int *rebuild);
+__global__ void k_lhs_elem(adc_ctx c, const int *rebuild);
+__global__ void k_lhs_gather(adc_ctx c, const int *rebuild);
+__global__ void k_lhs_ep(adc_ctx c, const int *rebuild, int nparts);
+__global__ void k_lhs_bc(adc_ctx c, const int *rebuild);
+__global__ void k_rhs_elem(adc_ctx c);
+__global__ void k_rhs_gather(adc_ctx c);
+__global__ void k_eta_bc(adc_ctx c, const adc_step_t *steps, const Flags *flags);
+__global__ void k_obc_rhs(adc_ctx c);
+
+__global__ void k_step_end(Flags *f, int *numitr_log, int cap) {
+  int k = f->cursor;
+  if (k < cap) numitr_log[k] = f->numitr;
+  f->cursor = k + 1;
+}
+
+// Device scratch for the rebuild flag lives after the flags struct.
+static int *rebuild_flag(adc_ctx *c) { return (int *)(c->flags + 1); }
+
+int launch_shift_friction(adc_ctx *c) {
+  k_shift_friction<<<nblk(c->np), kThreads, 0, c->stream>>>(*c, c->steps, c->flags);
+  c->launches++;
+  if (c->met_pending) {
+    k_apply_met<<<nblk(c->np), kThreads, 0, c->stream>>>(*c);
+    c->launches++;
+  }
+  return ADC_OK;
+}
+
+int launch_gwce_lhs(adc_ctx *c) {
+  int *rb = rebuild_flag(c);
+  k_lhs_begin<<<1, 1, 0, c->stream>>>(c->flags, rb);
+  k_lhs_elem<<<nblk(c->ne), kThreads, 0, c->stream>>>(*c, rb);
+  int nb = nblk(c->np);
+  k_lhs_gather<<<nb, kThreads, 0, c->stream>>>(*c, rb);
+  k_lhs_ep<<<1, 1024, 0, c->stream>>>(*c, rb, nb);
+  k_lhs_bc<<<nblk((long long)c->np + c->n_obc), kThreads, 0, c->stream>>>(*c, rb);
+  c->launches += 5;
+  return ADC_OK;
+}
+
+int launch_gwce_rhs(adc_ctx *c) {
+  k_rhs_elem<<<nblk(c->ne), kThreads, 0, c->stream>>>(*c);
+  k_rhs_gather<<<nblk(c->np), kThreads, 0, c->stream>>>(*c);
+  c->launches += 2;
+  if (c->neta > 0) {
+    k_eta_bc<<<nblk(c->neta), kThreads, 0, c->stream>>>(*c, c->steps, c->flags);
+    c->launches++;
+    if (c->n_obc_rhs_nodes > 0) {
+      k_obc_rhs<<<nblk(c->n_obc_rhs_nodes), kThreads, 0, c->stream>>>(*c);
+      c->launches++;
+    }
+  }
+  return ADC_OK;
+}
+
+// The whole 2DDI step (TIMESTEP order), without host synchronisation.
+static int enqueue_step(adc_ctx *c, bool timed) {
+  int rc;
+  if (timed) cudaEventRecord(c->ev[0], c->stream);
+  if ((rc = launch_shift_friction(c))) return rc;
+  if (timed) cudaEventRecord(c->ev[1], c->stream);
+  if ((rc = launch_gwce_lhs(c))) return rc;
+  if ((rc = launch_gwce_rhs(c))) return rc;
+  if (timed) cudaEventRecord(c->ev[2], c->stream);
+  if ((rc = launch_jcg(c, 1))) return rc;
+  if (timed) cudaEventRecord(c->ev[3], c->stream);
+  if ((rc = launch_wetdry(c))) return rc;
+  if (timed) cudaEventRecord(c->ev[4], c->stream);
+  if ((rc = launch_momentum(c))) return rc;
+  if (timed) cudaEventRecord(c->ev[5], c->stream);
+  return ADC_OK;
+}
+
+template <class T>
+static int dalloc(T **p, size_t n) {
+  if (n == 0) n = 1;
+  cudaError_t e = cudaMalloc((void **)p, n * sizeof(T));
+  if (e != cudaSuccess) {
+    set_error("cudaMalloc(%zu bytes): %s", n * sizeof(T), cudaGetErrorString(e));
+    return ADC_ERR_NOMEM;
+  }
+  return ADC_OK;
+}
+
+template <class T>
+static int up(T *d, const T *h, size_t n) {
+  if (n == 0) return ADC_OK;
+  ADC_CUDA(cudaMemcpy(d, h, n * sizeof(T), cudaMemcpyHostToDevice));
+  return ADC_OK;
+}
+
+template <class T>
+static int down(T *h, const T *d, size_t n) {
+  if (n == 0 || h == nullptr) return ADC_OK;
+  ADC_CUDA(cudaMemcpy(h, d, n * sizeof(T), cudaMemcpyDeviceToHost));
+  return ADC_OK;
+}
+
+#define TRY(x)                 \
+  do {                         \
+    int rc_ = (x);             \
+    if (rc_) return rc_;       \
+  } while (0)
+
+// ---------------------------------------------------------------- bind
+struct HostTables {
+  std::vector<int> nm, n2e_ptr, n2e, sl_ptr, sl_w, col, rlen, lhs_src, ell_of_sell;
+  std::vector<int> is_nbd, nbd, obc_slot, obc_zero, obc_rhs_ptr, obc_rhs_node, obc_rhs_ent,
+      obc_rhs_b, me_of_node, me_lbc;
+  std::vector<double> me_csi, me_sii;
+  std::vector<int> sell_of_ell;   // ELL (i + np*j), j >= 1 -> SELL idx or -1
+};
+
+static int build_tables(const adc_arrays_t *a, HostTables &T, int &nslices, int &nnz_pad) {
+  const int np = a->np, ne = a->ne, mnei = a->mnei, neta = a->neta;
+  T.nm.resize(3 * (size_t)ne);
+  for (int e = 0; e < ne; ++e)
+    for (int k = 0; k < 3; ++k) {
+      int v = a->nm[e + (size_t)ne * k];
+      if (v < 1 || v > np) { set_error("NM(%d,%d) = %d out of range", e + 1, k + 1, v); return ADC_ERR_MESH; }
+      T.nm[3 * (size_t)e + k] = v - 1;
+    }
+  T.n2e_ptr.assign(np + 1, 0);
+  for (int e = 0; e < ne; ++e)
+    for (int k = 0; k < 3; ++k) T.n2e_ptr[T.nm[3 * (size_t)e + k] + 1]++;
+  for (int i = 0; i < np; ++i) T.n2e_ptr[i + 1] += T.n2e_ptr[i];
+  T.n2e.resize(3 * (size_t)ne);
+  {
+    std::vector<int> fill(T.n2e_ptr.begin(), T.n2e_ptr.end() - 1);
+    for (int e = 0; e < ne; ++e)
+      for (int k = 0; k < 3; ++k) T.n2e[fill[T.nm[3 * (size_t)e + k]]++] = 3 * e + k;
+  }
+  // sliced ELL of the off-diagonal NeiTab slots
+  nslices = (np + kSlice - 1) / kSlice;
+  T.rlen.assign(np, 0);
+  T.sl_w.assign(nslices, 0);
+  T.sl_ptr.assign(nslices + 1, 0);
+  for (int i = 0; i < np; ++i) {
+    int nn = a->nneigh[i];
+    if (nn < 1 || nn > mnei) { set_error("NNeigh(%d) = %d", i + 1, nn); return ADC_ERR_MESH; }
+    T.rlen[i] = nn - 1;
+    if (a->neitab[i] != i + 1) { set_error("NeiTab(%d,1) is not the node itself", i + 1); return ADC_ERR_MESH; }
+    T.sl_w[i / kSlice] = std::max(T.sl_w[i / kSlice], nn - 1);
+  }
+  for (int s = 0; s < nslices; ++s) T.sl_ptr[s + 1] = T.sl_ptr[s] + T.sl_w[s] * kSlice;
+  nnz_pad = T.sl_ptr[nslices];
+  T.col.assign(std::max(nnz_pad, 1), 0);
+  T.ell_of_sell.assign(std::max(nnz_pad, 1), -1);
+  T.sell_of_ell.assign((size_t)np * mnei, -1);
+  for (int i = 0; i < np; ++i) {
+    int s = i / kSlice, lane = i % kSlice;
+    for (int k = 0; k < T.sl_w[s]; ++k) {
+      int idx = T.sl_ptr[s] + k * kSlice + lane;
+      if (k < T.rlen[i]) {
+        int j = a->neitab[i + (size_t)np * (k + 1)];
+        if (j < 1 || j > np) { set_error("NeiTab(%d,%d) = %d", i + 1, k + 2, j); return ADC_ERR_MESH; }
+        T.col[idx] = j - 1;
+        T.ell_of_sell[idx] = i + np * (k + 1);
+        T.sell_of_ell[i + (size_t)np * (k + 1)] = idx;
+      } else {
+        T.col[idx] = i;
+      }
+    }
+  }
+  // padded rows of the last slice point at row 0 (never used)
+  // LHS contribution map: element off-diagonal value q in 3..8 -> slot
+  T.lhs_src.assign(2 * (size_t)std::max(nnz_pad, 1), -1);
+  static const int qk[6] = {0, 0, 1, 1, 2, 2}, ql[6] = {0, 1, 0, 1, 0, 1};
+  for (int e = 0; e < ne; ++e) {
+    for (int t = 0; t < 6; ++t) {
+      int k = qk[t], l = ql[t];
+      int row = T.nm[3 * (size_t)e + k];
+      int J = a->csr_position[e + (size_t)ne * (k + 3 * l)];
+      if (J < 2 || J > a->nneigh[row]) { set_error("CSR_POSITION(%d,%d,%d) = %d", e + 1, k + 1, l + 1, J); return ADC_ERR_MESH; }
+      int idx = T.sell_of_ell[row + (size_t)np * (J - 1)];
+      if (idx < 0) { set_error("CSR slot missing"); return ADC_ERR_MESH; }
+      int v = 9 * e + 3 + t;
+      if (T.lhs_src[2 * (size_t)idx] < 0) T.lhs_src[2 * (size_t)idx] = v;
+      else if (T.lhs_src[2 * (size_t)idx + 1] < 0) T.lhs_src[2 * (size_t)idx + 1] = v;
+      else { set_error("edge shared by more than two elements"); return ADC_ERR_MESH; }
+    }
+  }
+  // elevation boundary tables
+  T.is_nbd.assign(np, -1);
+  T.nbd.resize(std::max(neta, 1));
+  for (int I = 0; I < neta; ++I) {
+    int b = a->nbd[I] - 1;
+    if (b < 0 || b >= np) { set_error("NBD(%d) out of range", I + 1); return ADC_ERR_MESH; }
+    T.nbd[I] = b;
+    T.is_nbd[b] = I;
+  }
+  const int nobc = neta * (mnei - 1);
+  T.obc_slot.assign(std::max(nobc, 1), -1);
+  T.obc_zero.assign(std::max(nobc, 1), 0);
+  std::vector<std::vector<std::pair<int, int>>> rhs_lists(np);   // (entry, b)
+  for (int I = 0; I < neta; ++I) {
+    int b = T.nbd[I];
+    for (int J = 2; J <= a->nneigh[b]; ++J) {
+      int q = I + neta * (J - 2);
+      int nb = a->neitab[b + (size_t)np * (J - 1)] - 1;
+      for (int IJ = 2; IJ <= a->nneigh[nb]; ++IJ)
+        if (a->neitab[nb + (size_t)np * (IJ - 1)] - 1 == b) {
+          T.obc_slot[q] = T.sell_of_ell[nb + (size_t)np * (IJ - 1)];
+          T.obc_zero[q] = (T.is_nbd[nb] >= 0) ? 1 : 0;
+        }
+      if (T.is_nbd[nb] < 0) rhs_lists[nb].push_back({q, b});
+    }
+  }
+  T.obc_rhs_ptr.assign(1, 0);
+  for (int i = 0; i < np; ++i) {
+    if (rhs_lists[i].empty()) continue;
+    T.obc_rhs_node.push_back(i);
+    for (auto &pr : rhs_lists[i]) {
+      T.obc_rhs_ent.push_back(pr.first);
+      T.obc_rhs_b.push_back(pr.second);
+    }
+    T.obc_rhs_ptr.push_back((int)T.obc_rhs_ent.size());
+  }
+  // momentum boundary table
+  T.me_of_node.assign(np, -1);
+  for (int J = 0; J < a->nvelme; ++J) {
+    int I = a->me2gw[J] - 1;
+    if (I < 0 || I >= a->nvel) { set_error("ME2GW(%d) out of range", J + 1); return ADC_ERR_MESH; }
+    int node = a->nbv[I] - 1;
+    if (node < 0 || node >= np) { set_error("NBV out of range"); return ADC_ERR_MESH; }
+    if (T.me_of_node[node] >= 0) { set_error("node %d has two momentum BC entries", node + 1); return ADC_ERR_MESH; }
+    T.me_of_node[node] = J;
+    T.me_lbc.push_back(a->lbcodei[I]);
+    T.me_csi.push_back(a->csii[I]);
+    T.me_sii.push_back(a->siii[I]);
+  }
+  return ADC_OK;
+}
+
+static int upload_state(adc_ctx *c) {
+  const adc_arrays_t *a = &c->host;
+  const int np = c->np, ne = c->ne;
+  TRY(up(c->eta1, a->eta1, np));
+  TRY(up(c->eta2, a->eta2, np));
+  TRY(up(c->etas, a->etas, np));
+  TRY(up(c->uu1, a->uu1, np));
+  TRY(up(c->vv1, a->vv1, np));
+  TRY(up(c->uu2, a->uu2, np));
+  TRY(up(c->vv2, a->vv2, np));
+  TRY(up(c->qx1, a->qx1, np));
+  TRY(up(c->qy1, a->qy1, np));
+  TRY(up(c->qx2, a->qx2, np));
+  TRY(up(c->qy2, a->qy2, np));
+  TRY(up(c->h1, a->h1, np));
+  TRY(up(c->h2, a->h2, np));
+  TRY(up(c->tk, a->tk, np));
+  TRY(up(c->tkm, a->tkm, 3 * (size_t)np));
+  TRY(up(c->totalarea, a->totalarea, np));
+  TRY(up(c->alphal, a->alphal, ne));
+  TRY(up(c->wsx1, a->wsx1, np));
+  TRY(up(c->wsy1, a->wsy1, np));
+  TRY(up(c->wsx2, a->wsx2, np));
+  TRY(up(c->wsy2, a->wsy2, np));
+  TRY(up(c->pr1, a->pr1, np));
+  TRY(up(c->pr2, a->pr2, np));
+  TRY(up(c->gwce_lv, a->gwce_lv, np));
+  TRY(up(c->mom_x, a->mom_lv_x, np));
+  TRY(up(c->mom_y, a->mom_lv_y, np));
+  TRY(up(c->nodecode, a->nodecode, np));
+  TRY(up(c->nnodecode, a->nnodecode, np));
+  TRY(up(c->noff, a->noff, ne));
+  TRY(up(c->mju, a->mju, np));
+  // COEF(NP,MNEI): column 1 -> diag, other NeiTab slots -> SELL
+  std::vector<double> d(np), o(std::max(c->nnz_pad, 1), 0.0);
+  for (int i = 0; i < np; ++i) d[i] = a->coef[i];
+  for (int idx = 0; idx < c->nnz_pad; ++idx)
+    if (c->h_ell_of_sell[idx] >= 0) o[idx] = a->coef[c->h_ell_of_sell[idx]];
+  TRY(up(c->diag, d.data(), np));
+  TRY(up(c->offd, o.data(), c->nnz_pad));
+  TRY(up(c->obccoef, a->obccoef, (size_t)c->neta * (c->mnei - 1)));
+  return ADC_OK;
+}
+
+static int download_state(adc_ctx *c) {
+  adc_arrays_t *a = &c->host;
+  const int np = c->np, ne = c->ne;
+  ADC_CUDA(cudaStreamSynchronize(c->stream));
+  TRY(down(a->eta1, c->eta1, np));
+  TRY(down(a->eta2, c->eta2, np));
+  TRY(down(a->etas, c->etas, np));
+  TRY(down(a->uu1, c->uu1, np));
+  TRY(down(a->vv1, c->vv1, np));
+  TRY(down(a->uu2, c->uu2, np));
+  TRY(down(a->vv2, c->vv2, np));
+  TRY(down(a->qx1, c->qx1, np));
+  TRY(down(a->qy1, c->qy1, np));
+  TRY(down(a->qx2, c->qx2, np));
+  TRY(down(a->qy2, c->qy2, np));
+  TRY(down(a->h1, c->h1, np));
+  TRY(down(a->h2, c->h2, np));
+  TRY(down(a->tk, c->tk, np));
+  TRY(down(a->tkm, c->tkm, 3 * (size_t)np));
+  TRY(down(a->totalarea, c->totalarea, np));
+  TRY(down(a->alphal, c->alphal, ne));
+  TRY(down(a->wsx1, c->wsx1, np));
+  TRY(down(a->wsy1, c->wsy1, np));
+  TRY(down(a->wsx2, c->wsx2, np));
+  TRY(down(a->wsy2, c->wsy2, np));
+  TRY(down(a->pr1, c->pr1, np));
+  TRY(down(a->pr2, c->pr2, np));
+  TRY(down(a->gwce_lv, c->gwce_lv, np));
+  TRY(down(a->mom_lv_x, c->mom_x, np));
+  TRY(down(a->mom_lv_y, c->mom_y, np));
+  TRY(down(a->nodecode, c->nodecode, np));
+  TRY(down(a->nnodecode, c->nnodecode, np));
+  TRY(down(a->noff, c->noff, ne));
+  TRY(down(a->mju, c->mju, np));
+  if (a->coef) {
+    std::vector<double> d(np), o(std::max(c->nnz_pad, 1));
+    TRY(down(d.data(), c->diag, np));
+    TRY(down(o.data(), c->offd, c->nnz_pad));
+    std::fill(a->coef, a->coef + (size_t)np * c->mnei, 0.0);
+    for (int i = 0; i < np; ++i) a->coef[i] = d[i];
+    for (int idx = 0; idx < c->nnz_pad; ++idx)
+      if (c->h_ell_of_sell[idx] >= 0) a->coef[c->h_ell_of_sell[idx]] = o[idx];
+  }
+  TRY(down(a->obccoef, c->obccoef, (size_t)c->neta * (c->mnei - 1)));
+  return ADC_OK;
+}
+
+static void free_ctx(adc_ctx *c) {
+  if (!c) return;
+  void **ptrs[] = {
+      (void **)&c->x, (void **)&c->y, (void **)&c->dp, (void **)&c->tau0, (void **)&c->evm,
+      (void **)&c->fric, (void **)&c->corif, (void **)&c->nneigh, (void **)&c->nm,
+      (void **)&c->fdx, (void **)&c->fdy, (void **)&c->areas, (void **)&c->n2e_ptr,
+      (void **)&c->n2e, (void **)&c->sl_ptr, (void **)&c->sl_w, (void **)&c->col,
+      (void **)&c->rlen, (void **)&c->lhs_src, (void **)&c->nbd, (void **)&c->is_nbd,
+      (void **)&c->amig, (void **)&c->per, (void **)&c->face, (void **)&c->ff,
+      (void **)&c->emo, (void **)&c->efa, (void **)&c->obc_slot, (void **)&c->obc_zero,
+      (void **)&c->obc_rhs_ptr, (void **)&c->obc_rhs_node, (void **)&c->obc_rhs_ent,
+      (void **)&c->obc_rhs_b, (void **)&c->me_of_node, (void **)&c->me_lbc,
+      (void **)&c->me_csi, (void **)&c->me_sii, (void **)&c->eta1, (void **)&c->eta2,
+      (void **)&c->etas, (void **)&c->uu1, (void **)&c->vv1, (void **)&c->uu2, (void **)&c->vv2,
+      (void **)&c->qx1, (void **)&c->qy1, (void **)&c->qx2, (void **)&c->qy2, (void **)&c->h1,
+      (void **)&c->h2, (void **)&c->tk, (void **)&c->tkm, (void **)&c->totalarea,
+      (void **)&c->alphal, (void **)&c->wsx1, (void **)&c->wsy1, (void **)&c->wsx2,
+      (void **)&c->wsy2, (void **)&c->pr1, (void **)&c->pr2, (void **)&c->gwce_lv,
+      (void **)&c->mom_x, (void **)&c->mom_y, (void **)&c->nodecode, (void **)&c->nnodecode,
+      (void **)&c->noff, (void **)&c->noffold, (void **)&c->mju, (void **)&c->ncele,
+      (void **)&c->diag, (void **)&c->offd, (void **)&c->obccoef, (void **)&c->ebuf,
+      (void **)&c->ebuf2, (void **)&c->red, (void **)&c->ev_cnt, (void **)&c->ev_a,
+      (void **)&c->ev_b, (void **)&c->ev_c, (void **)&c->ju1, (void **)&c->jd[0],
+      (void **)&c->jd[1], (void **)&c->jd[2], (void **)&c->jdt[0], (void **)&c->jdt[1],
+      (void **)&c->jw, (void **)&c->soff, (void **)&c->jpart, (void **)&c->jtri,
+      (void **)&c->itp, (void **)&c->bar, (void **)&c->flags, (void **)&c->steps,
+      (void **)&c->numitr_log, (void **)&c->met_wsx, (void **)&c->met_wsy,
+      (void **)&c->met_pr};
+  for (void **p : ptrs)
+    if (*p) { cudaFree(*p); *p = nullptr; }
+  if (c->graph_ok) cudaGraphExecDestroy(c->graph);
+  for (auto &e : c->ev)
+    if (e) cudaEventDestroy(e);
+  for (auto &e : c->run_ev)
+    if (e) cudaEventDestroy(e);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete[] c->h_ell_of_sell;
+  delete c;
+}
+
+static int bind_impl(const adc_params_t *p, const adc_arrays_t *a, int prec, adc_ctx **out) {
+  if (!p || !a || !out) { set_error("null argument"); return ADC_ERR_ARG; }
+  if (a->np <= 0 || a->ne <= 0 || a->mnei < 2 || a->neta < 0 || a->nbfr < 0) {
+    set_error("invalid sizes"); return ADC_ERR_ARG;
+  }
+  if (prec != ADC_PREC_FP64 && prec != ADC_PREC_MIXED) { set_error("bad precision mode"); return ADC_ERR_ARG; }
+  if (p->itmax < 0 || p->dt <= 0.0) { set_error("invalid parameters"); return ADC_ERR_ARG; }
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    set_error("no CUDA device available");
+    return ADC_ERR_CUDA;
+  }
+  HostTables T;
+  int nslices = 0, nnz_pad = 0;
+  TRY(build_tables(a, T, nslices, nnz_pad));
+  adc_ctx *c = new adc_ctx();
+  memset((void *)c, 0, sizeof(*c));
+  *out = nullptr;
+  c->np = a->np; c->ne = a->ne; c->mnei = a->mnei; c->neta = a->neta; c->nbfr = a->nbfr;
+  c->nvel = a->nvel; c->nvelme = a->nvelme; c->prec = prec; c->itmax = p->itmax;
+  c->p = *p;
+  c->host = *a;
+  c->nslices = nslices;
+  c->nnz_pad = nnz_pad;
+  c->n_obc = a->neta * (a->mnei - 1);
+  c->n_obc_rhs_nodes = (int)T.obc_rhs_node.size();
+  c->n_me = (int)T.me_lbc.size();
+  c->h_ell_of_sell = new int[std::max(nnz_pad, 1)];
+  std::copy(T.ell_of_sell.begin(), T.ell_of_sell.end(), c->h_ell_of_sell);
+  auto fail = [&](int rc) { free_ctx(c); return rc; };
+#define B(x) do { int rc_ = (x); if (rc_) return fail(rc_); } while (0)
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) return fail(ADC_ERR_CUDA);
+  for (auto &e : c->ev) cudaEventCreate(&e);
+  for (auto &e : c->run_ev) cudaEventCreate(&e);
+  const int np = c->np, ne = c->ne;
+  B(dalloc(&c->x, np)); B(up(c->x, a->x, np));
+  B(dalloc(&c->y, np)); B(up(c->y, a->y, np));
+  B(dalloc(&c->dp, np)); B(up(c->dp, a->dp, np));
+  B(dalloc(&c->tau0, np)); B(up(c->tau0, a->tau0var, np));
+  B(dalloc(&c->evm, np)); B(up(c->evm, a->evm, np));
+  B(dalloc(&c->fric, np)); B(up(c->fric, a->fric, np));
+  B(dalloc(&c->corif, np)); B(up(c->corif, a->corif, np));
+  B(dalloc(&c->nneigh, np)); B(up(c->nneigh, a->nneigh, np));
+  B(dalloc(&c->nm, 3 * (size_t)ne)); B(up(c->nm, T.nm.data(), T.nm.size()));
+  B(dalloc(&c->fdx, 3 * (size_t)ne)); B(up(c->fdx, a->fdxe, 3 * (size_t)ne));
+  B(dalloc(&c->fdy, 3 * (size_t)ne)); B(up(c->fdy, a->fdye, 3 * (size_t)ne));
+  B(dalloc(&c->areas, ne)); B(up(c->areas, a->areas, ne));
+  B(dalloc(&c->n2e_ptr, np + 1)); B(up(c->n2e_ptr, T.n2e_ptr.data(), np + 1));
+  B(dalloc(&c->n2e, 3 * (size_t)ne)); B(up(c->n2e, T.n2e.data(), T.n2e.size()));
+  B(dalloc(&c->sl_ptr, nslices + 1)); B(up(c->sl_ptr, T.sl_ptr.data(), nslices + 1));
+  B(dalloc(&c->sl_w, nslices)); B(up(c->sl_w, T.sl_w.data(), nslices));
+  B(dalloc(&c->col, std::max(nnz_pad, 1))); B(up(c->col, T.col.data(), T.col.size()));
+  B(dalloc(&c->rlen, np)); B(up(c->rlen, T.rlen.data(), np));
+  B(dalloc(&c->lhs_src, T.lhs_src.size())); B(up(c->lhs_src, T.lhs_src.data(), T.lhs_src.size()));
+  B(dalloc(&c->nbd, T.nbd.size())); B(up(c->nbd, T.nbd.data(), T.nbd.size()));
+  B(dalloc(&c->is_nbd, np)); B(up(c->is_nbd, T.is_nbd.data(), np));
+  int nbfr = std::max(a->nbfr, 1), neta = std::max(a->neta, 1);
+  B(dalloc(&c->amig, nbfr)); B(dalloc(&c->per, nbfr)); B(dalloc(&c->face, nbfr)); B(dalloc(&c->ff, nbfr));
+  B(dalloc(&c->emo, (size_t)nbfr * neta)); B(dalloc(&c->efa, (size_t)nbfr * neta));
+  if (a->nbfr > 0) {
+    B(up(c->amig, a->amig, a->nbfr)); B(up(c->per, a->per, a->nbfr));
+    B(up(c->face, a->face, a->nbfr)); B(up(c->ff, a->ff, a->nbfr));
+    B(up(c->emo, a->emo, (size_t)a->nbfr * a->neta)); B(up(c->efa, a->efa, (size_t)a->nbfr * a->neta));
+  }
+  B(dalloc(&c->obc_slot, T.obc_slot.size())); B(up(c->obc_slot, T.obc_slot.data(), T.obc_slot.size()));
+  B(dalloc(&c->obc_zero, T.obc_zero.size())); B(up(c->obc_zero, T.obc_zero.data(), T.obc_zero.size()));
+  B(dalloc(&c->obc_rhs_ptr, T.obc_rhs_ptr.size())); B(up(c->obc_rhs_ptr, T.obc_rhs_ptr.data(), T.obc_rhs_ptr.size()));
+  B(dalloc(&c->obc_rhs_node, std::max<size_t>(T.obc_rhs_node.size(), 1))); B(up(c->obc_rhs_node, T.obc_rhs_node.data(), T.obc_rhs_node.size()));
+  B(dalloc(&c->obc_rhs_ent, std::max<size_t>(T.obc_rhs_ent.size(), 1))); B(up(c->obc_rhs_ent, T.obc_rhs_ent.data(), T.obc_rhs_ent.size()));
+  B(dalloc(&c->obc_rhs_b, std::max<size_t>(T.obc_rhs_b.size(), 1))); B(up(c->obc_rhs_b, T.obc_rhs_b.data(), T.obc_rhs_b.size()));
+  B(dalloc(&c->me_of_node, np)); B(up(c->me_of_node, T.me_of_node.data(), np));
+  B(dalloc(&c->me_lbc, std::max<size_t>(T.me_lbc.size(), 1))); B(up(c->me_lbc, T.me_lbc.data(), T.me_lbc.size()));
+  B(dalloc(&c->me_csi, std::max<size_t>(T.me_csi.size(), 1))); B(up(c->me_csi, T.me_csi.data(), T.me_csi.size()));
+  B(dalloc(&c->me_sii, std::max<size_t>(T.me_sii.size(), 1))); B(up(c->me_sii, T.me_sii.data(), T.me_sii.size()));
+  double **node_f64[] = {&c->eta1, &c->eta2, &c->etas, &c->uu1, &c->vv1, &c->uu2, &c->vv2, &c->qx1,
+                         &c->qy1, &c->qx2, &c->qy2, &c->h1, &c->h2, &c->tk, &c->totalarea,
+                         &c->wsx1, &c->wsy1, &c->wsx2, &c->wsy2, &c->pr1, &c->pr2, &c->gwce_lv,
+                         &c->mom_x, &c->mom_y, &c->diag, &c->ju1, &c->jd[0], &c->jd[1], &c->jd[2],
+                         &c->jdt[0], &c->jdt[1], &c->jw, &c->met_wsx, &c->met_wsy, &c->met_pr};
+  for (double **q : node_f64) B(dalloc(q, np));
+  B(dalloc(&c->tkm, 3 * (size_t)np));
+  B(dalloc(&c->alphal, ne));
+  int **node_i32[] = {&c->nodecode, &c->nnodecode, &c->mju};
+  for (int **q : node_i32) B(dalloc(q, np));
+  B(dalloc(&c->noff, ne)); B(dalloc(&c->noffold, ne)); B(dalloc(&c->ncele, ne));
+  B(dalloc(&c->offd, std::max(nnz_pad, 1))); B(dalloc(&c->soff, std::max(nnz_pad, 1)));
+  B(dalloc(&c->obccoef, (size_t)std::max(c->n_obc, 1)));
+  B(dalloc(&c->ebuf, 9 * (size_t)ne)); B(dalloc(&c->ebuf2, 3 * (size_t)ne));
+  B(dalloc(&c->red, nblk(np) + 64));
+  c->ev_blocks = (ne + 255) / 256;
+  B(dalloc(&c->ev_cnt, c->ev_blocks));
+  B(dalloc(&c->ev_a, (size_t)c->ev_blocks * 256)); B(dalloc(&c->ev_b, (size_t)c->ev_blocks * 256));
+  B(dalloc(&c->ev_c, (size_t)c->ev_blocks * 256));
+  B(jcg_setup_grid(c));
+  B(dalloc(&c->jpart, 4 * (size_t)c->jcg_grid));
+  B(dalloc(&c->jtri, 4 * (size_t)std::max(c->itmax, 2)));
+  B(dalloc(&c->itp, 1)); B(dalloc(&c->bar, 1));
+  {
+    // Flags followed by the rebuild word.
+    char *f = nullptr;
+    if (cudaMalloc((void **)&f, sizeof(Flags) + 64) != cudaSuccess) return fail(ADC_ERR_NOMEM);
+    c->flags = (Flags *)f;
+  }
+  c->steps_cap = 1;
+  B(dalloc(&c->steps, 1));
+  c->numitr_cap = 1;
+  B(dalloc(&c->numitr_log, 1));
+  B(upload_state(c));
+  Itp itp;
+  memset(&itp, 0, sizeof(itp));
+  itp.rparm1 = p->convcr;
+  itp.srelpr = DBL_EPSILON;
+  itp.itmax = p->itmax;
+  B(up(c->itp, &itp, 1));
+  Bar bar = {0, 0};
+  B(up(c->bar, &bar, 1));
+  Flags fl;
+  memset(&fl, 0, sizeof(fl));
+  fl.ncchange = 1;   // adcirc.F:404: the matrix is built on the first step
+  B(up(c->flags, &fl, 1));
+  int zero = 0;
+  B(up(rebuild_flag(c), &zero, 1));
+  ADC_CUDA(cudaDeviceSynchronize());
+#undef B
+  *out = c;
+  return ADC_OK;
+}
+
+static int read_flags(adc_ctx *c, Flags &f) {
+  ADC_CUDA(cudaMemcpyAsync(&f, c->flags, sizeof(Flags), cudaMemcpyDeviceToHost, c->stream));
+  ADC_CUDA(cudaStreamSynchronize(c->stream));
+  if (f.timeout) { set_error("a bounded device-side wait expired"); return ADC_ERR_TIMEOUT; }
+  return ADC_OK;
+}
+
+static void fill_out(const Flags &f, adc_stepout_t *out) {
+  if (!out) return;
+  memset(out, 0, sizeof(*out));
+  out->numitr = f.numitr;
+  out->ier = f.ier;
+  out->ncchange = f.ncchange;
+  out->status = f.status;
+  out->ep = f.ep;
+  out->n_w1_events = f.n_w1_events;
+  out->zeta = f.zeta;
+  out->cme = f.cme;
+}
+
+static int set_single_step(adc_ctx *c, const adc_step_t *s) {
+  if (!s) { set_error("null step"); return ADC_ERR_ARG; }
+  ADC_CUDA(cudaMemcpyAsync(c->steps, s, sizeof(adc_step_t), cudaMemcpyHostToDevice, c->stream));
+  int zero = 0;
+  ADC_CUDA(cudaMemcpyAsync(&c->flags->cursor, &zero, sizeof(int), cudaMemcpyHostToDevice, c->stream));
+  ADC_CUDA(cudaStreamSynchronize(c->stream));
+  return ADC_OK;
+}
+
+}  // namespace adc
+
+using namespace adc;
+
+extern "C" {
+
+const char *adc_last_error(void) { return g_err.c_str(); }
+
+int adc_gpu_bind(const adc_params_t *p, const adc_arrays_t *a, int prec, adc_ctx **out) {
+  return bind_impl(p, a, prec, out);
+}
+
+int adc_gpu_free(adc_ctx *c) {
+  if (!c) return ADC_ERR_ARG;
+  cudaStreamSynchronize(c->stream);
+  free_ctx(c);
+  return ADC_OK;
+}
+
+int adc_shift_friction(adc_ctx *c, const adc_step_t *s) {
+  if (!c) return ADC_ERR_ARG;
+  TRY(set_single_step(c, s));
+  TRY(launch_shift_friction(c));
+  c->met_pending = 0;
+  ADC_CUDA(cudaGetLastError());
+  ADC_CUDA(cudaStreamSynchronize(c->stream));
+  return ADC_OK;
+}
+
+int adc_gwce_new(adc_ctx *c, const adc_step_t *s, adc_stepout_t *out) {
+  if (!c) return ADC_ERR_ARG;
+  TRY(set_single_step(c, s));
+  TRY(launch_gwce_lhs(c));
+  TRY(launch_gwce_rhs(c));
+  TRY(launch_jcg(c, 1));
+  ADC_CUDA(cudaGetLastError());
+  Flags f;
+  TRY(read_flags(c, f));
+  fill_out(f, out);
+  return f.status ? ADC_ERR_DIAG : ADC_OK;
+}
+
+int adc_wetdry(adc_ctx *c, const adc_step_t *s, adc_stepout_t *out) {
+  if (!c) return ADC_ERR_ARG;
+  TRY(set_single_step(c, s));
+  TRY(launch_wetdry(c));
+  ADC_CUDA(cudaGetLastError());
+  Flags f;
+  TRY(read_flags(c, f));
+  fill_out(f, out);
+  return ADC_OK;
+}
+
+int adc_momentum(adc_ctx *c, const adc_step_t *s) {
+  if (!c) return ADC_ERR_ARG;
+  TRY(set_single_step(c, s));
+  TRY(launch_momentum(c));
+  ADC_CUDA(cudaGetLastError());
+  ADC_CUDA(cudaStreamSynchronize(c->stream));
+  return ADC_OK;
+}
+
+int adc_timestep(adc_ctx *c, const adc_step_t *s, adc_stepout_t *out) {
+  if (!c) return ADC_ERR_ARG;
+  TRY(set_single_step(c, s));
+  TRY(enqueue_step(c, true));
+  c->met_pending = 0;
+  ADC_CUDA(cudaGetLastError());
+  Flags f;
+  TRY(read_flags(c, f));
+  fill_out(f, out);
+  return f.status ? ADC_ERR_DIAG : ADC_OK;
+}
+
+int adc_run(adc_ctx *c, int nsteps, const adc_step_t *steps, int *numitr, adc_stepout_t *last) {
+  if (!c || nsteps < 0 || (nsteps > 0 && !steps)) { set_error("bad arguments"); return ADC_ERR_ARG; }
+  if (nsteps == 0) return ADC_OK;
+  if (c->met_pending) { set_error("adc_run does not take per-step host met forcing"); return ADC_ERR_UNSUPPORTED; }
+  if (nsteps > c->steps_cap) {
+    cudaFree(c->steps);
+    c->steps = nullptr;
+    TRY(dalloc(&c->steps, nsteps));
+    c->steps_cap = nsteps;
+    if (c->graph_ok) { cudaGraphExecDestroy(c->graph); c->graph_ok = 0; }
+  }
+  if (nsteps > c->numitr_cap) {
+    cudaFree(c->numitr_log);
+    c->numitr_log = nullptr;
+    TRY(dalloc(&c->numitr_log, nsteps));
+    c->numitr_cap = nsteps;
+    if (c->graph_ok) { cudaGraphExecDestroy(c->graph); c->graph_ok = 0; }
+  }
+  ADC_CUDA(cudaMemcpyAsync(c->steps, steps, nsteps * sizeof(adc_step_t), cudaMemcpyHostToDevice, c->stream));
+  int zero = 0;
+  ADC_CUDA(cudaMemcpyAsync(&c->flags->cursor, &zero, sizeof(int), cudaMemcpyHostToDevice, c->stream));
+  if (!c->graph_ok) {
+    cudaGraph_t g;
+    int64_t l0 = c->launches;
+    cudaError_t e = cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal);
+    int rc = ADC_OK;
+    if (e == cudaSuccess) {
+      rc = enqueue_step(c, false);
+      k_step_end<<<1, 1, 0, c->stream>>>(c->flags, c->numitr_log, c->numitr_cap);
+      e = cudaStreamEndCapture(c->stream, &g);
+    }
+    c->graph_launches = (int)(c->launches - l0) + 1;
+    c->launches = l0;
+    if (e == cudaSuccess && rc == ADC_OK) {
+      e = cudaGraphInstantiate(&c->graph, g, 0);
+      cudaGraphDestroy(g);
+      c->graph_ok = (e == cudaSuccess);
+    }
+    cudaGetLastError();
+  }
+  ADC_CUDA(cudaEventRecord(c->run_ev[0], c->stream));
+  for (int k = 0; k < nsteps; ++k) {
+    if (c->graph_ok) {
+      ADC_CUDA(cudaGraphLaunch(c->graph, c->stream));
+      c->launches += c->graph_launches;
+    } else {
+      TRY(enqueue_step(c, false));
+      k_step_end<<<1, 1, 0, c->stream>>>(c->flags, c->numitr_log, c->numitr_cap);
+      c->launches++;
+    }
+  }
+  ADC_CUDA(cudaEventRecord(c->run_ev[1], c->stream));
+  ADC_CUDA(cudaGetLastError());
+  Flags f;
+  TRY(read_flags(c, f));
+  {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, c->run_ev[0], c->run_ev[1]);
+    c->last_run_ms = ms;
+  }
+  if (numitr) ADC_CUDA(cudaMemcpy(numitr, c->numitr_log, nsteps * sizeof(int), cudaMemcpyDeviceToHost));
+  fill_out(f, last);
+  return f.status ? ADC_ERR_DIAG : ADC_OK;
+}
+
+int adc_sync_to_host(adc_ctx *c) {
+  if (!c) return ADC_ERR_ARG;
+  return download_state(c);
+}
+
+int adc_sync_from_host(adc_ctx *c) {
+  if (!c) return ADC_ERR_ARG;
+  ADC_CUDA(cudaStreamSynchronize(c->stream));
+  return upload_state(c);
+}
+
+int adc_set_met(adc_ctx *c, const double *wsx2, const double *wsy2, const double *pr2) {
+  if (!c || !wsx2 || !wsy2 || !pr2) return ADC_ERR_ARG;
+  if (c->p.nws == 0) { set_error("met forcing given but NWS = 0"); return ADC_ERR_ARG; }
+  ADC_CUDA(cudaMemcpyAsync(c->met_wsx, wsx2, c->np * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  ADC_CUDA(cudaMemcpyAsync(c->met_wsy, wsy2, c->np * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  ADC_CUDA(cudaMemcpyAsync(c->met_pr, pr2, c->np * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  c->met_pending = 1;
+  return ADC_OK;
+}
+
+int adc_phase_times(adc_ctx *c, double *ms_shift, double *ms_gwce, double *ms_jcg,
+                    double *ms_wetdry, double *ms_momentum) {
+  if (!c) return ADC_ERR_ARG;
+  float t[5] = {0, 0, 0, 0, 0};
+  for (int k = 0; k < 5; ++k) cudaEventElapsedTime(&t[k], c->ev[k], c->ev[k + 1]);
+  if (ms_shift) *ms_shift = t[0];
+  if (ms_gwce) *ms_gwce = t[1];
+  if (ms_jcg) *ms_jcg = t[2];
+  if (ms_wetdry) *ms_wetdry = t[3];
+  if (ms_momentum) *ms_momentum = t[4];
+  return ADC_OK;
+}
+
+int64_t adc_launch_count(adc_ctx *c) { return c ? c->launches : -1; }
+
+double adc_last_run_ms(adc_ctx *c) { return c ? c->last_run_ms : -1.0; }
+
+}  // extern "C"

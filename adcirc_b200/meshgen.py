@@ -1,0 +1,334 @@
+"""Seeded synthetic meshes for the 2DDI hot path.
+
+The benchmark meshes are synthetic by specification (no external dataset is
+involved): a structured tidal channel (4,961 nodes), a small beach channel
+with wetting/drying for parity tests, and a graded ~600k-node storm-surge
+mesh.  Each generator returns a ``RawMesh``: node coordinates, bathymetric
+depth (positive down, ADCIRC's DP), counter-clockwise triangles, one
+elevation-specified (open) boundary and the land boundary segments with
+their ADCIRC IBTYPE codes, listed counter-clockwise (domain on the left) as
+in fort.14.
+"""
+from __future__ import annotations
+
+import dataclasses
+import numpy as np
+
+
+@dataclasses.dataclass
+class RawMesh:
+    name: str
+    x: np.ndarray          # (NP,) float64 [m]
+    y: np.ndarray          # (NP,) float64 [m]
+    dp: np.ndarray         # (NP,) float64, depth below datum [m]
+    nm: np.ndarray         # (NE,3) int, 0-based node ids
+    open_nodes: np.ndarray  # elevation boundary node ids (0-based), in order
+    land_segments: list    # list of (ibtype, node id array (0-based))
+    meta: dict
+
+
+def channel_mesh(nx: int = 121, ny: int = 41, lx: float = 60e3, ly: float = 20e3,
+                 depth0: float = 20.0, depth1: float = 5.0) -> RawMesh:
+    """Structured right-triangle channel: the 2DDI tidal channel case.
+
+    Nodes are numbered column by column (x fastest along y); the open
+    boundary is the x = 0 edge, the other three sides are mainland
+    (IBTYPE 0).  Depth varies linearly in x from ``depth0`` to ``depth1``.
+    """
+    xs = np.linspace(0.0, lx, nx)
+    ys = np.linspace(0.0, ly, ny)
+    X, Y = np.meshgrid(xs, ys, indexing="ij")  # (nx, ny)
+    x = X.ravel().astype(np.float64)
+    y = Y.ravel().astype(np.float64)
+    dp = depth0 + (depth1 - depth0) * (x / lx)
+
+    def nid(i, j):
+        return i * ny + j
+
+    tris = []
+    for i in range(nx - 1):
+        for j in range(ny - 1):
+            a, b, c, d = nid(i, j), nid(i + 1, j), nid(i + 1, j + 1), nid(i, j + 1)
+            tris.append((a, b, c))
+            tris.append((a, c, d))
+    nm = np.asarray(tris, dtype=np.int64)
+    # open boundary: x = 0, from top (0, ly) down to (0, 0)
+    open_nodes = np.array([nid(0, j) for j in range(ny - 1, -1, -1)], dtype=np.int64)
+    # mainland: (0,0) -> (lx,0) -> (lx,ly) -> (0,ly), counter-clockwise
+    land = [nid(i, 0) for i in range(nx)]
+    land += [nid(nx - 1, j) for j in range(1, ny)]
+    land += [nid(i, ny - 1) for i in range(nx - 2, -1, -1)]
+    return RawMesh("channel", x, y, dp, nm, open_nodes,
+                   [(0, np.asarray(land, dtype=np.int64))],
+                   {"nx": nx, "ny": ny, "lx": lx, "ly": ly})
+
+
+def beach_mesh(nx: int = 41, ny: int = 13, lx: float = 4e3, ly: float = 1.2e3,
+               depth0: float = 3.0, depth1: float = -1.5) -> RawMesh:
+    """Small sloping-beach channel whose closed end rises above the datum.
+
+    The tide floods and drains the upper beach, so every wet/dry branch
+    of the path (D1, W1, DE1, D2, the slope limiter) is exercised on a
+    mesh the oracle steps in well under a second.
+    """
+    m = channel_mesh(nx, ny, lx, ly, depth0, depth1)
+    # a gentle cross-channel bump so fronts are not aligned with the grid
+    m.dp = m.dp + 0.4 * np.sin(2.0 * np.pi * m.y / ly) * (m.x / lx)
+    m.name = "beach"
+    return m
+
+
+# --------------------------------------------------------------------------
+# Graded storm-surge mesh
+# --------------------------------------------------------------------------
+
+def _coastline(rng, lx, y0, amp, nmodes=400, beta=1.35):
+    k = np.arange(1, nmodes + 1, dtype=np.float64)
+    a = amp * k ** (-beta) * rng.standard_normal(nmodes)
+    ph = rng.uniform(0.0, 2.0 * np.pi, nmodes)
+
+    def yc(x):
+        x = np.asarray(x, dtype=np.float64)
+        s = np.zeros_like(x)
+        for kk, aa, pp in zip(k, a, ph):
+            s += aa * np.sin(2.0 * np.pi * kk * x / lx + pp)
+        return y0 + s
+    return yc
+
+
+def _grf(rng, lx, ly, dx, sigma, ell):
+    nx = int(np.ceil(lx / dx)) + 1
+    ny = int(np.ceil(ly / dx)) + 1
+    w = rng.standard_normal((nx, ny))
+    kx = np.fft.fftfreq(nx, d=dx) * 2 * np.pi
+    ky = np.fft.rfftfreq(ny, d=dx) * 2 * np.pi
+    KX, KY = np.meshgrid(kx, ky, indexing="ij")
+    filt = np.exp(-0.25 * (KX ** 2 + KY ** 2) * ell ** 2)
+    f = np.fft.irfft2(np.fft.rfft2(w) * filt, s=(nx, ny))
+    f *= sigma / max(f.std(), 1e-30)
+
+    def ev(x, y):
+        fx = np.clip(x / dx, 0, nx - 1.000001)
+        fy = np.clip(y / dx, 0, ny - 1.000001)
+        i = fx.astype(np.int64)
+        j = fy.astype(np.int64)
+        tx = fx - i
+        ty = fy - j
+        return ((1 - tx) * (1 - ty) * f[i, j] + tx * (1 - ty) * f[i + 1, j]
+                + (1 - tx) * ty * f[i, j + 1] + tx * ty * f[i + 1, j + 1])
+    return ev
+
+
+def _quadtree_leaves(lx, ly, h_fn, root):
+    """Cells split until their size is below the target edge length."""
+    nx0 = int(round(lx / root))
+    ny0 = int(round(ly / root))
+    I, J = np.meshgrid(np.arange(nx0), np.arange(ny0), indexing="ij")
+    cx = (I.ravel() + 0.5) * root
+    cy = (J.ravel() + 0.5) * root
+    size = np.full(cx.shape, root)
+    leaves = []
+    while cx.size:
+        h = h_fn(cx, cy, size)
+        split = size > h
+        leaves.append((cx[~split], cy[~split], size[~split]))
+        cx, cy, size = cx[split], cy[split], size[split]
+        if not cx.size:
+            break
+        q = size / 4.0
+        cx = np.concatenate([cx - q, cx + q, cx - q, cx + q])
+        cy = np.concatenate([cy - q, cy - q, cy + q, cy + q])
+        size = np.concatenate([size, size, size, size]) / 2.0
+    return (np.concatenate([l[0] for l in leaves]), np.concatenate([l[1] for l in leaves]),
+            np.concatenate([l[2] for l in leaves]))
+
+
+def surge_mesh(seed: int = 2024, target_nodes: int = 600_000, lx: float = 1000e3,
+               ly: float = 800e3, h_min: float = 60.0, h_max: float = 20e3,
+               coast_y: float = 640e3, coast_amp: float = 40e3,
+               shelf_width: float = 100e3, shelf_depth: float = 30.0,
+               ocean_depth: float = 4000.0, land_height: float = 6.0,
+               grf_sigma: float = 2.0, grf_ell: float = 5e3,
+               land_grading: float = 3.0) -> RawMesh:
+    """Graded storm-surge mesh (~600k nodes, ~1.18M triangles).
+
+    Points: seeded jittered quadtree sampling whose cell size follows the
+    target edge length h = min(h_max, h_min + alpha * d), d the distance to a
+    seeded fractal coastline (a stand-in for Poisson-disk sampling with the
+    same grading; the floodplain grades land_grading times faster); alpha is
+    bisected so the node count meets the target.
+    Triangles: Delaunay (scipy).  Bathymetry: shelf profile (ocean_depth
+    offshore, shelf break shelf_width offshore at shelf_depth, 0 m at the
+    coast, land rising to land_height) plus a Gaussian random field.
+    Open boundary: the south edge; the other sides are mainland (IBTYPE 0).
+    """
+    from scipy.spatial import Delaunay
+
+    rng = np.random.default_rng(seed)
+    yc = _coastline(rng, lx, coast_y, coast_amp)
+    # coastline sampled once for fast distance evaluation (vertical proxy)
+    xs = np.linspace(0, lx, 20001)
+    ycs = yc(xs)
+
+    def coast_at(x):
+        return np.interp(x, xs, ycs)
+
+    def make_h(alpha):
+        def h_fn(cx, cy, size):
+            s = coast_at(cx) - cy                  # > 0 offshore
+            d = np.maximum(np.abs(s) - 0.75 * size, 0.0)   # nearest point of the cell
+            a = np.where(s < 0, land_grading * alpha, alpha)
+            return np.minimum(h_max, h_min + a * d)
+        return h_fn
+
+    lo, hi = 0.005, 0.5
+    for _ in range(30):
+        mid = np.sqrt(lo * hi)
+        cx, _, _ = _quadtree_leaves(lx, ly, make_h(mid), h_max)
+        if cx.size > target_nodes:
+            lo = mid
+        else:
+            hi = mid
+        if abs(cx.size - target_nodes) < 0.01 * target_nodes:
+            break
+    alpha = mid
+    cx, cy, size = _quadtree_leaves(lx, ly, make_h(alpha), h_max)
+    jit = 0.3
+    px = cx + size * rng.uniform(-jit, jit, cx.size)
+    py = cy + size * rng.uniform(-jit, jit, cy.size)
+    # keep interior points off the boundary
+    m = 0.2 * size
+    px = np.clip(px, m, lx - m)
+    py = np.clip(py, m, ly - m)
+    # boundary points, spacing follows the local cell size, bulged outward
+    # by a tiny convex offset so every boundary point is a hull vertex
+    def edge_pts(x0, y0, x1, y1, n_out):
+        pts = []
+        t = 0.0
+        L = np.hypot(x1 - x0, y1 - y0)
+        while t < L:
+            xx = x0 + (x1 - x0) * t / L
+            yy = y0 + (y1 - y0) * t / L
+            pts.append((xx, yy, t))
+            h = float(make_h(alpha)(np.array([xx]), np.array([yy]), np.array([0.0]))[0])
+            t += max(h, 1.0)
+        pts = np.asarray(pts)
+        s = pts[:, 2] / L
+        bulge = 1e-6 * L * s * (1 - s) * 4.0
+        return pts[:, 0] + n_out[0] * bulge, pts[:, 1] + n_out[1] * bulge
+    bx, by = [], []
+    for (x0, y0, x1, y1, n) in [(0, 0, lx, 0, (0, -1)), (lx, 0, lx, ly, (1, 0)),
+                                (lx, ly, 0, ly, (0, 1)), (0, ly, 0, 0, (-1, 0))]:
+        ex, ey = edge_pts(x0, y0, x1, y1, n)
+        bx.append(ex)
+        by.append(ey)
+    bx = np.concatenate(bx)
+    by = np.concatenate(by)
+    nb = bx.size
+    x = np.concatenate([bx, px])
+    y = np.concatenate([by, py])
+    tri = Delaunay(np.column_stack([x, y]))
+    nm = tri.simplices.astype(np.int64)
+    # orient counter-clockwise
+    x1, y1 = x[nm[:, 0]], y[nm[:, 0]]
+    x2, y2 = x[nm[:, 1]], y[nm[:, 1]]
+    x3, y3 = x[nm[:, 2]], y[nm[:, 2]]
+    a2 = (x2 - x1) * (y3 - y1) - (x3 - x1) * (y2 - y1)
+    flip = a2 < 0
+    nm[flip, 1], nm[flip, 2] = nm[flip, 2].copy(), nm[flip, 1].copy()
+    # drop degenerate triangles (zero area) if any
+    keep = np.abs(a2) > 1e-6 * np.median(np.abs(a2))
+    nm = nm[keep]
+    used = np.zeros(x.size, bool)
+    used[nm.ravel()] = True
+    if not used.all():
+        remap = -np.ones(x.size, np.int64)
+        remap[used] = np.arange(used.sum())
+        x, y = x[used], y[used]
+        nm = remap[nm]
+        nb = int(used[:nb].sum())
+    # renumber for memory locality: nodes along a Hilbert curve, elements by
+    # their lowest node
+    key = _hilbert_key(x, y, lx, ly)
+    perm = np.argsort(key, kind="stable")
+    inv = np.empty_like(perm)
+    inv[perm] = np.arange(perm.size)
+    x, y = x[perm], y[perm]
+    nm = inv[nm]
+    ekey = np.lexsort((nm.max(axis=1), nm.min(axis=1)))
+    nm = nm[ekey]
+    # bathymetry
+    grf = _grf(rng, lx, ly, 1250.0, grf_sigma, grf_ell)
+    s = coast_at(x) - y  # > 0 offshore
+    shelf = shelf_depth * np.sqrt(np.clip(s / shelf_width, 0.0, 1.0))
+    slope = 0.5 * (1 + np.tanh((s - shelf_width - 25e3) / 12e3))
+    depth = shelf + (ocean_depth - shelf_depth) * slope * (s > shelf_width)
+    land = s < 0
+    depth = np.where(land, -land_height * np.clip(-s / 20e3, 0.0, 1.0), depth)
+    depth = depth + grf(x, y) * np.clip(1.0 - s / (2 * shelf_width), 0.0, 1.0)
+    depth = np.clip(depth, -land_height, ocean_depth)
+    # boundary node lists from hull ordering (counter-clockwise)
+    bnd = _hull_loop(nm, x.size)
+    # start the loop at the south-west corner
+    corner = int(np.argmin(x[bnd] + y[bnd]))
+    bnd = np.roll(bnd, -corner)
+    # counter-clockwise: south edge first (increasing x)
+    if x[bnd[1]] < x[bnd[0]]:
+        bnd = np.concatenate([bnd[:1], bnd[1:][::-1]])
+    tol = 1.0
+    south = np.abs(y[bnd]) < tol + 1e-6 * lx
+    # open boundary: the south edge, listed as in fort.14 from east to west
+    # (so that the land boundary continues counter-clockwise from it)
+    i_end = int(np.argmax(~south[1:])) + 1  # first non-south after start
+    open_ccw = bnd[:i_end]                   # west -> east along the south edge
+    open_nodes = open_ccw[::-1]
+    land_nodes = np.concatenate([bnd[i_end - 1:], bnd[:1]])  # SE corner -> ... -> SW corner
+    meta = {"seed": seed, "alpha": float(alpha), "coast_y": coast_y, "lx": lx, "ly": ly}
+    rm = RawMesh("surge", x.astype(np.float64), y.astype(np.float64), depth.astype(np.float64),
+                 nm, open_nodes.astype(np.int64), [(0, land_nodes.astype(np.int64))], meta)
+    rm.meta["coast_fn"] = coast_at
+    return rm
+
+
+def _hilbert_key(x, y, lx, ly, order=16):
+    n = 1 << order
+    xi = np.clip((x / lx * (n - 1)).astype(np.int64), 0, n - 1)
+    yi = np.clip((y / ly * (n - 1)).astype(np.int64), 0, n - 1)
+    d = np.zeros_like(xi)
+    s = n >> 1
+    while s > 0:
+        rx = ((xi & s) > 0).astype(np.int64)
+        ry = ((yi & s) > 0).astype(np.int64)
+        d += s * s * ((3 * rx) ^ ry)
+        # rotate
+        mask = ry == 0
+        flip = mask & (rx == 1)
+        xi = np.where(flip, s - 1 - xi, xi)
+        yi = np.where(flip, s - 1 - yi, yi)
+        xi2 = np.where(mask, yi, xi)
+        yi2 = np.where(mask, xi, yi)
+        xi, yi = xi2, yi2
+        s >>= 1
+    return d
+
+
+def _hull_loop(nm, npts):
+    """Boundary edges (used by exactly one triangle) chained into a loop,
+    oriented counter-clockwise (interior on the left)."""
+    e = np.concatenate([nm[:, [0, 1]], nm[:, [1, 2]], nm[:, [2, 0]]])
+    key = np.minimum(e[:, 0], e[:, 1]) * npts + np.maximum(e[:, 0], e[:, 1])
+    uniq, cnt = np.unique(key, return_counts=True)
+    bkeys = set(uniq[cnt == 1].tolist())
+    nxt = {}
+    for a, b, k in zip(e[:, 0], e[:, 1], key):
+        if int(k) in bkeys:
+            nxt[int(a)] = int(b)  # ccw triangles: boundary edge a->b has interior on the left
+    start = next(iter(nxt))
+    loop = [start]
+    cur = nxt[start]
+    while cur != start:
+        loop.append(cur)
+        cur = nxt[cur]
+        if len(loop) > len(nxt) + 1:
+            raise RuntimeError("boundary is not a single loop")
+    return np.asarray(loop, dtype=np.int64)

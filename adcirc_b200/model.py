@@ -1,0 +1,338 @@
+"""Host-side case assembly: the module arrays ADCIRC_Init would have built.
+
+``build_case`` turns a ``RawMesh`` plus forcing and fort.15-style
+parameters into the full set of Fortran-layout arrays bound by
+``adc_gpu_bind`` (include/adcgpu.h): mesh tables (mesh.F), boundary tables
+(boundaries.F), nodal attributes, tidal forcing tables and the cold-start
+state (cstart.F).  ``GpuModel`` wraps the device-resident step API.
+"""
+from __future__ import annotations
+
+import copy
+import ctypes as C
+import dataclasses
+import math
+
+import numpy as np
+
+from . import _lib
+from ._lib import AdcArrays, AdcParams, AdcStep, AdcStepOut, dp_, ip_, ptr
+
+G_DEFAULT = 9.80665          # constants.F90:45
+RHOWAT0 = 1000.0             # constants.F90:48
+PRBCKGRND_MB = 1013.0        # constants.F90:55
+
+STATE_F64 = ("eta1", "eta2", "etas", "uu1", "vv1", "uu2", "vv2", "qx1", "qy1", "qx2", "qy2",
+             "h1", "h2", "tk", "tkm", "totalarea", "alphal", "wsx1", "wsy1", "wsx2", "wsy2",
+             "pr1", "pr2", "coef", "obccoef", "gwce_lv", "mom_lv_x", "mom_lv_y")
+STATE_I32 = ("nodecode", "nnodecode", "noff", "mju")
+
+
+@dataclasses.dataclass
+class Schedule:
+    """TIMESTEP time and ramp bookkeeping (timestep.F:257-353)."""
+    dt: float
+    statim: float = 0.0      # days
+    reftim: float = 0.0      # days
+    nramp: int = 1
+    dramp: float = 0.5       # days (elevation ramp, DRampElev)
+    dramp_mete: float = 0.5  # days
+    dunramp_mete: float = 0.0
+
+    def step(self, it: int) -> AdcStep:
+        timeloc = it * self.dt + self.statim * 86400.0
+        timeh = it * self.dt + (self.statim - self.reftim) * 86400.0
+        if self.nramp == 0:
+            relev = rmete = 1.0
+        else:
+            relev = math.tanh((2.0 * timeloc / 86400.0) / self.dramp)
+            rmete = math.tanh((2.0 * (timeloc / 86400.0 - self.dunramp_mete)) / self.dramp_mete)
+        if self.dramp < 1.0e-6:
+            relev = 1.0
+        if self.dramp_mete < 1.0e-6:
+            rmete = 1.0
+        s = AdcStep()
+        s.it = it
+        s.timeloc = timeloc
+        s.timeh = timeh
+        s.rampelev = relev
+        s.rampmete = rmete
+        return s
+
+    def steps(self, it0: int, n: int):
+        arr = (AdcStep * n)()
+        for k in range(n):
+            arr[k] = self.step(it0 + k)
+        return arr
+
+
+@dataclasses.dataclass
+class Case:
+    name: str
+    params: dict
+    sizes: dict
+    arrays: dict                 # name -> numpy array (Fortran layout)
+    schedule: Schedule
+    meta: dict = dataclasses.field(default_factory=dict)
+
+    def clone(self) -> "Case":
+        c = copy.copy(self)
+        c.arrays = {k: v.copy(order="F") for k, v in self.arrays.items()}
+        c.params = dict(self.params)
+        return c
+
+    def params_struct(self) -> AdcParams:
+        p = AdcParams()
+        for k, v in self.params.items():
+            setattr(p, k, v)
+        return p
+
+    def arrays_struct(self) -> AdcArrays:
+        a = AdcArrays()
+        for k in ("np", "ne", "mnei", "neta", "nbfr", "nvel", "nvelme"):
+            setattr(a, k, int(self.sizes[k]))
+        for name, typ in _lib.ARRAY_FIELDS:
+            arr = self.arrays[name]
+            want = np.int32 if typ is ip_ else np.float64
+            assert arr.dtype == want and arr.flags.f_contiguous, name
+            setattr(a, name, ptr(arr, typ))
+        return a
+
+    def state(self):
+        return {k: self.arrays[k] for k in STATE_F64 + STATE_I32}
+
+
+def default_params(dt: float, **kw) -> dict:
+    p = dict(dt=dt, g=G_DEFAULT, a00=0.35, b00=0.30, c00=0.35, h0=0.05, velmin=0.01,
+             slim=1.0e9, hbreak=1.0, ftheta=1.0, fgamma=1.0, convcr=1.0e-10,
+             prbckgrnd_mh2o=100.0 * PRBCKGRND_MB / (RHOWAT0 * G_DEFAULT),
+             ifnlfa=1, ifnlct=1, ifnlcat=1, nolifa=2, iflinbf=0, ifnlbf=1, ifhybf=0,
+             itmax=200, nws=0, ifwind=1, isldia=0, pad_=0)
+    p.update(kw)
+    return p
+
+
+def _f(a, dtype):
+    return np.asfortranarray(np.asarray(a, dtype=dtype))
+
+
+def build_case(raw, params: dict, schedule: Schedule, tides, cf: float = 0.0025,
+               tau0: float = 0.005, eslm: float = 5.0, cori: float = 1.0e-4,
+               anginn: float = 110.0, eta0=None) -> Case:
+    """Assemble every array the hot path binds.
+
+    tides: list of (amig [rad/s], face [rad], ff, emo (NETA,), efa (NETA,) [rad])
+    """
+    lib = _lib.load()
+    npn = int(raw.x.size)
+    ne = int(raw.nm.shape[0])
+    x = _f(raw.x, np.float64)
+    y = _f(raw.y, np.float64)
+    dp = _f(raw.dp, np.float64)
+    nm = _f(raw.nm + 1, np.int32)                      # NM(NE,3)
+    fdxe = np.zeros((3, ne), np.float64, order="F")
+    fdye = np.zeros((3, ne), np.float64, order="F")
+    areas = np.zeros(ne, np.float64)
+    rc = lib.adc_mesh_geometry(npn, ne, ptr(x, dp_), ptr(y, dp_), ptr(nm, ip_), ptr(fdxe, dp_),
+                               ptr(fdye, dp_), ptr(areas, dp_))
+    if rc != 0:
+        raise RuntimeError(f"adc_mesh_geometry failed: {rc}")
+    mnei = lib.adc_mesh_mnei(npn, ne, ptr(nm, ip_))
+    nneigh = np.zeros(npn, np.int32)
+    neitab = np.zeros((npn, mnei), np.int32, order="F")
+    neimax = C.c_int(0)
+    rc = lib.adc_mesh_neighb(npn, ne, mnei, ptr(x, dp_), ptr(y, dp_), ptr(nm, ip_),
+                             ptr(nneigh, ip_), ptr(neitab, ip_), C.byref(neimax))
+    if rc != 0:
+        raise RuntimeError(f"adc_mesh_neighb failed: {rc}")
+    csr = np.zeros((ne, 3, 2), np.int32, order="F")
+    rc = lib.adc_mesh_csr_positions(npn, ne, mnei, ptr(nm, ip_), ptr(neitab, ip_),
+                                    neimax.value, ptr(csr, ip_))
+    if rc != 0:
+        raise RuntimeError(f"adc_mesh_csr_positions failed: {rc}")
+    # boundaries
+    nbd = _f(raw.open_nodes + 1, np.int32)
+    neta = int(nbd.size)
+    ibtype = np.array([t for t, _ in raw.land_segments], np.int32)
+    segs = [np.asarray(s, np.int64) + 1 for _, s in raw.land_segments]
+    seg_ptr = np.zeros(len(segs) + 1, np.int32)
+    seg_ptr[1:] = np.cumsum([s.size for s in segs])
+    seg_nodes = np.concatenate(segs).astype(np.int32)
+    nvel_max = int(seg_nodes.size + len(segs) + 1)
+    nbv = np.zeros(nvel_max, np.int32)
+    lbc = np.zeros(nvel_max, np.int32)
+    csii = np.zeros(nvel_max, np.float64)
+    siii = np.zeros(nvel_max, np.float64)
+    me2gw = np.zeros(nvel_max, np.int32)
+    nvel = C.c_int(0)
+    nvelme = C.c_int(0)
+    rc = lib.adc_boundary_setup(npn, ptr(x, dp_), ptr(y, dp_), len(segs), ptr(ibtype, ip_),
+                                ptr(seg_ptr, ip_), ptr(seg_nodes, ip_),
+                                math.cos(anginn * math.pi / 180.0), nvel_max, C.byref(nvel),
+                                ptr(nbv, ip_), ptr(lbc, ip_), ptr(csii, dp_), ptr(siii, dp_),
+                                C.byref(nvelme), ptr(me2gw, ip_))
+    if rc != 0:
+        raise RuntimeError(f"adc_boundary_setup failed: {rc}")
+    nv, nme = nvel.value, nvelme.value
+    nbfr = len(tides)
+    amig = _f([t[0] for t in tides], np.float64)
+    face = _f([t[1] for t in tides], np.float64)
+    ff = _f([t[2] for t in tides], np.float64)
+    per = _f([2.0 * math.pi / t[0] if t[0] != 0 else 0.0 for t in tides], np.float64)
+    emo = np.zeros((max(nbfr, 1), max(neta, 1)), np.float64, order="F")
+    efa = np.zeros((max(nbfr, 1), max(neta, 1)), np.float64, order="F")
+    for j, t in enumerate(tides):
+        emo[j, :neta] = t[3]
+        efa[j, :neta] = t[4]
+    A = dict(
+        x=x, y=y, dp=dp, nm=nm, nneigh=nneigh, neitab=neitab, fdxe=fdxe, fdye=fdye,
+        areas=areas, csr_position=csr,
+        tau0var=np.full(npn, tau0), evm=np.full(npn, eslm), fric=np.full(npn, cf),
+        corif=np.full(npn, cori),
+        nbd=nbd, amig=amig if nbfr else _f([0.0], np.float64),
+        per=per if nbfr else _f([0.0], np.float64),
+        face=face if nbfr else _f([0.0], np.float64),
+        ff=ff if nbfr else _f([0.0], np.float64), emo=emo, efa=efa,
+        nbv=_f(nbv[:max(nv, 1)], np.int32), lbcodei=_f(lbc[:max(nv, 1)], np.int32),
+        csii=_f(csii[:max(nv, 1)], np.float64), siii=_f(siii[:max(nv, 1)], np.float64),
+        me2gw=_f(me2gw[:max(nme, 1)], np.int32),
+    )
+    for k in STATE_F64:
+        A[k] = np.zeros(npn, np.float64)
+    A["tkm"] = np.zeros((3, npn), np.float64, order="F")
+    A["alphal"] = np.ones(ne, np.float64)
+    A["coef"] = np.zeros((npn, mnei), np.float64, order="F")
+    A["obccoef"] = np.zeros((max(neta, 1), mnei - 1), np.float64, order="F")
+    for k in STATE_I32:
+        A[k] = np.zeros(npn, np.int32)
+    A["noff"] = np.ones(ne, np.int32)
+    prb = params["prbckgrnd_mh2o"]
+    A["pr1"][:] = prb
+    A["pr2"][:] = prb
+    if eta0 is not None:
+        A["eta2"][:] = eta0
+    rc = lib.adc_coldstart(npn, ne, params["nolifa"], params["h0"], ptr(dp, dp_), ptr(nm, ip_),
+                           ptr(areas, dp_), ptr(A["eta1"], dp_), ptr(A["eta2"], dp_),
+                           ptr(A["nnodecode"], ip_), ptr(A["nodecode"], ip_), ptr(A["noff"], ip_),
+                           ptr(A["mju"], ip_), ptr(A["totalarea"], dp_))
+    if rc != 0:
+        raise RuntimeError(f"adc_coldstart failed: {rc}")
+    for k, v in A.items():
+        if not v.flags.f_contiguous:
+            A[k] = np.asfortranarray(v)
+    sizes = dict(np=npn, ne=ne, mnei=mnei, neta=neta, nbfr=nbfr, nvel=nv, nvelme=nme,
+                 neimax=neimax.value)
+    return Case(raw.name, dict(params), sizes, A, schedule, dict(raw.meta))
+
+
+# --------------------------------------------------------------------------
+# Named cases
+# --------------------------------------------------------------------------
+
+M2_PERIOD = 44712.0
+K1_PERIOD = 86164.0
+
+
+def channel_case(dt: float = 5.0, amp: float = 0.5, **kw) -> Case:
+    """Tidal channel: 121x41 nodes, 20 m -> 5 m, M2 0.5 m, dt 5 s."""
+    from .meshgen import channel_mesh
+    raw = channel_mesh()
+    neta = raw.open_nodes.size
+    tides = [(2.0 * math.pi / M2_PERIOD, 0.0, 1.0, np.full(neta, amp), np.zeros(neta))]
+    params = default_params(dt, **kw)
+    return build_case(raw, params, Schedule(dt=dt, dramp=0.5), tides)
+
+
+def beach_case(dt: float = 2.0, amp: float = 0.5, period: float = 10800.0, **kw) -> Case:
+    """Small beach channel with wetting and drying (parity case).
+
+    A three-hour boundary oscillation starting at mean level on the rise
+    floods and drains the upper beach within a few hundred steps.
+    """
+    from .meshgen import beach_mesh
+    raw = beach_mesh()
+    neta = raw.open_nodes.size
+    tides = [(2.0 * math.pi / period, 0.0, 1.0, np.full(neta, amp), np.zeros(neta))]
+    params = default_params(dt, **kw)
+    sched = Schedule(dt=dt, statim=0.0, reftim=0.25 * period / 86400.0, nramp=0)
+    return build_case(raw, params, sched, tides)
+
+
+def surge_case(seed: int = 2024, target_nodes: int = 600_000, dt: float = 1.0, **kw) -> Case:
+    """Graded ~600k-node storm-surge mesh with M2 + K1 on the open boundary."""
+    from .meshgen import surge_mesh
+    raw = surge_mesh(seed=seed, target_nodes=target_nodes)
+    neta = raw.open_nodes.size
+    xo = raw.x[raw.open_nodes] / raw.meta["lx"]
+    tides = [
+        (2.0 * math.pi / M2_PERIOD, 0.0, 1.0, 0.5 + 0.1 * xo, np.deg2rad(20.0 * xo)),
+        (2.0 * math.pi / K1_PERIOD, 0.0, 1.0, 0.2 + 0.05 * xo, np.deg2rad(10.0 * xo)),
+    ]
+    params = default_params(dt, **kw)
+    return build_case(raw, params, Schedule(dt=dt, dramp=0.25, dramp_mete=0.25), tides)
+
+
+# --------------------------------------------------------------------------
+# Device-resident model
+# --------------------------------------------------------------------------
+
+class AdcError(RuntimeError):
+    pass
+
+
+def _check(rc, what):
+    if rc != 0:
+        raise AdcError(f"{what} failed with status {rc}: {_lib.last_error()}")
+
+
+class GpuModel:
+    """The device-resident step behind the reference's subroutine boundary."""
+
+    def __init__(self, case: Case, prec: int = _lib.ADC_PREC_FP64):
+        self.lib = _lib.load()
+        self.case = case
+        self._p = case.params_struct()
+        self._a = case.arrays_struct()
+        h = C.c_void_p()
+        _check(self.lib.adc_gpu_bind(C.byref(self._p), C.byref(self._a), prec, C.byref(h)),
+               "adc_gpu_bind")
+        self.h = h
+
+    def close(self):
+        if self.h:
+            self.lib.adc_gpu_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def step(self, it: int) -> AdcStepOut:
+        s = self.case.schedule.step(it)
+        out = AdcStepOut()
+        _check(self.lib.adc_timestep(self.h, C.byref(s), C.byref(out)), "adc_timestep")
+        return out
+
+    def run(self, it0: int, n: int):
+        steps = self.case.schedule.steps(it0, n)
+        numitr = np.zeros(n, np.int32)
+        last = AdcStepOut()
+        _check(self.lib.adc_run(self.h, n, steps, ptr(numitr, ip_), C.byref(last)), "adc_run")
+        return numitr, last
+
+    def sync_to_host(self):
+        _check(self.lib.adc_sync_to_host(self.h), "adc_sync_to_host")
+        return self.case.state()
+
+    def phase_times(self):
+        v = [C.c_double() for _ in range(5)]
+        self.lib.adc_phase_times(self.h, *[C.byref(t) for t in v])
+        return dict(zip(("shift", "gwce", "jcg", "wetdry", "momentum"), [t.value for t in v]))
+
+    def launches(self) -> int:
+        return int(self.lib.adc_launch_count(self.h))
+
+    def last_run_ms(self) -> float:
+        return float(self.lib.adc_last_run_ms(self.h))

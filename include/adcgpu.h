@@ -1,0 +1,215 @@
+/*
+ * adcgpu.h -- C ABI of libadcgpu, a B200-native (sm_100a) implementation of
+ * ADCIRC's per-time-step 2DDI hot path: GWCE assembly, ITPACK JCG solve,
+ * wetting/drying and the lumped explicit momentum update.
+ *
+ * Conventions are those of the Fortran module arrays the reference hands
+ * to these routines: column-major storage, 1-based node and element
+ * numbers, INTEGER = int32_t, REAL(8) = double.  Every entry point is
+ * extern "C" with plain pointers so a Fortran host binds it through
+ * ISO_C_BINDING (include/adcgpu_iface.F90) and Python through ctypes.
+ *
+ * No entry point allocates on behalf of the caller except adc_gpu_bind
+ * (device mirrors) and adc_jcg (device staging for one solve).  Errors are
+ * returned as status codes; the library never calls exit().
+ */
+#ifndef ADCGPU_H
+#define ADCGPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define ADC_OK 0
+#define ADC_ERR_DIAG 1        /* GWCE diagonal <= 0: gwce.F:678-707 terminates */
+#define ADC_ERR_ARG (-1)      /* invalid argument or size */
+#define ADC_ERR_MESH (-2)     /* inconsistent mesh tables */
+#define ADC_ERR_CUDA (-3)     /* CUDA runtime error (message: adc_last_error) */
+#define ADC_ERR_NOMEM (-4)    /* device allocation failed */
+#define ADC_ERR_TIMEOUT (-5)  /* a bounded device-side wait expired */
+#define ADC_ERR_UNSUPPORTED (-6) /* option the library does not implement */
+
+/* precision modes for adc_gpu_bind */
+#define ADC_PREC_FP64 0       /* every kernel in FP64, reference arithmetic */
+#define ADC_PREC_MIXED 1      /* FP32 assembly/SpMV/momentum, FP64 reductions */
+
+/* Model parameters (fort.15 values and derived switches). */
+typedef struct {
+  double dt;             /* DTDP */
+  double g;              /* gravity, constants.F90:45 */
+  double a00, b00, c00;  /* GWCE time weights, read_input.F:2995 */
+  double h0, velmin;     /* wet/dry, read_input.F:3006 */
+  double slim;           /* slope limiter, global.F:796 */
+  double hbreak, ftheta, fgamma; /* hybrid friction, nodalattr.F:509-511 */
+  double convcr;         /* JCG tolerance, RPARM(1) (gwce.F:150) */
+  double prbckgrnd_mh2o; /* background pressure in m of water, wind.F:354 */
+  int ifnlfa, ifnlct, ifnlcat; /* adcirc.F:287-384 */
+  int nolifa;            /* 2 = wetting/drying active (wetdry.F:204) */
+  int iflinbf, ifnlbf, ifhybf; /* nodalattr.F:1975-1987 */
+  int itmax;             /* JCG ITMAX, IPARM(1) */
+  int nws;               /* nonzero: met forcing terms are active */
+  int ifwind;            /* adcirc.F:391 */
+  int isldia;            /* ITPACK output level IPARM(2) (no output is produced) */
+  int pad_;
+} adc_params_t;
+
+/* Pointers to the host arrays of module MESH / GLOBAL / BOUNDARIES /
+ * NodalAttributes.  adc_gpu_bind copies them to the device; state arrays
+ * are written back only by adc_sync_to_host. */
+typedef struct {
+  int np, ne, mnei, neta, nbfr, nvel, nvelme, pad_;
+  const double *x, *y, *dp;      /* (NP) */
+  const int *nm;                 /* NM(NE,3) */
+  const int *nneigh;             /* NNeigh(NP) */
+  const int *neitab;             /* NeiTab(NP,MNEI), 0 = padding */
+  const double *fdxe, *fdye;     /* FDXE(3,NE), FDYE(3,NE) */
+  const double *areas;           /* AREAS(NE) = 2 x element area */
+  const int *csr_position;       /* CSR_POSITION(NE,3,2) */
+  const double *tau0var, *evm, *fric, *corif; /* (NP) */
+  const int *nbd;                /* NBD(NETA) elevation-specified nodes */
+  const double *amig, *per, *face, *ff;       /* (NBFR) */
+  const double *emo, *efa;       /* EMO(NBFR,NETA), EFA(NBFR,NETA) [rad] */
+  const int *nbv, *lbcodei;      /* (NVEL) */
+  const double *csii, *siii;     /* (NVEL) */
+  const int *me2gw;              /* (NVELME) */
+  double *eta1, *eta2, *etas;
+  double *uu1, *vv1, *uu2, *vv2, *qx1, *qy1, *qx2, *qy2, *h1, *h2;
+  double *tk, *tkm;              /* TK(NP), TKM(3,NP) */
+  int *nodecode, *nnodecode, *noff, *mju;
+  double *totalarea, *alphal;
+  double *wsx1, *wsy1, *wsx2, *wsy2, *pr1, *pr2;
+  double *coef;                  /* COEF(NP,MNEI) */
+  double *obccoef;               /* OBCCoef(NETA,MNEI-1) */
+  double *gwce_lv, *mom_lv_x, *mom_lv_y;
+} adc_arrays_t;
+
+/* Per-step scalars TIMESTEP computes before the hot path (timestep.F:257-353). */
+typedef struct {
+  int it;
+  int pad_;
+  double timeloc, timeh, rampelev, rampmete;
+} adc_step_t;
+
+/* Host-visible results of a step or phase. */
+typedef struct {
+  int numitr;       /* NUMITR = IPARM(1) after JCG (gwce.F:2005) */
+  int ier;          /* JCG error flag (itpackv.F: 11, 12, 13, 401, 402) */
+  int ncchange;     /* NCCHANGE after wet/dry (wetdry.F:1413-1430) */
+  int status;       /* ADC_OK or ADC_ERR_DIAG */
+  double ep;        /* EP, RMS of the GWCE diagonal (gwce.F:646-650) */
+  double zeta;      /* RPARM(1) after the solve (itpackv.F:394 overwrite) */
+  double cme;       /* RPARM(2), eigenvalue estimate */
+  int n_w1_events;  /* W1 wetting events that raised TK (wetdry.F:593-618) */
+  int pad_;
+} adc_stepout_t;
+
+/* ------------------------------------------------------------------ */
+/* Drop-in for ITPACK JCG.                                             */
+/* ------------------------------------------------------------------ */
+
+/* Replaces `subroutine jcg (n,ndim,maxnz,jcoef,coef,rhs,u,iwksp,nw,wksp,
+ * iparm,rparm,ier)`, itpackv.F:63-64, called from gwce.F:2003-2004.
+ * Same arguments, by reference.  coef/jcoef/rhs come back unscaled as the
+ * reference leaves them (itpackv.F:430); u returns the solution; iparm(1)
+ * the iteration count; rparm(1) is overwritten on non-convergence
+ * (itpackv.F:394).  Mixed-sign diagonals (ITPACK's isym switch,
+ * itpackv.F:2417) return ier = 903 without solving. */
+void adc_jcg(const int *n, const int *ndim, const int *maxnz, int *jcoef,
+             double *coef, double *rhs, double *u, int *iwksp, const int *nw,
+             double *wksp, int *iparm, double *rparm, int *ier);
+
+/* Replaces `subroutine dfault (iparm,rparm)`, itpackv.F:1070. */
+void adc_dfault(int *iparm, double *rparm);
+
+/* Clears the ITPACK state that persists between jcg calls (the saved q1
+ * flag of itjcg, itpackv.F:459-604) to its program-start value. */
+void adc_jcg_reset(void);
+
+/* ------------------------------------------------------------------ */
+/* Device-resident 2DDI step (state stays in HBM between calls).       */
+/* ------------------------------------------------------------------ */
+
+typedef struct adc_ctx adc_ctx;
+
+/* Binds the module arrays once after ADCIRC_Init (adcirc.F:113-411) and
+ * uploads them.  prec is ADC_PREC_FP64 or ADC_PREC_MIXED. */
+int adc_gpu_bind(const adc_params_t *p, const adc_arrays_t *a, int prec, adc_ctx **out);
+int adc_gpu_free(adc_ctx *ctx);
+
+/* TIMESTEP glue before the GWCE: H init at it==1 (timestep.F:231-237),
+ * time-level shift and load-vector zeroing (:375-416), bottom friction
+ * (nodalattr.F:2399-2413) and the TKM copy (nodalattr.F:2700-2704). */
+int adc_shift_friction(adc_ctx *ctx, const adc_step_t *s);
+
+/* Replaces GWCE_New(IT,ITIME_BGN,TimeLoc,TimeH), gwce.F:237, called via
+ * solveGWCE (gwce.F:166, timestep.F:1069).  Fills numitr/ier/status/ep. */
+int adc_gwce_new(adc_ctx *ctx, const adc_step_t *s, adc_stepout_t *out);
+
+/* Replaces computeWettingAndDrying(it), wetdry.F:140, timestep.F:1088,
+ * followed by the H2 update of timestep.F:1097-1099.  Fills ncchange. */
+int adc_wetdry(adc_ctx *ctx, const adc_step_t *s, adc_stepout_t *out);
+
+/* Replaces Mom_Eqs_New_NC(), momentum.F:166, via solveMomentumEq
+ * (momentum.F:118, timestep.F:1103). */
+int adc_momentum(adc_ctx *ctx, const adc_step_t *s);
+
+/* The four calls above in TIMESTEP order for one step. */
+int adc_timestep(adc_ctx *ctx, const adc_step_t *s, adc_stepout_t *out);
+
+/* Runs nsteps consecutive steps without host round trips (one captured
+ * CUDA graph replayed per step).  numitr[k] (optional, host) receives
+ * NUMITR of step k; last receives the outputs of the final step. */
+int adc_run(adc_ctx *ctx, int nsteps, const adc_step_t *steps, int *numitr,
+            adc_stepout_t *last);
+
+/* Copies device state to the bound host arrays (output/hotstart steps). */
+int adc_sync_to_host(adc_ctx *ctx);
+/* Re-uploads the bound host state arrays (after a host-side change). */
+int adc_sync_from_host(adc_ctx *ctx);
+
+/* Supplies this step's met forcing WSX2/WSY2/PR2 (getMeteorologicalForcing,
+ * timestep.F:651) from host arrays of length NP; applied after the shift. */
+int adc_set_met(adc_ctx *ctx, const double *wsx2, const double *wsy2, const double *pr2);
+
+/* Device time of the phases of the last adc_timestep/adc_run (ms). */
+int adc_phase_times(adc_ctx *ctx, double *ms_shift, double *ms_gwce, double *ms_jcg,
+                    double *ms_wetdry, double *ms_momentum);
+
+/* Number of kernel launches issued by the library since bind. */
+int64_t adc_launch_count(adc_ctx *ctx);
+
+/* Device time (CUDA events on the library's stream) of the step loop of
+ * the last adc_run, excluding its host uploads and readback (ms). */
+double adc_last_run_ms(adc_ctx *ctx);
+
+/* Message of the last error (thread-local). */
+const char *adc_last_error(void);
+
+/* ------------------------------------------------------------------ */
+/* Host-side mesh tables (reference: mesh.F, built once at init).      */
+/* ------------------------------------------------------------------ */
+int adc_mesh_geometry(int np, int ne, const double *x, const double *y, int *nm,
+                      double *fdxe, double *fdye, double *areas);
+int adc_mesh_mnei(int np, int ne, const int *nm);
+int adc_mesh_neighb(int np, int ne, int mnei, const double *x, const double *y,
+                    const int *nm, int *nneigh, int *neitab, int *neimax);
+int adc_mesh_csr_positions(int np, int ne, int mnei, const int *nm, const int *neitab,
+                           int neimax, int *csr_position);
+int adc_boundary_setup(int np, const double *x, const double *y, int nbou,
+                       const int *ibtype, const int *seg_ptr, const int *seg_nodes,
+                       double cos_inner, int nvel_max, int *nvel, int *nbv,
+                       int *lbcodei, double *csii, double *siii, int *nvelme,
+                       int *me2gw);
+/* Cold-start wet/dry state (cstart.F:1332-1427) and totalAreaCalc
+ * (mesh.F:3360-3400). */
+int adc_coldstart(int np, int ne, int nolifa, double h0, const double *dp, const int *nm,
+                  const double *areas, double *eta1, double *eta2, int *nnodecode,
+                  int *nodecode, int *noff, int *mju, double *totalarea);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,154 @@
+"""GPU parity: libadcgpu (CUDA, sm_100a) against the CPU oracle.
+
+Tolerances (FP64 path): eta, velocity and flux fields within 1e-9 relative
+to the field's maximum magnitude; JCG iteration counts and the integer
+wet/dry flags (NODECODE, NOFF) exact.  The only arithmetic allowed to
+differ is the order of the JCG dot-product sums (tree vs sequential) and
+CUDA's cos at elevation-boundary nodes, both at the 1e-16 level.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+REL_TOL = 1e-9
+FIELDS = ("eta1", "eta2", "etas", "uu2", "vv2", "qx2", "qy2", "h2", "tk", "totalarea")
+
+
+def _rel(a, b):
+    scale = max(np.abs(b).max(), 1e-30)
+    return float(np.abs(a - b).max() / scale)
+
+
+def _pair(case_fn, nsteps, use_run=False):
+    import oracle
+    from adcirc_b200 import model
+    c0 = case_fn()
+    cg = c0.clone()
+    orc = oracle.OracleModel(c0)
+    gpu = model.GpuModel(cg)
+    its_o = np.array([orc.step(it).numitr for it in range(1, nsteps + 1)])
+    if use_run:
+        its_g, _ = gpu.run(1, nsteps)
+    else:
+        its_g = np.array([gpu.step(it).numitr for it in range(1, nsteps + 1)])
+    gpu.sync_to_host()
+    gpu.close()
+    orc.close()
+    return c0, cg, its_o, np.asarray(its_g)
+
+
+def _check(c0, cg, its_o, its_g):
+    a, b = c0.arrays, cg.arrays
+    errs = {f: _rel(b[f], a[f]) for f in FIELDS}
+    bad = {f: e for f, e in errs.items() if not e <= REL_TOL}
+    assert not bad, f"fields beyond {REL_TOL}: {bad}"
+    assert np.array_equal(a["nodecode"], b["nodecode"])
+    assert np.array_equal(a["noff"], b["noff"])
+    mism = int(np.sum(its_o != its_g))
+    assert mism == 0, f"JCG iteration counts differ in {mism} steps: {its_o} vs {its_g}"
+    return errs
+
+
+def test_channel_steps(lib, orc):
+    from adcirc_b200 import model
+    c0, cg, io, ig = _pair(model.channel_case, 60)
+    _check(c0, cg, io, ig)
+    assert io.min() > 0
+
+
+def test_channel_graph_run(lib, orc):
+    from adcirc_b200 import model
+    c0, cg, io, ig = _pair(model.channel_case, 120, use_run=True)
+    _check(c0, cg, io, ig)
+
+
+def test_beach_wetdry(lib, orc):
+    from adcirc_b200 import model
+    c0, cg, io, ig = _pair(model.beach_case, 400, use_run=True)
+    errs = _check(c0, cg, io, ig)
+    a = c0.arrays
+    # the case must actually exercise drying
+    assert (a["nodecode"] == 0).sum() > 0 and (a["nodecode"] == 1).sum() > 0
+    assert errs["eta2"] <= REL_TOL
+
+
+def test_lake_at_rest(lib):
+    from adcirc_b200 import model
+    case = model.channel_case(amp=0.0)
+    gpu = model.GpuModel(case)
+    numitr, last = gpu.run(1, 50)
+    gpu.sync_to_host()
+    a = case.arrays
+    assert np.all(a["eta2"] == 0.0) and np.all(a["uu2"] == 0.0) and np.all(a["vv2"] == 0.0)
+    assert np.all(numitr == 0)
+
+
+def test_deterministic(lib):
+    from adcirc_b200 import model
+    outs = []
+    for _ in range(2):
+        case = model.beach_case()
+        gpu = model.GpuModel(case)
+        gpu.run(1, 200)
+        gpu.sync_to_host()
+        outs.append((case.arrays["eta2"].copy(), case.arrays["uu2"].copy()))
+        gpu.close()
+    assert np.array_equal(outs[0][0], outs[1][0]) and np.array_equal(outs[0][1], outs[1][1])
+
+
+def _jcg_system(orc_mod):
+    """A GWCE system (COEF, NeiTab, GWCE_LV, ETAS) from the channel case."""
+    from adcirc_b200 import model
+    case = model.channel_case()
+    om = orc_mod.OracleModel(case)
+    for it in range(1, 4):
+        om.step(it)
+    om.shift_friction(4)
+    om.close()
+    a = case.arrays
+    n = case.sizes["np"]
+    rng = np.random.default_rng(7)
+    return (n, case.sizes["mnei"], a["neitab"].copy(order="F"), a["coef"].copy(order="F"),
+            rng.standard_normal(n), 1e-3 * rng.standard_normal(n))
+
+
+def _call_adc_jcg(lib, n, mnei, jcoef, coef, rhs, u, iparm, rparm):
+    from adcirc_b200._lib import dp_, ip_, ptr
+    nw = 4 * n + 4 * int(iparm[0])
+    wksp = np.zeros(nw)
+    iwksp = np.zeros(3 * n, np.int32)
+    ier = C.c_int(0)
+    lib.adc_jcg(C.byref(C.c_int(n)), C.byref(C.c_int(n)), C.byref(C.c_int(mnei)), ptr(jcoef, ip_),
+                ptr(coef, dp_), ptr(rhs, dp_), ptr(u, dp_), ptr(iwksp, ip_), C.byref(C.c_int(nw)),
+                ptr(wksp, dp_), ptr(iparm, ip_), ptr(rparm, dp_), C.byref(ier))
+    return ier.value
+
+
+@pytest.mark.parametrize("itmax,tol", [(200, 1e-10), (3, 1e-10)])
+def test_jcg_dropin(lib, orc, itmax, tol):
+    n, mnei, jc, cf, rhs, u0 = _jcg_system(orc)
+    res = []
+    lib.adc_jcg_reset()
+    orc.load().orc_itpack_reset()
+    for impl in ("gpu", "orc"):
+        jcoef, coef, r, u = jc.copy(order="F"), cf.copy(order="F"), rhs.copy(), u0.copy()
+        iparm, rparm = orc.dfault()
+        iparm[0] = itmax
+        rparm[0] = tol
+        if impl == "gpu":
+            ier = _call_adc_jcg(lib, n, mnei, jcoef, coef, r, u, iparm, rparm)
+        else:
+            ier = orc.jcg(n, n, mnei, jcoef, coef, r, u, iparm, rparm)
+        res.append((ier, u, coef, jcoef, r, iparm.copy(), rparm.copy()))
+    g, o = res
+    assert g[0] == o[0]
+    assert g[5][0] == o[5][0], "iteration count"
+    assert _rel(g[1], o[1]) <= 1e-9
+    assert np.array_equal(g[3], o[3])
+    assert _rel(g[2], o[2]) <= 1e-13      # the scal/unscal drift of COEF
+    assert _rel(g[4], o[4]) <= 1e-13      # rhs restored
+    if itmax == 3:
+        assert o[0] == 13 and abs(g[6][0] - o[6][0]) <= 1e-9 * abs(o[6][0])
