@@ -19,6 +19,7 @@
 namespace adc {
 
 constexpr int kSlice = 32;            // rows per SELL slice (one warp)
+constexpr int kGatherChunk = 8;       // per-node gathers issued together
 constexpr int kThreads = 256;
 constexpr long long kSpinCycles = 4000000000LL;  // ~2 s at 1.9 GHz
 
@@ -37,16 +38,22 @@ struct Flags {
   double cme;         // RPARM(2) after the last solve
 };
 
+// Per-iteration record the JCG scalar block publishes to the row blocks:
+// the parcon coefficients, the stop flag and the norm cadence.
+struct Rec {
+  double c1, c2, c3, c4;
+  int halt, need_unorm, in, pad_;
+};
+
 // ITPACK common blocks and saved locals (itpackv.F:/itcom1-3/, itjcg save,
-// chgcon save) for the device-side solver.  One thread of one block writes
-// them between grid barriers; every other thread reads them after.
+// chgcon save) kept between solves.  During a solve the JCG scalar block
+// holds them in registers and writes them back at the end.
 struct Itp {
   int in, itmax, halt, adapt, q1, chg_ier, isym, pad_;
   double zeta, cme, sme, gamma, rho, gamold, rhoold, delnnm, delsnm, udnm,
       stptst, cmold, srelpr, rparm1;
-  double c1, c2, c3, c4;
-  double dtnrm, unorm;
-  int need_unorm, pad2_;
+  Rec rec;
+  double dtnrm, unorm;   // peror norms
 };
 
 struct Bar {
@@ -102,11 +109,13 @@ struct adc_ctx {
   double *ev_c;
   int ev_blocks;
   // JCG
-  double *ju1, *jd[3], *jdt[2], *jw, *soff;
+  double *ju1, *jw, *soff;
+  double4 *jp[2];        // JCG (dtwd, d, d_prev, -) per node, double-buffered
   double *jpart;         // partial dots per block (4 each)
   double *jtri;          // tri(itmax,4)
   adc::Itp *itp;
   adc::Bar *bar;
+  void *jlines;          // JCG barrier lines: 2 x 128 B per row block
   int jcg_grid, jcg_rows_blocks;
   // flags / steps
   adc::Flags *flags;

@@ -111,23 +111,46 @@ __global__ void k_lhs_gather(adc_ctx c, const int *rebuild) {
   double d2 = 0.0;
   if (i < c.np) {
     double d = 0.0;
-    for (int q = c.n2e_ptr[i]; q < c.n2e_ptr[i + 1]; ++q) {
-      int ek = c.n2e[q];
-      int e = ek / 3, k = ek - 3 * e;
-      d = d + c.ebuf[9 * (size_t)e + k];
+    const int q0 = c.n2e_ptr[i], q1 = c.n2e_ptr[i + 1];
+    for (int qc = q0; qc < q1; qc += kGatherChunk) {
+      int ek[kGatherChunk];
+      double x[kGatherChunk];
+#pragma unroll
+      for (int k = 0; k < kGatherChunk; ++k) if (qc + k < q1) ek[k] = c.n2e[qc + k];
+#pragma unroll
+      for (int k = 0; k < kGatherChunk; ++k)
+        if (qc + k < q1) {
+          int e = ek[k] / 3, kk = ek[k] - 3 * e;
+          x[k] = c.ebuf[9 * (size_t)e + kk];
+        }
+#pragma unroll
+      for (int k = 0; k < kGatherChunk; ++k) if (qc + k < q1) d = d + x[k];
     }
     c.diag[i] = d;
     d2 = d * d;
     int s = i / kSlice, lane = i - s * kSlice;
     int base = c.sl_ptr[s] + lane;
     int len = c.rlen[i];
-    for (int k = 0; k < len; ++k) {
-      int idx = base + k * kSlice;
-      int a = c.lhs_src[2 * idx], b = c.lhs_src[2 * idx + 1];
-      double v = 0.0;
-      if (a >= 0) v = v + c.ebuf[a];
-      if (b >= 0) v = v + c.ebuf[b];
-      c.offd[idx] = v;
+    for (int kc = 0; kc < len; kc += kGatherChunk) {
+      int2 src[kGatherChunk];
+      double va[kGatherChunk], vb[kGatherChunk];
+#pragma unroll
+      for (int k = 0; k < kGatherChunk; ++k)
+        if (kc + k < len) src[k] = reinterpret_cast<const int2 *>(c.lhs_src)[base + (kc + k) * kSlice];
+#pragma unroll
+      for (int k = 0; k < kGatherChunk; ++k)
+        if (kc + k < len) {
+          va[k] = src[k].x >= 0 ? c.ebuf[src[k].x] : 0.0;
+          vb[k] = src[k].y >= 0 ? c.ebuf[src[k].y] : 0.0;
+        }
+#pragma unroll
+      for (int k = 0; k < kGatherChunk; ++k)
+        if (kc + k < len) {
+          double v = 0.0;
+          if (src[k].x >= 0) v = v + va[k];
+          if (src[k].y >= 0) v = v + vb[k];
+          c.offd[base + (kc + k) * kSlice] = v;
+        }
     }
   }
   __shared__ double sh[32];
@@ -195,7 +218,7 @@ __global__ void k_lhs_bc(adc_ctx c, const int *rebuild) {
 
 // --------------------------------------------------------------- RHS
 // gwce.F:1000-1617, one element, IM=0 branches.
-__global__ void k_rhs_elem(adc_ctx c) {
+__global__ void __launch_bounds__(256, 2) k_rhs_elem(adc_ctx c) {
   int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= c.ne) return;
   const adc_params_t &p = c.p;
@@ -308,7 +331,17 @@ __global__ void k_rhs_gather(adc_ctx c) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= c.np) return;
   double v = 0.0;
-  for (int q = c.n2e_ptr[i]; q < c.n2e_ptr[i + 1]; ++q) v = v + c.ebuf[c.n2e[q]];
+  const int q0 = c.n2e_ptr[i], q1 = c.n2e_ptr[i + 1];
+  for (int qc = q0; qc < q1; qc += kGatherChunk) {
+    int ek[kGatherChunk];
+    double x[kGatherChunk];
+#pragma unroll
+    for (int k = 0; k < kGatherChunk; ++k) if (qc + k < q1) ek[k] = c.n2e[qc + k];
+#pragma unroll
+    for (int k = 0; k < kGatherChunk; ++k) if (qc + k < q1) x[k] = c.ebuf[ek[k]];
+#pragma unroll
+    for (int k = 0; k < kGatherChunk; ++k) if (qc + k < q1) v = v + x[k];
+  }
   c.gwce_lv[i] = v;
   c.eta1[i] = c.eta2[i];
   c.h1[i] = c.h2[i];

@@ -34,14 +34,34 @@
 
 namespace adc {
 
+// 32-byte node record (dtwd, d, d_prev, -) moved with one 256-bit access.
+struct __align__(32) P4 {
+  double x, y, z, w;
+};
+
+__device__ __forceinline__ P4 ld_p4(const P4 *p) {
+  P4 r;
+  asm volatile("ld.global.v4.f64 {%0,%1,%2,%3}, [%4];"
+               : "=d"(r.x), "=d"(r.y), "=d"(r.z), "=d"(r.w)
+               : "l"(p));
+  return r;
+}
+
+__device__ __forceinline__ void st_p4(P4 *p, double x, double y, double z, double w) {
+  asm volatile("st.global.v4.f64 [%0], {%1,%2,%3,%4};" ::"l"(p), "d"(x), "d"(y), "d"(z), "d"(w)
+               : "memory");
+}
+
 struct JcgArgs {
   int n, nslices, nrb, itmax;
   const int *sl_ptr, *sl_w, *col, *rlen;
   double *offd, *soff, *diag, *rhs;
-  double *u, *u1, *d0, *d1, *d2, *t0, *t1, *w;
+  double *u, *u1, *w;
+  P4 *p0, *p1;
   double *part, *tri;
   Itp *itp;
   Bar *bar;
+  void *arrive, *release;   // ArriveLine[nrb], ReleaseLine[nrb]
   Flags *flags;
   int eta_update;
   int do_peror;
@@ -53,76 +73,111 @@ struct JcgArgs {
 __device__ __forceinline__ double vld(const double *p) { return *(const volatile double *)p; }
 
 // ---------------------------------------------------------------- barrier
-// Returns true if this block was the last to arrive (only thread 0's view
-// is meaningful; broadcast through shared memory by the caller).
-__device__ bool bar_arrive(Bar *bar, unsigned nblocks, unsigned &gen_seen) {
-  volatile unsigned *vgen = &bar->gen;
-  gen_seen = *vgen;
-  __threadfence();
-  unsigned prev = atomicAdd(&bar->count, 1u);
-  return prev == nblocks - 1;
-}
+// Contention-free flag barrier.  Row block b owns two 128-byte lines:
+// arrive[b] = {generation, three partial sums} and release[b] =
+// {generation}.  The scalar block (last block of the grid) polls the
+// arrival lines with all its threads, does the serial work of the phase and
+// writes every release line.  No two blocks poll the same line and there
+// are no atomics.  Generations count barriers from 1 within a launch; the
+// lines are cleared before every launch.  Waits are bounded (clock64).
+struct alignas(128) ArriveLine {
+  unsigned gen;
+  unsigned pad_;
+  double part[3];
+  char fill_[128 - 32];
+};
+struct alignas(128) ReleaseLine {
+  unsigned gen;
+  char fill_[124];
+};
 
-__device__ void bar_release(Bar *bar) {
-  bar->count = 0;
-  __threadfence();
-  atomicAdd(&bar->gen, 1u);
-}
-
-__device__ bool bar_wait(Bar *bar, unsigned gen_seen, Flags *flags) {
-  volatile unsigned *vgen = &bar->gen;
+__device__ bool spin_eq(const unsigned *p, unsigned g, Flags *flags) {
+  const volatile unsigned *v = p;
   long long t0 = clock64();
-  while (*vgen == gen_seen) {
+  while (*v != g) {
     if (*(volatile int *)&flags->timeout) return false;
     if (clock64() - t0 > kSpinCycles) {
       atomicExch(&flags->timeout, 1);
       return false;
     }
-    __nanosleep(64);
   }
-  __threadfence();
   return true;
 }
 
-// Plain grid barrier.  Returns false on timeout.
-__device__ bool grid_sync(const JcgArgs &a) {
+// Row-block side: post (optionally) partials and the arrival, wait for the
+// release.  Returns false on timeout.
+__device__ bool row_arrive_wait(const JcgArgs &a, unsigned g, bool post, double p0, double p1,
+                                double p2) {
   __shared__ int ok;
   __syncthreads();
   if (threadIdx.x == 0) {
-    unsigned g;
-    bool last = bar_arrive(a.bar, gridDim.x, g);
-    if (last) {
-      bar_release(a.bar);
-      ok = 1;
-    } else {
-      ok = bar_wait(a.bar, g, a.flags) ? 1 : 0;
+    ArriveLine *al = (ArriveLine *)a.arrive + blockIdx.x;
+    if (post) {
+      volatile double *vp = al->part;
+      vp[0] = p0;
+      vp[1] = p1;
+      vp[2] = p2;
     }
+    __threadfence();
+    *(volatile unsigned *)&al->gen = g;
+    ok = spin_eq(&((ReleaseLine *)a.release + blockIdx.x)->gen, g, a.flags) ? 1 : 0;
+    __threadfence();
   }
   __syncthreads();
   return ok != 0;
 }
 
+// Scalar-block side: wait for every row block's arrival.
+__device__ bool scalar_gather(const JcgArgs &a, unsigned g) {
+  __shared__ int bad;
+  if (threadIdx.x == 0) bad = 0;
+  __syncthreads();
+  for (int b = threadIdx.x; b < a.nrb; b += blockDim.x)
+    if (!spin_eq(&((ArriveLine *)a.arrive + b)->gen, g, a.flags)) bad = 1;
+  __threadfence();
+  __syncthreads();
+  return bad == 0;
+}
+
+__device__ void scalar_release(const JcgArgs &a, unsigned g) {
+  __threadfence();
+  __syncthreads();
+  for (int b = threadIdx.x; b < a.nrb; b += blockDim.x)
+    *(volatile unsigned *)&((ReleaseLine *)a.release + b)->gen = g;
+}
+
+// Serial ITPACK state of one solve, held in registers of the scalar block's
+// thread 0 (echall/itjcg/chgcon/pstop/parcon variables).
+struct ItpLocal {
+  double zeta, cme, gamma, rho, gamold, rhoold, delnnm, delsnm, udnm, stptst, cmold, rparm1;
+  int itmax, adapt, q1, isym, chg_ier;
+};
+
 // ---------------------------------------------------------------- scalars
-__device__ double determ_d(int ldt, int n, const double *tri, double *wk1, double *wk2,
-                           double xlmda) {
-  for (int i = 1; i <= n; ++i) wk1[i - 1] = tri[i - 1] - xlmda;
-  wk2[n - 1] = wk1[n - 1];
-  wk2[n - 2] = wk1[n - 2] * wk2[n - 1] + tri[ldt + n - 1];
-  if (n != 2)
-    for (int l = n - 2; l >= 1; --l) wk2[l - 1] = wk1[l - 1] * wk2[l] + tri[ldt + l] * wk2[l + 1];
-  return wk2[0];
+// determ (itpackv.F:1029-1068): the three-term recurrence for
+// det(tri - x I), evaluated with the two trailing values in registers
+// (same operations, same order as the wk1/wk2 arrays of the reference).
+// tri(i,1) = t1[i-1], tri(i,2) = t2[i-1], held in shared memory.
+__device__ double determ_d(int n, const double *t1, const double *t2, double xlmda) {
+  double w2 = t1[n - 1] - xlmda;                       // wk2(n)
+  double w1 = (t1[n - 2] - xlmda) * w2 + t2[n - 1];    // wk2(n-1)
+  for (int l = n - 2; l >= 1; --l) {
+    double w = (t1[l - 1] - xlmda) * w1 + t2[l] * w2;  // wk2(l)
+    w2 = w1;
+    w1 = w;
+  }
+  return w1;
 }
 
 // zbrent (itpackv.F:2521-2781): Brent root of the characteristic
 // polynomial of the CG tridiagonal on [a, b].
-__device__ void zbrent_d(int n, double *tri, int itmax, double eps, double t, double &a,
-                         double &b, int &maxfn, int &ier) {
+__device__ void zbrent_d(int n, const double *t1, const double *t2, double eps, double t,
+                         double &a, double &b, int &maxfn, int &ier) {
   double c = 0, d = 0, e = 0, p, q, r, s, fa, fb, fc, tol, rm, rone, temp;
   ier = 0;
-  double *wk1 = tri + 2 * itmax, *wk2 = tri + 3 * itmax;
   int ic = 2;
-  fa = determ_d(itmax, n, tri, wk1, wk2, a);
-  fb = determ_d(itmax, n, tri, wk1, wk2, b);
+  fa = determ_d(n, t1, t2, a);
+  fb = determ_d(n, t1, t2, b);
   s = b;
   if ((fa > 0.0 && fb > 0.0) || (fa < 0.0 && fb < 0.0)) {
     ier = 502;
@@ -190,7 +245,7 @@ __device__ void zbrent_d(int n, double *tri, int itmax, double eps, double t, do
     if (fabs(temp) <= 0.5 * tol) temp = copysign(0.5 * tol, rm);
     b = b + temp;
     s = b;
-    fb = determ_d(itmax, n, tri, wk1, wk2, s);
+    fb = determ_d(n, t1, t2, s);
     ic = ic + 1;
     if (fb == 0.0 || fc == 0.0) continue;
     if ((fb > 0.0 && fc < 0.0) || (fb < 0.0 && fc > 0.0)) continue;
@@ -215,9 +270,9 @@ __device__ double pow10_neg(int nsig) {
   return 1.0 / p;
 }
 
-// chgcon, jacobi case (itpackv.F:893-1027), for iteration `in`.
-__device__ void chgcon_d(volatile Itp *it, double *tri, int in) {
-  const int ldt = it->itmax;
+// chgcon, jacobi case (itpackv.F:893-1027), for iteration `in`.  The
+// tridiagonal lives in the scalar block's shared memory (t1, t2).
+__device__ void chgcon_d(ItpLocal *it, double *t1, double *t2, int in) {
   double start = it->cme, end1 = 0.0;
   int ip = in;
   if (ip == 0) {
@@ -227,8 +282,8 @@ __device__ void chgcon_d(volatile Itp *it, double *tri, int in) {
   }
   if (ip == 1) {
     end1 = 1.0 - 1.0 / it->gamma;
-    tri[0] = end1;
-    tri[ldt] = 0.0;
+    t1[0] = end1;
+    t2[0] = 0.0;
     it->cme = end1;
     return;
   }
@@ -237,8 +292,8 @@ __device__ void chgcon_d(volatile Itp *it, double *tri, int in) {
     return;
   }
   it->cmold = start;
-  tri[ip - 1] = 1.0 - 1.0 / it->gamma;
-  tri[ldt + ip - 1] = (1.0 - it->rho) / (it->rho * it->rhoold * it->gamma * it->gamold);
+  t1[ip - 1] = 1.0 - 1.0 / it->gamma;
+  t2[ip - 1] = (1.0 - it->rho) / (it->rho * it->rhoold * it->gamma * it->gamold);
   int ier = 0;
   if (it->isym != 0) {
     ier = 903;
@@ -246,7 +301,7 @@ __device__ void chgcon_d(volatile Itp *it, double *tri, int in) {
     int nsig = nsig_of(it->zeta);
     int maxfn = it->itmax > 50 ? it->itmax : 50;
     double a = start, b = 1.0;
-    zbrent_d(ip, tri, it->itmax, 0.0, pow10_neg(nsig), a, b, maxfn, ier);
+    zbrent_d(ip, t1, t2, 0.0, pow10_neg(nsig), a, b, maxfn, ier);
     end1 = b;
   }
   it->chg_ier = ier;
@@ -258,9 +313,8 @@ __device__ void chgcon_d(volatile Itp *it, double *tri, int in) {
 }
 
 // pstop_nrms (itpackv.F:809-890, iflag = 1) for iteration `in`.
-__device__ void pstop_d(volatile Itp *it, int in, double unrm, double dnrm) {
+__device__ int pstop_d(ItpLocal *it, int in, double unrm, double dnrm) {
   double con = it->cme, uold, tr, tl;
-  it->halt = 0;
   if (in < 1) {
     it->q1 = 0;
     it->udnm = 1.0;
@@ -279,12 +333,12 @@ __device__ void pstop_d(volatile Itp *it, int in, double unrm, double dnrm) {
     tr = tr * (1.0 - con);
   }
   it->stptst = tl / tr;
-  if (tl >= tr * it->zeta) return;
-  it->halt = 1;
+  if (tl >= tr * it->zeta) return 0;
+  return 1;
 }
 
 // parcon (itpackv.F:1774-1851) for iteration `in`.
-__device__ void parcon_d(volatile Itp *it, int in, double dtnrm) {
+__device__ void parcon_d(ItpLocal *it, int in, double dtnrm, double c[4]) {
   double rhoold = it->rho;
   double gamold = it->gamma;
   it->gamma = 1.0 / (1.0 - dtnrm / it->delnnm);
@@ -293,10 +347,39 @@ __device__ void parcon_d(volatile Itp *it, int in, double dtnrm) {
   it->delsnm = it->delnnm;
   it->gamold = gamold;
   it->rhoold = rhoold;
-  it->c1 = it->rho * it->gamma;
-  it->c2 = it->rho;
-  it->c3 = 1.0 - it->rho;
-  it->c4 = it->rho * (1.0 - it->gamma);
+  c[0] = it->rho * it->gamma;
+  c[1] = it->rho;
+  c[2] = 1.0 - it->rho;
+  c[3] = it->rho * (1.0 - it->gamma);
+}
+
+// ------------------------------------------------------------ row access
+// A row's off-diagonal slots are processed in chunks of kCh: the column and
+// value of every slot of the chunk are loaded first, then all neighbour
+// values are gathered, so the loads of a chunk are in flight together.
+// Accumulation keeps the slot order (pjac's j order).
+constexpr int kCh = 6;
+
+// L2 prefetch of the next slice of a warp: the column and value rows of its
+// slots and its own-row vector entries, one 128-byte line per lane.
+__device__ __forceinline__ void prefetch_l2(const void *p) {
+  asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
+
+__device__ __forceinline__ void prefetch_slice(int lane, int ptr, int w, int row0, const int *col,
+                                               const double *val, const P4 *pv,
+                                               const double *u0, const double *u1) {
+  // lines: col w, val 2w, pv 8, u0 2, u1 2
+  const int ncol = w, nval = 2 * w;
+  for (int l = lane; l < ncol + nval + 12; l += 32) {
+    const char *a;
+    if (l < ncol) a = (const char *)(col + ptr) + 128 * l;
+    else if (l < ncol + nval) a = (const char *)(val + ptr) + 128 * (l - ncol);
+    else if (l < ncol + nval + 8) a = (const char *)(pv + row0) + 128 * (l - ncol - nval);
+    else if (l < ncol + nval + 10) a = (const char *)(u0 + row0) + 128 * (l - ncol - nval - 8);
+    else a = (const char *)(u1 + row0) + 128 * (l - ncol - nval - 10);
+    prefetch_l2(a);
+  }
 }
 
 // ------------------------------------------------------------ reductions
@@ -320,55 +403,74 @@ __device__ void block_sum3(double &a, double &b, double &c) {
   __syncthreads();
 }
 
-// Reducing barrier: every block posts 3 partials; the last block to arrive
-// sums them in a fixed order, runs `scalar(sum0, sum1, sum2)` on thread 0
-// and releases the others.  Returns false on timeout.
+// Reducing phase end.  Row blocks post their block sums of (p0, p1, p2)
+// and wait; the scalar block sums the posts in block order and runs
+// `serial(s0, s1, s2)` on its thread 0 before releasing.
 template <class F>
-__device__ bool reduce_sync(const JcgArgs &a, double p0, double p1, double p2, F scalar) {
-  __shared__ int last_sh, ok_sh;
-  block_sum3(p0, p1, p2);
-  if (threadIdx.x == 0) {
-    a.part[4 * blockIdx.x + 0] = p0;
-    a.part[4 * blockIdx.x + 1] = p1;
-    a.part[4 * blockIdx.x + 2] = p2;
+__device__ bool phase_reduce(const JcgArgs &a, bool scalar_block, unsigned &g, double p0,
+                             double p1, double p2, F serial) {
+  ++g;
+  if (!scalar_block) {
+    block_sum3(p0, p1, p2);
+    return row_arrive_wait(a, g, true, p0, p1, p2);
   }
-  __syncthreads();
-  unsigned g = 0;
-  if (threadIdx.x == 0) {
-    last_sh = bar_arrive(a.bar, gridDim.x, g) ? 1 : 0;
-    ok_sh = 1;
+  if (!scalar_gather(a, g)) return false;
+  double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+  for (int b = threadIdx.x; b < a.nrb; b += blockDim.x) {
+    const volatile double *vp = ((ArriveLine *)a.arrive + b)->part;
+    s0 += vp[0];
+    s1 += vp[1];
+    s2 += vp[2];
   }
+  block_sum3(s0, s1, s2);
+  if (threadIdx.x == 0) serial(s0, s1, s2);
+  scalar_release(a, g);
   __syncthreads();
-  if (last_sh) {
-    __threadfence();
-    double s0 = 0.0, s1 = 0.0, s2 = 0.0;
-    for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) {
-      s0 += vld(&a.part[4 * b + 0]);
-      s1 += vld(&a.part[4 * b + 1]);
-      s2 += vld(&a.part[4 * b + 2]);
-    }
-    block_sum3(s0, s1, s2);
-    if (threadIdx.x == 0) {
-      scalar(s0, s1, s2);
-      __threadfence();
-      bar_release(a.bar);
-    }
-  } else if (threadIdx.x == 0) {
-    ok_sh = bar_wait(a.bar, g, a.flags) ? 1 : 0;
-  }
+  return true;
+}
+
+__device__ bool phase_sync(const JcgArgs &a, bool scalar_block, unsigned &g) {
+  ++g;
+  if (!scalar_block) return row_arrive_wait(a, g, false, 0.0, 0.0, 0.0);
+  if (!scalar_gather(a, g)) return false;
+  scalar_release(a, g);
   __syncthreads();
-  return ok_sh != 0;
+  return true;
+}
+
+__device__ Rec read_rec(const Rec *r) {
+  const volatile Rec *v = r;
+  Rec o;
+  o.c1 = v->c1;
+  o.c2 = v->c2;
+  o.c3 = v->c3;
+  o.c4 = v->c4;
+  o.halt = v->halt;
+  o.need_unorm = v->need_unorm;
+  o.in = v->in;
+  o.pad_ = 0;
+  return o;
 }
 
 // ------------------------------------------------------------ the kernel
-__global__ void __launch_bounds__(kThreads) jcg_kernel(JcgArgs a) {
+__global__ void __launch_bounds__(kThreads, 2) jcg_kernel(JcgArgs a) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
   const bool scalar_block = (blockIdx.x == (unsigned)a.nrb);
   const int s0 = scalar_block ? 0 : (int)((long long)a.nslices * blockIdx.x / a.nrb);
   const int s1 = scalar_block ? 0 : (int)((long long)a.nslices * (blockIdx.x + 1) / a.nrb);
-  volatile Itp *vit = a.itp;
-  volatile Itp *it = a.itp;
   const int n = a.n;
+  extern __shared__ double s_tri[];   // tri(:,1) and tri(:,2), scalar block only
+  double *t1 = s_tri, *t2 = s_tri + a.itmax + 1;
+  Rec *rec = &a.itp->rec;
+  __shared__ ItpLocal L;              // used by the scalar block's thread 0 only
+  unsigned gen = 0;                   // barrier generation within this launch
+  if (scalar_block && threadIdx.x == 0) {
+    const volatile Itp *g = a.itp;
+    L.zeta = g->zeta; L.cme = g->cme; L.gamma = g->gamma; L.rho = g->rho;
+    L.gamold = g->gamold; L.rhoold = g->rhoold; L.delnnm = g->delnnm; L.delsnm = g->delsnm;
+    L.udnm = g->udnm; L.stptst = g->stptst; L.cmold = g->cmold; L.rparm1 = g->rparm1;
+    L.itmax = g->itmax; L.adapt = g->adapt; L.q1 = g->q1; L.isym = g->isym; L.chg_ier = 0;
+  }
 
   // P0: scal part 1 -- u' = u*sqrt(d), w = 1/sqrt(d), rhs' = rhs*w.
   for (int s = s0 + warp; s < s1; s += nwarps) {
@@ -380,10 +482,9 @@ __global__ void __launch_bounds__(kThreads) jcg_kernel(JcgArgs a) {
       a.w[i] = wv;
       a.rhs[i] = a.rhs[i] * wv;
       a.u1[i] = 0.0;
-      a.d2[i] = 0.0;
     }
   }
-  if (!grid_sync(a)) return;
+  if (!phase_sync(a, scalar_block, gen)) return;
 
   // P1: scaled off-diagonals, the reference's unscal drift of the resident
   // matrix, and the initial pseudo-residual d0 = pjac(u') + rhs' - u'.
@@ -393,119 +494,171 @@ __global__ void __launch_bounds__(kThreads) jcg_kernel(JcgArgs a) {
       int len = a.rlen[i];
       int base = a.sl_ptr[s] + lane;
       double wi = a.w[i];
+      double ui = a.u[i];
       double winv_i = 1.0 / wi;
       double acc = a.rhs[i];
-      for (int k = 0; k < len; ++k) {
-        int idx = base + k * kSlice;
-        int j = a.col[idx];
-        double wj = a.w[j];
-        double sv = a.offd[idx] * wi * wj;
-        a.soff[idx] = sv;
-        a.offd[idx] = sv * winv_i * (1.0 / wj);
-        acc = acc - sv * a.u[j];
+      for (int c0 = 0; c0 < len; c0 += kCh) {
+        int jj[kCh];
+        double vo[kCh], wj[kCh], uj[kCh];
+#pragma unroll
+        for (int k = 0; k < kCh; ++k)
+          if (c0 + k < len) {
+            int idx = base + (c0 + k) * kSlice;
+            jj[k] = a.col[idx];
+            vo[k] = a.offd[idx];
+          }
+#pragma unroll
+        for (int k = 0; k < kCh; ++k)
+          if (c0 + k < len) {
+            wj[k] = a.w[jj[k]];
+            uj[k] = a.u[jj[k]];
+          }
+#pragma unroll
+        for (int k = 0; k < kCh; ++k)
+          if (c0 + k < len) {
+            int idx = base + (c0 + k) * kSlice;
+            double sv = vo[k] * wi * wj[k];
+            a.soff[idx] = sv;
+            a.offd[idx] = sv * winv_i * (1.0 / wj[k]);
+            acc = acc - sv * uj[k];
+          }
       }
-      a.d0[i] = acc - a.u[i];
+      st_p4(a.p0 + i, 0.0, acc - ui, 0.0, 0.0);   // (dtwd0 later, d0, d(-1) = 0)
       a.diag[i] = winv_i * winv_i;
     }
   }
-  if (!grid_sync(a)) return;
+  if (!phase_sync(a, scalar_block, gen)) return;
 
   // P2: dtwd0 = -A' d0 and the iteration-0 norms; the scalar block runs
-  // chgcon for in = 0 (ip = 0: cme = 0).
+  // chgcon for in = 0 (ip = 0: cme = 0) while the rows work.
+  Rec r = read_rec(rec);
   {
     double pd = 0.0, pt = 0.0, pu = 0.0;
-    const int need_u = vit->need_unorm;
     for (int s = s0 + warp; s < s1; s += nwarps) {
       int i = s * kSlice + lane;
       if (i < n) {
         int len = a.rlen[i];
         int base = a.sl_ptr[s] + lane;
         double acc = 0.0;
-        for (int k = 0; k < len; ++k) {
-          int idx = base + k * kSlice;
-          acc = acc - a.soff[idx] * a.d0[a.col[idx]];
+        for (int c0 = 0; c0 < len; c0 += kCh) {
+          int jj[kCh];
+          double vv[kCh], xx[kCh];
+#pragma unroll
+          for (int k = 0; k < kCh; ++k)
+            if (c0 + k < len) {
+              int idx = base + (c0 + k) * kSlice;
+              jj[k] = a.col[idx];
+              vv[k] = a.soff[idx];
+            }
+#pragma unroll
+          for (int k = 0; k < kCh; ++k)
+            if (c0 + k < len) xx[k] = a.p0[jj[k]].y;
+#pragma unroll
+          for (int k = 0; k < kCh; ++k)
+            if (c0 + k < len) acc = acc - vv[k] * xx[k];
         }
-        a.t0[i] = acc;
-        double di = a.d0[i];
+        a.p0[i].x = acc;
+        double di = a.p0[i].y;
         pd += di * di;
         pt += di * acc;
-        if (need_u) { double ui = a.u[i]; pu += ui * ui; }
+        if (r.need_unorm) { double ui = a.u[i]; pu += ui * ui; }
       }
     }
-    if (scalar_block && threadIdx.x == 0 && it->adapt) chgcon_d(it, a.tri, 0);
-    bool ok = reduce_sync(a, pd, pt, pu, [&](double sd, double st, double su) {
-      it->delnnm = sd;
-      double unorm = need_u ? su : 1.0;
-      pstop_d(it, 0, unorm, sd);
-      it->in = 0;
-      if (!it->halt) {
-        if (it->itmax == 0) {
-          it->halt = 2;   // not converged at in = itmax
-        } else {
-          parcon_d(it, 0, st);
-          it->need_unorm = !(it->q1 || ((1 > 5) && (1 % 5 != 0)));
-        }
+    if (scalar_block && threadIdx.x == 0 && L.adapt) chgcon_d(&L, t1, t2, 0);
+    const int need_u = r.need_unorm;
+    bool ok = phase_reduce(a, scalar_block, gen, pd, pt, pu, [&](double sd, double st, double su) {
+      L.delnnm = sd;
+      int halt = pstop_d(&L, 0, need_u ? su : 1.0, sd);
+      double c[4] = {0, 0, 0, 0};
+      if (!halt) {
+        if (L.itmax == 0) halt = 2;
+        else parcon_d(&L, 0, st, c);
       }
+      volatile Rec *vr = rec;
+      vr->c1 = c[0]; vr->c2 = c[1]; vr->c3 = c[2]; vr->c4 = c[3];
+      vr->halt = halt;
+      vr->need_unorm = !(L.q1 || ((1 > 5) && (1 % 5 != 0)));
+      vr->in = 0;
     });
     if (!ok) return;
   }
 
-  // Iteration phases.
-  double *D[3] = {a.d0, a.d1, a.d2};
-  double *T[2] = {a.t0, a.t1};
+  // Iteration phases: phase `in` forms u(in+1), d(in+1), dtwd(in+1) and the
+  // norms of iteration in+1.  P[in % 2][i] = (dtwd(in), d(in), d(in-1)) so
+  // a neighbour's three values arrive in one 32-byte sector.
+  P4 *P[2] = {a.p0, a.p1};
   double *U[2] = {a.u, a.u1};
   for (int in = 0; in < a.itmax; ++in) {
-    if (vit->halt) break;
-    const double c1 = vit->c1, c2 = vit->c2, c3 = vit->c3, c4 = vit->c4;
-    const int need_u = vit->need_unorm;
-    const double *dc = D[in % 3], *dp = D[(in + 2) % 3], *tc = T[in % 2];
-    double *dn = D[(in + 1) % 3], *tn = T[(in + 1) % 2];
+    r = read_rec(rec);
+    if (r.halt) break;
+    const double c1 = r.c1, c2 = r.c2, c3 = r.c3, c4 = r.c4;
+    const int need_u = r.need_unorm;
+    const P4 *pc = P[in % 2];
+    P4 *pn = P[(in + 1) % 2];
     const double *uc = U[in % 2];
     double *un = U[(in + 1) % 2];
     double pd = 0.0, pt = 0.0, pu = 0.0;
     for (int s = s0 + warp; s < s1; s += nwarps) {
       int i = s * kSlice + lane;
+      const int sn = s + nwarps;
+      if (sn < s1)
+        prefetch_slice(lane, a.sl_ptr[sn], a.sl_w[sn], sn * kSlice, a.col, a.soff, pc, uc, un);
       if (i < n) {
-        double unew = c1 * dc[i] + c2 * uc[i] + c3 * un[i];
-        double dnew = c1 * tc[i] + c4 * dc[i] + c3 * dp[i];
+        const P4 me = ld_p4(pc + i);
+        double unew = c1 * me.y + c2 * uc[i] + c3 * un[i];
+        double dnew = c1 * me.x + c4 * me.y + c3 * me.z;
         int len = a.rlen[i];
         int base = a.sl_ptr[s] + lane;
         double acc = 0.0;
-        for (int k = 0; k < len; ++k) {
-          int idx = base + k * kSlice;
-          int j = a.col[idx];
-          double dj = c1 * tc[j] + c4 * dc[j] + c3 * dp[j];
-          acc = acc - a.soff[idx] * dj;
+        for (int c0 = 0; c0 < len; c0 += kCh) {
+          int jj[kCh];
+          double vv[kCh];
+          P4 xx[kCh];
+#pragma unroll
+          for (int k = 0; k < kCh; ++k)
+            if (c0 + k < len) {
+              int idx = base + (c0 + k) * kSlice;
+              jj[k] = a.col[idx];
+              vv[k] = a.soff[idx];
+            }
+#pragma unroll
+          for (int k = 0; k < kCh; ++k)
+            if (c0 + k < len) xx[k] = ld_p4(pc + jj[k]);
+#pragma unroll
+          for (int k = 0; k < kCh; ++k)
+            if (c0 + k < len) {
+              double dj = c1 * xx[k].x + c4 * xx[k].y + c3 * xx[k].z;
+              acc = acc - vv[k] * dj;
+            }
         }
         un[i] = unew;
-        dn[i] = dnew;
-        tn[i] = acc;
+        st_p4(pn + i, acc, dnew, me.y, 0.0);
         pd += dnew * dnew;
         pt += dnew * acc;
         if (need_u) pu += unew * unew;
       }
     }
     const int m = in + 1;
-    if (scalar_block && threadIdx.x == 0 && it->adapt) chgcon_d(it, a.tri, m);
-    bool ok = reduce_sync(a, pd, pt, pu, [&](double sd, double st, double su) {
-      it->delnnm = sd;
-      double unorm = need_u ? su : 1.0;
-      pstop_d(it, m, unorm, sd);
-      it->in = m;
-      if (!it->halt) {
-        if (m >= it->itmax) {
-          it->halt = 2;
-        } else {
-          parcon_d(it, m, st);
-          int mm = m + 1;
-          it->need_unorm = !(it->q1 || ((mm > 5) && (mm % 5 != 0)));
-        }
+    if (scalar_block && threadIdx.x == 0 && L.adapt) chgcon_d(&L, t1, t2, m);
+    bool ok = phase_reduce(a, scalar_block, gen, pd, pt, pu, [&](double sd, double st, double su) {
+      L.delnnm = sd;
+      int halt = pstop_d(&L, m, need_u ? su : 1.0, sd);
+      double c[4] = {0, 0, 0, 0};
+      if (!halt) {
+        if (m >= L.itmax) halt = 2;
+        else parcon_d(&L, m, st, c);
       }
+      int mm = m + 1;
+      volatile Rec *vr = rec;
+      vr->c1 = c[0]; vr->c2 = c[1]; vr->c3 = c[2]; vr->c4 = c[3];
+      vr->halt = halt;
+      vr->need_unorm = !(L.q1 || ((mm > 5) && (mm % 5 != 0)));
+      vr->in = m;
     });
     if (!ok) return;
   }
-
-  const int fin = vit->in;
+  r = read_rec(rec);
+  const int fin = r.in;
   const double *usol = U[fin % 2];
 
   // Optional peror (itpackv.F:607-720): the norms behind digit1/digit2.
@@ -529,9 +682,9 @@ __global__ void __launch_bounds__(kThreads) jcg_kernel(JcgArgs a) {
         pr += wk2 * wk2;
       }
     }
-    bool ok = reduce_sync(a, pb, pr, 0.0, [&](double sb, double sr, double) {
-      it->dtnrm = sb;
-      it->unorm = sr;
+    bool ok = phase_reduce(a, scalar_block, gen, pb, pr, 0.0, [&](double sb, double sr, double) {
+      a.itp->dtnrm = sb;
+      a.itp->unorm = sr;
     });
     if (!ok) return;
   }
@@ -548,18 +701,30 @@ __global__ void __launch_bounds__(kThreads) jcg_kernel(JcgArgs a) {
       if (a.eta_update) a.eta2[i] = a.nodecode[i] * (uf + 0.0) + a.eta1[i];
     }
   }
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
-    int h = vit->halt;
+  if (scalar_block && threadIdx.x == 0) {
+    int h = r.halt;
+    if (h == 2) L.rparm1 = L.stptst;   // itpackv.F:394
+    volatile Itp *g = a.itp;
+    g->zeta = L.zeta; g->cme = L.cme; g->gamma = L.gamma; g->rho = L.rho;
+    g->gamold = L.gamold; g->rhoold = L.rhoold; g->delnnm = L.delnnm; g->delsnm = L.delsnm;
+    g->udnm = L.udnm; g->stptst = L.stptst; g->cmold = L.cmold; g->rparm1 = L.rparm1;
+    g->adapt = L.adapt; g->q1 = L.q1; g->chg_ier = L.chg_ier;
+    g->in = fin;
+    g->halt = h;
     a.flags->numitr = fin;
     a.flags->ier = (h == 2) ? 13 : 0;
-    if (h == 2) it->rparm1 = vit->stptst;   // itpackv.F:394
-    a.flags->zeta = vit->rparm1;
-    a.flags->cme = vit->cme;
+    a.flags->zeta = L.rparm1;
+    a.flags->cme = L.cme;
   }
 }
 
 // Per-solve ITPACK initialisation (echall, itpackv.F:1212-1255, plus the
 // zeta floor of jcg :223-232); q1 and rparm1 persist across solves.
+__global__ void jcg_clear_lines(unsigned *lines, int nwords) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nwords; k += gridDim.x * blockDim.x)
+    lines[k] = 0u;
+}
+
 __global__ void jcg_init_kernel(Itp *it, Bar *bar, int itmax) {
   bar->count = 0;
   it->zeta = it->rparm1;
@@ -573,7 +738,9 @@ __global__ void jcg_init_kernel(Itp *it, Bar *bar, int itmax) {
   it->delnnm = it->delsnm = it->gamma = it->rho = it->stptst = it->udnm = 0.0;
   double temp = 512.0 * DBL_EPSILON;
   if (it->zeta < temp) it->zeta = temp;
-  it->need_unorm = !(it->q1 || 0);
+  it->rec.halt = 0;
+  it->rec.in = 0;
+  it->rec.need_unorm = !it->q1;
 }
 
 }  // namespace adc
@@ -586,7 +753,9 @@ int jcg_setup_grid(adc_ctx *c) {
   int dev = 0, nsm = 0, per_sm = 0;
   ADC_CUDA(cudaGetDevice(&dev));
   ADC_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-  ADC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, jcg_kernel, kThreads, 0));
+  size_t smem = 2 * sizeof(double) * (c->itmax + 1);
+  if (smem > 48 * 1024) { set_error("itmax too large for the JCG scalar block"); return ADC_ERR_ARG; }
+  ADC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, jcg_kernel, kThreads, smem));
   if (per_sm < 1) { set_error("jcg kernel cannot be resident"); return ADC_ERR_CUDA; }
   long long maxb = (long long)per_sm * nsm;
   int nrb = (int)std::min<long long>(maxb - 1, c->nslices);
@@ -615,28 +784,31 @@ int launch_jcg_impl(adc_ctx *c, int eta_update, int do_peror, int run_init) {
   a.rhs = c->gwce_lv;
   a.u = c->etas;
   a.u1 = c->ju1;
-  a.d0 = c->jd[0];
-  a.d1 = c->jd[1];
-  a.d2 = c->jd[2];
-  a.t0 = c->jdt[0];
-  a.t1 = c->jdt[1];
+  a.p0 = (P4 *)c->jp[0];
+  a.p1 = (P4 *)c->jp[1];
   a.w = c->jw;
   a.part = c->jpart;
   a.tri = c->jtri;
   a.itp = c->itp;
   a.bar = c->bar;
+  a.arrive = c->jlines;
+  a.release = (char *)c->jlines + 128 * (size_t)c->jcg_rows_blocks;
   a.flags = c->flags;
   a.eta_update = eta_update;
   a.nodecode = c->nodecode;
   a.eta1 = c->eta1;
   a.eta2 = c->eta2;
+  int nwords = (int)(2 * 128 * (size_t)c->jcg_rows_blocks / 4);
+  jcg_clear_lines<<<8, 256, 0, c->stream>>>((unsigned *)c->jlines, nwords);
+  c->launches++;
   if (run_init) {
     jcg_init_kernel<<<1, 1, 0, c->stream>>>(c->itp, c->bar, c->itmax);
     c->launches++;
   }
   void *args[] = {&a};
+  size_t smem = 2 * sizeof(double) * (c->itmax + 1);
   ADC_CUDA(cudaLaunchCooperativeKernel((const void *)jcg_kernel, dim3(c->jcg_grid),
-                                       dim3(kThreads), args, 0, c->stream));
+                                       dim3(kThreads), args, smem, c->stream));
   c->launches++;
   return ADC_OK;
 }

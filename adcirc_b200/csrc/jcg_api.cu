@@ -29,8 +29,8 @@ struct Stage {
   Stage() { memset((void *)&c, 0, sizeof(c)); }
   ~Stage() {
     void *ptrs[] = {c.sl_ptr, c.sl_w, c.col, c.rlen, c.offd, c.soff, c.diag, c.gwce_lv,
-                    c.etas, c.ju1, c.jd[0], c.jd[1], c.jd[2], c.jdt[0], c.jdt[1], c.jw,
-                    c.jpart, c.jtri, c.itp, c.bar, c.flags};
+                    c.etas, c.ju1, c.jp[0], c.jp[1], c.jw,
+                    c.jpart, c.jtri, c.itp, c.bar, c.flags, c.jlines};
     for (void *p : ptrs)
       if (p) cudaFree(p);
     if (c.stream) cudaStreamDestroy(c.stream);
@@ -96,12 +96,15 @@ static int jcg_solve(int n, int ndim, int maxnz, int *jcoef, double *coef, doubl
   ADC_CUDA(alloc_up(&c.diag, diag.data(), n));
   ADC_CUDA(alloc_up(&c.gwce_lv, rhs, n));
   ADC_CUDA(alloc_up(&c.etas, u, n));
-  double **vec[] = {&c.ju1, &c.jd[0], &c.jd[1], &c.jd[2], &c.jdt[0], &c.jdt[1], &c.jw};
+  double **vec[] = {&c.ju1, &c.jw};
   for (double **v : vec) ADC_CUDA(alloc_up<double>(v, nullptr, n));
+  ADC_CUDA(alloc_up<double4>(&c.jp[0], nullptr, n));
+  ADC_CUDA(alloc_up<double4>(&c.jp[1], nullptr, n));
   int rc = jcg_setup_grid(&c);
   if (rc) return rc;
   ADC_CUDA(alloc_up<double>(&c.jpart, nullptr, 4 * (size_t)c.jcg_grid));
   ADC_CUDA(alloc_up<double>(&c.jtri, nullptr, 4 * (size_t)std::max(itmax, 2)));
+  ADC_CUDA(alloc_up<char>((char **)&c.jlines, nullptr, 2 * 128 * (size_t)c.jcg_rows_blocks));
   Itp it;
   memset(&it, 0, sizeof(it));
   it.zeta = rparm[0];
@@ -114,7 +117,7 @@ static int jcg_solve(int n, int ndim, int maxnz, int *jcoef, double *coef, doubl
   it.srelpr = DBL_EPSILON;
   double temp = 512.0 * DBL_EPSILON;
   if (it.zeta < temp) it.zeta = temp;
-  it.need_unorm = !it.q1;
+  it.rec.need_unorm = !it.q1;
   ADC_CUDA(alloc_up(&c.itp, &it, 1));
   Bar bar = {0, 0};
   ADC_CUDA(alloc_up(&c.bar, &bar, 1));

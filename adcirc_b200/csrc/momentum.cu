@@ -96,11 +96,25 @@ __global__ void k_mom_node(adc_ctx c) {
   const adc_params_t &p = c.p;
   const double DTO2 = p.dt / 2.0;
   double mx = 0.0, my = 0.0;
-  for (int q = c.n2e_ptr[i]; q < c.n2e_ptr[i + 1]; ++q) {
-    int ek = c.n2e[q];
-    int e = ek / 3, k = ek - 3 * e;
-    mx = mx + c.ebuf[6 * (size_t)e + k];
-    my = my + c.ebuf[6 * (size_t)e + 3 + k];
+  const int q0 = c.n2e_ptr[i], q1 = c.n2e_ptr[i + 1];
+  for (int qc = q0; qc < q1; qc += kGatherChunk) {
+    int ek[kGatherChunk];
+    double xa[kGatherChunk], xb[kGatherChunk];
+#pragma unroll
+    for (int k = 0; k < kGatherChunk; ++k) if (qc + k < q1) ek[k] = c.n2e[qc + k];
+#pragma unroll
+    for (int k = 0; k < kGatherChunk; ++k)
+      if (qc + k < q1) {
+        int e = ek[k] / 3, kk = ek[k] - 3 * e;
+        xa[k] = c.ebuf[6 * (size_t)e + kk];
+        xb[k] = c.ebuf[6 * (size_t)e + 3 + kk];
+      }
+#pragma unroll
+    for (int k = 0; k < kGatherChunk; ++k)
+      if (qc + k < q1) {
+        mx = mx + xa[k];
+        my = my + xb[k];
+      }
   }
   int NCI = c.nodecode[i];
   double ta = c.totalarea[i];

@@ -5,6 +5,7 @@
 #include <cfloat>
 #include <cmath>
 #include <cstdarg>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -381,10 +382,9 @@ static void free_ctx(adc_ctx *c) {
       (void **)&c->noff, (void **)&c->noffold, (void **)&c->mju, (void **)&c->ncele,
       (void **)&c->diag, (void **)&c->offd, (void **)&c->obccoef, (void **)&c->ebuf,
       (void **)&c->ebuf2, (void **)&c->red, (void **)&c->ev_cnt, (void **)&c->ev_a,
-      (void **)&c->ev_b, (void **)&c->ev_c, (void **)&c->ju1, (void **)&c->jd[0],
-      (void **)&c->jd[1], (void **)&c->jd[2], (void **)&c->jdt[0], (void **)&c->jdt[1],
-      (void **)&c->jw, (void **)&c->soff, (void **)&c->jpart, (void **)&c->jtri,
-      (void **)&c->itp, (void **)&c->bar, (void **)&c->flags, (void **)&c->steps,
+      (void **)&c->ev_b, (void **)&c->ev_c, (void **)&c->ju1, (void **)&c->jp[0],
+      (void **)&c->jp[1], (void **)&c->jw, (void **)&c->soff, (void **)&c->jpart, (void **)&c->jtri,
+      (void **)&c->itp, (void **)&c->bar, (void **)&c->jlines, (void **)&c->flags, (void **)&c->steps,
       (void **)&c->numitr_log, (void **)&c->met_wsx, (void **)&c->met_wsy,
       (void **)&c->met_pr};
   for (void **p : ptrs)
@@ -476,9 +476,10 @@ static int bind_impl(const adc_params_t *p, const adc_arrays_t *a, int prec, adc
   double **node_f64[] = {&c->eta1, &c->eta2, &c->etas, &c->uu1, &c->vv1, &c->uu2, &c->vv2, &c->qx1,
                          &c->qy1, &c->qx2, &c->qy2, &c->h1, &c->h2, &c->tk, &c->totalarea,
                          &c->wsx1, &c->wsy1, &c->wsx2, &c->wsy2, &c->pr1, &c->pr2, &c->gwce_lv,
-                         &c->mom_x, &c->mom_y, &c->diag, &c->ju1, &c->jd[0], &c->jd[1], &c->jd[2],
-                         &c->jdt[0], &c->jdt[1], &c->jw, &c->met_wsx, &c->met_wsy, &c->met_pr};
+                         &c->mom_x, &c->mom_y, &c->diag, &c->ju1, &c->jw, &c->met_wsx,
+                         &c->met_wsy, &c->met_pr};
   for (double **q : node_f64) B(dalloc(q, np));
+  B(dalloc(&c->jp[0], np)); B(dalloc(&c->jp[1], np));
   B(dalloc(&c->tkm, 3 * (size_t)np));
   B(dalloc(&c->alphal, ne));
   int **node_i32[] = {&c->nodecode, &c->nnodecode, &c->mju};
@@ -496,6 +497,7 @@ static int bind_impl(const adc_params_t *p, const adc_arrays_t *a, int prec, adc
   B(dalloc(&c->jpart, 4 * (size_t)c->jcg_grid));
   B(dalloc(&c->jtri, 4 * (size_t)std::max(c->itmax, 2)));
   B(dalloc(&c->itp, 1)); B(dalloc(&c->bar, 1));
+  B(dalloc((char **)&c->jlines, 2 * 128 * (size_t)c->jcg_rows_blocks));
   {
     // Flags followed by the rebuild word.
     char *f = nullptr;

@@ -227,11 +227,24 @@ __global__ void k_wd_d2(adc_ctx c) {
   if (i >= c.np) return;
   int mju = 0;
   double ta = 0.0;
-  for (int q = c.n2e_ptr[i]; q < c.n2e_ptr[i + 1]; ++q) {
-    int e = c.n2e[q] / 3;
-    int nc = c.ncele[e];
-    mju += nc;
-    ta = ta + nc * c.areas[e] / 2.0;
+  const int q0 = c.n2e_ptr[i], q1 = c.n2e_ptr[i + 1];
+  for (int qc = q0; qc < q1; qc += kGatherChunk) {
+    int ee[kGatherChunk], nc[kGatherChunk];
+    double ar[kGatherChunk];
+#pragma unroll
+    for (int k = 0; k < kGatherChunk; ++k) if (qc + k < q1) ee[k] = c.n2e[qc + k] / 3;
+#pragma unroll
+    for (int k = 0; k < kGatherChunk; ++k)
+      if (qc + k < q1) {
+        nc[k] = c.ncele[ee[k]];
+        ar[k] = c.areas[ee[k]];
+      }
+#pragma unroll
+    for (int k = 0; k < kGatherChunk; ++k)
+      if (qc + k < q1) {
+        mju += nc[k];
+        ta = ta + nc[k] * ar[k] / 2.0;
+      }
   }
   c.totalarea[i] = ta;
   int nn = c.nnodecode[i];
