@@ -1,0 +1,130 @@
+!-------------------------------------------------------------------------------!
+! adcgpu_iface.F90 -- ISO_C_BINDING interface to libadcgpu (include/adcgpu.h).
+!
+! A Fortran host (ADCIRC's TIMESTEP / GWCE_New) uses this module to call the
+! B200 implementation of the 2DDI hot path.  The types mirror adc_params_t,
+! adc_arrays_t, adc_step_t and adc_stepout_t field for field; array members
+! are C_LOC of the host's module arrays (column-major, 1-based contents).
+! Not compiled in this repository (no Fortran compiler is installed); built by
+! the host's own CMake with -lstdc++ and the library on the link line.
+!-------------------------------------------------------------------------------!
+module adcgpu_iface
+   use, intrinsic :: iso_c_binding
+   implicit none
+   private
+
+   integer(c_int), parameter, public :: ADC_OK = 0, ADC_ERR_DIAG = 1
+   integer(c_int), parameter, public :: ADC_PREC_FP64 = 0, ADC_PREC_MIXED = 1
+
+   type, bind(C), public :: adc_params_t
+      real(c_double) :: dt, g, a00, b00, c00, h0, velmin, slim, hbreak, ftheta, &
+                        fgamma, convcr, prbckgrnd_mh2o
+      integer(c_int) :: ifnlfa, ifnlct, ifnlcat, nolifa, iflinbf, ifnlbf, ifhybf, &
+                        itmax, nws, ifwind, isldia, pad_
+   end type
+
+   type, bind(C), public :: adc_arrays_t
+      integer(c_int) :: np, ne, mnei, neta, nbfr, nvel, nvelme, pad_
+      type(c_ptr) :: x, y, dp, nm, nneigh, neitab, fdxe, fdye, areas, csr_position
+      type(c_ptr) :: tau0var, evm, fric, corif
+      type(c_ptr) :: nbd, amig, per, face, ff, emo, efa, nbv, lbcodei, csii, siii, me2gw
+      type(c_ptr) :: eta1, eta2, etas, uu1, vv1, uu2, vv2, qx1, qy1, qx2, qy2, h1, h2
+      type(c_ptr) :: tk, tkm, nodecode, nnodecode, noff, mju, totalarea, alphal
+      type(c_ptr) :: wsx1, wsy1, wsx2, wsy2, pr1, pr2, coef, obccoef
+      type(c_ptr) :: gwce_lv, mom_lv_x, mom_lv_y
+   end type
+
+   type, bind(C), public :: adc_step_t
+      integer(c_int) :: it, pad_
+      real(c_double) :: timeloc, timeh, rampelev, rampmete
+   end type
+
+   type, bind(C), public :: adc_stepout_t
+      integer(c_int) :: numitr, ier, ncchange, status
+      real(c_double) :: ep, zeta, cme
+      integer(c_int) :: n_w1_events, pad_
+   end type
+
+   public :: adc_jcg, adc_dfault, adc_gpu_bind, adc_gpu_free, adc_shift_friction, &
+             adc_gwce_new, adc_wetdry, adc_momentum, adc_timestep, adc_sync_to_host, &
+             adc_sync_from_host, adc_set_met
+
+   interface
+      ! drop-in for ITPACK jcg (itpackv.F:63): identical argument list
+      subroutine adc_jcg(n, ndim, maxnz, jcoef, coef, rhs, u, iwksp, nw, wksp, &
+                         iparm, rparm, ier) bind(C, name="adc_jcg")
+         import :: c_int, c_double
+         integer(c_int), intent(in) :: n, ndim, maxnz, nw
+         integer(c_int), intent(inout) :: jcoef(ndim, maxnz), iwksp(*), iparm(12), ier
+         real(c_double), intent(inout) :: coef(ndim, maxnz), rhs(n), u(n), wksp(nw), rparm(12)
+      end subroutine
+
+      subroutine adc_dfault(iparm, rparm) bind(C, name="adc_dfault")
+         import :: c_int, c_double
+         integer(c_int), intent(out) :: iparm(12)
+         real(c_double), intent(out) :: rparm(12)
+      end subroutine
+
+      integer(c_int) function adc_gpu_bind(p, a, prec, ctx) bind(C, name="adc_gpu_bind")
+         import :: c_int, c_ptr, adc_params_t, adc_arrays_t
+         type(adc_params_t), intent(in) :: p
+         type(adc_arrays_t), intent(in) :: a
+         integer(c_int), value :: prec
+         type(c_ptr), intent(out) :: ctx
+      end function
+
+      integer(c_int) function adc_gpu_free(ctx) bind(C, name="adc_gpu_free")
+         import :: c_int, c_ptr
+         type(c_ptr), value :: ctx
+      end function
+
+      integer(c_int) function adc_shift_friction(ctx, s) bind(C, name="adc_shift_friction")
+         import :: c_int, c_ptr, adc_step_t
+         type(c_ptr), value :: ctx
+         type(adc_step_t), intent(in) :: s
+      end function
+
+      integer(c_int) function adc_gwce_new(ctx, s, o) bind(C, name="adc_gwce_new")
+         import :: c_int, c_ptr, adc_step_t, adc_stepout_t
+         type(c_ptr), value :: ctx
+         type(adc_step_t), intent(in) :: s
+         type(adc_stepout_t), intent(out) :: o
+      end function
+
+      integer(c_int) function adc_wetdry(ctx, s, o) bind(C, name="adc_wetdry")
+         import :: c_int, c_ptr, adc_step_t, adc_stepout_t
+         type(c_ptr), value :: ctx
+         type(adc_step_t), intent(in) :: s
+         type(adc_stepout_t), intent(out) :: o
+      end function
+
+      integer(c_int) function adc_momentum(ctx, s) bind(C, name="adc_momentum")
+         import :: c_int, c_ptr, adc_step_t
+         type(c_ptr), value :: ctx
+         type(adc_step_t), intent(in) :: s
+      end function
+
+      integer(c_int) function adc_timestep(ctx, s, o) bind(C, name="adc_timestep")
+         import :: c_int, c_ptr, adc_step_t, adc_stepout_t
+         type(c_ptr), value :: ctx
+         type(adc_step_t), intent(in) :: s
+         type(adc_stepout_t), intent(out) :: o
+      end function
+
+      integer(c_int) function adc_sync_to_host(ctx) bind(C, name="adc_sync_to_host")
+         import :: c_int, c_ptr
+         type(c_ptr), value :: ctx
+      end function
+
+      integer(c_int) function adc_sync_from_host(ctx) bind(C, name="adc_sync_from_host")
+         import :: c_int, c_ptr
+         type(c_ptr), value :: ctx
+      end function
+
+      integer(c_int) function adc_set_met(ctx, wsx2, wsy2, pr2) bind(C, name="adc_set_met")
+         import :: c_int, c_ptr, c_double
+         type(c_ptr), value :: ctx
+         real(c_double), intent(in) :: wsx2(*), wsy2(*), pr2(*)
+      end function
+   end interface
+end module adcgpu_iface
