@@ -90,6 +90,7 @@ def load():
         "adc_jcg": (None, [ip_, ip_, ip_, ip_, dp_, dp_, dp_, ip_, ip_, dp_, ip_, dp_, ip_]),
         "adc_dfault": (None, [ip_, dp_]),
         "adc_jcg_reset": (None, []),
+        "adc_jcg_noalloc": (None, [ip_, ip_, ip_, ip_, dp_, dp_, dp_, ip_, ip_, dp_, ip_, dp_, ip_]),
         "adc_gpu_bind": (C.c_int, [C.POINTER(AdcParams), C.POINTER(AdcArrays), C.c_int,
                                     C.POINTER(vp)]),
         "adc_gpu_free": (C.c_int, [vp]),

@@ -23,6 +23,8 @@ int launch_jcg_impl(adc_ctx *c, int eta_update, int do_peror, int run_init);
 
 // ITPACK state that survives between jcg calls: itjcg's SAVEd q1 flag.
 static int g_q1 = 0;
+int jcg_q1_get() { return g_q1; }
+void jcg_q1_set(int v) { g_q1 = v; }
 
 struct Stage {
   adc_ctx c;

@@ -128,6 +128,21 @@ void adc_dfault(int *iparm, double *rparm);
  * flag of itjcg, itpackv.F:459-604) to its program-start value. */
 void adc_jcg_reset(void);
 
+/* jcg for callers that may not allocate device memory (a host that owns
+ * every device byte through its own pool, code that runs during a CUDA
+ * graph capture or on a thread where cudaMalloc is off limits).  No
+ * counterpart in the reference: same arguments and results as adc_jcg, but
+ * every device buffer is carved from one file-scope __device__ array of
+ * 32 MiB that each GPU loading the library holds until exit.  Systems
+ * needing more than about n*(20*(maxnz-1)+104) + 64 KiB bytes return
+ * ier = 905.  The first call on a device resolves the array's address and
+ * should come before any stream capture.  Calls share the array: calls
+ * whose GPU work overlaps race.  No cudaMalloc/cudaFree, no stream
+ * creation, no host heap allocation; work runs on the legacy stream. */
+void adc_jcg_noalloc(const int *n, const int *ndim, const int *maxnz, int *jcoef,
+                     double *coef, double *rhs, double *u, int *iwksp, const int *nw,
+                     double *wksp, int *iparm, double *rparm, int *ier);
+
 /* ------------------------------------------------------------------ */
 /* Device-resident 2DDI step (state stays in HBM between calls).       */
 /* ------------------------------------------------------------------ */
