@@ -117,6 +117,8 @@ struct adc_ctx {
   adc::Bar *bar;
   void *jlines;          // JCG barrier lines: 2 x 128 B per row block
   int jcg_grid, jcg_rows_blocks;
+  int jcg_wmax, jcg_spb, jcg_tma;   // widest slice, slices per block, bulk-copy path
+  size_t jcg_smem;
   // flags / steps
   adc::Flags *flags;
   adc_step_t *steps;     // device step table

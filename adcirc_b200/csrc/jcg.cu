@@ -25,6 +25,7 @@
 //  * Every barrier wait is bounded (clock64); on expiry the kernel records
 //    a timeout and all blocks return.
 #include "adc_internal.cuh"
+#include "tma.cuh"
 
 #include <cfloat>
 #include <cmath>
@@ -65,6 +66,8 @@ struct JcgArgs {
   Flags *flags;
   int eta_update;
   int do_peror;
+  int wmax;      // widest slice (slots)
+  int max_spb;   // most slices any row block owns
   const int *nodecode;
   const double *eta1;
   double *eta2;
@@ -453,14 +456,32 @@ __device__ Rec read_rec(const Rec *r) {
 }
 
 // ------------------------------------------------------------ the kernel
+template <bool kTma>
 __global__ void __launch_bounds__(kThreads, 2) jcg_kernel(JcgArgs a) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
   const bool scalar_block = (blockIdx.x == (unsigned)a.nrb);
   const int s0 = scalar_block ? 0 : (int)((long long)a.nslices * blockIdx.x / a.nrb);
   const int s1 = scalar_block ? 0 : (int)((long long)a.nslices * (blockIdx.x + 1) / a.nrb);
   const int n = a.n;
-  extern __shared__ double s_tri[];   // tri(:,1) and tri(:,2), scalar block only
-  double *t1 = s_tri, *t2 = s_tri + a.itmax + 1;
+  extern __shared__ __align__(128) unsigned char s_dyn[];
+  // dynamic shared memory: tri(:,1) and tri(:,2) (scalar block), then for
+  // the bulk-copy path 2 mbarriers per warp, the block's slice table and
+  // 2 staging buffers per warp
+  double *t1 = (double *)s_dyn, *t2 = t1 + a.itmax + 1;
+  const size_t tri_bytes = (2 * sizeof(double) * (a.itmax + 1) + 127) & ~(size_t)127;
+  uint64_t *s_bar = (uint64_t *)(s_dyn + tri_bytes);
+  int2 *s_meta = (int2 *)(s_dyn + tri_bytes + 128);
+  const size_t meta_bytes = ((size_t)a.max_spb * sizeof(int2) + 127) & ~(size_t)127;
+  const size_t stage_bytes = ((size_t)a.wmax * 384 + 1664 + 127) & ~(size_t)127;
+  unsigned char *s_stage = s_dyn + tri_bytes + 128 + meta_bytes;
+  uint32_t parbits = 0u;        // bit st: mbarrier phase of this warp's stage st
+  if (kTma && !scalar_block) {
+    if (threadIdx.x < 2 * (blockDim.x >> 5)) mbar_init(&s_bar[threadIdx.x], 1);
+    for (int k = threadIdx.x; k < s1 - s0; k += blockDim.x)
+      s_meta[k] = make_int2(a.sl_ptr[s0 + k], a.sl_w[s0 + k]);
+    mbar_fence_init();
+    __syncthreads();
+  }
   Rec *rec = &a.itp->rec;
   __shared__ ItpLocal L;              // used by the scalar block's thread 0 only
   unsigned gen = 0;                   // barrier generation within this launch
@@ -598,45 +619,142 @@ __global__ void __launch_bounds__(kThreads, 2) jcg_kernel(JcgArgs a) {
     const double *uc = U[in % 2];
     double *un = U[(in + 1) % 2];
     double pd = 0.0, pt = 0.0, pu = 0.0;
-    for (int s = s0 + warp; s < s1; s += nwarps) {
-      int i = s * kSlice + lane;
-      const int sn = s + nwarps;
-      if (sn < s1)
-        prefetch_slice(lane, a.sl_ptr[sn], a.sl_w[sn], sn * kSlice, a.col, a.soff, pc, uc, un);
-      if (i < n) {
-        const P4 me = ld_p4(pc + i);
-        double unew = c1 * me.y + c2 * uc[i] + c3 * un[i];
-        double dnew = c1 * me.x + c4 * me.y + c3 * me.z;
-        int len = a.rlen[i];
-        int base = a.sl_ptr[s] + lane;
-        double acc = 0.0;
-        for (int c0 = 0; c0 < len; c0 += kCh) {
-          int jj[kCh];
-          double vv[kCh];
-          P4 xx[kCh];
-#pragma unroll
-          for (int k = 0; k < kCh; ++k)
-            if (c0 + k < len) {
-              int idx = base + (c0 + k) * kSlice;
-              jj[k] = a.col[idx];
-              vv[k] = a.soff[idx];
-            }
-#pragma unroll
-          for (int k = 0; k < kCh; ++k)
-            if (c0 + k < len) xx[k] = ld_p4(pc + jj[k]);
-#pragma unroll
-          for (int k = 0; k < kCh; ++k)
-            if (c0 + k < len) {
-              double dj = c1 * xx[k].x + c4 * xx[k].y + c3 * xx[k].z;
-              acc = acc - vv[k] * dj;
-            }
+    if (!kTma) {
+      for (int s = s0 + warp; s < s1; s += nwarps) {
+        int i = s * kSlice + lane;
+        const int sn = s + nwarps;
+        if (sn < s1)
+          prefetch_slice(lane, a.sl_ptr[sn], a.sl_w[sn], sn * kSlice, a.col, a.soff, pc, uc, un);
+        if (i < n) {
+          const P4 me = ld_p4(pc + i);
+          double unew = c1 * me.y + c2 * uc[i] + c3 * un[i];
+          double dnew = c1 * me.x + c4 * me.y + c3 * me.z;
+          int len = a.rlen[i];
+          int base = a.sl_ptr[s] + lane;
+          double acc = 0.0;
+          for (int c0 = 0; c0 < len; c0 += kCh) {
+            int jj[kCh];
+            double vv[kCh];
+            P4 xx[kCh];
+  #pragma unroll
+            for (int k = 0; k < kCh; ++k)
+              if (c0 + k < len) {
+                int idx = base + (c0 + k) * kSlice;
+                jj[k] = a.col[idx];
+                vv[k] = a.soff[idx];
+              }
+  #pragma unroll
+            for (int k = 0; k < kCh; ++k)
+              if (c0 + k < len) xx[k] = ld_p4(pc + jj[k]);
+  #pragma unroll
+            for (int k = 0; k < kCh; ++k)
+              if (c0 + k < len) {
+                double dj = c1 * xx[k].x + c4 * xx[k].y + c3 * xx[k].z;
+                acc = acc - vv[k] * dj;
+              }
+          }
+          un[i] = unew;
+          st_p4(pn + i, acc, dnew, me.y, 0.0);
+          pd += dnew * dnew;
+          pt += dnew * acc;
+          if (need_u) pu += unew * unew;
         }
-        un[i] = unew;
-        st_p4(pn + i, acc, dnew, me.y, 0.0);
-        pd += dnew * dnew;
-        pt += dnew * acc;
-        if (need_u) pu += unew * unew;
       }
+    } else if (!scalar_block) {
+      // Bulk-copy pipeline: while a warp gathers for slice k, the column,
+      // value, own-record and u rows of slice k+1 stream into its other
+      // staging buffer.
+      unsigned char *const stg0 = s_stage + (size_t)(2 * warp) * stage_bytes;
+      uint64_t *const bar0 = &s_bar[2 * warp];
+      auto issue = [&](int sl, int st) {
+        if (lane == 0) {
+          const int2 mt = s_meta[sl - s0];
+          const int w = mt.y;
+          unsigned char *b = stg0 + (size_t)st * stage_bytes;
+          uint64_t *bar = bar0 + st;
+          const uint32_t bytes = (uint32_t)w * 384u + 1024u + 512u + 128u;
+          fence_proxy_async_all();
+          mbar_expect_tx(bar, bytes);
+          if (w > 0) {
+            bulk_load(b, a.col + mt.x, (uint32_t)w * 128u, bar);
+            bulk_load(b + (size_t)w * 128, a.soff + mt.x, (uint32_t)w * 256u, bar);
+          }
+          const size_t r0 = (size_t)sl * kSlice;
+          unsigned char *q = b + (size_t)a.wmax * 384;
+          bulk_load(q, pc + r0, 1024u, bar);
+          bulk_load(q + 1024, uc + r0, 256u, bar);
+          bulk_load(q + 1280, un + r0, 256u, bar);
+          bulk_load(q + 1536, a.rlen + r0, 128u, bar);
+        }
+      };
+      int k = 0;
+      if (s0 + warp < s1) issue(s0 + warp, 0);
+      for (int sl = s0 + warp; sl < s1; sl += nwarps, ++k) {
+        const int st = k & 1;
+        if (sl + nwarps < s1) issue(sl + nwarps, st ^ 1);
+        // bounded wait for this slice's bytes
+        {
+          long long t0 = clock64();
+          bool ok = true;
+          while (!mbar_try_wait(bar0 + st, (parbits >> st) & 1u)) {
+            if (clock64() - t0 > kSpinCycles) { ok = false; break; }
+          }
+          if (!ok) {
+            if (lane == 0) {
+              atomicExch(&a.flags->timeout, 1);
+              // let the copy already issued into the other buffer land
+              if (sl + nwarps < s1) {
+                long long t1w = clock64();
+                while (!mbar_try_wait(bar0 + (st ^ 1), (parbits >> (st ^ 1)) & 1u) &&
+                       clock64() - t1w < kSpinCycles) {
+                }
+              }
+            }
+            __syncwarp();
+            break;
+          }
+          parbits ^= 1u << st;
+        }
+        const int2 mt = s_meta[sl - s0];
+        const int w = mt.y;
+        const unsigned char *b = stg0 + (size_t)st * stage_bytes;
+        const int *scol = (const int *)b;
+        const double *sval = (const double *)(b + (size_t)w * 128);
+        const unsigned char *q = b + (size_t)a.wmax * 384;
+        const int i = sl * kSlice + lane;
+        if (i < n) {
+          const P4 me = ((const P4 *)q)[lane];
+          const double ucv = ((const double *)(q + 1024))[lane];
+          const double unv = ((const double *)(q + 1280))[lane];
+          const int len = ((const int *)(q + 1536))[lane];
+          double unew = c1 * me.y + c2 * ucv + c3 * unv;
+          double dnew = c1 * me.x + c4 * me.y + c3 * me.z;
+          double acc = 0.0;
+          for (int c0 = 0; c0 < len; c0 += kCh) {
+            int jj[kCh];
+            P4 xx[kCh];
+#pragma unroll
+            for (int kk = 0; kk < kCh; ++kk)
+              if (c0 + kk < len) jj[kk] = scol[(c0 + kk) * kSlice + lane];
+#pragma unroll
+            for (int kk = 0; kk < kCh; ++kk)
+              if (c0 + kk < len) xx[kk] = ld_p4(pc + jj[kk]);
+#pragma unroll
+            for (int kk = 0; kk < kCh; ++kk)
+              if (c0 + kk < len) {
+                double dj = c1 * xx[kk].x + c4 * xx[kk].y + c3 * xx[kk].z;
+                acc = acc - sval[(c0 + kk) * kSlice + lane] * dj;
+              }
+          }
+          un[i] = unew;
+          st_p4(pn + i, acc, dnew, me.y, 0.0);
+          pd += dnew * dnew;
+          pt += dnew * acc;
+          if (need_u) pu += unew * unew;
+        }
+        __syncwarp();
+      }
+      fence_proxy_async_global();
     }
     const int m = in + 1;
     if (scalar_block && threadIdx.x == 0 && L.adapt) chgcon_d(&L, t1, t2, m);
@@ -749,22 +867,55 @@ using namespace adc;
 
 namespace adc {
 
+static size_t jcg_smem_bytes(int itmax, bool tma, int wmax, int max_spb) {
+  size_t tri = (2 * sizeof(double) * (itmax + 1) + 127) & ~(size_t)127;
+  if (!tma) return tri;
+  size_t meta = ((size_t)max_spb * sizeof(int2) + 127) & ~(size_t)127;
+  size_t stage = ((size_t)wmax * 384 + 1664 + 127) & ~(size_t)127;
+  return tri + 128 + meta + 2 * (size_t)(kThreads / 32) * stage;
+}
+
+// Grid of the persistent solver: as many 256-thread row blocks as can be
+// co-resident (2 per SM), plus the scalar block; the bulk-copy pipeline is
+// used when its staging buffers fit next to that occupancy.
 int jcg_setup_grid(adc_ctx *c) {
-  int dev = 0, nsm = 0, per_sm = 0;
+  int dev = 0, nsm = 0;
   ADC_CUDA(cudaGetDevice(&dev));
   ADC_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-  size_t smem = 2 * sizeof(double) * (c->itmax + 1);
-  if (smem > 48 * 1024) { set_error("itmax too large for the JCG scalar block"); return ADC_ERR_ARG; }
-  ADC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, jcg_kernel, kThreads, smem));
-  if (per_sm < 1) { set_error("jcg kernel cannot be resident"); return ADC_ERR_CUDA; }
-  long long maxb = (long long)per_sm * nsm;
-  int nrb = (int)std::min<long long>(maxb - 1, c->nslices);
-  // keep at least ~8 slices per block so barrier cost stays amortised
-  nrb = std::max(1, std::min(nrb, std::max(1, c->nslices / 8)));
-  if (nrb > maxb - 1) nrb = (int)(maxb - 1);
-  c->jcg_rows_blocks = nrb;
-  c->jcg_grid = nrb + 1;
-  return ADC_OK;
+  if (2 * sizeof(double) * (c->itmax + 1) > 48 * 1024) {
+    set_error("itmax too large for the JCG scalar block");
+    return ADC_ERR_ARG;
+  }
+  if (c->jcg_wmax <= 0) c->jcg_wmax = 1;
+  for (int tma = 1; tma >= 0; --tma) {
+    const void *fn = tma ? (const void *)jcg_kernel<true> : (const void *)jcg_kernel<false>;
+    // first guess of the block count, then the slice table size it implies
+    int nrb = std::max(1, std::min(2 * nsm - 1, std::max(1, c->nslices / 8)));
+    int spb = (c->nslices + nrb - 1) / nrb + 1;
+    size_t smem = jcg_smem_bytes(c->itmax, tma, c->jcg_wmax, spb);
+    if (smem > 200 * 1024) continue;
+    ADC_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    ADC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kThreads, smem));
+    // the staged path only pays while two row blocks share an SM
+    if (per_sm < (tma ? 2 : 1)) continue;
+    long long maxb = (long long)per_sm * nsm;
+    if (nrb > maxb - 1) {
+      nrb = (int)(maxb - 1);
+      if (nrb < 1) continue;
+      spb = (c->nslices + nrb - 1) / nrb + 1;
+      smem = jcg_smem_bytes(c->itmax, tma, c->jcg_wmax, spb);
+      ADC_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    }
+    c->jcg_rows_blocks = nrb;
+    c->jcg_grid = nrb + 1;
+    c->jcg_tma = tma;
+    c->jcg_spb = spb;
+    c->jcg_smem = smem;
+    return ADC_OK;
+  }
+  set_error("jcg kernel cannot be resident");
+  return ADC_ERR_CUDA;
 }
 
 int launch_jcg_impl(adc_ctx *c, int eta_update, int do_peror, int run_init) {
@@ -798,6 +949,8 @@ int launch_jcg_impl(adc_ctx *c, int eta_update, int do_peror, int run_init) {
   a.nodecode = c->nodecode;
   a.eta1 = c->eta1;
   a.eta2 = c->eta2;
+  a.wmax = c->jcg_wmax;
+  a.max_spb = c->jcg_spb;
   int nwords = (int)(2 * 128 * (size_t)c->jcg_rows_blocks / 4);
   jcg_clear_lines<<<8, 256, 0, c->stream>>>((unsigned *)c->jlines, nwords);
   c->launches++;
@@ -806,9 +959,9 @@ int launch_jcg_impl(adc_ctx *c, int eta_update, int do_peror, int run_init) {
     c->launches++;
   }
   void *args[] = {&a};
-  size_t smem = 2 * sizeof(double) * (c->itmax + 1);
-  ADC_CUDA(cudaLaunchCooperativeKernel((const void *)jcg_kernel, dim3(c->jcg_grid),
-                                       dim3(kThreads), args, smem, c->stream));
+  const void *fn = c->jcg_tma ? (const void *)jcg_kernel<true> : (const void *)jcg_kernel<false>;
+  ADC_CUDA(cudaLaunchCooperativeKernel(fn, dim3(c->jcg_grid), dim3(kThreads), args, c->jcg_smem,
+                                       c->stream));
   c->launches++;
   return ADC_OK;
 }

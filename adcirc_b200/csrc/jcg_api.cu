@@ -92,16 +92,26 @@ static int jcg_solve(int n, int ndim, int maxnz, int *jcoef, double *coef, doubl
   ADC_CUDA(alloc_up(&c.sl_ptr, sl_ptr.data(), sl_ptr.size()));
   ADC_CUDA(alloc_up(&c.sl_w, sl_w.data(), sl_w.size()));
   ADC_CUDA(alloc_up(&c.col, col.data(), col.size()));
+  rlen.resize((size_t)nslices * kSlice, 0);
   ADC_CUDA(alloc_up(&c.rlen, rlen.data(), rlen.size()));
+  c.jcg_wmax = *std::max_element(sl_w.begin(), sl_w.end());
   ADC_CUDA(alloc_up(&c.offd, off.data(), off.size()));
   ADC_CUDA(alloc_up<double>(&c.soff, nullptr, off.size()));
   ADC_CUDA(alloc_up(&c.diag, diag.data(), n));
   ADC_CUDA(alloc_up(&c.gwce_lv, rhs, n));
-  ADC_CUDA(alloc_up(&c.etas, u, n));
+  const size_t npad = (size_t)nslices * kSlice;
+  ADC_CUDA(alloc_up<double>(&c.etas, nullptr, npad));
+  ADC_CUDA(cudaMemset(c.etas, 0, npad * sizeof(double)));
+  ADC_CUDA(cudaMemcpy(c.etas, u, n * sizeof(double), cudaMemcpyHostToDevice));
   double **vec[] = {&c.ju1, &c.jw};
-  for (double **v : vec) ADC_CUDA(alloc_up<double>(v, nullptr, n));
-  ADC_CUDA(alloc_up<double4>(&c.jp[0], nullptr, n));
-  ADC_CUDA(alloc_up<double4>(&c.jp[1], nullptr, n));
+  for (double **v : vec) {
+    ADC_CUDA(alloc_up<double>(v, nullptr, npad));
+    ADC_CUDA(cudaMemset(*v, 0, npad * sizeof(double)));
+  }
+  ADC_CUDA(alloc_up<double4>(&c.jp[0], nullptr, npad));
+  ADC_CUDA(alloc_up<double4>(&c.jp[1], nullptr, npad));
+  ADC_CUDA(cudaMemset(c.jp[0], 0, npad * sizeof(double4)));
+  ADC_CUDA(cudaMemset(c.jp[1], 0, npad * sizeof(double4)));
   int rc = jcg_setup_grid(&c);
   if (rc) return rc;
   ADC_CUDA(alloc_up<double>(&c.jpart, nullptr, 4 * (size_t)c.jcg_grid));

@@ -128,6 +128,7 @@ static int noalloc_solve(int n, int ndim, int maxnz, int *jcoef, double *coef, d
   c.nnz_pad = (int)slots;
   c.itmax = itmax;
   c.stream = 0;   // legacy default stream: nothing is created
+  c.jcg_wmax = w > 0 ? w : 1;
   rc = jcg_setup_grid(&c);
   if (rc) return rc;
   Carve cv{(char *)base, 0, kNoAllocBytes};
@@ -139,11 +140,12 @@ static int noalloc_solve(int n, int ndim, int maxnz, int *jcoef, double *coef, d
   c.soff = cv.take<double>(slots);
   c.diag = cv.take<double>(n);
   c.gwce_lv = cv.take<double>(n);
-  c.etas = cv.take<double>(n);
-  c.ju1 = cv.take<double>(n);
-  c.jw = cv.take<double>(n);
-  c.jp[0] = cv.take<double4>(n);
-  c.jp[1] = cv.take<double4>(n);
+  const size_t npad = (size_t)nslices * kSlice;
+  c.etas = cv.take<double>(npad);
+  c.ju1 = cv.take<double>(npad);
+  c.jw = cv.take<double>(npad);
+  c.jp[0] = cv.take<double4>(npad);
+  c.jp[1] = cv.take<double4>(npad);
   c.jpart = cv.take<double>(4 * (size_t)c.jcg_grid);
   c.jtri = cv.take<double>(4 * (size_t)(itmax > 2 ? itmax : 2));
   c.jlines = cv.take<char>(2 * 128 * (size_t)c.jcg_rows_blocks);
@@ -172,6 +174,10 @@ static int noalloc_solve(int n, int ndim, int maxnz, int *jcoef, double *coef, d
                                                                        c.col);
   ADC_CUDA(cudaGetLastError());
   ADC_CUDA(cudaMemcpy(c.gwce_lv, rhs, n * sizeof(double), cudaMemcpyHostToDevice));
+  ADC_CUDA(cudaMemset(c.etas, 0, npad * sizeof(double)));
+  ADC_CUDA(cudaMemset(c.ju1, 0, npad * sizeof(double)));
+  ADC_CUDA(cudaMemset(c.jp[0], 0, npad * sizeof(double4)));
+  ADC_CUDA(cudaMemset(c.jp[1], 0, npad * sizeof(double4)));
   ADC_CUDA(cudaMemcpy(c.etas, u, n * sizeof(double), cudaMemcpyHostToDevice));
   Itp it;
   memset(&it, 0, sizeof(it));

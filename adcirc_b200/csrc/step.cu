@@ -451,7 +451,13 @@ static int bind_impl(const adc_params_t *p, const adc_arrays_t *a, int prec, adc
   B(dalloc(&c->sl_ptr, nslices + 1)); B(up(c->sl_ptr, T.sl_ptr.data(), nslices + 1));
   B(dalloc(&c->sl_w, nslices)); B(up(c->sl_w, T.sl_w.data(), nslices));
   B(dalloc(&c->col, std::max(nnz_pad, 1))); B(up(c->col, T.col.data(), T.col.size()));
-  B(dalloc(&c->rlen, np)); B(up(c->rlen, T.rlen.data(), np));
+  const size_t npad = (size_t)nslices * kSlice;   // row arrays read by whole slices
+  {
+    std::vector<int> rl(npad, 0);
+    std::copy(T.rlen.begin(), T.rlen.end(), rl.begin());
+    B(dalloc(&c->rlen, npad)); B(up(c->rlen, rl.data(), npad));
+  }
+  c->jcg_wmax = *std::max_element(T.sl_w.begin(), T.sl_w.end());
   B(dalloc(&c->lhs_src, T.lhs_src.size())); B(up(c->lhs_src, T.lhs_src.data(), T.lhs_src.size()));
   B(dalloc(&c->nbd, T.nbd.size())); B(up(c->nbd, T.nbd.data(), T.nbd.size()));
   B(dalloc(&c->is_nbd, np)); B(up(c->is_nbd, T.is_nbd.data(), np));
@@ -478,8 +484,12 @@ static int bind_impl(const adc_params_t *p, const adc_arrays_t *a, int prec, adc
                          &c->wsx1, &c->wsy1, &c->wsx2, &c->wsy2, &c->pr1, &c->pr2, &c->gwce_lv,
                          &c->mom_x, &c->mom_y, &c->diag, &c->ju1, &c->jw, &c->met_wsx,
                          &c->met_wsy, &c->met_pr};
-  for (double **q : node_f64) B(dalloc(q, np));
-  B(dalloc(&c->jp[0], np)); B(dalloc(&c->jp[1], np));
+  for (double **q : node_f64) B(dalloc(q, npad));
+  B(dalloc(&c->jp[0], npad)); B(dalloc(&c->jp[1], npad));
+  ADC_CUDA(cudaMemset(c->etas, 0, npad * sizeof(double)));
+  ADC_CUDA(cudaMemset(c->ju1, 0, npad * sizeof(double)));
+  ADC_CUDA(cudaMemset(c->jp[0], 0, npad * sizeof(double4)));
+  ADC_CUDA(cudaMemset(c->jp[1], 0, npad * sizeof(double4)));
   B(dalloc(&c->tkm, 3 * (size_t)np));
   B(dalloc(&c->alphal, ne));
   int **node_i32[] = {&c->nodecode, &c->nnodecode, &c->mju};
