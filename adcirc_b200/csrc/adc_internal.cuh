@@ -65,6 +65,11 @@ struct Ctx;
 
 }  // namespace adc
 
+// Host copies of the sliced ELL handed to the solver setup (0-based columns).
+struct JcgHostSell {
+  const int *sl_ptr, *sl_w, *col, *rlen;
+};
+
 struct adc_ctx {
   // sizes
   int np, ne, mnei, neta, nbfr, nvel, nvelme, prec;
@@ -117,8 +122,12 @@ struct adc_ctx {
   adc::Bar *bar;
   void *jlines;          // JCG barrier lines: 2 x 128 B per row block
   int jcg_grid, jcg_rows_blocks;
-  int jcg_wmax, jcg_spb, jcg_tma;   // widest slice, slices per block, bulk-copy path
+  // JCG resident variant (block-local indices, halo lists, export flags)
+  int jcg_res, jcg_rows_max, jcg_halo_max, jcg_stage_bytes;
   size_t jcg_smem;
+  unsigned short *jlcol;
+  int *jhalo_ptr, *jhalo_ids;
+  unsigned char *jexp;
   // flags / steps
   adc::Flags *flags;
   adc_step_t *steps;     // device step table

@@ -66,8 +66,14 @@ struct JcgArgs {
   Flags *flags;
   int eta_update;
   int do_peror;
-  int wmax;      // widest slice (slots)
-  int max_spb;   // most slices any row block owns
+  // resident variant
+  int rows_max;               // rows of the largest row block
+  int halo_max;               // halo nodes of the largest row block
+  int stage_bytes;            // one staged slice: local columns + values
+  const unsigned short *lcol; // per slot: block-local value index
+  const int *halo_ptr;        // [nrb + 1] into halo_ids
+  const int *halo_ids;        // halo nodes of each row block (global rows)
+  const unsigned char *exp;   // per row: read by another row block
   const int *nodecode;
   const double *eta1;
   double *eta2;
@@ -456,32 +462,29 @@ __device__ Rec read_rec(const Rec *r) {
 }
 
 // ------------------------------------------------------------ the kernel
-template <bool kTma>
+template <int kRes>
 __global__ void __launch_bounds__(kThreads, 2) jcg_kernel(JcgArgs a) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
   const bool scalar_block = (blockIdx.x == (unsigned)a.nrb);
   const int s0 = scalar_block ? 0 : (int)((long long)a.nslices * blockIdx.x / a.nrb);
   const int s1 = scalar_block ? 0 : (int)((long long)a.nslices * (blockIdx.x + 1) / a.nrb);
   const int n = a.n;
+  const int r0 = s0 * kSlice, rows = (s1 - s0) * kSlice;   // the block's rows [r0, r0 + rows)
   extern __shared__ __align__(128) unsigned char s_dyn[];
-  // dynamic shared memory: tri(:,1) and tri(:,2) (scalar block), then for
-  // the bulk-copy path 2 mbarriers per warp, the block's slice table and
-  // 2 staging buffers per warp
+  // Dynamic shared memory.  Scalar block: tri(:,1) and tri(:,2).  Row blocks
+  // of the resident variant: dtwd of the block's rows; two value buffers
+  // (d of the rows, then the halo's new d) that trade roles every
+  // iteration; per row its length and export bit; the slice table; one
+  // mbarrier and two staging buffers per warp.
   double *t1 = (double *)s_dyn, *t2 = t1 + a.itmax + 1;
-  const size_t tri_bytes = (2 * sizeof(double) * (a.itmax + 1) + 127) & ~(size_t)127;
-  uint64_t *s_bar = (uint64_t *)(s_dyn + tri_bytes);
-  int2 *s_meta = (int2 *)(s_dyn + tri_bytes + 128);
-  const size_t meta_bytes = ((size_t)a.max_spb * sizeof(int2) + 127) & ~(size_t)127;
-  const size_t stage_bytes = ((size_t)a.wmax * 384 + 1664 + 127) & ~(size_t)127;
-  unsigned char *s_stage = s_dyn + tri_bytes + 128 + meta_bytes;
-  uint32_t parbits = 0u;        // bit st: mbarrier phase of this warp's stage st
-  if (kTma && !scalar_block) {
-    if (threadIdx.x < 2 * (blockDim.x >> 5)) mbar_init(&s_bar[threadIdx.x], 1);
-    for (int k = threadIdx.x; k < s1 - s0; k += blockDim.x)
-      s_meta[k] = make_int2(a.sl_ptr[s0 + k], a.sl_w[s0 + k]);
-    mbar_fence_init();
-    __syncthreads();
-  }
+  const int RB = a.rows_max, VB = a.rows_max + a.halo_max;
+  double *S_t = (double *)s_dyn;
+  double *S_dd = S_t + RB;
+  unsigned char *S_le = (unsigned char *)(S_dd + 2 * VB);
+  int2 *S_meta = (int2 *)(S_le + ((RB + 127) & ~127));
+  uint64_t *S_bar = (uint64_t *)(S_meta + ((RB / kSlice + 15) & ~15));
+  unsigned char *S_stage = (unsigned char *)(S_bar + 16);
+  uint32_t parbits = 0u;   // bit st: phase of this warp's mbarrier st
   Rec *rec = &a.itp->rec;
   __shared__ ItpLocal L;              // used by the scalar block's thread 0 only
   unsigned gen = 0;                   // barrier generation within this launch
@@ -553,6 +556,21 @@ __global__ void __launch_bounds__(kThreads, 2) jcg_kernel(JcgArgs a) {
   // P2: dtwd0 = -A' d0 and the iteration-0 norms; the scalar block runs
   // chgcon for in = 0 (ip = 0: cme = 0) while the rows work.
   Rec r = read_rec(rec);
+  if (kRes && !scalar_block) {
+    for (int idx = threadIdx.x; idx < rows; idx += blockDim.x) {
+      const int i = r0 + idx;
+      const bool in = i < n;
+      S_le[idx] = in ? (unsigned char)(a.rlen[i] | (a.exp[i] ? 128 : 0)) : 0;
+      S_t[idx] = 0.0;
+      S_dd[idx] = in ? a.p0[i].y : 0.0;   // d0
+      S_dd[VB + idx] = 0.0;               // d(-1)
+    }
+    for (int k = threadIdx.x; k < s1 - s0; k += blockDim.x)
+      S_meta[k] = make_int2(a.sl_ptr[s0 + k], a.sl_w[s0 + k]);
+    if (threadIdx.x < 2 * nwarps) mbar_init(&S_bar[threadIdx.x], 1);
+    mbar_fence_init();
+    __syncthreads();
+  }
   {
     double pd = 0.0, pt = 0.0, pu = 0.0;
     for (int s = s0 + warp; s < s1; s += nwarps) {
@@ -579,6 +597,7 @@ __global__ void __launch_bounds__(kThreads, 2) jcg_kernel(JcgArgs a) {
             if (c0 + k < len) acc = acc - vv[k] * xx[k];
         }
         a.p0[i].x = acc;
+        if (kRes) S_t[i - r0] = acc;
         double di = a.p0[i].y;
         pd += di * di;
         pt += di * acc;
@@ -609,6 +628,7 @@ __global__ void __launch_bounds__(kThreads, 2) jcg_kernel(JcgArgs a) {
   // a neighbour's three values arrive in one 32-byte sector.
   P4 *P[2] = {a.p0, a.p1};
   double *U[2] = {a.u, a.u1};
+  int cur = 0;   // resident variant: S_dd half holding d(in)
   for (int in = 0; in < a.itmax; ++in) {
     r = read_rec(rec);
     if (r.halt) break;
@@ -619,7 +639,7 @@ __global__ void __launch_bounds__(kThreads, 2) jcg_kernel(JcgArgs a) {
     const double *uc = U[in % 2];
     double *un = U[(in + 1) % 2];
     double pd = 0.0, pt = 0.0, pu = 0.0;
-    if (!kTma) {
+    if (!kRes) {
       for (int s = s0 + warp; s < s1; s += nwarps) {
         int i = s * kSlice + lane;
         const int sn = s + nwarps;
@@ -661,43 +681,56 @@ __global__ void __launch_bounds__(kThreads, 2) jcg_kernel(JcgArgs a) {
         }
       }
     } else if (!scalar_block) {
-      // Bulk-copy pipeline: while a warp gathers for slice k, the column,
-      // value, own-record and u rows of slice k+1 stream into its other
-      // staging buffer.
-      unsigned char *const stg0 = s_stage + (size_t)(2 * warp) * stage_bytes;
-      uint64_t *const bar0 = &s_bar[2 * warp];
+      // Resident variant.  Bulk copies of each warp's first two slices
+      // (block-local columns + values) start before phase A.
+      unsigned char *const stg0 = S_stage + (size_t)(2 * warp) * a.stage_bytes;
+      uint64_t *const bar0 = &S_bar[2 * warp];
       auto issue = [&](int sl, int st) {
         if (lane == 0) {
-          const int2 mt = s_meta[sl - s0];
-          const int w = mt.y;
-          unsigned char *b = stg0 + (size_t)st * stage_bytes;
-          uint64_t *bar = bar0 + st;
-          const uint32_t bytes = (uint32_t)w * 384u + 1024u + 512u + 128u;
-          fence_proxy_async_all();
-          mbar_expect_tx(bar, bytes);
+          const int2 mt = S_meta[sl - s0];
+          const uint32_t w = (uint32_t)mt.y;
+          unsigned char *b = stg0 + (size_t)st * a.stage_bytes;
+          mbar_expect_tx(bar0 + st, w * 320u);
           if (w > 0) {
-            bulk_load(b, a.col + mt.x, (uint32_t)w * 128u, bar);
-            bulk_load(b + (size_t)w * 128, a.soff + mt.x, (uint32_t)w * 256u, bar);
+            bulk_load(b, a.lcol + mt.x, w * 64u, bar0 + st);
+            bulk_load(b + w * 64u, a.soff + mt.x, w * 256u, bar0 + st);
           }
-          const size_t r0 = (size_t)sl * kSlice;
-          unsigned char *q = b + (size_t)a.wmax * 384;
-          bulk_load(q, pc + r0, 1024u, bar);
-          bulk_load(q + 1024, uc + r0, 256u, bar);
-          bulk_load(q + 1280, un + r0, 256u, bar);
-          bulk_load(q + 1536, a.rlen + r0, 128u, bar);
         }
       };
-      int k = 0;
+      if (lane == 0) fence_proxy_async_all();
       if (s0 + warp < s1) issue(s0 + warp, 0);
+      if (s0 + warp + nwarps < s1) issue(s0 + warp + nwarps, 1);
+      // Phase A: the 3-term update of the block's rows, d(in+1) written
+      // over d(in-1); then the new d of the halo nodes from their owners'
+      // exported records (same expression, same bits).
+      double *Sd = S_dd + cur * VB, *Sdn = S_dd + (cur ^ 1) * VB;
+      for (int idx = threadIdx.x; idx < rows; idx += blockDim.x) {
+        const int i = r0 + idx;
+        if (i < n) {
+          const double dn = c1 * S_t[idx] + c4 * Sd[idx] + c3 * Sdn[idx];
+          const double unew = c1 * Sd[idx] + c2 * uc[i] + c3 * un[i];
+          Sdn[idx] = dn;
+          un[i] = unew;
+          if (need_u) pu += unew * unew;
+        }
+      }
+      {
+        const int h0 = a.halo_ptr[blockIdx.x], nh = a.halo_ptr[blockIdx.x + 1] - h0;
+        for (int h = threadIdx.x; h < nh; h += blockDim.x) {
+          const P4 o = ld_p4(pc + a.halo_ids[h0 + h]);
+          Sdn[RB + h] = c1 * o.x + c4 * o.y + c3 * o.z;
+        }
+      }
+      __syncthreads();
+      // Phase B: the SpMV from shared memory, slot order as in pjac.
+      int k = 0;
       for (int sl = s0 + warp; sl < s1; sl += nwarps, ++k) {
         const int st = k & 1;
-        if (sl + nwarps < s1) issue(sl + nwarps, st ^ 1);
-        // bounded wait for this slice's bytes
         {
-          long long t0 = clock64();
+          long long tw = clock64();
           bool ok = true;
           while (!mbar_try_wait(bar0 + st, (parbits >> st) & 1u)) {
-            if (clock64() - t0 > kSpinCycles) { ok = false; break; }
+            if (clock64() - tw > kSpinCycles) { ok = false; break; }
           }
           if (!ok) {
             if (lane == 0) {
@@ -715,46 +748,31 @@ __global__ void __launch_bounds__(kThreads, 2) jcg_kernel(JcgArgs a) {
           }
           parbits ^= 1u << st;
         }
-        const int2 mt = s_meta[sl - s0];
-        const int w = mt.y;
-        const unsigned char *b = stg0 + (size_t)st * stage_bytes;
-        const int *scol = (const int *)b;
-        const double *sval = (const double *)(b + (size_t)w * 128);
-        const unsigned char *q = b + (size_t)a.wmax * 384;
+        const int w = S_meta[sl - s0].y;
+        const unsigned char *b = stg0 + (size_t)st * a.stage_bytes;
+        const unsigned short *lc = (const unsigned short *)b;
+        const double *lv = (const double *)(b + (size_t)w * 64);
         const int i = sl * kSlice + lane;
+        const int idx = i - r0;
+        double acc = 0.0;
+        double dn = 0.0;
+        const unsigned le = S_le[idx];
         if (i < n) {
-          const P4 me = ((const P4 *)q)[lane];
-          const double ucv = ((const double *)(q + 1024))[lane];
-          const double unv = ((const double *)(q + 1280))[lane];
-          const int len = ((const int *)(q + 1536))[lane];
-          double unew = c1 * me.y + c2 * ucv + c3 * unv;
-          double dnew = c1 * me.x + c4 * me.y + c3 * me.z;
-          double acc = 0.0;
-          for (int c0 = 0; c0 < len; c0 += kCh) {
-            int jj[kCh];
-            P4 xx[kCh];
-#pragma unroll
-            for (int kk = 0; kk < kCh; ++kk)
-              if (c0 + kk < len) jj[kk] = scol[(c0 + kk) * kSlice + lane];
-#pragma unroll
-            for (int kk = 0; kk < kCh; ++kk)
-              if (c0 + kk < len) xx[kk] = ld_p4(pc + jj[kk]);
-#pragma unroll
-            for (int kk = 0; kk < kCh; ++kk)
-              if (c0 + kk < len) {
-                double dj = c1 * xx[kk].x + c4 * xx[kk].y + c3 * xx[kk].z;
-                acc = acc - sval[(c0 + kk) * kSlice + lane] * dj;
-              }
-          }
-          un[i] = unew;
-          st_p4(pn + i, acc, dnew, me.y, 0.0);
-          pd += dnew * dnew;
-          pt += dnew * acc;
-          if (need_u) pu += unew * unew;
+          const int len = (int)(le & 127u);
+#pragma unroll 4
+          for (int q = 0; q < len; ++q) acc = acc - lv[q * kSlice + lane] * Sdn[lc[q * kSlice + lane]];
+          dn = Sdn[idx];
         }
         __syncwarp();
+        if (sl + 2 * nwarps < s1) issue(sl + 2 * nwarps, st);
+        if (i < n) {
+          if (le & 128u) st_p4(pn + i, acc, dn, Sd[idx], 0.0);
+          S_t[idx] = acc;
+          pd += dn * dn;
+          pt += dn * acc;
+        }
       }
-      fence_proxy_async_global();
+      cur ^= 1;
     }
     const int m = in + 1;
     if (scalar_block && threadIdx.x == 0 && L.adapt) chgcon_d(&L, t1, t2, m);
@@ -867,18 +885,75 @@ using namespace adc;
 
 namespace adc {
 
-static size_t jcg_smem_bytes(int itmax, bool tma, int wmax, int max_spb) {
-  size_t tri = (2 * sizeof(double) * (itmax + 1) + 127) & ~(size_t)127;
-  if (!tma) return tri;
-  size_t meta = ((size_t)max_spb * sizeof(int2) + 127) & ~(size_t)127;
-  size_t stage = ((size_t)wmax * 384 + 1664 + 127) & ~(size_t)127;
-  return tri + 128 + meta + 2 * (size_t)(kThreads / 32) * stage;
+static size_t round_up(size_t v, size_t m) { return (v + m - 1) / m * m; }
+
+static size_t jcg_stage_bytes(int wmax) { return round_up((size_t)std::max(wmax, 1) * 320, 128); }
+
+// Dynamic shared memory of one block (the largest of the scalar block's
+// tridiagonal and a resident row block's layout, see jcg_kernel).
+static size_t jcg_smem_bytes(int itmax, bool res, int rows_max, int halo_max, int wmax) {
+  size_t tri = round_up(2 * sizeof(double) * (itmax + 1), 128);
+  if (!res) return tri;
+  size_t rb = (size_t)rows_max, vb = rb + (size_t)halo_max;
+  size_t rowb = 8 * rb + 16 * vb + round_up(rb, 128) + 8 * round_up(rb / kSlice, 16) + 128 +
+                16 * jcg_stage_bytes(wmax);
+  return std::max(tri, rowb);
+}
+
+static int jcg_row_block_begin(int nslices, int nrb, int b) {
+  return (int)((long long)nslices * b / nrb);
+}
+
+// Block-local column indices of the resident variant.  Row block b owns the
+// rows of slices [s0, s1); a neighbour in that range maps to its offset
+// from the block's first row, any other neighbour to rows_max + its
+// position in the block's halo list (first appearance in slot order).
+// exp[j] = 1 marks rows that another block reads.
+static void jcg_local_tables(int n, int nslices, int nrb, int rows_max, const int *sl_ptr,
+                             const int *sl_w, const int *col, const int *rlen,
+                             std::vector<unsigned short> &lcol, std::vector<int> &halo_ptr,
+                             std::vector<int> &halo_ids, std::vector<unsigned char> &exp,
+                             int &halo_max) {
+  lcol.assign(std::max(sl_ptr[nslices], 1), 0);
+  halo_ptr.assign(nrb + 1, 0);
+  halo_ids.clear();
+  exp.assign((size_t)nslices * kSlice, 0);
+  std::vector<int> stamp(n, -1), hid(n, 0);
+  halo_max = 0;
+  for (int b = 0; b < nrb; ++b) {
+    const int s0 = jcg_row_block_begin(nslices, nrb, b), s1 = jcg_row_block_begin(nslices, nrb, b + 1);
+    const int r0 = s0 * kSlice, rows = (s1 - s0) * kSlice;
+    int nh = 0;
+    for (int sl = s0; sl < s1; ++sl)
+      for (int k = 0; k < sl_w[sl]; ++k)
+        for (int lane = 0; lane < kSlice; ++lane) {
+          const int i = sl * kSlice + lane;
+          if (i >= n || k >= rlen[i]) continue;
+          const size_t q = (size_t)sl_ptr[sl] + (size_t)k * kSlice + lane;
+          const int j = col[q];
+          if (j >= r0 && j < r0 + rows) {
+            lcol[q] = (unsigned short)(j - r0);
+            continue;
+          }
+          if (stamp[j] != b) {
+            stamp[j] = b;
+            hid[j] = nh++;
+            halo_ids.push_back(j);
+            exp[j] = 1;
+          }
+          lcol[q] = (unsigned short)(rows_max + hid[j]);
+        }
+    halo_ptr[b + 1] = halo_ptr[b] + nh;
+    halo_max = std::max(halo_max, nh);
+  }
 }
 
 // Grid of the persistent solver: as many 256-thread row blocks as can be
-// co-resident (2 per SM), plus the scalar block; the bulk-copy pipeline is
-// used when its staging buffers fit next to that occupancy.
-int jcg_setup_grid(adc_ctx *c) {
+// co-resident (2 per SM), plus the scalar block.  The resident variant is
+// used when host copies of the sliced ELL are given and each row block's
+// vectors and staging buffers fit in shared memory at 2 blocks per SM;
+// its tables are built and uploaded here.
+int jcg_setup_grid(adc_ctx *c, const JcgHostSell *h) {
   int dev = 0, nsm = 0;
   ADC_CUDA(cudaGetDevice(&dev));
   ADC_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
@@ -886,36 +961,67 @@ int jcg_setup_grid(adc_ctx *c) {
     set_error("itmax too large for the JCG scalar block");
     return ADC_ERR_ARG;
   }
-  if (c->jcg_wmax <= 0) c->jcg_wmax = 1;
-  for (int tma = 1; tma >= 0; --tma) {
-    const void *fn = tma ? (const void *)jcg_kernel<true> : (const void *)jcg_kernel<false>;
-    // first guess of the block count, then the slice table size it implies
-    int nrb = std::max(1, std::min(2 * nsm - 1, std::max(1, c->nslices / 8)));
-    int spb = (c->nslices + nrb - 1) / nrb + 1;
-    size_t smem = jcg_smem_bytes(c->itmax, tma, c->jcg_wmax, spb);
-    if (smem > 200 * 1024) continue;
-    ADC_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    int per_sm = 0;
-    ADC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kThreads, smem));
-    // the staged path only pays while two row blocks share an SM
-    if (per_sm < (tma ? 2 : 1)) continue;
-    long long maxb = (long long)per_sm * nsm;
-    if (nrb > maxb - 1) {
-      nrb = (int)(maxb - 1);
-      if (nrb < 1) continue;
-      spb = (c->nslices + nrb - 1) / nrb + 1;
-      smem = jcg_smem_bytes(c->itmax, tma, c->jcg_wmax, spb);
-      ADC_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  // keep at least ~8 slices per block so the barrier cost stays amortised
+  const int nrb0 = std::max(1, std::min(2 * nsm - 1, std::max(1, c->nslices / 8)));
+  c->jcg_res = 0;
+  if (h) {
+    const int nrb = nrb0;
+    const int rows_max = (c->nslices + nrb - 1) / nrb * kSlice;
+    int wmax = 1;
+    for (int sl = 0; sl < c->nslices; ++sl) wmax = std::max(wmax, h->sl_w[sl]);
+    std::vector<unsigned short> lcol;
+    std::vector<int> hptr, hids;
+    std::vector<unsigned char> exp;
+    int halo_max = 0;
+    bool fits = wmax < 128;
+    if (fits) {
+      jcg_local_tables(c->np, c->nslices, nrb, rows_max, h->sl_ptr, h->sl_w, h->col, h->rlen,
+                       lcol, hptr, hids, exp, halo_max);
+      fits = rows_max + halo_max < 65536;
     }
-    c->jcg_rows_blocks = nrb;
-    c->jcg_grid = nrb + 1;
-    c->jcg_tma = tma;
-    c->jcg_spb = spb;
-    c->jcg_smem = smem;
-    return ADC_OK;
+    size_t smem = jcg_smem_bytes(c->itmax, true, rows_max, halo_max, wmax);
+    int per_sm = 0;
+    if (fits && smem <= 200 * 1024) {
+      const void *fn = (const void *)jcg_kernel<1>;
+      ADC_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      ADC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kThreads, smem));
+    }
+    if (per_sm >= 2 && (long long)per_sm * nsm >= nrb + 1) {
+      ADC_CUDA(cudaMalloc((void **)&c->jlcol, lcol.size() * sizeof(unsigned short)));
+      ADC_CUDA(cudaMemcpy(c->jlcol, lcol.data(), lcol.size() * sizeof(unsigned short),
+                          cudaMemcpyHostToDevice));
+      ADC_CUDA(cudaMalloc((void **)&c->jhalo_ptr, hptr.size() * sizeof(int)));
+      ADC_CUDA(cudaMemcpy(c->jhalo_ptr, hptr.data(), hptr.size() * sizeof(int), cudaMemcpyHostToDevice));
+      ADC_CUDA(cudaMalloc((void **)&c->jhalo_ids, std::max<size_t>(hids.size(), 1) * sizeof(int)));
+      if (!hids.empty())
+        ADC_CUDA(cudaMemcpy(c->jhalo_ids, hids.data(), hids.size() * sizeof(int), cudaMemcpyHostToDevice));
+      ADC_CUDA(cudaMalloc((void **)&c->jexp, exp.size()));
+      ADC_CUDA(cudaMemcpy(c->jexp, exp.data(), exp.size(), cudaMemcpyHostToDevice));
+      c->jcg_rows_blocks = nrb;
+      c->jcg_grid = nrb + 1;
+      c->jcg_res = 1;
+      c->jcg_rows_max = rows_max;
+      c->jcg_halo_max = halo_max;
+      c->jcg_stage_bytes = (int)jcg_stage_bytes(wmax);
+      c->jcg_smem = smem;
+      return ADC_OK;
+    }
   }
-  set_error("jcg kernel cannot be resident");
-  return ADC_ERR_CUDA;
+  const void *fn = (const void *)jcg_kernel<0>;
+  size_t smem = jcg_smem_bytes(c->itmax, false, 0, 0, 1);
+  ADC_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int per_sm = 0;
+  ADC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kThreads, smem));
+  if (per_sm < 1) {
+    set_error("jcg kernel cannot be resident");
+    return ADC_ERR_CUDA;
+  }
+  const long long maxb = (long long)per_sm * nsm;
+  const int nrb = (int)std::max<long long>(1, std::min<long long>(nrb0, maxb - 1));
+  c->jcg_rows_blocks = nrb;
+  c->jcg_grid = nrb + 1;
+  c->jcg_smem = smem;
+  return ADC_OK;
 }
 
 int launch_jcg_impl(adc_ctx *c, int eta_update, int do_peror, int run_init) {
@@ -949,8 +1055,13 @@ int launch_jcg_impl(adc_ctx *c, int eta_update, int do_peror, int run_init) {
   a.nodecode = c->nodecode;
   a.eta1 = c->eta1;
   a.eta2 = c->eta2;
-  a.wmax = c->jcg_wmax;
-  a.max_spb = c->jcg_spb;
+  a.rows_max = c->jcg_rows_max;
+  a.halo_max = c->jcg_halo_max;
+  a.stage_bytes = c->jcg_stage_bytes;
+  a.lcol = c->jlcol;
+  a.halo_ptr = c->jhalo_ptr;
+  a.halo_ids = c->jhalo_ids;
+  a.exp = c->jexp;
   int nwords = (int)(2 * 128 * (size_t)c->jcg_rows_blocks / 4);
   jcg_clear_lines<<<8, 256, 0, c->stream>>>((unsigned *)c->jlines, nwords);
   c->launches++;
@@ -959,7 +1070,7 @@ int launch_jcg_impl(adc_ctx *c, int eta_update, int do_peror, int run_init) {
     c->launches++;
   }
   void *args[] = {&a};
-  const void *fn = c->jcg_tma ? (const void *)jcg_kernel<true> : (const void *)jcg_kernel<false>;
+  const void *fn = c->jcg_res ? (const void *)jcg_kernel<1> : (const void *)jcg_kernel<0>;
   ADC_CUDA(cudaLaunchCooperativeKernel(fn, dim3(c->jcg_grid), dim3(kThreads), args, c->jcg_smem,
                                        c->stream));
   c->launches++;

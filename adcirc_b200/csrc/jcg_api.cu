@@ -18,7 +18,7 @@
 #include <algorithm>
 
 namespace adc {
-int jcg_setup_grid(adc_ctx *c);
+int jcg_setup_grid(adc_ctx *c, const JcgHostSell *h);
 int launch_jcg_impl(adc_ctx *c, int eta_update, int do_peror, int run_init);
 
 // ITPACK state that survives between jcg calls: itjcg's SAVEd q1 flag.
@@ -31,7 +31,7 @@ struct Stage {
   Stage() { memset((void *)&c, 0, sizeof(c)); }
   ~Stage() {
     void *ptrs[] = {c.sl_ptr, c.sl_w, c.col, c.rlen, c.offd, c.soff, c.diag, c.gwce_lv,
-                    c.etas, c.ju1, c.jp[0], c.jp[1], c.jw,
+                    c.etas, c.ju1, c.jp[0], c.jp[1], c.jw, c.jexp, c.jlcol, c.jhalo_ptr, c.jhalo_ids,
                     c.jpart, c.jtri, c.itp, c.bar, c.flags, c.jlines};
     for (void *p : ptrs)
       if (p) cudaFree(p);
@@ -94,7 +94,6 @@ static int jcg_solve(int n, int ndim, int maxnz, int *jcoef, double *coef, doubl
   ADC_CUDA(alloc_up(&c.col, col.data(), col.size()));
   rlen.resize((size_t)nslices * kSlice, 0);
   ADC_CUDA(alloc_up(&c.rlen, rlen.data(), rlen.size()));
-  c.jcg_wmax = *std::max_element(sl_w.begin(), sl_w.end());
   ADC_CUDA(alloc_up(&c.offd, off.data(), off.size()));
   ADC_CUDA(alloc_up<double>(&c.soff, nullptr, off.size()));
   ADC_CUDA(alloc_up(&c.diag, diag.data(), n));
@@ -112,7 +111,8 @@ static int jcg_solve(int n, int ndim, int maxnz, int *jcoef, double *coef, doubl
   ADC_CUDA(alloc_up<double4>(&c.jp[1], nullptr, npad));
   ADC_CUDA(cudaMemset(c.jp[0], 0, npad * sizeof(double4)));
   ADC_CUDA(cudaMemset(c.jp[1], 0, npad * sizeof(double4)));
-  int rc = jcg_setup_grid(&c);
+  const JcgHostSell hs{sl_ptr.data(), sl_w.data(), col.data(), rlen.data()};
+  int rc = jcg_setup_grid(&c, &hs);
   if (rc) return rc;
   ADC_CUDA(alloc_up<double>(&c.jpart, nullptr, 4 * (size_t)c.jcg_grid));
   ADC_CUDA(alloc_up<double>(&c.jtri, nullptr, 4 * (size_t)std::max(itmax, 2)));

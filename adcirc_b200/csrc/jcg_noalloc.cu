@@ -9,7 +9,7 @@
 // buffer (matrix, vectors, barrier lines, ITPACK scalars) out of the static
 // array below.  Limits and behaviour:
 //  * capacity ADC_JCG_NOALLOC_BYTES (32 MiB); a system needs about
-//    n * (20 * (maxnz - 1) + 104) bytes plus 64 KiB, e.g. n <= 80,000 at
+//    n * (20 * (maxnz - 1) + 112) bytes plus 64 KiB, e.g. n <= 80,000 at
 //    maxnz = 16; larger systems return ier = 905 with a message in
 //    adc_last_error();
 //  * the array is held by every GPU that loads the library until the
@@ -29,7 +29,7 @@
 #include <cstring>
 
 namespace adc {
-int jcg_setup_grid(adc_ctx *c);
+int jcg_setup_grid(adc_ctx *c, const JcgHostSell *h);
 int launch_jcg_impl(adc_ctx *c, int eta_update, int do_peror, int run_init);
 int jcg_q1_get();
 void jcg_q1_set(int v);
@@ -128,8 +128,7 @@ static int noalloc_solve(int n, int ndim, int maxnz, int *jcoef, double *coef, d
   c.nnz_pad = (int)slots;
   c.itmax = itmax;
   c.stream = 0;   // legacy default stream: nothing is created
-  c.jcg_wmax = w > 0 ? w : 1;
-  rc = jcg_setup_grid(&c);
+  rc = jcg_setup_grid(&c, nullptr);   // the direct variant: no host tables
   if (rc) return rc;
   Carve cv{(char *)base, 0, kNoAllocBytes};
   c.sl_ptr = cv.take<int>(nslices + 1);
@@ -154,7 +153,7 @@ static int noalloc_solve(int n, int ndim, int maxnz, int *jcoef, double *coef, d
   c.flags = cv.take<Flags>(1);
   if (!c.flags) {
     set_error("adc_jcg_noalloc: n = %d, maxnz = %d needs more than the %zu-byte static scratch "
-              "(about n*(20*(maxnz-1)+104) bytes plus 64 KiB)", n, maxnz, kNoAllocBytes);
+              "(about n*(20*(maxnz-1)+112) bytes plus 64 KiB)", n, maxnz, kNoAllocBytes);
     return ADC_ERR_NOMEM;
   }
   // matrix: column 1 is the diagonal, columns 2..maxnz the sliced ELL
@@ -238,7 +237,7 @@ void adc_jcg_noalloc(const int *n_, const int *ndim_, const int *maxnz_, int *jc
   const int itmax = iparm[0];
   if (n <= 0) { *ier = 11; return; }
   if (ndim < n || maxnz < 1) { *ier = 11; set_error("ndim < n or maxnz < 1"); return; }
-  const size_t need = (size_t)n * (20 * (size_t)(maxnz - 1) + 104) + 65536;
+  const size_t need = (size_t)n * (20 * (size_t)(maxnz - 1) + 112) + 65536;
   if (need > kNoAllocBytes) {
     *ier = 905;
     set_error("adc_jcg_noalloc: n = %d, maxnz = %d needs about %zu bytes; the static scratch "

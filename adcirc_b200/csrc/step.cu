@@ -29,7 +29,7 @@ int cuda_fail(cudaError_t e, const char *what) {
   return ADC_ERR_CUDA;
 }
 
-int jcg_setup_grid(adc_ctx *c);
+int jcg_setup_grid(adc_ctx *c, const JcgHostSell *h);
 
 // kernels defined in the other translation units
 __global__ void k_shift_friction(adc_ctx c, const adc_step_t *steps, const Flags *flags);
@@ -383,7 +383,8 @@ static void free_ctx(adc_ctx *c) {
       (void **)&c->diag, (void **)&c->offd, (void **)&c->obccoef, (void **)&c->ebuf,
       (void **)&c->ebuf2, (void **)&c->red, (void **)&c->ev_cnt, (void **)&c->ev_a,
       (void **)&c->ev_b, (void **)&c->ev_c, (void **)&c->ju1, (void **)&c->jp[0],
-      (void **)&c->jp[1], (void **)&c->jw, (void **)&c->soff, (void **)&c->jpart, (void **)&c->jtri,
+      (void **)&c->jp[1], (void **)&c->jw, (void **)&c->jexp, (void **)&c->jlcol,
+      (void **)&c->jhalo_ptr, (void **)&c->jhalo_ids, (void **)&c->soff, (void **)&c->jpart, (void **)&c->jtri,
       (void **)&c->itp, (void **)&c->bar, (void **)&c->jlines, (void **)&c->flags, (void **)&c->steps,
       (void **)&c->numitr_log, (void **)&c->met_wsx, (void **)&c->met_wsy,
       (void **)&c->met_pr};
@@ -457,7 +458,6 @@ static int bind_impl(const adc_params_t *p, const adc_arrays_t *a, int prec, adc
     std::copy(T.rlen.begin(), T.rlen.end(), rl.begin());
     B(dalloc(&c->rlen, npad)); B(up(c->rlen, rl.data(), npad));
   }
-  c->jcg_wmax = *std::max_element(T.sl_w.begin(), T.sl_w.end());
   B(dalloc(&c->lhs_src, T.lhs_src.size())); B(up(c->lhs_src, T.lhs_src.data(), T.lhs_src.size()));
   B(dalloc(&c->nbd, T.nbd.size())); B(up(c->nbd, T.nbd.data(), T.nbd.size()));
   B(dalloc(&c->is_nbd, np)); B(up(c->is_nbd, T.is_nbd.data(), np));
@@ -503,7 +503,10 @@ static int bind_impl(const adc_params_t *p, const adc_arrays_t *a, int prec, adc
   B(dalloc(&c->ev_cnt, c->ev_blocks));
   B(dalloc(&c->ev_a, (size_t)c->ev_blocks * 256)); B(dalloc(&c->ev_b, (size_t)c->ev_blocks * 256));
   B(dalloc(&c->ev_c, (size_t)c->ev_blocks * 256));
-  B(jcg_setup_grid(c));
+  {
+    const JcgHostSell hs{T.sl_ptr.data(), T.sl_w.data(), T.col.data(), T.rlen.data()};
+    B(jcg_setup_grid(c, &hs));
+  }
   B(dalloc(&c->jpart, 4 * (size_t)c->jcg_grid));
   B(dalloc(&c->jtri, 4 * (size_t)std::max(c->itmax, 2)));
   B(dalloc(&c->itp, 1)); B(dalloc(&c->bar, 1));

@@ -134,7 +134,7 @@ void adc_jcg_reset(void);
  * counterpart in the reference: same arguments and results as adc_jcg, but
  * every device buffer is carved from one file-scope __device__ array of
  * 32 MiB that each GPU loading the library holds until exit.  Systems
- * needing more than about n*(20*(maxnz-1)+104) + 64 KiB bytes return
+ * needing more than about n*(20*(maxnz-1)+112) + 64 KiB bytes return
  * ier = 905.  The first call on a device resolves the array's address and
  * should come before any stream capture.  Calls share the array: calls
  * whose GPU work overlaps race.  No cudaMalloc/cudaFree, no stream
