@@ -368,6 +368,7 @@ __device__ void parcon_d(ItpLocal *it, int in, double dtnrm, double c[4]) {
 // values are gathered, so the loads of a chunk are in flight together.
 // Accumulation keeps the slot order (pjac's j order).
 constexpr int kCh = 6;
+constexpr int kRowUnroll = 8;   // rows per thread whose loads issue together
 
 // L2 prefetch of the next slice of a warp: the column and value rows of its
 // slots and its own-row vector entries, one 128-byte line per lane.
@@ -461,6 +462,76 @@ __device__ Rec read_rec(const Rec *r) {
   return o;
 }
 
+// Per-warp double-buffered bulk copies of whole slices (block-local
+// columns + one value array) into shared memory, for the resident variant.
+// Every copy that is issued is waited for before the next phase.
+struct SlicePipe {
+  unsigned char *stg0;        // this warp's two buffers
+  uint64_t *bar0;             // and their mbarriers
+  const int2 *meta;           // per slice of the block: (first slot, width)
+  const unsigned short *lcol;
+  Flags *flags;
+  int stage_bytes, s0, s1, first, step, lane;
+  uint32_t parbits;
+
+  __device__ void issue(int sl, int st, const double *vals) {
+    if (lane == 0) {
+      const int2 mt = meta[sl - s0];
+      const uint32_t w = (uint32_t)mt.y;
+      unsigned char *b = stg0 + (size_t)st * stage_bytes;
+      mbar_expect_tx(bar0 + st, w * 320u);
+      if (w > 0) {
+        bulk_load(b, lcol + mt.x, w * 64u, bar0 + st);
+        bulk_load(b + w * 64u, vals + mt.x, w * 256u, bar0 + st);
+      }
+    }
+  }
+  // Orders earlier generic writes of `vals` before the copies, then starts
+  // the warp's first two slices.
+  __device__ void begin(const double *vals) {
+    if (lane == 0) fence_proxy_async_all();
+    if (first < s1) issue(first, 0, vals);
+    if (first + step < s1) issue(first + step, 1, vals);
+  }
+  __device__ bool wait(int st, bool other_in_flight) {
+    long long tw = clock64();
+    while (!mbar_try_wait(bar0 + st, (parbits >> st) & 1u)) {
+      if (clock64() - tw > kSpinCycles) {
+        if (lane == 0) {
+          atomicExch(&flags->timeout, 1);
+          // let the copy already issued into the other buffer land
+          if (other_in_flight) {
+            long long t1w = clock64();
+            while (!mbar_try_wait(bar0 + (st ^ 1), (parbits >> (st ^ 1)) & 1u) &&
+                   clock64() - t1w < kSpinCycles) {
+            }
+          }
+        }
+        __syncwarp();
+        return false;
+      }
+    }
+    parbits ^= 1u << st;
+    return true;
+  }
+  // body(sl, lc, lv): one slice from shared memory; lc/lv hold slot q of
+  // lane l at [q * 32 + l].  Returns false on an expired wait.
+  template <class F>
+  __device__ bool run(const double *vals, F body) {
+    int k = 0;
+    for (int sl = first; sl < s1; sl += step, ++k) {
+      const int st = k & 1;
+      if (!wait(st, sl + step < s1)) return false;
+      const int w = meta[sl - s0].y;
+      const unsigned char *b = stg0 + (size_t)st * stage_bytes;
+      body(sl, (const unsigned short *)b, (const double *)(b + (size_t)w * 64));
+      __syncwarp();
+      if (sl + 2 * step < s1) issue(sl + 2 * step, st, vals);
+    }
+    return true;
+  }
+};
+
 // ------------------------------------------------------------ the kernel
 template <int kRes>
 __global__ void __launch_bounds__(kThreads, 2) jcg_kernel(JcgArgs a) {
@@ -484,7 +555,8 @@ __global__ void __launch_bounds__(kThreads, 2) jcg_kernel(JcgArgs a) {
   int2 *S_meta = (int2 *)(S_le + ((RB + 127) & ~127));
   uint64_t *S_bar = (uint64_t *)(S_meta + ((RB / kSlice + 15) & ~15));
   unsigned char *S_stage = (unsigned char *)(S_bar + 16);
-  uint32_t parbits = 0u;   // bit st: phase of this warp's mbarrier st
+  SlicePipe pipe{S_stage + (size_t)(2 * warp) * a.stage_bytes, &S_bar[2 * warp], S_meta, a.lcol,
+                 a.flags, a.stage_bytes, s0, s1, s0 + warp, nwarps, lane, 0u};
   Rec *rec = &a.itp->rec;
   __shared__ ItpLocal L;              // used by the scalar block's thread 0 only
   unsigned gen = 0;                   // barrier generation within this launch
@@ -496,116 +568,210 @@ __global__ void __launch_bounds__(kThreads, 2) jcg_kernel(JcgArgs a) {
     L.itmax = g->itmax; L.adapt = g->adapt; L.q1 = g->q1; L.isym = g->isym; L.chg_ier = 0;
   }
 
-  // P0: scal part 1 -- u' = u*sqrt(d), w = 1/sqrt(d), rhs' = rhs*w.
-  for (int s = s0 + warp; s < s1; s += nwarps) {
-    int i = s * kSlice + lane;
-    if (i < n) {
-      double work = sqrt(a.diag[i]);
-      a.u[i] = a.u[i] * work;
-      double wv = 1.0 / work;
-      a.w[i] = wv;
-      a.rhs[i] = a.rhs[i] * wv;
-      a.u1[i] = 0.0;
-    }
-  }
-  if (!phase_sync(a, scalar_block, gen)) return;
-
-  // P1: scaled off-diagonals, the reference's unscal drift of the resident
-  // matrix, and the initial pseudo-residual d0 = pjac(u') + rhs' - u'.
-  for (int s = s0 + warp; s < s1; s += nwarps) {
-    int i = s * kSlice + lane;
-    if (i < n) {
-      int len = a.rlen[i];
-      int base = a.sl_ptr[s] + lane;
-      double wi = a.w[i];
-      double ui = a.u[i];
-      double winv_i = 1.0 / wi;
-      double acc = a.rhs[i];
-      for (int c0 = 0; c0 < len; c0 += kCh) {
-        int jj[kCh];
-        double vo[kCh], wj[kCh], uj[kCh];
-#pragma unroll
-        for (int k = 0; k < kCh; ++k)
-          if (c0 + k < len) {
-            int idx = base + (c0 + k) * kSlice;
-            jj[k] = a.col[idx];
-            vo[k] = a.offd[idx];
-          }
-#pragma unroll
-        for (int k = 0; k < kCh; ++k)
-          if (c0 + k < len) {
-            wj[k] = a.w[jj[k]];
-            uj[k] = a.u[jj[k]];
-          }
-#pragma unroll
-        for (int k = 0; k < kCh; ++k)
-          if (c0 + k < len) {
-            int idx = base + (c0 + k) * kSlice;
-            double sv = vo[k] * wi * wj[k];
-            a.soff[idx] = sv;
-            a.offd[idx] = sv * winv_i * (1.0 / wj[k]);
-            acc = acc - sv * uj[k];
-          }
-      }
-      st_p4(a.p0 + i, 0.0, acc - ui, 0.0, 0.0);   // (dtwd0 later, d0, d(-1) = 0)
-      a.diag[i] = winv_i * winv_i;
-    }
-  }
-  if (!phase_sync(a, scalar_block, gen)) return;
-
-  // P2: dtwd0 = -A' d0 and the iteration-0 norms; the scalar block runs
-  // chgcon for in = 0 (ip = 0: cme = 0) while the rows work.
+  // P2 needs the unorm flag of iteration 0, set before the launch.
   Rec r = read_rec(rec);
-  if (kRes && !scalar_block) {
-    for (int idx = threadIdx.x; idx < rows; idx += blockDim.x) {
-      const int i = r0 + idx;
-      const bool in = i < n;
-      S_le[idx] = in ? (unsigned char)(a.rlen[i] | (a.exp[i] ? 128 : 0)) : 0;
-      S_t[idx] = 0.0;
-      S_dd[idx] = in ? a.p0[i].y : 0.0;   // d0
-      S_dd[VB + idx] = 0.0;               // d(-1)
+  const int need_u0 = r.need_unorm;
+  double pd = 0.0, pt = 0.0, pu = 0.0;
+  if (!kRes) {
+    // P0: scal part 1 -- u' = u*sqrt(d), w = 1/sqrt(d), rhs' = rhs*w.
+    for (int s = s0 + warp; s < s1; s += nwarps) {
+      int i = s * kSlice + lane;
+      if (i < n) {
+        double work = sqrt(a.diag[i]);
+        a.u[i] = a.u[i] * work;
+        double wv = 1.0 / work;
+        a.w[i] = wv;
+        a.rhs[i] = a.rhs[i] * wv;
+        a.u1[i] = 0.0;
+      }
     }
-    for (int k = threadIdx.x; k < s1 - s0; k += blockDim.x)
-      S_meta[k] = make_int2(a.sl_ptr[s0 + k], a.sl_w[s0 + k]);
-    if (threadIdx.x < 2 * nwarps) mbar_init(&S_bar[threadIdx.x], 1);
-    mbar_fence_init();
-    __syncthreads();
-  }
-  {
-    double pd = 0.0, pt = 0.0, pu = 0.0;
+    if (!phase_sync(a, scalar_block, gen)) return;
+
+    // P1: scaled off-diagonals, the reference's unscal drift of the resident
+    // matrix, and the initial pseudo-residual d0 = pjac(u') + rhs' - u'.
     for (int s = s0 + warp; s < s1; s += nwarps) {
       int i = s * kSlice + lane;
       if (i < n) {
         int len = a.rlen[i];
         int base = a.sl_ptr[s] + lane;
-        double acc = 0.0;
+        double wi = a.w[i];
+        double ui = a.u[i];
+        double winv_i = 1.0 / wi;
+        double acc = a.rhs[i];
         for (int c0 = 0; c0 < len; c0 += kCh) {
           int jj[kCh];
-          double vv[kCh], xx[kCh];
-#pragma unroll
+          double vo[kCh], wj[kCh], uj[kCh];
+  #pragma unroll
           for (int k = 0; k < kCh; ++k)
             if (c0 + k < len) {
               int idx = base + (c0 + k) * kSlice;
               jj[k] = a.col[idx];
-              vv[k] = a.soff[idx];
+              vo[k] = a.offd[idx];
             }
-#pragma unroll
+  #pragma unroll
           for (int k = 0; k < kCh; ++k)
-            if (c0 + k < len) xx[k] = a.p0[jj[k]].y;
-#pragma unroll
+            if (c0 + k < len) {
+              wj[k] = a.w[jj[k]];
+              uj[k] = a.u[jj[k]];
+            }
+  #pragma unroll
           for (int k = 0; k < kCh; ++k)
-            if (c0 + k < len) acc = acc - vv[k] * xx[k];
+            if (c0 + k < len) {
+              int idx = base + (c0 + k) * kSlice;
+              double sv = vo[k] * wi * wj[k];
+              a.soff[idx] = sv;
+              a.offd[idx] = sv * winv_i * (1.0 / wj[k]);
+              acc = acc - sv * uj[k];
+            }
         }
-        a.p0[i].x = acc;
-        if (kRes) S_t[i - r0] = acc;
-        double di = a.p0[i].y;
-        pd += di * di;
-        pt += di * acc;
-        if (r.need_unorm) { double ui = a.u[i]; pu += ui * ui; }
+        st_p4(a.p0 + i, 0.0, acc - ui, 0.0, 0.0);   // (dtwd0 later, d0, d(-1) = 0)
+        a.diag[i] = winv_i * winv_i;
       }
     }
+    if (!phase_sync(a, scalar_block, gen)) return;
+
+    // P2: dtwd0 = -A' d0 and the iteration-0 norms; the scalar block runs
+    // chgcon for in = 0 (ip = 0: cme = 0) while the rows work.
+    {
+      for (int s = s0 + warp; s < s1; s += nwarps) {
+        int i = s * kSlice + lane;
+        if (i < n) {
+          int len = a.rlen[i];
+          int base = a.sl_ptr[s] + lane;
+          double acc = 0.0;
+          for (int c0 = 0; c0 < len; c0 += kCh) {
+            int jj[kCh];
+            double vv[kCh], xx[kCh];
+  #pragma unroll
+            for (int k = 0; k < kCh; ++k)
+              if (c0 + k < len) {
+                int idx = base + (c0 + k) * kSlice;
+                jj[k] = a.col[idx];
+                vv[k] = a.soff[idx];
+              }
+  #pragma unroll
+            for (int k = 0; k < kCh; ++k)
+              if (c0 + k < len) xx[k] = a.p0[jj[k]].y;
+  #pragma unroll
+            for (int k = 0; k < kCh; ++k)
+              if (c0 + k < len) acc = acc - vv[k] * xx[k];
+          }
+          a.p0[i].x = acc;
+          double di = a.p0[i].y;
+          pd += di * di;
+          pt += di * acc;
+          if (need_u0) { double ui = a.u[i]; pu += ui * ui; }
+        }
+      }
+    }
+  } else {
+    // Resident prologue.  Shared memory first holds, per row of the block
+    // and per halo node, w = 1/sqrt(diag) and u' (P1), then d0 (P2).
+    double *Uv = S_dd, *Wv = S_dd + VB;
+    if (!scalar_block) {
+      for (int idx = threadIdx.x; idx < rows; idx += blockDim.x) {
+        const int i = r0 + idx;
+        S_le[idx] = i < n ? (unsigned char)(a.rlen[i] | (a.exp[i] ? 128 : 0)) : 0;
+      }
+      for (int k = threadIdx.x; k < s1 - s0; k += blockDim.x)
+        S_meta[k] = make_int2(a.sl_ptr[s0 + k], a.sl_w[s0 + k]);
+      if (threadIdx.x < 2 * nwarps) mbar_init(&S_bar[threadIdx.x], 1);
+      mbar_fence_init();
+      // P0: scal part 1 -- u' = u*sqrt(d), w = 1/sqrt(d), rhs' = rhs*w,
+      // eight rows per thread with their loads issued together.
+      for (int base = threadIdx.x; base < rows; base += kRowUnroll * blockDim.x) {
+        double dg[kRowUnroll], uu[kRowUnroll], rh[kRowUnroll];
+#pragma unroll
+        for (int k = 0; k < kRowUnroll; ++k) {
+          const int idx = base + k * blockDim.x, i = r0 + idx;
+          if (idx < rows && i < n) { dg[k] = a.diag[i]; uu[k] = a.u[i]; rh[k] = a.rhs[i]; }
+        }
+#pragma unroll
+        for (int k = 0; k < kRowUnroll; ++k) {
+          const int idx = base + k * blockDim.x, i = r0 + idx;
+          if (idx < rows && i < n) {
+            double work = sqrt(dg[k]);
+            const double up = uu[k] * work;
+            double wv = 1.0 / work;
+            a.u[i] = up;
+            a.w[i] = wv;
+            a.rhs[i] = rh[k] * wv;
+            a.u1[i] = 0.0;
+            Uv[idx] = up;
+            Wv[idx] = wv;
+            if (need_u0) pu += up * up;
+          }
+        }
+      }
+    }
+    if (!phase_sync(a, scalar_block, gen)) return;
+    // P1: scaled off-diagonals, the reference's unscal drift of the resident
+    // matrix, and d0 = pjac(u') + rhs' - u' (kept in S_t until P2).
+    if (!scalar_block) {
+      pipe.begin(a.offd);
+      const int h0 = a.halo_ptr[blockIdx.x], nh = a.halo_ptr[blockIdx.x + 1] - h0;
+      for (int h = threadIdx.x; h < nh; h += blockDim.x) {
+        const int j = a.halo_ids[h0 + h];
+        Uv[RB + h] = a.u[j];
+        Wv[RB + h] = a.w[j];
+      }
+      __syncthreads();
+      bool ok = pipe.run(a.offd, [&](int sl, const unsigned short *lc, const double *lv) {
+        const int i = sl * kSlice + lane, idx = i - r0;
+        if (i < n) {
+          const int len = S_le[idx] & 127;
+          const int base = S_meta[sl - s0].x + lane;
+          const double wi = Wv[idx], ui = Uv[idx];
+          const double winv_i = 1.0 / wi;
+          double acc = a.rhs[i];
+          for (int q = 0; q < len; ++q) {
+            const int lq = lc[q * kSlice + lane];
+            const double wj = Wv[lq];
+            const double sv = lv[q * kSlice + lane] * wi * wj;
+            a.soff[base + q * kSlice] = sv;
+            a.offd[base + q * kSlice] = sv * winv_i * (1.0 / wj);
+            acc = acc - sv * Uv[lq];
+          }
+          const double d0 = acc - ui;
+          if (S_le[idx] & 128) st_p4(a.p0 + i, 0.0, d0, 0.0, 0.0);
+          a.diag[i] = winv_i * winv_i;
+          S_t[idx] = d0;
+        }
+      });
+      if (!ok) atomicExch(&a.flags->timeout, 1);
+      fence_proxy_async_all();   // soff is read by bulk copies from here on
+    }
+    if (!phase_sync(a, scalar_block, gen)) return;
+    // P2: dtwd0 = -A' d0 and the iteration-0 norms.
+    if (!scalar_block) {
+      pipe.begin(a.soff);
+      double *Dv = S_dd;
+      for (int idx = threadIdx.x; idx < rows; idx += blockDim.x) {
+        Dv[idx] = S_t[idx];
+        S_dd[VB + idx] = 0.0;   // d(-1)
+      }
+      const int h0 = a.halo_ptr[blockIdx.x], nh = a.halo_ptr[blockIdx.x + 1] - h0;
+      for (int h = threadIdx.x; h < nh; h += blockDim.x) Dv[RB + h] = a.p0[a.halo_ids[h0 + h]].y;
+      __syncthreads();
+      bool ok = pipe.run(a.soff, [&](int sl, const unsigned short *lc, const double *lv) {
+        const int i = sl * kSlice + lane, idx = i - r0;
+        if (i < n) {
+          const int len = S_le[idx] & 127;
+          double acc = 0.0;
+          for (int q = 0; q < len; ++q) acc = acc - lv[q * kSlice + lane] * Dv[lc[q * kSlice + lane]];
+          if (S_le[idx] & 128) a.p0[i].x = acc;
+          S_t[idx] = acc;
+          const double di = Dv[idx];
+          pd += di * di;
+          pt += di * acc;
+        }
+      });
+      if (!ok) atomicExch(&a.flags->timeout, 1);
+    }
+  }
+  {
     if (scalar_block && threadIdx.x == 0 && L.adapt) chgcon_d(&L, t1, t2, 0);
-    const int need_u = r.need_unorm;
+    const int need_u = need_u0;
     bool ok = phase_reduce(a, scalar_block, gen, pd, pt, pu, [&](double sd, double st, double su) {
       L.delnnm = sd;
       int halt = pstop_d(&L, 0, need_u ? su : 1.0, sd);
@@ -681,37 +847,30 @@ __global__ void __launch_bounds__(kThreads, 2) jcg_kernel(JcgArgs a) {
         }
       }
     } else if (!scalar_block) {
-      // Resident variant.  Bulk copies of each warp's first two slices
-      // (block-local columns + values) start before phase A.
-      unsigned char *const stg0 = S_stage + (size_t)(2 * warp) * a.stage_bytes;
-      uint64_t *const bar0 = &S_bar[2 * warp];
-      auto issue = [&](int sl, int st) {
-        if (lane == 0) {
-          const int2 mt = S_meta[sl - s0];
-          const uint32_t w = (uint32_t)mt.y;
-          unsigned char *b = stg0 + (size_t)st * a.stage_bytes;
-          mbar_expect_tx(bar0 + st, w * 320u);
-          if (w > 0) {
-            bulk_load(b, a.lcol + mt.x, w * 64u, bar0 + st);
-            bulk_load(b + w * 64u, a.soff + mt.x, w * 256u, bar0 + st);
-          }
-        }
-      };
-      if (lane == 0) fence_proxy_async_all();
-      if (s0 + warp < s1) issue(s0 + warp, 0);
-      if (s0 + warp + nwarps < s1) issue(s0 + warp + nwarps, 1);
+      // Resident variant.  The warp's first two slices start streaming
+      // before phase A.
+      pipe.begin(a.soff);
       // Phase A: the 3-term update of the block's rows, d(in+1) written
       // over d(in-1); then the new d of the halo nodes from their owners'
       // exported records (same expression, same bits).
       double *Sd = S_dd + cur * VB, *Sdn = S_dd + (cur ^ 1) * VB;
-      for (int idx = threadIdx.x; idx < rows; idx += blockDim.x) {
-        const int i = r0 + idx;
-        if (i < n) {
-          const double dn = c1 * S_t[idx] + c4 * Sd[idx] + c3 * Sdn[idx];
-          const double unew = c1 * Sd[idx] + c2 * uc[i] + c3 * un[i];
-          Sdn[idx] = dn;
-          un[i] = unew;
-          if (need_u) pu += unew * unew;
+      for (int base = threadIdx.x; base < rows; base += kRowUnroll * blockDim.x) {
+        double ucv[kRowUnroll], unv[kRowUnroll];
+#pragma unroll
+        for (int k = 0; k < kRowUnroll; ++k) {
+          const int idx = base + k * blockDim.x, i = r0 + idx;
+          if (idx < rows && i < n) { ucv[k] = uc[i]; unv[k] = un[i]; }
+        }
+#pragma unroll
+        for (int k = 0; k < kRowUnroll; ++k) {
+          const int idx = base + k * blockDim.x, i = r0 + idx;
+          if (idx < rows && i < n) {
+            const double dn = c1 * S_t[idx] + c4 * Sd[idx] + c3 * Sdn[idx];
+            const double unew = c1 * Sd[idx] + c2 * ucv[k] + c3 * unv[k];
+            Sdn[idx] = dn;
+            un[i] = unew;
+            if (need_u) pu += unew * unew;
+          }
         }
       }
       {
@@ -723,55 +882,22 @@ __global__ void __launch_bounds__(kThreads, 2) jcg_kernel(JcgArgs a) {
       }
       __syncthreads();
       // Phase B: the SpMV from shared memory, slot order as in pjac.
-      int k = 0;
-      for (int sl = s0 + warp; sl < s1; sl += nwarps, ++k) {
-        const int st = k & 1;
-        {
-          long long tw = clock64();
-          bool ok = true;
-          while (!mbar_try_wait(bar0 + st, (parbits >> st) & 1u)) {
-            if (clock64() - tw > kSpinCycles) { ok = false; break; }
-          }
-          if (!ok) {
-            if (lane == 0) {
-              atomicExch(&a.flags->timeout, 1);
-              // let the copy already issued into the other buffer land
-              if (sl + nwarps < s1) {
-                long long t1w = clock64();
-                while (!mbar_try_wait(bar0 + (st ^ 1), (parbits >> (st ^ 1)) & 1u) &&
-                       clock64() - t1w < kSpinCycles) {
-                }
-              }
-            }
-            __syncwarp();
-            break;
-          }
-          parbits ^= 1u << st;
-        }
-        const int w = S_meta[sl - s0].y;
-        const unsigned char *b = stg0 + (size_t)st * a.stage_bytes;
-        const unsigned short *lc = (const unsigned short *)b;
-        const double *lv = (const double *)(b + (size_t)w * 64);
-        const int i = sl * kSlice + lane;
-        const int idx = i - r0;
-        double acc = 0.0;
-        double dn = 0.0;
-        const unsigned le = S_le[idx];
+      bool ok = pipe.run(a.soff, [&](int sl, const unsigned short *lc, const double *lv) {
+        const int i = sl * kSlice + lane, idx = i - r0;
         if (i < n) {
+          const unsigned le = S_le[idx];
           const int len = (int)(le & 127u);
+          double acc = 0.0;
 #pragma unroll 4
           for (int q = 0; q < len; ++q) acc = acc - lv[q * kSlice + lane] * Sdn[lc[q * kSlice + lane]];
-          dn = Sdn[idx];
-        }
-        __syncwarp();
-        if (sl + 2 * nwarps < s1) issue(sl + 2 * nwarps, st);
-        if (i < n) {
+          const double dn = Sdn[idx];
           if (le & 128u) st_p4(pn + i, acc, dn, Sd[idx], 0.0);
           S_t[idx] = acc;
           pd += dn * dn;
           pt += dn * acc;
         }
-      }
+      });
+      if (!ok) atomicExch(&a.flags->timeout, 1);
       cur ^= 1;
     }
     const int m = in + 1;
