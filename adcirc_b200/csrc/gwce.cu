@@ -64,11 +64,44 @@ __global__ void k_apply_met(adc_ctx c) {
 }
 
 // --------------------------------------------------------------- LHS
-// The rebuild runs only when NCChange > 0 (gwce.F:430-431).
-__global__ void k_lhs_begin(Flags *f, int *rebuild) {
+// The rebuild runs only when NCChange > 0 (gwce.F:430-431).  words[0] is
+// the rebuild decision; words[1] is set by a solve that left the ITPACK
+// unscal drift of COEF pending; words[2] says whether this step applies it
+// (only when COEF is kept, since a rebuild overwrites it).
+__global__ void k_lhs_begin(Flags *f, int *words) {
   int r = f->ncchange > 0;
-  *rebuild = r;
+  words[0] = r;
+  words[2] = (!r && words[1]) ? 1 : 0;
+  words[1] = 0;
   if (r) f->ncchange = 0;
+}
+
+// Moves the COEF drift from a point after the solve to the next step that
+// keeps COEF, so steps that rebuild COEF never pay for it.  It repeats the
+// exact operations of the solve's scal/unscal pass (itpackv.F:2393-2398,
+// 2458-2463) with the w = 1/sqrt(diag) that solve used, so COEF ends with
+// the same bits as if the solve had written it.
+__global__ void k_lhs_drift(adc_ctx c, const int *apply) {
+  if (!*apply) return;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= c.np) return;
+  const double wi = c.jw[i];
+  const double winv_i = 1.0 / wi;
+  const int s = i / kSlice, lane = i - s * kSlice;
+  const int base = c.sl_ptr[s] + lane, len = c.rlen[i];
+  for (int k = 0; k < len; ++k) {
+    const int q = base + k * kSlice;
+    const double wj = c.jw[c.col[q]];
+    const double sv = c.offd[q] * wi * wj;
+    c.offd[q] = sv * winv_i * (1.0 / wj);
+  }
+}
+
+// Single-thread helper: make a pending drift apply now (before COEF is
+// copied to the host).
+__global__ void k_lhs_drift_flush(int *words) {
+  words[2] = words[1];
+  words[1] = 0;
 }
 
 // gwce.F:456-593: nine consistent-mass + gravity entries per element.

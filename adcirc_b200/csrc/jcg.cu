@@ -74,6 +74,8 @@ struct JcgArgs {
   const int *halo_ptr;        // [nrb + 1] into halo_ids
   const int *halo_ids;        // halo nodes of each row block (global rows)
   const unsigned char *exp;   // per row: read by another row block
+  int defer_drift;            // 1: leave the COEF unscal drift to the next step
+  int *drift_pending;         // set to 1 when the drift is left pending
   const int *nodecode;
   const double *eta1;
   double *eta2;
@@ -113,10 +115,25 @@ __device__ bool spin_eq(const unsigned *p, unsigned g, Flags *flags) {
   return true;
 }
 
+__device__ Rec read_rec(const Rec *r) {
+  const volatile Rec *v = r;
+  Rec o;
+  o.c1 = v->c1;
+  o.c2 = v->c2;
+  o.c3 = v->c3;
+  o.c4 = v->c4;
+  o.halt = v->halt;
+  o.need_unorm = v->need_unorm;
+  o.in = v->in;
+  o.pad_ = 0;
+  return o;
+}
+
 // Row-block side: post (optionally) partials and the arrival, wait for the
-// release.  Returns false on timeout.
+// release.  With `srec`, thread 0 also fetches the ITPACK record the
+// release publishes, for the whole block.  Returns false on timeout.
 __device__ bool row_arrive_wait(const JcgArgs &a, unsigned g, bool post, double p0, double p1,
-                                double p2) {
+                                double p2, Rec *srec = nullptr) {
   __shared__ int ok;
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -131,6 +148,7 @@ __device__ bool row_arrive_wait(const JcgArgs &a, unsigned g, bool post, double 
     *(volatile unsigned *)&al->gen = g;
     ok = spin_eq(&((ReleaseLine *)a.release + blockIdx.x)->gen, g, a.flags) ? 1 : 0;
     __threadfence();
+    if (srec) *srec = read_rec(&a.itp->rec);
   }
   __syncthreads();
   return ok != 0;
@@ -369,6 +387,7 @@ __device__ void parcon_d(ItpLocal *it, int in, double dtnrm, double c[4]) {
 // Accumulation keeps the slot order (pjac's j order).
 constexpr int kCh = 6;
 constexpr int kRowUnroll = 8;   // rows per thread whose loads issue together
+constexpr int kHaloPre = 2;     // halo records per thread fetched ahead of the row update
 
 // L2 prefetch of the next slice of a warp: the column and value rows of its
 // slots and its own-row vector entries, one 128-byte line per lane.
@@ -418,11 +437,11 @@ __device__ void block_sum3(double &a, double &b, double &c) {
 // `serial(s0, s1, s2)` on its thread 0 before releasing.
 template <class F>
 __device__ bool phase_reduce(const JcgArgs &a, bool scalar_block, unsigned &g, double p0,
-                             double p1, double p2, F serial) {
+                             double p1, double p2, F serial, Rec *srec = nullptr) {
   ++g;
   if (!scalar_block) {
     block_sum3(p0, p1, p2);
-    return row_arrive_wait(a, g, true, p0, p1, p2);
+    return row_arrive_wait(a, g, true, p0, p1, p2, srec);
   }
   if (!scalar_gather(a, g)) return false;
   double s0 = 0.0, s1 = 0.0, s2 = 0.0;
@@ -433,7 +452,10 @@ __device__ bool phase_reduce(const JcgArgs &a, bool scalar_block, unsigned &g, d
     s2 += vp[2];
   }
   block_sum3(s0, s1, s2);
-  if (threadIdx.x == 0) serial(s0, s1, s2);
+  if (threadIdx.x == 0) {
+    serial(s0, s1, s2);
+    if (srec) *srec = read_rec(&a.itp->rec);
+  }
   scalar_release(a, g);
   __syncthreads();
   return true;
@@ -448,19 +470,6 @@ __device__ bool phase_sync(const JcgArgs &a, bool scalar_block, unsigned &g) {
   return true;
 }
 
-__device__ Rec read_rec(const Rec *r) {
-  const volatile Rec *v = r;
-  Rec o;
-  o.c1 = v->c1;
-  o.c2 = v->c2;
-  o.c3 = v->c3;
-  o.c4 = v->c4;
-  o.halt = v->halt;
-  o.need_unorm = v->need_unorm;
-  o.in = v->in;
-  o.pad_ = 0;
-  return o;
-}
 
 // Per-warp double-buffered bulk copies of whole slices (block-local
 // columns + one value array) into shared memory, for the resident variant.
@@ -559,6 +568,7 @@ __global__ void __launch_bounds__(kThreads, 2) jcg_kernel(JcgArgs a) {
                  a.flags, a.stage_bytes, s0, s1, s0 + warp, nwarps, lane, 0u};
   Rec *rec = &a.itp->rec;
   __shared__ ItpLocal L;              // used by the scalar block's thread 0 only
+  __shared__ Rec s_rec;               // the record of the last reducing barrier
   unsigned gen = 0;                   // barrier generation within this launch
   if (scalar_block && threadIdx.x == 0) {
     const volatile Itp *g = a.itp;
@@ -620,7 +630,7 @@ __global__ void __launch_bounds__(kThreads, 2) jcg_kernel(JcgArgs a) {
               int idx = base + (c0 + k) * kSlice;
               double sv = vo[k] * wi * wj[k];
               a.soff[idx] = sv;
-              a.offd[idx] = sv * winv_i * (1.0 / wj[k]);
+              if (!a.defer_drift) a.offd[idx] = sv * winv_i * (1.0 / wj[k]);
               acc = acc - sv * uj[k];
             }
         }
@@ -729,7 +739,7 @@ __global__ void __launch_bounds__(kThreads, 2) jcg_kernel(JcgArgs a) {
             const double wj = Wv[lq];
             const double sv = lv[q * kSlice + lane] * wi * wj;
             a.soff[base + q * kSlice] = sv;
-            a.offd[base + q * kSlice] = sv * winv_i * (1.0 / wj);
+            if (!a.defer_drift) a.offd[base + q * kSlice] = sv * winv_i * (1.0 / wj);
             acc = acc - sv * Uv[lq];
           }
           const double d0 = acc - ui;
@@ -785,7 +795,7 @@ __global__ void __launch_bounds__(kThreads, 2) jcg_kernel(JcgArgs a) {
       vr->halt = halt;
       vr->need_unorm = !(L.q1 || ((1 > 5) && (1 % 5 != 0)));
       vr->in = 0;
-    });
+    }, &s_rec);
     if (!ok) return;
   }
 
@@ -796,7 +806,7 @@ __global__ void __launch_bounds__(kThreads, 2) jcg_kernel(JcgArgs a) {
   double *U[2] = {a.u, a.u1};
   int cur = 0;   // resident variant: S_dd half holding d(in)
   for (int in = 0; in < a.itmax; ++in) {
-    r = read_rec(rec);
+    r = s_rec;
     if (r.halt) break;
     const double c1 = r.c1, c2 = r.c2, c3 = r.c3, c4 = r.c4;
     const int need_u = r.need_unorm;
@@ -854,6 +864,13 @@ __global__ void __launch_bounds__(kThreads, 2) jcg_kernel(JcgArgs a) {
       // over d(in-1); then the new d of the halo nodes from their owners'
       // exported records (same expression, same bits).
       double *Sd = S_dd + cur * VB, *Sdn = S_dd + (cur ^ 1) * VB;
+      const int h0 = a.halo_ptr[blockIdx.x], nh = a.halo_ptr[blockIdx.x + 1] - h0;
+      P4 hv[kHaloPre];   // the first halo records, loaded with the rows' vectors
+#pragma unroll
+      for (int k = 0; k < kHaloPre; ++k) {
+        const int h = threadIdx.x + k * blockDim.x;
+        if (h < nh) hv[k] = ld_p4(pc + a.halo_ids[h0 + h]);
+      }
       for (int base = threadIdx.x; base < rows; base += kRowUnroll * blockDim.x) {
         double ucv[kRowUnroll], unv[kRowUnroll];
 #pragma unroll
@@ -873,12 +890,14 @@ __global__ void __launch_bounds__(kThreads, 2) jcg_kernel(JcgArgs a) {
           }
         }
       }
-      {
-        const int h0 = a.halo_ptr[blockIdx.x], nh = a.halo_ptr[blockIdx.x + 1] - h0;
-        for (int h = threadIdx.x; h < nh; h += blockDim.x) {
-          const P4 o = ld_p4(pc + a.halo_ids[h0 + h]);
-          Sdn[RB + h] = c1 * o.x + c4 * o.y + c3 * o.z;
-        }
+#pragma unroll
+      for (int k = 0; k < kHaloPre; ++k) {
+        const int h = threadIdx.x + k * blockDim.x;
+        if (h < nh) Sdn[RB + h] = c1 * hv[k].x + c4 * hv[k].y + c3 * hv[k].z;
+      }
+      for (int h = threadIdx.x + kHaloPre * blockDim.x; h < nh; h += blockDim.x) {
+        const P4 o = ld_p4(pc + a.halo_ids[h0 + h]);
+        Sdn[RB + h] = c1 * o.x + c4 * o.y + c3 * o.z;
       }
       __syncthreads();
       // Phase B: the SpMV from shared memory, slot order as in pjac.
@@ -916,10 +935,10 @@ __global__ void __launch_bounds__(kThreads, 2) jcg_kernel(JcgArgs a) {
       vr->halt = halt;
       vr->need_unorm = !(L.q1 || ((mm > 5) && (mm % 5 != 0)));
       vr->in = m;
-    });
+    }, &s_rec);
     if (!ok) return;
   }
-  r = read_rec(rec);
+  r = s_rec;
   const int fin = r.in;
   const double *usol = U[fin % 2];
 
@@ -973,6 +992,7 @@ __global__ void __launch_bounds__(kThreads, 2) jcg_kernel(JcgArgs a) {
     g->adapt = L.adapt; g->q1 = L.q1; g->chg_ier = L.chg_ier;
     g->in = fin;
     g->halt = h;
+    if (a.defer_drift) *a.drift_pending = 1;
     a.flags->numitr = fin;
     a.flags->ier = (h == 2) ? 13 : 0;
     a.flags->zeta = L.rparm1;
@@ -1150,7 +1170,7 @@ int jcg_setup_grid(adc_ctx *c, const JcgHostSell *h) {
   return ADC_OK;
 }
 
-int launch_jcg_impl(adc_ctx *c, int eta_update, int do_peror, int run_init) {
+int launch_jcg_impl(adc_ctx *c, int eta_update, int do_peror, int run_init, int defer_drift) {
   JcgArgs a;
   a.do_peror = do_peror;
   a.n = c->np;
@@ -1188,6 +1208,9 @@ int launch_jcg_impl(adc_ctx *c, int eta_update, int do_peror, int run_init) {
   a.halo_ptr = c->jhalo_ptr;
   a.halo_ids = c->jhalo_ids;
   a.exp = c->jexp;
+  a.defer_drift = defer_drift;
+  // the word after the step flags (allocated only by the time-step context)
+  a.drift_pending = defer_drift ? (int *)(c->flags + 1) + 1 : nullptr;
   int nwords = (int)(2 * 128 * (size_t)c->jcg_rows_blocks / 4);
   jcg_clear_lines<<<8, 256, 0, c->stream>>>((unsigned *)c->jlines, nwords);
   c->launches++;
@@ -1203,6 +1226,7 @@ int launch_jcg_impl(adc_ctx *c, int eta_update, int do_peror, int run_init) {
   return ADC_OK;
 }
 
-int launch_jcg(adc_ctx *c, int eta_update) { return launch_jcg_impl(c, eta_update, 0, 1); }
+// The time-step solve defers the COEF drift to the next GWCE (k_lhs_drift).
+int launch_jcg(adc_ctx *c, int eta_update) { return launch_jcg_impl(c, eta_update, 0, 1, 1); }
 
 }  // namespace adc

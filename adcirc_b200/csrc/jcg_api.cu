@@ -19,7 +19,7 @@
 
 namespace adc {
 int jcg_setup_grid(adc_ctx *c, const JcgHostSell *h);
-int launch_jcg_impl(adc_ctx *c, int eta_update, int do_peror, int run_init);
+int launch_jcg_impl(adc_ctx *c, int eta_update, int do_peror, int run_init, int defer_drift);
 
 // ITPACK state that survives between jcg calls: itjcg's SAVEd q1 flag.
 static int g_q1 = 0;
@@ -136,7 +136,7 @@ static int jcg_solve(int n, int ndim, int maxnz, int *jcoef, double *coef, doubl
   Flags fl;
   memset(&fl, 0, sizeof(fl));
   ADC_CUDA(alloc_up(&c.flags, &fl, 1));
-  rc = launch_jcg_impl(&c, 0, iparm[11] >= 0 ? 1 : 0, 0);
+  rc = launch_jcg_impl(&c, 0, iparm[11] >= 0 ? 1 : 0, 0, 0);
   if (rc) return rc;
   ADC_CUDA(cudaStreamSynchronize(c.stream));
   ADC_CUDA(cudaMemcpy(&fl, c.flags, sizeof(fl), cudaMemcpyDeviceToHost));

@@ -30,7 +30,7 @@
 
 namespace adc {
 int jcg_setup_grid(adc_ctx *c, const JcgHostSell *h);
-int launch_jcg_impl(adc_ctx *c, int eta_update, int do_peror, int run_init);
+int launch_jcg_impl(adc_ctx *c, int eta_update, int do_peror, int run_init, int defer_drift);
 int jcg_q1_get();
 void jcg_q1_set(int v);
 
@@ -197,7 +197,7 @@ static int noalloc_solve(int n, int ndim, int maxnz, int *jcoef, double *coef, d
   Flags fl;
   memset(&fl, 0, sizeof(fl));
   ADC_CUDA(cudaMemcpy(c.flags, &fl, sizeof(fl), cudaMemcpyHostToDevice));
-  rc = launch_jcg_impl(&c, 0, iparm[11] >= 0 ? 1 : 0, 0);
+  rc = launch_jcg_impl(&c, 0, iparm[11] >= 0 ? 1 : 0, 0, 0);
   if (rc) return rc;
   ADC_CUDA(cudaStreamSynchronize(0));
   ADC_CUDA(cudaMemcpy(&fl, c.flags, sizeof(fl), cudaMemcpyDeviceToHost));

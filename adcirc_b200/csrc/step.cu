@@ -34,7 +34,9 @@ int jcg_setup_grid(adc_ctx *c, const JcgHostSell *h);
 // kernels defined in the other translation units
 __global__ void k_shift_friction(adc_ctx c, const adc_step_t *steps, const Flags *flags);
 __global__ void k_apply_met(adc_ctx c);
-__global__ void k_lhs_begin(Flags *f, int *rebuild);
+__global__ void k_lhs_begin(Flags *f, int *words);
+__global__ void k_lhs_drift(adc_ctx c, const int *apply);
+__global__ void k_lhs_drift_flush(int *words);
 __global__ void k_lhs_elem(adc_ctx c, const int *rebuild);
 __global__ void k_lhs_gather(adc_ctx c, const int *rebuild);
 __global__ void k_lhs_ep(adc_ctx c, const int *rebuild, int nparts);
@@ -66,12 +68,13 @@ int launch_shift_friction(adc_ctx *c) {
 int launch_gwce_lhs(adc_ctx *c) {
   int *rb = rebuild_flag(c);
   k_lhs_begin<<<1, 1, 0, c->stream>>>(c->flags, rb);
-  k_lhs_elem<<<nblk(c->ne), kThreads, 0, c->stream>>>(*c, rb);
   int nb = nblk(c->np);
+  k_lhs_drift<<<nb, kThreads, 0, c->stream>>>(*c, rb + 2);
+  k_lhs_elem<<<nblk(c->ne), kThreads, 0, c->stream>>>(*c, rb);
   k_lhs_gather<<<nb, kThreads, 0, c->stream>>>(*c, rb);
   k_lhs_ep<<<1, 1024, 0, c->stream>>>(*c, rb, nb);
   k_lhs_bc<<<nblk((long long)c->np + c->n_obc), kThreads, 0, c->stream>>>(*c, rb);
-  c->launches += 5;
+  c->launches += 6;
   return ADC_OK;
 }
 
@@ -309,6 +312,10 @@ static int upload_state(adc_ctx *c) {
     if (c->h_ell_of_sell[idx] >= 0) o[idx] = a->coef[c->h_ell_of_sell[idx]];
   TRY(up(c->diag, d.data(), np));
   TRY(up(c->offd, o.data(), c->nnz_pad));
+  {
+    int zero3[3] = {0, 0, 0};   // the host COEF is authoritative: no drift pending
+    TRY(up(rebuild_flag(c), zero3, 3));
+  }
   TRY(up(c->obccoef, a->obccoef, (size_t)c->neta * (c->mnei - 1)));
   return ADC_OK;
 }
@@ -348,6 +355,12 @@ static int download_state(adc_ctx *c) {
   TRY(down(a->noff, c->noff, ne));
   TRY(down(a->mju, c->mju, np));
   if (a->coef) {
+    // COEF as the reference holds it: apply a drift the last solve left pending
+    int *w = rebuild_flag(c);
+    k_lhs_drift_flush<<<1, 1, 0, c->stream>>>(w);
+    k_lhs_drift<<<nblk(np), kThreads, 0, c->stream>>>(*c, w + 2);
+    ADC_CUDA(cudaGetLastError());
+    ADC_CUDA(cudaStreamSynchronize(c->stream));
     std::vector<double> d(np), o(std::max(c->nnz_pad, 1));
     TRY(down(d.data(), c->diag, np));
     TRY(down(o.data(), c->offd, c->nnz_pad));
@@ -534,8 +547,8 @@ static int bind_impl(const adc_params_t *p, const adc_arrays_t *a, int prec, adc
   memset(&fl, 0, sizeof(fl));
   fl.ncchange = 1;   // adcirc.F:404: the matrix is built on the first step
   B(up(c->flags, &fl, 1));
-  int zero = 0;
-  B(up(rebuild_flag(c), &zero, 1));
+  int zero3[3] = {0, 0, 0};
+  B(up(rebuild_flag(c), zero3, 3));
   ADC_CUDA(cudaDeviceSynchronize());
 #undef B
   *out = c;
