@@ -60,6 +60,17 @@ class AdcStep(C.Structure):
                 ("timeh", C.c_double), ("rampelev", C.c_double), ("rampmete", C.c_double)]
 
 
+class AdcVortexFix(C.Structure):
+    _fields_ = [(n, C.c_double) for n in ("time", "x", "y", "cpress", "vmax", "rmw", "tvx", "tvy")]
+
+
+class AdcVortex(C.Structure):
+    _fields_ = [("nfix", C.c_int), ("avg_minute", C.c_int), ("hemisphere", C.c_int),
+                ("pad_", C.c_int)] + [(n, C.c_double) for n in (
+                    "start_time", "bladj", "rho_air", "wind_mult", "drag_limit")] + [
+                ("fix", C.POINTER(AdcVortexFix))]
+
+
 class AdcStepOut(C.Structure):
     _fields_ = [("numitr", C.c_int), ("ier", C.c_int), ("ncchange", C.c_int),
                 ("status", C.c_int), ("ep", C.c_double), ("zeta", C.c_double),
@@ -103,6 +114,7 @@ def load():
         "adc_sync_to_host": (C.c_int, [vp]),
         "adc_sync_from_host": (C.c_int, [vp]),
         "adc_set_met": (C.c_int, [vp, dp_, dp_, dp_]),
+        "adc_set_vortex": (C.c_int, [vp, C.POINTER(AdcVortex)]),
         "adc_phase_times": (C.c_int, [vp, dp_, dp_, dp_, dp_, dp_]),
         "adc_launch_count": (C.c_int64, [vp]),
         "adc_last_run_ms": (C.c_double, [vp]),

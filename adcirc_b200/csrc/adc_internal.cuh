@@ -70,6 +70,15 @@ struct JcgHostSell {
   const int *sl_ptr, *sl_w, *col, *rlen;
 };
 
+// Track state of the parametric vortex (GetHollandStormData's module
+// counter and WTRATIO, nws08.F90:68, 114) and this step's storm scalars.
+struct VortexState {
+  int counter;   // 0-based index of the fix after the current time
+  int err;       // set when the run passes the last fix
+  double wtratio;
+  double x, y, cpress, dpdef, spd, b, rmw, tvx, tvy;
+};
+
 struct adc_ctx {
   // sizes
   int np, ne, mnei, neta, nbfr, nvel, nvelme, prec;
@@ -137,6 +146,11 @@ struct adc_ctx {
   // met forcing staging
   double *met_wsx, *met_wsy, *met_pr;
   int met_pending;
+  // parametric vortex forcing (NWS = 8)
+  int vortex_on;
+  adc_vortex_t vpar;
+  adc_vortex_fix_t *vfix;
+  VortexState *vstate;
   // timing
   cudaEvent_t ev[6];
   int64_t launches;

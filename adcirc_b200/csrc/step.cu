@@ -55,9 +55,13 @@ __global__ void k_step_end(Flags *f, int *numitr_log, int cap) {
 // Device scratch for the rebuild flag lives after the flags struct.
 static int *rebuild_flag(adc_ctx *c) { return (int *)(c->flags + 1); }
 
+int launch_met_vortex(adc_ctx *c);
+
 int launch_shift_friction(adc_ctx *c) {
   k_shift_friction<<<nblk(c->np), kThreads, 0, c->stream>>>(*c, c->steps, c->flags);
   c->launches++;
+  int rc = launch_met_vortex(c);
+  if (rc) return rc;
   if (c->met_pending) {
     k_apply_met<<<nblk(c->np), kThreads, 0, c->stream>>>(*c);
     c->launches++;
@@ -400,7 +404,7 @@ static void free_ctx(adc_ctx *c) {
       (void **)&c->jhalo_ptr, (void **)&c->jhalo_ids, (void **)&c->soff, (void **)&c->jpart, (void **)&c->jtri,
       (void **)&c->itp, (void **)&c->bar, (void **)&c->jlines, (void **)&c->flags, (void **)&c->steps,
       (void **)&c->numitr_log, (void **)&c->met_wsx, (void **)&c->met_wsy,
-      (void **)&c->met_pr};
+      (void **)&c->met_pr, (void **)&c->vfix, (void **)&c->vstate};
   for (void **p : ptrs)
     if (*p) { cudaFree(*p); *p = nullptr; }
   if (c->graph_ok) cudaGraphExecDestroy(c->graph);
@@ -623,7 +627,7 @@ int adc_gwce_new(adc_ctx *c, const adc_step_t *s, adc_stepout_t *out) {
   Flags f;
   TRY(read_flags(c, f));
   fill_out(f, out);
-  return f.status ? ADC_ERR_DIAG : ADC_OK;
+  return f.status;   // ADC_OK, ADC_ERR_DIAG (GWCE) or ADC_ERR_ARG (met track ended)
 }
 
 int adc_wetdry(adc_ctx *c, const adc_step_t *s, adc_stepout_t *out) {
@@ -655,7 +659,7 @@ int adc_timestep(adc_ctx *c, const adc_step_t *s, adc_stepout_t *out) {
   Flags f;
   TRY(read_flags(c, f));
   fill_out(f, out);
-  return f.status ? ADC_ERR_DIAG : ADC_OK;
+  return f.status;   // ADC_OK, ADC_ERR_DIAG (GWCE) or ADC_ERR_ARG (met track ended)
 }
 
 int adc_run(adc_ctx *c, int nsteps, const adc_step_t *steps, int *numitr, adc_stepout_t *last) {
@@ -720,7 +724,7 @@ int adc_run(adc_ctx *c, int nsteps, const adc_step_t *steps, int *numitr, adc_st
   }
   if (numitr) ADC_CUDA(cudaMemcpy(numitr, c->numitr_log, nsteps * sizeof(int), cudaMemcpyDeviceToHost));
   fill_out(f, last);
-  return f.status ? ADC_ERR_DIAG : ADC_OK;
+  return f.status;   // ADC_OK, ADC_ERR_DIAG (GWCE) or ADC_ERR_ARG (met track ended)
 }
 
 int adc_sync_to_host(adc_ctx *c) {

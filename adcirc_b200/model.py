@@ -74,6 +74,7 @@ class Case:
     arrays: dict                 # name -> numpy array (Fortran layout)
     schedule: Schedule
     meta: dict = dataclasses.field(default_factory=dict)
+    vortex: "Vortex | None" = None   # NWS = 8 parametric-vortex track
 
     def clone(self) -> "Case":
         c = copy.copy(self)
@@ -100,6 +101,56 @@ class Case:
 
     def state(self):
         return {k: self.arrays[k] for k in STATE_F64 + STATE_I32}
+
+
+@dataclasses.dataclass
+class Vortex:
+    """A parametric-vortex track in mesh coordinates (fort.22 for NWS = 8).
+
+    fixes: (n, 8) float64 rows of (time [s], x [m], y [m], central pressure
+    [Pa], Vmax [m/s, 10 m], RMW [km], TVX, TVY [m/s]).
+    """
+    fixes: np.ndarray
+    start_time: float = 0.0
+    avg_minute: int = 1
+    hemisphere: int = 1
+    bladj: float = 0.9
+    rho_air: float = 1.293        # constants.F90 default rhoAir
+    wind_mult: float = 1.0
+    drag_limit: float = 0.0035    # wind.F default WindDragLimit
+
+    def struct(self):
+        """(AdcVortex, backing fix array); keep both alive while in use."""
+        fx = np.ascontiguousarray(self.fixes, dtype=np.float64)
+        arr = (_lib.AdcVortexFix * len(fx))()
+        for k, row in enumerate(fx):
+            arr[k] = _lib.AdcVortexFix(*[float(v) for v in row])
+        v = _lib.AdcVortex()
+        v.nfix, v.avg_minute, v.hemisphere = len(fx), self.avg_minute, self.hemisphere
+        v.start_time, v.bladj, v.rho_air = self.start_time, self.bladj, self.rho_air
+        v.wind_mult, v.drag_limit = self.wind_mult, self.drag_limit
+        v.fix = C.cast(arr, C.POINTER(_lib.AdcVortexFix))
+        return v, arr
+
+
+def straight_track(x0: float, y0: float, heading_deg: float, speed: float, pc_hpa: float,
+                   rmw_km: float, holland_b: float, hours: float, interval_h: float = 6.0,
+                   bladj: float = 0.9, rho_air: float = 1.293) -> Vortex:
+    """Straight constant-speed track whose limited Holland B equals
+    `holland_b`: Vmax is chosen so that HollandGet's B = rhoAir*e*spd^2/dp
+    (nws08.F90:631) reproduces it after the translation removal and the
+    boundary-layer adjustment (nws08.F90:621-627)."""
+    dp = PRBCKGRND_MB * 100.0 - pc_hpa * 100.0
+    spd_bl = math.sqrt(holland_b * dp / (rho_air * math.e))
+    vmax = spd_bl * bladj + speed
+    h = math.radians(heading_deg)
+    tvx, tvy = speed * math.cos(h), speed * math.sin(h)
+    n = int(math.ceil(hours / interval_h)) + 1
+    rows = []
+    for k in range(n):
+        t = k * interval_h * 3600.0
+        rows.append((t, x0 + tvx * t, y0 + tvy * t, pc_hpa * 100.0, vmax, rmw_km, tvx, tvy))
+    return Vortex(np.array(rows), bladj=bladj, rho_air=rho_air)
 
 
 def default_params(dt: float, **kw) -> dict:
@@ -233,14 +284,22 @@ M2_PERIOD = 44712.0
 K1_PERIOD = 86164.0
 
 
-def channel_case(dt: float = 5.0, amp: float = 0.5, **kw) -> Case:
-    """Tidal channel: 121x41 nodes, 20 m -> 5 m, M2 0.5 m, dt 5 s."""
+def channel_case(dt: float = 5.0, amp: float = 0.5, vortex: bool = False, **kw) -> Case:
+    """Tidal channel: 121x41 nodes, 20 m -> 5 m, M2 0.5 m, dt 5 s.  With
+    `vortex`, a small Holland vortex (Rmax 8 km) crosses the channel."""
     from .meshgen import channel_mesh
     raw = channel_mesh()
     neta = raw.open_nodes.size
     tides = [(2.0 * math.pi / M2_PERIOD, 0.0, 1.0, np.full(neta, amp), np.zeros(neta))]
+    if vortex:
+        kw.setdefault("nws", 8)
     params = default_params(dt, **kw)
-    return build_case(raw, params, Schedule(dt=dt, dramp=0.5), tides)
+    sched = Schedule(dt=dt, dramp=0.5, dramp_mete=0.02 if vortex else 0.5)
+    case = build_case(raw, params, sched, tides)
+    if vortex:
+        case.vortex = straight_track(30.3e3, 3.7e3, 80.0, 6.0, 960.0, 8.0, 1.3, hours=12.0,
+                                     interval_h=3.0)
+    return case
 
 
 def beach_case(dt: float = 2.0, amp: float = 0.5, period: float = 10800.0, **kw) -> Case:
@@ -258,8 +317,12 @@ def beach_case(dt: float = 2.0, amp: float = 0.5, period: float = 10800.0, **kw)
     return build_case(raw, params, sched, tides)
 
 
-def surge_case(seed: int = 2024, target_nodes: int = 600_000, dt: float = 1.0, **kw) -> Case:
-    """Graded ~600k-node storm-surge mesh with M2 + K1 on the open boundary."""
+def surge_case(seed: int = 2024, target_nodes: int = 600_000, dt: float = 1.0,
+               vortex: bool = True, **kw) -> Case:
+    """Graded ~600k-node storm-surge mesh, M2 + K1 on the open boundary and a
+    Holland vortex (pc 940 hPa, Rmax 40 km, B 1.3) on a straight northward
+    track at 5 m/s that makes landfall on the coast (y ~ 640 km) after
+    about 19 h."""
     from .meshgen import surge_mesh
     raw = surge_mesh(seed=seed, target_nodes=target_nodes)
     neta = raw.open_nodes.size
@@ -268,8 +331,14 @@ def surge_case(seed: int = 2024, target_nodes: int = 600_000, dt: float = 1.0, *
         (2.0 * math.pi / M2_PERIOD, 0.0, 1.0, 0.5 + 0.1 * xo, np.deg2rad(20.0 * xo)),
         (2.0 * math.pi / K1_PERIOD, 0.0, 1.0, 0.2 + 0.05 * xo, np.deg2rad(10.0 * xo)),
     ]
+    if vortex:
+        kw.setdefault("nws", 8)
     params = default_params(dt, **kw)
-    return build_case(raw, params, Schedule(dt=dt, dramp=0.25, dramp_mete=0.25), tides)
+    case = build_case(raw, params, Schedule(dt=dt, dramp=0.25, dramp_mete=0.25), tides)
+    if vortex:
+        case.vortex = straight_track(0.5 * raw.meta["lx"] + 1234.5, 300e3 + 678.9, 90.0, 5.0,
+                                     940.0, 40.0, 1.3, hours=30.0)
+    return case
 
 
 # --------------------------------------------------------------------------
@@ -297,6 +366,9 @@ class GpuModel:
         _check(self.lib.adc_gpu_bind(C.byref(self._p), C.byref(self._a), prec, C.byref(h)),
                "adc_gpu_bind")
         self.h = h
+        if case.vortex is not None:
+            v, arr = case.vortex.struct()
+            _check(self.lib.adc_set_vortex(self.h, C.byref(v)), "adc_set_vortex")
 
     def close(self):
         if self.h:

@@ -37,6 +37,16 @@ UNIT = "sim-days/wall-hour"
 HBM_FALLBACK_GBS = 6650.0
 
 
+def forcing(case):
+    """One-line description of the met forcing of a case."""
+    v = getattr(case, "vortex", None)
+    if v is None:
+        return "no met forcing"
+    f = v.fixes[0]
+    return (f"Holland vortex NWS=8 (pc {f[3] / 100:.0f} hPa, Rmax {f[5]:.0f} km, "
+            f"B 1.3, {np.hypot(f[6], f[7]):.0f} m/s straight track)")
+
+
 def _peaks():
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -158,7 +168,8 @@ def bench_reference(args, rank, world):
         "warmup": 0, "ms_per_step": 1000.0 * el / n, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "impl": "reference",
-        "config": {"workload": f"{args.case}: {case.sizes['np']} nodes, {case.sizes['ne']} elements, dt {dt} s",
+        "config": {"workload": f"{args.case}: {case.sizes['np']} nodes, {case.sizes['ne']} elements, dt {dt} s, "
+                               f"M2+K1 tides, {forcing(case)}, wet/dry on, plain FP64 JCG",
                    "parallelism": "serial (1 core)"},
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
                          "sample": f"{n} time steps from cold start ({el:.1f} s)"},
@@ -233,7 +244,8 @@ def bench_gpu(args, rank, world, dist):
         "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64" if prec == _lib.ADC_PREC_FP64 else "f32/f64", "data": "synthetic",
         "config": {"workload": f"{args.case}: {npn} nodes, {case.sizes['ne']} elements, dt {dt} s, "
-                               f"M2+K1 tides, wet/dry on, {'plain FP64 JCG' if prec == 0 else 'mixed FP32/FP64'}",
+                               f"M2+K1 tides, {forcing(case)}, wet/dry on, "
+                               f"{'plain FP64 JCG' if prec == 0 else 'mixed FP32/FP64'}",
                    "nodes": npn, "elements": case.sizes["ne"], "parallelism": f"replicas x{world}",
                    "l2": "resident state ~0.35 GB > 126 MB L2 (no flush)",
                    "first_step": 1 + W},

@@ -93,6 +93,37 @@ typedef struct {
   double timeloc, timeh, rampelev, rampmete;
 } adc_step_t;
 
+/* One fix of a parametric-vortex track: the fields of a fort.22 best-track
+ * line that HollandGet consumes (nws08.F90:827-878), in mesh units.  The
+ * reference reads longitude/latitude in degrees (ICS=2); this library runs
+ * the Cartesian meshes of the path, so the centre is in mesh coordinates
+ * (m) and distances are Euclidean. */
+typedef struct {
+  double time;    /* CastTime: seconds since cold start */
+  double x, y;    /* storm centre (Lon, Lat) in mesh coordinates, m */
+  double cpress;  /* CPress: central pressure, Pa */
+  double vmax;    /* Spd: maximum sustained 10 m wind, m/s */
+  double rmw;     /* RMW: radius to maximum winds, km */
+  double tvx, tvy;/* TVX, TVY: storm translation velocity, m/s */
+} adc_vortex_fix_t;
+
+/* Holland vortex forcing (NWS = 8; HollandGet nws08.F90:562-717 with the
+ * radial-velocity-weighted background wind, the limited B of BCalc, no
+ * inflow angle, and the NWS = 8 stress of wind.F:1172-1198 with capped
+ * Garratt drag wind.F:514-539). */
+typedef struct {
+  int nfix;               /* number of track fixes (>= 2), times increasing */
+  int avg_minute;         /* windspeed_averaging_minute: 1 applies one2ten */
+  int hemisphere;         /* sign(1, lat) of the reference: +1 north, -1 south */
+  int pad_;
+  double start_time;      /* TimeLoc at cold start: picks the first fix pair (NWS08INIT) */
+  double bladj;           /* BLAdj, boundary-layer adjustment (fort.15) */
+  double rho_air;         /* rhoAir, kg/m^3 (constants.F90 default 1.293) */
+  double wind_mult;       /* WindMultiplier (nws08Control) */
+  double drag_limit;      /* WindDragLimit (wind.F default 0.0035) */
+  const adc_vortex_fix_t *fix;
+} adc_vortex_t;
+
 /* Host-visible results of a step or phase. */
 typedef struct {
   int numitr;       /* NUMITR = IPARM(1) after JCG (gwce.F:2005) */
@@ -188,6 +219,15 @@ int adc_sync_from_host(adc_ctx *ctx);
 /* Supplies this step's met forcing WSX2/WSY2/PR2 (getMeteorologicalForcing,
  * timestep.F:651) from host arrays of length NP; applied after the shift. */
 int adc_set_met(adc_ctx *ctx, const double *wsx2, const double *wsy2, const double *pr2);
+
+/* Replaces getMeteorologicalForcing for NWS = 8 (timestep.F:651,
+ * wind.F:1172-1198): uploads a vortex track once; every later step (and
+ * adc_run's replayed steps) then forms WSX2/WSY2/PR2 on the device from the
+ * track interpolated to TimeLoc (GetHollandStormData, nws08.F90:827-878).
+ * Requires NWS != 0 in the bound parameters; nfix < 2 or times that do not
+ * increase give ADC_ERR_ARG.  A step past the last fix sets the step status
+ * to ADC_ERR_ARG (the reference terminates there). */
+int adc_set_vortex(adc_ctx *ctx, const adc_vortex_t *vortex);
 
 /* Device time of the phases of the last adc_timestep/adc_run (ms). */
 int adc_phase_times(adc_ctx *ctx, double *ms_shift, double *ms_gwce, double *ms_jcg,

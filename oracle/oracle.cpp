@@ -488,6 +488,13 @@ inline int NM(const orc_arrays_t *a, int ie, int k) { /* 0-based ie,k -> 0-based
 struct orc_model {
   orc_params_t p;
   orc_arrays_t *a;
+  /* NWS = 8 vortex: track, options and GetHollandStormData's module state
+   * (bestTrackCounter, WTRATIO; nws08.F90:68, 114) */
+  int vortex_on = 0;
+  orc_vortex_t vpar;
+  std::vector<orc_vortex_fix_t> vfix;
+  int vcounter = 0;
+  double vwtratio = 1.0;
   int iparm[12];
   double rparm[12];
   int ncchange;
@@ -1166,11 +1173,112 @@ int orc_model_momentum(orc_model *m, const orc_step_t *s) {
   return 0;
 }
 
+int orc_model_set_vortex(orc_model *m, const orc_vortex_t *v) {
+  if (!v || !v->fix || v->nfix < 2 || !(v->bladj > 0.0) || !(v->rho_air > 0.0)) return 1;
+  for (int i = 1; i < v->nfix; ++i)
+    if (!(v->fix[i].time > v->fix[i - 1].time)) return 1;
+  /* NWS08INIT, nws08.F90:459-477 */
+  int i0 = -1;
+  for (int i = 1; i < v->nfix; ++i)
+    if (std::ceil(v->start_time) >= v->fix[i - 1].time && std::floor(v->start_time) < v->fix[i].time) {
+      i0 = i;
+      break;
+    }
+  if (i0 < 0) return 1;
+  m->vfix.assign(v->fix, v->fix + v->nfix);
+  m->vpar = *v;
+  m->vpar.fix = nullptr;
+  m->vcounter = i0;
+  m->vwtratio = 1.0;
+  m->vortex_on = 1;
+  return 0;
+}
+
+/* getMeteorologicalForcing for NWS = 8 on a Cartesian mesh: HollandGet
+ * (nws08.F90:562-717; radial-velocity-weighted background wind, limited B,
+ * no inflow angle, thetaLatDep false; Euclidean distance and atan2(dy,dx)
+ * in mesh metres in place of the ICS = 2 haversine/DEG2RAD geometry) and
+ * the NWS = 8 stress of wind.F:1172-1198 with capped Garratt drag
+ * (wind.F:514-539). */
+int orc_model_met(orc_model *m, const orc_step_t *s) {
+  if (!m->vortex_on) return 0;
+  orc_arrays_t *a = m->a;
+  const orc_params_t &p = m->p;
+  const orc_vortex_t &vp = m->vpar;
+  const std::vector<orc_vortex_fix_t> &f = m->vfix;
+  const double E = 2.718281828459045, ONE2TEN = 0.8928, PRB = 1013.0, RHOW = 1000.0;
+  int err = 0;
+  /* GetHollandStormData, nws08.F90:838-876 (position uses the previous
+   * WTRATIO) */
+  int i = m->vcounter;
+  if (s->timeloc > f[i].time) {
+    i = i + 1;
+    if (i >= vp.nfix) { err = 1; i = vp.nfix - 1; }
+  }
+  const double lon = f[i - 1].x + m->vwtratio * (f[i].x - f[i - 1].x);
+  const double lat = f[i - 1].y + m->vwtratio * (f[i].y - f[i - 1].y);
+  const double wt = (s->timeloc - f[i - 1].time) / (f[i].time - f[i - 1].time);
+  m->vwtratio = wt;
+  const double cpress = f[i - 1].cpress + wt * (f[i].cpress - f[i - 1].cpress);
+  double spd = f[i - 1].vmax + wt * (f[i].vmax - f[i - 1].vmax);
+  double rmw = f[i - 1].rmw + wt * (f[i].rmw - f[i - 1].rmw);
+  const double tvx = f[i - 1].tvx + wt * (f[i].tvx - f[i - 1].tvx);
+  const double tvy = f[i - 1].tvy + wt * (f[i].tvy - f[i - 1].tvy);
+  m->vcounter = i;
+  /* HollandGet, nws08.F90:616-639 */
+  double dpdef = PRB * 100.0 - cpress;
+  if (dpdef < 100.0) dpdef = 100.0;
+  const double ts = std::sqrt(tvx * tvx + tvy * tvy);
+  spd = spd - 1.0 * ts;
+  spd = spd / vp.bladj;
+  double B = vp.rho_air * E * (spd * spd) / dpdef;
+  if (B < 1.0) B = 1.0;
+  if (B > 2.5) B = 2.5;
+  rmw = rmw * 1000.0;
+  const double hemi = vp.hemisphere >= 0 ? 1.0 : -1.0;
+  const double awr = vp.rho_air / RHOW;
+  for (int n = 0; n < a->np; ++n) {
+    /* nws08.F90:642-715 */
+    const double dx = a->x[n] - lon, dy = a->y[n] - lat;
+    const double theta = std::atan2(dy, dx);
+    const double rad = std::sqrt(dx * dx + dy * dy);
+    const double cf = a->corif[n];
+    const double alpha = std::pow(rmw / rad, B);
+    double press = cpress + dpdef * std::exp(-alpha);
+    double vr = std::sqrt(alpha * std::exp(1.0 - alpha) * spd * (spd + 0.0) + 0.25 * (rad * rad) * (cf * cf)) -
+                0.5 * rad * std::fabs(cf);
+    vr = vr * vp.wind_mult;
+    vr = vr * vp.bladj;
+    double wx = (-hemi) * vr * std::sin(theta + hemi * 0.0);
+    double wy = hemi * vr * std::cos(theta + hemi * 0.0);
+    /* calcTranslationSpeed, nws08.F90:746-749 */
+    wx = wx + (std::fabs(vr) / spd) * tvx;
+    wy = wy + (std::fabs(vr) / spd) * tvy;
+    if (vp.avg_minute == 1) {
+      wx = wx * ONE2TEN;
+      wy = wy * ONE2TEN;
+    }
+    press = std::max(0.85e5, std::min(1.1e5, press));
+    wx = std::max(-200.0, std::min(200.0, wx));
+    wy = std::max(-200.0, std::min(200.0, wy));
+    const double prn2 = press / (RHOW * p.g);
+    /* wind.F:1174-1193 */
+    const double mag = std::sqrt(wx * wx + wy * wy);
+    const double drag = std::min(0.001 * (0.75 + 0.067 * mag), vp.drag_limit);
+    a->wsx2[n] = s->rampmete * awr * drag * wx * mag;
+    a->wsy2[n] = s->rampmete * awr * drag * wy * mag;
+    const double prdiff = s->rampmete * (prn2 - p.prbckgrnd_mh2o);
+    a->pr2[n] = p.prbckgrnd_mh2o + prdiff;
+  }
+  return err;
+}
+
 int orc_model_step(orc_model *m, const orc_step_t *s, orc_stepout_t *out) {
   orc_stepout_t tmp;
   if (!out) out = &tmp;
   std::memset(out, 0, sizeof(*out));
   orc_model_shift_friction(m, s);
+  if (orc_model_met(m, s)) { out->status = -1; return -1; }
   int st = orc_model_gwce(m, s, out);
   if (st != 0) return st;
   orc_model_wetdry(m, s, out);

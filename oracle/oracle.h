@@ -84,6 +84,19 @@ typedef struct {
   double timeloc, timeh, rampelev, rampmete;
 } orc_step_t;
 
+/* Parametric-vortex track (fort.22 fields HollandGet consumes,
+ * nws08.F90:827-878) in mesh units; same layout as adc_vortex_fix_t /
+ * adc_vortex_t in include/adcgpu.h. */
+typedef struct {
+  double time, x, y, cpress, vmax, rmw, tvx, tvy;
+} orc_vortex_fix_t;
+
+typedef struct {
+  int nfix, avg_minute, hemisphere, pad_;
+  double start_time, bladj, rho_air, wind_mult, drag_limit;
+  const orc_vortex_fix_t *fix;
+} orc_vortex_t;
+
 /* Outputs of one step. */
 typedef struct {
   int numitr;      /* IPARM(1) returned by JCG */
@@ -116,6 +129,13 @@ int orc_model_shift_friction(orc_model *m, const orc_step_t *s);
 int orc_model_gwce(orc_model *m, const orc_step_t *s, orc_stepout_t *out);
 int orc_model_wetdry(orc_model *m, const orc_step_t *s, orc_stepout_t *out);
 int orc_model_momentum(orc_model *m, const orc_step_t *s);
+/* NWS = 8 forcing: copies the track; every later step forms WSX2/WSY2/PR2
+ * from it after the shift (getMeteorologicalForcing, timestep.F:651).
+ * Returns nonzero for an invalid track. */
+int orc_model_set_vortex(orc_model *m, const orc_vortex_t *v);
+/* The met phase alone (HollandGet + wind.F:1172-1198); nonzero once the
+ * run passes the last fix. */
+int orc_model_met(orc_model *m, const orc_step_t *s);
 void orc_model_set_ncchange(orc_model *m, int ncchange);
 int orc_model_get_ncchange(const orc_model *m);
 double orc_model_get_zeta(const orc_model *m);

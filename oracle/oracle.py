@@ -64,6 +64,17 @@ class OrcStepOut(C.Structure):
                 ("cme", C.c_double), ("n_w1_events", C.c_int), ("pad_", C.c_int)]
 
 
+class OrcVortexFix(C.Structure):
+    _fields_ = [(n, C.c_double) for n in ("time", "x", "y", "cpress", "vmax", "rmw", "tvx", "tvy")]
+
+
+class OrcVortex(C.Structure):
+    _fields_ = [("nfix", C.c_int), ("avg_minute", C.c_int), ("hemisphere", C.c_int),
+                ("pad_", C.c_int)] + [(n, C.c_double) for n in (
+                    "start_time", "bladj", "rho_air", "wind_mult", "drag_limit")] + [
+                ("fix", C.POINTER(OrcVortexFix))]
+
+
 _lib = None
 
 
@@ -92,6 +103,10 @@ def load():
     for f in ("orc_model_shift_friction", "orc_model_momentum"):
         getattr(lib, f).argtypes = [C.c_void_p, C.POINTER(OrcStep)]
         getattr(lib, f).restype = C.c_int
+    lib.orc_model_set_vortex.argtypes = [C.c_void_p, C.POINTER(OrcVortex)]
+    lib.orc_model_set_vortex.restype = C.c_int
+    lib.orc_model_met.argtypes = [C.c_void_p, C.POINTER(OrcStep)]
+    lib.orc_model_met.restype = C.c_int
     lib.orc_model_set_ncchange.argtypes = [C.c_void_p, C.c_int]
     lib.orc_model_get_ncchange.argtypes = [C.c_void_p]
     lib.orc_model_get_ncchange.restype = C.c_int
@@ -123,6 +138,28 @@ class OracleModel:
             assert arr.flags.f_contiguous
             setattr(self.a, name, _ptr(arr, typ))
         self.h = self.lib.orc_model_create(C.byref(self.p), C.byref(self.a))
+        vortex = getattr(case, "vortex", None)
+        if vortex is not None:
+            self.set_vortex(vortex)
+
+    def set_vortex(self, vortex):
+        """vortex: an object with the adcirc_b200.model.Vortex fields."""
+        fx = np.ascontiguousarray(vortex.fixes, dtype=np.float64)
+        arr = (OrcVortexFix * len(fx))()
+        for k, row in enumerate(fx):
+            arr[k] = OrcVortexFix(*[float(v) for v in row])
+        v = OrcVortex()
+        v.nfix, v.avg_minute, v.hemisphere = len(fx), vortex.avg_minute, vortex.hemisphere
+        v.start_time, v.bladj, v.rho_air = vortex.start_time, vortex.bladj, vortex.rho_air
+        v.wind_mult, v.drag_limit = vortex.wind_mult, vortex.drag_limit
+        v.fix = C.cast(arr, C.POINTER(OrcVortexFix))
+        rc = self.lib.orc_model_set_vortex(self.h, C.byref(v))
+        if rc != 0:
+            raise ValueError("invalid vortex track")
+
+    def met(self, it):
+        """The met phase alone for step `it`; nonzero once past the track."""
+        return self.lib.orc_model_met(self.h, C.byref(self._st(it)))
 
     def close(self):
         if self.h:

@@ -45,6 +45,11 @@ def _check(c0, cg, its_o, its_g):
     errs = {f: _rel(b[f], a[f]) for f in FIELDS}
     bad = {f: e for f, e in errs.items() if not e <= REL_TOL}
     assert not bad, f"fields beyond {REL_TOL}: {bad}"
+    # COEF as the host sees it after sync: rebuilt, scaled and unscaled by
+    # every solve, including the drift a solve leaves for the next step
+    # (only EP at elevation-boundary rows comes from a differently ordered sum)
+    errs["coef"] = _rel(b["coef"], a["coef"])
+    assert errs["coef"] <= 1e-12, f"COEF differs: {errs['coef']}"
     assert np.array_equal(a["nodecode"], b["nodecode"])
     assert np.array_equal(a["noff"], b["noff"])
     mism = int(np.sum(its_o != its_g))
