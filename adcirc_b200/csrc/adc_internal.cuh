@@ -184,6 +184,25 @@ int launch_jcg(adc_ctx *c, int eta_update);
 int launch_wetdry(adc_ctx *c);
 int launch_momentum(adc_ctx *c);
 
+// Stores K consecutive doubles per lane (lane l owns out[K*l .. K*l+K-1]
+// of the warp's span) as K coalesced 32-wide stores through shared memory
+// `sh` (32*K doubles per warp).  Every lane of the warp must call it;
+// `nvalid` lanes carry data.
+template <int K>
+__device__ __forceinline__ void warp_store_k(double *out, const double (&v)[K], int nvalid,
+                                             double *sh) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int k = 0; k < K; ++k) sh[lane * K + k] = v[k];
+  __syncwarp();
+#pragma unroll
+  for (int m = 0; m < K; ++m) {
+    const int idx = m * 32 + lane;
+    if (idx < nvalid * K) out[idx] = sh[idx];
+  }
+  __syncwarp();
+}
+
 // Deterministic block reduction of one double (fixed tree).
 __device__ __forceinline__ double warp_sum(double v) {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);

@@ -107,8 +107,12 @@ __global__ void k_lhs_drift_flush(int *words) {
 // gwce.F:456-593: nine consistent-mass + gravity entries per element.
 __global__ void k_lhs_elem(adc_ctx c, const int *rebuild) {
   if (!*rebuild) return;
+  __shared__ double sh[kThreads / 32][32 * 9];
+  const int e0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31);   // the warp's first element
+  if (e0 >= c.ne) return;                                          // whole warp past the end
+  const int nvalid = min(32, c.ne - e0);
   int e = blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= c.ne) return;
+  if (e >= c.ne) e = c.ne - 1;   // idle lanes recompute the last element; not stored
   const adc_params_t &p = c.p;
   const double DT = p.dt;
   int n1 = c.nm[3 * e], n2 = c.nm[3 * e + 1], n3 = c.nm[3 * e + 2];
@@ -124,7 +128,7 @@ __global__ void k_lhs_elem(adc_ctx c, const int *rebuild) {
   double MsOn = 2 * AreaIE * (1.0 / DT + Tau0Avg / 2.0) / DT / 12.0;
   double MsOff = 1 * AreaIE * (1.0 / DT + Tau0Avg / 2.0) / DT / 12.0;
   double nc = (double)NCEle;
-  double *o = c.ebuf + 9 * (size_t)e;
+  double o[9];
   o[0] = (MsOn + GA * (FDX1 * FDX1 + FDY1 * FDY1)) * nc;
   o[1] = (MsOn + GA * (FDX2 * FDX2 + FDY2 * FDY2)) * nc;
   o[2] = (MsOn + GA * (FDX3 * FDX3 + FDY3 * FDY3)) * nc;
@@ -134,6 +138,7 @@ __global__ void k_lhs_elem(adc_ctx c, const int *rebuild) {
   o[6] = (MsOff + GA * (FDX2 * FDX3 + FDY2 * FDY3)) * nc;  // (n2, J23)
   o[7] = (MsOff + GA * (FDX3 * FDX1 + FDY3 * FDY1)) * nc;  // (n3, J31)
   o[8] = (MsOff + GA * (FDX3 * FDX2 + FDY3 * FDY2)) * nc;  // (n3, J32)
+  warp_store_k<9>(c.ebuf + 9 * (size_t)e0, o, nvalid, sh[threadIdx.x >> 5]);
 }
 
 // Per-row gather of COEF in element order, and the per-block partial of
@@ -252,8 +257,12 @@ __global__ void k_lhs_bc(adc_ctx c, const int *rebuild) {
 // --------------------------------------------------------------- RHS
 // gwce.F:1000-1617, one element, IM=0 branches.
 __global__ void __launch_bounds__(256, 2) k_rhs_elem(adc_ctx c) {
+  __shared__ double sh[kThreads / 32][32 * 3];
+  const int e0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31);
+  if (e0 >= c.ne) return;
+  const int nvalid = min(32, c.ne - e0);
   int e = blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= c.ne) return;
+  if (e >= c.ne) e = c.ne - 1;   // idle lanes recompute the last element; not stored
   const adc_params_t &p = c.p;
   const double DT = p.dt, G = p.g, A00 = p.a00, B00 = p.b00, C00 = p.c00;
   int n1 = c.nm[3 * e], n2 = c.nm[3 * e + 1], n3 = c.nm[3 * e + 2];
@@ -353,10 +362,8 @@ __global__ void __launch_bounds__(256, 2) k_rhs_elem(adc_ctx c) {
               c1 * (A00pB00 * (FDX3 * E1XGrad2A + FDY3 * E1YGrad2A)) +
               (JXAvg * FDX3 + JYAvg * FDY3) * 0.5 + Tau0SpaVar;
   double nc = (double)NCEle;
-  double *o = c.ebuf + 3 * (size_t)e;
-  o[0] = T1 * nc;
-  o[1] = T2 * nc;
-  o[2] = T3 * nc;
+  const double o[3] = {T1 * nc, T2 * nc, T3 * nc};
+  warp_store_k<3>(c.ebuf + 3 * (size_t)e0, o, nvalid, sh[threadIdx.x >> 5]);
 }
 
 // GWCE_LV gather (element order) fused with gwce.F:1622-1631.

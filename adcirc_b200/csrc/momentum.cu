@@ -15,8 +15,12 @@
 namespace adc {
 
 __global__ void k_mom_elem(adc_ctx c) {
+  __shared__ double sh[kThreads / 32][32 * 6];
+  const int e0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31);
+  if (e0 >= c.ne) return;
+  const int nvalid = min(32, c.ne - e0);
   int e = blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= c.ne) return;
+  if (e >= c.ne) e = c.ne - 1;   // idle lanes recompute the last element; not stored
   const adc_params_t &p = c.p;
   const double DT = p.dt;
   const double THIRD = 1.0 / 3.0, GO2 = p.g / 2.0;
@@ -61,13 +65,14 @@ __global__ void k_mom_elem(adc_ctx c) {
   double fct = nc * DT;
   double ax = -p.ifnlct * ADVX - GO2 * DBTPDXA - 0.0;
   double ay = -p.ifnlct * ADVY - GO2 * DBTPDYA - 0.0;
-  double *o = c.ebuf + 6 * (size_t)e;
+  double o[6];
   o[0] = fct * (ax - (1.5 * ((EH1 * DU1DX) * FDX1 + (EH1 * DU1DY) * FDY1)) / H1N1);
   o[1] = fct * (ax - (1.5 * ((EH2 * DU1DX) * FDX2 + (EH2 * DU1DY) * FDY2)) / H1N2);
   o[2] = fct * (ax - (1.5 * ((EH3 * DU1DX) * FDX3 + (EH3 * DU1DY) * FDY3)) / H1N3);
   o[3] = fct * (ay - (1.5 * ((EH1 * DV1DX) * FDX1 + (EH1 * DV1DY) * FDY1)) / H1N1);
   o[4] = fct * (ay - (1.5 * ((EH2 * DV1DX) * FDX2 + (EH2 * DV1DY) * FDY2)) / H1N2);
   o[5] = fct * (ay - (1.5 * ((EH3 * DV1DX) * FDX3 + (EH3 * DV1DY) * FDY3)) / H1N3);
+  warp_store_k<6>(c.ebuf + 6 * (size_t)e0, o, nvalid, sh[threadIdx.x >> 5]);
 }
 
 // gfortran's inline NORM2 for TKM(:,i) (scaled sum of squares starting
