@@ -21,6 +21,10 @@ ADC_ERR_TIMEOUT = -5
 ADC_ERR_UNSUPPORTED = -6
 ADC_PREC_FP64 = 0
 ADC_PREC_MIXED = 1
+ADC_WARM_START = 2
+ADC_F32_ASSEMBLY = 4
+ADC_F32_SPMV = 8
+ADC_F32_MOMENTUM = 16
 
 
 class AdcParams(C.Structure):
@@ -115,6 +119,7 @@ def load():
         "adc_sync_from_host": (C.c_int, [vp]),
         "adc_set_met": (C.c_int, [vp, dp_, dp_, dp_]),
         "adc_set_vortex": (C.c_int, [vp, C.POINTER(AdcVortex)]),
+        "adc_warm_start_stats": (C.c_int, [vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
         "adc_phase_times": (C.c_int, [vp, dp_, dp_, dp_, dp_, dp_]),
         "adc_launch_count": (C.c_int64, [vp]),
         "adc_last_run_ms": (C.c_double, [vp]),

@@ -79,6 +79,13 @@ struct VortexState {
   double x, y, cpress, dpdef, spd, b, rmw, tvx, tvy;
 };
 
+// Choice and statistics of the extrapolated JCG initial guess.
+struct WarmState {
+  int use;         // this step starts from the extrapolated guess
+  int pad_;
+  long long n_used, n_fallback;
+};
+
 struct adc_ctx {
   // sizes
   int np, ne, mnei, neta, nbfr, nvel, nvelme, prec;
@@ -135,6 +142,9 @@ struct adc_ctx {
   int jcg_res, jcg_rows_max, jcg_halo_max, jcg_stage_bytes;
   size_t jcg_smem;
   unsigned short *jlcol;
+  float *soff32;               // FP32 scaled matrix (mixed mode, resident variant)
+  double *etas_prev;           // last step's reference guess (ADC_WARM_START)
+  WarmState *warm;
   int *jhalo_ptr, *jhalo_ids;
   unsigned char *jexp;
   // flags / steps
@@ -184,13 +194,18 @@ int launch_jcg(adc_ctx *c, int eta_update);
 int launch_wetdry(adc_ctx *c);
 int launch_momentum(adc_ctx *c);
 
-// Stores K consecutive doubles per lane (lane l owns out[K*l .. K*l+K-1]
+// Which parts run in FP32 (ADC_PREC_MIXED selects all of them).
+inline bool f32_assembly(const adc_ctx *c) { return c->prec & (ADC_PREC_MIXED | ADC_F32_ASSEMBLY); }
+inline bool f32_spmv(const adc_ctx *c) { return c->prec & (ADC_PREC_MIXED | ADC_F32_SPMV); }
+inline bool f32_momentum(const adc_ctx *c) { return c->prec & (ADC_PREC_MIXED | ADC_F32_MOMENTUM); }
+inline bool any_f32(const adc_ctx *c) { return f32_assembly(c) || f32_spmv(c) || f32_momentum(c); }
+
+// Stores K consecutive values per lane (lane l owns out[K*l .. K*l+K-1]
 // of the warp's span) as K coalesced 32-wide stores through shared memory
-// `sh` (32*K doubles per warp).  Every lane of the warp must call it;
+// `sh` (32*K values per warp).  Every lane of the warp must call it;
 // `nvalid` lanes carry data.
-template <int K>
-__device__ __forceinline__ void warp_store_k(double *out, const double (&v)[K], int nvalid,
-                                             double *sh) {
+template <int K, class T>
+__device__ __forceinline__ void warp_store_k(T *out, const T (&v)[K], int nvalid, T *sh) {
   const int lane = threadIdx.x & 31;
 #pragma unroll
   for (int k = 0; k < K; ++k) sh[lane * K + k] = v[k];

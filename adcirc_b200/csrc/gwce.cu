@@ -105,30 +105,31 @@ __global__ void k_lhs_drift_flush(int *words) {
 }
 
 // gwce.F:456-593: nine consistent-mass + gravity entries per element.
+template <class R>
 __global__ void k_lhs_elem(adc_ctx c, const int *rebuild) {
   if (!*rebuild) return;
-  __shared__ double sh[kThreads / 32][32 * 9];
+  __shared__ R sh[kThreads / 32][32 * 9];
   const int e0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31);   // the warp's first element
   if (e0 >= c.ne) return;                                          // whole warp past the end
   const int nvalid = min(32, c.ne - e0);
   int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= c.ne) e = c.ne - 1;   // idle lanes recompute the last element; not stored
   const adc_params_t &p = c.p;
-  const double DT = p.dt;
+  const R DT = R(p.dt);
   int n1 = c.nm[3 * e], n2 = c.nm[3 * e + 1], n3 = c.nm[3 * e + 2];
   int NCEle = c.nodecode[n1] * c.nodecode[n2] * c.nodecode[n3] * c.noff[e];
-  double FDX1 = c.fdx[3 * e], FDX2 = c.fdx[3 * e + 1], FDX3 = c.fdx[3 * e + 2];
-  double FDY1 = c.fdy[3 * e], FDY2 = c.fdy[3 * e + 1], FDY3 = c.fdy[3 * e + 2];
-  double AreaIE2 = c.areas[e];
-  double AreaIE = AreaIE2 * 0.5;
-  double AreaIE4 = AreaIE2 * 2.0;
-  double DPAvg = (c.dp[n1] + c.dp[n2] + c.dp[n3]) / 3.0;
-  double GA = c.alphal[e] * p.a00 * p.g * DPAvg / AreaIE4;
-  double Tau0Avg = (c.tau0[n1] + c.tau0[n2] + c.tau0[n3]) / 3.0;
-  double MsOn = 2 * AreaIE * (1.0 / DT + Tau0Avg / 2.0) / DT / 12.0;
-  double MsOff = 1 * AreaIE * (1.0 / DT + Tau0Avg / 2.0) / DT / 12.0;
-  double nc = (double)NCEle;
-  double o[9];
+  R FDX1 = c.fdx[3 * e], FDX2 = c.fdx[3 * e + 1], FDX3 = c.fdx[3 * e + 2];
+  R FDY1 = c.fdy[3 * e], FDY2 = c.fdy[3 * e + 1], FDY3 = c.fdy[3 * e + 2];
+  R AreaIE2 = c.areas[e];
+  R AreaIE = AreaIE2 * R(0.5);
+  R AreaIE4 = AreaIE2 * R(2.0);
+  R DPAvg = (c.dp[n1] + c.dp[n2] + c.dp[n3]) / R(3.0);
+  R GA = R(c.alphal[e]) * R(p.a00) * R(p.g) * DPAvg / AreaIE4;
+  R Tau0Avg = (c.tau0[n1] + c.tau0[n2] + c.tau0[n3]) / R(3.0);
+  R MsOn = 2 * AreaIE * (R(1.0) / DT + Tau0Avg / R(2.0)) / DT / R(12.0);
+  R MsOff = 1 * AreaIE * (R(1.0) / DT + Tau0Avg / R(2.0)) / DT / R(12.0);
+  R nc = (R)NCEle;
+  R o[9];
   o[0] = (MsOn + GA * (FDX1 * FDX1 + FDY1 * FDY1)) * nc;
   o[1] = (MsOn + GA * (FDX2 * FDX2 + FDY2 * FDY2)) * nc;
   o[2] = (MsOn + GA * (FDX3 * FDX3 + FDY3 * FDY3)) * nc;
@@ -138,56 +139,58 @@ __global__ void k_lhs_elem(adc_ctx c, const int *rebuild) {
   o[6] = (MsOff + GA * (FDX2 * FDX3 + FDY2 * FDY3)) * nc;  // (n2, J23)
   o[7] = (MsOff + GA * (FDX3 * FDX1 + FDY3 * FDY1)) * nc;  // (n3, J31)
   o[8] = (MsOff + GA * (FDX3 * FDX2 + FDY3 * FDY2)) * nc;  // (n3, J32)
-  warp_store_k<9>(c.ebuf + 9 * (size_t)e0, o, nvalid, sh[threadIdx.x >> 5]);
+  warp_store_k<9>(reinterpret_cast<R *>(c.ebuf) + 9 * (size_t)e0, o, nvalid, sh[threadIdx.x >> 5]);
 }
 
 // Per-row gather of COEF in element order, and the per-block partial of
 // sum(diag^2) for EP (gwce.F:646-650).
+template <class R>
 __global__ void k_lhs_gather(adc_ctx c, const int *rebuild) {
   if (!*rebuild) return;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const R *eb = reinterpret_cast<const R *>(c.ebuf);
   double d2 = 0.0;
   if (i < c.np) {
-    double d = 0.0;
+    R d = R(0.0);
     const int q0 = c.n2e_ptr[i], q1 = c.n2e_ptr[i + 1];
     for (int qc = q0; qc < q1; qc += kGatherChunk) {
       int ek[kGatherChunk];
-      double x[kGatherChunk];
+      R x[kGatherChunk];
 #pragma unroll
       for (int k = 0; k < kGatherChunk; ++k) if (qc + k < q1) ek[k] = c.n2e[qc + k];
 #pragma unroll
       for (int k = 0; k < kGatherChunk; ++k)
         if (qc + k < q1) {
           int e = ek[k] / 3, kk = ek[k] - 3 * e;
-          x[k] = c.ebuf[9 * (size_t)e + kk];
+          x[k] = eb[9 * (size_t)e + kk];
         }
 #pragma unroll
       for (int k = 0; k < kGatherChunk; ++k) if (qc + k < q1) d = d + x[k];
     }
-    c.diag[i] = d;
-    d2 = d * d;
+    c.diag[i] = (double)d;
+    d2 = (double)d * (double)d;
     int s = i / kSlice, lane = i - s * kSlice;
     int base = c.sl_ptr[s] + lane;
     int len = c.rlen[i];
     for (int kc = 0; kc < len; kc += kGatherChunk) {
       int2 src[kGatherChunk];
-      double va[kGatherChunk], vb[kGatherChunk];
+      R va[kGatherChunk], vb[kGatherChunk];
 #pragma unroll
       for (int k = 0; k < kGatherChunk; ++k)
         if (kc + k < len) src[k] = reinterpret_cast<const int2 *>(c.lhs_src)[base + (kc + k) * kSlice];
 #pragma unroll
       for (int k = 0; k < kGatherChunk; ++k)
         if (kc + k < len) {
-          va[k] = src[k].x >= 0 ? c.ebuf[src[k].x] : 0.0;
-          vb[k] = src[k].y >= 0 ? c.ebuf[src[k].y] : 0.0;
+          va[k] = src[k].x >= 0 ? eb[src[k].x] : R(0.0);
+          vb[k] = src[k].y >= 0 ? eb[src[k].y] : R(0.0);
         }
 #pragma unroll
       for (int k = 0; k < kGatherChunk; ++k)
         if (kc + k < len) {
-          double v = 0.0;
+          R v = R(0.0);
           if (src[k].x >= 0) v = v + va[k];
           if (src[k].y >= 0) v = v + vb[k];
-          c.offd[base + (kc + k) * kSlice] = v;
+          c.offd[base + (kc + k) * kSlice] = (double)v;
         }
     }
   }
@@ -256,90 +259,117 @@ __global__ void k_lhs_bc(adc_ctx c, const int *rebuild) {
 
 // --------------------------------------------------------------- RHS
 // gwce.F:1000-1617, one element, IM=0 branches.
-__global__ void __launch_bounds__(256, 2) k_rhs_elem(adc_ctx c) {
-  __shared__ double sh[kThreads / 32][32 * 3];
+template <class R>
+__global__ void __launch_bounds__(256, sizeof(R) == 4 ? 3 : 2) k_rhs_elem(adc_ctx c) {
+  __shared__ R sh[kThreads / 32][32 * 3];
   const int e0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31);
   if (e0 >= c.ne) return;
   const int nvalid = min(32, c.ne - e0);
   int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= c.ne) e = c.ne - 1;   // idle lanes recompute the last element; not stored
   const adc_params_t &p = c.p;
-  const double DT = p.dt, G = p.g, A00 = p.a00, B00 = p.b00, C00 = p.c00;
+  const R DT = R(p.dt), G = R(p.g), A00 = R(p.a00), B00 = R(p.b00), C00 = R(p.c00);
   int n1 = c.nm[3 * e], n2 = c.nm[3 * e + 1], n3 = c.nm[3 * e + 2];
   int NCEle = c.nodecode[n1] * c.nodecode[n2] * c.nodecode[n3] * c.noff[e];
-  double E0N1 = c.eta1[n1], E0N2 = c.eta1[n2], E0N3 = c.eta1[n3];
-  double E1N1 = c.eta2[n1], E1N2 = c.eta2[n2], E1N3 = c.eta2[n3];
-  double E1N1SQ = E1N1 * E1N1, E1N2SQ = E1N2 * E1N2, E1N3SQ = E1N3 * E1N3;
-  double ESN1 = c.etas[n1], ESN2 = c.etas[n2], ESN3 = c.etas[n3];
-  double U1N1 = c.uu1[n1], U1N2 = c.uu1[n2], U1N3 = c.uu1[n3];
-  double V1N1 = c.vv1[n1], V1N2 = c.vv1[n2], V1N3 = c.vv1[n3];
-  double QX1N1 = c.qx1[n1], QX1N2 = c.qx1[n2], QX1N3 = c.qx1[n3];
-  double QY1N1 = c.qy1[n1], QY1N2 = c.qy1[n2], QY1N3 = c.qy1[n3];
-  double H1N1 = c.h2[n1], H1N2 = c.h2[n2], H1N3 = c.h2[n3];
-  double EVMN1 = c.evm[n1], EVMN2 = c.evm[n2], EVMN3 = c.evm[n3];
-  double T0N1 = c.tau0[n1], T0N2 = c.tau0[n2], T0N3 = c.tau0[n3];
+  R E0N1 = c.eta1[n1], E0N2 = c.eta1[n2], E0N3 = c.eta1[n3];
+  R E1N1 = c.eta2[n1], E1N2 = c.eta2[n2], E1N3 = c.eta2[n3];
+  R E1N1SQ = E1N1 * E1N1, E1N2SQ = E1N2 * E1N2, E1N3SQ = E1N3 * E1N3;
+  R ESN1 = c.etas[n1], ESN2 = c.etas[n2], ESN3 = c.etas[n3];
+  R U1N1 = c.uu1[n1], U1N2 = c.uu1[n2], U1N3 = c.uu1[n3];
+  R V1N1 = c.vv1[n1], V1N2 = c.vv1[n2], V1N3 = c.vv1[n3];
+  R QX1N1 = c.qx1[n1], QX1N2 = c.qx1[n2], QX1N3 = c.qx1[n3];
+  R QY1N1 = c.qy1[n1], QY1N2 = c.qy1[n2], QY1N3 = c.qy1[n3];
+  R H1N1 = c.h2[n1], H1N2 = c.h2[n2], H1N3 = c.h2[n3];
+  R EVMN1 = c.evm[n1], EVMN2 = c.evm[n2], EVMN3 = c.evm[n3];
+  R T0N1 = c.tau0[n1], T0N2 = c.tau0[n2], T0N3 = c.tau0[n3];
   const bool met = p.nws != 0;
-  double Pr1N1 = 0.0, Pr1N2 = 0.0, Pr1N3 = 0.0;
-  if (met) { Pr1N1 = c.pr1[n1]; Pr1N2 = c.pr1[n2]; Pr1N3 = c.pr1[n3]; }
+  R Pr1N1 = R(0.0), Pr1N2 = R(0.0), Pr1N3 = R(0.0);
+  if (met) {
+    if constexpr (sizeof(R) == 4) {
+      // only the gradient of PR1 is used: FP32 carries its deviation from
+      // the background pressure, not the ~10 m total
+      const double pb = p.prbckgrnd_mh2o;
+      Pr1N1 = R(c.pr1[n1] - pb); Pr1N2 = R(c.pr1[n2] - pb); Pr1N3 = R(c.pr1[n3] - pb);
+    } else {
+      Pr1N1 = c.pr1[n1]; Pr1N2 = c.pr1[n2]; Pr1N3 = c.pr1[n3];
+    }
+  }
   const double *tk1 = c.tkm + 3 * n1, *tk2 = c.tkm + 3 * n2, *tk3 = c.tkm + 3 * n3;
-  double BSXN1 = tk1[0] * QX1N1 + tk1[2] * QY1N1;
-  double BSYN1 = tk1[2] * QX1N1 + tk1[1] * QY1N1;
-  double BSXN2 = tk2[0] * QX1N2 + tk2[2] * QY1N2;
-  double BSYN2 = tk2[2] * QX1N2 + tk2[1] * QY1N2;
-  double BSXN3 = tk3[0] * QX1N3 + tk3[2] * QY1N3;
-  double BSYN3 = tk3[2] * QX1N3 + tk3[1] * QY1N3;
-  double AreaIE2 = c.areas[e];
-  double AreaIE = AreaIE2 / 2.0;
-  double AreaIE4 = 2.0 * AreaIE2;
-  double FDX1 = c.fdx[3 * e], FDX2 = c.fdx[3 * e + 1], FDX3 = c.fdx[3 * e + 2];
-  double FDY1 = c.fdy[3 * e], FDY2 = c.fdy[3 * e + 1], FDY3 = c.fdy[3 * e + 2];
-  double E0XGrad2A = E0N1 * FDX1 + E0N2 * FDX2 + E0N3 * FDX3;
-  double E0YGrad2A = E0N1 * FDY1 + E0N2 * FDY2 + E0N3 * FDY3;
-  double E1XGrad2A = E1N1 * FDX1 + E1N2 * FDX2 + E1N3 * FDX3;
-  double E1YGrad2A = E1N1 * FDY1 + E1N2 * FDY2 + E1N3 * FDY3;
-  double Tau0XGrad2A = T0N1 * FDX1 + T0N2 * FDX2 + T0N3 * FDX3;
-  double Tau0YGrad2A = T0N1 * FDY1 + T0N2 * FDY2 + T0N3 * FDY3;
-  double EVMXGrad = (EVMN1 * FDX1 + EVMN2 * FDX2 + EVMN3 * FDX3) / AreaIE2;
-  double EVMYGrad = (EVMN1 * FDY1 + EVMN2 * FDY2 + EVMN3 * FDY3) / AreaIE2;
-  double EVMAvgODT = ((EVMN1 + EVMN2 + EVMN3) / 3.0) / DT;
-  double MX = (EVMXGrad * (QX1N1 * FDX1 + QX1N2 * FDX2 + QX1N3 * FDX3) +
+  R BSXN1 = R(tk1[0]) * QX1N1 + R(tk1[2]) * QY1N1;
+  R BSYN1 = R(tk1[2]) * QX1N1 + R(tk1[1]) * QY1N1;
+  R BSXN2 = R(tk2[0]) * QX1N2 + R(tk2[2]) * QY1N2;
+  R BSYN2 = R(tk2[2]) * QX1N2 + R(tk2[1]) * QY1N2;
+  R BSXN3 = R(tk3[0]) * QX1N3 + R(tk3[2]) * QY1N3;
+  R BSYN3 = R(tk3[2]) * QX1N3 + R(tk3[1]) * QY1N3;
+  R AreaIE2 = c.areas[e];
+  R AreaIE = AreaIE2 / R(2.0);
+  R AreaIE4 = R(2.0) * AreaIE2;
+  R FDX1 = c.fdx[3 * e], FDX2 = c.fdx[3 * e + 1], FDX3 = c.fdx[3 * e + 2];
+  R FDY1 = c.fdy[3 * e], FDY2 = c.fdy[3 * e + 1], FDY3 = c.fdy[3 * e + 2];
+  R E0XGrad2A, E0YGrad2A, E1XGrad2A, E1YGrad2A, E1SQXGrad2A, E1SQYGrad2A;
+  if constexpr (sizeof(R) == 4) {
+    // Elevation gradients cancel metre-sized nodal values down to
+    // centimetres: they are formed in FP64 and only then narrowed.
+    const double *fx = c.fdx + 3 * e, *fy = c.fdy + 3 * e;
+    const double a1 = c.eta1[n1], a2 = c.eta1[n2], a3 = c.eta1[n3];
+    const double b1 = c.eta2[n1], b2 = c.eta2[n2], b3 = c.eta2[n3];
+    E0XGrad2A = R(a1 * fx[0] + a2 * fx[1] + a3 * fx[2]);
+    E0YGrad2A = R(a1 * fy[0] + a2 * fy[1] + a3 * fy[2]);
+    E1XGrad2A = R(b1 * fx[0] + b2 * fx[1] + b3 * fx[2]);
+    E1YGrad2A = R(b1 * fy[0] + b2 * fy[1] + b3 * fy[2]);
+    E1SQXGrad2A = R(b1 * b1 * fx[0] + b2 * b2 * fx[1] + b3 * b3 * fx[2]);
+    E1SQYGrad2A = R(b1 * b1 * fy[0] + b2 * b2 * fy[1] + b3 * b3 * fy[2]);
+  } else {
+    E0XGrad2A = E0N1 * FDX1 + E0N2 * FDX2 + E0N3 * FDX3;
+    E0YGrad2A = E0N1 * FDY1 + E0N2 * FDY2 + E0N3 * FDY3;
+    E1XGrad2A = E1N1 * FDX1 + E1N2 * FDX2 + E1N3 * FDX3;
+    E1YGrad2A = E1N1 * FDY1 + E1N2 * FDY2 + E1N3 * FDY3;
+    E1SQXGrad2A = E1N1SQ * FDX1 + E1N2SQ * FDX2 + E1N3SQ * FDX3;
+    E1SQYGrad2A = E1N1SQ * FDY1 + E1N2SQ * FDY2 + E1N3SQ * FDY3;
+  }
+  R Tau0XGrad2A = T0N1 * FDX1 + T0N2 * FDX2 + T0N3 * FDX3;
+  R Tau0YGrad2A = T0N1 * FDY1 + T0N2 * FDY2 + T0N3 * FDY3;
+  R EVMXGrad = (EVMN1 * FDX1 + EVMN2 * FDX2 + EVMN3 * FDX3) / AreaIE2;
+  R EVMYGrad = (EVMN1 * FDY1 + EVMN2 * FDY2 + EVMN3 * FDY3) / AreaIE2;
+  R EVMAvgODT = ((EVMN1 + EVMN2 + EVMN3) / R(3.0)) / DT;
+  R MX = (EVMXGrad * (QX1N1 * FDX1 + QX1N2 * FDX2 + QX1N3 * FDX3) +
                EVMYGrad * (QY1N1 * FDX1 + QY1N2 * FDX2 + QY1N3 * FDX3) -
                EVMAvgODT * (ESN1 * FDX1 + ESN2 * FDX2 + ESN3 * FDX3)) / AreaIE2;
-  double MY = (EVMXGrad * (QX1N1 * FDY1 + QX1N2 * FDY2 + QX1N3 * FDY3) +
+  R MY = (EVMXGrad * (QX1N1 * FDY1 + QX1N2 * FDY2 + QX1N3 * FDY3) +
                EVMYGrad * (QY1N1 * FDY1 + QY1N2 * FDY2 + QY1N3 * FDY3) -
                EVMAvgODT * (ESN1 * FDY1 + ESN2 * FDY2 + ESN3 * FDY3)) / AreaIE2;
-  double CorifAvg = (c.corif[n1] + c.corif[n2] + c.corif[n3]) / 3.0;
-  double Tau0Avg = (T0N1 + T0N2 + T0N3) / 3.0;
-  double Tau0QXAvg = (T0N1 * QX1N1 + T0N2 * QX1N2 + T0N3 * QX1N3) / 3.0;
-  double Tau0QYAvg = (T0N1 * QY1N1 + T0N2 * QY1N2 + T0N3 * QY1N3) / 3.0;
-  double U1Avg = (U1N1 + U1N2 + U1N3) / 3.0;
-  double V1Avg = (V1N1 + V1N2 + V1N3) / 3.0;
-  double QX1Avg = (QX1N1 + QX1N2 + QX1N3) / 3.0;
-  double QY1Avg = (QY1N1 + QY1N2 + QY1N3) / 3.0;
-  double ESAvg = (ESN1 + ESN2 + ESN3) / 3.0;
-  double DPAvg = (c.dp[n1] + c.dp[n2] + c.dp[n3]) / 3.0;
-  double al = c.alphal[e];
-  double GDPAvgOAreaIE4 = al * G * DPAvg / AreaIE4;
-  double GDPAvgOAreaIE4_S0 = GDPAvgOAreaIE4;   // DPAvgS0 == DPAvg when IFNL_HDP = 0
-  double HAvg = (H1N1 + H1N2 + H1N3) / 3.0;
-  double GHAvg = al * G * HAvg;
-  double GHAvgOAreaIE2 = GHAvg / AreaIE2;
-  double BSXAvg = (BSXN1 + BSXN2 + BSXN3) / 3.0;
-  double BSYAvg = (BSYN1 + BSYN2 + BSYN3) / 3.0;
-  double WSXAvg = 0.0, WSYAvg = 0.0;
+  R CorifAvg = (c.corif[n1] + c.corif[n2] + c.corif[n3]) / R(3.0);
+  R Tau0Avg = (T0N1 + T0N2 + T0N3) / R(3.0);
+  R Tau0QXAvg = (T0N1 * QX1N1 + T0N2 * QX1N2 + T0N3 * QX1N3) / R(3.0);
+  R Tau0QYAvg = (T0N1 * QY1N1 + T0N2 * QY1N2 + T0N3 * QY1N3) / R(3.0);
+  R U1Avg = (U1N1 + U1N2 + U1N3) / R(3.0);
+  R V1Avg = (V1N1 + V1N2 + V1N3) / R(3.0);
+  R QX1Avg = (QX1N1 + QX1N2 + QX1N3) / R(3.0);
+  R QY1Avg = (QY1N1 + QY1N2 + QY1N3) / R(3.0);
+  R ESAvg = (ESN1 + ESN2 + ESN3) / R(3.0);
+  R DPAvg = (c.dp[n1] + c.dp[n2] + c.dp[n3]) / R(3.0);
+  R al = c.alphal[e];
+  R GDPAvgOAreaIE4 = al * G * DPAvg / AreaIE4;
+  R GDPAvgOAreaIE4_S0 = GDPAvgOAreaIE4;   // DPAvgS0 == DPAvg when IFNL_HDP = 0
+  R HAvg = (H1N1 + H1N2 + H1N3) / R(3.0);
+  R GHAvg = al * G * HAvg;
+  R GHAvgOAreaIE2 = GHAvg / AreaIE2;
+  R BSXAvg = (BSXN1 + BSXN2 + BSXN3) / R(3.0);
+  R BSYAvg = (BSYN1 + BSYN2 + BSYN3) / R(3.0);
+  R WSXAvg = R(0.0), WSYAvg = R(0.0);
   if (met) {
-    WSXAvg = (c.wsx1[n1] + c.wsx1[n2] + c.wsx1[n3]) / 3.0;
-    WSYAvg = (c.wsy1[n1] + c.wsy1[n2] + c.wsy1[n3]) / 3.0;
+    WSXAvg = (c.wsx1[n1] + c.wsx1[n2] + c.wsx1[n3]) / R(3.0);
+    WSYAvg = (c.wsy1[n1] + c.wsy1[n2] + c.wsy1[n3]) / R(3.0);
   }
-  double MsFacR = AreaIE * (1.0 / DT - Tau0Avg / 2.0) / DT / 12.0;
-  double GOAreaIE4 = al * G / AreaIE4;
-  double Tau0SpaVar = (QX1Avg * Tau0XGrad2A + QY1Avg * Tau0YGrad2A) / 6.0;
-  double A00pB00 = A00 + B00;
-  double fa = p.ifnlfa * GOAreaIE4;
-  double JXAvg = CorifAvg * QY1Avg - fa * (E1N1SQ * FDX1 + E1N2SQ * FDX2 + E1N3SQ * FDX3) -
+  R MsFacR = AreaIE * (R(1.0) / DT - Tau0Avg / R(2.0)) / DT / R(12.0);
+  R GOAreaIE4 = al * G / AreaIE4;
+  R Tau0SpaVar = (QX1Avg * Tau0XGrad2A + QY1Avg * Tau0YGrad2A) / R(6.0);
+  R A00pB00 = A00 + B00;
+  R fa = p.ifnlfa * GOAreaIE4;
+  R JXAvg = CorifAvg * QY1Avg - fa * E1SQXGrad2A -
                  GHAvgOAreaIE2 * (Pr1N1 * FDX1 + Pr1N2 * FDX2 + Pr1N3 * FDX3) + WSXAvg -
                  BSXAvg + MX + Tau0QXAvg;
-  double JYAvg = -CorifAvg * QX1Avg - fa * (E1N1SQ * FDY1 + E1N2SQ * FDY2 + E1N3SQ * FDY3) -
+  R JYAvg = -CorifAvg * QX1Avg - fa * E1SQYGrad2A -
                  GHAvgOAreaIE2 * (Pr1N1 * FDY1 + Pr1N2 * FDY2 + Pr1N3 * FDY3) + WSYAvg -
                  BSYAvg + MY + Tau0QYAvg;
   JXAvg = JXAvg - p.ifnlct * (QX1Avg * (U1N1 * FDX1 + U1N2 * FDX2 + U1N3 * FDX3) +
@@ -348,41 +378,43 @@ __global__ void __launch_bounds__(256, 2) k_rhs_elem(adc_ctx c) {
   JYAvg = JYAvg - p.ifnlct * (QX1Avg * (V1N1 * FDX1 + V1N2 * FDX2 + V1N3 * FDX3) +
                               QY1Avg * (V1N1 * FDY1 + V1N2 * FDY2 + V1N3 * FDY3)) / AreaIE2 +
           p.ifnlcat * V1Avg * ESAvg / DT;
-  double c0 = GDPAvgOAreaIE4_S0, c1 = GDPAvgOAreaIE4;
-  double T1 = (2 * ESN1 + 1 * (ESN2 + ESN3)) * MsFacR -
+  R c0 = GDPAvgOAreaIE4_S0, c1 = GDPAvgOAreaIE4;
+  R T1 = (2 * ESN1 + 1 * (ESN2 + ESN3)) * MsFacR -
               c0 * (C00 * (FDX1 * E0XGrad2A + FDY1 * E0YGrad2A)) -
               c1 * (A00pB00 * (FDX1 * E1XGrad2A + FDY1 * E1YGrad2A)) +
-              (JXAvg * FDX1 + JYAvg * FDY1) * 0.5 + Tau0SpaVar;
-  double T2 = (2 * ESN2 + 1 * (ESN1 + ESN3)) * MsFacR -
+              (JXAvg * FDX1 + JYAvg * FDY1) * R(0.5) + Tau0SpaVar;
+  R T2 = (2 * ESN2 + 1 * (ESN1 + ESN3)) * MsFacR -
               c0 * (C00 * (FDX2 * E0XGrad2A + FDY2 * E0YGrad2A)) -
               c1 * (A00pB00 * (FDX2 * E1XGrad2A + FDY2 * E1YGrad2A)) +
-              (JXAvg * FDX2 + JYAvg * FDY2) * 0.5 + Tau0SpaVar;
-  double T3 = (2 * ESN3 + 1 * (ESN1 + ESN2)) * MsFacR -
+              (JXAvg * FDX2 + JYAvg * FDY2) * R(0.5) + Tau0SpaVar;
+  R T3 = (2 * ESN3 + 1 * (ESN1 + ESN2)) * MsFacR -
               c0 * (C00 * (FDX3 * E0XGrad2A + FDY3 * E0YGrad2A)) -
               c1 * (A00pB00 * (FDX3 * E1XGrad2A + FDY3 * E1YGrad2A)) +
-              (JXAvg * FDX3 + JYAvg * FDY3) * 0.5 + Tau0SpaVar;
-  double nc = (double)NCEle;
-  const double o[3] = {T1 * nc, T2 * nc, T3 * nc};
-  warp_store_k<3>(c.ebuf + 3 * (size_t)e0, o, nvalid, sh[threadIdx.x >> 5]);
+              (JXAvg * FDX3 + JYAvg * FDY3) * R(0.5) + Tau0SpaVar;
+  R nc = (R)NCEle;
+  const R o[3] = {T1 * nc, T2 * nc, T3 * nc};
+  warp_store_k<3>(reinterpret_cast<R *>(c.ebuf) + 3 * (size_t)e0, o, nvalid, sh[threadIdx.x >> 5]);
 }
 
 // GWCE_LV gather (element order) fused with gwce.F:1622-1631.
+template <class R>
 __global__ void k_rhs_gather(adc_ctx c) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= c.np) return;
-  double v = 0.0;
+  const R *eb = reinterpret_cast<const R *>(c.ebuf);
+  R v = R(0.0);
   const int q0 = c.n2e_ptr[i], q1 = c.n2e_ptr[i + 1];
   for (int qc = q0; qc < q1; qc += kGatherChunk) {
     int ek[kGatherChunk];
-    double x[kGatherChunk];
+    R x[kGatherChunk];
 #pragma unroll
     for (int k = 0; k < kGatherChunk; ++k) if (qc + k < q1) ek[k] = c.n2e[qc + k];
 #pragma unroll
-    for (int k = 0; k < kGatherChunk; ++k) if (qc + k < q1) x[k] = c.ebuf[ek[k]];
+    for (int k = 0; k < kGatherChunk; ++k) if (qc + k < q1) x[k] = eb[ek[k]];
 #pragma unroll
     for (int k = 0; k < kGatherChunk; ++k) if (qc + k < q1) v = v + x[k];
   }
-  c.gwce_lv[i] = v;
+  c.gwce_lv[i] = (double)v;
   c.eta1[i] = c.eta2[i];
   c.h1[i] = c.h2[i];
   c.eta2[i] = 0.0;
@@ -419,5 +451,14 @@ __global__ void k_obc_rhs(adc_ctx c) {
     v = v - c.etas[c.obc_rhs_b[q]] * c.obccoef[c.obc_rhs_ent[q]];
   c.gwce_lv[nb] = v;
 }
+
+template __global__ void k_lhs_elem<double>(adc_ctx, const int *);
+template __global__ void k_lhs_elem<float>(adc_ctx, const int *);
+template __global__ void k_lhs_gather<double>(adc_ctx, const int *);
+template __global__ void k_lhs_gather<float>(adc_ctx, const int *);
+template __global__ void k_rhs_elem<double>(adc_ctx);
+template __global__ void k_rhs_elem<float>(adc_ctx);
+template __global__ void k_rhs_gather<double>(adc_ctx);
+template __global__ void k_rhs_gather<float>(adc_ctx);
 
 }  // namespace adc

@@ -32,6 +32,7 @@
 #include <cstring>
 #include <vector>
 #include <algorithm>
+#include <type_traits>
 
 namespace adc {
 
@@ -57,6 +58,7 @@ struct JcgArgs {
   int n, nslices, nrb, itmax;
   const int *sl_ptr, *sl_w, *col, *rlen;
   double *offd, *soff, *diag, *rhs;
+  float *soff32;                // FP32 copy of the scaled matrix (mixed mode)
   double *u, *u1, *w;
   P4 *p0, *p1;
   double *part, *tri;
@@ -74,7 +76,8 @@ struct JcgArgs {
   const int *halo_ptr;        // [nrb + 1] into halo_ids
   const int *halo_ids;        // halo nodes of each row block (global rows)
   const unsigned char *exp;   // per row: read by another row block
-  int defer_drift;            // 1: leave the COEF unscal drift to the next step
+  int defer_drift;            // 1: leave the COEF unscal drift to the next step;
+                              // 2: drop it (mixed mode, COEF is rebuilt or kept as is)
   int *drift_pending;         // set to 1 when the drift is left pending
   const int *nodecode;
   const double *eta1;
@@ -483,21 +486,25 @@ struct SlicePipe {
   int stage_bytes, s0, s1, first, step, lane;
   uint32_t parbits;
 
-  __device__ void issue(int sl, int st, const double *vals) {
+  // V: the staged value type (FP64 matrix, or FP32 in the mixed mode)
+  template <class V>
+  __device__ void issue(int sl, int st, const V *vals) {
     if (lane == 0) {
       const int2 mt = meta[sl - s0];
       const uint32_t w = (uint32_t)mt.y;
+      const uint32_t vb = w * 32u * (uint32_t)sizeof(V);
       unsigned char *b = stg0 + (size_t)st * stage_bytes;
-      mbar_expect_tx(bar0 + st, w * 320u);
+      mbar_expect_tx(bar0 + st, w * 64u + vb);
       if (w > 0) {
         bulk_load(b, lcol + mt.x, w * 64u, bar0 + st);
-        bulk_load(b + w * 64u, vals + mt.x, w * 256u, bar0 + st);
+        bulk_load(b + w * 64u, vals + mt.x, vb, bar0 + st);
       }
     }
   }
   // Orders earlier generic writes of `vals` before the copies, then starts
   // the warp's first two slices.
-  __device__ void begin(const double *vals) {
+  template <class V>
+  __device__ void begin(const V *vals) {
     if (lane == 0) fence_proxy_async_all();
     if (first < s1) issue(first, 0, vals);
     if (first + step < s1) issue(first + step, 1, vals);
@@ -525,15 +532,15 @@ struct SlicePipe {
   }
   // body(sl, lc, lv): one slice from shared memory; lc/lv hold slot q of
   // lane l at [q * 32 + l].  Returns false on an expired wait.
-  template <class F>
-  __device__ bool run(const double *vals, F body) {
+  template <class V, class F>
+  __device__ bool run(const V *vals, F body) {
     int k = 0;
     for (int sl = first; sl < s1; sl += step, ++k) {
       const int st = k & 1;
       if (!wait(st, sl + step < s1)) return false;
       const int w = meta[sl - s0].y;
       const unsigned char *b = stg0 + (size_t)st * stage_bytes;
-      body(sl, (const unsigned short *)b, (const double *)(b + (size_t)w * 64));
+      body(sl, (const unsigned short *)b, (const V *)(b + (size_t)w * 64));
       __syncwarp();
       if (sl + 2 * step < s1) issue(sl + 2 * step, st, vals);
     }
@@ -542,8 +549,12 @@ struct SlicePipe {
 };
 
 // ------------------------------------------------------------ the kernel
-template <int kRes>
+// kRes: 1 = resident variant.  VT: storage type of the scaled matrix the
+// iterations stream (double; float in the mixed-precision mode, where the
+// products still accumulate in FP64).
+template <int kRes, class VT>
 __global__ void __launch_bounds__(kThreads, 2) jcg_kernel(JcgArgs a) {
+  VT *const sv_store = std::is_same<VT, float>::value ? (VT *)a.soff32 : (VT *)a.soff;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
   const bool scalar_block = (blockIdx.x == (unsigned)a.nrb);
   const int s0 = scalar_block ? 0 : (int)((long long)a.nslices * blockIdx.x / a.nrb);
@@ -738,7 +749,7 @@ __global__ void __launch_bounds__(kThreads, 2) jcg_kernel(JcgArgs a) {
             const int lq = lc[q * kSlice + lane];
             const double wj = Wv[lq];
             const double sv = lv[q * kSlice + lane] * wi * wj;
-            a.soff[base + q * kSlice] = sv;
+            sv_store[base + q * kSlice] = (VT)sv;
             if (!a.defer_drift) a.offd[base + q * kSlice] = sv * winv_i * (1.0 / wj);
             acc = acc - sv * Uv[lq];
           }
@@ -754,7 +765,7 @@ __global__ void __launch_bounds__(kThreads, 2) jcg_kernel(JcgArgs a) {
     if (!phase_sync(a, scalar_block, gen)) return;
     // P2: dtwd0 = -A' d0 and the iteration-0 norms.
     if (!scalar_block) {
-      pipe.begin(a.soff);
+      pipe.begin((const VT *)sv_store);
       double *Dv = S_dd;
       for (int idx = threadIdx.x; idx < rows; idx += blockDim.x) {
         Dv[idx] = S_t[idx];
@@ -763,12 +774,13 @@ __global__ void __launch_bounds__(kThreads, 2) jcg_kernel(JcgArgs a) {
       const int h0 = a.halo_ptr[blockIdx.x], nh = a.halo_ptr[blockIdx.x + 1] - h0;
       for (int h = threadIdx.x; h < nh; h += blockDim.x) Dv[RB + h] = a.p0[a.halo_ids[h0 + h]].y;
       __syncthreads();
-      bool ok = pipe.run(a.soff, [&](int sl, const unsigned short *lc, const double *lv) {
+      bool ok = pipe.run((const VT *)sv_store, [&](int sl, const unsigned short *lc, const VT *lv) {
         const int i = sl * kSlice + lane, idx = i - r0;
         if (i < n) {
           const int len = S_le[idx] & 127;
           double acc = 0.0;
-          for (int q = 0; q < len; ++q) acc = acc - lv[q * kSlice + lane] * Dv[lc[q * kSlice + lane]];
+          for (int q = 0; q < len; ++q)
+            acc = acc - (double)lv[q * kSlice + lane] * Dv[lc[q * kSlice + lane]];
           if (S_le[idx] & 128) a.p0[i].x = acc;
           S_t[idx] = acc;
           const double di = Dv[idx];
@@ -859,7 +871,7 @@ __global__ void __launch_bounds__(kThreads, 2) jcg_kernel(JcgArgs a) {
     } else if (!scalar_block) {
       // Resident variant.  The warp's first two slices start streaming
       // before phase A.
-      pipe.begin(a.soff);
+      pipe.begin((const VT *)sv_store);
       // Phase A: the 3-term update of the block's rows, d(in+1) written
       // over d(in-1); then the new d of the halo nodes from their owners'
       // exported records (same expression, same bits).
@@ -901,14 +913,15 @@ __global__ void __launch_bounds__(kThreads, 2) jcg_kernel(JcgArgs a) {
       }
       __syncthreads();
       // Phase B: the SpMV from shared memory, slot order as in pjac.
-      bool ok = pipe.run(a.soff, [&](int sl, const unsigned short *lc, const double *lv) {
+      bool ok = pipe.run((const VT *)sv_store, [&](int sl, const unsigned short *lc, const VT *lv) {
         const int i = sl * kSlice + lane, idx = i - r0;
         if (i < n) {
           const unsigned le = S_le[idx];
           const int len = (int)(le & 127u);
           double acc = 0.0;
 #pragma unroll 4
-          for (int q = 0; q < len; ++q) acc = acc - lv[q * kSlice + lane] * Sdn[lc[q * kSlice + lane]];
+          for (int q = 0; q < len; ++q)
+            acc = acc - (double)lv[q * kSlice + lane] * Sdn[lc[q * kSlice + lane]];
           const double dn = Sdn[idx];
           if (le & 128u) st_p4(pn + i, acc, dn, Sd[idx], 0.0);
           S_t[idx] = acc;
@@ -957,7 +970,7 @@ __global__ void __launch_bounds__(kThreads, 2) jcg_kernel(JcgArgs a) {
         double cc = usol[i];
         for (int k = 0; k < len; ++k) {
           int idx = base + k * kSlice;
-          cc = cc - a.soff[idx] * usol[a.col[idx]];
+          cc = cc - (double)sv_store[idx] * usol[a.col[idx]];
         }
         double wk2 = (a.rhs[i] - cc) / wv;
         pr += wk2 * wk2;
@@ -992,7 +1005,7 @@ __global__ void __launch_bounds__(kThreads, 2) jcg_kernel(JcgArgs a) {
     g->adapt = L.adapt; g->q1 = L.q1; g->chg_ier = L.chg_ier;
     g->in = fin;
     g->halt = h;
-    if (a.defer_drift) *a.drift_pending = 1;
+    if (a.defer_drift == 1) *a.drift_pending = 1;
     a.flags->numitr = fin;
     a.flags->ier = (h == 2) ? 13 : 0;
     a.flags->zeta = L.rparm1;
@@ -1128,7 +1141,8 @@ int jcg_setup_grid(adc_ctx *c, const JcgHostSell *h) {
     size_t smem = jcg_smem_bytes(c->itmax, true, rows_max, halo_max, wmax);
     int per_sm = 0;
     if (fits && smem <= 200 * 1024) {
-      const void *fn = (const void *)jcg_kernel<1>;
+      const void *fn = f32_spmv(c) ? (const void *)jcg_kernel<1, float>
+                                                  : (const void *)jcg_kernel<1, double>;
       ADC_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
       ADC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kThreads, smem));
     }
@@ -1153,7 +1167,7 @@ int jcg_setup_grid(adc_ctx *c, const JcgHostSell *h) {
       return ADC_OK;
     }
   }
-  const void *fn = (const void *)jcg_kernel<0>;
+  const void *fn = (const void *)jcg_kernel<0, double>;
   size_t smem = jcg_smem_bytes(c->itmax, false, 0, 0, 1);
   ADC_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int per_sm = 0;
@@ -1183,6 +1197,7 @@ int launch_jcg_impl(adc_ctx *c, int eta_update, int do_peror, int run_init, int 
   a.rlen = c->rlen;
   a.offd = c->offd;
   a.soff = c->soff;
+  a.soff32 = c->soff32;
   a.diag = c->diag;
   a.rhs = c->gwce_lv;
   a.u = c->etas;
@@ -1219,7 +1234,11 @@ int launch_jcg_impl(adc_ctx *c, int eta_update, int do_peror, int run_init, int 
     c->launches++;
   }
   void *args[] = {&a};
-  const void *fn = c->jcg_res ? (const void *)jcg_kernel<1> : (const void *)jcg_kernel<0>;
+  // the FP32 matrix copy exists only for the resident variant of the mixed mode
+  const bool vt32 = c->jcg_res && f32_spmv(c) && c->soff32;
+  const void *fn = !c->jcg_res ? (const void *)jcg_kernel<0, double>
+                   : vt32      ? (const void *)jcg_kernel<1, float>
+                               : (const void *)jcg_kernel<1, double>;
   ADC_CUDA(cudaLaunchCooperativeKernel(fn, dim3(c->jcg_grid), dim3(kThreads), args, c->jcg_smem,
                                        c->stream));
   c->launches++;
@@ -1227,6 +1246,9 @@ int launch_jcg_impl(adc_ctx *c, int eta_update, int do_peror, int run_init, int 
 }
 
 // The time-step solve defers the COEF drift to the next GWCE (k_lhs_drift).
-int launch_jcg(adc_ctx *c, int eta_update) { return launch_jcg_impl(c, eta_update, 0, 1, 1); }
+int launch_jcg(adc_ctx *c, int eta_update) {
+  // a mode with FP32 parts keeps no bitwise COEF history, so the drift is dropped
+  return launch_jcg_impl(c, eta_update, 0, 1, any_f32(c) ? 2 : 1);
+}
 
 }  // namespace adc

@@ -14,65 +14,95 @@
 
 namespace adc {
 
+template <class R>
 __global__ void k_mom_elem(adc_ctx c) {
-  __shared__ double sh[kThreads / 32][32 * 6];
+  __shared__ R sh[kThreads / 32][32 * 6];
   const int e0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31);
   if (e0 >= c.ne) return;
   const int nvalid = min(32, c.ne - e0);
   int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= c.ne) e = c.ne - 1;   // idle lanes recompute the last element; not stored
   const adc_params_t &p = c.p;
-  const double DT = p.dt;
-  const double THIRD = 1.0 / 3.0, GO2 = p.g / 2.0;
+  const R DT = R(p.dt);
+  const R THIRD = R(R(1.0)) / R(R(3.0)), GO2 = R(p.g) / R(R(2.0));
   const bool met = p.nws != 0;
   int n1 = c.nm[3 * e], n2 = c.nm[3 * e + 1], n3 = c.nm[3 * e + 2];
   int NCEle = c.nodecode[n1] * c.nodecode[n2] * c.nodecode[n3] * c.noff[e];
-  double U1N1 = c.uu1[n1], U1N2 = c.uu1[n2], U1N3 = c.uu1[n3];
-  double V1N1 = c.vv1[n1], V1N2 = c.vv1[n2], V1N3 = c.vv1[n3];
-  double H1N1 = c.h1[n1], H1N2 = c.h1[n2], H1N3 = c.h1[n3];
-  double AreaIE2 = c.areas[e];
-  double AreaIE = 0.5 * AreaIE2;
-  double FDX1 = c.fdx[3 * e], FDX2 = c.fdx[3 * e + 1], FDX3 = c.fdx[3 * e + 2];
-  double FDY1 = c.fdy[3 * e], FDY2 = c.fdy[3 * e + 1], FDY3 = c.fdy[3 * e + 2];
-  double U1Avg = THIRD * (U1N1 + U1N2 + U1N3);
-  double V1Avg = THIRD * (V1N1 + V1N2 + V1N3);
-  double DU1DXA = (U1N1 * FDX1 + U1N2 * FDX2 + U1N3 * FDX3) * 0.5;
-  double DU1DYA = (U1N1 * FDY1 + U1N2 * FDY2 + U1N3 * FDY3) * 0.5;
-  double DV1DXA = (V1N1 * FDX1 + V1N2 * FDX2 + V1N3 * FDX3) * 0.5;
-  double DV1DYA = (V1N1 * FDY1 + V1N2 * FDY2 + V1N3 * FDY3) * 0.5;
-  double EVMEle = THIRD * (c.evm[n1] + c.evm[n2] + c.evm[n3]);
-  double al = c.alphal[e];
-  double B11 = al * c.eta1[n1], B21 = al * c.eta2[n1];
-  double B12 = al * c.eta1[n2], B22 = al * c.eta2[n2];
-  double B13 = al * c.eta1[n3], B23 = al * c.eta2[n3];
+  R U1N1 = c.uu1[n1], U1N2 = c.uu1[n2], U1N3 = c.uu1[n3];
+  R V1N1 = c.vv1[n1], V1N2 = c.vv1[n2], V1N3 = c.vv1[n3];
+  R H1N1 = c.h1[n1], H1N2 = c.h1[n2], H1N3 = c.h1[n3];
+  R AreaIE2 = c.areas[e];
+  R AreaIE = R(0.5) * AreaIE2;
+  R FDX1 = c.fdx[3 * e], FDX2 = c.fdx[3 * e + 1], FDX3 = c.fdx[3 * e + 2];
+  R FDY1 = c.fdy[3 * e], FDY2 = c.fdy[3 * e + 1], FDY3 = c.fdy[3 * e + 2];
+  R U1Avg = THIRD * (U1N1 + U1N2 + U1N3);
+  R V1Avg = THIRD * (V1N1 + V1N2 + V1N3);
+  R DU1DXA = (U1N1 * FDX1 + U1N2 * FDX2 + U1N3 * FDX3) * R(0.5);
+  R DU1DYA = (U1N1 * FDY1 + U1N2 * FDY2 + U1N3 * FDY3) * R(0.5);
+  R DV1DXA = (V1N1 * FDX1 + V1N2 * FDX2 + V1N3 * FDX3) * R(0.5);
+  R DV1DYA = (V1N1 * FDY1 + V1N2 * FDY2 + V1N3 * FDY3) * R(0.5);
+  R EVMEle = THIRD * (c.evm[n1] + c.evm[n2] + c.evm[n3]);
+  R al = c.alphal[e];
+  R B11 = al * c.eta1[n1], B21 = al * c.eta2[n1];
+  R B12 = al * c.eta1[n2], B22 = al * c.eta2[n2];
+  R B13 = al * c.eta1[n3], B23 = al * c.eta2[n3];
   if (met) {
-    B11 = B11 + c.pr1[n1]; B21 = B21 + c.pr2[n1];
-    B12 = B12 + c.pr1[n2]; B22 = B22 + c.pr2[n2];
-    B13 = B13 + c.pr1[n3]; B23 = B23 + c.pr2[n3];
+    if constexpr (sizeof(R) == 4) {
+      // only gradients of B are used: FP32 carries the pressure's deviation
+      // from the background, not the ~10 m total
+      const double pb = p.prbckgrnd_mh2o;
+      B11 = B11 + R(c.pr1[n1] - pb); B21 = B21 + R(c.pr2[n1] - pb);
+      B12 = B12 + R(c.pr1[n2] - pb); B22 = B22 + R(c.pr2[n2] - pb);
+      B13 = B13 + R(c.pr1[n3] - pb); B23 = B23 + R(c.pr2[n3] - pb);
+    } else {
+      B11 = B11 + c.pr1[n1]; B21 = B21 + c.pr2[n1];
+      B12 = B12 + c.pr1[n2]; B22 = B22 + c.pr2[n2];
+      B13 = B13 + c.pr1[n3]; B23 = B23 + c.pr2[n3];
+    }
   }
-  double DBTPDX1A = B11 * FDX1 + B12 * FDX2 + B13 * FDX3;
-  double DBTPDX2A = B21 * FDX1 + B22 * FDX2 + B23 * FDX3;
-  double DBTPDY1A = B11 * FDY1 + B12 * FDY2 + B13 * FDY3;
-  double DBTPDY2A = B21 * FDY1 + B22 * FDY2 + B23 * FDY3;
-  double DBTPDXA = 0.5 * (DBTPDX1A + DBTPDX2A);   // Cfac1 = Cfac2 = 1
-  double DBTPDYA = 0.5 * (DBTPDY1A + DBTPDY2A);
-  double ADVX = U1Avg * DU1DXA + V1Avg * DU1DYA;
-  double ADVY = U1Avg * DV1DXA + V1Avg * DV1DYA;
-  double DU1DX = DU1DXA / AreaIE, DU1DY = DU1DYA / AreaIE;
-  double DV1DX = DV1DXA / AreaIE, DV1DY = DV1DYA / AreaIE;
-  double EH1 = EVMEle * H1N1, EH2 = EVMEle * H1N2, EH3 = EVMEle * H1N3;
-  double nc = (double)NCEle;
-  double fct = nc * DT;
-  double ax = -p.ifnlct * ADVX - GO2 * DBTPDXA - 0.0;
-  double ay = -p.ifnlct * ADVY - GO2 * DBTPDYA - 0.0;
-  double o[6];
-  o[0] = fct * (ax - (1.5 * ((EH1 * DU1DX) * FDX1 + (EH1 * DU1DY) * FDY1)) / H1N1);
-  o[1] = fct * (ax - (1.5 * ((EH2 * DU1DX) * FDX2 + (EH2 * DU1DY) * FDY2)) / H1N2);
-  o[2] = fct * (ax - (1.5 * ((EH3 * DU1DX) * FDX3 + (EH3 * DU1DY) * FDY3)) / H1N3);
-  o[3] = fct * (ay - (1.5 * ((EH1 * DV1DX) * FDX1 + (EH1 * DV1DY) * FDY1)) / H1N1);
-  o[4] = fct * (ay - (1.5 * ((EH2 * DV1DX) * FDX2 + (EH2 * DV1DY) * FDY2)) / H1N2);
-  o[5] = fct * (ay - (1.5 * ((EH3 * DV1DX) * FDX3 + (EH3 * DV1DY) * FDY3)) / H1N3);
-  warp_store_k<6>(c.ebuf + 6 * (size_t)e0, o, nvalid, sh[threadIdx.x >> 5]);
+  R DBTPDX1A, DBTPDX2A, DBTPDY1A, DBTPDY2A;
+  if constexpr (sizeof(R) == 4) {
+    // barotropic-pressure gradients cancel metre-sized nodal values: FP64,
+    // then narrowed
+    const double *fx = c.fdx + 3 * e, *fy = c.fdy + 3 * e;
+    const double ald = c.alphal[e];
+    double b11 = ald * c.eta1[n1], b21 = ald * c.eta2[n1];
+    double b12 = ald * c.eta1[n2], b22 = ald * c.eta2[n2];
+    double b13 = ald * c.eta1[n3], b23 = ald * c.eta2[n3];
+    if (met) {
+      b11 += c.pr1[n1]; b21 += c.pr2[n1];
+      b12 += c.pr1[n2]; b22 += c.pr2[n2];
+      b13 += c.pr1[n3]; b23 += c.pr2[n3];
+    }
+    DBTPDX1A = R(b11 * fx[0] + b12 * fx[1] + b13 * fx[2]);
+    DBTPDX2A = R(b21 * fx[0] + b22 * fx[1] + b23 * fx[2]);
+    DBTPDY1A = R(b11 * fy[0] + b12 * fy[1] + b13 * fy[2]);
+    DBTPDY2A = R(b21 * fy[0] + b22 * fy[1] + b23 * fy[2]);
+  } else {
+    DBTPDX1A = B11 * FDX1 + B12 * FDX2 + B13 * FDX3;
+    DBTPDX2A = B21 * FDX1 + B22 * FDX2 + B23 * FDX3;
+    DBTPDY1A = B11 * FDY1 + B12 * FDY2 + B13 * FDY3;
+    DBTPDY2A = B21 * FDY1 + B22 * FDY2 + B23 * FDY3;
+  }
+  R DBTPDXA = R(0.5) * (DBTPDX1A + DBTPDX2A);   // Cfac1 = Cfac2 = 1
+  R DBTPDYA = R(0.5) * (DBTPDY1A + DBTPDY2A);
+  R ADVX = U1Avg * DU1DXA + V1Avg * DU1DYA;
+  R ADVY = U1Avg * DV1DXA + V1Avg * DV1DYA;
+  R DU1DX = DU1DXA / AreaIE, DU1DY = DU1DYA / AreaIE;
+  R DV1DX = DV1DXA / AreaIE, DV1DY = DV1DYA / AreaIE;
+  R EH1 = EVMEle * H1N1, EH2 = EVMEle * H1N2, EH3 = EVMEle * H1N3;
+  R nc = (R)NCEle;
+  R fct = nc * DT;
+  R ax = -p.ifnlct * ADVX - GO2 * DBTPDXA - R(0.0);
+  R ay = -p.ifnlct * ADVY - GO2 * DBTPDYA - R(0.0);
+  R o[6];
+  o[0] = fct * (ax - (R(1.5) * ((EH1 * DU1DX) * FDX1 + (EH1 * DU1DY) * FDY1)) / H1N1);
+  o[1] = fct * (ax - (R(1.5) * ((EH2 * DU1DX) * FDX2 + (EH2 * DU1DY) * FDY2)) / H1N2);
+  o[2] = fct * (ax - (R(1.5) * ((EH3 * DU1DX) * FDX3 + (EH3 * DU1DY) * FDY3)) / H1N3);
+  o[3] = fct * (ay - (R(1.5) * ((EH1 * DV1DX) * FDX1 + (EH1 * DV1DY) * FDY1)) / H1N1);
+  o[4] = fct * (ay - (R(1.5) * ((EH2 * DV1DX) * FDX2 + (EH2 * DV1DY) * FDY2)) / H1N2);
+  o[5] = fct * (ay - (R(1.5) * ((EH3 * DV1DX) * FDX3 + (EH3 * DV1DY) * FDY3)) / H1N3);
+  warp_store_k<6>(reinterpret_cast<R *>(c.ebuf) + 6 * (size_t)e0, o, nvalid, sh[threadIdx.x >> 5]);
 }
 
 // gfortran's inline NORM2 for TKM(:,i) (scaled sum of squares starting
@@ -95,32 +125,35 @@ __device__ double norm2_3(const double *x) {
   return scale * sqrt(result);
 }
 
+template <class R>
 __global__ void k_mom_node(adc_ctx c) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= c.np) return;
   const adc_params_t &p = c.p;
   const double DTO2 = p.dt / 2.0;
-  double mx = 0.0, my = 0.0;
+  const R *eb = reinterpret_cast<const R *>(c.ebuf);
+  R mxr = R(0.0), myr = R(0.0);
   const int q0 = c.n2e_ptr[i], q1 = c.n2e_ptr[i + 1];
   for (int qc = q0; qc < q1; qc += kGatherChunk) {
     int ek[kGatherChunk];
-    double xa[kGatherChunk], xb[kGatherChunk];
+    R xa[kGatherChunk], xb[kGatherChunk];
 #pragma unroll
     for (int k = 0; k < kGatherChunk; ++k) if (qc + k < q1) ek[k] = c.n2e[qc + k];
 #pragma unroll
     for (int k = 0; k < kGatherChunk; ++k)
       if (qc + k < q1) {
         int e = ek[k] / 3, kk = ek[k] - 3 * e;
-        xa[k] = c.ebuf[6 * (size_t)e + kk];
-        xb[k] = c.ebuf[6 * (size_t)e + 3 + kk];
+        xa[k] = eb[6 * (size_t)e + kk];
+        xb[k] = eb[6 * (size_t)e + 3 + kk];
       }
 #pragma unroll
     for (int k = 0; k < kGatherChunk; ++k)
       if (qc + k < q1) {
-        mx = mx + xa[k];
-        my = my + xb[k];
+        mxr = mxr + xa[k];
+        myr = myr + xb[k];
       }
   }
+  double mx = (double)mxr, my = (double)myr;
   int NCI = c.nodecode[i];
   double ta = c.totalarea[i];
   if (ta != 0.0) {
@@ -189,10 +222,20 @@ __global__ void k_mom_node(adc_ctx c) {
 }
 
 int launch_momentum(adc_ctx *c) {
-  k_mom_elem<<<nblk(c->ne), kThreads, 0, c->stream>>>(*c);
-  k_mom_node<<<nblk(c->np), kThreads, 0, c->stream>>>(*c);
+  if (f32_momentum(c)) {   // FP32 element terms and their gather
+    k_mom_elem<float><<<nblk(c->ne), kThreads, 0, c->stream>>>(*c);
+    k_mom_node<float><<<nblk(c->np), kThreads, 0, c->stream>>>(*c);
+  } else {
+    k_mom_elem<double><<<nblk(c->ne), kThreads, 0, c->stream>>>(*c);
+    k_mom_node<double><<<nblk(c->np), kThreads, 0, c->stream>>>(*c);
+  }
   c->launches += 2;
   return ADC_OK;
 }
+
+template __global__ void k_mom_elem<double>(adc_ctx);
+template __global__ void k_mom_elem<float>(adc_ctx);
+template __global__ void k_mom_node<double>(adc_ctx);
+template __global__ void k_mom_node<float>(adc_ctx);
 
 }  // namespace adc

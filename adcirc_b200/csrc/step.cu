@@ -37,12 +37,12 @@ __global__ void k_apply_met(adc_ctx c);
 __global__ void k_lhs_begin(Flags *f, int *words);
 __global__ void k_lhs_drift(adc_ctx c, const int *apply);
 __global__ void k_lhs_drift_flush(int *words);
-__global__ void k_lhs_elem(adc_ctx c, const int *rebuild);
-__global__ void k_lhs_gather(adc_ctx c, const int *rebuild);
+template <class R> __global__ void k_lhs_elem(adc_ctx c, const int *rebuild);
+template <class R> __global__ void k_lhs_gather(adc_ctx c, const int *rebuild);
 __global__ void k_lhs_ep(adc_ctx c, const int *rebuild, int nparts);
 __global__ void k_lhs_bc(adc_ctx c, const int *rebuild);
-__global__ void k_rhs_elem(adc_ctx c);
-__global__ void k_rhs_gather(adc_ctx c);
+template <class R> __global__ void k_rhs_elem(adc_ctx c);
+template <class R> __global__ void k_rhs_gather(adc_ctx c);
 __global__ void k_eta_bc(adc_ctx c, const adc_step_t *steps, const Flags *flags);
 __global__ void k_obc_rhs(adc_ctx c);
 
@@ -56,6 +56,7 @@ __global__ void k_step_end(Flags *f, int *numitr_log, int cap) {
 static int *rebuild_flag(adc_ctx *c) { return (int *)(c->flags + 1); }
 
 int launch_met_vortex(adc_ctx *c);
+int launch_warm_start(adc_ctx *c);
 
 int launch_shift_friction(adc_ctx *c) {
   k_shift_friction<<<nblk(c->np), kThreads, 0, c->stream>>>(*c, c->steps, c->flags);
@@ -74,8 +75,13 @@ int launch_gwce_lhs(adc_ctx *c) {
   k_lhs_begin<<<1, 1, 0, c->stream>>>(c->flags, rb);
   int nb = nblk(c->np);
   k_lhs_drift<<<nb, kThreads, 0, c->stream>>>(*c, rb + 2);
-  k_lhs_elem<<<nblk(c->ne), kThreads, 0, c->stream>>>(*c, rb);
-  k_lhs_gather<<<nb, kThreads, 0, c->stream>>>(*c, rb);
+  if (f32_assembly(c)) {   // FP32 element assembly
+    k_lhs_elem<float><<<nblk(c->ne), kThreads, 0, c->stream>>>(*c, rb);
+    k_lhs_gather<float><<<nb, kThreads, 0, c->stream>>>(*c, rb);
+  } else {
+    k_lhs_elem<double><<<nblk(c->ne), kThreads, 0, c->stream>>>(*c, rb);
+    k_lhs_gather<double><<<nb, kThreads, 0, c->stream>>>(*c, rb);
+  }
   k_lhs_ep<<<1, 1024, 0, c->stream>>>(*c, rb, nb);
   k_lhs_bc<<<nblk((long long)c->np + c->n_obc), kThreads, 0, c->stream>>>(*c, rb);
   c->launches += 6;
@@ -83,8 +89,13 @@ int launch_gwce_lhs(adc_ctx *c) {
 }
 
 int launch_gwce_rhs(adc_ctx *c) {
-  k_rhs_elem<<<nblk(c->ne), kThreads, 0, c->stream>>>(*c);
-  k_rhs_gather<<<nblk(c->np), kThreads, 0, c->stream>>>(*c);
+  if (f32_assembly(c)) {
+    k_rhs_elem<float><<<nblk(c->ne), kThreads, 0, c->stream>>>(*c);
+    k_rhs_gather<float><<<nblk(c->np), kThreads, 0, c->stream>>>(*c);
+  } else {
+    k_rhs_elem<double><<<nblk(c->ne), kThreads, 0, c->stream>>>(*c);
+    k_rhs_gather<double><<<nblk(c->np), kThreads, 0, c->stream>>>(*c);
+  }
   c->launches += 2;
   if (c->neta > 0) {
     k_eta_bc<<<nblk(c->neta), kThreads, 0, c->stream>>>(*c, c->steps, c->flags);
@@ -105,6 +116,7 @@ static int enqueue_step(adc_ctx *c, bool timed) {
   if (timed) cudaEventRecord(c->ev[1], c->stream);
   if ((rc = launch_gwce_lhs(c))) return rc;
   if ((rc = launch_gwce_rhs(c))) return rc;
+  if ((rc = launch_warm_start(c))) return rc;
   if (timed) cudaEventRecord(c->ev[2], c->stream);
   if ((rc = launch_jcg(c, 1))) return rc;
   if (timed) cudaEventRecord(c->ev[3], c->stream);
@@ -401,7 +413,7 @@ static void free_ctx(adc_ctx *c) {
       (void **)&c->ebuf2, (void **)&c->red, (void **)&c->ev_cnt, (void **)&c->ev_a,
       (void **)&c->ev_b, (void **)&c->ev_c, (void **)&c->ju1, (void **)&c->jp[0],
       (void **)&c->jp[1], (void **)&c->jw, (void **)&c->jexp, (void **)&c->jlcol,
-      (void **)&c->jhalo_ptr, (void **)&c->jhalo_ids, (void **)&c->soff, (void **)&c->jpart, (void **)&c->jtri,
+      (void **)&c->jhalo_ptr, (void **)&c->jhalo_ids, (void **)&c->soff32, (void **)&c->etas_prev, (void **)&c->warm, (void **)&c->soff, (void **)&c->jpart, (void **)&c->jtri,
       (void **)&c->itp, (void **)&c->bar, (void **)&c->jlines, (void **)&c->flags, (void **)&c->steps,
       (void **)&c->numitr_log, (void **)&c->met_wsx, (void **)&c->met_wsy,
       (void **)&c->met_pr, (void **)&c->vfix, (void **)&c->vstate};
@@ -422,7 +434,10 @@ static int bind_impl(const adc_params_t *p, const adc_arrays_t *a, int prec, adc
   if (a->np <= 0 || a->ne <= 0 || a->mnei < 2 || a->neta < 0 || a->nbfr < 0) {
     set_error("invalid sizes"); return ADC_ERR_ARG;
   }
-  if (prec != ADC_PREC_FP64 && prec != ADC_PREC_MIXED) { set_error("bad precision mode"); return ADC_ERR_ARG; }
+  if (prec & ~(ADC_PREC_MIXED | ADC_WARM_START | ADC_F32_ASSEMBLY | ADC_F32_SPMV | ADC_F32_MOMENTUM)) {
+    set_error("bad precision mode %d", prec);
+    return ADC_ERR_ARG;
+  }
   if (p->itmax < 0 || p->dt <= 0.0) { set_error("invalid parameters"); return ADC_ERR_ARG; }
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
@@ -513,9 +528,16 @@ static int bind_impl(const adc_params_t *p, const adc_arrays_t *a, int prec, adc
   for (int **q : node_i32) B(dalloc(q, np));
   B(dalloc(&c->noff, ne)); B(dalloc(&c->noffold, ne)); B(dalloc(&c->ncele, ne));
   B(dalloc(&c->offd, std::max(nnz_pad, 1))); B(dalloc(&c->soff, std::max(nnz_pad, 1)));
+  if (f32_spmv(c)) B(dalloc(&c->soff32, std::max(nnz_pad, 1)));
   B(dalloc(&c->obccoef, (size_t)std::max(c->n_obc, 1)));
   B(dalloc(&c->ebuf, 9 * (size_t)ne)); B(dalloc(&c->ebuf2, 3 * (size_t)ne));
-  B(dalloc(&c->red, nblk(np) + 64));
+  B(dalloc(&c->red, 2 * (size_t)nblk(np) + 64));
+  if (c->prec & ADC_WARM_START) {
+    B(dalloc(&c->etas_prev, npad));
+    ADC_CUDA(cudaMemset(c->etas_prev, 0, npad * sizeof(double)));
+    B(dalloc(&c->warm, 1));
+    ADC_CUDA(cudaMemset(c->warm, 0, sizeof(WarmState)));
+  }
   c->ev_blocks = (ne + 255) / 256;
   B(dalloc(&c->ev_cnt, c->ev_blocks));
   B(dalloc(&c->ev_a, (size_t)c->ev_blocks * 256)); B(dalloc(&c->ev_b, (size_t)c->ev_blocks * 256));
@@ -622,6 +644,7 @@ int adc_gwce_new(adc_ctx *c, const adc_step_t *s, adc_stepout_t *out) {
   TRY(set_single_step(c, s));
   TRY(launch_gwce_lhs(c));
   TRY(launch_gwce_rhs(c));
+  TRY(launch_warm_start(c));
   TRY(launch_jcg(c, 1));
   ADC_CUDA(cudaGetLastError());
   Flags f;

@@ -35,6 +35,14 @@ extern "C" {
 /* precision modes for adc_gpu_bind */
 #define ADC_PREC_FP64 0       /* every kernel in FP64, reference arithmetic */
 #define ADC_PREC_MIXED 1      /* FP32 assembly/SpMV/momentum, FP64 reductions */
+#define ADC_WARM_START 2      /* flag OR'ed into the mode: extrapolated JCG initial
+                                 guess with fallback to the reference guess */
+/* Single FP32 components (flags OR'ed into the mode; ADC_PREC_MIXED is all
+ * three).  CG dot products, norms, the stopping test, the eta update and
+ * the state stay FP64 in every mode. */
+#define ADC_F32_ASSEMBLY 4    /* GWCE LHS and RHS element terms and their gathers */
+#define ADC_F32_SPMV 8        /* the JCG matrix the iterations stream (FP64 products) */
+#define ADC_F32_MOMENTUM 16   /* momentum element terms and their gather */
 
 /* Model parameters (fort.15 values and derived switches). */
 typedef struct {
@@ -181,7 +189,8 @@ void adc_jcg_noalloc(const int *n, const int *ndim, const int *maxnz, int *jcoef
 typedef struct adc_ctx adc_ctx;
 
 /* Binds the module arrays once after ADCIRC_Init (adcirc.F:113-411) and
- * uploads them.  prec is ADC_PREC_FP64 or ADC_PREC_MIXED. */
+ * uploads them.  prec is ADC_PREC_FP64 or an OR of ADC_PREC_MIXED,
+ * ADC_F32_* and ADC_WARM_START. */
 int adc_gpu_bind(const adc_params_t *p, const adc_arrays_t *a, int prec, adc_ctx **out);
 int adc_gpu_free(adc_ctx *ctx);
 
@@ -228,6 +237,12 @@ int adc_set_met(adc_ctx *ctx, const double *wsx2, const double *wsy2, const doub
  * increase give ADC_ERR_ARG.  A step past the last fix sets the step status
  * to ADC_ERR_ARG (the reference terminates there). */
 int adc_set_vortex(adc_ctx *ctx, const adc_vortex_t *vortex);
+
+/* No reference counterpart (the reference always starts JCG from ETAS as
+ * GWCE_New leaves it, gwce.F:2002-2004).  With ADC_WARM_START in the bind
+ * mode, counts of the steps that started from the extrapolated guess and of
+ * those that fell back to the reference guess. */
+int adc_warm_start_stats(adc_ctx *ctx, long long *used, long long *fallback);
 
 /* Device time of the phases of the last adc_timestep/adc_run (ms). */
 int adc_phase_times(adc_ctx *ctx, double *ms_shift, double *ms_gwce, double *ms_jcg,
