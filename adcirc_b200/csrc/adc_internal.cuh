@@ -167,6 +167,8 @@ struct adc_ctx {
   // graph
   cudaGraphExec_t graph;
   int graph_ok;
+  cudaGraphExec_t graph1;   // one timed step (adc_timestep), phase events inside
+  int graph1_ok, graph1_launches;
   int graph_launches;    // kernel launches per replayed step
   cudaEvent_t run_ev[2];
   double last_run_ms;
@@ -193,6 +195,14 @@ int launch_gwce_rhs(adc_ctx *c);
 int launch_jcg(adc_ctx *c, int eta_update);
 int launch_wetdry(adc_ctx *c);
 int launch_momentum(adc_ctx *c);
+
+// Drops the captured step graphs (after a change they would not see).
+inline void drop_graphs(adc_ctx *c) {
+  if (c->graph_ok) cudaGraphExecDestroy(c->graph);
+  if (c->graph1_ok) cudaGraphExecDestroy(c->graph1);
+  c->graph_ok = 0;
+  c->graph1_ok = 0;
+}
 
 // Which parts run in FP32 (ADC_PREC_MIXED selects all of them).
 inline bool f32_assembly(const adc_ctx *c) { return c->prec & (ADC_PREC_MIXED | ADC_F32_ASSEMBLY); }

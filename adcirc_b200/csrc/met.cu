@@ -178,9 +178,6 @@ extern "C" int adc_set_vortex(adc_ctx *c, const adc_vortex_t *v) {
   c->vpar = *v;
   c->vpar.fix = nullptr;
   c->vortex_on = 1;
-  if (c->graph_ok) {   // replayed steps must include the forcing
-    cudaGraphExecDestroy(c->graph);
-    c->graph_ok = 0;
-  }
+  drop_graphs(c);   // replayed steps must include the forcing
   return ADC_OK;
 }

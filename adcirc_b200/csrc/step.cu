@@ -2,6 +2,8 @@
 // graph replay, host synchronisation and the ITPACK jcg drop-in.
 #include "adc_internal.cuh"
 
+#include <cstdio>
+
 #include <cfloat>
 #include <cmath>
 #include <cstdarg>
@@ -111,19 +113,19 @@ int launch_gwce_rhs(adc_ctx *c) {
 // The whole 2DDI step (TIMESTEP order), without host synchronisation.
 static int enqueue_step(adc_ctx *c, bool timed) {
   int rc;
-  if (timed) cudaEventRecord(c->ev[0], c->stream);
+  if (timed) cudaEventRecordWithFlags(c->ev[0], c->stream, cudaEventRecordExternal);
   if ((rc = launch_shift_friction(c))) return rc;
-  if (timed) cudaEventRecord(c->ev[1], c->stream);
+  if (timed) cudaEventRecordWithFlags(c->ev[1], c->stream, cudaEventRecordExternal);
   if ((rc = launch_gwce_lhs(c))) return rc;
   if ((rc = launch_gwce_rhs(c))) return rc;
   if ((rc = launch_warm_start(c))) return rc;
-  if (timed) cudaEventRecord(c->ev[2], c->stream);
+  if (timed) cudaEventRecordWithFlags(c->ev[2], c->stream, cudaEventRecordExternal);
   if ((rc = launch_jcg(c, 1))) return rc;
-  if (timed) cudaEventRecord(c->ev[3], c->stream);
+  if (timed) cudaEventRecordWithFlags(c->ev[3], c->stream, cudaEventRecordExternal);
   if ((rc = launch_wetdry(c))) return rc;
-  if (timed) cudaEventRecord(c->ev[4], c->stream);
+  if (timed) cudaEventRecordWithFlags(c->ev[4], c->stream, cudaEventRecordExternal);
   if ((rc = launch_momentum(c))) return rc;
-  if (timed) cudaEventRecord(c->ev[5], c->stream);
+  if (timed) cudaEventRecordWithFlags(c->ev[5], c->stream, cudaEventRecordExternal);
   return ADC_OK;
 }
 
@@ -419,7 +421,7 @@ static void free_ctx(adc_ctx *c) {
       (void **)&c->met_pr, (void **)&c->vfix, (void **)&c->vstate};
   for (void **p : ptrs)
     if (*p) { cudaFree(*p); *p = nullptr; }
-  if (c->graph_ok) cudaGraphExecDestroy(c->graph);
+  drop_graphs(c);
   for (auto &e : c->ev)
     if (e) cudaEventDestroy(e);
   for (auto &e : c->run_ev)
@@ -601,12 +603,45 @@ static void fill_out(const Flags &f, adc_stepout_t *out) {
   out->cme = f.cme;
 }
 
+// The step's scalars and a zero cursor, in stream order (the host copies
+// are pageable, so both are consumed before the calls return).
 static int set_single_step(adc_ctx *c, const adc_step_t *s) {
   if (!s) { set_error("null step"); return ADC_ERR_ARG; }
   ADC_CUDA(cudaMemcpyAsync(c->steps, s, sizeof(adc_step_t), cudaMemcpyHostToDevice, c->stream));
   int zero = 0;
   ADC_CUDA(cudaMemcpyAsync(&c->flags->cursor, &zero, sizeof(int), cudaMemcpyHostToDevice, c->stream));
-  ADC_CUDA(cudaStreamSynchronize(c->stream));
+  return ADC_OK;
+}
+
+// One timed step.  Without host-supplied met forcing it replays a captured
+// graph of the step (phase events included), so the per-step call pays no
+// per-kernel launch cost.
+static int run_single_step(adc_ctx *c) {
+  if (c->met_pending) return enqueue_step(c, true);
+  if (!c->graph1_ok) {
+    cudaGraph_t g = nullptr;
+    int64_t l0 = c->launches;
+    cudaError_t e = cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal);
+    int rc = ADC_OK;
+    if (e == cudaSuccess) {
+      rc = enqueue_step(c, true);
+      cudaError_t e2 = cudaStreamEndCapture(c->stream, &g);
+      if (e2 != cudaSuccess) e = e2;
+    }
+    c->graph1_launches = (int)(c->launches - l0);
+    c->launches = l0;
+    if (e == cudaSuccess && rc == ADC_OK && g) {
+      e = cudaGraphInstantiate(&c->graph1, g, 0);
+      c->graph1_ok = (e == cudaSuccess);
+    }
+    if (g) cudaGraphDestroy(g);
+    if (!c->graph1_ok)
+      fprintf(stderr, "adcgpu: single-step graph not used (%s, rc %d)\n", cudaGetErrorString(e), rc);
+    cudaGetLastError();
+  }
+  if (!c->graph1_ok) return enqueue_step(c, true);
+  ADC_CUDA(cudaGraphLaunch(c->graph1, c->stream));
+  c->launches += c->graph1_launches;
   return ADC_OK;
 }
 
@@ -676,7 +711,7 @@ int adc_momentum(adc_ctx *c, const adc_step_t *s) {
 int adc_timestep(adc_ctx *c, const adc_step_t *s, adc_stepout_t *out) {
   if (!c) return ADC_ERR_ARG;
   TRY(set_single_step(c, s));
-  TRY(enqueue_step(c, true));
+  TRY(run_single_step(c));
   c->met_pending = 0;
   ADC_CUDA(cudaGetLastError());
   Flags f;
@@ -694,14 +729,14 @@ int adc_run(adc_ctx *c, int nsteps, const adc_step_t *steps, int *numitr, adc_st
     c->steps = nullptr;
     TRY(dalloc(&c->steps, nsteps));
     c->steps_cap = nsteps;
-    if (c->graph_ok) { cudaGraphExecDestroy(c->graph); c->graph_ok = 0; }
+    drop_graphs(c);
   }
   if (nsteps > c->numitr_cap) {
     cudaFree(c->numitr_log);
     c->numitr_log = nullptr;
     TRY(dalloc(&c->numitr_log, nsteps));
     c->numitr_cap = nsteps;
-    if (c->graph_ok) { cudaGraphExecDestroy(c->graph); c->graph_ok = 0; }
+    drop_graphs(c);
   }
   ADC_CUDA(cudaMemcpyAsync(c->steps, steps, nsteps * sizeof(adc_step_t), cudaMemcpyHostToDevice, c->stream));
   int zero = 0;

@@ -115,15 +115,21 @@ class ClockSampler:
                 "samples": len(self.samples)}
 
 
-def jcg_bytes(nnz_o: int, npn: int, iters: float) -> float:
-    """Algorithmic HBM bytes of one JCG solve (persistent kernel).
+def jcg_bytes(nnz_o: int, npn: int, iters: float, vbytes: int = 8) -> float:
+    """Algorithmic HBM bytes of one JCG solve (persistent kernel), counted
+    as a streaming implementation would move them.
 
-    Per off-diagonal slot: 8 B value + 4 B column per SpMV pass; the scaling
-    pass reads value+column and writes the scaled and the drifted values.
-    Per row: see the phase list in jcg.cu (prologue 64+44+24 B, 68 B per
-    iteration, epilogue 60 B).
+    Per off-diagonal slot: the scaling pass, which also forms d0, reads the
+    FP64 value + column and writes the scaled value (vbytes: 8, or 4 for the
+    FP32 matrix copy); each later SpMV pass (dtwd0, one per iteration) reads
+    value + 4 B column.
+    Per row: prologue 64+44+24 B, 68 B per iteration (own record 32, u and
+    u1 16, row length 4, writes 32+8 minus the neighbours' records counted
+    once), epilogue 60 B.
     """
-    return nnz_o * (28.0 + 12.0 + 12.0 * iters) + npn * (64.0 + 44.0 + 24.0 + 68.0 * iters + 60.0)
+    slot = vbytes + 4.0
+    return (nnz_o * (12.0 + vbytes + slot * (1.0 + iters)) +
+            npn * (64.0 + 44.0 + 24.0 + 68.0 * iters + 60.0))
 
 
 def make_case(name: str):
@@ -179,6 +185,48 @@ def bench_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+PATHS = {
+    # name: (bind mode, description)
+    "plain": (0, "plain FP64 (reference arithmetic)"),
+    "chosen": (8 | 16, "FP32 SpMV matrix + FP32 momentum element terms, FP64 assembly, "
+                       "dot products, norms, stopping test and state"),
+    "mixed": (1, "FP32 GWCE assembly + SpMV matrix + momentum, FP64 reductions and state"),
+}
+
+
+def _timed(gpu, it, W, K, dist):
+    """W untimed steps, then K steps replayed as one graph, device-timed."""
+    import torch
+    if W > 0:
+        gpu.run(it, W)
+        it += W
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    l0 = gpu.launches()
+    numitr, _ = gpu.run(it, K)
+    torch.cuda.synchronize()
+    it += K
+    ms = gpu.last_run_ms()
+    if dist:
+        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    return it, ms, np.asarray(numitr), gpu.launches() - l0
+
+
+def _accuracy(a, ref):
+    """max |d eta|, RMS |d u| and wet/dry mismatches of state `a` against `ref`."""
+    d = np.abs(a["eta2"] - ref["eta2"])
+    both = (a["nodecode"] == 1) & (ref["nodecode"] == 1)
+    mm = a["nodecode"] != ref["nodecode"]
+    du = np.sqrt(np.mean((a["uu2"] - ref["uu2"]) ** 2 + (a["vv2"] - ref["vv2"]) ** 2))
+    return {"max_deta_m": float(d.max()),
+            "max_deta_both_wet_m": float(d[both].max()) if both.any() else 0.0,
+            "p99_deta_m": float(np.percentile(d, 99)),
+            "rms_du_ms": float(du), "wetdry_mismatch": int(mm.sum())}
+
+
 def bench_gpu(args, rank, world, dist):
     import torch
     from adcirc_b200 import build, model, _lib
@@ -188,75 +236,92 @@ def bench_gpu(args, rank, world, dist):
     case = make_case(args.case)
     cpu_case = case.clone() if (rank == 0 and world == 1 and not args.no_cpu) else None
     dt = case.params["dt"]
-    prec = _lib.ADC_PREC_MIXED if args.prec == "mixed" else _lib.ADC_PREC_FP64
-    gpu = model.GpuModel(case, prec=prec)
-    it = 1
     W, K = args.warmup, args.steps
-    if W > 0:
-        gpu.run(it, W)
-        it += W
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    l0 = gpu.launches()
+    names = ["chosen", "plain"] + ([] if args.no_mixed else ["mixed"])
+    cases = {n: case.clone() for n in names}
+    models = {n: model.GpuModel(cases[n], prec=PATHS[n][0]) for n in names}
+    its = {n: 1 for n in names}
+    res = {}
     with ClockSampler(local) as clk:
-        numitr, last = gpu.run(it, K)
-    torch.cuda.synchronize()
-    it += K
-    ms = gpu.last_run_ms()
-    launches = gpu.launches() - l0
-    if dist:
-        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = world * sim_days_per_hour(K, dt, ms / 1000.0)
-    # per-phase device times and JCG roofline (CUDA events on the library stream)
+        for n in names:
+            its[n], ms, numitr, launches = _timed(models[n], its[n], W, K, dist)
+            res[n] = {"value": world * sim_days_per_hour(K, dt, ms / 1000.0), "ms_per_step": ms / K,
+                      "jcg_iters_per_step": float(numitr.mean()), "gpu_launches": int(launches),
+                      "mode": PATHS[n][0], "arithmetic": PATHS[n][1]}
+    gpu = models["chosen"]
+    # per-phase device times and the JCG roofline of the chosen path
     n_ph = 20
     ph = {"shift": 0.0, "gwce": 0.0, "jcg": 0.0, "wetdry": 0.0, "momentum": 0.0}
     iters = []
-    for k in range(n_ph):
-        o = gpu.step(it)
-        it += 1
-        iters.append(o.numitr)
-        for kk, vv in gpu.phase_times().items():
-            ph[kk] += vv / n_ph
+    for n in names:   # every path advances the same steps
+        for k in range(n_ph):
+            o = models[n].step(its[n] + k)
+            if n == "chosen":
+                iters.append(o.numitr)
+                for kk, vv in gpu.phase_times().items():
+                    ph[kk] += vv / n_ph
+        its[n] += n_ph
     # e2e through the per-step public call (host round trip every step)
     K2 = min(K, args.e2e_steps)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for k in range(K2):
-        gpu.step(it)
-        it += 1
+        gpu.step(its["chosen"] + k)
     el = time.perf_counter() - t0
+    for n in names:
+        if n != "chosen":
+            models[n].run(its[n], K2)
+        its[n] += K2
     if dist:
         t = torch.tensor([el], dtype=torch.float64, device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         el = float(t.item())
     e2e = world * sim_days_per_hour(K2, dt, el)
+    # accuracy of the FP32 paths against the FP64 path at hourly outputs
+    acc = {n: [] for n in names if n != "plain"}
+    hours = []
+    spd = int(round(3600.0 / dt))
+    for h in range(1, args.accuracy_hours + 1):
+        target = h * spd + 1          # next step to run once hour h is complete
+        if target <= its["plain"]:
+            continue
+        for n in names:
+            models[n].run(its[n], target - its[n])
+            its[n] = target
+            models[n].sync_to_host()
+        hours.append(h)
+        for n in acc:
+            acc[n].append(_accuracy(cases[n].arrays, cases["plain"].arrays))
     a = case.arrays
     nnz_o = int((a["nneigh"] - 1).sum())
     npn = case.sizes["np"]
     mean_it = float(np.mean(iters))
     peak, peak_kind = _peaks()
-    achieved = jcg_bytes(nnz_o, npn, mean_it) / (ph["jcg"] / 1000.0) / 1e9 if ph["jcg"] > 0 else 0.0
+    achieved = (jcg_bytes(nnz_o, npn, mean_it, vbytes=4) / (ph["jcg"] / 1000.0) / 1e9
+                if ph["jcg"] > 0 else 0.0)
+    worst = {n: {k: max(x[k] for x in v) for k in v[0]} if v else None for n, v in acc.items()}
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
-        "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64" if prec == _lib.ADC_PREC_FP64 else "f32/f64", "data": "synthetic",
+        "metric": METRIC, "value": res["chosen"]["value"], "unit": UNIT, "n_gpus": world,
+        "steps": K, "warmup": W, "ms_per_step": res["chosen"]["ms_per_step"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64+f32", "data": "synthetic",
         "config": {"workload": f"{args.case}: {npn} nodes, {case.sizes['ne']} elements, dt {dt} s, "
-                               f"M2+K1 tides, {forcing(case)}, wet/dry on, "
-                               f"{'plain FP64 JCG' if prec == 0 else 'mixed FP32/FP64'}",
+                               f"M2+K1 tides, {forcing(case)}, wet/dry on",
+                   "path": "chosen: " + PATHS["chosen"][1],
                    "nodes": npn, "elements": case.sizes["ne"], "parallelism": f"replicas x{world}",
                    "l2": "resident state ~0.35 GB > 126 MB L2 (no flush)",
                    "first_step": 1 + W},
-        "jcg_iters_per_step": float(np.mean(numitr)),
+        "speedup_vs_plain_fp64": res["chosen"]["value"] / res["plain"]["value"],
+        "paths": res,
+        "accuracy_vs_fp64": {"hours": hours, "worst": worst, "per_hour": acc},
+        "jcg_iters_per_step": res["chosen"]["jcg_iters_per_step"],
         "phase_ms": ph,
         "roofline": {"bound": "hbm", "kernel": "jcg_kernel", "achieved": achieved, "peak": peak,
                      "unit": "GB/s", "frac": achieved / peak, "traffic": None,
                      "peak_kind": peak_kind, "iters_per_launch": mean_it},
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": 44, "d2h_bytes_per_step": 56,
                 "steps": K2, "api": "adc_timestep per step"},
-        "gpu_launches": int(launches),
+        "gpu_launches": res["chosen"]["gpu_launches"],
         "clocks": clk.summary(),
     }
     if cpu_case is not None:
@@ -264,7 +329,8 @@ def bench_gpu(args, rank, world, dist):
         line["cpu_baseline"] = {"value": sim_days_per_hour(n, dt, el_c), "unit": UNIT, "cores": 1,
                                 "kind": "port",
                                 "sample": f"{n} time steps of the same mesh from cold start ({el_c:.1f} s)"}
-    gpu.close()
+    for m in models.values():
+        m.close()
     if rank == 0:
         print(json.dumps(line), flush=True)
 
@@ -276,7 +342,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=200)
     ap.add_argument("--impl", default="adcgpu", choices=["adcgpu", "reference"])
     ap.add_argument("--case", default="surge", choices=["surge", "channel"])
-    ap.add_argument("--prec", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--accuracy-hours", type=int, default=3,
+                    help="hourly outputs at which the FP32 paths are compared with FP64")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the all-FP32-assembly path")
     ap.add_argument("--e2e-steps", type=int, default=500)
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--no-cpu", action="store_true")
