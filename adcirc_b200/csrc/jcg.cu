@@ -87,35 +87,60 @@ struct JcgArgs {
 __device__ __forceinline__ double vld(const double *p) { return *(const volatile double *)p; }
 
 // ---------------------------------------------------------------- barrier
-// Contention-free flag barrier.  Row block b owns two 128-byte lines:
-// arrive[b] = {generation, three partial sums} and release[b] =
-// {generation}.  The scalar block (last block of the grid) polls the
-// arrival lines with all its threads, does the serial work of the phase and
-// writes every release line.  No two blocks poll the same line and there
-// are no atomics.  Generations count barriers from 1 within a launch; the
-// lines are cleared before every launch.  Waits are bounded (clock64).
+// Contention-free flag barrier that carries its data.  Row block b owns two
+// 128-byte lines: arrive[b] holds its three partial sums, release[b] the
+// ITPACK record of the phase (c1..c4 and a packed word), each slot
+// double-buffered by the barrier generation's parity.  An empty slot holds
+// kEmpty, a signalling-NaN bit pattern that no arithmetic produces; the
+// writer fills the words, the reader polls until every word is filled,
+// keeps the values of that same read and empties the slot again.  One L2
+// round trip therefore both signals and delivers.  Every word is an aligned
+// 8-byte access (single-copy atomic) and no two blocks poll the same line;
+// the scalar block (the last block of the grid) polls all arrival lines,
+// runs the serial ITPACK step and writes every release line.  A slot is
+// refilled only two barriers later, after its reader has emptied it and
+// that has been ordered before the intervening barrier.  Waits are bounded.
+constexpr unsigned long long kEmpty = 0x7FF4DEADBEEF0001ull;
+
 struct alignas(128) ArriveLine {
-  unsigned gen;
-  unsigned pad_;
-  double part[3];
-  char fill_[128 - 32];
+  unsigned long long part[2][4];
+  char fill_[64];
 };
 struct alignas(128) ReleaseLine {
-  unsigned gen;
-  char fill_[124];
+  unsigned long long rec[2][5];
+  char fill_[48];
 };
 
-__device__ bool spin_eq(const unsigned *p, unsigned g, Flags *flags) {
-  const volatile unsigned *v = p;
-  long long t0 = clock64();
-  while (*v != g) {
+__device__ __forceinline__ unsigned long long dbits(double x) {
+  return (unsigned long long)__double_as_longlong(x);
+}
+__device__ __forceinline__ double bitsd(unsigned long long u) {
+  return __longlong_as_double((long long)u);
+}
+
+// Release/acquire fence at GPU scope: orders a block's results before the
+// barrier words it writes, and the words it polled before what it reads next.
+__device__ __forceinline__ void fence_gpu() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
+
+// Polls N words until all are filled; v receives them.  Bounded.
+template <int N>
+__device__ bool poll_full(volatile unsigned long long *p, unsigned long long (&v)[N],
+                          Flags *flags) {
+  const long long t0 = clock64();
+  for (;;) {
+    bool full = true;
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+      v[k] = p[k];
+      full = full && (v[k] != kEmpty);
+    }
+    if (full) return true;
     if (*(volatile int *)&flags->timeout) return false;
     if (clock64() - t0 > kSpinCycles) {
       atomicExch(&flags->timeout, 1);
       return false;
     }
   }
-  return true;
 }
 
 __device__ Rec read_rec(const Rec *r) {
@@ -132,48 +157,47 @@ __device__ Rec read_rec(const Rec *r) {
   return o;
 }
 
-// Row-block side: post (optionally) partials and the arrival, wait for the
-// release.  With `srec`, thread 0 also fetches the ITPACK record the
-// release publishes, for the whole block.  Returns false on timeout.
-__device__ bool row_arrive_wait(const JcgArgs &a, unsigned g, bool post, double p0, double p1,
-                                double p2, Rec *srec = nullptr) {
+// The record's integers in one word (never kEmpty: the top 16 bits are 0).
+__device__ __forceinline__ unsigned long long pack_rec(const Rec &r) {
+  return (unsigned long long)(unsigned)r.in | ((unsigned long long)(r.halt & 0xff) << 32) |
+         ((unsigned long long)(r.need_unorm & 0xff) << 40);
+}
+
+// Row-block side: post the block's partial sums, wait for the release and,
+// with `srec`, hand its ITPACK record to the whole block.  Returns false on
+// timeout.
+__device__ bool row_arrive_wait(const JcgArgs &a, unsigned g, double p0, double p1, double p2,
+                                Rec *srec = nullptr) {
   __shared__ int ok;
   __syncthreads();
   if (threadIdx.x == 0) {
-    ArriveLine *al = (ArriveLine *)a.arrive + blockIdx.x;
-    if (post) {
-      volatile double *vp = al->part;
-      vp[0] = p0;
-      vp[1] = p1;
-      vp[2] = p2;
+    const int par = g & 1;
+    fence_gpu();   // the block's results before its arrival
+    volatile unsigned long long *ap = ((ArriveLine *)a.arrive + blockIdx.x)->part[par];
+    ap[0] = dbits(p0);
+    ap[1] = dbits(p1);
+    ap[2] = dbits(p2);
+    volatile unsigned long long *rp = ((ReleaseLine *)a.release + blockIdx.x)->rec[par];
+    unsigned long long v[5];
+    ok = poll_full<5>(rp, v, a.flags) ? 1 : 0;
+    fence_gpu();
+    if (ok) {
+#pragma unroll
+      for (int k = 0; k < 5; ++k) rp[k] = kEmpty;
+      if (srec) {
+        srec->c1 = bitsd(v[0]);
+        srec->c2 = bitsd(v[1]);
+        srec->c3 = bitsd(v[2]);
+        srec->c4 = bitsd(v[3]);
+        srec->in = (int)(unsigned)(v[4] & 0xffffffffull);
+        srec->halt = (int)((v[4] >> 32) & 0xff);
+        srec->need_unorm = (int)((v[4] >> 40) & 0xff);
+        srec->pad_ = 0;
+      }
     }
-    __threadfence();
-    *(volatile unsigned *)&al->gen = g;
-    ok = spin_eq(&((ReleaseLine *)a.release + blockIdx.x)->gen, g, a.flags) ? 1 : 0;
-    __threadfence();
-    if (srec) *srec = read_rec(&a.itp->rec);
   }
   __syncthreads();
   return ok != 0;
-}
-
-// Scalar-block side: wait for every row block's arrival.
-__device__ bool scalar_gather(const JcgArgs &a, unsigned g) {
-  __shared__ int bad;
-  if (threadIdx.x == 0) bad = 0;
-  __syncthreads();
-  for (int b = threadIdx.x; b < a.nrb; b += blockDim.x)
-    if (!spin_eq(&((ArriveLine *)a.arrive + b)->gen, g, a.flags)) bad = 1;
-  __threadfence();
-  __syncthreads();
-  return bad == 0;
-}
-
-__device__ void scalar_release(const JcgArgs &a, unsigned g) {
-  __threadfence();
-  __syncthreads();
-  for (int b = threadIdx.x; b < a.nrb; b += blockDim.x)
-    *(volatile unsigned *)&((ReleaseLine *)a.release + b)->gen = g;
 }
 
 // Serial ITPACK state of one solve, held in registers of the scalar block's
@@ -435,42 +459,75 @@ __device__ void block_sum3(double &a, double &b, double &c) {
   __syncthreads();
 }
 
-// Reducing phase end.  Row blocks post their block sums of (p0, p1, p2)
-// and wait; the scalar block sums the posts in block order and runs
-// `serial(s0, s1, s2)` on its thread 0 before releasing.
+// Scalar-block side of a barrier: gather every row block's partials (in
+// block order, fixed tree), run `serial` on thread 0 (it fills *srec), and
+// release every row block with the record.  Returns false on timeout.
 template <class F>
-__device__ bool phase_reduce(const JcgArgs &a, bool scalar_block, unsigned &g, double p0,
-                             double p1, double p2, F serial, Rec *srec = nullptr) {
-  ++g;
-  if (!scalar_block) {
-    block_sum3(p0, p1, p2);
-    return row_arrive_wait(a, g, true, p0, p1, p2, srec);
-  }
-  if (!scalar_gather(a, g)) return false;
+__device__ bool scalar_phase(const JcgArgs &a, unsigned g, F serial, Rec *srec) {
+  __shared__ int bad;
+  const int par = g & 1;
+  if (threadIdx.x == 0) bad = 0;
+  __syncthreads();
   double s0 = 0.0, s1 = 0.0, s2 = 0.0;
   for (int b = threadIdx.x; b < a.nrb; b += blockDim.x) {
-    const volatile double *vp = ((ArriveLine *)a.arrive + b)->part;
-    s0 += vp[0];
-    s1 += vp[1];
-    s2 += vp[2];
+    volatile unsigned long long *ap = ((ArriveLine *)a.arrive + b)->part[par];
+    unsigned long long v[3];
+    if (!poll_full<3>(ap, v, a.flags)) {
+      bad = 1;
+      break;
+    }
+    s0 += bitsd(v[0]);
+    s1 += bitsd(v[1]);
+    s2 += bitsd(v[2]);
   }
+  fence_gpu();
+  __syncthreads();
+  if (bad) return false;
   block_sum3(s0, s1, s2);
-  if (threadIdx.x == 0) {
-    serial(s0, s1, s2);
-    if (srec) *srec = read_rec(&a.itp->rec);
+  if (threadIdx.x == 0) serial(s0, s1, s2);
+  __syncthreads();
+  unsigned long long w[5] = {dbits(srec->c1), dbits(srec->c2), dbits(srec->c3), dbits(srec->c4),
+                             pack_rec(*srec)};
+  fence_gpu();
+  for (int b = threadIdx.x; b < a.nrb; b += blockDim.x) {
+    volatile unsigned long long *rp = ((ReleaseLine *)a.release + b)->rec[par];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) rp[k] = w[k];
   }
-  scalar_release(a, g);
+  // empty the arrival slots off the critical path: they are refilled two
+  // barriers later, after this block's next release
+  for (int b = threadIdx.x; b < a.nrb; b += blockDim.x) {
+    volatile unsigned long long *ap = ((ArriveLine *)a.arrive + b)->part[par];
+    ap[0] = kEmpty;
+    ap[1] = kEmpty;
+    ap[2] = kEmpty;
+  }
   __syncthreads();
   return true;
 }
 
-__device__ bool phase_sync(const JcgArgs &a, bool scalar_block, unsigned &g) {
+// Reducing phase end.  Row blocks post their block sums of (p0, p1, p2)
+// and wait; the scalar block sums the posts in block order and runs
+// `serial(s0, s1, s2)`, which fills *srec, before releasing.
+template <class F>
+__device__ bool phase_reduce(const JcgArgs &a, bool scalar_block, unsigned &g, double p0,
+                             double p1, double p2, F serial, Rec *srec) {
   ++g;
-  if (!scalar_block) return row_arrive_wait(a, g, false, 0.0, 0.0, 0.0);
-  if (!scalar_gather(a, g)) return false;
-  scalar_release(a, g);
-  __syncthreads();
-  return true;
+  if (!scalar_block) {
+    block_sum3(p0, p1, p2);
+    return row_arrive_wait(a, g, p0, p1, p2, srec);
+  }
+  return scalar_phase(a, g, serial, srec);
+}
+
+// Plain barrier (no partials, no record).
+__device__ bool phase_sync(const JcgArgs &a, bool scalar_block, unsigned &g, Rec *scratch) {
+  ++g;
+  if (!scalar_block) return row_arrive_wait(a, g, 0.0, 0.0, 0.0);
+  return scalar_phase(a, g, [&](double, double, double) {
+    scratch->c1 = scratch->c2 = scratch->c3 = scratch->c4 = 0.0;
+    scratch->halt = scratch->need_unorm = scratch->in = 0;
+  }, scratch);
 }
 
 
@@ -501,11 +558,11 @@ struct SlicePipe {
       }
     }
   }
-  // Orders earlier generic writes of `vals` before the copies, then starts
-  // the warp's first two slices.
+  // Starts the warp's first two slices; with `fence`, first orders earlier
+  // generic writes of `vals` before the copies.
   template <class V>
-  __device__ void begin(const V *vals) {
-    if (lane == 0) fence_proxy_async_all();
+  __device__ void begin(const V *vals, bool fence) {
+    if (fence && lane == 0) fence_proxy_async_all();
     if (first < s1) issue(first, 0, vals);
     if (first + step < s1) issue(first + step, 1, vals);
   }
@@ -573,13 +630,16 @@ __global__ void __launch_bounds__(kThreads, 2) jcg_kernel(JcgArgs a) {
   double *S_dd = S_t + RB;
   unsigned char *S_le = (unsigned char *)(S_dd + 2 * VB);
   int2 *S_meta = (int2 *)(S_le + ((RB + 127) & ~127));
-  uint64_t *S_bar = (uint64_t *)(S_meta + ((RB / kSlice + 15) & ~15));
+  int *S_hid = (int *)(S_meta + ((RB / kSlice + 15) & ~15));   // the block's halo nodes
+  uint64_t *S_bar = (uint64_t *)(S_hid + ((a.halo_max + 31) & ~31));
   unsigned char *S_stage = (unsigned char *)(S_bar + 16);
+  const int nhalo = (kRes && !scalar_block) ? a.halo_ptr[blockIdx.x + 1] - a.halo_ptr[blockIdx.x] : 0;
   SlicePipe pipe{S_stage + (size_t)(2 * warp) * a.stage_bytes, &S_bar[2 * warp], S_meta, a.lcol,
                  a.flags, a.stage_bytes, s0, s1, s0 + warp, nwarps, lane, 0u};
   Rec *rec = &a.itp->rec;
   __shared__ ItpLocal L;              // used by the scalar block's thread 0 only
   __shared__ Rec s_rec;               // the record of the last reducing barrier
+  __shared__ Rec s_scr;               // record slot of the barriers that carry none
   unsigned gen = 0;                   // barrier generation within this launch
   if (scalar_block && threadIdx.x == 0) {
     const volatile Itp *g = a.itp;
@@ -606,7 +666,7 @@ __global__ void __launch_bounds__(kThreads, 2) jcg_kernel(JcgArgs a) {
         a.u1[i] = 0.0;
       }
     }
-    if (!phase_sync(a, scalar_block, gen)) return;
+    if (!phase_sync(a, scalar_block, gen, &s_scr)) return;
 
     // P1: scaled off-diagonals, the reference's unscal drift of the resident
     // matrix, and the initial pseudo-residual d0 = pjac(u') + rhs' - u'.
@@ -649,7 +709,7 @@ __global__ void __launch_bounds__(kThreads, 2) jcg_kernel(JcgArgs a) {
         a.diag[i] = winv_i * winv_i;
       }
     }
-    if (!phase_sync(a, scalar_block, gen)) return;
+    if (!phase_sync(a, scalar_block, gen, &s_scr)) return;
 
     // P2: dtwd0 = -A' d0 and the iteration-0 norms; the scalar block runs
     // chgcon for in = 0 (ip = 0: cme = 0) while the rows work.
@@ -690,26 +750,37 @@ __global__ void __launch_bounds__(kThreads, 2) jcg_kernel(JcgArgs a) {
     // and per halo node, w = 1/sqrt(diag) and u' (P1), then d0 (P2).
     double *Uv = S_dd, *Wv = S_dd + VB;
     if (!scalar_block) {
-      for (int idx = threadIdx.x; idx < rows; idx += blockDim.x) {
-        const int i = r0 + idx;
-        S_le[idx] = i < n ? (unsigned char)(a.rlen[i] | (a.exp[i] ? 128 : 0)) : 0;
+      // Everything the prologue needs from global memory is requested
+      // before any of it is stored, so the loads share one round trip: the
+      // slice table, the halo list, and per row its length, export bit and
+      // the diagonal, u and rhs of P0 (scal part 1: u' = u*sqrt(d),
+      // w = 1/sqrt(d), rhs' = rhs*w).
+      const int nsl = s1 - s0;
+      const int h0 = a.halo_ptr[blockIdx.x];
+      int2 mt = make_int2(0, 0);
+      if ((int)threadIdx.x < nsl) mt = make_int2(a.sl_ptr[s0 + threadIdx.x], a.sl_w[s0 + threadIdx.x]);
+      int hid[kHaloPre];
+#pragma unroll
+      for (int k = 0; k < kHaloPre; ++k) {
+        const int h = threadIdx.x + k * blockDim.x;
+        hid[k] = h < nhalo ? a.halo_ids[h0 + h] : 0;
       }
-      for (int k = threadIdx.x; k < s1 - s0; k += blockDim.x)
-        S_meta[k] = make_int2(a.sl_ptr[s0 + k], a.sl_w[s0 + k]);
-      if (threadIdx.x < 2 * nwarps) mbar_init(&S_bar[threadIdx.x], 1);
-      mbar_fence_init();
-      // P0: scal part 1 -- u' = u*sqrt(d), w = 1/sqrt(d), rhs' = rhs*w,
-      // eight rows per thread with their loads issued together.
       for (int base = threadIdx.x; base < rows; base += kRowUnroll * blockDim.x) {
         double dg[kRowUnroll], uu[kRowUnroll], rh[kRowUnroll];
+        int rl[kRowUnroll];
+        unsigned char ex[kRowUnroll];
 #pragma unroll
         for (int k = 0; k < kRowUnroll; ++k) {
           const int idx = base + k * blockDim.x, i = r0 + idx;
-          if (idx < rows && i < n) { dg[k] = a.diag[i]; uu[k] = a.u[i]; rh[k] = a.rhs[i]; }
+          if (idx < rows && i < n) {
+            dg[k] = a.diag[i]; uu[k] = a.u[i]; rh[k] = a.rhs[i];
+            rl[k] = a.rlen[i]; ex[k] = a.exp[i];
+          }
         }
 #pragma unroll
         for (int k = 0; k < kRowUnroll; ++k) {
           const int idx = base + k * blockDim.x, i = r0 + idx;
+          if (idx < rows) S_le[idx] = i < n ? (unsigned char)(rl[k] | (ex[k] ? 128 : 0)) : 0;
           if (idx < rows && i < n) {
             double work = sqrt(dg[k]);
             const double up = uu[k] * work;
@@ -724,15 +795,27 @@ __global__ void __launch_bounds__(kThreads, 2) jcg_kernel(JcgArgs a) {
           }
         }
       }
+      if ((int)threadIdx.x < nsl) S_meta[threadIdx.x] = mt;
+      for (int k = threadIdx.x + blockDim.x; k < nsl; k += blockDim.x)
+        S_meta[k] = make_int2(a.sl_ptr[s0 + k], a.sl_w[s0 + k]);
+#pragma unroll
+      for (int k = 0; k < kHaloPre; ++k) {
+        const int h = threadIdx.x + k * blockDim.x;
+        if (h < nhalo) S_hid[h] = hid[k];
+      }
+      for (int h = threadIdx.x + kHaloPre * blockDim.x; h < nhalo; h += blockDim.x)
+        S_hid[h] = a.halo_ids[h0 + h];
+      if (threadIdx.x < 2 * nwarps) mbar_init(&S_bar[threadIdx.x], 1);
+      mbar_fence_init();
     }
-    if (!phase_sync(a, scalar_block, gen)) return;
+    if (!phase_sync(a, scalar_block, gen, &s_scr)) return;
     // P1: scaled off-diagonals, the reference's unscal drift of the resident
     // matrix, and d0 = pjac(u') + rhs' - u' (kept in S_t until P2).
     if (!scalar_block) {
-      pipe.begin(a.offd);
-      const int h0 = a.halo_ptr[blockIdx.x], nh = a.halo_ptr[blockIdx.x + 1] - h0;
+      pipe.begin(a.offd, false);   // offd was last written by an earlier kernel
+      const int nh = nhalo;
       for (int h = threadIdx.x; h < nh; h += blockDim.x) {
-        const int j = a.halo_ids[h0 + h];
+        const int j = S_hid[h];
         Uv[RB + h] = a.u[j];
         Wv[RB + h] = a.w[j];
       }
@@ -762,17 +845,17 @@ __global__ void __launch_bounds__(kThreads, 2) jcg_kernel(JcgArgs a) {
       if (!ok) atomicExch(&a.flags->timeout, 1);
       fence_proxy_async_all();   // soff is read by bulk copies from here on
     }
-    if (!phase_sync(a, scalar_block, gen)) return;
+    if (!phase_sync(a, scalar_block, gen, &s_scr)) return;
     // P2: dtwd0 = -A' d0 and the iteration-0 norms.
     if (!scalar_block) {
-      pipe.begin((const VT *)sv_store);
+      pipe.begin((const VT *)sv_store, true);   // the scaled matrix was just written
       double *Dv = S_dd;
       for (int idx = threadIdx.x; idx < rows; idx += blockDim.x) {
         Dv[idx] = S_t[idx];
         S_dd[VB + idx] = 0.0;   // d(-1)
       }
-      const int h0 = a.halo_ptr[blockIdx.x], nh = a.halo_ptr[blockIdx.x + 1] - h0;
-      for (int h = threadIdx.x; h < nh; h += blockDim.x) Dv[RB + h] = a.p0[a.halo_ids[h0 + h]].y;
+      const int nh = nhalo;
+      for (int h = threadIdx.x; h < nh; h += blockDim.x) Dv[RB + h] = a.p0[S_hid[h]].y;
       __syncthreads();
       bool ok = pipe.run((const VT *)sv_store, [&](int sl, const unsigned short *lc, const VT *lv) {
         const int i = sl * kSlice + lane, idx = i - r0;
@@ -802,7 +885,7 @@ __global__ void __launch_bounds__(kThreads, 2) jcg_kernel(JcgArgs a) {
         if (L.itmax == 0) halt = 2;
         else parcon_d(&L, 0, st, c);
       }
-      volatile Rec *vr = rec;
+      Rec *vr = &s_rec;
       vr->c1 = c[0]; vr->c2 = c[1]; vr->c3 = c[2]; vr->c4 = c[3];
       vr->halt = halt;
       vr->need_unorm = !(L.q1 || ((1 > 5) && (1 % 5 != 0)));
@@ -871,17 +954,17 @@ __global__ void __launch_bounds__(kThreads, 2) jcg_kernel(JcgArgs a) {
     } else if (!scalar_block) {
       // Resident variant.  The warp's first two slices start streaming
       // before phase A.
-      pipe.begin((const VT *)sv_store);
+      pipe.begin((const VT *)sv_store, false);   // unchanged since P2's fence
       // Phase A: the 3-term update of the block's rows, d(in+1) written
       // over d(in-1); then the new d of the halo nodes from their owners'
       // exported records (same expression, same bits).
       double *Sd = S_dd + cur * VB, *Sdn = S_dd + (cur ^ 1) * VB;
-      const int h0 = a.halo_ptr[blockIdx.x], nh = a.halo_ptr[blockIdx.x + 1] - h0;
+      const int nh = nhalo;
       P4 hv[kHaloPre];   // the first halo records, loaded with the rows' vectors
 #pragma unroll
       for (int k = 0; k < kHaloPre; ++k) {
         const int h = threadIdx.x + k * blockDim.x;
-        if (h < nh) hv[k] = ld_p4(pc + a.halo_ids[h0 + h]);
+        if (h < nh) hv[k] = ld_p4(pc + S_hid[h]);
       }
       for (int base = threadIdx.x; base < rows; base += kRowUnroll * blockDim.x) {
         double ucv[kRowUnroll], unv[kRowUnroll];
@@ -908,7 +991,7 @@ __global__ void __launch_bounds__(kThreads, 2) jcg_kernel(JcgArgs a) {
         if (h < nh) Sdn[RB + h] = c1 * hv[k].x + c4 * hv[k].y + c3 * hv[k].z;
       }
       for (int h = threadIdx.x + kHaloPre * blockDim.x; h < nh; h += blockDim.x) {
-        const P4 o = ld_p4(pc + a.halo_ids[h0 + h]);
+        const P4 o = ld_p4(pc + S_hid[h]);
         Sdn[RB + h] = c1 * o.x + c4 * o.y + c3 * o.z;
       }
       __syncthreads();
@@ -943,7 +1026,7 @@ __global__ void __launch_bounds__(kThreads, 2) jcg_kernel(JcgArgs a) {
         else parcon_d(&L, m, st, c);
       }
       int mm = m + 1;
-      volatile Rec *vr = rec;
+      Rec *vr = &s_rec;
       vr->c1 = c[0]; vr->c2 = c[1]; vr->c3 = c[2]; vr->c4 = c[3];
       vr->halt = halt;
       vr->need_unorm = !(L.q1 || ((mm > 5) && (mm % 5 != 0)));
@@ -979,7 +1062,8 @@ __global__ void __launch_bounds__(kThreads, 2) jcg_kernel(JcgArgs a) {
     bool ok = phase_reduce(a, scalar_block, gen, pb, pr, 0.0, [&](double sb, double sr, double) {
       a.itp->dtnrm = sb;
       a.itp->unorm = sr;
-    });
+      s_scr = s_rec;
+    }, &s_scr);
     if (!ok) return;
   }
 
@@ -1015,9 +1099,9 @@ __global__ void __launch_bounds__(kThreads, 2) jcg_kernel(JcgArgs a) {
 
 // Per-solve ITPACK initialisation (echall, itpackv.F:1212-1255, plus the
 // zeta floor of jcg :223-232); q1 and rparm1 persist across solves.
-__global__ void jcg_clear_lines(unsigned *lines, int nwords) {
+__global__ void jcg_clear_lines(unsigned long long *lines, int nwords) {
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nwords; k += gridDim.x * blockDim.x)
-    lines[k] = 0u;
+    lines[k] = kEmpty;
 }
 
 __global__ void jcg_init_kernel(Itp *it, Bar *bar, int itmax) {
@@ -1054,8 +1138,8 @@ static size_t jcg_smem_bytes(int itmax, bool res, int rows_max, int halo_max, in
   size_t tri = round_up(2 * sizeof(double) * (itmax + 1), 128);
   if (!res) return tri;
   size_t rb = (size_t)rows_max, vb = rb + (size_t)halo_max;
-  size_t rowb = 8 * rb + 16 * vb + round_up(rb, 128) + 8 * round_up(rb / kSlice, 16) + 128 +
-                16 * jcg_stage_bytes(wmax);
+  size_t rowb = 8 * rb + 16 * vb + round_up(rb, 128) + 8 * round_up(rb / kSlice, 16) +
+                4 * round_up((size_t)halo_max, 32) + 128 + 16 * jcg_stage_bytes(wmax);
   return std::max(tri, rowb);
 }
 
@@ -1226,8 +1310,8 @@ int launch_jcg_impl(adc_ctx *c, int eta_update, int do_peror, int run_init, int 
   a.defer_drift = defer_drift;
   // the word after the step flags (allocated only by the time-step context)
   a.drift_pending = defer_drift ? (int *)(c->flags + 1) + 1 : nullptr;
-  int nwords = (int)(2 * 128 * (size_t)c->jcg_rows_blocks / 4);
-  jcg_clear_lines<<<8, 256, 0, c->stream>>>((unsigned *)c->jlines, nwords);
+  int nwords = (int)(2 * 128 * (size_t)c->jcg_rows_blocks / 8);
+  jcg_clear_lines<<<8, 256, 0, c->stream>>>((unsigned long long *)c->jlines, nwords);
   c->launches++;
   if (run_init) {
     jcg_init_kernel<<<1, 1, 0, c->stream>>>(c->itp, c->bar, c->itmax);
