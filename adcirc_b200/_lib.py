@@ -119,6 +119,8 @@ def load():
         "adc_sync_from_host": (C.c_int, [vp]),
         "adc_set_met": (C.c_int, [vp, dp_, dp_, dp_]),
         "adc_set_vortex": (C.c_int, [vp, C.POINTER(AdcVortex)]),
+        "adc_hotstart_write": (C.c_int, [vp, C.c_char_p]),
+        "adc_hotstart_read": (C.c_int, [vp, C.c_char_p]),
         "adc_warm_start_stats": (C.c_int, [vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
         "adc_phase_times": (C.c_int, [vp, dp_, dp_, dp_, dp_, dp_]),
         "adc_launch_count": (C.c_int64, [vp]),

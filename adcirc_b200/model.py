@@ -381,6 +381,12 @@ class GpuModel:
         except Exception:
             pass
 
+    def hotstart_write(self, path) -> None:
+        _check(self.lib.adc_hotstart_write(self.h, str(path).encode()), "adc_hotstart_write")
+
+    def hotstart_read(self, path) -> None:
+        _check(self.lib.adc_hotstart_read(self.h, str(path).encode()), "adc_hotstart_read")
+
     def step(self, it: int) -> AdcStepOut:
         s = self.case.schedule.step(it)
         out = AdcStepOut()

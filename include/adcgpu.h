@@ -238,6 +238,18 @@ int adc_set_met(adc_ctx *ctx, const double *wsx2, const double *wsy2, const doub
  * to ADC_ERR_ARG (the reference terminates there). */
 int adc_set_vortex(adc_ctx *ctx, const adc_vortex_t *vortex);
 
+/* Hotstart: the counterparts of the reference's fort.67/68 dump
+ * (write_output.F:4429-5582) and load (hstart.F:47-2048), in this
+ * library's own binary format.  The file holds every array and scalar the
+ * device step carries between steps (state, the GWCE matrix and EP, ITPACK's
+ * persistent scalars, a pending unscal drift, vortex and warm-start state),
+ * so a run resumed from it continues bit for bit.  adc_hotstart_read needs
+ * a context bound to the same mesh and mode (and, with a vortex, one on
+ * which adc_set_vortex was called); it returns ADC_ERR_ARG, with the
+ * reason in adc_last_error(), for any other file. */
+int adc_hotstart_write(adc_ctx *ctx, const char *path);
+int adc_hotstart_read(adc_ctx *ctx, const char *path);
+
 /* No reference counterpart (the reference always starts JCG from ETAS as
  * GWCE_New leaves it, gwce.F:2002-2004).  With ADC_WARM_START in the bind
  * mode, counts of the steps that started from the extrapolated guess and of

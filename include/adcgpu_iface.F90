@@ -45,9 +45,23 @@ module adcgpu_iface
       integer(c_int) :: n_w1_events, pad_
    end type
 
+   integer(c_int), parameter, public :: ADC_WARM_START = 2, ADC_F32_ASSEMBLY = 4, &
+                                        ADC_F32_SPMV = 8, ADC_F32_MOMENTUM = 16
+
+   type, bind(C), public :: adc_vortex_fix_t
+      real(c_double) :: time, x, y, cpress, vmax, rmw, tvx, tvy
+   end type
+
+   type, bind(C), public :: adc_vortex_t
+      integer(c_int) :: nfix, avg_minute, hemisphere, pad_
+      real(c_double) :: start_time, bladj, rho_air, wind_mult, drag_limit
+      type(c_ptr) :: fix
+   end type
+
    public :: adc_jcg, adc_dfault, adc_gpu_bind, adc_gpu_free, adc_shift_friction, &
              adc_gwce_new, adc_wetdry, adc_momentum, adc_timestep, adc_sync_to_host, &
-             adc_sync_from_host, adc_set_met
+             adc_sync_from_host, adc_set_met, adc_set_vortex, adc_hotstart_write, &
+             adc_hotstart_read
 
    interface
       ! drop-in for ITPACK jcg (itpackv.F:63): identical argument list
@@ -125,6 +139,27 @@ module adcgpu_iface
          import :: c_int, c_ptr, c_double
          type(c_ptr), value :: ctx
          real(c_double), intent(in) :: wsx2(*), wsy2(*), pr2(*)
+      end function
+
+      ! NWS = 8 vortex track (fix points in mesh coordinates; see adcgpu.h)
+      integer(c_int) function adc_set_vortex(ctx, v) bind(C, name="adc_set_vortex")
+         import :: c_int, c_ptr, adc_vortex_t
+         type(c_ptr), value :: ctx
+         type(adc_vortex_t), intent(in) :: v
+      end function
+
+      ! hotstart dump/load (write_output.F:4429-5582, hstart.F:47-2048);
+      ! path is a NUL-terminated character array (trim(name)//c_null_char)
+      integer(c_int) function adc_hotstart_write(ctx, path) bind(C, name="adc_hotstart_write")
+         import :: c_int, c_ptr, c_char
+         type(c_ptr), value :: ctx
+         character(kind=c_char), intent(in) :: path(*)
+      end function
+
+      integer(c_int) function adc_hotstart_read(ctx, path) bind(C, name="adc_hotstart_read")
+         import :: c_int, c_ptr, c_char
+         type(c_ptr), value :: ctx
+         character(kind=c_char), intent(in) :: path(*)
       end function
    end interface
 end module adcgpu_iface
