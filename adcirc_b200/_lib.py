@@ -119,6 +119,14 @@ def load():
         "adc_sync_from_host": (C.c_int, [vp]),
         "adc_set_met": (C.c_int, [vp, dp_, dp_, dp_]),
         "adc_set_vortex": (C.c_int, [vp, C.POINTER(AdcVortex)]),
+        "adc_fort14_dims": (C.c_int, [C.c_char_p, ip_]),
+        "adc_fort14_read": (C.c_int, [C.c_char_p, C.c_char_p, dp_, dp_, dp_, ip_, ip_, ip_, ip_, ip_, ip_]),
+        "adc_fort14_write": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int, C.c_int, dp_, dp_, dp_, ip_,
+                                       C.c_int, ip_, ip_, C.c_int, ip_, ip_, ip_]),
+        "adc_fort6x_header": (C.c_int, [C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p, C.c_int,
+                                        C.c_int, C.c_double, C.c_int, C.c_int]),
+        "adc_fort6x_append": (C.c_int, [C.c_char_p, C.c_double, C.c_int, C.c_int, dp_, dp_, ip_,
+                                        C.c_double]),
         "adc_hotstart_write": (C.c_int, [vp, C.c_char_p]),
         "adc_hotstart_read": (C.c_int, [vp, C.c_char_p]),
         "adc_warm_start_stats": (C.c_int, [vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),

@@ -238,6 +238,36 @@ int adc_set_met(adc_ctx *ctx, const double *wsx2, const double *wsy2, const doub
  * to ADC_ERR_ARG (the reference terminates there). */
 int adc_set_vortex(adc_ctx *ctx, const adc_vortex_t *vortex);
 
+/* ------------------------------------------------------------------ */
+/* ADCIRC text files at the path's edges (host only; no GPU needed).    */
+/* ------------------------------------------------------------------ */
+
+/* fort.14 mesh (read14, mesh.F:319-581).  dims = {NP, NE, NOPE, NETA,
+ * NBOU, NVEL}.  Node labels map to 1..NP in file order, as read14 does.
+ * Barrier (IBTYPE 3/4/5 families) and periodic (94) land segments return
+ * ADC_ERR_UNSUPPORTED. */
+int adc_fort14_dims(const char *path, int dims[6]);
+/* title receives up to 80 characters plus NUL; nm is NM(NE,3); nbdv (NETA)
+ * and nbvv (NVEL) are the concatenated segment node lists, segment
+ * lengths in nvdll (NOPE) and nvell (NBOU). */
+int adc_fort14_read(const char *path, char *title, double *x, double *y, double *dp, int *nm,
+                    int *nvdll, int *nbdv, int *nvell, int *ibtype, int *nbvv);
+/* Writes the same tables (every double to 17 significant digits). */
+int adc_fort14_write(const char *path, const char *title, int np, int ne, const double *x,
+                     const double *y, const double *dp, const int *nm, int nope, const int *nvdll,
+                     const int *nbdv, int nbou, const int *nvell, const int *ibtype,
+                     const int *nbvv);
+
+/* Full-domain ASCII output files fort.63 (irtype 1) and fort.64 (irtype 2):
+ * the header of header63/64 (globalio.F:1005-1085) and one record per call
+ * as writeFullFormat/storeOne/storeTwo write them (globalio.F:544-643,
+ * 802-930).  With nodecode, dry nodes get `alternate` (-99999 in the
+ * reference's elevation output). */
+int adc_fort6x_header(const char *path, const char *rundes, const char *runid, const char *agrid,
+                      int ndsets, int np, double dt_out, int nspool, int irtype);
+int adc_fort6x_append(const char *path, double timeloc, int it, int np, const double *v1,
+                      const double *v2, const int *nodecode, double alternate);
+
 /* Hotstart: the counterparts of the reference's fort.67/68 dump
  * (write_output.F:4429-5582) and load (hstart.F:47-2048), in this
  * library's own binary format.  The file holds every array and scalar the
