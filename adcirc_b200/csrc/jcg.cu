@@ -785,10 +785,9 @@ __global__ void __launch_bounds__(kThreads, 2) jcg_kernel(JcgArgs a) {
             double work = sqrt(dg[k]);
             const double up = uu[k] * work;
             double wv = 1.0 / work;
-            a.u[i] = up;
+            a.u1[i] = up;   // u' goes to u1: u keeps the raw guess until P2
             a.w[i] = wv;
             a.rhs[i] = rh[k] * wv;
-            a.u1[i] = 0.0;
             Uv[idx] = up;
             Wv[idx] = wv;
             if (need_u0) pu += up * up;
@@ -808,7 +807,10 @@ __global__ void __launch_bounds__(kThreads, 2) jcg_kernel(JcgArgs a) {
       if (threadIdx.x < 2 * nwarps) mbar_init(&S_bar[threadIdx.x], 1);
       mbar_fence_init();
     }
-    if (!phase_sync(a, scalar_block, gen, &s_scr)) return;
+    // No grid barrier after P0: P1 reads only this block's own P0 results,
+    // and forms the halo's u' and w itself from the raw u and diag, which
+    // no block overwrites before P2.
+    __syncthreads();
     // P1: scaled off-diagonals, the reference's unscal drift of the resident
     // matrix, and d0 = pjac(u') + rhs' - u' (kept in S_t until P2).
     if (!scalar_block) {
@@ -816,8 +818,9 @@ __global__ void __launch_bounds__(kThreads, 2) jcg_kernel(JcgArgs a) {
       const int nh = nhalo;
       for (int h = threadIdx.x; h < nh; h += blockDim.x) {
         const int j = S_hid[h];
-        Uv[RB + h] = a.u[j];
-        Wv[RB + h] = a.w[j];
+        double work = sqrt(a.diag[j]);   // the owner's P0 expressions
+        Uv[RB + h] = a.u[j] * work;
+        Wv[RB + h] = 1.0 / work;
       }
       __syncthreads();
       bool ok = pipe.run(a.offd, [&](int sl, const unsigned short *lc, const double *lv) {
@@ -838,7 +841,6 @@ __global__ void __launch_bounds__(kThreads, 2) jcg_kernel(JcgArgs a) {
           }
           const double d0 = acc - ui;
           if (S_le[idx] & 128) st_p4(a.p0 + i, 0.0, d0, 0.0, 0.0);
-          a.diag[i] = winv_i * winv_i;
           S_t[idx] = d0;
         }
       });
@@ -853,6 +855,13 @@ __global__ void __launch_bounds__(kThreads, 2) jcg_kernel(JcgArgs a) {
       for (int idx = threadIdx.x; idx < rows; idx += blockDim.x) {
         Dv[idx] = S_t[idx];
         S_dd[VB + idx] = 0.0;   // d(-1)
+        const int i = r0 + idx;
+        if (i < n) {
+          // every block has read the raw u and diag by now (the P1 barrier)
+          a.u[i] = 0.0;   // u(-1) of the recurrence
+          const double winv_i = 1.0 / a.w[i];
+          a.diag[i] = winv_i * winv_i;   // scal/unscal of the diagonal
+        }
       }
       const int nh = nhalo;
       for (int h = threadIdx.x; h < nh; h += blockDim.x) Dv[RB + h] = a.p0[S_hid[h]].y;
@@ -898,7 +907,8 @@ __global__ void __launch_bounds__(kThreads, 2) jcg_kernel(JcgArgs a) {
   // norms of iteration in+1.  P[in % 2][i] = (dtwd(in), d(in), d(in-1)) so
   // a neighbour's three values arrive in one 32-byte sector.
   P4 *P[2] = {a.p0, a.p1};
-  double *U[2] = {a.u, a.u1};
+  // u(in) and u(in-1): the resident prologue leaves u' in u1 and zeroes u
+  double *U[2] = {kRes ? a.u1 : a.u, kRes ? a.u : a.u1};
   int cur = 0;   // resident variant: S_dd half holding d(in)
   for (int in = 0; in < a.itmax; ++in) {
     r = s_rec;
