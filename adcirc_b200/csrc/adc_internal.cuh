@@ -204,6 +204,28 @@ inline void drop_graphs(adc_ctx *c) {
   c->graph1_ok = 0;
 }
 
+// Programmatic dependent launch.  Step kernels are launched so that the
+// next kernel's grid is set up while the previous one drains; each kernel
+// first waits (griddepcontrol.wait) until its predecessor has completed
+// and its memory is visible, so nothing runs early.
+__device__ __forceinline__ void griddep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
+template <typename... KArgs, typename... Args>
+inline void launch_k(void (*kernel)(KArgs...), dim3 grid, dim3 block, cudaStream_t stream,
+                     Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+}
+
 // Which parts run in FP32 (ADC_PREC_MIXED selects all of them).
 inline bool f32_assembly(const adc_ctx *c) { return c->prec & (ADC_PREC_MIXED | ADC_F32_ASSEMBLY); }
 inline bool f32_spmv(const adc_ctx *c) { return c->prec & (ADC_PREC_MIXED | ADC_F32_SPMV); }

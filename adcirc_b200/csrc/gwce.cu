@@ -16,6 +16,7 @@ namespace adc {
 // timestep.F:231-237 (IT==1 H init), :375-416 (time-level shift, zeroing),
 // nodalattr.F:2399-2413 (quadratic/linear/hybrid friction), :2700-2704.
 __global__ void k_shift_friction(adc_ctx c, const adc_step_t *steps, const Flags *flags) {
+  griddep_wait();
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= c.np) return;
   const adc_step_t st = steps[flags->cursor];
@@ -56,6 +57,7 @@ __global__ void k_shift_friction(adc_ctx c, const adc_step_t *steps, const Flags
 
 // Met forcing supplied by the host for this step (WSX2, WSY2, PR2).
 __global__ void k_apply_met(adc_ctx c) {
+  griddep_wait();
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= c.np) return;
   c.wsx2[i] = c.met_wsx[i];
@@ -69,6 +71,7 @@ __global__ void k_apply_met(adc_ctx c) {
 // unscal drift of COEF pending; words[2] says whether this step applies it
 // (only when COEF is kept, since a rebuild overwrites it).
 __global__ void k_lhs_begin(Flags *f, int *words) {
+  griddep_wait();
   int r = f->ncchange > 0;
   words[0] = r;
   words[2] = (!r && words[1]) ? 1 : 0;
@@ -82,6 +85,7 @@ __global__ void k_lhs_begin(Flags *f, int *words) {
 // 2458-2463) with the w = 1/sqrt(diag) that solve used, so COEF ends with
 // the same bits as if the solve had written it.
 __global__ void k_lhs_drift(adc_ctx c, const int *apply) {
+  griddep_wait();
   if (!*apply) return;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= c.np) return;
@@ -100,6 +104,7 @@ __global__ void k_lhs_drift(adc_ctx c, const int *apply) {
 // Single-thread helper: make a pending drift apply now (before COEF is
 // copied to the host).
 __global__ void k_lhs_drift_flush(int *words) {
+  griddep_wait();
   words[2] = words[1];
   words[1] = 0;
 }
@@ -107,6 +112,7 @@ __global__ void k_lhs_drift_flush(int *words) {
 // gwce.F:456-593: nine consistent-mass + gravity entries per element.
 template <class R>
 __global__ void k_lhs_elem(adc_ctx c, const int *rebuild) {
+  griddep_wait();
   if (!*rebuild) return;
   __shared__ R sh[kThreads / 32][32 * 9];
   const int e0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31);   // the warp's first element
@@ -146,6 +152,7 @@ __global__ void k_lhs_elem(adc_ctx c, const int *rebuild) {
 // sum(diag^2) for EP (gwce.F:646-650).
 template <class R>
 __global__ void k_lhs_gather(adc_ctx c, const int *rebuild) {
+  griddep_wait();
   if (!*rebuild) return;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   const R *eb = reinterpret_cast<const R *>(c.ebuf);
@@ -207,6 +214,7 @@ __global__ void k_lhs_gather(adc_ctx c, const int *rebuild) {
 }
 
 __global__ void k_lhs_ep(adc_ctx c, const int *rebuild, int nparts) {
+  griddep_wait();
   if (!*rebuild) return;
   __shared__ double sh[32];
   double s = 0.0;
@@ -226,6 +234,7 @@ __global__ void k_lhs_ep(adc_ctx c, const int *rebuild, int nparts) {
 // checks.  Thread t < NP handles row t; thread NP + q handles the q-th
 // (I, J) column entry.
 __global__ void k_lhs_bc(adc_ctx c, const int *rebuild) {
+  griddep_wait();
   if (!*rebuild) return;
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   const double EP = c.flags->ep;
@@ -261,6 +270,7 @@ __global__ void k_lhs_bc(adc_ctx c, const int *rebuild) {
 // gwce.F:1000-1617, one element, IM=0 branches.
 template <class R>
 __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 3 : 2) k_rhs_elem(adc_ctx c) {
+  griddep_wait();
   __shared__ R sh[kThreads / 32][32 * 3];
   const int e0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31);
   if (e0 >= c.ne) return;
@@ -399,6 +409,7 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 3 : 2) k_rhs_elem(adc_ct
 // GWCE_LV gather (element order) fused with gwce.F:1622-1631.
 template <class R>
 __global__ void k_rhs_gather(adc_ctx c) {
+  griddep_wait();
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= c.np) return;
   const R *eb = reinterpret_cast<const R *>(c.ebuf);
@@ -422,6 +433,7 @@ __global__ void k_rhs_gather(adc_ctx c) {
 
 // gwce.F:1638-1651 periodic elevation BC and :1846-1850 load-vector rows.
 __global__ void k_eta_bc(adc_ctx c, const adc_step_t *steps, const Flags *flags) {
+  griddep_wait();
   int I = blockIdx.x * blockDim.x + threadIdx.x;
   if (I >= c.neta) return;
   const adc_step_t st = steps[flags->cursor];
@@ -443,6 +455,7 @@ __global__ void k_eta_bc(adc_ctx c, const adc_step_t *steps, const Flags *flags)
 
 // gwce.F:1851-1854 column correction, per affected neighbour in (I, J) order.
 __global__ void k_obc_rhs(adc_ctx c) {
+  griddep_wait();
   int r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= c.n_obc_rhs_nodes) return;
   int nb = c.obc_rhs_node[r];

@@ -611,6 +611,7 @@ struct SlicePipe {
 // products still accumulate in FP64).
 template <int kRes, class VT>
 __global__ void __launch_bounds__(kThreads, 2) jcg_kernel(JcgArgs a) {
+  griddep_wait();
   VT *const sv_store = std::is_same<VT, float>::value ? (VT *)a.soff32 : (VT *)a.soff;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
   const bool scalar_block = (blockIdx.x == (unsigned)a.nrb);
@@ -1110,11 +1111,13 @@ __global__ void __launch_bounds__(kThreads, 2) jcg_kernel(JcgArgs a) {
 // Per-solve ITPACK initialisation (echall, itpackv.F:1212-1255, plus the
 // zeta floor of jcg :223-232); q1 and rparm1 persist across solves.
 __global__ void jcg_clear_lines(unsigned long long *lines, int nwords) {
+  griddep_wait();
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nwords; k += gridDim.x * blockDim.x)
     lines[k] = kEmpty;
 }
 
 __global__ void jcg_init_kernel(Itp *it, Bar *bar, int itmax) {
+  griddep_wait();
   bar->count = 0;
   it->zeta = it->rparm1;
   // cme keeps rparm(2) of the previous solve; chgcon(0) resets it to 0
@@ -1321,10 +1324,10 @@ int launch_jcg_impl(adc_ctx *c, int eta_update, int do_peror, int run_init, int 
   // the word after the step flags (allocated only by the time-step context)
   a.drift_pending = defer_drift ? (int *)(c->flags + 1) + 1 : nullptr;
   int nwords = (int)(2 * 128 * (size_t)c->jcg_rows_blocks / 8);
-  jcg_clear_lines<<<8, 256, 0, c->stream>>>((unsigned long long *)c->jlines, nwords);
+  launch_k(jcg_clear_lines, 8, 256, c->stream, (unsigned long long *)c->jlines, nwords);
   c->launches++;
   if (run_init) {
-    jcg_init_kernel<<<1, 1, 0, c->stream>>>(c->itp, c->bar, c->itmax);
+    launch_k(jcg_init_kernel, 1, 1, c->stream, c->itp, c->bar, c->itmax);
     c->launches++;
   }
   void *args[] = {&a};

@@ -29,6 +29,7 @@ constexpr double kRhoWat0 = 1000.0;            // constants.F90:49
 // HollandGet (nws08.F90:602-639).  The position is interpolated with the
 // WTRATIO left by the previous call, as the reference does.
 __global__ void k_vortex_state(adc_ctx c, const adc_step_t *steps, Flags *flags) {
+  griddep_wait();
   VortexState &v = *c.vstate;
   const adc_vortex_fix_t *f = c.vfix;
   const double timeloc = steps[flags->cursor].timeloc;
@@ -77,6 +78,7 @@ __global__ void k_vortex_state(adc_ctx c, const adc_step_t *steps, Flags *flags)
 // stress and pressure of wind.F:1172-1198 (capped Garratt drag,
 // wind.F:514-539; no directional reduction, canopy or ice).
 __global__ void k_vortex_nodes(adc_ctx c, const adc_step_t *steps, const Flags *flags) {
+  griddep_wait();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= c.np) return;
   const VortexState &v = *c.vstate;
@@ -122,8 +124,8 @@ __global__ void k_vortex_nodes(adc_ctx c, const adc_step_t *steps, const Flags *
 
 int launch_met_vortex(adc_ctx *c) {
   if (!c->vortex_on) return ADC_OK;
-  k_vortex_state<<<1, 1, 0, c->stream>>>(*c, c->steps, c->flags);
-  k_vortex_nodes<<<nblk(c->np), kThreads, 0, c->stream>>>(*c, c->steps, c->flags);
+  launch_k(k_vortex_state, 1, 1, c->stream, *c, c->steps, c->flags);
+  launch_k(k_vortex_nodes, nblk(c->np), kThreads, c->stream, *c, c->steps, c->flags);
   c->launches += 2;
   return ADC_OK;
 }

@@ -16,6 +16,7 @@ namespace adc {
 
 template <class R>
 __global__ void k_mom_elem(adc_ctx c) {
+  griddep_wait();
   __shared__ R sh[kThreads / 32][32 * 6];
   const int e0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31);
   if (e0 >= c.ne) return;
@@ -127,6 +128,7 @@ __device__ double norm2_3(const double *x) {
 
 template <class R>
 __global__ void k_mom_node(adc_ctx c) {
+  griddep_wait();
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= c.np) return;
   const adc_params_t &p = c.p;
@@ -223,11 +225,11 @@ __global__ void k_mom_node(adc_ctx c) {
 
 int launch_momentum(adc_ctx *c) {
   if (f32_momentum(c)) {   // FP32 element terms and their gather
-    k_mom_elem<float><<<nblk(c->ne), kThreads, 0, c->stream>>>(*c);
-    k_mom_node<float><<<nblk(c->np), kThreads, 0, c->stream>>>(*c);
+    launch_k(k_mom_elem<float>, nblk(c->ne), kThreads, c->stream, *c);
+    launch_k(k_mom_node<float>, nblk(c->np), kThreads, c->stream, *c);
   } else {
-    k_mom_elem<double><<<nblk(c->ne), kThreads, 0, c->stream>>>(*c);
-    k_mom_node<double><<<nblk(c->np), kThreads, 0, c->stream>>>(*c);
+    launch_k(k_mom_elem<double>, nblk(c->ne), kThreads, c->stream, *c);
+    launch_k(k_mom_node<double>, nblk(c->np), kThreads, c->stream, *c);
   }
   c->launches += 2;
   return ADC_OK;

@@ -49,6 +49,7 @@ __global__ void k_eta_bc(adc_ctx c, const adc_step_t *steps, const Flags *flags)
 __global__ void k_obc_rhs(adc_ctx c);
 
 __global__ void k_step_end(Flags *f, int *numitr_log, int cap) {
+  griddep_wait();
   int k = f->cursor;
   if (k < cap) numitr_log[k] = f->numitr;
   f->cursor = k + 1;
@@ -61,12 +62,12 @@ int launch_met_vortex(adc_ctx *c);
 int launch_warm_start(adc_ctx *c);
 
 int launch_shift_friction(adc_ctx *c) {
-  k_shift_friction<<<nblk(c->np), kThreads, 0, c->stream>>>(*c, c->steps, c->flags);
+  launch_k(k_shift_friction, nblk(c->np), kThreads, c->stream, *c, c->steps, c->flags);
   c->launches++;
   int rc = launch_met_vortex(c);
   if (rc) return rc;
   if (c->met_pending) {
-    k_apply_met<<<nblk(c->np), kThreads, 0, c->stream>>>(*c);
+    launch_k(k_apply_met, nblk(c->np), kThreads, c->stream, *c);
     c->launches++;
   }
   return ADC_OK;
@@ -74,36 +75,36 @@ int launch_shift_friction(adc_ctx *c) {
 
 int launch_gwce_lhs(adc_ctx *c) {
   int *rb = rebuild_flag(c);
-  k_lhs_begin<<<1, 1, 0, c->stream>>>(c->flags, rb);
+  launch_k(k_lhs_begin, 1, 1, c->stream, c->flags, rb);
   int nb = nblk(c->np);
-  k_lhs_drift<<<nb, kThreads, 0, c->stream>>>(*c, rb + 2);
+  launch_k(k_lhs_drift, nb, kThreads, c->stream, *c, rb + 2);
   if (f32_assembly(c)) {   // FP32 element assembly
-    k_lhs_elem<float><<<nblk(c->ne), kThreads, 0, c->stream>>>(*c, rb);
-    k_lhs_gather<float><<<nb, kThreads, 0, c->stream>>>(*c, rb);
+    launch_k(k_lhs_elem<float>, nblk(c->ne), kThreads, c->stream, *c, rb);
+    launch_k(k_lhs_gather<float>, nb, kThreads, c->stream, *c, rb);
   } else {
-    k_lhs_elem<double><<<nblk(c->ne), kThreads, 0, c->stream>>>(*c, rb);
-    k_lhs_gather<double><<<nb, kThreads, 0, c->stream>>>(*c, rb);
+    launch_k(k_lhs_elem<double>, nblk(c->ne), kThreads, c->stream, *c, rb);
+    launch_k(k_lhs_gather<double>, nb, kThreads, c->stream, *c, rb);
   }
-  k_lhs_ep<<<1, 1024, 0, c->stream>>>(*c, rb, nb);
-  k_lhs_bc<<<nblk((long long)c->np + c->n_obc), kThreads, 0, c->stream>>>(*c, rb);
+  launch_k(k_lhs_ep, 1, 1024, c->stream, *c, rb, nb);
+  launch_k(k_lhs_bc, nblk((long long)c->np + c->n_obc), kThreads, c->stream, *c, rb);
   c->launches += 6;
   return ADC_OK;
 }
 
 int launch_gwce_rhs(adc_ctx *c) {
   if (f32_assembly(c)) {
-    k_rhs_elem<float><<<nblk(c->ne), kThreads, 0, c->stream>>>(*c);
-    k_rhs_gather<float><<<nblk(c->np), kThreads, 0, c->stream>>>(*c);
+    launch_k(k_rhs_elem<float>, nblk(c->ne), kThreads, c->stream, *c);
+    launch_k(k_rhs_gather<float>, nblk(c->np), kThreads, c->stream, *c);
   } else {
-    k_rhs_elem<double><<<nblk(c->ne), kThreads, 0, c->stream>>>(*c);
-    k_rhs_gather<double><<<nblk(c->np), kThreads, 0, c->stream>>>(*c);
+    launch_k(k_rhs_elem<double>, nblk(c->ne), kThreads, c->stream, *c);
+    launch_k(k_rhs_gather<double>, nblk(c->np), kThreads, c->stream, *c);
   }
   c->launches += 2;
   if (c->neta > 0) {
-    k_eta_bc<<<nblk(c->neta), kThreads, 0, c->stream>>>(*c, c->steps, c->flags);
+    launch_k(k_eta_bc, nblk(c->neta), kThreads, c->stream, *c, c->steps, c->flags);
     c->launches++;
     if (c->n_obc_rhs_nodes > 0) {
-      k_obc_rhs<<<nblk(c->n_obc_rhs_nodes), kThreads, 0, c->stream>>>(*c);
+      launch_k(k_obc_rhs, nblk(c->n_obc_rhs_nodes), kThreads, c->stream, *c);
       c->launches++;
     }
   }
@@ -375,8 +376,8 @@ static int download_state(adc_ctx *c) {
   if (a->coef) {
     // COEF as the reference holds it: apply a drift the last solve left pending
     int *w = rebuild_flag(c);
-    k_lhs_drift_flush<<<1, 1, 0, c->stream>>>(w);
-    k_lhs_drift<<<nblk(np), kThreads, 0, c->stream>>>(*c, w + 2);
+    launch_k(k_lhs_drift_flush, 1, 1, c->stream, w);
+    launch_k(k_lhs_drift, nblk(np), kThreads, c->stream, *c, w + 2);
     ADC_CUDA(cudaGetLastError());
     ADC_CUDA(cudaStreamSynchronize(c->stream));
     std::vector<double> d(np), o(std::max(c->nnz_pad, 1));
@@ -748,7 +749,7 @@ int adc_run(adc_ctx *c, int nsteps, const adc_step_t *steps, int *numitr, adc_st
     int rc = ADC_OK;
     if (e == cudaSuccess) {
       rc = enqueue_step(c, false);
-      k_step_end<<<1, 1, 0, c->stream>>>(c->flags, c->numitr_log, c->numitr_cap);
+      launch_k(k_step_end, 1, 1, c->stream, c->flags, c->numitr_log, c->numitr_cap);
       e = cudaStreamEndCapture(c->stream, &g);
     }
     c->graph_launches = (int)(c->launches - l0) + 1;
@@ -767,7 +768,7 @@ int adc_run(adc_ctx *c, int nsteps, const adc_step_t *steps, int *numitr, adc_st
       c->launches += c->graph_launches;
     } else {
       TRY(enqueue_step(c, false));
-      k_step_end<<<1, 1, 0, c->stream>>>(c->flags, c->numitr_log, c->numitr_cap);
+      launch_k(k_step_end, 1, 1, c->stream, c->flags, c->numitr_log, c->numitr_cap);
       c->launches++;
     }
   }

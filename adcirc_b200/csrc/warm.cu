@@ -17,6 +17,7 @@ namespace adc {
 // guess p = 2u - u_prev (p = u at elevation-specified rows), and their
 // block sums of squares.
 __global__ void k_warm_resid(adc_ctx c) {
+  griddep_wait();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   double r2u = 0.0, r2p = 0.0;
   if (i < c.np) {
@@ -75,6 +76,7 @@ __global__ void k_warm_resid(adc_ctx c) {
 
 // One block: totals in block order, then the choice and its statistics.
 __global__ void k_warm_choose(adc_ctx c, int nparts) {
+  griddep_wait();
   __shared__ double sh[2][32];
   double su = 0.0, sp = 0.0;
   for (int b = threadIdx.x; b < nparts; b += blockDim.x) {
@@ -105,6 +107,7 @@ __global__ void k_warm_choose(adc_ctx c, int nparts) {
 // Applies the choice and remembers this step's reference guess (the last
 // solution) for the next extrapolation.
 __global__ void k_warm_apply(adc_ctx c) {
+  griddep_wait();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= c.np) return;
   const double u = c.etas[i], uprev = c.etas_prev[i];
@@ -115,9 +118,9 @@ __global__ void k_warm_apply(adc_ctx c) {
 int launch_warm_start(adc_ctx *c) {
   if (!(c->prec & ADC_WARM_START)) return ADC_OK;
   const int nb = nblk(c->np);
-  k_warm_resid<<<nb, kThreads, 0, c->stream>>>(*c);
-  k_warm_choose<<<1, 1024, 0, c->stream>>>(*c, nb);
-  k_warm_apply<<<nb, kThreads, 0, c->stream>>>(*c);
+  launch_k(k_warm_resid, nb, kThreads, c->stream, *c);
+  launch_k(k_warm_choose, 1, 1024, c->stream, *c, nb);
+  launch_k(k_warm_apply, nb, kThreads, c->stream, *c);
   c->launches += 3;
   return ADC_OK;
 }

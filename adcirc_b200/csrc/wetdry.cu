@@ -19,6 +19,7 @@ constexpr int kW1Block = 256;
 
 // D1, wetdry.F:234-285.
 __global__ void k_wd_d1(adc_ctx c) {
+  griddep_wait();
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i == 0) c.flags->n_w1_events = 0;
   if (i >= c.np) return;
@@ -41,6 +42,7 @@ __device__ __forceinline__ double hyb_term(const adc_params_t &p, double h1) {
 
 // W1, wetdry.F:332-809, plus NOFFOLD/NOFF initialisation (:222-225).
 __global__ void __launch_bounds__(kW1Block) k_wd_w1(adc_ctx c) {
+  griddep_wait();
   int e = blockIdx.x * blockDim.x + threadIdx.x;
   bool ev = false;
   int ea = 0, eb = 0;
@@ -110,6 +112,7 @@ __global__ void __launch_bounds__(kW1Block) k_wd_w1(adc_ctx c) {
 
 // Sequential-semantics resolution of the W1 TK events (one block).
 __global__ void __launch_bounds__(1024) k_wd_chain(adc_ctx c) {
+  griddep_wait();
   __shared__ int s_any;
   if (threadIdx.x == 0) s_any = c.flags->n_w1_events;
   __syncthreads();
@@ -202,6 +205,7 @@ __global__ void __launch_bounds__(1024) k_wd_chain(adc_ctx c) {
 // DE1 (wetdry.F:1110-1162), then NCEle for D2 and the NOFF change count
 // (:1428-1430).
 __global__ void k_wd_de1(adc_ctx c) {
+  griddep_wait();
   int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= c.ne) return;
   int NM1 = c.nm[3 * e], NM2 = c.nm[3 * e + 1], NM3 = c.nm[3 * e + 2];
@@ -223,6 +227,7 @@ __global__ void k_wd_de1(adc_ctx c) {
 // D2 (wetdry.F:1361-1391), NODECODE update (:1413-1418) and the H2 update
 // of timestep.F:1097-1099.
 __global__ void k_wd_d2(adc_ctx c) {
+  griddep_wait();
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= c.np) return;
   int mju = 0;
@@ -261,6 +266,7 @@ __global__ void k_wd_d2(adc_ctx c) {
 }
 
 __global__ void k_h2_update(adc_ctx c) {
+  griddep_wait();
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= c.np) return;
   c.h2[i] = c.dp[i] + c.p.ifnlfa * c.eta2[i];
@@ -268,6 +274,7 @@ __global__ void k_h2_update(adc_ctx c) {
 
 // computeAlpha, wetdry.F:1561-1652.
 __global__ void k_wd_alpha(adc_ctx c) {
+  griddep_wait();
   int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= c.ne) return;
   int NM1 = c.nm[3 * e], NM2 = c.nm[3 * e + 1], NM3 = c.nm[3 * e + 2];
@@ -307,16 +314,16 @@ __global__ void k_wd_alpha(adc_ctx c) {
 int launch_wetdry(adc_ctx *c) {
   const adc_ctx &cv = *c;
   if (c->p.nolifa != 2) {
-    k_h2_update<<<nblk(c->np), kThreads, 0, c->stream>>>(cv);
+    launch_k(k_h2_update, nblk(c->np), kThreads, c->stream, cv);
     c->launches++;
     return ADC_OK;
   }
-  k_wd_d1<<<nblk(c->np), kThreads, 0, c->stream>>>(cv);
-  k_wd_w1<<<c->ev_blocks, kW1Block, 0, c->stream>>>(cv);
-  k_wd_chain<<<1, 1024, 0, c->stream>>>(cv);
-  k_wd_de1<<<nblk(c->ne), kThreads, 0, c->stream>>>(cv);
-  k_wd_d2<<<nblk(c->np), kThreads, 0, c->stream>>>(cv);
-  k_wd_alpha<<<nblk(c->ne), kThreads, 0, c->stream>>>(cv);
+  launch_k(k_wd_d1, nblk(c->np), kThreads, c->stream, cv);
+  launch_k(k_wd_w1, c->ev_blocks, kW1Block, c->stream, cv);
+  launch_k(k_wd_chain, 1, 1024, c->stream, cv);
+  launch_k(k_wd_de1, nblk(c->ne), kThreads, c->stream, cv);
+  launch_k(k_wd_d2, nblk(c->np), kThreads, c->stream, cv);
+  launch_k(k_wd_alpha, nblk(c->ne), kThreads, c->stream, cv);
   c->launches += 6;
   return ADC_OK;
 }
