@@ -132,6 +132,28 @@ def jcg_bytes(nnz_o: int, npn: int, iters: float, vbytes: int = 8) -> float:
             npn * (64.0 + 44.0 + 24.0 + 68.0 * iters + 60.0))
 
 
+def profiled_traffic(kernel: str = "jcg_kernel<1, float>"):
+    """DRAM bytes (read + write) of one launch of `kernel`, from the committed
+    ncu summary profiles/surge_kernels_full.md, or None."""
+    p = ROOT / "profiles" / "surge_kernels_full.md"
+    if not p.exists():
+        return None
+    cols, vals = None, {}
+    for line in p.read_text().splitlines():
+        cells = [c.strip() for c in line.strip().strip("|").split("|")]
+        if line.startswith("| metric |"):
+            cols = [c.strip("`") for c in cells[1:]]
+        elif cols and line.startswith("| DRAM read") or cols and line.startswith("| DRAM write"):
+            vals[cells[0]] = cells[1:]
+    if not cols or kernel not in cols or len(vals) != 2:
+        return None
+    k = cols.index(kernel)
+    try:
+        return sum(float(v[k]) * 1e6 for v in vals.values())   # Mbyte -> bytes
+    except (ValueError, IndexError):
+        return None
+
+
 def make_case(name: str):
     from adcirc_b200 import model
     if name == "surge":
@@ -317,7 +339,9 @@ def bench_gpu(args, rank, world, dist):
         "jcg_iters_per_step": res["chosen"]["jcg_iters_per_step"],
         "phase_ms": ph,
         "roofline": {"bound": "hbm", "kernel": "jcg_kernel", "achieved": achieved, "peak": peak,
-                     "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                     "unit": "GB/s", "frac": achieved / peak, "traffic": profiled_traffic(),
+                     "traffic_source": "profiles/surge_kernels_full.md (ncu, one launch of "
+                                       "jcg_kernel<1, float>, DRAM bytes read + written)",
                      "peak_kind": peak_kind, "iters_per_launch": mean_it},
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": 44, "d2h_bytes_per_step": 56,
                 "steps": K2, "api": "adc_timestep per step"},
