@@ -125,7 +125,9 @@ struct adc_ctx {
   double *ebuf2;         // 3*NE doubles (momentum y)
   double *red;           // reduction partials
   // W1 events
-  int *ev_cnt;           // per element-block event counts
+  int *ev_cnt;           // per element-block event counts, then their offsets
+  int *evu_i;            // unordered W1 events (a, b, element) while they fit a chunk
+  double *evu_c;
   int *ev_a, *ev_b;      // per element: NM123, partner (compacted per block)
   double *ev_c;
   int ev_blocks;

@@ -414,7 +414,7 @@ static void free_ctx(adc_ctx *c) {
       (void **)&c->noff, (void **)&c->noffold, (void **)&c->mju, (void **)&c->ncele,
       (void **)&c->diag, (void **)&c->offd, (void **)&c->obccoef, (void **)&c->ebuf,
       (void **)&c->ebuf2, (void **)&c->red, (void **)&c->ev_cnt, (void **)&c->ev_a,
-      (void **)&c->ev_b, (void **)&c->ev_c, (void **)&c->ju1, (void **)&c->jp[0],
+      (void **)&c->ev_b, (void **)&c->ev_c, (void **)&c->evu_i, (void **)&c->evu_c, (void **)&c->ju1, (void **)&c->jp[0],
       (void **)&c->jp[1], (void **)&c->jw, (void **)&c->jexp, (void **)&c->jlcol,
       (void **)&c->jhalo_ptr, (void **)&c->jhalo_ids, (void **)&c->soff32, (void **)&c->etas_prev, (void **)&c->warm, (void **)&c->soff, (void **)&c->jpart, (void **)&c->jtri,
       (void **)&c->itp, (void **)&c->bar, (void **)&c->jlines, (void **)&c->flags, (void **)&c->steps,
@@ -542,7 +542,8 @@ static int bind_impl(const adc_params_t *p, const adc_arrays_t *a, int prec, adc
     ADC_CUDA(cudaMemset(c->warm, 0, sizeof(WarmState)));
   }
   c->ev_blocks = (ne + 255) / 256;
-  B(dalloc(&c->ev_cnt, c->ev_blocks));
+  B(dalloc(&c->ev_cnt, 2 * ((size_t)c->ev_blocks + 1)));   // counts, then offsets
+  B(dalloc(&c->evu_i, 3 * 1024)); B(dalloc(&c->evu_c, 1024));   // one W1 chunk (wetdry.cu)
   B(dalloc(&c->ev_a, (size_t)c->ev_blocks * 256)); B(dalloc(&c->ev_b, (size_t)c->ev_blocks * 256));
   B(dalloc(&c->ev_c, (size_t)c->ev_blocks * 256));
   {

@@ -6,9 +6,9 @@
 // node and element passes run one thread per item.  The exception is the
 // W1 friction update (wetdry.F:593-618): it applies, in element order,
 // TK(a) = TK(b) = max(candidate, TK(a), TK(b)) for each wetting event.
-// Events are compacted per block in element order and resolved by one warp
-// in batches of 32, with in-batch dependencies settled by shuffles, which
-// reproduces the sequential result exactly.
+// Events are compacted per block in element order, and one block resolves
+// the ordered list through each event's predecessors on its two nodes
+// (k_wd_chain), which reproduces the sequential result exactly.
 #include "adc_internal.cuh"
 
 #include <cfloat>
@@ -16,6 +16,7 @@
 namespace adc {
 
 constexpr int kW1Block = 256;
+constexpr int kChainFast = 1024;   // W1 events resolved in shared memory at a time
 
 // D1, wetdry.F:234-285.
 __global__ void k_wd_d1(adc_ctx c) {
@@ -98,15 +99,195 @@ __global__ void __launch_bounds__(kW1Block) k_wd_w1(adc_ctx c) {
     if (k < w) off += wcnt[k];
     tot += wcnt[k];
   }
+  // each event goes to its block's ordered slot and, while the step has at
+  // most kChainFast events, to an unordered list tagged with its element
+  __shared__ int s_ubase;
+  if (threadIdx.x == 0) {
+    c.ev_cnt[blockIdx.x] = tot;
+    s_ubase = tot ? atomicAdd(&c.flags->n_w1_events, tot) : 0;
+  }
+  __syncthreads();
   if (ev) {
-    int pos = blockIdx.x * kW1Block + off + __popc(m & ((1u << lane) - 1u));
+    const int r = off + __popc(m & ((1u << lane) - 1u));
+    const int pos = blockIdx.x * kW1Block + r;
     c.ev_a[pos] = ea;
     c.ev_b[pos] = eb;
     c.ev_c[pos] = ec;
+    const int u = s_ubase + r;
+    if (u < kChainFast) {
+      c.evu_i[3 * u] = ea;
+      c.evu_i[3 * u + 1] = eb;
+      c.evu_i[3 * u + 2] = e;
+      c.evu_c[u] = ec;
+    }
   }
-  if (threadIdx.x == 0) {
-    c.ev_cnt[blockIdx.x] = tot;
-    if (tot) atomicAdd(&c.flags->n_w1_events, tot);
+}
+
+// The ordered event list is resolved by the whole block, kChainFast events
+// at a time.
+// With the events in element order, the value event e assigns is
+//   val(e) = max(cand(e), prior(a_e), prior(b_e)),
+// where prior(x) is val of the latest earlier event touching node x, or
+// the TK that x had before the pass.  Each event's two predecessors are
+// found by a backward search; the values then follow by repeated
+// max-propagation along those edges until nothing changes (at most the
+// depth of the event DAG, each edge pointing to an earlier event), and the
+// last event touching a node writes it.  Max is exact, so this equals the
+// sequential result bit for bit.
+
+struct ChainSmem {
+  int a[kChainFast], b[kChainFast];   // the event's two nodes
+  double v[kChainFast];               // candidate, then the value it assigns
+  short pa[kChainFast], pb[kChainFast];
+  unsigned char lasta[kChainFast], lastb[kChainFast];
+  int ord[kChainFast];                // the event's element (its order)
+  unsigned long long key[2 * kChainFast];   // (node, order, slot, side) sort keys
+};
+
+// k_wd_chain's working set (file scope, so its accesses compile to
+// shared-memory instructions).
+__shared__ ChainSmem g_chain;
+
+// One chunk of the ordered list.  With `loaded` the chunk's nodes and
+// candidates are already in shared memory, else they come from la/lb/lc.
+__device__ void chain_block(adc_ctx &c, const int *la, const int *lb, const double *lc,
+                            int total, bool loaded) {
+  int *s_a = g_chain.a, *s_b = g_chain.b;
+  double *s_v = g_chain.v;
+  short *s_pa = g_chain.pa, *s_pb = g_chain.pb;
+  unsigned char *s_lasta = g_chain.lasta, *s_lastb = g_chain.lastb;
+  for (int e = threadIdx.x; e < total; e += blockDim.x) {
+    if (!loaded) {
+      s_a[e] = la[e];
+      s_b[e] = lb[e];
+      s_v[e] = lc[e];   // the event's candidate
+      g_chain.ord[e] = e;
+    }
+    s_lasta[e] = 1;
+    s_lastb[e] = 1;
+  }
+  __syncthreads();
+  // predecessors: sort the (node, event, side) pairs; the entry before a
+  // pair in sorted order, if it has the same node, is the latest earlier
+  // event on that node (bitonic sort in shared memory)
+  unsigned long long *key = g_chain.key;
+  const int nk = 2 * total;
+  int P = 1;
+  while (P < nk) P <<= 1;
+  for (int i = threadIdx.x; i < P; i += blockDim.x) {
+    unsigned long long k = ~0ull;   // padding sorts last
+    if (i < nk) {
+      const int e = i >> 1, side = i & 1;
+      const unsigned long long node = (unsigned)(side ? s_b[e] : s_a[e]);
+      k = (node << 33) | ((unsigned long long)(unsigned)g_chain.ord[e] << 12) |
+          ((unsigned long long)e << 1) | (unsigned long long)side;
+    }
+    key[i] = k;
+  }
+  __syncthreads();
+  // thread i holds key i (P <= 2 * kChainFast <= 2 * blockDim.x: two keys
+  // per thread at most); partners within a warp trade by shuffle, others
+  // through shared memory
+  for (int kk = 2; kk <= P; kk <<= 1)
+    for (int j = kk >> 1; j > 0; j >>= 1) {
+      if (j >= 32) {
+        for (int i = threadIdx.x; i < P; i += blockDim.x) {
+          const int ixj = i ^ j;
+          if (ixj > i) {
+            const unsigned long long x = key[i], y = key[ixj];
+            const bool up = (i & kk) == 0;
+            if ((x > y) == up) {
+              key[i] = y;
+              key[ixj] = x;
+            }
+          }
+        }
+        __syncthreads();
+      } else {
+        // runs of intra-warp stages: every thread updates its own keys
+        for (int i0 = threadIdx.x & ~31; i0 < P; i0 += blockDim.x) {
+          const int i = i0 + (threadIdx.x & 31);
+          unsigned long long x = key[i];
+          for (int jj = j; jj > 0; jj >>= 1) {
+            const unsigned long long y = __shfl_xor_sync(0xffffffffu, x, jj);
+            const bool up = (i & kk) == 0, lower = (i & jj) == 0;
+            // the lower partner keeps the min when sorting up, the max otherwise
+            const bool keep_min = (lower == up);
+            x = keep_min ? (x < y ? x : y) : (x > y ? x : y);
+          }
+          key[i] = x;
+        }
+        __syncthreads();
+        break;   // the intra-warp stages of this kk are done
+      }
+    }
+  for (int i = threadIdx.x; i < nk; i += blockDim.x) {
+    const unsigned long long k = key[i];
+    const int e = (int)((k >> 1) & 2047), side = (int)(k & 1);
+    int pred = -1;
+    if (i > 0 && (key[i - 1] >> 33) == (k >> 33)) pred = (int)((key[i - 1] >> 1) & 2047);
+    if (side) s_pb[e] = (short)pred;
+    else s_pa[e] = (short)pred;
+  }
+  __syncthreads();
+  // initial values, one thread per event so the global loads overlap
+  for (int e = threadIdx.x; e < total; e += blockDim.x) {
+    double v = s_v[e];
+    if (s_pa[e] < 0) {
+      const double t = c.tk[s_a[e]];
+      if (t > v) v = t;
+    }
+    if (s_pb[e] < 0) {
+      const double t = c.tk[s_b[e]];
+      if (t > v) v = t;
+    }
+    s_v[e] = v;
+  }
+  __syncthreads();
+  // a predecessor found for node x is no longer the last event touching x;
+  // each (predecessor, node) pair has one such later event at most
+  for (int e = threadIdx.x; e < total; e += blockDim.x) {
+    const int pa = s_pa[e], pb = s_pb[e];
+    if (pa >= 0) {
+      if (s_a[pa] == s_a[e]) s_lasta[pa] = 0;
+      else s_lastb[pa] = 0;
+    }
+    if (pb >= 0) {
+      if (s_a[pb] == s_b[e]) s_lasta[pb] = 0;
+      else s_lastb[pb] = 0;
+    }
+  }
+  // max-propagation along the predecessor edges (values only grow; a round
+  // in which nothing changes is the fixed point); bounded by the list length
+  for (int round = 0; round <= total; ++round) {
+    int changed = 0;
+    for (int e = threadIdx.x; e < total; e += blockDim.x) {
+      const int pa = s_pa[e], pb = s_pb[e];
+      double v = s_v[e];
+      double nv = v;
+      if (pa >= 0 && s_v[pa] > nv) nv = s_v[pa];
+      if (pb >= 0 && s_v[pb] > nv) nv = s_v[pb];
+      if (nv != v) {
+        s_v[e] = nv;
+        changed = 1;
+      }
+    }
+    if (!__syncthreads_or(changed)) break;
+  }
+  for (int e = threadIdx.x; e < total; e += blockDim.x) {
+    const double v = s_v[e];
+    if (s_lasta[e]) {
+      const int a = s_a[e];
+      c.tk[a] = v;
+      c.tkm[3 * a] = v;
+      c.tkm[3 * a + 1] = v;
+    }
+    if (s_lastb[e]) {
+      const int b = s_b[e];
+      c.tk[b] = v;
+      c.tkm[3 * b] = v;
+      c.tkm[3 * b + 1] = v;
+    }
   }
 }
 
@@ -117,14 +298,28 @@ __global__ void __launch_bounds__(1024) k_wd_chain(adc_ctx c) {
   if (threadIdx.x == 0) s_any = c.flags->n_w1_events;
   __syncthreads();
   if (s_any == 0) return;
-  // exclusive scan of the per-block counts (fixed partition per thread)
+  if (s_any <= kChainFast && c.ne < (1 << 21)) {
+    // the unordered list W1 wrote: its element tags give the order
+    const int total = s_any;
+    for (int e = threadIdx.x; e < total; e += blockDim.x) {
+      g_chain.a[e] = c.evu_i[3 * e];
+      g_chain.b[e] = c.evu_i[3 * e + 1];
+      g_chain.ord[e] = c.evu_i[3 * e + 2];
+      g_chain.v[e] = c.evu_c[e];
+    }
+    __syncthreads();
+    chain_block(c, nullptr, nullptr, nullptr, total, true);
+    return;
+  }
+  // long lists: ordered by an exclusive scan of the per-block counts (fixed
+  // partition per thread), then resolved in chunks
   const int nb = c.ev_blocks;
   const int T = blockDim.x;
   const int per = (nb + T - 1) / T;
   const int b0 = threadIdx.x * per, b1 = min(nb, b0 + per);
   int mysum = 0;
   for (int b = b0; b < b1; ++b) mysum += c.ev_cnt[b];
-  __shared__ int sc[1024];
+  int *sc = (int *)g_chain.key;   // scan scratch, free until the chunks start
   sc[threadIdx.x] = mysum;
   __syncthreads();
   for (int o = 1; o < T; o <<= 1) {
@@ -133,72 +328,70 @@ __global__ void __launch_bounds__(1024) k_wd_chain(adc_ctx c) {
     sc[threadIdx.x] += v;
     __syncthreads();
   }
-  int base = sc[threadIdx.x] - mysum;
+  const int base = sc[threadIdx.x] - mysum;
   const int total = sc[T - 1];
-  // gather events into one contiguous ordered list (reuses ebuf2 as doubles
-  // for candidates and the tail of ev arrays is not touched)
-  int *la = (int *)c.ebuf2;
-  int *lb = la + c.ne;
-  double *lc = c.ebuf2 + c.ne;   // ebuf2 holds 3*NE doubles
-  for (int b = b0; b < b1; ++b) {
-    int n = c.ev_cnt[b];
-    for (int k = 0; k < n; ++k) {
-      int src = b * kW1Block + k;
-      la[base + k] = c.ev_a[src];
-      lb[base + k] = c.ev_b[src];
-      lc[base + k] = c.ev_c[src];
+  // exclusive event offsets of every W1 block (off[nb] = total), then the
+  // blocks' events copied into one ordered list by whole warps at a time
+  int *off = c.ev_cnt + nb + 1;
+  {
+    int o = base;
+    for (int b = b0; b < b1; ++b) {
+      off[b] = o;
+      o += c.ev_cnt[b];
     }
-    base += n;
+    if (threadIdx.x == 0) off[nb] = total;
   }
   __syncthreads();
-  __threadfence_block();
-  if (threadIdx.x >= 32) return;
-  const int lane = threadIdx.x;
-  for (int s = 0; s < total; s += 32) {
-    int m = min(32, total - s);
-    bool act = lane < m;
-    int a = act ? la[s + lane] : -1 - lane;
-    int b = act ? lb[s + lane] : -1000 - lane;
-    double cand = act ? lc[s + lane] : 0.0;
-    double A = act ? c.tk[a] : 0.0;
-    double B = act ? c.tk[b] : 0.0;
-    int pa = -1, pb = -1;
-    bool last_a = true, last_b = true;
-    for (int j = 0; j < 32; ++j) {
-      int aj = __shfl_sync(0xffffffffu, a, j);
-      int bj = __shfl_sync(0xffffffffu, b, j);
-      if (j < lane) {
-        if (aj == a || bj == a) pa = j;
-        if (aj == b || bj == b) pb = j;
-      } else if (j > lane && j < m) {
-        if (aj == a || bj == a) last_a = false;
-        if (aj == b || bj == b) last_b = false;
+  int *la = (int *)c.ebuf2;      // ebuf2 holds 3*NE doubles: 2*NE ints, then NE doubles
+  int *lb = la + c.ne;
+  double *lc = c.ebuf2 + c.ne;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = T >> 5;
+  constexpr int kGroup = 8;   // chunks of 32 blocks whose offsets load together
+  for (int g0 = warp * 32; g0 < nb; g0 += kGroup * nwarps * 32) {
+    int og[kGroup], ng[kGroup];
+#pragma unroll
+    for (int q = 0; q < kGroup; ++q) {
+      const int b = g0 + q * nwarps * 32 + lane;
+      og[q] = 0;
+      ng[q] = 0;
+      if (b < nb) {
+        og[q] = off[b];
+        ng[q] = off[b + 1] - og[q];
       }
     }
-    double v = cand;
-    if (pa < 0 && A > v) v = A;
-    if (pb < 0 && B > v) v = B;
-    for (int r = 0; r < 33; ++r) {
-      double va = __shfl_sync(0xffffffffu, v, pa >= 0 ? pa : lane);
-      double vb = __shfl_sync(0xffffffffu, v, pb >= 0 ? pb : lane);
-      double nv = v;
-      if (pa >= 0 && va > nv) nv = va;
-      if (pb >= 0 && vb > nv) nv = vb;
-      bool ch = nv != v;
-      v = nv;
-      if (!__any_sync(0xffffffffu, ch)) break;
+#pragma unroll
+    for (int q = 0; q < kGroup; ++q) {
+      const int bw = g0 + q * nwarps * 32;
+      const int o0 = og[q], n = ng[q];
+      unsigned m = __ballot_sync(0xffffffffu, n > 0);
+      while (m) {
+        const int j = __ffs(m) - 1;
+        m &= m - 1;
+        const int jo = __shfl_sync(0xffffffffu, o0, j), jn = __shfl_sync(0xffffffffu, n, j);
+        for (int k = lane; k < jn; k += 32) {
+          const int src = (bw + j) * kW1Block + k, p = jo + k;
+          const int ea = c.ev_a[src], eb = c.ev_b[src];
+          const double ec = c.ev_c[src];
+          if (p < kChainFast) {   // the first chunk goes straight to shared memory
+            g_chain.a[p] = ea;
+            g_chain.b[p] = eb;
+            g_chain.v[p] = ec;
+            g_chain.ord[p] = p;
+          } else {
+            la[p] = ea;
+            lb[p] = eb;
+            lc[p] = ec;
+          }
+        }
+      }
     }
-    if (act && last_a) {
-      c.tk[a] = v;
-      c.tkm[3 * a] = v;
-      c.tkm[3 * a + 1] = v;
-    }
-    if (act && last_b) {
-      c.tk[b] = v;
-      c.tkm[3 * b] = v;
-      c.tkm[3 * b + 1] = v;
-    }
-    __syncwarp();
+  }
+  __syncthreads();
+  // consecutive chunks of the ordered list; a chunk's first events read the
+  // TK the previous chunk left in memory
+  for (int s0 = 0; s0 < total; s0 += kChainFast) {
+    chain_block(c, la + s0, lb + s0, lc + s0, min(kChainFast, total - s0), s0 == 0);
+    __syncthreads();
   }
 }
 

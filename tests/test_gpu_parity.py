@@ -157,3 +157,38 @@ def test_jcg_dropin(lib, orc, itmax, tol):
     assert _rel(g[4], o[4]) <= 1e-13      # rhs restored
     if itmax == 3:
         assert o[0] == 13 and abs(g[6][0] - o[6][0]) <= 1e-9 * abs(o[6][0])
+
+
+@pytest.mark.parametrize("ny", [401, 2101])
+def test_w1_chain_burst(lib, orc, ny):
+    """A wetting front across a long beach: one wet/dry pass with hundreds
+    (ny=401) to thousands (ny=2101) of W1 events whose TK updates chain
+    through shared nodes from row to row.  The order-dependent result
+    (wetdry.F:593-618) must match the sequential oracle bit for bit, for the
+    block-wide resolution of short lists and the batched one of long lists."""
+    import oracle
+    from adcirc_b200 import _lib, meshgen, model
+    raw = meshgen.channel_mesh(nx=41, ny=ny, lx=4e3, ly=0.1e3 * (ny - 1), depth0=3.0, depth1=-1.5)
+    rng = np.random.default_rng(7)
+    eta0 = np.where(raw.dp > 0.05, rng.uniform(0.5, 1.0, raw.dp.size), 0.0)
+    params = model.default_params(0.1)
+    tides = [(1e-4, 0.0, 1.0, np.zeros(raw.open_nodes.size), np.zeros(raw.open_nodes.size))]
+    base = model.build_case(raw, params, model.Schedule(dt=0.1, nramp=0), tides, eta0=eta0)
+    tk = rng.uniform(0.0, 8.0, raw.dp.size)
+    base.arrays["tk"][:] = tk
+    base.arrays["tkm"][:] = 0.0
+    base.arrays["tkm"][0::3] = tk
+    base.arrays["tkm"][1::3] = tk
+    c0, cg = base.clone(), base.clone()
+    o = oracle.OracleModel(c0)
+    oo = o.wetdry(1)
+    g = model.GpuModel(cg)
+    go = _lib.AdcStepOut()
+    assert lib.adc_wetdry(g.h, C.byref(base.schedule.step(1)), C.byref(go)) == 0
+    g.sync_to_host()
+    g.close()
+    o.close()
+    assert go.n_w1_events == oo.n_w1_events
+    assert (300 if ny == 401 else 2000) <= go.n_w1_events, go.n_w1_events
+    for f in ("tk", "tkm", "nodecode", "nnodecode", "noff", "eta2"):
+        assert np.array_equal(cg.arrays[f], c0.arrays[f]), f
