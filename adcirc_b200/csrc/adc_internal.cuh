@@ -120,6 +120,12 @@ struct adc_ctx {
   double *gwce_lv, *mom_x, *mom_y;
   int *nodecode, *nnodecode, *noff, *noffold, *mju, *ncele;
   double *diag, *offd, *obccoef;
+  // incremental GWCE LHS rebuild: cached element entries and the inputs they
+  // were built with, rows to gather again, boundary rows (always gathered)
+  // and each row's gathered diagonal
+  double *lhs_ebuf, *lhs_al, *diag_gathered;
+  int *lhs_nc;
+  unsigned char *lhs_dirty, *bc_row;
   // scratch
   double *ebuf;          // element contributions, 9*NE doubles
   double *ebuf2;         // 3*NE doubles (momentum y)

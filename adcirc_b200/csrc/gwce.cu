@@ -88,6 +88,8 @@ __global__ void k_lhs_drift(adc_ctx c, const int *apply) {
   griddep_wait();
   if (!*apply) return;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
+  // the drift changes every row's off-diagonals: the next rebuild gathers all
+  if (i == 0) const_cast<int *>(apply)[1] = 1;
   if (i >= c.np) return;
   const double wi = c.jw[i];
   const double winv_i = 1.0 / wi;
@@ -110,32 +112,38 @@ __global__ void k_lhs_drift_flush(int *words) {
 }
 
 // gwce.F:456-593: nine consistent-mass + gravity entries per element.
+// The entries depend on the element's static geometry and depth and on two
+// per-step inputs, NCEle and ALPHAL; an element is recomputed only when
+// those differ from the values its cached entries were built with (every
+// element on the first rebuild and after a host upload), and the nodes of
+// a recomputed element are marked for the row gather.  The cached entries
+// equal what a full rebuild writes, bit for bit.
 template <class R>
 __global__ void k_lhs_elem(adc_ctx c, const int *rebuild) {
   griddep_wait();
   if (!*rebuild) return;
-  __shared__ R sh[kThreads / 32][32 * 9];
-  const int e0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31);   // the warp's first element
-  if (e0 >= c.ne) return;                                          // whole warp past the end
-  const int nvalid = min(32, c.ne - e0);
-  int e = blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= c.ne) e = c.ne - 1;   // idle lanes recompute the last element; not stored
-  const adc_params_t &p = c.p;
-  const R DT = R(p.dt);
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= c.ne) return;
   int n1 = c.nm[3 * e], n2 = c.nm[3 * e + 1], n3 = c.nm[3 * e + 2];
   int NCEle = c.nodecode[n1] * c.nodecode[n2] * c.nodecode[n3] * c.noff[e];
+  const double ald = c.alphal[e];
+  if (c.lhs_nc[e] == NCEle &&
+      __double_as_longlong(c.lhs_al[e]) == __double_as_longlong(ald))
+    return;
+  const adc_params_t &p = c.p;
+  const R DT = R(p.dt);
   R FDX1 = c.fdx[3 * e], FDX2 = c.fdx[3 * e + 1], FDX3 = c.fdx[3 * e + 2];
   R FDY1 = c.fdy[3 * e], FDY2 = c.fdy[3 * e + 1], FDY3 = c.fdy[3 * e + 2];
   R AreaIE2 = c.areas[e];
   R AreaIE = AreaIE2 * R(0.5);
   R AreaIE4 = AreaIE2 * R(2.0);
   R DPAvg = (c.dp[n1] + c.dp[n2] + c.dp[n3]) / R(3.0);
-  R GA = R(c.alphal[e]) * R(p.a00) * R(p.g) * DPAvg / AreaIE4;
+  R GA = R(ald) * R(p.a00) * R(p.g) * DPAvg / AreaIE4;
   R Tau0Avg = (c.tau0[n1] + c.tau0[n2] + c.tau0[n3]) / R(3.0);
   R MsOn = 2 * AreaIE * (R(1.0) / DT + Tau0Avg / R(2.0)) / DT / R(12.0);
   R MsOff = 1 * AreaIE * (R(1.0) / DT + Tau0Avg / R(2.0)) / DT / R(12.0);
   R nc = (R)NCEle;
-  R o[9];
+  R *o = reinterpret_cast<R *>(c.lhs_ebuf) + 9 * (size_t)e;
   o[0] = (MsOn + GA * (FDX1 * FDX1 + FDY1 * FDY1)) * nc;
   o[1] = (MsOn + GA * (FDX2 * FDX2 + FDY2 * FDY2)) * nc;
   o[2] = (MsOn + GA * (FDX3 * FDX3 + FDY3 * FDY3)) * nc;
@@ -145,7 +153,11 @@ __global__ void k_lhs_elem(adc_ctx c, const int *rebuild) {
   o[6] = (MsOff + GA * (FDX2 * FDX3 + FDY2 * FDY3)) * nc;  // (n2, J23)
   o[7] = (MsOff + GA * (FDX3 * FDX1 + FDY3 * FDY1)) * nc;  // (n3, J31)
   o[8] = (MsOff + GA * (FDX3 * FDX2 + FDY3 * FDY2)) * nc;  // (n3, J32)
-  warp_store_k<9>(reinterpret_cast<R *>(c.ebuf) + 9 * (size_t)e0, o, nvalid, sh[threadIdx.x >> 5]);
+  c.lhs_nc[e] = NCEle;
+  c.lhs_al[e] = ald;
+  c.lhs_dirty[n1] = 1;
+  c.lhs_dirty[n2] = 1;
+  c.lhs_dirty[n3] = 1;
 }
 
 // Per-row gather of COEF in element order, and the per-block partial of
@@ -155,9 +167,17 @@ __global__ void k_lhs_gather(adc_ctx c, const int *rebuild) {
   griddep_wait();
   if (!*rebuild) return;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const R *eb = reinterpret_cast<const R *>(c.ebuf);
+  const R *eb = reinterpret_cast<const R *>(c.lhs_ebuf);
   double d2 = 0.0;
-  if (i < c.np) {
+  // rows whose elements did not change keep their gathered off-diagonals;
+  // only their diagonal, which each solve's scal/unscal rewrites, returns
+  // to the gathered value
+  const bool all = rebuild[3] != 0;
+  if (i < c.np && !all && !c.lhs_dirty[i] && !c.bc_row[i]) {
+    const double d = c.diag_gathered[i];
+    c.diag[i] = d;
+    d2 = d * d;
+  } else if (i < c.np) {
     R d = R(0.0);
     const int q0 = c.n2e_ptr[i], q1 = c.n2e_ptr[i + 1];
     for (int qc = q0; qc < q1; qc += kGatherChunk) {
@@ -175,6 +195,8 @@ __global__ void k_lhs_gather(adc_ctx c, const int *rebuild) {
       for (int k = 0; k < kGatherChunk; ++k) if (qc + k < q1) d = d + x[k];
     }
     c.diag[i] = (double)d;
+    c.diag_gathered[i] = (double)d;
+    c.lhs_dirty[i] = 0;
     d2 = (double)d * (double)d;
     int s = i / kSlice, lane = i - s * kSlice;
     int base = c.sl_ptr[s] + lane;
@@ -226,7 +248,10 @@ __global__ void k_lhs_ep(adc_ctx c, const int *rebuild, int nparts) {
   if (w == 0) {
     s = lane < (int)(blockDim.x >> 5) ? sh[lane] : 0.0;
     s = warp_sum(s);
-    if (lane == 0) c.flags->ep = sqrt(s / c.np);
+    if (lane == 0) {
+      c.flags->ep = sqrt(s / c.np);
+      *const_cast<int *>(rebuild + 3) = 0;   // every row is gathered again
+    }
   }
 }
 

@@ -169,5 +169,12 @@ extern "C" int adc_hotstart_read(adc_ctx *c, const char *path) {
   }
   std::fclose(f);
   c->met_pending = 0;
+  // the cached GWCE element entries describe the old state: rebuild in full
+  {
+    int *w = (int *)(c->flags + 1);
+    int all = 1;
+    ADC_CUDA(cudaMemcpy(w + 3, &all, sizeof(int), cudaMemcpyHostToDevice));
+    ADC_CUDA(cudaMemset(c->lhs_nc, 0xff, (size_t)c->ne * sizeof(int)));
+  }
   return ADC_OK;
 }

@@ -332,8 +332,11 @@ static int upload_state(adc_ctx *c) {
   TRY(up(c->diag, d.data(), np));
   TRY(up(c->offd, o.data(), c->nnz_pad));
   {
-    int zero3[3] = {0, 0, 0};   // the host COEF is authoritative: no drift pending
-    TRY(up(rebuild_flag(c), zero3, 3));
+    // the host COEF is authoritative: no drift pending, and the next rebuild
+    // recomputes every element and gathers every row
+    int words[4] = {0, 0, 0, 1};
+    TRY(up(rebuild_flag(c), words, 4));
+    ADC_CUDA(cudaMemset(c->lhs_nc, 0xff, (size_t)c->ne * sizeof(int)));
   }
   TRY(up(c->obccoef, a->obccoef, (size_t)c->neta * (c->mnei - 1)));
   return ADC_OK;
@@ -412,7 +415,9 @@ static void free_ctx(adc_ctx *c) {
       (void **)&c->wsy2, (void **)&c->pr1, (void **)&c->pr2, (void **)&c->gwce_lv,
       (void **)&c->mom_x, (void **)&c->mom_y, (void **)&c->nodecode, (void **)&c->nnodecode,
       (void **)&c->noff, (void **)&c->noffold, (void **)&c->mju, (void **)&c->ncele,
-      (void **)&c->diag, (void **)&c->offd, (void **)&c->obccoef, (void **)&c->ebuf,
+      (void **)&c->diag, (void **)&c->offd, (void **)&c->obccoef, (void **)&c->lhs_ebuf,
+      (void **)&c->lhs_al, (void **)&c->diag_gathered, (void **)&c->lhs_nc, (void **)&c->lhs_dirty,
+      (void **)&c->bc_row, (void **)&c->ebuf,
       (void **)&c->ebuf2, (void **)&c->red, (void **)&c->ev_cnt, (void **)&c->ev_a,
       (void **)&c->ev_b, (void **)&c->ev_c, (void **)&c->evu_i, (void **)&c->evu_c, (void **)&c->ju1, (void **)&c->jp[0],
       (void **)&c->jp[1], (void **)&c->jw, (void **)&c->jexp, (void **)&c->jlcol,
@@ -505,6 +510,24 @@ static int bind_impl(const adc_params_t *p, const adc_arrays_t *a, int prec, adc
     B(up(c->emo, a->emo, (size_t)a->nbfr * a->neta)); B(up(c->efa, a->efa, (size_t)a->nbfr * a->neta));
   }
   B(dalloc(&c->obc_slot, T.obc_slot.size())); B(up(c->obc_slot, T.obc_slot.data(), T.obc_slot.size()));
+  {
+    // rows the boundary pass rewrites (elevation-specified rows and the rows
+    // holding OBCCoef entries) are gathered on every rebuild
+    std::vector<unsigned char> bc(np, 0);
+    for (int b : T.nbd) bc[b] = 1;
+    for (size_t q = 0; q < T.obc_slot.size(); ++q) {
+      const int slot = T.obc_slot[q];
+      if (slot < 0) continue;
+      int sl = (int)(std::upper_bound(T.sl_ptr.begin(), T.sl_ptr.end(), slot) - T.sl_ptr.begin()) - 1;
+      int row = sl * kSlice + (slot - T.sl_ptr[sl]) % kSlice;
+      if (row < np) bc[row] = 1;
+    }
+    B(dalloc(&c->bc_row, np)); B(up(c->bc_row, bc.data(), np));
+  }
+  B(dalloc(&c->lhs_ebuf, 9 * (size_t)ne)); B(dalloc(&c->lhs_al, ne)); B(dalloc(&c->lhs_nc, ne));
+  ADC_CUDA(cudaMemset(c->lhs_nc, 0xff, (size_t)ne * sizeof(int)));   // no element cached yet
+  B(dalloc(&c->lhs_dirty, np)); ADC_CUDA(cudaMemset(c->lhs_dirty, 1, np));
+  B(dalloc(&c->diag_gathered, np));
   B(dalloc(&c->obc_zero, T.obc_zero.size())); B(up(c->obc_zero, T.obc_zero.data(), T.obc_zero.size()));
   B(dalloc(&c->obc_rhs_ptr, T.obc_rhs_ptr.size())); B(up(c->obc_rhs_ptr, T.obc_rhs_ptr.data(), T.obc_rhs_ptr.size()));
   B(dalloc(&c->obc_rhs_node, std::max<size_t>(T.obc_rhs_node.size(), 1))); B(up(c->obc_rhs_node, T.obc_rhs_node.data(), T.obc_rhs_node.size()));
@@ -577,8 +600,8 @@ static int bind_impl(const adc_params_t *p, const adc_arrays_t *a, int prec, adc
   memset(&fl, 0, sizeof(fl));
   fl.ncchange = 1;   // adcirc.F:404: the matrix is built on the first step
   B(up(c->flags, &fl, 1));
-  int zero3[3] = {0, 0, 0};
-  B(up(rebuild_flag(c), zero3, 3));
+  int words[4] = {0, 0, 0, 1};   // rebuild, drift pending/apply, gather every row
+  B(up(rebuild_flag(c), words, 4));
   ADC_CUDA(cudaDeviceSynchronize());
 #undef B
   *out = c;
