@@ -127,6 +127,7 @@ def load():
                                         C.c_int, C.c_double, C.c_int, C.c_int]),
         "adc_fort6x_append": (C.c_int, [C.c_char_p, C.c_double, C.c_int, C.c_int, dp_, dp_, ip_,
                                         C.c_double]),
+        "adc_selftest_div_const": (C.c_int, [C.c_longlong, C.c_ulonglong, C.POINTER(C.c_longlong)]),
         "adc_hotstart_write": (C.c_int, [vp, C.c_char_p]),
         "adc_hotstart_read": (C.c_int, [vp, C.c_char_p]),
         "adc_warm_start_stats": (C.c_int, [vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),

@@ -240,6 +240,31 @@ inline bool f32_spmv(const adc_ctx *c) { return c->prec & (ADC_PREC_MIXED | ADC_
 inline bool f32_momentum(const adc_ctx *c) { return c->prec & (ADC_PREC_MIXED | ADC_F32_MOMENTUM); }
 inline bool any_f32(const adc_ctx *c) { return f32_assembly(c) || f32_spmv(c) || f32_momentum(c); }
 
+// Correctly rounded division by a constant known in advance, after
+// Brisebarre, Muller and Raina, "Accelerating correctly rounded
+// floating-point division when the divisor is known in advance" (IEEE
+// Trans. Computers 53(8), 2004): with zh = RN(1/y), q = RN(x*zh) is
+// corrected once by the exact remainder r = x - q*y (one FMA) as
+// RN(q + r*zh).  For y = 3*2^k the exact quotient's significand has a
+// fractional part of 0, 1/3 or 2/3 ulp, never within 1/6 ulp of a rounding
+// midpoint, while the corrected value is within a tiny fraction of an ulp
+// of it, so the result is RN(x/y) for finite x in the normal range; an
+// exact quotient keeps q itself, so the sign of a zero is kept.  The
+// library's self-check (adc_selftest_div_const) compares it bit for bit
+// with IEEE division on 2^30 random and adversarial inputs per divisor.
+// It replaces full divisions in the FP64 element kernels' averages.
+__device__ __forceinline__ double div_known(double x, double y, double zh) {
+  const double q = x * zh;
+  const double r = fma(-q, y, x);
+  return r == 0.0 ? q : fma(r, zh, q);
+}
+__device__ __forceinline__ double div3(double x) { return div_known(x, 3.0, 1.0 / 3.0); }
+__device__ __forceinline__ double div6(double x) { return div_known(x, 6.0, 1.0 / 6.0); }
+__device__ __forceinline__ double div12(double x) { return div_known(x, 12.0, 1.0 / 12.0); }
+__device__ __forceinline__ float div3(float x) { return x / 3.0f; }
+__device__ __forceinline__ float div6(float x) { return x / 6.0f; }
+__device__ __forceinline__ float div12(float x) { return x / 12.0f; }
+
 // Stores K consecutive values per lane (lane l owns out[K*l .. K*l+K-1]
 // of the warp's span) as K coalesced 32-wide stores through shared memory
 // `sh` (32*K values per warp).  Every lane of the warp must call it;

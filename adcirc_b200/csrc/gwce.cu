@@ -366,39 +366,39 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 3 : 2) k_rhs_elem(adc_ct
   R Tau0YGrad2A = T0N1 * FDY1 + T0N2 * FDY2 + T0N3 * FDY3;
   R EVMXGrad = (EVMN1 * FDX1 + EVMN2 * FDX2 + EVMN3 * FDX3) / AreaIE2;
   R EVMYGrad = (EVMN1 * FDY1 + EVMN2 * FDY2 + EVMN3 * FDY3) / AreaIE2;
-  R EVMAvgODT = ((EVMN1 + EVMN2 + EVMN3) / R(3.0)) / DT;
+  R EVMAvgODT = (div3(EVMN1 + EVMN2 + EVMN3)) / DT;
   R MX = (EVMXGrad * (QX1N1 * FDX1 + QX1N2 * FDX2 + QX1N3 * FDX3) +
                EVMYGrad * (QY1N1 * FDX1 + QY1N2 * FDX2 + QY1N3 * FDX3) -
                EVMAvgODT * (ESN1 * FDX1 + ESN2 * FDX2 + ESN3 * FDX3)) / AreaIE2;
   R MY = (EVMXGrad * (QX1N1 * FDY1 + QX1N2 * FDY2 + QX1N3 * FDY3) +
                EVMYGrad * (QY1N1 * FDY1 + QY1N2 * FDY2 + QY1N3 * FDY3) -
                EVMAvgODT * (ESN1 * FDY1 + ESN2 * FDY2 + ESN3 * FDY3)) / AreaIE2;
-  R CorifAvg = (c.corif[n1] + c.corif[n2] + c.corif[n3]) / R(3.0);
-  R Tau0Avg = (T0N1 + T0N2 + T0N3) / R(3.0);
-  R Tau0QXAvg = (T0N1 * QX1N1 + T0N2 * QX1N2 + T0N3 * QX1N3) / R(3.0);
-  R Tau0QYAvg = (T0N1 * QY1N1 + T0N2 * QY1N2 + T0N3 * QY1N3) / R(3.0);
-  R U1Avg = (U1N1 + U1N2 + U1N3) / R(3.0);
-  R V1Avg = (V1N1 + V1N2 + V1N3) / R(3.0);
-  R QX1Avg = (QX1N1 + QX1N2 + QX1N3) / R(3.0);
-  R QY1Avg = (QY1N1 + QY1N2 + QY1N3) / R(3.0);
-  R ESAvg = (ESN1 + ESN2 + ESN3) / R(3.0);
-  R DPAvg = (c.dp[n1] + c.dp[n2] + c.dp[n3]) / R(3.0);
+  R CorifAvg = div3(c.corif[n1] + c.corif[n2] + c.corif[n3]);
+  R Tau0Avg = div3(T0N1 + T0N2 + T0N3);
+  R Tau0QXAvg = div3(T0N1 * QX1N1 + T0N2 * QX1N2 + T0N3 * QX1N3);
+  R Tau0QYAvg = div3(T0N1 * QY1N1 + T0N2 * QY1N2 + T0N3 * QY1N3);
+  R U1Avg = div3(U1N1 + U1N2 + U1N3);
+  R V1Avg = div3(V1N1 + V1N2 + V1N3);
+  R QX1Avg = div3(QX1N1 + QX1N2 + QX1N3);
+  R QY1Avg = div3(QY1N1 + QY1N2 + QY1N3);
+  R ESAvg = div3(ESN1 + ESN2 + ESN3);
+  R DPAvg = div3(c.dp[n1] + c.dp[n2] + c.dp[n3]);
   R al = c.alphal[e];
   R GDPAvgOAreaIE4 = al * G * DPAvg / AreaIE4;
   R GDPAvgOAreaIE4_S0 = GDPAvgOAreaIE4;   // DPAvgS0 == DPAvg when IFNL_HDP = 0
-  R HAvg = (H1N1 + H1N2 + H1N3) / R(3.0);
+  R HAvg = div3(H1N1 + H1N2 + H1N3);
   R GHAvg = al * G * HAvg;
   R GHAvgOAreaIE2 = GHAvg / AreaIE2;
-  R BSXAvg = (BSXN1 + BSXN2 + BSXN3) / R(3.0);
-  R BSYAvg = (BSYN1 + BSYN2 + BSYN3) / R(3.0);
+  R BSXAvg = div3(BSXN1 + BSXN2 + BSXN3);
+  R BSYAvg = div3(BSYN1 + BSYN2 + BSYN3);
   R WSXAvg = R(0.0), WSYAvg = R(0.0);
   if (met) {
-    WSXAvg = (c.wsx1[n1] + c.wsx1[n2] + c.wsx1[n3]) / R(3.0);
-    WSYAvg = (c.wsy1[n1] + c.wsy1[n2] + c.wsy1[n3]) / R(3.0);
+    WSXAvg = div3(c.wsx1[n1] + c.wsx1[n2] + c.wsx1[n3]);
+    WSYAvg = div3(c.wsy1[n1] + c.wsy1[n2] + c.wsy1[n3]);
   }
-  R MsFacR = AreaIE * (R(1.0) / DT - Tau0Avg / R(2.0)) / DT / R(12.0);
+  R MsFacR = div12(AreaIE * (R(1.0) / DT - Tau0Avg / R(2.0)) / DT);
   R GOAreaIE4 = al * G / AreaIE4;
-  R Tau0SpaVar = (QX1Avg * Tau0XGrad2A + QY1Avg * Tau0YGrad2A) / R(6.0);
+  R Tau0SpaVar = div6(QX1Avg * Tau0XGrad2A + QY1Avg * Tau0YGrad2A);
   R A00pB00 = A00 + B00;
   R fa = p.ifnlfa * GOAreaIE4;
   R JXAvg = CorifAvg * QY1Avg - fa * E1SQXGrad2A -

@@ -280,6 +280,11 @@ int adc_fort6x_append(const char *path, double timeloc, int it, int np, const do
 int adc_hotstart_write(adc_ctx *ctx, const char *path);
 int adc_hotstart_read(adc_ctx *ctx, const char *path);
 
+/* Self-check (no reference counterpart): counts, over n generated inputs
+ * per divisor, where the library's division by the constants 3, 6 and 12
+ * (used in the FP64 element kernels) differs in any bit from IEEE division. */
+int adc_selftest_div_const(long long n, unsigned long long seed, long long *mismatches);
+
 /* No reference counterpart (the reference always starts JCG from ETAS as
  * GWCE_New leaves it, gwce.F:2002-2004).  With ADC_WARM_START in the bind
  * mode, counts of the steps that started from the extrapolated guess and of
