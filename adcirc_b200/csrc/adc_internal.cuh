@@ -91,6 +91,8 @@ struct adc_ctx {
   int np, ne, mnei, neta, nbfr, nvel, nvelme, prec;
   int nslices, nnz_pad, n_obc, n_obc_rhs_nodes, n_me, itmax;
   adc_params_t p;
+  int dt_pow2;           // DT is a power of two (its reciprocal is exact)
+  double inv_dt;
   adc_arrays_t host;     // bound host arrays (for sync)
   cudaStream_t stream;
   // node data

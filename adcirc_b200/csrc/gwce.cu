@@ -304,6 +304,11 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 3 : 2) k_rhs_elem(adc_ct
   if (e >= c.ne) e = c.ne - 1;   // idle lanes recompute the last element; not stored
   const adc_params_t &p = c.p;
   const R DT = R(p.dt), G = R(p.g), A00 = R(p.a00), B00 = R(p.b00), C00 = R(p.c00);
+  // x / DT: with a power-of-two DT, the product with its exact reciprocal
+  // gives the same bits
+  const bool dt2 = c.dt_pow2 != 0;
+  const R IDT = R(c.inv_dt);
+  auto odt = [&](R x) { return dt2 ? x * IDT : x / DT; };
   int n1 = c.nm[3 * e], n2 = c.nm[3 * e + 1], n3 = c.nm[3 * e + 2];
   int NCEle = c.nodecode[n1] * c.nodecode[n2] * c.nodecode[n3] * c.noff[e];
   R E0N1 = c.eta1[n1], E0N2 = c.eta1[n2], E0N3 = c.eta1[n3];
@@ -366,7 +371,7 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 3 : 2) k_rhs_elem(adc_ct
   R Tau0YGrad2A = T0N1 * FDY1 + T0N2 * FDY2 + T0N3 * FDY3;
   R EVMXGrad = (EVMN1 * FDX1 + EVMN2 * FDX2 + EVMN3 * FDX3) / AreaIE2;
   R EVMYGrad = (EVMN1 * FDY1 + EVMN2 * FDY2 + EVMN3 * FDY3) / AreaIE2;
-  R EVMAvgODT = (div3(EVMN1 + EVMN2 + EVMN3)) / DT;
+  R EVMAvgODT = odt(div3(EVMN1 + EVMN2 + EVMN3));
   R MX = (EVMXGrad * (QX1N1 * FDX1 + QX1N2 * FDX2 + QX1N3 * FDX3) +
                EVMYGrad * (QY1N1 * FDX1 + QY1N2 * FDX2 + QY1N3 * FDX3) -
                EVMAvgODT * (ESN1 * FDX1 + ESN2 * FDX2 + ESN3 * FDX3)) / AreaIE2;
@@ -396,7 +401,7 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 3 : 2) k_rhs_elem(adc_ct
     WSXAvg = div3(c.wsx1[n1] + c.wsx1[n2] + c.wsx1[n3]);
     WSYAvg = div3(c.wsy1[n1] + c.wsy1[n2] + c.wsy1[n3]);
   }
-  R MsFacR = div12(AreaIE * (R(1.0) / DT - Tau0Avg / R(2.0)) / DT);
+  R MsFacR = div12(odt(AreaIE * ((dt2 ? IDT : R(1.0) / DT) - Tau0Avg / R(2.0))));
   R GOAreaIE4 = al * G / AreaIE4;
   R Tau0SpaVar = div6(QX1Avg * Tau0XGrad2A + QY1Avg * Tau0YGrad2A);
   R A00pB00 = A00 + B00;
@@ -409,10 +414,10 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 3 : 2) k_rhs_elem(adc_ct
                  BSYAvg + MY + Tau0QYAvg;
   JXAvg = JXAvg - p.ifnlct * (QX1Avg * (U1N1 * FDX1 + U1N2 * FDX2 + U1N3 * FDX3) +
                               QY1Avg * (U1N1 * FDY1 + U1N2 * FDY2 + U1N3 * FDY3)) / AreaIE2 +
-          p.ifnlcat * U1Avg * ESAvg / DT;
+          odt(p.ifnlcat * U1Avg * ESAvg);
   JYAvg = JYAvg - p.ifnlct * (QX1Avg * (V1N1 * FDX1 + V1N2 * FDX2 + V1N3 * FDX3) +
                               QY1Avg * (V1N1 * FDY1 + V1N2 * FDY2 + V1N3 * FDY3)) / AreaIE2 +
-          p.ifnlcat * V1Avg * ESAvg / DT;
+          odt(p.ifnlcat * V1Avg * ESAvg);
   R c0 = GDPAvgOAreaIE4_S0, c1 = GDPAvgOAreaIE4;
   R T1 = (2 * ESN1 + 1 * (ESN2 + ESN3)) * MsFacR -
               c0 * (C00 * (FDX1 * E0XGrad2A + FDY1 * E0YGrad2A)) -

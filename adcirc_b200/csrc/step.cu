@@ -460,6 +460,11 @@ static int bind_impl(const adc_params_t *p, const adc_arrays_t *a, int prec, adc
   *out = nullptr;
   c->np = a->np; c->ne = a->ne; c->mnei = a->mnei; c->neta = a->neta; c->nbfr = a->nbfr;
   c->nvel = a->nvel; c->nvelme = a->nvelme; c->prec = prec; c->itmax = p->itmax;
+  {
+    int ex = 0;
+    c->dt_pow2 = (p->dt > 0.0 && std::frexp(p->dt, &ex) == 0.5) ? 1 : 0;
+    c->inv_dt = 1.0 / p->dt;
+  }
   c->p = *p;
   c->host = *a;
   c->nslices = nslices;
