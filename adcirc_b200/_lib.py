@@ -41,7 +41,7 @@ ARRAY_FIELDS = [
     ("tau0var", dp_), ("evm", dp_), ("fric", dp_), ("corif", dp_),
     ("nbd", ip_), ("amig", dp_), ("per", dp_), ("face", dp_), ("ff", dp_),
     ("emo", dp_), ("efa", dp_), ("nbv", ip_), ("lbcodei", ip_), ("csii", dp_), ("siii", dp_),
-    ("me2gw", ip_),
+    ("me2gw", ip_), ("bndlen2o3", dp_),
     ("eta1", dp_), ("eta2", dp_), ("etas", dp_),
     ("uu1", dp_), ("vv1", dp_), ("uu2", dp_), ("vv2", dp_), ("qx1", dp_), ("qy1", dp_),
     ("qx2", dp_), ("qy2", dp_), ("h1", dp_), ("h2", dp_),
@@ -61,7 +61,13 @@ class AdcArrays(C.Structure):
 
 class AdcStep(C.Structure):
     _fields_ = [("it", C.c_int), ("pad_", C.c_int), ("timeloc", C.c_double),
-                ("timeh", C.c_double), ("rampelev", C.c_double), ("rampmete", C.c_double)]
+                ("timeh", C.c_double), ("rampelev", C.c_double), ("rampmete", C.c_double),
+                ("rampextflux", C.c_double)]
+
+
+class AdcFlux(C.Structure):
+    _fields_ = [("nffr", C.c_int), ("pad_", C.c_int)] + [
+        (n, dp_) for n in ("famig", "fper", "fff", "fface", "qnam", "qnph")]
 
 
 class AdcVortexFix(C.Structure):
@@ -99,7 +105,7 @@ def load():
         "adc_mesh_neighb": (C.c_int, [C.c_int, C.c_int, C.c_int, dp_, dp_, ip_, ip_, ip_, ip_]),
         "adc_mesh_csr_positions": (C.c_int, [C.c_int, C.c_int, C.c_int, ip_, ip_, C.c_int, ip_]),
         "adc_boundary_setup": (C.c_int, [C.c_int, dp_, dp_, C.c_int, ip_, ip_, ip_, C.c_double,
-                                          C.c_int, ip_, ip_, ip_, dp_, dp_, ip_, ip_]),
+                                          C.c_int, ip_, ip_, ip_, dp_, dp_, ip_, ip_, dp_]),
         "adc_coldstart": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_double, dp_, ip_, dp_, dp_,
                                      dp_, ip_, ip_, ip_, ip_, dp_]),
         "adc_jcg": (None, [ip_, ip_, ip_, ip_, dp_, dp_, dp_, ip_, ip_, dp_, ip_, dp_, ip_]),
@@ -119,6 +125,7 @@ def load():
         "adc_sync_from_host": (C.c_int, [vp]),
         "adc_set_met": (C.c_int, [vp, dp_, dp_, dp_]),
         "adc_set_vortex": (C.c_int, [vp, C.POINTER(AdcVortex)]),
+        "adc_set_flux": (C.c_int, [vp, C.POINTER(AdcFlux)]),
         "adc_fort14_dims": (C.c_int, [C.c_char_p, ip_]),
         "adc_fort14_read": (C.c_int, [C.c_char_p, C.c_char_p, dp_, dp_, dp_, ip_, ip_, ip_, ip_, ip_, ip_]),
         "adc_fort14_write": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int, C.c_int, dp_, dp_, dp_, ip_,

@@ -1,0 +1,177 @@
+// flux.cu -- specified normal flux boundaries (IBTYPE 2, 12, 22).
+//
+// Three pieces of the reference's flux-boundary path:
+//  * QN0 <- QN1 <- QN2 <- 0 (timestep.F:606-613), then QN2 as the sum of the
+//    periodic flux constituents (timestep.F:861-880; ICS = 1, so the normal
+//    flux is not rotated);
+//  * the GWCE boundary line integral (gwce.F:1737-1834): a force per
+//    boundary entry, then for each pair of consecutive entries a
+//    contribution to both nodes.  The reference adds these in entry order;
+//    here one thread per boundary node adds its contributions in that same
+//    order (a table built at bind lists them), so GWCE_LV gets the same bits;
+//  * the specified normal velocity -QN2/H2 of the momentum boundary
+//    conditions (momentum.F:815-856), read in k_mom_node.
+#include "adc_internal.cuh"
+
+#include <cstring>
+#include <vector>
+
+namespace adc {
+
+__global__ void k_flux_forcing(adc_ctx c, const adc_step_t *steps, const Flags *flags) {
+  griddep_wait();
+  const int I = blockIdx.x * blockDim.x + threadIdx.x;
+  if (I >= c.nvel) return;
+  double *qn0 = c.qn, *qn1 = c.qn + c.nvel, *qn2 = c.qn + 2 * c.nvel;
+  qn0[I] = qn1[I];
+  qn1[I] = qn2[I];
+  double q = 0.0;
+  const int lb = c.blbc[I];
+  if (c.flux_on && (lb == 2 || lb == 12 || lb == 22)) {
+    const adc_step_t st = steps[flags->cursor];
+    const int nf = c.nffr;
+    const double *famig = c.fconst, *fper = famig + nf, *fff = fper + nf, *fface = fff + nf;
+    const double *qnam = c.fqn, *qnph = c.fqn + (size_t)nf * c.nvel;
+    for (int J = 0; J < nf; ++J) {
+      int NCYC = 0;
+      if (fper[J] != 0.0) NCYC = (int)(st.timeh / fper[J]);
+      const double ARGJ = famig[J] * (st.timeh - NCYC * fper[J]) + fface[J];
+      const double RFF = fff[J] * st.rampextflux;
+      q = q + qnam[J + (size_t)nf * I] * RFF * cos(ARGJ - qnph[J + (size_t)nf * I]);
+    }
+  }
+  qn2[I] = q;
+}
+
+// The force of each boundary entry (LBCODEI <= 29 types, gwce.F:1783).
+__global__ void k_flux_qforce(adc_ctx c) {
+  griddep_wait();
+  const int J = blockIdx.x * blockDim.x + threadIdx.x;
+  if (J >= c.nvel) return;
+  const double *qn0 = c.qn, *qn1 = c.qn + c.nvel, *qn2 = c.qn + 2 * c.nvel;
+  const double DT2 = c.p.dt * 2.0;
+  c.qforce[J] = (qn2[J] - qn0[J]) / DT2 + c.tau0[c.bnv[J]] * qn1[J];
+}
+
+// One thread per boundary node: its contributions in entry order.
+__global__ void k_flux_rhs(adc_ctx c) {
+  griddep_wait();
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= c.n_fx) return;
+  const int n = c.fx_node[k];
+  double v = c.gwce_lv[n];
+  for (int q = c.fx_ptr[k]; q < c.fx_ptr[k + 1]; ++q) {
+    const int ent = c.fx_ent[q], j = ent >> 1;
+    const int NCI = c.nodecode[c.bnv[j - 1]], NCJ = c.nodecode[c.bnv[j]];
+    const double B = NCI * NCJ * c.bbl[j - 1] / 4.0;
+    const double qi = c.qforce[j - 1], qj = c.qforce[j];
+    if ((ent & 1) == 0) v = v + B * (2.0 * qi + qj);   // the segment's first node
+    else v = v + B * (2.0 * qj + qi);                  // its second node
+  }
+  c.gwce_lv[n] = v;
+}
+
+int launch_flux_forcing(adc_ctx *c) {
+  if (!c->nfluxf) return ADC_OK;
+  launch_k(k_flux_forcing, nblk(c->nvel), kThreads, c->stream, *c, c->steps, c->flags);
+  c->launches++;
+  return ADC_OK;
+}
+
+int launch_flux_rhs(adc_ctx *c) {
+  if (!c->nfluxf) return ADC_OK;
+  launch_k(k_flux_qforce, nblk(c->nvel), kThreads, c->stream, *c);
+  launch_k(k_flux_rhs, nblk(c->n_fx), kThreads, c->stream, *c);
+  c->launches += 2;
+  return ADC_OK;
+}
+
+// Bind-time tables: boundary entries, and per boundary node the ordered
+// list of (segment, side) contributions of the GWCE line integral.
+int flux_tables(adc_ctx *c, const adc_arrays_t *a) {
+  const int nv = a->nvel;
+  c->nvel = nv;
+  c->nfluxf = 0;
+  for (int I = 0; I < nv; ++I) {
+    const int lb = a->lbcodei[I];
+    if (lb == 2 || lb == 12 || lb == 22) c->nfluxf = 1;
+    if (lb == 30 || lb == 32 || lb == 40 || lb == 41 || lb == 52 || lb == 64) {
+      set_error("boundary code %d (radiation, zero-gradient or river-radiation flux) is not "
+                "implemented", lb);
+      return ADC_ERR_UNSUPPORTED;
+    }
+  }
+  const size_t nva = (size_t)(nv > 0 ? nv : 1);
+  ADC_CUDA(cudaMalloc((void **)&c->qn, 3 * nva * sizeof(double)));
+  ADC_CUDA(cudaMemset(c->qn, 0, 3 * nva * sizeof(double)));
+  if (!c->nfluxf) return ADC_OK;
+  std::vector<int> bnv(nv);
+  for (int I = 0; I < nv; ++I) bnv[I] = a->nbv[I] - 1;
+  std::vector<std::vector<int>> lists(c->np);
+  std::vector<int> order;
+  auto add = [&](int node, int ent) {
+    if (lists[node].empty()) order.push_back(node);
+    lists[node].push_back(ent);
+  };
+  for (int j = 1; j < nv; ++j) {
+    add(bnv[j - 1], j << 1);
+    add(bnv[j], (j << 1) | 1);
+  }
+  std::vector<int> ptr(1, 0), ent;
+  for (int n : order) {
+    ent.insert(ent.end(), lists[n].begin(), lists[n].end());
+    ptr.push_back((int)ent.size());
+  }
+  c->n_fx = (int)order.size();
+  auto up_i = [&](int **d, const std::vector<int> &h) -> int {
+    ADC_CUDA(cudaMalloc((void **)d, std::max<size_t>(h.size(), 1) * sizeof(int)));
+    if (!h.empty()) ADC_CUDA(cudaMemcpy(*d, h.data(), h.size() * sizeof(int), cudaMemcpyHostToDevice));
+    return ADC_OK;
+  };
+  int rc;
+  if ((rc = up_i(&c->bnv, bnv))) return rc;
+  if ((rc = up_i(&c->blbc, std::vector<int>(a->lbcodei, a->lbcodei + nv)))) return rc;
+  if ((rc = up_i(&c->fx_node, order))) return rc;
+  if ((rc = up_i(&c->fx_ptr, ptr))) return rc;
+  if ((rc = up_i(&c->fx_ent, ent))) return rc;
+  ADC_CUDA(cudaMalloc((void **)&c->bbl, nva * sizeof(double)));
+  ADC_CUDA(cudaMemcpy(c->bbl, a->bndlen2o3, nv * sizeof(double), cudaMemcpyHostToDevice));
+  ADC_CUDA(cudaMalloc((void **)&c->qforce, nva * sizeof(double)));
+  return ADC_OK;
+}
+
+}  // namespace adc
+
+using namespace adc;
+
+extern "C" int adc_set_flux(adc_ctx *c, const adc_flux_t *f) {
+  if (!c || !f || f->nffr < 1 || !f->famig || !f->fper || !f->fff || !f->fface || !f->qnam ||
+      !f->qnph) {
+    set_error("adc_set_flux: at least one flux constituent and every table are required");
+    return ADC_ERR_ARG;
+  }
+  if (!c->nfluxf) {
+    set_error("adc_set_flux: the mesh has no specified-flux boundary (IBTYPE 2, 12 or 22)");
+    return ADC_ERR_ARG;
+  }
+  const int nf = f->nffr, nv = c->nvel;
+  std::vector<double> cst(4 * (size_t)nf);
+  std::memcpy(cst.data(), f->famig, nf * sizeof(double));
+  std::memcpy(cst.data() + nf, f->fper, nf * sizeof(double));
+  std::memcpy(cst.data() + 2 * nf, f->fff, nf * sizeof(double));
+  std::memcpy(cst.data() + 3 * nf, f->fface, nf * sizeof(double));
+  if (c->fconst) cudaFree(c->fconst);
+  if (c->fqn) cudaFree(c->fqn);
+  c->fconst = nullptr;
+  c->fqn = nullptr;
+  ADC_CUDA(cudaMalloc((void **)&c->fconst, cst.size() * sizeof(double)));
+  ADC_CUDA(cudaMemcpy(c->fconst, cst.data(), cst.size() * sizeof(double), cudaMemcpyHostToDevice));
+  ADC_CUDA(cudaMalloc((void **)&c->fqn, 2 * (size_t)nf * nv * sizeof(double)));
+  ADC_CUDA(cudaMemcpy(c->fqn, f->qnam, (size_t)nf * nv * sizeof(double), cudaMemcpyHostToDevice));
+  ADC_CUDA(cudaMemcpy(c->fqn + (size_t)nf * nv, f->qnph, (size_t)nf * nv * sizeof(double),
+                      cudaMemcpyHostToDevice));
+  c->nffr = nf;
+  c->flux_on = 1;
+  drop_graphs(c);   // replayed steps must see the forcing
+  return ADC_OK;
+}

@@ -6,7 +6,8 @@
 // this library's own: it holds every array and scalar the device step
 // carries from one step to the next (state fields, the GWCE matrix and EP,
 // ITPACK's persistent scalars, the pending unscal drift, the vortex track
-// state and the warm-start history), so N steps equal N/2 steps, a dump, a
+// state, the specified boundary fluxes of the last two steps and the
+// warm-start history), so N steps equal N/2 steps, a dump, a
 // load into a freshly bound context of the same mesh and mode, and N/2
 // more steps, bit for bit.
 //
@@ -59,6 +60,7 @@ static std::vector<HsRec> hs_records(adc_ctx *c) {
       {"itpack", c->itp, sizeof(Itp)},
   };
   if (c->vortex_on) r.push_back({"vortex", c->vstate, sizeof(VortexState)});
+  if (c->nfluxf) r.push_back({"flux_qn", c->qn, 3 * (size_t)c->nvel * d});
   if (c->prec & ADC_WARM_START) {
     r.push_back({"etas_prev", c->etas_prev, np * d});
     r.push_back({"warm", c->warm, sizeof(WarmState)});

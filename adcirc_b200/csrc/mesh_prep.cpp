@@ -11,7 +11,7 @@
  *   adc_mesh_mnei          mesh.F:1712-1726   MNEI = max element count + 2
  *   adc_mesh_neighb        mesh.F:3089-3318   NeiTab sorted by angle, NNeigh
  *   adc_mesh_csr_positions mesh.F:5261-5282   CSR_POSITION(NE,3,2)
- *   adc_boundary_setup     mesh.F:2100-2800   NBV, LBCODEI, CSII, SIII, ME2GW
+ *   adc_boundary_setup     mesh.F:2100-2800   NBV, LBCODEI, CSII, SIII, ME2GW, BNDLEN2O3
  *
  * All arrays use the reference layout: column-major, 1-based node numbers.
  */
@@ -176,13 +176,16 @@ int adc_boundary_setup(int np, const double *x, const double *y, int nbou,
                        const int *ibtype, const int *seg_ptr, const int *seg_nodes,
                        double cos_inner, int nvel_max, int *nvel_out, int *nbv,
                        int *lbcodei, double *csii, double *siii, int *nvelme_out,
-                       int *me2gw) {
+                       int *me2gw, double *bndlen2o3) {
   int jgw = 0, jme = 0;
+  /* specified-flow types take the momentum equation where segments overlap */
+  auto specified_flow = [](int code) { return code == 2 || code == 12 || code == 22; };
   for (int k = 0; k < nbou; ++k) {
     int t = ibtype[k];
     bool island = (t == 1 || t == 11 || t == 21);
     bool mainland = (t == 0 || t == 10 || t == 20);
-    if (!island && !mainland) return ADC_ERR_ARG;
+    bool flux = specified_flow(t);   /* external boundaries with normal flow */
+    if (!island && !mainland && !flux) return ADC_ERR_ARG;
     std::vector<int> nbvv;
     int nvell = seg_ptr[k + 1] - seg_ptr[k];
     if (nvell < 2) return ADC_ERR_ARG;
@@ -235,18 +238,29 @@ int adc_boundary_setup(int np, const double *x, const double *y, int nbou,
       if (costheta > cos_inner && cross > 0.0) {
         if (t == 0) lbcodei[jgw - 1] = 10;
         if (t == 1) lbcodei[jgw - 1] = 11;
+        if (t == 2) lbcodei[jgw - 1] = 12;
+      }
+      /* 2/3 of the segment to the next node, mesh.F:2301-2303 (zero after
+         the last node of an unclosed segment) */
+      if (bndlen2o3) {
+        const double delx = xgj - xgi, dely = ygj - ygi;
+        bndlen2o3[jgw - 1] = 2.0 * (std::sqrt(delx * delx + dely * dely)) / 3.0;
       }
       double xl = std::sqrt((xgk - xgj) * (xgk - xgj) + (ygk - ygj) * (ygk - ygj));
       csii[jgw - 1] = 1.0 * (ygj - ygk) / xl;
       siii[jgw - 1] = (xgk - xgj) / xl;
-      /* momentum-equation key, mesh.F:2516-2568 (no specified-flow types here) */
+      /* momentum-equation key, mesh.F:2516-2568: a node shared by two
+         segments keeps one entry, the specified-flow one if there is one */
       if (i == 1) {
         if (jgw == 1) { jme++; me2gw[jme - 1] = jgw; }
         if (jgw != 1 && nbv[jgw - 1] != nbv[jgw - 2]) { jme++; me2gw[jme - 1] = jgw; }
+        if (jgw != 1 && nbv[jgw - 1] == nbv[jgw - 2] && specified_flow(lbcodei[jgw - 1]) && jme > 0)
+          me2gw[jme - 1] = jgw;
       }
       if (i > 1 && i < nvell) { jme++; me2gw[jme - 1] = jgw; }
       if (i == nvell) {
         if (nbv[jgw - 1] != nbvv[1] && nbv[jgw - 1] != nbv[0]) { jme++; me2gw[jme - 1] = jgw; }
+        if (nbvv[i] == nbv[0] && specified_flow(lbcodei[jgw - 1])) me2gw[0] = jgw;
       }
     }
   }

@@ -181,8 +181,9 @@ __global__ void k_mom_node(adc_ctx c) {
   if (me >= 0) {
     int lb = c.me_lbc[me];
     double csi = c.me_csi[me], sii = c.me_sii[me];
+    const double qn2 = c.qn[2 * c.nvel + c.me_i[me]];   // zero on land boundaries
     if (lb >= 0 && lb <= 9) {
-      double VelNorm = -0.0 / c.h2[i];   // -QN2/H2 with QN2 = 0 (land)
+      double VelNorm = -qn2 / c.h2[i];
       if (fabs(norm2_3(tkm) - sqrt(2.0) * c.tk[i]) < DBL_EPSILON) {
         mx = (sii * mx - csi * my - VelNorm * a3) * NCI;
         my = VelNorm * a1 * NCI;
@@ -202,7 +203,7 @@ __global__ void k_mom_node(adc_ctx c) {
       }
     }
     if (lb >= 10 && lb <= 19) {
-      double VelNorm = -0.0 / c.h2[i];
+      double VelNorm = -qn2 / c.h2[i];
       mx = 0.0 * NCI;
       my = VelNorm * NCI;
       a1 = sii;

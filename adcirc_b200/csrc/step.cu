@@ -59,6 +59,9 @@ __global__ void k_step_end(Flags *f, int *numitr_log, int cap) {
 static int *rebuild_flag(adc_ctx *c) { return (int *)(c->flags + 1); }
 
 int launch_met_vortex(adc_ctx *c);
+int launch_flux_forcing(adc_ctx *c);
+int launch_flux_rhs(adc_ctx *c);
+int flux_tables(adc_ctx *c, const adc_arrays_t *a);
 int launch_warm_start(adc_ctx *c);
 
 int launch_shift_friction(adc_ctx *c) {
@@ -70,7 +73,7 @@ int launch_shift_friction(adc_ctx *c) {
     launch_k(k_apply_met, nblk(c->np), kThreads, c->stream, *c);
     c->launches++;
   }
-  return ADC_OK;
+  return launch_flux_forcing(c);   // timestep.F:606-613 and 861-880, after the met forcing
 }
 
 int launch_gwce_lhs(adc_ctx *c) {
@@ -100,6 +103,8 @@ int launch_gwce_rhs(adc_ctx *c) {
     launch_k(k_rhs_gather<double>, nblk(c->np), kThreads, c->stream, *c);
   }
   c->launches += 2;
+  int rc = launch_flux_rhs(c);   // gwce.F:1737-1834, before the elevation rows
+  if (rc) return rc;
   if (c->neta > 0) {
     launch_k(k_eta_bc, nblk(c->neta), kThreads, c->stream, *c, c->steps, c->flags);
     c->launches++;
@@ -165,7 +170,7 @@ static int down(T *h, const T *d, size_t n) {
 struct HostTables {
   std::vector<int> nm, n2e_ptr, n2e, sl_ptr, sl_w, col, rlen, lhs_src, ell_of_sell;
   std::vector<int> is_nbd, nbd, obc_slot, obc_zero, obc_rhs_ptr, obc_rhs_node, obc_rhs_ent,
-      obc_rhs_b, me_of_node, me_lbc;
+      obc_rhs_b, me_of_node, me_lbc, me_i;
   std::vector<double> me_csi, me_sii;
   std::vector<int> sell_of_ell;   // ELL (i + np*j), j >= 1 -> SELL idx or -1
 };
@@ -285,6 +290,7 @@ static int build_tables(const adc_arrays_t *a, HostTables &T, int &nslices, int 
     if (T.me_of_node[node] >= 0) { set_error("node %d has two momentum BC entries", node + 1); return ADC_ERR_MESH; }
     T.me_of_node[node] = J;
     T.me_lbc.push_back(a->lbcodei[I]);
+    T.me_i.push_back(I);
     T.me_csi.push_back(a->csii[I]);
     T.me_sii.push_back(a->siii[I]);
   }
@@ -407,7 +413,9 @@ static void free_ctx(adc_ctx *c) {
       (void **)&c->emo, (void **)&c->efa, (void **)&c->obc_slot, (void **)&c->obc_zero,
       (void **)&c->obc_rhs_ptr, (void **)&c->obc_rhs_node, (void **)&c->obc_rhs_ent,
       (void **)&c->obc_rhs_b, (void **)&c->me_of_node, (void **)&c->me_lbc,
-      (void **)&c->me_csi, (void **)&c->me_sii, (void **)&c->eta1, (void **)&c->eta2,
+      (void **)&c->me_csi, (void **)&c->me_sii, (void **)&c->me_i, (void **)&c->qn,
+      (void **)&c->qforce, (void **)&c->fconst, (void **)&c->fqn, (void **)&c->bnv, (void **)&c->blbc,
+      (void **)&c->bbl, (void **)&c->fx_node, (void **)&c->fx_ptr, (void **)&c->fx_ent, (void **)&c->eta1, (void **)&c->eta2,
       (void **)&c->etas, (void **)&c->uu1, (void **)&c->vv1, (void **)&c->uu2, (void **)&c->vv2,
       (void **)&c->qx1, (void **)&c->qy1, (void **)&c->qx2, (void **)&c->qy2, (void **)&c->h1,
       (void **)&c->h2, (void **)&c->tk, (void **)&c->tkm, (void **)&c->totalarea,
@@ -539,6 +547,8 @@ static int bind_impl(const adc_params_t *p, const adc_arrays_t *a, int prec, adc
   B(dalloc(&c->obc_rhs_ent, std::max<size_t>(T.obc_rhs_ent.size(), 1))); B(up(c->obc_rhs_ent, T.obc_rhs_ent.data(), T.obc_rhs_ent.size()));
   B(dalloc(&c->obc_rhs_b, std::max<size_t>(T.obc_rhs_b.size(), 1))); B(up(c->obc_rhs_b, T.obc_rhs_b.data(), T.obc_rhs_b.size()));
   B(dalloc(&c->me_of_node, np)); B(up(c->me_of_node, T.me_of_node.data(), np));
+  B(dalloc(&c->me_i, std::max<size_t>(T.me_i.size(), 1))); B(up(c->me_i, T.me_i.data(), T.me_i.size()));
+  B(flux_tables(c, a));
   B(dalloc(&c->me_lbc, std::max<size_t>(T.me_lbc.size(), 1))); B(up(c->me_lbc, T.me_lbc.data(), T.me_lbc.size()));
   B(dalloc(&c->me_csi, std::max<size_t>(T.me_csi.size(), 1))); B(up(c->me_csi, T.me_csi.data(), T.me_csi.size()));
   B(dalloc(&c->me_sii, std::max<size_t>(T.me_sii.size(), 1))); B(up(c->me_sii, T.me_sii.data(), T.me_sii.size()));

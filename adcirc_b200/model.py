@@ -38,6 +38,7 @@ class Schedule:
     dramp: float = 0.5       # days (elevation ramp, DRampElev)
     dramp_mete: float = 0.5  # days
     dunramp_mete: float = 0.0
+    dramp_extflux: float | None = None   # days; None: the elevation ramp's
 
     def step(self, it: int) -> AdcStep:
         timeloc = it * self.dt + self.statim * 86400.0
@@ -57,6 +58,11 @@ class Schedule:
         s.timeh = timeh
         s.rampelev = relev
         s.rampmete = rmete
+        dfx = self.dramp if self.dramp_extflux is None else self.dramp_extflux
+        if self.nramp == 0 or dfx < 1.0e-6:
+            s.rampextflux = 1.0
+        else:
+            s.rampextflux = math.tanh((2.0 * timeloc / 86400.0) / dfx)
         return s
 
     def steps(self, it0: int, n: int):
@@ -75,6 +81,7 @@ class Case:
     schedule: Schedule
     meta: dict = dataclasses.field(default_factory=dict)
     vortex: "Vortex | None" = None   # NWS = 8 parametric-vortex track
+    flux: "Flux | None" = None       # specified normal flux (IBTYPE 2/12/22)
 
     def clone(self) -> "Case":
         c = copy.copy(self)
@@ -101,6 +108,31 @@ class Case:
 
     def state(self):
         return {k: self.arrays[k] for k in STATE_F64 + STATE_I32}
+
+
+@dataclasses.dataclass
+class Flux:
+    """Periodic specified normal flux on the flux boundaries (IBTYPE 2, 12,
+    22): constituents (rad/s, s, nodal factor, rad) and per boundary entry
+    (NVEL) amplitudes [m^2/s] and phases [rad], zero off flux entries."""
+    famig: np.ndarray
+    fper: np.ndarray
+    fff: np.ndarray
+    fface: np.ndarray
+    qnam: np.ndarray   # (NFFR, NVEL)
+    qnph: np.ndarray   # (NFFR, NVEL)
+
+    def struct(self, cls=None):
+        """(struct, backing arrays); keep both alive while in use."""
+        cls = cls or _lib.AdcFlux
+        keep = [np.ascontiguousarray(a, np.float64) for a in (self.famig, self.fper, self.fff,
+                                                                self.fface)]
+        keep += [np.asfortranarray(a, np.float64) for a in (self.qnam, self.qnph)]
+        f = cls()
+        f.nffr = int(keep[0].size)
+        for name, a in zip(("famig", "fper", "fff", "fface", "qnam", "qnph"), keep):
+            setattr(f, name, a.ctypes.data_as(dp_))
+        return f, keep
 
 
 @dataclasses.dataclass
@@ -215,13 +247,14 @@ def build_case(raw, params: dict, schedule: Schedule, tides, cf: float = 0.0025,
     csii = np.zeros(nvel_max, np.float64)
     siii = np.zeros(nvel_max, np.float64)
     me2gw = np.zeros(nvel_max, np.int32)
+    bndlen = np.zeros(nvel_max, np.float64)
     nvel = C.c_int(0)
     nvelme = C.c_int(0)
     rc = lib.adc_boundary_setup(npn, ptr(x, dp_), ptr(y, dp_), len(segs), ptr(ibtype, ip_),
                                 ptr(seg_ptr, ip_), ptr(seg_nodes, ip_),
                                 math.cos(anginn * math.pi / 180.0), nvel_max, C.byref(nvel),
                                 ptr(nbv, ip_), ptr(lbc, ip_), ptr(csii, dp_), ptr(siii, dp_),
-                                C.byref(nvelme), ptr(me2gw, ip_))
+                                C.byref(nvelme), ptr(me2gw, ip_), ptr(bndlen, dp_))
     if rc != 0:
         raise RuntimeError(f"adc_boundary_setup failed: {rc}")
     nv, nme = nvel.value, nvelme.value
@@ -247,6 +280,7 @@ def build_case(raw, params: dict, schedule: Schedule, tides, cf: float = 0.0025,
         nbv=_f(nbv[:max(nv, 1)], np.int32), lbcodei=_f(lbc[:max(nv, 1)], np.int32),
         csii=_f(csii[:max(nv, 1)], np.float64), siii=_f(siii[:max(nv, 1)], np.float64),
         me2gw=_f(me2gw[:max(nme, 1)], np.int32),
+        bndlen2o3=_f(bndlen[:max(nv, 1)], np.float64),
     )
     for k in STATE_F64:
         A[k] = np.zeros(npn, np.float64)
@@ -284,18 +318,35 @@ M2_PERIOD = 44712.0
 K1_PERIOD = 86164.0
 
 
-def channel_case(dt: float = 5.0, amp: float = 0.5, vortex: bool = False, **kw) -> Case:
+def channel_case(dt: float = 5.0, amp: float = 0.5, vortex: bool = False,
+                 river: float | None = None, river_type: int = 2, **kw) -> Case:
     """Tidal channel: 121x41 nodes, 20 m -> 5 m, M2 0.5 m, dt 5 s.  With
-    `vortex`, a small Holland vortex (Rmax 8 km) crosses the channel."""
+    `vortex`, a small Holland vortex (Rmax 8 km) crosses the channel.  With
+    `river` [m^2/s per unit width], the closed east end becomes a
+    specified-flux boundary (IBTYPE `river_type`, 2 or 22) carrying that
+    steady inflow, ramped in over 0.02 days."""
     from .meshgen import channel_mesh
     raw = channel_mesh()
+    if river is not None:
+        nx, ny = 121, 41
+        nid = lambda i, j: i * ny + j
+        south = np.array([nid(i, 0) for i in range(nx)])
+        east = np.array([nid(nx - 1, j) for j in range(ny)])
+        north = np.array([nid(i, ny - 1) for i in range(nx - 1, -1, -1)])
+        raw.land_segments = [(0, south), (river_type, east), (0, north)]
     neta = raw.open_nodes.size
     tides = [(2.0 * math.pi / M2_PERIOD, 0.0, 1.0, np.full(neta, amp), np.zeros(neta))]
     if vortex:
         kw.setdefault("nws", 8)
     params = default_params(dt, **kw)
-    sched = Schedule(dt=dt, dramp=0.5, dramp_mete=0.02 if vortex else 0.5)
+    sched = Schedule(dt=dt, dramp=0.5, dramp_mete=0.02 if vortex else 0.5, dramp_extflux=0.02)
     case = build_case(raw, params, sched, tides)
+    if river is not None:
+        lbc = case.arrays["lbcodei"]
+        nv = lbc.size
+        qnam = np.zeros((1, nv))
+        qnam[0, (lbc == 2) | (lbc == 12) | (lbc == 22)] = river
+        case.flux = Flux(np.zeros(1), np.zeros(1), np.ones(1), np.zeros(1), qnam, np.zeros((1, nv)))
     if vortex:
         case.vortex = straight_track(30.3e3, 3.7e3, 80.0, 6.0, 960.0, 8.0, 1.3, hours=12.0,
                                      interval_h=3.0)
@@ -369,6 +420,9 @@ class GpuModel:
         if case.vortex is not None:
             v, arr = case.vortex.struct()
             _check(self.lib.adc_set_vortex(self.h, C.byref(v)), "adc_set_vortex")
+        if case.flux is not None:
+            f, keep = case.flux.struct()
+            _check(self.lib.adc_set_flux(self.h, C.byref(f)), "adc_set_flux")
 
     def close(self):
         if self.h:

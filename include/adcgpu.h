@@ -9,8 +9,9 @@
  * extern "C" with plain pointers so a Fortran host binds it through
  * ISO_C_BINDING (include/adcgpu_iface.F90) and Python through ctypes.
  *
- * No entry point allocates on behalf of the caller except adc_gpu_bind
- * (device mirrors) and adc_jcg (device staging for one solve).  Errors are
+ * Entry points that allocate device memory: adc_gpu_bind (device mirrors),
+ * adc_set_vortex and adc_set_flux (forcing tables), adc_jcg (staging for one
+ * solve) and the self-check; adc_jcg_noalloc allocates nothing.  Errors are
  * returned as status codes; the library never calls exit().
  */
 #ifndef ADCGPU_H
@@ -83,6 +84,7 @@ typedef struct {
   const int *nbv, *lbcodei;      /* (NVEL) */
   const double *csii, *siii;     /* (NVEL) */
   const int *me2gw;              /* (NVELME) */
+  const double *bndlen2o3;       /* (NVEL) 2/3 of each boundary segment's length */
   double *eta1, *eta2, *etas;
   double *uu1, *vv1, *uu2, *vv2, *qx1, *qy1, *qx2, *qy2, *h1, *h2;
   double *tk, *tkm;              /* TK(NP), TKM(3,NP) */
@@ -99,7 +101,21 @@ typedef struct {
   int it;
   int pad_;
   double timeloc, timeh, rampelev, rampmete;
+  double rampextflux;    /* RampExtFlux, the ramp of specified boundary fluxes */
 } adc_step_t;
+
+/* Periodic specified normal flux on flux boundaries (IBTYPE 2, 12, 22):
+ * the fort.15 flux constituents timestep.F:861-880 sums each step. */
+typedef struct {
+  int nffr;              /* NFFR > 0 constituents */
+  int pad_;
+  const double *famig;   /* FAMIG(NFFR), rad/s */
+  const double *fper;    /* FPER(NFFR), s (0: no whole-period removal) */
+  const double *fff;     /* FFF(NFFR), nodal factors */
+  const double *fface;   /* FFACE(NFFR), rad */
+  const double *qnam;    /* QNAM(NFFR,NVEL), normal flux per unit width, m^2/s */
+  const double *qnph;    /* QNPH(NFFR,NVEL), rad */
+} adc_flux_t;
 
 /* One fix of a parametric-vortex track: the fields of a fort.22 best-track
  * line that HollandGet consumes (nws08.F90:827-878), in mesh units.  The
@@ -285,6 +301,15 @@ int adc_hotstart_read(adc_ctx *ctx, const char *path);
  * (used in the FP64 element kernels) differs in any bit from IEEE division. */
 int adc_selftest_div_const(long long n, unsigned long long seed, long long *mismatches);
 
+/* Specified normal flux (NFLUXF = 1, IBTYPE 2/12/22 with NFFR > 0): uploads
+ * the flux constituents once; every later step forms QN2 on the device
+ * (timestep.F:861-880) after shifting QN0 <- QN1 <- QN2 (timestep.F:606-613),
+ * the GWCE gains the boundary flux integral (gwce.F:1737-1834) and the
+ * momentum equation the specified normal velocity -QN2/H2 (momentum.F:
+ * 815-856).  Without a call the fluxes stay zero.  ADC_ERR_ARG if the mesh
+ * has no flux boundary or nffr < 1. */
+int adc_set_flux(adc_ctx *ctx, const adc_flux_t *flux);
+
 /* No reference counterpart (the reference always starts JCG from ETAS as
  * GWCE_New leaves it, gwce.F:2002-2004).  With ADC_WARM_START in the bind
  * mode, counts of the steps that started from the extrapolated guess and of
@@ -319,7 +344,7 @@ int adc_boundary_setup(int np, const double *x, const double *y, int nbou,
                        const int *ibtype, const int *seg_ptr, const int *seg_nodes,
                        double cos_inner, int nvel_max, int *nvel, int *nbv,
                        int *lbcodei, double *csii, double *siii, int *nvelme,
-                       int *me2gw);
+                       int *me2gw, double *bndlen2o3);
 /* Cold-start wet/dry state (cstart.F:1332-1427) and totalAreaCalc
  * (mesh.F:3360-3400). */
 int adc_coldstart(int np, int ne, int nolifa, double h0, const double *dp, const int *nm,

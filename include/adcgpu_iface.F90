@@ -28,6 +28,7 @@ module adcgpu_iface
       type(c_ptr) :: x, y, dp, nm, nneigh, neitab, fdxe, fdye, areas, csr_position
       type(c_ptr) :: tau0var, evm, fric, corif
       type(c_ptr) :: nbd, amig, per, face, ff, emo, efa, nbv, lbcodei, csii, siii, me2gw
+      type(c_ptr) :: bndlen2o3
       type(c_ptr) :: eta1, eta2, etas, uu1, vv1, uu2, vv2, qx1, qy1, qx2, qy2, h1, h2
       type(c_ptr) :: tk, tkm, nodecode, nnodecode, noff, mju, totalarea, alphal
       type(c_ptr) :: wsx1, wsy1, wsx2, wsy2, pr1, pr2, coef, obccoef
@@ -36,7 +37,12 @@ module adcgpu_iface
 
    type, bind(C), public :: adc_step_t
       integer(c_int) :: it, pad_
-      real(c_double) :: timeloc, timeh, rampelev, rampmete
+      real(c_double) :: timeloc, timeh, rampelev, rampmete, rampextflux
+   end type
+
+   type, bind(C), public :: adc_flux_t
+      integer(c_int) :: nffr, pad_
+      type(c_ptr) :: famig, fper, fff, fface, qnam, qnph
    end type
 
    type, bind(C), public :: adc_stepout_t
@@ -61,7 +67,7 @@ module adcgpu_iface
    public :: adc_jcg, adc_dfault, adc_gpu_bind, adc_gpu_free, adc_shift_friction, &
              adc_gwce_new, adc_wetdry, adc_momentum, adc_timestep, adc_sync_to_host, &
              adc_sync_from_host, adc_set_met, adc_set_vortex, adc_hotstart_write, &
-             adc_hotstart_read
+             adc_hotstart_read, adc_set_flux
 
    interface
       ! drop-in for ITPACK jcg (itpackv.F:63): identical argument list
@@ -146,6 +152,13 @@ module adcgpu_iface
          import :: c_int, c_ptr, adc_vortex_t
          type(c_ptr), value :: ctx
          type(adc_vortex_t), intent(in) :: v
+      end function
+
+      ! periodic specified normal flux (timestep.F:861-880)
+      integer(c_int) function adc_set_flux(ctx, f) bind(C, name="adc_set_flux")
+         import :: c_int, c_ptr, adc_flux_t
+         type(c_ptr), value :: ctx
+         type(adc_flux_t), intent(in) :: f
       end function
 
       ! hotstart dump/load (write_output.F:4429-5582, hstart.F:47-2048);

@@ -490,6 +490,9 @@ struct orc_model {
   orc_arrays_t *a;
   /* NWS = 8 vortex: track, options and GetHollandStormData's module state
    * (bestTrackCounter, WTRATIO; nws08.F90:68, 114) */
+  /* specified normal flux: NFLUXF, the constituents and QN0/QN1/QN2 (NVEL) */
+  int nfluxf = 0, flux_on = 0, nffr = 0;
+  std::vector<double> famig, fper, fff, fface, qnam, qnph, qn0, qn1, qn2;
   int vortex_on = 0;
   orc_vortex_t vpar;
   std::vector<orc_vortex_fix_t> vfix;
@@ -541,6 +544,14 @@ orc_model *orc_model_create(const orc_params_t *p, orc_arrays_t *a) {
   m->rparm[0] = p->convcr;
   m->nw = 4 * a->np + 4 * p->itmax;
   m->iwksp.assign(3 * (size_t)a->np, 0);
+  /* NFLUXF, mesh.F:1907 etc.: any specified-flux segment */
+  for (int I = 0; I < a->nvel; ++I) {
+    const int lb = a->lbcodei[I];
+    if (lb == 2 || lb == 12 || lb == 22) m->nfluxf = 1;
+  }
+  m->qn0.assign(std::max(a->nvel, 1), 0.0);
+  m->qn1 = m->qn0;
+  m->qn2 = m->qn0;
   m->wksp.assign((size_t)4 * a->np + 400 + 4 * (size_t)p->itmax, 0.0);
   m->tk_tmp.assign(a->np, 0.0);
   m->ncchange = 1; /* adcirc.F:404 */
@@ -598,7 +609,45 @@ int orc_model_shift_friction(orc_model *m, const orc_step_t *s) {
     a->tkm[3 * (size_t)i + 1] = a->tk[i];
     a->tkm[3 * (size_t)i + 2] = 0.0;
   }
+  /* shift of the specified normal flux, timestep.F:606-613 */
+  for (int I = 0; I < a->nvel; ++I) {
+    m->qn0[I] = m->qn1[I];
+    m->qn1[I] = m->qn2[I];
+    m->qn2[I] = 0.0;
+  }
   return 0;
+}
+
+int orc_model_set_flux(orc_model *m, const orc_flux_t *f) {
+  if (!f || f->nffr < 1 || !m->nfluxf) return 1;
+  const int nf = f->nffr, nv = m->a->nvel;
+  m->nffr = nf;
+  m->famig.assign(f->famig, f->famig + nf);
+  m->fper.assign(f->fper, f->fper + nf);
+  m->fff.assign(f->fff, f->fff + nf);
+  m->fface.assign(f->fface, f->fface + nf);
+  m->qnam.assign(f->qnam, f->qnam + (size_t)nf * nv);
+  m->qnph.assign(f->qnph, f->qnph + (size_t)nf * nv);
+  m->flux_on = 1;
+  return 0;
+}
+
+/* periodic specified normal flux, timestep.F:861-880 (ICS = 1: no rotation) */
+static void orc_model_flux(orc_model *m, const orc_step_t *s) {
+  if (!m->nfluxf || !m->flux_on) return;
+  orc_arrays_t *a = m->a;
+  for (int J = 0; J < m->nffr; ++J) {
+    int NCYC = 0;
+    if (m->fper[J] != 0.0) NCYC = (int)(s->timeh / m->fper[J]);
+    const double ARGJ = m->famig[J] * (s->timeh - NCYC * m->fper[J]) + m->fface[J];
+    const double RFF = m->fff[J] * s->rampextflux;
+    for (int I = 0; I < a->nvel; ++I) {
+      const int lb = a->lbcodei[I];
+      if (lb == 2 || lb == 12 || lb == 22)
+        m->qn2[I] = m->qn2[I] + m->qnam[J + (size_t)m->nffr * I] * RFF *
+                                    std::cos(ARGJ - m->qnph[J + (size_t)m->nffr * I]);
+    }
+  }
 }
 
 /* GWCE_New, gwce.F:237-2111, IM=0 (KGQ lateral stress, NC advection),
@@ -808,6 +857,22 @@ int orc_model_gwce(orc_model *m, const orc_step_t *s, orc_stepout_t *out) {
       double ARG = ARGJ - a->efa[J + (size_t)a->nbfr * I];
       int b = a->nbd[I] - 1;
       a->eta2[b] = a->eta2[b] + a->emo[J + (size_t)a->nbfr * I] * RFF * std::cos(ARG);
+    }
+  }
+  /* boundary flux integral, gwce.F:1737-1834 (LBCODEI <= 29 types) */
+  if (m->nfluxf) {
+    const double DT2 = p.dt * 2.0;
+    int NBDJ = a->nbv[0] - 1;
+    double QFORCEJ = (m->qn2[0] - m->qn0[0]) / DT2 + a->tau0var[NBDJ] * m->qn1[0];
+    for (int J = 1; J < a->nvel; ++J) {
+      const int NBDI = NBDJ;
+      NBDJ = a->nbv[J] - 1;
+      const double QFORCEI = QFORCEJ;
+      QFORCEJ = (m->qn2[J] - m->qn0[J]) / DT2 + a->tau0var[NBDJ] * m->qn1[J];
+      const int NCI = a->nodecode[NBDI], NCJ = a->nodecode[NBDJ];
+      const double B = NCI * NCJ * a->bndlen2o3[J - 1] / 4.0;
+      a->gwce_lv[NBDI] = a->gwce_lv[NBDI] + B * (2.0 * QFORCEI + QFORCEJ);
+      a->gwce_lv[NBDJ] = a->gwce_lv[NBDJ] + B * (2.0 * QFORCEJ + QFORCEI);
     }
   }
   /* elevation BC into the load vector, gwce.F:1846-1855 */
@@ -1121,7 +1186,7 @@ int orc_model_momentum(orc_model *m, const orc_step_t *s) {
     AUV[4 * (size_t)i + 2] = VCOEFXY * NCI;
     AUV[4 * (size_t)i + 3] = VCOEFYX * NCI;
   }
-  /* velocity BCs, momentum.F:810-862 (LBCODEI 0-9 and 10-19; QN2 = 0) */
+  /* velocity BCs, momentum.F:810-862 (LBCODEI 0-9 and 10-19) */
   const double sqrt2 = std::sqrt(2.0);
   for (int J = 0; J < a->nvelme; ++J) {
     int I = a->me2gw[J] - 1;
@@ -1131,7 +1196,7 @@ int orc_model_momentum(orc_model *m, const orc_step_t *s) {
     double *auv = &AUV[4 * (size_t)NBDI];
     double csi = a->csii[I], sii = a->siii[I];
     if (lb >= 0 && lb <= 9) {
-      double VelNorm = -0.0 / a->h2[NBDI];
+      double VelNorm = -m->qn2[I] / a->h2[NBDI];
       if (std::fabs(gf_norm2(&a->tkm[3 * (size_t)NBDI], 3) - sqrt2 * a->tk[NBDI]) < DBL_EPSILON) {
         a->mom_lv_x[NBDI] = (sii * a->mom_lv_x[NBDI] - csi * a->mom_lv_y[NBDI] - VelNorm * auv[2]) * NCI;
         a->mom_lv_y[NBDI] = VelNorm * auv[0] * NCI;
@@ -1149,7 +1214,7 @@ int orc_model_momentum(orc_model *m, const orc_step_t *s) {
       }
     }
     if (lb >= 10 && lb <= 19) {
-      double VelNorm = -0.0 / a->h2[NBDI];
+      double VelNorm = -m->qn2[I] / a->h2[NBDI];
       double VelTan = 0.0;
       a->mom_lv_x[NBDI] = VelTan * NCI;
       a->mom_lv_y[NBDI] = VelNorm * NCI;
@@ -1279,6 +1344,7 @@ int orc_model_step(orc_model *m, const orc_step_t *s, orc_stepout_t *out) {
   std::memset(out, 0, sizeof(*out));
   orc_model_shift_friction(m, s);
   if (orc_model_met(m, s)) { out->status = -1; return -1; }
+  orc_model_flux(m, s);
   int st = orc_model_gwce(m, s, out);
   if (st != 0) return st;
   orc_model_wetdry(m, s, out);

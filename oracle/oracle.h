@@ -65,6 +65,7 @@ typedef struct {
   const int *nbv, *lbcodei; /* (NVEL) */
   const double *csii, *siii;/* (NVEL) */
   const int *me2gw;         /* (NVELME) */
+  const double *bndlen2o3;  /* (NVEL) */
   /* state (in/out) */
   double *eta1, *eta2, *etas;
   double *uu1, *vv1, *uu2, *vv2, *qx1, *qy1, *qx2, *qy2, *h1, *h2;
@@ -81,8 +82,14 @@ typedef struct {
 typedef struct {
   int it;
   int pad_;
-  double timeloc, timeh, rampelev, rampmete;
+  double timeloc, timeh, rampelev, rampmete, rampextflux;
 } orc_step_t;
+
+/* Periodic specified normal flux (same layout as adc_flux_t). */
+typedef struct {
+  int nffr, pad_;
+  const double *famig, *fper, *fff, *fface, *qnam, *qnph;
+} orc_flux_t;
 
 /* Parametric-vortex track (fort.22 fields HollandGet consumes,
  * nws08.F90:827-878) in mesh units; same layout as adc_vortex_fix_t /
@@ -136,6 +143,8 @@ int orc_model_set_vortex(orc_model *m, const orc_vortex_t *v);
 /* The met phase alone (HollandGet + wind.F:1172-1198); nonzero once the
  * run passes the last fix. */
 int orc_model_met(orc_model *m, const orc_step_t *s);
+/* Specified normal flux (timestep.F:861-880); nonzero without flux boundaries. */
+int orc_model_set_flux(orc_model *m, const orc_flux_t *f);
 void orc_model_set_ncchange(orc_model *m, int ncchange);
 int orc_model_get_ncchange(const orc_model *m);
 double orc_model_get_zeta(const orc_model *m);

@@ -35,7 +35,7 @@ _ARR = [
     ("tau0var", dp_), ("evm", dp_), ("fric", dp_), ("corif", dp_),
     ("nbd", ip_), ("amig", dp_), ("per", dp_), ("face", dp_), ("ff", dp_),
     ("emo", dp_), ("efa", dp_), ("nbv", ip_), ("lbcodei", ip_), ("csii", dp_), ("siii", dp_),
-    ("me2gw", ip_),
+    ("me2gw", ip_), ("bndlen2o3", dp_),
     ("eta1", dp_), ("eta2", dp_), ("etas", dp_),
     ("uu1", dp_), ("vv1", dp_), ("uu2", dp_), ("vv2", dp_), ("qx1", dp_), ("qy1", dp_),
     ("qx2", dp_), ("qy2", dp_), ("h1", dp_), ("h2", dp_),
@@ -55,7 +55,13 @@ class OrcArrays(C.Structure):
 
 class OrcStep(C.Structure):
     _fields_ = [("it", C.c_int), ("pad_", C.c_int), ("timeloc", C.c_double),
-                ("timeh", C.c_double), ("rampelev", C.c_double), ("rampmete", C.c_double)]
+                ("timeh", C.c_double), ("rampelev", C.c_double), ("rampmete", C.c_double),
+                ("rampextflux", C.c_double)]
+
+
+class OrcFlux(C.Structure):
+    _fields_ = [("nffr", C.c_int), ("pad_", C.c_int)] + [
+        (n, dp_) for n in ("famig", "fper", "fff", "fface", "qnam", "qnph")]
 
 
 class OrcStepOut(C.Structure):
@@ -103,6 +109,8 @@ def load():
     for f in ("orc_model_shift_friction", "orc_model_momentum"):
         getattr(lib, f).argtypes = [C.c_void_p, C.POINTER(OrcStep)]
         getattr(lib, f).restype = C.c_int
+    lib.orc_model_set_flux.argtypes = [C.c_void_p, C.POINTER(OrcFlux)]
+    lib.orc_model_set_flux.restype = C.c_int
     lib.orc_model_set_vortex.argtypes = [C.c_void_p, C.POINTER(OrcVortex)]
     lib.orc_model_set_vortex.restype = C.c_int
     lib.orc_model_met.argtypes = [C.c_void_p, C.POINTER(OrcStep)]
@@ -141,6 +149,11 @@ class OracleModel:
         vortex = getattr(case, "vortex", None)
         if vortex is not None:
             self.set_vortex(vortex)
+        flux = getattr(case, "flux", None)
+        if flux is not None:
+            f, keep = flux.struct(OrcFlux)
+            if self.lib.orc_model_set_flux(self.h, C.byref(f)) != 0:
+                raise ValueError("invalid flux forcing")
 
     def set_vortex(self, vortex):
         """vortex: an object with the adcirc_b200.model.Vortex fields."""
@@ -176,6 +189,7 @@ class OracleModel:
         s = self.case.schedule.step(it)
         o = OrcStep()
         o.it, o.timeloc, o.timeh, o.rampelev, o.rampmete = s.it, s.timeloc, s.timeh, s.rampelev, s.rampmete
+        o.rampextflux = s.rampextflux
         return o
 
     def step(self, it) -> OrcStepOut:

@@ -79,3 +79,8 @@ def test_hotstart_rejects_other_mesh_or_mode(lib, tmp_path):
     with pytest.raises(model.AdcError):
         g2.hotstart_read(bad)
     g2.close()
+
+
+def test_resume_channel_river(lib, tmp_path):
+    from adcirc_b200 import model
+    _resume_equal(lambda: model.channel_case(river=0.5), 80, 0, tmp_path, use_run=True)

@@ -192,3 +192,18 @@ def test_w1_chain_burst(lib, orc, ny):
     assert (300 if ny == 401 else 2000) <= go.n_w1_events, go.n_w1_events
     for f in ("tk", "tkm", "nodecode", "nnodecode", "noff", "eta2"):
         assert np.array_equal(cg.arrays[f], c0.arrays[f]), f
+
+
+@pytest.mark.parametrize("river_type", [2, 22])
+def test_channel_river_flux(lib, orc, river_type):
+    """A specified-flux (river) boundary at the closed end: the periodic flux
+    forcing, the GWCE boundary integral (gwce.F:1737-1834) and, for IBTYPE 2,
+    the specified normal velocity of the momentum equation, against the
+    oracle over a graph-replayed run."""
+    from adcirc_b200 import model
+    c0, cg, io, ig = _pair(lambda: model.channel_case(river=0.5, river_type=river_type), 150,
+                           use_run=True)
+    _check(c0, cg, io, ig)
+    a = c0.arrays
+    east = a["x"] > 59.9e3
+    assert a["uu2"][east].mean() < -0.02   # the inflow reaches the boundary nodes

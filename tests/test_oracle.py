@@ -140,3 +140,22 @@ def test_beach_wets_and_dries(orc):
     assert len(seen) > 3, "the wet area never changed"
     assert min(seen) >= 0 and max(seen) <= case.sizes["np"]
     assert wet0 > 0
+
+
+@pytest.mark.parametrize("river_type", [2, 22])
+def test_river_inflow_oracle(orc, river_type):
+    """With no tide, a steady inflow of q m^2/s per unit width through the
+    east end raises the water and drives the flow at the boundary to about
+    -q/H (a specified-flux boundary, timestep.F:861-880, gwce.F:1737-1834)."""
+    from adcirc_b200 import model
+    c = model.channel_case(amp=0.0, river=0.5, river_type=river_type)
+    o = orc.OracleModel(c)
+    for it in range(1, 401):
+        o.step(it)
+    o.close()
+    a = c.arrays
+    east = a["x"] > 59.9e3
+    u = a["uu2"][east].mean()
+    assert -0.12 < u < -0.08, u          # q / H = 0.5 / 5
+    assert 0.0 < a["eta2"].mean() < 0.02
+    assert np.isfinite(a["eta2"]).all()
