@@ -260,14 +260,15 @@ inline bool any_f32(const adc_ctx *c) { return f32_assembly(c) || f32_spmv(c) ||
 // fractional part of 0, 1/3 or 2/3 ulp, never within 1/6 ulp of a rounding
 // midpoint, while the corrected value is within a tiny fraction of an ulp
 // of it, so the result is RN(x/y) for finite x in the normal range; an
-// exact quotient keeps q itself, so the sign of a zero is kept.  The
+// exact quotient keeps q itself, so the sign of a zero is kept, and a
+// non-finite q (x = +-inf or NaN) is returned as it is, as x/y would give.  The
 // library's self-check (adc_selftest_div_const) compares it bit for bit
 // with IEEE division on 2^30 random and adversarial inputs per divisor.
 // It replaces full divisions in the FP64 element kernels' averages.
 __device__ __forceinline__ double div_known(double x, double y, double zh) {
   const double q = x * zh;
   const double r = fma(-q, y, x);
-  return r == 0.0 ? q : fma(r, zh, q);
+  return (r == 0.0 || !isfinite(q)) ? q : fma(r, zh, q);
 }
 __device__ __forceinline__ double div3(double x) { return div_known(x, 3.0, 1.0 / 3.0); }
 __device__ __forceinline__ double div6(double x) { return div_known(x, 6.0, 1.0 / 6.0); }

@@ -1,27 +1,30 @@
 // jcg_noalloc.cu -- the ITPACK jcg entry point for callers that must not
 // allocate: all device staging lives in one file-scope __device__ array.
 //
-// Callers inside a CUDA graph capture, hosts that own every device byte
-// through their own pool (a coupled model sharing the GPU), or code that
-// runs where cudaMalloc may not be called, cannot use adc_jcg, which stages
-// each solve in freshly allocated device memory.  adc_jcg_noalloc takes the
-// same arguments and performs the same solve, but carves every device
-// buffer (matrix, vectors, barrier lines, ITPACK scalars) out of the static
-// array below.  Limits and behaviour:
+// Some hosts cannot let a library call cudaMalloc: a coupled model that
+// owns every device byte through its own pool and accounts for it, or a
+// process that runs under a fixed device-memory budget set when it
+// started.  adc_jcg stages each solve in freshly allocated device memory,
+// so those hosts cannot use it.  adc_jcg_noalloc takes the same arguments
+// and performs the same solve, but carves every device buffer (matrix,
+// vectors, barrier lines, ITPACK scalars) out of the static array below.
+// Limits and behaviour:
 //  * capacity ADC_JCG_NOALLOC_BYTES (32 MiB); a system needs about
-//    n * (20 * (maxnz - 1) + 112) bytes plus 64 KiB, e.g. n <= 80,000 at
-//    maxnz = 16; larger systems return ier = 905 with a message in
-//    adc_last_error();
+//    n * (20 * (maxnz - 1) + 112) bytes plus 32 bytes per ITMAX, e.g.
+//    n <= 80,000 at maxnz = 16; the exact layout is checked before any
+//    device work, and a system that does not fit returns ier = 905 with a
+//    message in adc_last_error();
 //  * the array is held by every GPU that loads the library until the
 //    process exits;
 //  * the first call on a device resolves the array's device address
-//    (cudaGetSymbolAddress) for that device, so it should come before any
-//    stream capture;
+//    (cudaGetSymbolAddress) for that device;
 //  * every call shares the array and finds the previous call's contents;
 //    the solver clears what must start at zero; calls whose GPU work
 //    overlaps (other host threads, other streams) race on it;
+//  * the call is synchronous: it copies with cudaMemcpy/cudaMemset on the
+//    legacy default stream and returns once the solution is on the host;
 //  * it issues no cudaMalloc, cudaFree or stream creation and no host heap
-//    allocation; work runs on the legacy default stream.
+//    allocation.
 #include "adc_internal.cuh"
 
 #include <cfloat>
@@ -57,19 +60,66 @@ static int noalloc_base(void **out) {
   return ADC_OK;
 }
 
-// Bump allocator over the static array.
+// Bump allocator over the static array.  A request that does not fit
+// makes the carve fail for good: every later take returns nullptr too and
+// `failed` stays set, so no partly carved layout reaches a kernel.
 struct Carve {
   char *base;
   size_t off, cap;
+  bool failed;
   template <class T>
   T *take(size_t n) {
     size_t bytes = ((std::max<size_t>(n, 1) * sizeof(T)) + 255) & ~(size_t)255;
-    if (off + bytes > cap) return nullptr;
-    T *p = (T *)(base + off);
+    if (failed || off + bytes > cap) {
+      failed = true;
+      return nullptr;
+    }
+    T *p = base ? (T *)(base + off) : nullptr;
     off += bytes;
     return p;
   }
 };
+
+// Lays out every buffer of one solve, in one fixed order, over `cv`.  With
+// cv.base == nullptr it only counts bytes (the size precheck).
+static void noalloc_carve(Carve &cv, adc_ctx &c, int n, int nslices, size_t slots, int itmax) {
+  const size_t npad = (size_t)nslices * kSlice;
+  c.sl_ptr = cv.take<int>(nslices + 1);
+  c.sl_w = cv.take<int>(nslices);
+  c.rlen = cv.take<int>(npad);
+  c.col = cv.take<int>(slots);
+  c.offd = cv.take<double>(slots);
+  c.soff = cv.take<double>(slots);
+  c.diag = cv.take<double>(n);
+  c.gwce_lv = cv.take<double>(n);
+  c.etas = cv.take<double>(npad);
+  c.ju1 = cv.take<double>(npad);
+  c.jw = cv.take<double>(npad);
+  c.jp[0] = cv.take<double4>(npad);
+  c.jp[1] = cv.take<double4>(npad);
+  c.jpart = cv.take<double>(4 * (size_t)c.jcg_grid);
+  c.jtri = cv.take<double>(4 * (size_t)(itmax > 2 ? itmax : 2));
+  c.jlines = cv.take<char>(2 * 128 * (size_t)c.jcg_rows_blocks);
+  c.itp = cv.take<Itp>(1);
+  c.bar = cv.take<Bar>(1);
+  c.flags = cv.take<Flags>(1);
+}
+
+// Exact scratch bytes of one solve with the largest row-block count the
+// solver can choose for n rows (jcg_setup_grid never uses more than
+// max(1, slices/8) row blocks), or SIZE_MAX when it would not fit.
+static size_t noalloc_need(int n, int maxnz, int itmax) {
+  const int w = maxnz - 1;
+  const int nslices = (n + kSlice - 1) / kSlice;
+  const size_t slots = (size_t)nslices * kSlice * (w > 0 ? w : 1);
+  adc_ctx c;
+  memset((void *)&c, 0, sizeof(c));
+  c.jcg_rows_blocks = std::max(1, nslices / 8);
+  c.jcg_grid = c.jcg_rows_blocks + 1;
+  Carve cv{nullptr, 0, kNoAllocBytes, false};
+  noalloc_carve(cv, c, n, nslices, slots, itmax);
+  return cv.failed ? SIZE_MAX : cv.off;
+}
 
 __global__ void k_noalloc_layout(int n, int nslices, int w, int *sl_ptr, int *sl_w, int *rlen,
                                  int *col) {
@@ -121,6 +171,7 @@ static int noalloc_solve(int n, int ndim, int maxnz, int *jcoef, double *coef, d
   const int w = maxnz - 1;
   const int nslices = (n + kSlice - 1) / kSlice;
   const size_t slots = (size_t)nslices * kSlice * (w > 0 ? w : 1);
+  const size_t npad = (size_t)nslices * kSlice;
   adc_ctx c;
   memset((void *)&c, 0, sizeof(c));
   c.np = n;
@@ -130,30 +181,11 @@ static int noalloc_solve(int n, int ndim, int maxnz, int *jcoef, double *coef, d
   c.stream = 0;   // legacy default stream: nothing is created
   rc = jcg_setup_grid(&c, nullptr);   // the direct variant: no host tables
   if (rc) return rc;
-  Carve cv{(char *)base, 0, kNoAllocBytes};
-  c.sl_ptr = cv.take<int>(nslices + 1);
-  c.sl_w = cv.take<int>(nslices);
-  c.rlen = cv.take<int>((size_t)nslices * kSlice);
-  c.col = cv.take<int>(slots);
-  c.offd = cv.take<double>(slots);
-  c.soff = cv.take<double>(slots);
-  c.diag = cv.take<double>(n);
-  c.gwce_lv = cv.take<double>(n);
-  const size_t npad = (size_t)nslices * kSlice;
-  c.etas = cv.take<double>(npad);
-  c.ju1 = cv.take<double>(npad);
-  c.jw = cv.take<double>(npad);
-  c.jp[0] = cv.take<double4>(npad);
-  c.jp[1] = cv.take<double4>(npad);
-  c.jpart = cv.take<double>(4 * (size_t)c.jcg_grid);
-  c.jtri = cv.take<double>(4 * (size_t)(itmax > 2 ? itmax : 2));
-  c.jlines = cv.take<char>(2 * 128 * (size_t)c.jcg_rows_blocks);
-  c.itp = cv.take<Itp>(1);
-  c.bar = cv.take<Bar>(1);
-  c.flags = cv.take<Flags>(1);
-  if (!c.flags) {
-    set_error("adc_jcg_noalloc: n = %d, maxnz = %d needs more than the %zu-byte static scratch "
-              "(about n*(20*(maxnz-1)+112) bytes plus 64 KiB)", n, maxnz, kNoAllocBytes);
+  Carve cv{(char *)base, 0, kNoAllocBytes, false};
+  noalloc_carve(cv, c, n, nslices, slots, itmax);
+  if (cv.failed) {
+    set_error("adc_jcg_noalloc: n = %d, maxnz = %d, itmax = %d does not fit the %zu-byte "
+              "static scratch", n, maxnz, itmax, kNoAllocBytes);
     return ADC_ERR_NOMEM;
   }
   // matrix: column 1 is the diagonal, columns 2..maxnz the sliced ELL
@@ -237,11 +269,16 @@ void adc_jcg_noalloc(const int *n_, const int *ndim_, const int *maxnz_, int *jc
   const int itmax = iparm[0];
   if (n <= 0) { *ier = 11; return; }
   if (ndim < n || maxnz < 1) { *ier = 11; set_error("ndim < n or maxnz < 1"); return; }
-  const size_t need = (size_t)n * (20 * (size_t)(maxnz - 1) + 112) + 65536;
+  if (2 * sizeof(double) * ((size_t)itmax + 1) > 48 * 1024) {
+    *ier = 905;
+    set_error("adc_jcg_noalloc: itmax = %d is above the JCG scalar block's limit of 3071", itmax);
+    return;
+  }
+  const size_t need = noalloc_need(n, maxnz, itmax);
   if (need > kNoAllocBytes) {
     *ier = 905;
-    set_error("adc_jcg_noalloc: n = %d, maxnz = %d needs about %zu bytes; the static scratch "
-              "holds %zu", n, maxnz, need, kNoAllocBytes);
+    set_error("adc_jcg_noalloc: n = %d, maxnz = %d, itmax = %d needs more than the %zu-byte "
+              "static scratch", n, maxnz, itmax, kNoAllocBytes);
     return;
   }
   // structural part of scal (itpackv.F:2340-2391), in place on the caller's arrays

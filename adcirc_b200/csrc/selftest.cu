@@ -5,7 +5,7 @@
 // with IEEE division bit for bit over random finite inputs of every
 // exponent in the normal range, over inputs built next to multiples of the
 // divisor (quotients with a zero, one-third and two-thirds fractional ulp),
-// and over signed zeros.
+// over signed zeros and infinities, and over a NaN.
 #include "adc_internal.cuh"
 
 namespace adc {
@@ -36,7 +36,14 @@ __global__ void k_selftest_div(long long n, unsigned long long seed, unsigned lo
     }
     if (k == 0) x = 0.0;
     if (k == 1) x = -0.0;
+    if (k == 2) x = __longlong_as_double(0x7FF0000000000000ll);    // +inf
+    if (k == 3) x = __longlong_as_double((long long)0xFFF0000000000000ull);  // -inf
+    if (k == 4) x = __longlong_as_double(0x7FF8000000000000ll);    // NaN
     const double q3 = x / 3.0, q6 = x / 6.0, q12 = x / 12.0;
+    if (isnan(x)) {   // a NaN must stay a NaN (payload bits are not compared)
+      local += !isnan(div3(x)) + !isnan(div6(x)) + !isnan(div12(x));
+      continue;
+    }
     if (__double_as_longlong(div3(x)) != __double_as_longlong(q3)) ++local;
     if (__double_as_longlong(div6(x)) != __double_as_longlong(q6)) ++local;
     if (__double_as_longlong(div12(x)) != __double_as_longlong(q12)) ++local;

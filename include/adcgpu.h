@@ -183,17 +183,18 @@ void adc_dfault(int *iparm, double *rparm);
  * flag of itjcg, itpackv.F:459-604) to its program-start value. */
 void adc_jcg_reset(void);
 
-/* jcg for callers that may not allocate device memory (a host that owns
- * every device byte through its own pool, code that runs during a CUDA
- * graph capture or on a thread where cudaMalloc is off limits).  No
- * counterpart in the reference: same arguments and results as adc_jcg, but
- * every device buffer is carved from one file-scope __device__ array of
- * 32 MiB that each GPU loading the library holds until exit.  Systems
- * needing more than about n*(20*(maxnz-1)+112) + 64 KiB bytes return
- * ier = 905.  The first call on a device resolves the array's address and
- * should come before any stream capture.  Calls share the array: calls
- * whose GPU work overlaps race.  No cudaMalloc/cudaFree, no stream
- * creation, no host heap allocation; work runs on the legacy stream. */
+/* jcg for callers that may not allocate device memory: a host that owns
+ * every device byte through its own pool, or one that runs under a fixed
+ * device-memory budget.  No counterpart in the reference: same arguments
+ * and results as adc_jcg, but every device buffer is carved from one
+ * file-scope __device__ array of 32 MiB that each GPU loading the library
+ * holds until exit.  Systems needing more than about
+ * n*(20*(maxnz-1)+112) bytes + 32 bytes per ITMAX (checked exactly before
+ * any device work) return ier = 905.  The first call on a device resolves
+ * the array's address.  Calls share the array: calls whose GPU work
+ * overlaps race.  The call is synchronous (cudaMemcpy/cudaMemset on the
+ * legacy default stream); it makes no cudaMalloc/cudaFree, no stream
+ * creation and no host heap allocation. */
 void adc_jcg_noalloc(const int *n, const int *ndim, const int *maxnz, int *jcoef,
                      double *coef, double *rhs, double *u, int *iwksp, const int *nw,
                      double *wksp, int *iparm, double *rparm, int *ier);
