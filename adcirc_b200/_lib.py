@@ -87,6 +87,12 @@ class AdcStepOut(C.Structure):
                 ("cme", C.c_double), ("n_w1_events", C.c_int), ("pad_", C.c_int)]
 
 
+class AdcScalars(C.Structure):
+    _fields_ = [("ncchange", C.c_int), ("q1", C.c_int), ("vortex_counter", C.c_int),
+                ("pad_", C.c_int), ("ep", C.c_double), ("rparm1", C.c_double),
+                ("rparm2", C.c_double), ("vortex_wtratio", C.c_double)]
+
+
 _lib = None
 
 
@@ -140,6 +146,7 @@ def load():
         "adc_warm_start_stats": (C.c_int, [vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
         "adc_phase_times": (C.c_int, [vp, dp_, dp_, dp_, dp_, dp_]),
         "adc_launch_count": (C.c_int64, [vp]),
+        "adc_get_scalars": (C.c_int, [vp, C.POINTER(AdcScalars)]),
         "adc_last_run_ms": (C.c_double, [vp]),
         "adc_last_error": (C.c_char_p, []),
     }

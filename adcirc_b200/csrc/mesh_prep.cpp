@@ -192,7 +192,11 @@ int adc_boundary_setup(int np, const double *x, const double *y, int nbou,
     nbvv.resize(nvell + 3);
     for (int i = 1; i <= nvell; ++i) nbvv[i] = seg_nodes[seg_ptr[k] + i - 1];
     nbvv[0] = nbvv[1]; /* unclosed external */
+    /* a two-node island closed here gets its normal from the node pair
+       itself (FLG_IBLEN2, mesh.F:2231, 2421-2424) */
+    bool iblen2 = false;
     if (island && nbvv[nvell] != nbvv[1]) {
+      iblen2 = (nvell == 2);
       nvell = nvell + 1;
       nbvv.resize(nvell + 3);
       nbvv[nvell] = nbvv[1];
@@ -246,6 +250,7 @@ int adc_boundary_setup(int np, const double *x, const double *y, int nbou,
         const double delx = xgj - xgi, dely = ygj - ygi;
         bndlen2o3[jgw - 1] = 2.0 * (std::sqrt(delx * delx + dely * dely)) / 3.0;
       }
+      if (iblen2) { xgj = xgi; ygj = ygi; }
       double xl = std::sqrt((xgk - xgj) * (xgk - xgj) + (ygk - ygj) * (ygk - ygj));
       csii[jgw - 1] = 1.0 * (ygj - ygk) / xl;
       siii[jgw - 1] = (xgk - xgj) / xl;

@@ -859,6 +859,29 @@ int adc_phase_times(adc_ctx *c, double *ms_shift, double *ms_gwce, double *ms_jc
   return ADC_OK;
 }
 
+int adc_get_scalars(adc_ctx *c, adc_scalars_t *out) {
+  if (!c || !out) return ADC_ERR_ARG;
+  Flags f;
+  TRY(read_flags(c, f));
+  Itp it;
+  ADC_CUDA(cudaMemcpy(&it, c->itp, sizeof(Itp), cudaMemcpyDeviceToHost));
+  memset(out, 0, sizeof(*out));
+  out->ncchange = f.ncchange;
+  out->q1 = it.q1;
+  out->ep = f.ep;
+  out->rparm1 = it.rparm1;
+  out->rparm2 = it.cme;
+  out->vortex_counter = -1;
+  out->vortex_wtratio = 0.0;
+  if (c->vortex_on) {
+    VortexState v;
+    ADC_CUDA(cudaMemcpy(&v, c->vstate, sizeof(VortexState), cudaMemcpyDeviceToHost));
+    out->vortex_counter = v.counter;
+    out->vortex_wtratio = v.wtratio;
+  }
+  return ADC_OK;
+}
+
 int64_t adc_launch_count(adc_ctx *c) { return c ? c->launches : -1; }
 
 double adc_last_run_ms(adc_ctx *c) { return c ? c->last_run_ms : -1.0; }

@@ -199,14 +199,35 @@ def _f(a, dtype):
     return np.asfortranarray(np.asarray(a, dtype=dtype))
 
 
+@dataclasses.dataclass
+class MeshPrep:
+    """The one-time table builders build_case calls, each with the argument
+    list of the library's adc_mesh_geometry, adc_mesh_mnei, adc_mesh_neighb,
+    adc_mesh_csr_positions, adc_boundary_setup and adc_coldstart (0 on
+    success).  `product_prep()` gives the library's own."""
+    geometry: object
+    mnei: object
+    neighb: object
+    csr_positions: object
+    boundary_setup: object
+    coldstart: object
+
+
+def product_prep() -> MeshPrep:
+    lib = _lib.load()
+    return MeshPrep(lib.adc_mesh_geometry, lib.adc_mesh_mnei, lib.adc_mesh_neighb,
+                    lib.adc_mesh_csr_positions, lib.adc_boundary_setup, lib.adc_coldstart)
+
+
 def build_case(raw, params: dict, schedule: Schedule, tides, cf: float = 0.0025,
                tau0: float = 0.005, eslm: float = 5.0, cori: float = 1.0e-4,
-               anginn: float = 110.0, eta0=None) -> Case:
+               anginn: float = 110.0, eta0=None, prep: MeshPrep | None = None) -> Case:
     """Assemble every array the hot path binds.
 
     tides: list of (amig [rad/s], face [rad], ff, emo (NETA,), efa (NETA,) [rad])
+    prep: the table builders (default: the library's, `product_prep()`).
     """
-    lib = _lib.load()
+    lib = prep if prep is not None else product_prep()
     npn = int(raw.x.size)
     ne = int(raw.nm.shape[0])
     x = _f(raw.x, np.float64)
@@ -216,20 +237,22 @@ def build_case(raw, params: dict, schedule: Schedule, tides, cf: float = 0.0025,
     fdxe = np.zeros((3, ne), np.float64, order="F")
     fdye = np.zeros((3, ne), np.float64, order="F")
     areas = np.zeros(ne, np.float64)
-    rc = lib.adc_mesh_geometry(npn, ne, ptr(x, dp_), ptr(y, dp_), ptr(nm, ip_), ptr(fdxe, dp_),
+    rc = lib.geometry(npn, ne, ptr(x, dp_), ptr(y, dp_), ptr(nm, ip_), ptr(fdxe, dp_),
                                ptr(fdye, dp_), ptr(areas, dp_))
     if rc != 0:
         raise RuntimeError(f"adc_mesh_geometry failed: {rc}")
-    mnei = lib.adc_mesh_mnei(npn, ne, ptr(nm, ip_))
+    mnei = lib.mnei(npn, ne, ptr(nm, ip_))
+    if mnei < 3:
+        raise RuntimeError(f"adc_mesh_mnei failed: {mnei}")
     nneigh = np.zeros(npn, np.int32)
     neitab = np.zeros((npn, mnei), np.int32, order="F")
     neimax = C.c_int(0)
-    rc = lib.adc_mesh_neighb(npn, ne, mnei, ptr(x, dp_), ptr(y, dp_), ptr(nm, ip_),
+    rc = lib.neighb(npn, ne, mnei, ptr(x, dp_), ptr(y, dp_), ptr(nm, ip_),
                              ptr(nneigh, ip_), ptr(neitab, ip_), C.byref(neimax))
     if rc != 0:
         raise RuntimeError(f"adc_mesh_neighb failed: {rc}")
     csr = np.zeros((ne, 3, 2), np.int32, order="F")
-    rc = lib.adc_mesh_csr_positions(npn, ne, mnei, ptr(nm, ip_), ptr(neitab, ip_),
+    rc = lib.csr_positions(npn, ne, mnei, ptr(nm, ip_), ptr(neitab, ip_),
                                     neimax.value, ptr(csr, ip_))
     if rc != 0:
         raise RuntimeError(f"adc_mesh_csr_positions failed: {rc}")
@@ -250,7 +273,7 @@ def build_case(raw, params: dict, schedule: Schedule, tides, cf: float = 0.0025,
     bndlen = np.zeros(nvel_max, np.float64)
     nvel = C.c_int(0)
     nvelme = C.c_int(0)
-    rc = lib.adc_boundary_setup(npn, ptr(x, dp_), ptr(y, dp_), len(segs), ptr(ibtype, ip_),
+    rc = lib.boundary_setup(npn, ptr(x, dp_), ptr(y, dp_), len(segs), ptr(ibtype, ip_),
                                 ptr(seg_ptr, ip_), ptr(seg_nodes, ip_),
                                 math.cos(anginn * math.pi / 180.0), nvel_max, C.byref(nvel),
                                 ptr(nbv, ip_), ptr(lbc, ip_), ptr(csii, dp_), ptr(siii, dp_),
@@ -296,7 +319,7 @@ def build_case(raw, params: dict, schedule: Schedule, tides, cf: float = 0.0025,
     A["pr2"][:] = prb
     if eta0 is not None:
         A["eta2"][:] = eta0
-    rc = lib.adc_coldstart(npn, ne, params["nolifa"], params["h0"], ptr(dp, dp_), ptr(nm, ip_),
+    rc = lib.coldstart(npn, ne, params["nolifa"], params["h0"], ptr(dp, dp_), ptr(nm, ip_),
                            ptr(areas, dp_), ptr(A["eta1"], dp_), ptr(A["eta2"], dp_),
                            ptr(A["nnodecode"], ip_), ptr(A["nodecode"], ip_), ptr(A["noff"], ip_),
                            ptr(A["mju"], ip_), ptr(A["totalarea"], dp_))
@@ -319,7 +342,8 @@ K1_PERIOD = 86164.0
 
 
 def channel_case(dt: float = 5.0, amp: float = 0.5, vortex: bool = False,
-                 river: float | None = None, river_type: int = 2, **kw) -> Case:
+                 river: float | None = None, river_type: int = 2, prep: MeshPrep | None = None,
+                 **kw) -> Case:
     """Tidal channel: 121x41 nodes, 20 m -> 5 m, M2 0.5 m, dt 5 s.  With
     `vortex`, a small Holland vortex (Rmax 8 km) crosses the channel.  With
     `river` [m^2/s per unit width], the closed east end becomes a
@@ -340,7 +364,7 @@ def channel_case(dt: float = 5.0, amp: float = 0.5, vortex: bool = False,
         kw.setdefault("nws", 8)
     params = default_params(dt, **kw)
     sched = Schedule(dt=dt, dramp=0.5, dramp_mete=0.02 if vortex else 0.5, dramp_extflux=0.02)
-    case = build_case(raw, params, sched, tides)
+    case = build_case(raw, params, sched, tides, prep=prep)
     if river is not None:
         lbc = case.arrays["lbcodei"]
         nv = lbc.size
@@ -353,7 +377,8 @@ def channel_case(dt: float = 5.0, amp: float = 0.5, vortex: bool = False,
     return case
 
 
-def beach_case(dt: float = 2.0, amp: float = 0.5, period: float = 10800.0, **kw) -> Case:
+def beach_case(dt: float = 2.0, amp: float = 0.5, period: float = 10800.0,
+               prep: MeshPrep | None = None, **kw) -> Case:
     """Small beach channel with wetting and drying (parity case).
 
     A three-hour boundary oscillation starting at mean level on the rise
@@ -365,17 +390,18 @@ def beach_case(dt: float = 2.0, amp: float = 0.5, period: float = 10800.0, **kw)
     tides = [(2.0 * math.pi / period, 0.0, 1.0, np.full(neta, amp), np.zeros(neta))]
     params = default_params(dt, **kw)
     sched = Schedule(dt=dt, statim=0.0, reftim=0.25 * period / 86400.0, nramp=0)
-    return build_case(raw, params, sched, tides)
+    return build_case(raw, params, sched, tides, prep=prep)
 
 
 def surge_case(seed: int = 2024, target_nodes: int = 600_000, dt: float = 1.0,
-               vortex: bool = True, **kw) -> Case:
+               vortex: bool = True, prep: MeshPrep | None = None, raw=None, **kw) -> Case:
     """Graded ~600k-node storm-surge mesh, M2 + K1 on the open boundary and a
     Holland vortex (pc 940 hPa, Rmax 40 km, B 1.3) on a straight northward
     track at 5 m/s that makes landfall on the coast (y ~ 640 km) after
     about 19 h."""
     from .meshgen import surge_mesh
-    raw = surge_mesh(seed=seed, target_nodes=target_nodes)
+    if raw is None:
+        raw = surge_mesh(seed=seed, target_nodes=target_nodes)
     neta = raw.open_nodes.size
     xo = raw.x[raw.open_nodes] / raw.meta["lx"]
     tides = [
@@ -385,7 +411,7 @@ def surge_case(seed: int = 2024, target_nodes: int = 600_000, dt: float = 1.0,
     if vortex:
         kw.setdefault("nws", 8)
     params = default_params(dt, **kw)
-    case = build_case(raw, params, Schedule(dt=dt, dramp=0.25, dramp_mete=0.25), tides)
+    case = build_case(raw, params, Schedule(dt=dt, dramp=0.25, dramp_mete=0.25), tides, prep=prep)
     if vortex:
         case.vortex = straight_track(0.5 * raw.meta["lx"] + 1234.5, 300e3 + 678.9, 90.0, 5.0,
                                      940.0, 40.0, 1.3, hours=30.0)
@@ -457,6 +483,12 @@ class GpuModel:
     def sync_to_host(self):
         _check(self.lib.adc_sync_to_host(self.h), "adc_sync_to_host")
         return self.case.state()
+
+    def scalars(self) -> dict:
+        """Step-to-step module scalars (adc_get_scalars)."""
+        sc = _lib.AdcScalars()
+        _check(self.lib.adc_get_scalars(self.h, C.byref(sc)), "adc_get_scalars")
+        return {k: getattr(sc, k) for k, _ in sc._fields_ if k != "pad_"}
 
     def phase_times(self):
         v = [C.c_double() for _ in range(5)]

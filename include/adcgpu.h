@@ -317,6 +317,26 @@ int adc_set_flux(adc_ctx *ctx, const adc_flux_t *flux);
  * those that fell back to the reference guess. */
 int adc_warm_start_stats(adc_ctx *ctx, long long *used, long long *fallback);
 
+/* Scalars the device step carries from one step to the next that live in
+ * the reference's modules: NCChange (gwce.F:430, wetdry.F:1430), EP
+ * (gwce.F:646-650), RPARM(1:2) after the last solve (itpackv.F:394, 442),
+ * itjcg's SAVEd q1 flag (itpackv.F:459-604) and NWS = 8's track position
+ * bestTrackCounter/WTRATIO (nws08.F90:68, 114, 827-878).  Together with the
+ * arrays adc_sync_to_host writes they are the whole step-to-step state, so a
+ * host (or a checker) can continue a run from them. */
+typedef struct {
+  int ncchange;        /* NCChange: nonzero rebuilds the GWCE matrix next step */
+  int q1;              /* itjcg's q1 (skip the |u| norm in the stopping test) */
+  int vortex_counter;  /* 0-based index of the track fix after the current time */
+  int pad_;
+  double ep;           /* EP of the last matrix rebuild */
+  double rparm1;       /* RPARM(1), zeta (overwritten on non-convergence) */
+  double rparm2;       /* RPARM(2), cme: the eigenvalue estimate */
+  double vortex_wtratio; /* WTRATIO used for the storm position */
+} adc_scalars_t;
+
+int adc_get_scalars(adc_ctx *ctx, adc_scalars_t *out);
+
 /* Device time of the phases of the last adc_timestep/adc_run (ms). */
 int adc_phase_times(adc_ctx *ctx, double *ms_shift, double *ms_gwce, double *ms_jcg,
                     double *ms_wetdry, double *ms_momentum);

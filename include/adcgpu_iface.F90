@@ -51,6 +51,12 @@ module adcgpu_iface
       integer(c_int) :: n_w1_events, pad_
    end type
 
+   ! step-to-step module scalars (NCChange, EP, RPARM(1:2), q1, vortex track)
+   type, bind(C), public :: adc_scalars_t
+      integer(c_int) :: ncchange, q1, vortex_counter, pad_
+      real(c_double) :: ep, rparm1, rparm2, vortex_wtratio
+   end type
+
    integer(c_int), parameter, public :: ADC_WARM_START = 2, ADC_F32_ASSEMBLY = 4, &
                                         ADC_F32_SPMV = 8, ADC_F32_MOMENTUM = 16
 
@@ -173,6 +179,12 @@ module adcgpu_iface
          import :: c_int, c_ptr, c_char
          type(c_ptr), value :: ctx
          character(kind=c_char), intent(in) :: path(*)
+      end function
+
+      integer(c_int) function adc_get_scalars(ctx, sc) bind(C, name="adc_get_scalars")
+         import :: c_int, c_ptr, adc_scalars_t
+         type(c_ptr), value :: ctx
+         type(adc_scalars_t), intent(out) :: sc
       end function
    end interface
 end module adcgpu_iface

@@ -1356,6 +1356,23 @@ int orc_model_step(orc_model *m, const orc_step_t *s, orc_stepout_t *out) {
   return 0;
 }
 
+/* Continue a run from another implementation's step-to-step state: the
+ * module scalars NCChange, EP, RPARM(1:2), itjcg's SAVEd q1 and the NWS = 8
+ * track position (bestTrackCounter, WTRATIO).  The arrays come in through
+ * the bound orc_arrays_t. */
+void orc_model_set_scalars(orc_model *m, int ncchange, double ep, double rparm1, double rparm2,
+                           int q1, int vcounter, double vwtratio) {
+  m->ncchange = ncchange;
+  m->ep = ep;
+  m->rparm[0] = rparm1;
+  m->rparm[1] = rparm2;
+  g_itp.q1 = (q1 != 0);
+  if (m->vortex_on && vcounter >= 0) {
+    m->vcounter = vcounter;
+    m->vwtratio = vwtratio;
+  }
+}
+
 void orc_coldstart(const orc_params_t *p, orc_arrays_t *a) {
   const int np = a->np, ne = a->ne;
   for (int i = 0; i < np; ++i) a->nnodecode[i] = 1;

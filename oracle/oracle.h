@@ -148,11 +148,33 @@ int orc_model_set_flux(orc_model *m, const orc_flux_t *f);
 void orc_model_set_ncchange(orc_model *m, int ncchange);
 int orc_model_get_ncchange(const orc_model *m);
 double orc_model_get_zeta(const orc_model *m);
+/* Continue from another implementation's step-to-step state (the module
+ * scalars; the arrays come in through the bound orc_arrays_t). */
+void orc_model_set_scalars(orc_model *m, int ncchange, double ep, double rparm1, double rparm2,
+                           int q1, int vcounter, double vwtratio);
 
 /* Cold-start wet/dry state (cstart.F:1332-1427) and totalAreaCalc
  * (mesh.F:3360-3400): sets NNODECODE, NODECODE, NOFF, ETA2, ETA1, MJU,
  * TotalArea. */
 void orc_coldstart(const orc_params_t *p, orc_arrays_t *a);
+
+/* Static mesh and boundary tables (oracle_mesh.cpp, mesh.F), with the
+ * argument lists of the library's adc_mesh_* / adc_boundary_setup /
+ * adc_coldstart.  0 on success, negative on an invalid mesh. */
+int orc_mesh_geometry(int np, int ne, const double *x, const double *y, int *nm,
+                      double *fdxe, double *fdye, double *areas);
+int orc_mesh_mnei(int np, int ne, const int *nm);
+int orc_mesh_neighb(int np, int ne, int mnei, const double *x, const double *y, const int *nm,
+                    int *nneigh, int *neitab, int *neimax);
+int orc_mesh_csr_positions(int np, int ne, int mnei, const int *nm, const int *neitab,
+                           int neimax, int *csr_position);
+int orc_boundary_setup(int np, const double *x, const double *y, int nbou, const int *ibtype,
+                       const int *seg_ptr, const int *seg_nodes, double costset, int nvel_max,
+                       int *nvel_out, int *nbv, int *lbcodei, double *csii, double *siii,
+                       int *nvelme_out, int *me2gw, double *bndlen2o3);
+int orc_coldstart_arrays(int np, int ne, int nolifa, double h0, const double *dp, const int *nm,
+                         const double *areas, double *eta1, double *eta2, int *nnodecode,
+                         int *nodecode, int *noff, int *mju, double *totalarea);
 
 #ifdef __cplusplus
 }

@@ -121,6 +121,22 @@ def load():
     lib.orc_model_get_zeta.argtypes = [C.c_void_p]
     lib.orc_model_get_zeta.restype = C.c_double
     lib.orc_coldstart.argtypes = [C.POINTER(OrcParams), C.POINTER(OrcArrays)]
+    lib.orc_model_set_scalars.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_double,
+                                          C.c_double, C.c_int, C.c_int, C.c_double]
+    lib.orc_model_set_scalars.restype = None
+    sig = {
+        "orc_mesh_geometry": [C.c_int, C.c_int, dp_, dp_, ip_, dp_, dp_, dp_],
+        "orc_mesh_mnei": [C.c_int, C.c_int, ip_],
+        "orc_mesh_neighb": [C.c_int, C.c_int, C.c_int, dp_, dp_, ip_, ip_, ip_, ip_],
+        "orc_mesh_csr_positions": [C.c_int, C.c_int, C.c_int, ip_, ip_, C.c_int, ip_],
+        "orc_boundary_setup": [C.c_int, dp_, dp_, C.c_int, ip_, ip_, ip_, C.c_double, C.c_int,
+                               ip_, ip_, ip_, dp_, dp_, ip_, ip_, dp_],
+        "orc_coldstart_arrays": [C.c_int, C.c_int, C.c_int, C.c_double, dp_, ip_, dp_, dp_, dp_,
+                                 ip_, ip_, ip_, ip_, dp_],
+    }
+    for name, args in sig.items():
+        getattr(lib, name).argtypes = args
+        getattr(lib, name).restype = C.c_int
     _lib = lib
     return lib
 
@@ -169,6 +185,13 @@ class OracleModel:
         rc = self.lib.orc_model_set_vortex(self.h, C.byref(v))
         if rc != 0:
             raise ValueError("invalid vortex track")
+
+    def set_scalars(self, sc: dict):
+        """Continue from another implementation's state: `sc` holds the
+        fields of adc_scalars_t (the arrays are the case's, set beforehand)."""
+        self.lib.orc_model_set_scalars(self.h, int(sc["ncchange"]), float(sc["ep"]),
+                                       float(sc["rparm1"]), float(sc["rparm2"]), int(sc["q1"]),
+                                       int(sc["vortex_counter"]), float(sc["vortex_wtratio"]))
 
     def met(self, it):
         """The met phase alone for step `it`; nonzero once past the track."""
@@ -236,6 +259,18 @@ def jcg(n, ndim, maxnz, jcoef, coef, rhs, u, iparm, rparm):
                 _ptr(iwksp, ip_), C.byref(C.c_int(nw)), _ptr(wksp, dp_), _ptr(iparm, ip_),
                 _ptr(rparm, dp_), C.byref(ier))
     return ier.value
+
+
+def mesh_prep():
+    """The oracle's own table builders (oracle_mesh.cpp), with the argument
+    lists of the library's: pass as `prep=` to adcirc_b200.model.build_case
+    (or a named case) to build a case without the library."""
+    import types
+    lib = load()
+    return types.SimpleNamespace(
+        geometry=lib.orc_mesh_geometry, mnei=lib.orc_mesh_mnei, neighb=lib.orc_mesh_neighb,
+        csr_positions=lib.orc_mesh_csr_positions, boundary_setup=lib.orc_boundary_setup,
+        coldstart=lib.orc_coldstart_arrays)
 
 
 def dfault():

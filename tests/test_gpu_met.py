@@ -8,7 +8,7 @@ import ctypes as C
 import numpy as np
 import pytest
 
-from test_gpu_parity import REL_TOL, _check, _pair, _rel
+from test_gpu_parity import REL_TOL, _check, _pair, _rel, oracle_and_gpu_cases
 
 pytestmark = pytest.mark.gpu
 
@@ -16,8 +16,7 @@ pytestmark = pytest.mark.gpu
 def test_vortex_fields_first_steps(lib, orc):
     import oracle
     from adcirc_b200 import model
-    c0 = model.channel_case(vortex=True)
-    cg = c0.clone()
+    c0, cg = oracle_and_gpu_cases(lambda **k: model.channel_case(vortex=True, **k))
     o = oracle.OracleModel(c0)
     g = model.GpuModel(cg)
     for it in (1, 2, 3):
@@ -33,7 +32,7 @@ def test_vortex_fields_first_steps(lib, orc):
 
 def test_vortex_channel_steps(lib, orc):
     from adcirc_b200 import model
-    c0, cg, io, ig = _pair(lambda: model.channel_case(vortex=True), 60)
+    c0, cg, io, ig = _pair(lambda **k: model.channel_case(vortex=True, **k), 60)
     errs = _check(c0, cg, io, ig)
     # the storm must actually force the channel
     assert np.abs(c0.arrays["wsx2"]).max() > 1e-4
@@ -42,7 +41,7 @@ def test_vortex_channel_steps(lib, orc):
 
 def test_vortex_graph_run(lib, orc):
     from adcirc_b200 import model
-    c0, cg, io, ig = _pair(lambda: model.channel_case(vortex=True), 150, use_run=True)
+    c0, cg, io, ig = _pair(lambda **k: model.channel_case(vortex=True, **k), 150, use_run=True)
     _check(c0, cg, io, ig)
 
 

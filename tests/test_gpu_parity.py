@@ -22,11 +22,24 @@ def _rel(a, b):
     return float(np.abs(a - b).max() / scale)
 
 
+def oracle_and_gpu_cases(case_fn):
+    """(oracle case, GPU case): the oracle's built with its own restatement of
+    the static tables (oracle/oracle_mesh.cpp), the GPU's with the library's;
+    the two sets must agree bit for bit before any step is compared."""
+    import oracle
+    c0 = case_fn(prep=oracle.mesh_prep())
+    cg = case_fn()
+    assert c0.sizes == cg.sizes
+    bad = [k for k in c0.arrays if not np.array_equal(c0.arrays[k], cg.arrays[k])]
+    assert not bad, f"static tables differ: {bad}"
+    return c0, cg
+
+
 def _pair(case_fn, nsteps, use_run=False):
+    """`case_fn(prep=...)` builds the case; see oracle_and_gpu_cases."""
     import oracle
     from adcirc_b200 import model
-    c0 = case_fn()
-    cg = c0.clone()
+    c0, cg = oracle_and_gpu_cases(case_fn)
     orc = oracle.OracleModel(c0)
     gpu = model.GpuModel(cg)
     its_o = np.array([orc.step(it).numitr for it in range(1, nsteps + 1)])
@@ -173,13 +186,17 @@ def test_w1_chain_burst(lib, orc, ny):
     eta0 = np.where(raw.dp > 0.05, rng.uniform(0.5, 1.0, raw.dp.size), 0.0)
     params = model.default_params(0.1)
     tides = [(1e-4, 0.0, 1.0, np.zeros(raw.open_nodes.size), np.zeros(raw.open_nodes.size))]
-    base = model.build_case(raw, params, model.Schedule(dt=0.1, nramp=0), tides, eta0=eta0)
     tk = rng.uniform(0.0, 8.0, raw.dp.size)
-    base.arrays["tk"][:] = tk
-    base.arrays["tkm"][:] = 0.0
-    base.arrays["tkm"][0::3] = tk
-    base.arrays["tkm"][1::3] = tk
-    c0, cg = base.clone(), base.clone()
+
+    def build(**k):
+        c = model.build_case(raw, params, model.Schedule(dt=0.1, nramp=0), tides, eta0=eta0, **k)
+        c.arrays["tk"][:] = tk
+        c.arrays["tkm"][:] = 0.0
+        c.arrays["tkm"][0::3] = tk
+        c.arrays["tkm"][1::3] = tk
+        return c
+    c0, cg = oracle_and_gpu_cases(build)
+    base = cg
     o = oracle.OracleModel(c0)
     oo = o.wetdry(1)
     g = model.GpuModel(cg)
@@ -201,7 +218,7 @@ def test_channel_river_flux(lib, orc, river_type):
     the specified normal velocity of the momentum equation, against the
     oracle over a graph-replayed run."""
     from adcirc_b200 import model
-    c0, cg, io, ig = _pair(lambda: model.channel_case(river=0.5, river_type=river_type), 150,
+    c0, cg, io, ig = _pair(lambda **k: model.channel_case(river=0.5, river_type=river_type, **k), 150,
                            use_run=True)
     _check(c0, cg, io, ig)
     a = c0.arrays
