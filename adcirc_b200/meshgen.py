@@ -149,7 +149,7 @@ def surge_mesh(seed: int = 2024, target_nodes: int = 600_000, lx: float = 1000e3
                shelf_width: float = 100e3, shelf_depth: float = 30.0,
                ocean_depth: float = 4000.0, land_height: float = 6.0,
                grf_sigma: float = 2.0, grf_ell: float = 5e3,
-               land_grading: float = 3.0) -> RawMesh:
+               land_grading: float = 3.0, jitter: float = 0.3) -> RawMesh:
     """Graded storm-surge mesh (~600k nodes, ~1.18M triangles).
 
     Points: seeded jittered quadtree sampling whose cell size follows the
@@ -193,7 +193,7 @@ def surge_mesh(seed: int = 2024, target_nodes: int = 600_000, lx: float = 1000e3
             break
     alpha = mid
     cx, cy, size = _quadtree_leaves(lx, ly, make_h(alpha), h_max)
-    jit = 0.3
+    jit = jitter
     px = cx + size * rng.uniform(-jit, jit, cx.size)
     py = cy + size * rng.uniform(-jit, jit, cy.size)
     # keep interior points off the boundary

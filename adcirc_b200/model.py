@@ -199,6 +199,21 @@ def _f(a, dtype):
     return np.asfortranarray(np.asarray(a, dtype=dtype))
 
 
+def tau0_nodal(scheme: float, depth: np.ndarray) -> np.ndarray:
+    """Tau0Var for a negative fort.15 TAU0 (nodalattr.F:1872-1876 via
+    Tau0NodalValue, nodalattr.F:2084-2100): -2 varies smoothly with depth
+    (0.005 below 200 m, 1/depth from 200 m to 1 m, 1 above), any other
+    negative value switches from 0.005 to 0.020 at 10 m depth."""
+    d = np.asarray(depth, np.float64)
+    if scheme == -2.0:
+        out = np.where(d >= 200.0, np.float64(np.float32(0.005)), 0.0)   # REAL literal 0.005
+        mid = (d < 200.0) & (d >= 1.0)
+        out[mid] = np.float64(np.float32(1.0)) / d[mid]
+        out[d < 1.0] = 1.0
+        return out
+    return np.where(d <= 10.0, 0.020, 0.005)
+
+
 @dataclasses.dataclass
 class MeshPrep:
     """The one-time table builders build_case calls, each with the argument
@@ -294,7 +309,8 @@ def build_case(raw, params: dict, schedule: Schedule, tides, cf: float = 0.0025,
     A = dict(
         x=x, y=y, dp=dp, nm=nm, nneigh=nneigh, neitab=neitab, fdxe=fdxe, fdye=fdye,
         areas=areas, csr_position=csr,
-        tau0var=np.full(npn, tau0), evm=np.full(npn, eslm), fric=np.full(npn, cf),
+        tau0var=np.full(npn, tau0) if tau0 >= 0.0 else tau0_nodal(tau0, dp),
+        evm=np.full(npn, eslm), fric=np.full(npn, cf),
         corif=np.full(npn, cori),
         nbd=nbd, amig=amig if nbfr else _f([0.0], np.float64),
         per=per if nbfr else _f([0.0], np.float64),
@@ -394,11 +410,14 @@ def beach_case(dt: float = 2.0, amp: float = 0.5, period: float = 10800.0,
 
 
 def surge_case(seed: int = 2024, target_nodes: int = 600_000, dt: float = 1.0,
-               vortex: bool = True, prep: MeshPrep | None = None, raw=None, **kw) -> Case:
+               vortex: bool = True, prep: MeshPrep | None = None, raw=None,
+               tau0: float = -1.0, **kw) -> Case:
     """Graded ~600k-node storm-surge mesh, M2 + K1 on the open boundary and a
     Holland vortex (pc 940 hPa, Rmax 40 km, B 1.3) on a straight northward
     track at 5 m/s that makes landfall on the coast (y ~ 640 km) after
-    about 19 h."""
+    about 19 h.  TAU0 = -1 (the default depth switch: 0.020 at depths of
+    10 m or less, 0.005 deeper); a constant 0.005 lets a grid-scale
+    oscillation grow on the flooded coastal lowland within four hours."""
     from .meshgen import surge_mesh
     if raw is None:
         raw = surge_mesh(seed=seed, target_nodes=target_nodes)
@@ -411,7 +430,8 @@ def surge_case(seed: int = 2024, target_nodes: int = 600_000, dt: float = 1.0,
     if vortex:
         kw.setdefault("nws", 8)
     params = default_params(dt, **kw)
-    case = build_case(raw, params, Schedule(dt=dt, dramp=0.25, dramp_mete=0.25), tides, prep=prep)
+    case = build_case(raw, params, Schedule(dt=dt, dramp=0.25, dramp_mete=0.25), tides, prep=prep,
+                      tau0=tau0)
     if vortex:
         case.vortex = straight_track(0.5 * raw.meta["lx"] + 1234.5, 300e3 + 678.9, 90.0, 5.0,
                                      940.0, 40.0, 1.3, hours=30.0)

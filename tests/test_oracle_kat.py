@@ -1,0 +1,40 @@
+"""Known answers the oracle must meet (no GPU): volume conservation in a
+closed basin, the inflow mass balance, and mirror symmetry.  See
+kat_cases.py for why each holds for the discrete scheme."""
+import numpy as np
+
+import kat_cases as K
+
+
+def test_closed_basin_conserves_volume(orc):
+    c = K.closed_basin(prep=orc.mesh_prep())
+    v0 = K.basin_volume(c)
+    om = orc.OracleModel(c)
+    drift = []
+    for it in range(1, 401):
+        om.step(it)
+        drift.append(K.basin_volume(c) - v0)
+    om.close()
+    assert np.abs(c.arrays["eta2"]).max() > 0.05          # the hump is still moving
+    assert max(abs(d) for d in drift) <= 1e-8 * v0, max(abs(d) for d in drift) / v0
+
+
+def test_river_inflow_mass_balance(orc):
+    c = K.river_basin(prep=orc.mesh_prep())
+    om = orc.OracleModel(c)
+    om.run(1, 719)
+    v1 = K.basin_volume(c)
+    om.run(720, 721)
+    v2 = K.basin_volume(c)
+    om.close()
+    q = K.inflow_volume(c, 720, 1441)
+    assert abs((v2 - v1) - q) <= 1e-6 * q, ((v2 - v1) - q) / q
+
+
+def test_mirror_symmetry(orc):
+    c = K.mirror_channel(prep=orc.mesh_prep())
+    om = orc.OracleModel(c)
+    om.run(1, 720)
+    om.close()
+    asym = K.asymmetry(c)
+    assert asym["eta"] <= 1e-12 and asym["u"] <= 1e-12 and asym["v"] <= 1e-9, asym
