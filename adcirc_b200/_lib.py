@@ -147,6 +147,7 @@ def load():
         "adc_phase_times": (C.c_int, [vp, dp_, dp_, dp_, dp_, dp_]),
         "adc_launch_count": (C.c_int64, [vp]),
         "adc_get_scalars": (C.c_int, [vp, C.POINTER(AdcScalars)]),
+        "adc_kernel_times": (C.c_int, [vp, dp_, C.c_int]),
         "adc_last_run_ms": (C.c_double, [vp]),
         "adc_last_error": (C.c_char_p, []),
     }

@@ -158,7 +158,7 @@ struct adc_ctx {
   void *jlines;          // JCG barrier lines: 2 x 128 B per row block
   int jcg_grid, jcg_rows_blocks;
   // JCG resident variant (block-local indices, halo lists, export flags)
-  int jcg_res, jcg_rows_max, jcg_halo_max, jcg_stage_bytes;
+  int jcg_res, jcg_rows_max, jcg_halo_max, jcg_stage_bytes, jcg_stage_wcap;
   size_t jcg_smem;
   unsigned short *jlcol;
   float *soff32;               // FP32 scaled matrix (mixed mode, resident variant)
@@ -182,6 +182,8 @@ struct adc_ctx {
   VortexState *vstate;
   // timing
   cudaEvent_t ev[6];
+  cudaEvent_t kev[2 * 6];   // start/end of the kernel spans of adc_kernel_times
+  int kmark;                // record kev while capturing the timed single-step graph
   int64_t launches;
   // graph
   cudaGraphExec_t graph;
@@ -243,6 +245,12 @@ inline void launch_k(void (*kernel)(KArgs...), dim3 grid, dim3 block, cudaStream
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+}
+
+// Kernel spans timed in the single-step graph (adc_kernel_times).
+enum KSpan { KS_LHS_ELEM = 0, KS_LHS_GATHER, KS_RHS_ELEM, KS_RHS_GATHER, KS_MOM_ELEM, KS_MOM_NODE };
+inline void kmark(adc_ctx *c, int span, int end) {
+  if (c->kmark) cudaEventRecordWithFlags(c->kev[2 * span + end], c->stream, cudaEventRecordExternal);
 }
 
 // Which parts run in FP32 (ADC_PREC_MIXED selects all of them).

@@ -72,6 +72,7 @@ struct JcgArgs {
   int rows_max;               // rows of the largest row block
   int halo_max;               // halo nodes of the largest row block
   int stage_bytes;            // one staged slice: local columns + values
+  int stage_wcap;             // widest slice that is staged; wider ones are read in place
   const unsigned short *lcol; // per slot: block-local value index
   const int *halo_ptr;        // [nrb + 1] into halo_ids
   const int *halo_ids;        // halo nodes of each row block (global rows)
@@ -542,11 +543,14 @@ struct SlicePipe {
   Flags *flags;
   int stage_bytes, s0, s1, first, step, lane;
   uint32_t parbits;
+  int wcap;                   // slices wider than this are not staged
+
+  __device__ bool staged(int sl) const { return meta[sl - s0].y <= wcap; }
 
   // V: the staged value type (FP64 matrix, or FP32 in the mixed mode)
   template <class V>
   __device__ void issue(int sl, int st, const V *vals) {
-    if (lane == 0) {
+    if (lane == 0 && staged(sl)) {
       const int2 mt = meta[sl - s0];
       const uint32_t w = (uint32_t)mt.y;
       const uint32_t vb = w * 32u * (uint32_t)sizeof(V);
@@ -587,17 +591,23 @@ struct SlicePipe {
     parbits ^= 1u << st;
     return true;
   }
-  // body(sl, lc, lv): one slice from shared memory; lc/lv hold slot q of
-  // lane l at [q * 32 + l].  Returns false on an expired wait.
+  // body(sl, lc, lv): one slice from shared memory (or, for a slice wider
+  // than wcap, in place from global memory, which has the same layout);
+  // lc/lv hold slot q of lane l at [q * 32 + l].  Returns false on an
+  // expired wait.
   template <class V, class F>
   __device__ bool run(const V *vals, F body) {
     int k = 0;
     for (int sl = first; sl < s1; sl += step, ++k) {
       const int st = k & 1;
-      if (!wait(st, sl + step < s1)) return false;
-      const int w = meta[sl - s0].y;
-      const unsigned char *b = stg0 + (size_t)st * stage_bytes;
-      body(sl, (const unsigned short *)b, (const V *)(b + (size_t)w * 64));
+      const int2 mt = meta[sl - s0];
+      if (mt.y > wcap) {
+        body(sl, lcol + mt.x, vals + mt.x);
+      } else {
+        if (!wait(st, sl + step < s1 && staged(sl + step))) return false;
+        const unsigned char *b = stg0 + (size_t)st * stage_bytes;
+        body(sl, (const unsigned short *)b, (const V *)(b + (size_t)mt.y * 64));
+      }
       __syncwarp();
       if (sl + 2 * step < s1) issue(sl + 2 * step, st, vals);
     }
@@ -636,7 +646,7 @@ __global__ void __launch_bounds__(kThreads, 2) jcg_kernel(JcgArgs a) {
   unsigned char *S_stage = (unsigned char *)(S_bar + 16);
   const int nhalo = (kRes && !scalar_block) ? a.halo_ptr[blockIdx.x + 1] - a.halo_ptr[blockIdx.x] : 0;
   SlicePipe pipe{S_stage + (size_t)(2 * warp) * a.stage_bytes, &S_bar[2 * warp], S_meta, a.lcol,
-                 a.flags, a.stage_bytes, s0, s1, s0 + warp, nwarps, lane, 0u};
+                 a.flags, a.stage_bytes, s0, s1, s0 + warp, nwarps, lane, 0u, a.stage_wcap};
   Rec *rec = &a.itp->rec;
   __shared__ ItpLocal L;              // used by the scalar block's thread 0 only
   __shared__ Rec s_rec;               // the record of the last reducing barrier
@@ -1235,13 +1245,19 @@ int jcg_setup_grid(adc_ctx *c, const JcgHostSell *h) {
                        lcol, hptr, hids, exp, halo_max);
       fits = rows_max + halo_max < 65536;
     }
-    size_t smem = jcg_smem_bytes(c->itmax, true, rows_max, halo_max, wmax);
-    int per_sm = 0;
-    if (fits && smem <= 200 * 1024) {
-      const void *fn = f32_spmv(c) ? (const void *)jcg_kernel<1, float>
-                                                  : (const void *)jcg_kernel<1, double>;
+    // Stage slices up to width wcap in shared memory; a few wider slices
+    // (rows with the most neighbours) are read in place, so that two row
+    // blocks still fit on an SM.
+    size_t smem = 0;
+    int per_sm = 0, wcap = wmax;
+    const void *fn = f32_spmv(c) ? (const void *)jcg_kernel<1, float>
+                                 : (const void *)jcg_kernel<1, double>;
+    for (; fits && wcap >= std::max(1, wmax - 4); --wcap) {
+      smem = jcg_smem_bytes(c->itmax, true, rows_max, halo_max, wcap);
+      if (smem > 200 * 1024) continue;
       ADC_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
       ADC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kThreads, smem));
+      if (per_sm >= 2) break;
     }
     if (per_sm >= 2 && (long long)per_sm * nsm >= nrb + 1) {
       ADC_CUDA(cudaMalloc((void **)&c->jlcol, lcol.size() * sizeof(unsigned short)));
@@ -1259,7 +1275,8 @@ int jcg_setup_grid(adc_ctx *c, const JcgHostSell *h) {
       c->jcg_res = 1;
       c->jcg_rows_max = rows_max;
       c->jcg_halo_max = halo_max;
-      c->jcg_stage_bytes = (int)jcg_stage_bytes(wmax);
+      c->jcg_stage_bytes = (int)jcg_stage_bytes(wcap);
+      c->jcg_stage_wcap = wcap;
       c->jcg_smem = smem;
       return ADC_OK;
     }
@@ -1316,6 +1333,7 @@ int launch_jcg_impl(adc_ctx *c, int eta_update, int do_peror, int run_init, int 
   a.rows_max = c->jcg_rows_max;
   a.halo_max = c->jcg_halo_max;
   a.stage_bytes = c->jcg_stage_bytes;
+  a.stage_wcap = c->jcg_stage_wcap;
   a.lcol = c->jlcol;
   a.halo_ptr = c->jhalo_ptr;
   a.halo_ids = c->jhalo_ids;

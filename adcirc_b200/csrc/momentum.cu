@@ -225,13 +225,19 @@ __global__ void k_mom_node(adc_ctx c) {
 }
 
 int launch_momentum(adc_ctx *c) {
+  kmark(c, KS_MOM_ELEM, 0);
   if (f32_momentum(c)) {   // FP32 element terms and their gather
     launch_k(k_mom_elem<float>, nblk(c->ne), kThreads, c->stream, *c);
+    kmark(c, KS_MOM_ELEM, 1);
+    kmark(c, KS_MOM_NODE, 0);
     launch_k(k_mom_node<float>, nblk(c->np), kThreads, c->stream, *c);
   } else {
     launch_k(k_mom_elem<double>, nblk(c->ne), kThreads, c->stream, *c);
+    kmark(c, KS_MOM_ELEM, 1);
+    kmark(c, KS_MOM_NODE, 0);
     launch_k(k_mom_node<double>, nblk(c->np), kThreads, c->stream, *c);
   }
+  kmark(c, KS_MOM_NODE, 1);
   c->launches += 2;
   return ADC_OK;
 }

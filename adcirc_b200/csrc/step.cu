@@ -81,13 +81,19 @@ int launch_gwce_lhs(adc_ctx *c) {
   launch_k(k_lhs_begin, 1, 1, c->stream, c->flags, rb);
   int nb = nblk(c->np);
   launch_k(k_lhs_drift, nb, kThreads, c->stream, *c, rb + 2);
+  kmark(c, KS_LHS_ELEM, 0);
   if (f32_assembly(c)) {   // FP32 element assembly
     launch_k(k_lhs_elem<float>, nblk(c->ne), kThreads, c->stream, *c, rb);
+    kmark(c, KS_LHS_ELEM, 1);
+    kmark(c, KS_LHS_GATHER, 0);
     launch_k(k_lhs_gather<float>, nb, kThreads, c->stream, *c, rb);
   } else {
     launch_k(k_lhs_elem<double>, nblk(c->ne), kThreads, c->stream, *c, rb);
+    kmark(c, KS_LHS_ELEM, 1);
+    kmark(c, KS_LHS_GATHER, 0);
     launch_k(k_lhs_gather<double>, nb, kThreads, c->stream, *c, rb);
   }
+  kmark(c, KS_LHS_GATHER, 1);
   launch_k(k_lhs_ep, 1, 1024, c->stream, *c, rb, nb);
   launch_k(k_lhs_bc, nblk((long long)c->np + c->n_obc), kThreads, c->stream, *c, rb);
   c->launches += 6;
@@ -95,13 +101,19 @@ int launch_gwce_lhs(adc_ctx *c) {
 }
 
 int launch_gwce_rhs(adc_ctx *c) {
+  kmark(c, KS_RHS_ELEM, 0);
   if (f32_assembly(c)) {
     launch_k(k_rhs_elem<float>, nblk(c->ne), kThreads, c->stream, *c);
+    kmark(c, KS_RHS_ELEM, 1);
+    kmark(c, KS_RHS_GATHER, 0);
     launch_k(k_rhs_gather<float>, nblk(c->np), kThreads, c->stream, *c);
   } else {
     launch_k(k_rhs_elem<double>, nblk(c->ne), kThreads, c->stream, *c);
+    kmark(c, KS_RHS_ELEM, 1);
+    kmark(c, KS_RHS_GATHER, 0);
     launch_k(k_rhs_gather<double>, nblk(c->np), kThreads, c->stream, *c);
   }
+  kmark(c, KS_RHS_GATHER, 1);
   c->launches += 2;
   int rc = launch_flux_rhs(c);   // gwce.F:1737-1834, before the elevation rows
   if (rc) return rc;
@@ -119,6 +131,7 @@ int launch_gwce_rhs(adc_ctx *c) {
 // The whole 2DDI step (TIMESTEP order), without host synchronisation.
 static int enqueue_step(adc_ctx *c, bool timed) {
   int rc;
+  c->kmark = timed ? 1 : 0;
   if (timed) cudaEventRecordWithFlags(c->ev[0], c->stream, cudaEventRecordExternal);
   if ((rc = launch_shift_friction(c))) return rc;
   if (timed) cudaEventRecordWithFlags(c->ev[1], c->stream, cudaEventRecordExternal);
@@ -132,6 +145,7 @@ static int enqueue_step(adc_ctx *c, bool timed) {
   if (timed) cudaEventRecordWithFlags(c->ev[4], c->stream, cudaEventRecordExternal);
   if ((rc = launch_momentum(c))) return rc;
   if (timed) cudaEventRecordWithFlags(c->ev[5], c->stream, cudaEventRecordExternal);
+  c->kmark = 0;
   return ADC_OK;
 }
 
@@ -440,6 +454,8 @@ static void free_ctx(adc_ctx *c) {
     if (e) cudaEventDestroy(e);
   for (auto &e : c->run_ev)
     if (e) cudaEventDestroy(e);
+  for (auto &e : c->kev)
+    if (e) cudaEventDestroy(e);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete[] c->h_ell_of_sell;
   delete c;
@@ -486,6 +502,7 @@ static int bind_impl(const adc_params_t *p, const adc_arrays_t *a, int prec, adc
 #define B(x) do { int rc_ = (x); if (rc_) return fail(rc_); } while (0)
   if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) return fail(ADC_ERR_CUDA);
   for (auto &e : c->ev) cudaEventCreate(&e);
+  for (auto &e : c->kev) cudaEventCreate(&e);
   for (auto &e : c->run_ev) cudaEventCreate(&e);
   const int np = c->np, ne = c->ne;
   B(dalloc(&c->x, np)); B(up(c->x, a->x, np));
@@ -879,6 +896,23 @@ int adc_get_scalars(adc_ctx *c, adc_scalars_t *out) {
     out->vortex_counter = v.counter;
     out->vortex_wtratio = v.wtratio;
   }
+  return ADC_OK;
+}
+
+int adc_kernel_times(adc_ctx *c, double *ms, int n) {
+  if (!c || !ms || n < 0) return ADC_ERR_ARG;
+  float t[ADC_NKT] = {0};
+  auto span = [&](int k, cudaEvent_t a, cudaEvent_t b) { cudaEventElapsedTime(&t[k], a, b); };
+  span(ADC_KT_LHS_ELEM, c->kev[2 * KS_LHS_ELEM], c->kev[2 * KS_LHS_ELEM + 1]);
+  span(ADC_KT_LHS_GATHER, c->kev[2 * KS_LHS_GATHER], c->kev[2 * KS_LHS_GATHER + 1]);
+  span(ADC_KT_RHS_ELEM, c->kev[2 * KS_RHS_ELEM], c->kev[2 * KS_RHS_ELEM + 1]);
+  span(ADC_KT_RHS_GATHER, c->kev[2 * KS_RHS_GATHER], c->kev[2 * KS_RHS_GATHER + 1]);
+  span(ADC_KT_JCG, c->ev[2], c->ev[3]);
+  span(ADC_KT_WETDRY, c->ev[3], c->ev[4]);
+  span(ADC_KT_MOM_ELEM, c->kev[2 * KS_MOM_ELEM], c->kev[2 * KS_MOM_ELEM + 1]);
+  span(ADC_KT_MOM_NODE, c->kev[2 * KS_MOM_NODE], c->kev[2 * KS_MOM_NODE + 1]);
+  cudaGetLastError();
+  for (int k = 0; k < n && k < ADC_NKT; ++k) ms[k] = t[k];
   return ADC_OK;
 }
 

@@ -143,24 +143,82 @@ def _quadtree_leaves(lx, ly, h_fn, root):
             np.concatenate([l[2] for l in leaves]))
 
 
+def _poisson_disk(px, py, h, fixed, beta, rng):
+    """Thin candidate points to a Poisson-disk set: no two kept points closer
+    than beta * min(h_i, h_j).  Conflicts come from each point's nearest
+    candidates; a maximal independent set of the conflict graph is taken by
+    random priorities (Luby's rounds), with the `fixed` points (boundary)
+    always kept."""
+    from scipy.spatial import cKDTree
+    pts = np.column_stack([px, py])
+    tree = cKDTree(pts)
+    k = 12
+    dist, idx = tree.query(pts, k=k)
+    i = np.repeat(np.arange(px.size), k - 1)
+    j = idx[:, 1:].ravel()
+    d = dist[:, 1:].ravel()
+    ok = j < px.size
+    i, j, d = i[ok], j[ok], d[ok]
+    conflict = d < beta * np.minimum(h[i], h[j])
+    i, j = i[conflict], j[conflict]
+    keep = i < j
+    i, j = np.concatenate([i[keep], j[~keep]]), np.concatenate([j[keep], i[~keep]])
+    pair = np.unique(i.astype(np.int64) * px.size + j)
+    i, j = pair // px.size, pair % px.size
+    prio = rng.random(px.size)
+    prio[fixed] = 2.0 + prio[fixed]          # boundary points win every conflict
+    state = np.zeros(px.size, np.int8)       # 0 undecided, 1 kept, -1 removed
+    while True:
+        live = (state[i] == 0) & (state[j] == 0)
+        i, j = i[live], j[live]
+        if i.size == 0:
+            break
+        # a point loses a round if some undecided neighbour has a higher priority
+        lose = np.zeros(px.size, bool)
+        lose[np.where(prio[i] < prio[j], i, j)] = True
+        win = (state == 0) & ~lose
+        state[win] = 1
+        kill = np.concatenate([j[win[i]], i[win[j]]])
+        state[kill[state[kill] == 0]] = -1
+    state[state == 0] = 1
+    return state == 1
+
+
+def _edge_points(x0, y0, x1, y1, h_of):
+    """Points along a domain edge at the local target spacing: the k-th
+    point sits where the integral of 1/h along the edge reaches k (the
+    endpoints included)."""
+    L = float(np.hypot(x1 - x0, y1 - y0))
+    t = np.linspace(0.0, L, int(L / 5.0) + 2)
+    xs = x0 + (x1 - x0) * t / L
+    ys = y0 + (y1 - y0) * t / L
+    inv = 1.0 / h_of(xs, ys)
+    n_int = np.concatenate([[0.0], np.cumsum(0.5 * (inv[1:] + inv[:-1]) * np.diff(t))])
+    n = max(int(round(n_int[-1])), 1)
+    tk = np.interp(np.linspace(0.0, n_int[-1], n + 1), n_int, t)
+    return x0 + (x1 - x0) * tk / L, y0 + (y1 - y0) * tk / L
+
+
 def surge_mesh(seed: int = 2024, target_nodes: int = 600_000, lx: float = 1000e3,
                ly: float = 800e3, h_min: float = 60.0, h_max: float = 20e3,
                coast_y: float = 640e3, coast_amp: float = 40e3,
                shelf_width: float = 100e3, shelf_depth: float = 30.0,
                ocean_depth: float = 4000.0, land_height: float = 6.0,
                grf_sigma: float = 2.0, grf_ell: float = 5e3,
-               land_grading: float = 3.0, jitter: float = 0.3) -> RawMesh:
-    """Graded storm-surge mesh (~600k nodes, ~1.18M triangles).
+               land_grading: float = 3.0, beta: float = 0.75, verbose: bool = False) -> RawMesh:
+    """Graded storm-surge mesh (~600k nodes, ~1.2M triangles).
 
-    Points: seeded jittered quadtree sampling whose cell size follows the
-    target edge length h = min(h_max, h_min + alpha * d), d the distance to a
-    seeded fractal coastline (a stand-in for Poisson-disk sampling with the
-    same grading; the floodplain grades land_grading times faster); alpha is
-    bisected so the node count meets the target.
-    Triangles: Delaunay (scipy).  Bathymetry: shelf profile (ocean_depth
-    offshore, shelf break shelf_width offshore at shelf_depth, 0 m at the
-    coast, land rising to land_height) plus a Gaussian random field.
-    Open boundary: the south edge; the other sides are mainland (IBTYPE 0).
+    Points: seeded Poisson-disk sampling whose spacing follows the target
+    edge length h = min(h_max, h_min + alpha * d), d the distance to a
+    seeded fractal coastline (the floodplain grades land_grading times
+    faster): two uniform candidates per quadtree cell no larger than h are
+    thinned so no two points are closer than beta * h; the domain edges
+    carry points at spacing h; alpha is bisected so the node count meets the
+    target.  Triangles: Delaunay (scipy).  Bathymetry: shelf profile
+    (ocean_depth offshore, shelf break shelf_width offshore at shelf_depth,
+    0 m at the coast, land rising to land_height) plus a Gaussian random
+    field.  Open boundary: the south edge; the other sides are mainland
+    (IBTYPE 0).
     """
     from scipy.spatial import Delaunay
 
@@ -181,52 +239,75 @@ def surge_mesh(seed: int = 2024, target_nodes: int = 600_000, lx: float = 1000e3
             return np.minimum(h_max, h_min + a * d)
         return h_fn
 
+    def h_at(px, py):
+        sd = coast_at(px) - py
+        a = np.where(sd < 0, land_grading * alpha_cur[0], alpha_cur[0])
+        return np.minimum(h_max, h_min + a * np.abs(sd))
+
+    alpha_cur = [0.05]
+
+    def candidates(alpha):
+        alpha_cur[0] = alpha
+        cx, cy, size = _quadtree_leaves(lx, ly, make_h(alpha), h_max)
+        cx = np.repeat(cx, 2)
+        cy = np.repeat(cy, 2)
+        size = np.repeat(size, 2)
+        px = cx + size * rng.uniform(-0.5, 0.5, cx.size)
+        py = cy + size * rng.uniform(-0.5, 0.5, cy.size)
+        return px, py
+
+    # the thinned set keeps a stable fraction of the candidates: calibrate
+    # it once, then bisect alpha on the candidate count
     lo, hi = 0.005, 0.5
-    for _ in range(30):
+    frac = 0.19
+    for _ in range(40):
         mid = np.sqrt(lo * hi)
         cx, _, _ = _quadtree_leaves(lx, ly, make_h(mid), h_max)
-        if cx.size > target_nodes:
+        if 2 * cx.size * frac > target_nodes:
             lo = mid
         else:
             hi = mid
-        if abs(cx.size - target_nodes) < 0.01 * target_nodes:
+        if abs(2 * cx.size * frac - target_nodes) < 0.005 * target_nodes:
             break
     alpha = mid
-    cx, cy, size = _quadtree_leaves(lx, ly, make_h(alpha), h_max)
-    jit = jitter
-    px = cx + size * rng.uniform(-jit, jit, cx.size)
-    py = cy + size * rng.uniform(-jit, jit, cy.size)
-    # keep interior points off the boundary
-    m = 0.2 * size
-    px = np.clip(px, m, lx - m)
-    py = np.clip(py, m, ly - m)
-    # boundary points, spacing follows the local cell size, bulged outward
-    # by a tiny convex offset so every boundary point is a hull vertex
-    def edge_pts(x0, y0, x1, y1, n_out):
-        pts = []
-        t = 0.0
-        L = np.hypot(x1 - x0, y1 - y0)
-        while t < L:
-            xx = x0 + (x1 - x0) * t / L
-            yy = y0 + (y1 - y0) * t / L
-            pts.append((xx, yy, t))
-            h = float(make_h(alpha)(np.array([xx]), np.array([yy]), np.array([0.0]))[0])
-            t += max(h, 1.0)
-        pts = np.asarray(pts)
-        s = pts[:, 2] / L
-        bulge = 1e-6 * L * s * (1 - s) * 4.0
-        return pts[:, 0] + n_out[0] * bulge, pts[:, 1] + n_out[1] * bulge
-    bx, by = [], []
-    for (x0, y0, x1, y1, n) in [(0, 0, lx, 0, (0, -1)), (lx, 0, lx, ly, (1, 0)),
-                                (lx, ly, 0, ly, (0, 1)), (0, ly, 0, 0, (-1, 0))]:
-        ex, ey = edge_pts(x0, y0, x1, y1, n)
-        bx.append(ex)
-        by.append(ey)
-    bx = np.concatenate(bx)
-    by = np.concatenate(by)
-    nb = bx.size
-    x = np.concatenate([bx, px])
-    y = np.concatenate([by, py])
+    for attempt in range(3):
+        px, py = candidates(alpha)
+        hb = h_at(px, py)
+        inside = ((px > 0.5 * hb) & (px < lx - 0.5 * hb) & (py > 0.5 * hb) & (py < ly - 0.5 * hb))
+        px, py, hb = px[inside], py[inside], hb[inside]
+        bx, by = [], []
+        for (x0, y0, x1, y1) in [(0, 0, lx, 0), (lx, 0, lx, ly), (lx, ly, 0, ly), (0, ly, 0, 0)]:
+            ex, ey = _edge_points(x0, y0, x1, y1, h_at)
+            bx.append(ex[:-1])
+            by.append(ey[:-1])
+        bx = np.concatenate(bx)
+        by = np.concatenate(by)
+        nb = bx.size
+        ax = np.concatenate([bx, px])
+        ay = np.concatenate([by, py])
+        fixed = np.zeros(ax.size, bool)
+        fixed[:nb] = True
+        kept = _poisson_disk(ax, ay, h_at(ax, ay), fixed, beta, rng)
+        n_kept = int(kept.sum())
+        if verbose:
+            print(f"surge_mesh: alpha {alpha:.5f} candidates {ax.size} kept {n_kept}")
+        if abs(n_kept - target_nodes) < 0.015 * target_nodes:
+            break
+        # the node count scales about as alpha^-0.95 for these gradings
+        alpha *= (n_kept / target_nodes) ** (1.0 / 0.95)
+    x = ax[kept]
+    y = ay[kept]
+    # boundary points bulge outward by a tiny convex offset so that every
+    # one is a hull vertex of the triangulation
+    onb = np.zeros(x.size, bool)
+    onb[:nb] = True
+    for (cond, nx_, ny_, L) in [(np.abs(y) < 1e-6, 0.0, -1.0, lx), (np.abs(x - lx) < 1e-6, 1.0, 0.0, ly),
+                                (np.abs(y - ly) < 1e-6, 0.0, 1.0, lx), (np.abs(x) < 1e-6, -1.0, 0.0, ly)]:
+        m = onb & cond
+        sfrac = (x[m] / L) if nx_ == 0.0 else (y[m] / L)
+        bulge = 1e-6 * L * sfrac * (1 - sfrac) * 4.0
+        x[m] = x[m] + nx_ * bulge
+        y[m] = y[m] + ny_ * bulge
     tri = Delaunay(np.column_stack([x, y]))
     nm = tri.simplices.astype(np.int64)
     # orient counter-clockwise

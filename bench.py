@@ -2,23 +2,36 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl adcgpu|reference]
 
-A "step" is one ADCIRC time step (dt = 1 s) of the ~600k-node synthetic
-surge mesh: friction and time-level shift, GWCE assembly, the JCG solve,
-wetting/drying and the momentum update, all device resident.  The value is
-simulated days per wall-clock hour over K timed steps after W warm-up
-steps.  For N > 1 (torchrun) every rank runs an independent replica on its
-own GPU (the path does not shard without a domain decomposition): value is
-the aggregate over ranks, timed as the max over ranks.
+A bench step is one simulated hour of the ~600k-node synthetic surge mesh:
+3600 ADCIRC time steps (dt = 1 s) of friction and time-level shift, GWCE
+assembly, the JCG solve, wetting/drying and the momentum update, all device
+resident and replayed as a captured CUDA graph.  W warm-up hours run first,
+then K timed hours; every hour ends with an output (the state read back to
+the host), which is outside the device-timed region.  The defaults cover
+the specified simulated day (4 + 20 hours); the storm makes landfall at
+about 19 h.
+
+Every precision path runs the same hours and is compared with the plain
+FP64 path at each hourly output (max |d eta| over all nodes, over nodes wet
+in both runs, RMS |d u|, wet/dry flag mismatches).  `value` is the fastest
+path whose max |d eta| stays within 1 mm at every hour; the plain FP64 path
+always qualifies.  The plain FP64 GPU path itself is tied to the FP64
+oracle by the parity tests (tests/test_gpu_surge.py: cold start and a
+mid-storm window on this mesh), and a short oracle check runs here too.
+
+For N > 1 (torchrun) every rank runs an independent replica on its own GPU
+(the path does not shard without a domain decomposition): value is the
+aggregate over ranks, timed as the max over ranks.
 
 --impl reference times the CPU restatement of the reference (the serial
-FP64 oracle, the reference's own Fortran cannot be built on this image) on
-a bounded sample of the same workload.
+FP64 oracle; the reference's own Fortran cannot be built on this image) on
+a bounded sample of the same workload, with the case built without the GPU
+library.
 """
 from __future__ import annotations
 
 import argparse
 import json
-import math
 import os
 import statistics
 import subprocess
@@ -35,6 +48,8 @@ sys.path.insert(0, str(ROOT))
 METRIC = "sim-days/wall-hour, 600k-node surge mesh: chosen vs plain FP64 GPU, Δη≤1mm"
 UNIT = "sim-days/wall-hour"
 HBM_FALLBACK_GBS = 6650.0
+BOUND_M = 1.0e-3            # the metric's accuracy bound on max |d eta|
+HOUR_STEPS = 3600           # time steps per bench step at dt = 1 s
 
 
 def forcing(case):
@@ -45,6 +60,15 @@ def forcing(case):
     f = v.fixes[0]
     return (f"Holland vortex NWS=8 (pc {f[3] / 100:.0f} hPa, Rmax {f[5]:.0f} km, "
             f"B 1.3, {np.hypot(f[6], f[7]):.0f} m/s straight track)")
+
+
+def settings(case):
+    p = case.params
+    fr = ("hybrid friction CF 0.0025, HBREAK %g m, FTHETA %g, FGAMMA %.3f" % (p["hbreak"], p["ftheta"],
+                                                                             p["fgamma"])
+          if p.get("ifhybf") else "quadratic friction")
+    return (f"{fr}, ESLM {float(case.arrays['evm'][0]):g} m^2/s, SLIM {p['slim']:g}, TAU0 -1 "
+            f"(0.020 at <=10 m, else 0.005), H0 {p['h0']} m, JCG tol {p['convcr']:g}, ITMAX {p['itmax']}")
 
 
 def _peaks():
@@ -115,6 +139,10 @@ class ClockSampler:
                 "samples": len(self.samples)}
 
 
+# ----------------------------------------------------------------------------
+# Algorithmic bytes per launch (what each roofline's `achieved` is built on)
+# ----------------------------------------------------------------------------
+
 def jcg_bytes(nnz_o: int, npn: int, iters: float, vbytes: int = 8) -> float:
     """Algorithmic HBM bytes of one JCG solve (persistent kernel), counted
     as a streaming implementation would move them.
@@ -132,42 +160,51 @@ def jcg_bytes(nnz_o: int, npn: int, iters: float, vbytes: int = 8) -> float:
             npn * (64.0 + 44.0 + 24.0 + 68.0 * iters + 60.0))
 
 
-def profiled_traffic(kernel: str = "jcg_kernel<1, float>"):
-    """DRAM bytes (read + write) of one launch of `kernel`, from the committed
-    ncu summary profiles/surge_kernels_full.md, or None."""
-    p = ROOT / "profiles" / "surge_kernels_full.md"
-    if not p.exists():
-        return None
-    cols, vals = None, {}
-    for line in p.read_text().splitlines():
-        cells = [c.strip() for c in line.strip().strip("|").split("|")]
-        if line.startswith("| metric |"):
-            cols = [c.strip("`") for c in cells[1:]]
-        elif cols and line.startswith("| DRAM read") or cols and line.startswith("| DRAM write"):
-            vals[cells[0]] = cells[1:]
-    if not cols or kernel not in cols or len(vals) != 2:
-        return None
-    k = cols.index(kernel)
-    try:
-        return sum(float(v[k]) * 1e6 for v in vals.values())   # Mbyte -> bytes
-    except (ValueError, IndexError):
-        return None
+def kernel_bytes(npn: int, ne: int, f32_mom: bool = False) -> dict:
+    """Algorithmic bytes of one launch of the element and gather kernels.
+
+    rhs_elem   per node: 19 gathered FP64 nodal fields + NODECODE read once
+               (156 B); per element: NM 12 + FDXE/FDYE 48 + AREAS 8 + ALPHAL
+               8 + NOFF 4 (80 B) and three FP64 contributions written (24 B).
+    rhs_gather per node: CSR pointer 4 + GWCE_LV write 8 + 40 B of nodal
+               I/O; per element-vertex entry: index 4 + contribution 8.
+    mom_elem   per node: 12 gathered FP64 nodal fields + NODECODE (100 B);
+               per element: 80 B element data + 6 contributions (48 B, or
+               24 B in FP32).
+    mom_node   per node: CSR pointer 4 + 15 FP64 nodal fields read and 6
+               written (168 B) + boundary data; per entry: index 4 + two
+               contributions (16 B, or 8 B in FP32).
+    """
+    cb = 4 if f32_mom else 8
+    return {
+        "rhs_elem": npn * 156.0 + ne * (80.0 + 24.0),
+        "rhs_gather": npn * (4.0 + 8.0 + 40.0) + 3.0 * ne * 12.0,
+        "mom_elem": npn * 100.0 + ne * (80.0 + 6.0 * cb),
+        "mom_node": npn * (4.0 + 168.0) + 3.0 * ne * (4.0 + 2.0 * cb),
+    }
 
 
-def make_case(name: str):
+# ----------------------------------------------------------------------------
+
+def make_case(name: str, prep=None):
     from adcirc_b200 import model
     if name == "surge":
-        return model.surge_case()
+        return model.surge_case(prep=prep)
     if name == "channel":
-        return model.channel_case()
+        return model.channel_case(prep=prep)
     raise ValueError(name)
+
+
+def _oracle():
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle
+    oracle.build()
+    return oracle
 
 
 def run_cpu_baseline(case, max_seconds: float = 20.0, min_steps: int = 2, it0: int = 1):
     """The oracle (serial FP64 restatement) on a bounded sample of steps."""
-    sys.path.insert(0, str(ROOT / "oracle"))
-    import oracle
-    oracle.build()
+    oracle = _oracle()
     c = case.clone()
     om = oracle.OracleModel(c)
     t0 = time.perf_counter()
@@ -184,23 +221,51 @@ def run_cpu_baseline(case, max_seconds: float = 20.0, min_steps: int = 2, it0: i
 
 
 def bench_reference(args, rank, world):
+    """The oracle timed on the host cores: each bench step is a bounded
+    sample of one simulated hour (as many time steps as fit in
+    --ref-seconds), run in sequence from cold start."""
     if rank != 0:
         return
-    case = make_case(args.case)
+    oracle = _oracle()
+    case = make_case(args.case, prep=oracle.mesh_prep())   # no GPU library on this arm
     dt = case.params["dt"]
-    budget = min(90.0, max(10.0, 3.0 * (args.steps + args.warmup)))
-    n, el, its = run_cpu_baseline(case, max_seconds=budget)
-    v = sim_days_per_hour(n, dt, el)
+    om = oracle.OracleModel(case)
+    it = 1
+    its = []
+
+    def sample(seconds):
+        nonlocal it
+        t0 = time.perf_counter()
+        n = 0
+        while True:
+            its.append(om.step(it).numitr)
+            it += 1
+            n += 1
+            el = time.perf_counter() - t0
+            if el >= seconds:
+                return n, el
+    for _ in range(args.warmup):
+        sample(min(args.ref_seconds, 2.0))
+    n_tot, el_tot = 0, 0.0
+    for _ in range(args.steps):
+        n, el = sample(args.ref_seconds)
+        n_tot += n
+        el_tot += el
+    om.close()
+    v = sim_days_per_hour(n_tot, dt, el_tot)
     line = {
-        "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": n,
-        "warmup": 0, "ms_per_step": 1000.0 * el / n, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "impl": "reference",
-        "config": {"workload": f"{args.case}: {case.sizes['np']} nodes, {case.sizes['ne']} elements, dt {dt} s, "
-                               f"M2+K1 tides, {forcing(case)}, wet/dry on, plain FP64 JCG",
-                   "parallelism": "serial (1 core)"},
+        "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1000.0 * el_tot / n_tot * (HOUR_STEPS if
+                                                                        args.case == "surge" else 1),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "impl": "reference",
+        "config": {"workload": f"{args.case}: {case.sizes['np']} nodes, {case.sizes['ne']} elements, "
+                               f"dt {dt} s, M2+K1 tides, {forcing(case)}, wet/dry on, plain FP64 JCG",
+                   "parallelism": "serial (1 core)", "bench_step": "one simulated hour (sampled)"},
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
-                         "sample": f"{n} time steps from cold start ({el:.1f} s)"},
+                         "sample": f"{n_tot} time steps from cold start in {args.steps} samples of "
+                                   f"{args.ref_seconds:g} s ({el_tot:.1f} s), after {args.warmup} "
+                                   f"warm-up samples"},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "jcg_iters_per_step": float(np.mean(its)),
     }
@@ -210,31 +275,13 @@ def bench_reference(args, rank, world):
 PATHS = {
     # name: (bind mode, description)
     "plain": (0, "plain FP64 (reference arithmetic)"),
-    "chosen": (8 | 16, "FP32 SpMV matrix + FP32 momentum element terms, FP64 assembly, "
-                       "dot products, norms, stopping test and state"),
+    "spmv32": (8, "FP32 copy of the scaled JCG matrix (FP64 products, dot products, norms, "
+                  "stopping test, assembly, momentum and state)"),
+    "spmv32_mom32": (8 | 16, "FP32 SpMV matrix + FP32 momentum element terms, FP64 assembly, "
+                             "dot products, norms, stopping test and state"),
     "mixed": (1, "FP32 GWCE assembly + SpMV matrix + momentum, FP64 reductions and state"),
+    "warm": (2, "plain FP64 with the extrapolated JCG initial guess (residual-tested fallback)"),
 }
-
-
-def _timed(gpu, it, W, K, dist):
-    """W untimed steps, then K steps replayed as one graph, device-timed."""
-    import torch
-    if W > 0:
-        gpu.run(it, W)
-        it += W
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    l0 = gpu.launches()
-    numitr, _ = gpu.run(it, K)
-    torch.cuda.synchronize()
-    it += K
-    ms = gpu.last_run_ms()
-    if dist:
-        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    return it, ms, np.asarray(numitr), gpu.launches() - l0
 
 
 def _accuracy(a, ref):
@@ -249,112 +296,224 @@ def _accuracy(a, ref):
             "rms_du_ms": float(du), "wetdry_mismatch": int(mm.sum())}
 
 
-def bench_gpu(args, rank, world, dist):
+def _snap(arrays):
+    return {k: arrays[k].copy() for k in ("eta2", "uu2", "vv2", "nodecode")}
+
+
+def _sync_dev(dist):
     import torch
-    from adcirc_b200 import build, model, _lib
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+
+
+def run_path(name, case, W, K, dist, ref_snaps, stop_on_fail):
+    """Binds `case` in mode PATHS[name] and runs W + K hours.  Returns the
+    per-hour records, the timed device ms (max over ranks) and the model."""
+    from adcirc_b200 import model
+    gpu = model.GpuModel(case, prec=PATHS[name][0])
+    it = 1
+    hours = []
+    ms_timed = 0.0
+    launches = 0
+    snaps = []
+    failed_at = None
+    for h in range(1, W + K + 1):
+        timed = h > W
+        _sync_dev(dist)
+        l0 = gpu.launches()
+        numitr, last = gpu.run(it, HOUR_STEPS)
+        _sync_dev(dist)
+        ms = gpu.last_run_ms()
+        if dist:
+            import torch
+            t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        it += HOUR_STEPS
+        if timed:
+            ms_timed += ms
+            launches += gpu.launches() - l0
+        gpu.sync_to_host()                       # the hourly output
+        rec = {"hour": h, "ms_per_time_step": ms / HOUR_STEPS, "jcg_iters_mean": float(np.mean(numitr)),
+               "jcg_iters_max": int(np.max(numitr)), "status": int(last.status),
+               "finite": bool(np.isfinite(case.arrays["eta2"]).all())}
+        if ref_snaps is None:
+            snaps.append(_snap(case.arrays))
+        else:
+            rec.update(_accuracy(case.arrays, ref_snaps[h - 1]))
+            if failed_at is None and not rec["max_deta_m"] <= BOUND_M:
+                failed_at = h
+        hours.append(rec)
+        if not rec["finite"] or rec["status"] != 0:
+            failed_at = failed_at or h
+            break
+        if failed_at is not None and stop_on_fail:
+            break
+    return {"hours": hours, "ms_timed": ms_timed, "launches": launches, "it": it,
+            "failed_at": failed_at, "snaps": snaps if ref_snaps is None else None}, gpu
+
+
+def oracle_check(case_fn, nsteps=5):
+    """Cold-start steps of the plain FP64 GPU path against the FP64 oracle
+    (built with the oracle's own static tables): max relative field error
+    and iteration counts."""
+    from adcirc_b200 import model
+    oracle = _oracle()
+    c0 = case_fn(prep=oracle.mesh_prep())
+    cg = case_fn()
+    om = oracle.OracleModel(c0)
+    its_o = [om.step(it).numitr for it in range(1, nsteps + 1)]
+    om.close()
+    g = model.GpuModel(cg)
+    its_g, _ = g.run(1, nsteps)
+    g.sync_to_host()
+    g.close()
+    rel = {}
+    for f in ("eta2", "uu2", "vv2"):
+        a, b = c0.arrays[f], cg.arrays[f]
+        rel[f] = float(np.abs(a - b).max() / max(np.abs(a).max(), 1e-30))
+    return {"steps": nsteps, "max_rel": rel, "iters_oracle": its_o,
+            "iters_gpu": [int(x) for x in its_g], "iters_equal": list(its_o) == list(its_g)}
+
+
+def bench_gpu(args, rank, world, dist):
+    import copy
+    import torch
+    from adcirc_b200 import build, model, meshgen
     build.build()
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
-    case = make_case(args.case)
-    cpu_case = case.clone() if (rank == 0 and world == 1 and not args.no_cpu) else None
-    dt = case.params["dt"]
+    raw = meshgen.surge_mesh() if args.case == "surge" else None
+
+    def case_fn(prep=None):
+        if args.case == "surge":
+            return model.surge_case(raw=copy.deepcopy(raw), prep=prep)
+        return model.channel_case(prep=prep)
+
+    base = case_fn()
+    dt = base.params["dt"]
+    npn, ne = base.sizes["np"], base.sizes["ne"]
     W, K = args.warmup, args.steps
-    names = ["chosen", "plain"] + ([] if args.no_mixed else ["mixed"])
-    cases = {n: case.clone() for n in names}
-    models = {n: model.GpuModel(cases[n], prec=PATHS[n][0]) for n in names}
-    its = {n: 1 for n in names}
+    names = ["plain"] + [p for p in args.paths.split(",") if p and p != "plain"]
     res = {}
+    models = {}
+    plain_snaps = None
     with ClockSampler(local) as clk:
         for n in names:
-            its[n], ms, numitr, launches = _timed(models[n], its[n], W, K, dist)
-            res[n] = {"value": world * sim_days_per_hour(K, dt, ms / 1000.0), "ms_per_step": ms / K,
-                      "jcg_iters_per_step": float(numitr.mean()), "gpu_launches": int(launches),
-                      "mode": PATHS[n][0], "arithmetic": PATHS[n][1]}
-    gpu = models["chosen"]
-    # per-phase device times and the JCG roofline of the chosen path
-    n_ph = 20
-    ph = {"shift": 0.0, "gwce": 0.0, "jcg": 0.0, "wetdry": 0.0, "momentum": 0.0}
-    iters = []
-    for n in names:   # every path advances the same steps
-        for k in range(n_ph):
-            o = models[n].step(its[n] + k)
-            if n == "chosen":
-                iters.append(o.numitr)
-                for kk, vv in gpu.phase_times().items():
-                    ph[kk] += vv / n_ph
-        its[n] += n_ph
-    # e2e through the per-step public call (host round trip every step)
-    K2 = min(K, args.e2e_steps)
-    torch.cuda.synchronize()
+            r, gpu = run_path(n, base.clone(), W, K, dist, plain_snaps, stop_on_fail=(n != "plain"))
+            if n == "plain":
+                plain_snaps = r.pop("snaps")
+            else:
+                r.pop("snaps")
+            ran_all = len(r["hours"]) == W + K
+            within = ran_all and r["failed_at"] is None
+            res[n] = {
+                "mode": PATHS[n][0], "arithmetic": PATHS[n][1],
+                "value": (world * sim_days_per_hour(K * HOUR_STEPS, dt, r["ms_timed"] / 1000.0)
+                          if ran_all and r["ms_timed"] > 0 else None),
+                "ms_per_time_step": r["ms_timed"] / (K * HOUR_STEPS) if ran_all else None,
+                "within_bound_all_hours": bool(within) if n != "plain" else True,
+                "first_hour_beyond_1mm": r["failed_at"], "hours_run": len(r["hours"]),
+                "jcg_iters_per_step": float(np.mean([x["jcg_iters_mean"] for x in r["hours"][W:]]))
+                if ran_all else None,
+                "gpu_launches": r["launches"], "per_hour": r["hours"]}
+            models[n] = (gpu, r["it"])
+    chosen = max((n for n in names if res[n]["within_bound_all_hours"] and res[n]["value"]),
+                 key=lambda n: res[n]["value"])
+    gpu, it = models[chosen]
+    # per-kernel device times: single steps through the captured step graph
+    kt_sum, iters = {}, []
+    n_kt = 20
+    for k in range(n_kt):
+        o = gpu.step(it + k)
+        iters.append(o.numitr)
+        for kk, vv in gpu.kernel_times().items():
+            kt_sum[kk] = kt_sum.get(kk, 0.0) + vv / n_kt
+    it += n_kt
+    # e2e: the reference-facing per-step call with host round trips, plus
+    # the hourly output read back to the host
+    e2e_steps = int(round(args.e2e_hours * HOUR_STEPS))
+    st = np.dtype(np.float64).itemsize
+    sync_bytes = sum(v.nbytes for k, v in base.arrays.items() if k in model.STATE_F64 + model.STATE_I32)
+    _sync_dev(dist)
     t0 = time.perf_counter()
-    for k in range(K2):
-        gpu.step(its["chosen"] + k)
+    for k in range(e2e_steps):
+        gpu.step(it + k)
+        if (k + 1) % HOUR_STEPS == 0:
+            gpu.sync_to_host()
     el = time.perf_counter() - t0
-    for n in names:
-        if n != "chosen":
-            models[n].run(its[n], K2)
-        its[n] += K2
+    it += e2e_steps
     if dist:
         t = torch.tensor([el], dtype=torch.float64, device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         el = float(t.item())
-    e2e = world * sim_days_per_hour(K2, dt, el)
-    # accuracy of the FP32 paths against the FP64 path at hourly outputs
-    acc = {n: [] for n in names if n != "plain"}
-    hours = []
-    spd = int(round(3600.0 / dt))
-    for h in range(1, args.accuracy_hours + 1):
-        target = h * spd + 1          # next step to run once hour h is complete
-        if target <= its["plain"]:
-            continue
-        for n in names:
-            models[n].run(its[n], target - its[n])
-            its[n] = target
-            models[n].sync_to_host()
-        hours.append(h)
-        for n in acc:
-            acc[n].append(_accuracy(cases[n].arrays, cases["plain"].arrays))
-    a = case.arrays
-    nnz_o = int((a["nneigh"] - 1).sum())
-    npn = case.sizes["np"]
-    mean_it = float(np.mean(iters))
+    e2e = world * sim_days_per_hour(e2e_steps, dt, el)
+    from adcirc_b200 import _lib
+    import ctypes as C
+    h2d = HOUR_STEPS * C.sizeof(_lib.AdcStep)
+    d2h = HOUR_STEPS * C.sizeof(_lib.AdcStepOut) + sync_bytes
+    for g, _ in models.values():
+        g.close()
+    # rooflines
     peak, peak_kind = _peaks()
-    achieved = (jcg_bytes(nnz_o, npn, mean_it, vbytes=4) / (ph["jcg"] / 1000.0) / 1e9
-                if ph["jcg"] > 0 else 0.0)
-    worst = {n: {k: max(x[k] for x in v) for k in v[0]} if v else None for n, v in acc.items()}
+    a = base.arrays
+    nnz_o = int((a["nneigh"] - 1).sum())
+    mean_it = float(np.mean(iters))
+    mode = PATHS[chosen][0]
+    vb = 4 if mode & 9 else 8
+    kb = kernel_bytes(npn, ne, f32_mom=bool(mode & 17))
+    jb = jcg_bytes(nnz_o, npn, mean_it, vbytes=vb)
+    rl = {}
+    for k, nbytes in [("jcg", jb)] + list(kb.items()):
+        ms = kt_sum.get(k, 0.0)
+        ach = nbytes / (ms / 1000.0) / 1e9 if ms > 0 else 0.0
+        rl[k] = {"ms": ms, "algorithmic_bytes": nbytes, "achieved_gbs": ach, "frac": ach / peak}
+    rl["jcg"]["iters_per_launch"] = mean_it
+    rl["jcg"]["us_per_iteration"] = 1000.0 * kt_sum.get("jcg", 0.0) / max(mean_it, 1e-9)
+    for k in ("lhs_elem", "lhs_gather", "wetdry"):
+        rl[k] = {"ms": kt_sum.get(k, 0.0), "algorithmic_bytes": None,
+                 "note": "work varies per step (incremental rebuild, front activity)"}
+    ocheck = oracle_check(case_fn) if (rank == 0 and not args.no_oracle) else None
     line = {
-        "metric": METRIC, "value": res["chosen"]["value"], "unit": UNIT, "n_gpus": world,
-        "steps": K, "warmup": W, "ms_per_step": res["chosen"]["ms_per_step"],
+        "metric": METRIC, "value": res[chosen]["value"], "unit": UNIT, "n_gpus": world,
+        "steps": K, "warmup": W, "ms_per_step": res[chosen]["ms_per_time_step"] * HOUR_STEPS,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64+f32", "data": "synthetic",
-        "config": {"workload": f"{args.case}: {npn} nodes, {case.sizes['ne']} elements, dt {dt} s, "
-                               f"M2+K1 tides, {forcing(case)}, wet/dry on",
-                   "path": "chosen: " + PATHS["chosen"][1],
-                   "nodes": npn, "elements": case.sizes["ne"], "parallelism": f"replicas x{world}",
-                   "l2": "resident state ~0.35 GB > 126 MB L2 (no flush)",
-                   "first_step": 1 + W},
-        "speedup_vs_plain_fp64": res["chosen"]["value"] / res["plain"]["value"],
+        "dtype": "f64" if mode == 0 else "f64+f32", "data": "synthetic",
+        "config": {"workload": f"{args.case}: {npn} nodes, {ne} elements, dt {dt} s, M2+K1 tides, "
+                               f"{forcing(base)}, wet/dry on, {settings(base)}",
+                   "bench_step": f"one simulated hour ({HOUR_STEPS} time steps, one graph replay "
+                                 f"per time step) followed by the hourly output",
+                   "timed_hours": [W + 1, W + K], "path": f"{chosen}: {PATHS[chosen][1]}",
+                   "nodes": npn, "elements": ne, "parallelism": f"replicas x{world}",
+                   "l2": "resident state ~0.35 GB > 126 MB L2 (no flush)"},
+        "chosen_path": chosen,
+        "speedup_vs_plain_fp64": res[chosen]["value"] / res["plain"]["value"],
+        "accuracy_bound": {"max_deta_m": BOUND_M, "comparator": "plain FP64 GPU path, hourly outputs"},
         "paths": res,
-        "accuracy_vs_fp64": {"hours": hours, "worst": worst, "per_hour": acc},
-        "jcg_iters_per_step": res["chosen"]["jcg_iters_per_step"],
-        "phase_ms": ph,
-        "roofline": {"bound": "hbm", "kernel": "jcg_kernel", "achieved": achieved, "peak": peak,
-                     "unit": "GB/s", "frac": achieved / peak, "traffic": profiled_traffic(),
-                     "traffic_source": "profiles/surge_kernels_full.md (ncu, one launch of "
-                                       "jcg_kernel<1, float>, DRAM bytes read + written)",
-                     "peak_kind": peak_kind, "iters_per_launch": mean_it},
-        "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": 44, "d2h_bytes_per_step": 56,
-                "steps": K2, "api": "adc_timestep per step"},
-        "gpu_launches": res["chosen"]["gpu_launches"],
+        "oracle_check": ocheck,
+        "jcg_iters_per_step": res[chosen]["jcg_iters_per_step"],
+        "kernel_ms": kt_sum,
+        "roofline": {"bound": "hbm", "kernel": "jcg_kernel", "achieved": rl["jcg"]["achieved_gbs"],
+                     "peak": peak, "unit": "GB/s", "frac": rl["jcg"]["frac"], "traffic": None,
+                     "traffic_note": "DRAM bytes per launch come from an ncu capture, summarised "
+                                     "in profiles/", "peak_kind": peak_kind,
+                     "iters_per_launch": mean_it,
+                     "us_per_iteration": rl["jcg"]["us_per_iteration"]},
+        "rooflines": rl,
+        "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "time_steps": e2e_steps, "api": "adc_timestep per time step + adc_sync_to_host "
+                                                "every simulated hour"},
+        "gpu_launches": res[chosen]["gpu_launches"],
         "clocks": clk.summary(),
     }
-    if cpu_case is not None:
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu_case = case_fn(prep=_oracle().mesh_prep())
         n, el_c, its_c = run_cpu_baseline(cpu_case, max_seconds=args.cpu_seconds)
         line["cpu_baseline"] = {"value": sim_days_per_hour(n, dt, el_c), "unit": UNIT, "cores": 1,
                                 "kind": "port",
-                                "sample": f"{n} time steps of the same mesh from cold start ({el_c:.1f} s)"}
-    for m in models.values():
-        m.close()
+                                "sample": f"{n} time steps of the same mesh from cold start "
+                                          f"({el_c:.1f} s), JCG iterations {np.mean(its_c):.1f}/step"}
     if rank == 0:
         print(json.dumps(line), flush=True)
 
@@ -362,16 +521,18 @@ def bench_gpu(args, rank, world, dist):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=6000)
-    ap.add_argument("--warmup", type=int, default=200)
+    ap.add_argument("--steps", type=int, default=20, help="timed simulated hours")
+    ap.add_argument("--warmup", type=int, default=4, help="warm-up simulated hours")
     ap.add_argument("--impl", default="adcgpu", choices=["adcgpu", "reference"])
     ap.add_argument("--case", default="surge", choices=["surge", "channel"])
-    ap.add_argument("--accuracy-hours", type=int, default=3,
-                    help="hourly outputs at which the FP32 paths are compared with FP64")
-    ap.add_argument("--no-mixed", action="store_true", help="skip the all-FP32-assembly path")
-    ap.add_argument("--e2e-steps", type=int, default=500)
+    ap.add_argument("--paths", default="spmv32,spmv32_mom32",
+                    help="paths compared with plain FP64 (comma list of " + ",".join(PATHS) + ")")
+    ap.add_argument("--e2e-hours", type=float, default=1.0)
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    ap.add_argument("--ref-seconds", type=float, default=3.0,
+                    help="reference arm: host seconds sampled per bench step")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-oracle", action="store_true")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -383,7 +544,7 @@ def main():
         backend = "nccl" if args.impl == "adcgpu" else "gloo"
         if backend == "nccl":
             torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-        td.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+        td.init_process_group(backend, timeout=datetime.timedelta(seconds=900))
         dist = td
     try:
         if args.impl == "reference":

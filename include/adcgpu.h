@@ -341,6 +341,20 @@ int adc_get_scalars(adc_ctx *ctx, adc_scalars_t *out);
 int adc_phase_times(adc_ctx *ctx, double *ms_shift, double *ms_gwce, double *ms_jcg,
                     double *ms_wetdry, double *ms_momentum);
 
+/* Device time (ms) of single kernels and passes of the last adc_timestep
+ * (events inside its captured step graph), in this order; n entries are
+ * written.  No reference counterpart (measurement only). */
+#define ADC_KT_LHS_ELEM 0     /* GWCE matrix element terms (gwce.F:427-592) */
+#define ADC_KT_LHS_GATHER 1   /* their node-centric gather into COEF */
+#define ADC_KT_RHS_ELEM 2     /* GWCE load-vector element terms (gwce.F:1000-1615) */
+#define ADC_KT_RHS_GATHER 3   /* their gather into GWCE_LV */
+#define ADC_KT_JCG 4          /* the JCG solve (itpackv.F:63-604), all kernels */
+#define ADC_KT_WETDRY 5       /* computeWettingAndDrying + H2 (wetdry.F:140-1652) */
+#define ADC_KT_MOM_ELEM 6     /* momentum element terms (momentum.F:298-699) */
+#define ADC_KT_MOM_NODE 7     /* momentum nodal solve (momentum.F:713-1182) */
+#define ADC_NKT 8
+int adc_kernel_times(adc_ctx *ctx, double *ms, int n);
+
 /* Number of kernel launches issued by the library since bind. */
 int64_t adc_launch_count(adc_ctx *ctx);
 
