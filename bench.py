@@ -377,6 +377,22 @@ def oracle_check(case_fn, nsteps=5):
             "iters_gpu": [int(x) for x in its_g], "iters_equal": list(its_o) == list(its_g)}
 
 
+def profile_run(args):
+    """A short run for profilers: binds --profile-path on the bench case and
+    replays --profile-steps time steps from cold start."""
+    import torch
+    from adcirc_b200 import build, model
+    build.build()
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    case = make_case(args.case)
+    gpu = model.GpuModel(case, prec=PATHS[args.profile_path][0])
+    numitr, last = gpu.run(1, args.profile_steps)
+    torch.cuda.synchronize()
+    print(f"profile run: {args.profile_steps} steps, status {last.status}, "
+          f"JCG iterations {list(numitr)[-5:]}, {gpu.launches()} launches", flush=True)
+    gpu.close()
+
+
 def bench_gpu(args, rank, world, dist):
     import copy
     import torch
@@ -533,6 +549,10 @@ def main():
                     help="reference arm: host seconds sampled per bench step")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-oracle", action="store_true")
+    ap.add_argument("--profile-steps", type=int, default=0,
+                    help="profiling run: replay this many time steps of --profile-path and "
+                         "exit without a JSON line")
+    ap.add_argument("--profile-path", default="plain", choices=list(PATHS))
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -547,7 +567,9 @@ def main():
         td.init_process_group(backend, timeout=datetime.timedelta(seconds=900))
         dist = td
     try:
-        if args.impl == "reference":
+        if args.profile_steps > 0:
+            profile_run(args)
+        elif args.impl == "reference":
             bench_reference(args, rank, world)
         else:
             bench_gpu(args, rank, world, dist)

@@ -1,6 +1,6 @@
 """GPU parity on the benchmark mesh and over long runs.
 
-* The 601,937-node storm-surge mesh (the workload bench.py times) from cold
+* The ~600k-node storm-surge mesh (the workload bench.py times) from cold
   start: the resident JCG variant at full size (hundreds of row blocks,
   halo lists, block-local uint16 columns, staged slices), the incremental
   GWCE matrix rebuild and the wet/dry passes, against the oracle.
@@ -54,7 +54,7 @@ def test_surge_cold_start(lib, orc, surge_raw):
     import oracle
     from adcirc_b200 import model
     c0, cg = _surge_pair(surge_raw)
-    assert c0.sizes["np"] == 601_937
+    assert 590_000 <= c0.sizes["np"] <= 610_000
     n = 20
     om = oracle.OracleModel(c0)
     its_o = om.run(1, n)
