@@ -64,7 +64,7 @@ struct JcgArgs {
   double *part, *tri;
   Itp *itp;
   Bar *bar;
-  void *arrive, *release;   // ArriveLine[nrb], ReleaseLine[nrb]
+  void *arrive;             // ArriveLine[nrb + 1]: the row blocks' and the scalar block's
   Flags *flags;
   int eta_update;
   int do_peror;
@@ -88,28 +88,26 @@ struct JcgArgs {
 __device__ __forceinline__ double vld(const double *p) { return *(const volatile double *)p; }
 
 // ---------------------------------------------------------------- barrier
-// Contention-free flag barrier that carries its data.  Row block b owns two
-// 128-byte lines: arrive[b] holds its three partial sums, release[b] the
-// ITPACK record of the phase (c1..c4 and a packed word), each slot
-// double-buffered by the barrier generation's parity.  An empty slot holds
-// kEmpty, a signalling-NaN bit pattern that no arithmetic produces; the
-// writer fills the words, the reader polls until every word is filled,
-// keeps the values of that same read and empties the slot again.  One L2
-// round trip therefore both signals and delivers.  Every word is an aligned
-// 8-byte access (single-copy atomic) and no two blocks poll the same line;
-// the scalar block (the last block of the grid) polls all arrival lines,
-// runs the serial ITPACK step and writes every release line.  A slot is
-// refilled only two barriers later, after its reader has emptied it and
-// that has been ordered before the intervening barrier.  Waits are bounded.
+// Contention-free flag barrier that carries its data, read by every block.
+// Each block owns one 128-byte arrival line of four slots, used in turn by
+// the barrier generations (slot g & 3); a row block posts its three partial
+// sums there, the scalar block (the last block of the grid) posts the
+// eigenvalue estimate cme that its chgcon produced for this barrier.  An
+// empty word holds kEmpty, a signalling-NaN bit pattern no arithmetic
+// produces.  Every block polls all arrival lines until each word of the
+// current slot is filled, sums the row blocks' partials in one fixed order
+// (the same in every block, so every block holds the same bits) and runs
+// the serial ITPACK step (pstop_nrms, parcon) itself on its own copy of the
+// ITPACK scalars: one L2 round trip both signals and delivers, and no
+// release step follows.  A block empties its own slot (g + 2) & 3 when it
+// posts generation g: every reader of generation g - 2 has finished
+// reading before any block can post generation g (it first had to see
+// everyone's generation g - 1 arrival).  Every word is an aligned 8-byte
+// access (single-copy atomic); waits are bounded.
 constexpr unsigned long long kEmpty = 0x7FF4DEADBEEF0001ull;
 
 struct alignas(128) ArriveLine {
-  unsigned long long part[2][4];
-  char fill_[64];
-};
-struct alignas(128) ReleaseLine {
-  unsigned long long rec[2][5];
-  char fill_[48];
+  unsigned long long slot[4][4];   // (p0, p1, p2, -) of a row block; (cme, 0, 0, -) of the scalar block
 };
 
 __device__ __forceinline__ unsigned long long dbits(double x) {
@@ -162,43 +160,6 @@ __device__ Rec read_rec(const Rec *r) {
 __device__ __forceinline__ unsigned long long pack_rec(const Rec &r) {
   return (unsigned long long)(unsigned)r.in | ((unsigned long long)(r.halt & 0xff) << 32) |
          ((unsigned long long)(r.need_unorm & 0xff) << 40);
-}
-
-// Row-block side: post the block's partial sums, wait for the release and,
-// with `srec`, hand its ITPACK record to the whole block.  Returns false on
-// timeout.
-__device__ bool row_arrive_wait(const JcgArgs &a, unsigned g, double p0, double p1, double p2,
-                                Rec *srec = nullptr) {
-  __shared__ int ok;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    const int par = g & 1;
-    fence_gpu();   // the block's results before its arrival
-    volatile unsigned long long *ap = ((ArriveLine *)a.arrive + blockIdx.x)->part[par];
-    ap[0] = dbits(p0);
-    ap[1] = dbits(p1);
-    ap[2] = dbits(p2);
-    volatile unsigned long long *rp = ((ReleaseLine *)a.release + blockIdx.x)->rec[par];
-    unsigned long long v[5];
-    ok = poll_full<5>(rp, v, a.flags) ? 1 : 0;
-    fence_gpu();
-    if (ok) {
-#pragma unroll
-      for (int k = 0; k < 5; ++k) rp[k] = kEmpty;
-      if (srec) {
-        srec->c1 = bitsd(v[0]);
-        srec->c2 = bitsd(v[1]);
-        srec->c3 = bitsd(v[2]);
-        srec->c4 = bitsd(v[3]);
-        srec->in = (int)(unsigned)(v[4] & 0xffffffffull);
-        srec->halt = (int)((v[4] >> 32) & 0xff);
-        srec->need_unorm = (int)((v[4] >> 40) & 0xff);
-        srec->pad_ = 0;
-      }
-    }
-  }
-  __syncthreads();
-  return ok != 0;
 }
 
 // Serial ITPACK state of one solve, held in registers of the scalar block's
@@ -460,75 +421,107 @@ __device__ void block_sum3(double &a, double &b, double &c) {
   __syncthreads();
 }
 
-// Scalar-block side of a barrier: gather every row block's partials (in
-// block order, fixed tree), run `serial` on thread 0 (it fills *srec), and
-// release every row block with the record.  Returns false on timeout.
+// One barrier of generation g for every block.  Row blocks post their
+// block sums of (p0, p1, p2), the scalar block posts `cme`; then every block
+// gathers the row blocks' posts in block order (thread t takes blocks t,
+// t + blockDim, ...; then a fixed tree) and thread 0 runs
+// `serial(s0, s1, s2, cme)`.  Returns false on timeout.
 template <class F>
-__device__ bool scalar_phase(const JcgArgs &a, unsigned g, F serial, Rec *srec) {
+__device__ bool grid_phase(const JcgArgs &a, bool scalar_block, unsigned g, double p0, double p1,
+                           double p2, double cme, F serial) {
   __shared__ int bad;
-  const int par = g & 1;
-  if (threadIdx.x == 0) bad = 0;
-  __syncthreads();
-  double s0 = 0.0, s1 = 0.0, s2 = 0.0;
-  for (int b = threadIdx.x; b < a.nrb; b += blockDim.x) {
-    volatile unsigned long long *ap = ((ArriveLine *)a.arrive + b)->part[par];
-    unsigned long long v[3];
-    if (!poll_full<3>(ap, v, a.flags)) {
-      bad = 1;
-      break;
+  __shared__ double s_cme;
+  const int sl = g & 3, sl_old = (g + 2) & 3;
+  if (!scalar_block) block_sum3(p0, p1, p2);
+  if (threadIdx.x == 0) {
+    bad = 0;
+    volatile unsigned long long *own = ((ArriveLine *)a.arrive + blockIdx.x)->slot[0];
+    own[4 * sl_old + 0] = kEmpty;
+    own[4 * sl_old + 1] = kEmpty;
+    own[4 * sl_old + 2] = kEmpty;
+    fence_gpu();   // the block's results (and the emptied slot) before its arrival
+    if (scalar_block) {
+      own[4 * sl + 0] = dbits(cme);
+      own[4 * sl + 1] = 0ull;
+      own[4 * sl + 2] = 0ull;
+    } else {
+      own[4 * sl + 0] = dbits(p0);
+      own[4 * sl + 1] = dbits(p1);
+      own[4 * sl + 2] = dbits(p2);
     }
-    s0 += bitsd(v[0]);
-    s1 += bitsd(v[1]);
-    s2 += bitsd(v[2]);
+  }
+  __syncthreads();
+  // A thread's lines (b = t, t + blockDim, ...; at most kPollLines) are
+  // polled together, so the last arrival costs one round trip; the sums
+  // then run in block order as before.
+  constexpr int kPollLines = 4;
+  double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+  unsigned long long v[kPollLines][3];
+  const int nl = (a.nrb + 1 - (int)threadIdx.x + (int)blockDim.x - 1) / (int)blockDim.x;
+  if (nl > kPollLines) {
+    // more lines than one thread polls (the grid setup never makes this):
+    // report it as an expired wait so the host sees an error
+    atomicExch(&a.flags->timeout, 1);
+    bad = 1;
+  } else if (nl > 0) {
+    unsigned filled = 0;
+    const unsigned all = (1u << nl) - 1u;
+    const long long t0 = clock64();
+    while (filled != all) {
+#pragma unroll
+      for (int k = 0; k < kPollLines; ++k) {
+        if (k >= nl || (filled >> k & 1u)) continue;
+        volatile unsigned long long *ap =
+            ((ArriveLine *)a.arrive + (threadIdx.x + k * blockDim.x))->slot[sl];
+        v[k][0] = ap[0];
+        v[k][1] = ap[1];
+        v[k][2] = ap[2];
+      }
+#pragma unroll
+      for (int k = 0; k < kPollLines; ++k)
+        if (k < nl && v[k][0] != kEmpty && v[k][1] != kEmpty && v[k][2] != kEmpty) filled |= 1u << k;
+      if (filled == all) break;
+      if (*(volatile int *)&a.flags->timeout || clock64() - t0 > kSpinCycles) {
+        atomicExch(&a.flags->timeout, 1);
+        bad = 1;
+        break;
+      }
+    }
+    if (filled == all) {
+      for (int k = 0; k < nl; ++k) {
+        const int b = threadIdx.x + k * blockDim.x;
+        if (b == a.nrb) {
+          s_cme = bitsd(v[k][0]);
+        } else {
+          s0 += bitsd(v[k][0]);
+          s1 += bitsd(v[k][1]);
+          s2 += bitsd(v[k][2]);
+        }
+      }
+    }
   }
   fence_gpu();
   __syncthreads();
   if (bad) return false;
   block_sum3(s0, s1, s2);
-  if (threadIdx.x == 0) serial(s0, s1, s2);
-  __syncthreads();
-  unsigned long long w[5] = {dbits(srec->c1), dbits(srec->c2), dbits(srec->c3), dbits(srec->c4),
-                             pack_rec(*srec)};
-  fence_gpu();
-  for (int b = threadIdx.x; b < a.nrb; b += blockDim.x) {
-    volatile unsigned long long *rp = ((ReleaseLine *)a.release + b)->rec[par];
-#pragma unroll
-    for (int k = 0; k < 5; ++k) rp[k] = w[k];
-  }
-  // empty the arrival slots off the critical path: they are refilled two
-  // barriers later, after this block's next release
-  for (int b = threadIdx.x; b < a.nrb; b += blockDim.x) {
-    volatile unsigned long long *ap = ((ArriveLine *)a.arrive + b)->part[par];
-    ap[0] = kEmpty;
-    ap[1] = kEmpty;
-    ap[2] = kEmpty;
-  }
+  if (threadIdx.x == 0) serial(s0, s1, s2, s_cme);
   __syncthreads();
   return true;
 }
 
-// Reducing phase end.  Row blocks post their block sums of (p0, p1, p2)
-// and wait; the scalar block sums the posts in block order and runs
-// `serial(s0, s1, s2)`, which fills *srec, before releasing.
+// Reducing phase end: `serial(s0, s1, s2, cme)` runs in every block on the
+// same sums.
 template <class F>
 __device__ bool phase_reduce(const JcgArgs &a, bool scalar_block, unsigned &g, double p0,
-                             double p1, double p2, F serial, Rec *srec) {
+                             double p1, double p2, double cme, F serial) {
   ++g;
-  if (!scalar_block) {
-    block_sum3(p0, p1, p2);
-    return row_arrive_wait(a, g, p0, p1, p2, srec);
-  }
-  return scalar_phase(a, g, serial, srec);
+  return grid_phase(a, scalar_block, g, p0, p1, p2, cme, serial);
 }
 
 // Plain barrier (no partials, no record).
-__device__ bool phase_sync(const JcgArgs &a, bool scalar_block, unsigned &g, Rec *scratch) {
+__device__ bool phase_sync(const JcgArgs &a, bool scalar_block, unsigned &g) {
   ++g;
-  if (!scalar_block) return row_arrive_wait(a, g, 0.0, 0.0, 0.0);
-  return scalar_phase(a, g, [&](double, double, double) {
-    scratch->c1 = scratch->c2 = scratch->c3 = scratch->c4 = 0.0;
-    scratch->halt = scratch->need_unorm = scratch->in = 0;
-  }, scratch);
+  return grid_phase(a, scalar_block, g, 0.0, 0.0, 0.0, 0.0, [](double, double, double, double) {});
 }
 
 
@@ -650,9 +643,8 @@ __global__ void __launch_bounds__(kThreads, 2) jcg_kernel(JcgArgs a) {
   Rec *rec = &a.itp->rec;
   __shared__ ItpLocal L;              // used by the scalar block's thread 0 only
   __shared__ Rec s_rec;               // the record of the last reducing barrier
-  __shared__ Rec s_scr;               // record slot of the barriers that carry none
   unsigned gen = 0;                   // barrier generation within this launch
-  if (scalar_block && threadIdx.x == 0) {
+  if (threadIdx.x == 0) {   // every block steps its own copy of the ITPACK scalars
     const volatile Itp *g = a.itp;
     L.zeta = g->zeta; L.cme = g->cme; L.gamma = g->gamma; L.rho = g->rho;
     L.gamold = g->gamold; L.rhoold = g->rhoold; L.delnnm = g->delnnm; L.delsnm = g->delsnm;
@@ -677,7 +669,7 @@ __global__ void __launch_bounds__(kThreads, 2) jcg_kernel(JcgArgs a) {
         a.u1[i] = 0.0;
       }
     }
-    if (!phase_sync(a, scalar_block, gen, &s_scr)) return;
+    if (!phase_sync(a, scalar_block, gen)) return;
 
     // P1: scaled off-diagonals, the reference's unscal drift of the resident
     // matrix, and the initial pseudo-residual d0 = pjac(u') + rhs' - u'.
@@ -720,7 +712,7 @@ __global__ void __launch_bounds__(kThreads, 2) jcg_kernel(JcgArgs a) {
         a.diag[i] = winv_i * winv_i;
       }
     }
-    if (!phase_sync(a, scalar_block, gen, &s_scr)) return;
+    if (!phase_sync(a, scalar_block, gen)) return;
 
     // P2: dtwd0 = -A' d0 and the iteration-0 norms; the scalar block runs
     // chgcon for in = 0 (ip = 0: cme = 0) while the rows work.
@@ -858,7 +850,7 @@ __global__ void __launch_bounds__(kThreads, 2) jcg_kernel(JcgArgs a) {
       if (!ok) atomicExch(&a.flags->timeout, 1);
       fence_proxy_async_all();   // soff is read by bulk copies from here on
     }
-    if (!phase_sync(a, scalar_block, gen, &s_scr)) return;
+    if (!phase_sync(a, scalar_block, gen)) return;
     // P2: dtwd0 = -A' d0 and the iteration-0 norms.
     if (!scalar_block) {
       pipe.begin((const VT *)sv_store, true);   // the scaled matrix was just written
@@ -897,7 +889,9 @@ __global__ void __launch_bounds__(kThreads, 2) jcg_kernel(JcgArgs a) {
   {
     if (scalar_block && threadIdx.x == 0 && L.adapt) chgcon_d(&L, t1, t2, 0);
     const int need_u = need_u0;
-    bool ok = phase_reduce(a, scalar_block, gen, pd, pt, pu, [&](double sd, double st, double su) {
+    bool ok = phase_reduce(a, scalar_block, gen, pd, pt, pu, L.cme,
+                           [&](double sd, double st, double su, double cme) {
+      L.cme = cme;   // chgcon's estimate, from the scalar block
       L.delnnm = sd;
       int halt = pstop_d(&L, 0, need_u ? su : 1.0, sd);
       double c[4] = {0, 0, 0, 0};
@@ -910,7 +904,7 @@ __global__ void __launch_bounds__(kThreads, 2) jcg_kernel(JcgArgs a) {
       vr->halt = halt;
       vr->need_unorm = !(L.q1 || ((1 > 5) && (1 % 5 != 0)));
       vr->in = 0;
-    }, &s_rec);
+    });
     if (!ok) return;
   }
 
@@ -1038,7 +1032,9 @@ __global__ void __launch_bounds__(kThreads, 2) jcg_kernel(JcgArgs a) {
     }
     const int m = in + 1;
     if (scalar_block && threadIdx.x == 0 && L.adapt) chgcon_d(&L, t1, t2, m);
-    bool ok = phase_reduce(a, scalar_block, gen, pd, pt, pu, [&](double sd, double st, double su) {
+    bool ok = phase_reduce(a, scalar_block, gen, pd, pt, pu, L.cme,
+                           [&](double sd, double st, double su, double cme) {
+      L.cme = cme;   // chgcon's estimate, from the scalar block
       L.delnnm = sd;
       int halt = pstop_d(&L, m, need_u ? su : 1.0, sd);
       double c[4] = {0, 0, 0, 0};
@@ -1052,7 +1048,7 @@ __global__ void __launch_bounds__(kThreads, 2) jcg_kernel(JcgArgs a) {
       vr->halt = halt;
       vr->need_unorm = !(L.q1 || ((mm > 5) && (mm % 5 != 0)));
       vr->in = m;
-    }, &s_rec);
+    });
     if (!ok) return;
   }
   r = s_rec;
@@ -1080,11 +1076,13 @@ __global__ void __launch_bounds__(kThreads, 2) jcg_kernel(JcgArgs a) {
         pr += wk2 * wk2;
       }
     }
-    bool ok = phase_reduce(a, scalar_block, gen, pb, pr, 0.0, [&](double sb, double sr, double) {
-      a.itp->dtnrm = sb;
-      a.itp->unorm = sr;
-      s_scr = s_rec;
-    }, &s_scr);
+    bool ok = phase_reduce(a, scalar_block, gen, pb, pr, 0.0, 0.0,
+                           [&](double sb, double sr, double, double) {
+      if (scalar_block) {
+        a.itp->dtnrm = sb;
+        a.itp->unorm = sr;
+      }
+    });
     if (!ok) return;
   }
 
@@ -1324,7 +1322,6 @@ int launch_jcg_impl(adc_ctx *c, int eta_update, int do_peror, int run_init, int 
   a.itp = c->itp;
   a.bar = c->bar;
   a.arrive = c->jlines;
-  a.release = (char *)c->jlines + 128 * (size_t)c->jcg_rows_blocks;
   a.flags = c->flags;
   a.eta_update = eta_update;
   a.nodecode = c->nodecode;
