@@ -451,53 +451,20 @@ __device__ bool grid_phase(const JcgArgs &a, bool scalar_block, unsigned g, doub
     }
   }
   __syncthreads();
-  // A thread's lines (b = t, t + blockDim, ...; at most kPollLines) are
-  // polled together, so the last arrival costs one round trip; the sums
-  // then run in block order as before.
-  constexpr int kPollLines = 4;
   double s0 = 0.0, s1 = 0.0, s2 = 0.0;
-  unsigned long long v[kPollLines][3];
-  const int nl = (a.nrb + 1 - (int)threadIdx.x + (int)blockDim.x - 1) / (int)blockDim.x;
-  if (nl > kPollLines) {
-    // more lines than one thread polls (the grid setup never makes this):
-    // report it as an expired wait so the host sees an error
-    atomicExch(&a.flags->timeout, 1);
-    bad = 1;
-  } else if (nl > 0) {
-    unsigned filled = 0;
-    const unsigned all = (1u << nl) - 1u;
-    const long long t0 = clock64();
-    while (filled != all) {
-#pragma unroll
-      for (int k = 0; k < kPollLines; ++k) {
-        if (k >= nl || (filled >> k & 1u)) continue;
-        volatile unsigned long long *ap =
-            ((ArriveLine *)a.arrive + (threadIdx.x + k * blockDim.x))->slot[sl];
-        v[k][0] = ap[0];
-        v[k][1] = ap[1];
-        v[k][2] = ap[2];
-      }
-#pragma unroll
-      for (int k = 0; k < kPollLines; ++k)
-        if (k < nl && v[k][0] != kEmpty && v[k][1] != kEmpty && v[k][2] != kEmpty) filled |= 1u << k;
-      if (filled == all) break;
-      if (*(volatile int *)&a.flags->timeout || clock64() - t0 > kSpinCycles) {
-        atomicExch(&a.flags->timeout, 1);
-        bad = 1;
-        break;
-      }
+  for (int b = threadIdx.x; b <= a.nrb; b += blockDim.x) {
+    volatile unsigned long long *ap = ((ArriveLine *)a.arrive + b)->slot[sl];
+    unsigned long long v[3];
+    if (!poll_full<3>(ap, v, a.flags)) {
+      bad = 1;
+      break;
     }
-    if (filled == all) {
-      for (int k = 0; k < nl; ++k) {
-        const int b = threadIdx.x + k * blockDim.x;
-        if (b == a.nrb) {
-          s_cme = bitsd(v[k][0]);
-        } else {
-          s0 += bitsd(v[k][0]);
-          s1 += bitsd(v[k][1]);
-          s2 += bitsd(v[k][2]);
-        }
-      }
+    if (b == a.nrb) {
+      s_cme = bitsd(v[0]);
+    } else {
+      s0 += bitsd(v[0]);
+      s1 += bitsd(v[1]);
+      s2 += bitsd(v[2]);
     }
   }
   fence_gpu();
