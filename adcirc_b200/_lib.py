@@ -22,6 +22,7 @@ ADC_ERR_UNSUPPORTED = -6
 ADC_PREC_FP64 = 0
 ADC_PREC_MIXED = 1
 ADC_WARM_START = 2
+ADC_LEARNED_START = 32
 ADC_F32_ASSEMBLY = 4
 ADC_F32_SPMV = 8
 ADC_F32_MOMENTUM = 16
@@ -148,6 +149,14 @@ def load():
         "adc_launch_count": (C.c_int64, [vp]),
         "adc_get_scalars": (C.c_int, [vp, C.POINTER(AdcScalars)]),
         "adc_kernel_times": (C.c_int, [vp, dp_, C.c_int]),
+        "adc_predictor_nparams": (C.c_int, []),
+        "adc_set_predictor": (C.c_int, [vp, C.POINTER(C.c_float), C.c_int]),
+        "adc_get_predictor": (C.c_int, [vp, C.POINTER(C.c_float), C.c_int]),
+        "adc_predictor_train": (C.c_int, [vp, C.c_int, C.c_float]),
+        "adc_predictor_stats": (C.c_int, [vp, dp_, C.POINTER(C.c_longlong)]),
+        "adc_predictor_forward": (C.c_int, [vp, dp_, C.POINTER(C.c_float)]),
+        "adc_predictor_gradient": (C.c_int, [vp, C.POINTER(C.c_float), C.c_int]),
+        "adc_predictor_gradient_at": (C.c_int, [vp, dp_, C.POINTER(C.c_float), C.c_int]),
         "adc_last_run_ms": (C.c_double, [vp]),
         "adc_last_error": (C.c_char_p, []),
     }

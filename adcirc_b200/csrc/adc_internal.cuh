@@ -11,6 +11,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <cuda_bf16.h>
 #include <cstdint>
 #include <cstdio>
 
@@ -62,6 +63,7 @@ struct Bar {
 };
 
 struct Ctx;
+struct Mpnn;
 
 }  // namespace adc
 
@@ -164,6 +166,8 @@ struct adc_ctx {
   float *soff32;               // FP32 scaled matrix (mixed mode, resident variant)
   double *etas_prev;           // last step's reference guess (ADC_WARM_START)
   WarmState *warm;
+  adc::Mpnn *mp;               // learned initial guess (mpnn.cu), built on first use
+  int *h_neitab, *h_nneigh;    // host copies of NeiTab/NNeigh (the predictor's 1-ring)
   int *jhalo_ptr, *jhalo_ids;
   unsigned char *jexp;
   // flags / steps

@@ -63,6 +63,7 @@ int launch_flux_forcing(adc_ctx *c);
 int launch_flux_rhs(adc_ctx *c);
 int flux_tables(adc_ctx *c, const adc_arrays_t *a);
 int launch_warm_start(adc_ctx *c);
+int launch_predictor_train(adc_ctx *c);
 
 int launch_shift_friction(adc_ctx *c) {
   launch_k(k_shift_friction, nblk(c->np), kThreads, c->stream, *c, c->steps, c->flags);
@@ -140,6 +141,7 @@ static int enqueue_step(adc_ctx *c, bool timed) {
   if ((rc = launch_warm_start(c))) return rc;
   if (timed) cudaEventRecordWithFlags(c->ev[2], c->stream, cudaEventRecordExternal);
   if ((rc = launch_jcg(c, 1))) return rc;
+  if ((rc = launch_predictor_train(c))) return rc;   // nothing unless training is on
   if (timed) cudaEventRecordWithFlags(c->ev[3], c->stream, cudaEventRecordExternal);
   if ((rc = launch_wetdry(c))) return rc;
   if (timed) cudaEventRecordWithFlags(c->ev[4], c->stream, cudaEventRecordExternal);
@@ -415,8 +417,14 @@ static int download_state(adc_ctx *c) {
   return ADC_OK;
 }
 
+void mp_free(adc_ctx *c);
+
 static void free_ctx(adc_ctx *c) {
   if (!c) return;
+  mp_free(c);
+  delete[] c->h_nneigh;
+  delete[] c->h_neitab;
+  c->h_nneigh = c->h_neitab = nullptr;
   void **ptrs[] = {
       (void **)&c->x, (void **)&c->y, (void **)&c->dp, (void **)&c->tau0, (void **)&c->evm,
       (void **)&c->fric, (void **)&c->corif, (void **)&c->nneigh, (void **)&c->nm,
@@ -466,7 +474,8 @@ static int bind_impl(const adc_params_t *p, const adc_arrays_t *a, int prec, adc
   if (a->np <= 0 || a->ne <= 0 || a->mnei < 2 || a->neta < 0 || a->nbfr < 0) {
     set_error("invalid sizes"); return ADC_ERR_ARG;
   }
-  if (prec & ~(ADC_PREC_MIXED | ADC_WARM_START | ADC_F32_ASSEMBLY | ADC_F32_SPMV | ADC_F32_MOMENTUM)) {
+  if (prec & ~(ADC_PREC_MIXED | ADC_WARM_START | ADC_F32_ASSEMBLY | ADC_F32_SPMV | ADC_F32_MOMENTUM |
+               ADC_LEARNED_START)) {
     set_error("bad precision mode %d", prec);
     return ADC_ERR_ARG;
   }
@@ -593,9 +602,16 @@ static int bind_impl(const adc_params_t *p, const adc_arrays_t *a, int prec, adc
   if (c->prec & ADC_WARM_START) {
     B(dalloc(&c->etas_prev, npad));
     ADC_CUDA(cudaMemset(c->etas_prev, 0, npad * sizeof(double)));
+  }
+  if (c->prec & (ADC_WARM_START | ADC_LEARNED_START)) {
     B(dalloc(&c->warm, 1));
     ADC_CUDA(cudaMemset(c->warm, 0, sizeof(WarmState)));
   }
+  // host copies of the ring tables, for the learned predictor's graph
+  c->h_nneigh = new int[np];
+  c->h_neitab = new int[(size_t)np * a->mnei];
+  memcpy(c->h_nneigh, a->nneigh, np * sizeof(int));
+  memcpy(c->h_neitab, a->neitab, (size_t)np * a->mnei * sizeof(int));
   c->ev_blocks = (ne + 255) / 256;
   B(dalloc(&c->ev_cnt, 2 * ((size_t)c->ev_blocks + 1)));   // counts, then offsets
   B(dalloc(&c->evu_i, 3 * 1024)); B(dalloc(&c->evu_c, 1024));   // one W1 chunk (wetdry.cu)
@@ -738,6 +754,7 @@ int adc_gwce_new(adc_ctx *c, const adc_step_t *s, adc_stepout_t *out) {
   TRY(launch_gwce_rhs(c));
   TRY(launch_warm_start(c));
   TRY(launch_jcg(c, 1));
+  TRY(launch_predictor_train(c));
   ADC_CUDA(cudaGetLastError());
   Flags f;
   TRY(read_flags(c, f));

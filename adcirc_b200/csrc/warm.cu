@@ -16,13 +16,13 @@ namespace adc {
 // Per row: residuals of the reference guess u and of the extrapolated
 // guess p = 2u - u_prev (p = u at elevation-specified rows), and their
 // block sums of squares.
-__global__ void k_warm_resid(adc_ctx c) {
+__global__ void k_warm_resid(adc_ctx c, const double *lg) {
   griddep_wait();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   double r2u = 0.0, r2p = 0.0;
   if (i < c.np) {
     const double ui = c.etas[i];
-    const double pi = c.is_nbd[i] >= 0 ? ui : 2.0 * ui - c.etas_prev[i];
+    const double pi = lg ? lg[i] : (c.is_nbd[i] >= 0 ? ui : 2.0 * ui - c.etas_prev[i]);
     const double d = c.diag[i];
     double ru = c.gwce_lv[i] - d * ui;
     double rp = c.gwce_lv[i] - d * pi;
@@ -42,7 +42,7 @@ __global__ void k_warm_resid(adc_ctx c) {
       for (int k = 0; k < kGatherChunk; ++k)
         if (k0 + k < len) {
           uj[k] = c.etas[jj[k]];
-          pj[k] = c.is_nbd[jj[k]] >= 0 ? uj[k] : 2.0 * uj[k] - c.etas_prev[jj[k]];
+          pj[k] = lg ? lg[jj[k]] : (c.is_nbd[jj[k]] >= 0 ? uj[k] : 2.0 * uj[k] - c.etas_prev[jj[k]]);
         }
 #pragma unroll
       for (int k = 0; k < kGatherChunk; ++k)
@@ -104,23 +104,35 @@ __global__ void k_warm_choose(adc_ctx c, int nparts) {
   }
 }
 
-// Applies the choice and remembers this step's reference guess (the last
-// solution) for the next extrapolation.
-__global__ void k_warm_apply(adc_ctx c) {
+// Applies the choice.  The extrapolated guess also remembers this step's
+// reference guess (the last solution) for the next extrapolation; the
+// learned guess `lg` holds the reference guess wherever it predicts
+// nothing.
+__global__ void k_warm_apply(adc_ctx c, const double *lg) {
   griddep_wait();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= c.np) return;
+  if (lg) {
+    if (c.warm->use) c.etas[i] = lg[i];
+    return;
+  }
   const double u = c.etas[i], uprev = c.etas_prev[i];
   c.etas_prev[i] = u;
   if (c.warm->use && c.is_nbd[i] < 0) c.etas[i] = 2.0 * u - uprev;
 }
 
+int launch_predictor_forward(adc_ctx *c);
+const double *mp_guess(const adc_ctx *c);
+
 int launch_warm_start(adc_ctx *c) {
-  if (!(c->prec & ADC_WARM_START)) return ADC_OK;
+  int rc = launch_predictor_forward(c);   // nothing unless a predictor is used or trained
+  if (rc) return rc;
+  const double *lg = mp_guess(c);
+  if (!lg && !(c->prec & ADC_WARM_START)) return ADC_OK;
   const int nb = nblk(c->np);
-  launch_k(k_warm_resid, nb, kThreads, c->stream, *c);
+  launch_k(k_warm_resid, nb, kThreads, c->stream, *c, lg);
   launch_k(k_warm_choose, 1, 1024, c->stream, *c, nb);
-  launch_k(k_warm_apply, nb, kThreads, c->stream, *c);
+  launch_k(k_warm_apply, nb, kThreads, c->stream, *c, lg);
   c->launches += 3;
   return ADC_OK;
 }
@@ -131,7 +143,7 @@ using namespace adc;
 
 extern "C" int adc_warm_start_stats(adc_ctx *c, long long *used, long long *fallback) {
   if (!c) return ADC_ERR_ARG;
-  if (!(c->prec & ADC_WARM_START)) {
+  if (!c->warm) {
     if (used) *used = 0;
     if (fallback) *fallback = 0;
     return ADC_OK;

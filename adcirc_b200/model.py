@@ -527,6 +527,54 @@ class GpuModel:
         self.lib.adc_phase_times(self.h, *[C.byref(t) for t in v])
         return dict(zip(("shift", "gwce", "jcg", "wetdry", "momentum"), [t.value for t in v]))
 
+    # learned initial guess (adc_set_predictor and friends)
+    def set_predictor(self, params: np.ndarray) -> None:
+        v = np.ascontiguousarray(params, np.float32)
+        _check(self.lib.adc_set_predictor(self.h, v.ctypes.data_as(C.POINTER(C.c_float)), v.size),
+               "adc_set_predictor")
+
+    def get_predictor(self) -> np.ndarray:
+        v = np.zeros(self.lib.adc_predictor_nparams(), np.float32)
+        _check(self.lib.adc_get_predictor(self.h, v.ctypes.data_as(C.POINTER(C.c_float)), v.size),
+               "adc_get_predictor")
+        return v
+
+    def predictor_train(self, on: bool, lr: float = 1e-3) -> None:
+        _check(self.lib.adc_predictor_train(self.h, 1 if on else 0, float(lr)), "adc_predictor_train")
+
+    def predictor_stats(self):
+        loss = C.c_double(0.0)
+        n = C.c_longlong(0)
+        _check(self.lib.adc_predictor_stats(self.h, C.byref(loss), C.byref(n)), "adc_predictor_stats")
+        return loss.value, n.value
+
+    def predictor_forward(self, hidden: bool = False):
+        g = np.zeros(self.case.sizes["np"])
+        h = np.zeros(self.case.sizes["np"] * 64, np.float32) if hidden else None
+        _check(self.lib.adc_predictor_forward(self.h, ptr(g, dp_),
+                                              h.ctypes.data_as(C.POINTER(C.c_float)) if hidden else None),
+               "adc_predictor_forward")
+        return (g, h.reshape(-1, 64)) if hidden else g
+
+    def predictor_gradient(self) -> np.ndarray:
+        v = np.zeros(self.lib.adc_predictor_nparams(), np.float32)
+        _check(self.lib.adc_predictor_gradient(self.h, v.ctypes.data_as(C.POINTER(C.c_float)), v.size),
+               "adc_predictor_gradient")
+        return v
+
+    def predictor_gradient_at(self, target: np.ndarray) -> np.ndarray:
+        t = np.ascontiguousarray(target, np.float64)
+        v = np.zeros(self.lib.adc_predictor_nparams(), np.float32)
+        _check(self.lib.adc_predictor_gradient_at(self.h, ptr(t, dp_),
+                                                  v.ctypes.data_as(C.POINTER(C.c_float)), v.size),
+               "adc_predictor_gradient_at")
+        return v
+
+    def warm_start_stats(self):
+        u, f = C.c_longlong(0), C.c_longlong(0)
+        _check(self.lib.adc_warm_start_stats(self.h, C.byref(u), C.byref(f)), "adc_warm_start_stats")
+        return u.value, f.value
+
     KERNEL_SPANS = ("lhs_elem", "lhs_gather", "rhs_elem", "rhs_gather", "jcg", "wetdry",
                     "mom_elem", "mom_node")
 

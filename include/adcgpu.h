@@ -44,6 +44,9 @@ extern "C" {
 #define ADC_F32_ASSEMBLY 4    /* GWCE LHS and RHS element terms and their gathers */
 #define ADC_F32_SPMV 8        /* the JCG matrix the iterations stream (FP64 products) */
 #define ADC_F32_MOMENTUM 16   /* momentum element terms and their gather */
+#define ADC_LEARNED_START 32  /* flag OR'ed into the mode: JCG starts from the learned
+                                 predictor's guess (adc_set_predictor) when its initial
+                                 residual is smaller than the reference guess's */
 
 /* Model parameters (fort.15 values and derived switches). */
 typedef struct {
@@ -336,6 +339,44 @@ typedef struct {
 } adc_scalars_t;
 
 int adc_get_scalars(adc_ctx *ctx, adc_scalars_t *out);
+
+/* Learned JCG initial guess (no reference counterpart; the reference starts
+ * from ETAS as GWCE_New leaves it, gwce.F:1846-1850, 2002-2004).  A
+ * message-passing network over each node's NeiTab ring (input layer 9 -> 64,
+ * three layers h' = ReLU(Ws h + Wn mean_ring(h) + b) of width 64, a linear
+ * head) predicts a correction s_out * out to that guess at wet nodes off the
+ * elevation boundary, from the normalised eta^k, ETAS, u, v, depth, wet
+ * flag, p - p_background and wind stress.  BF16 weights and activations,
+ * FP32 accumulation on the tensor cores.  Parameters are a flat FP32 array
+ * of adc_predictor_nparams() values: W_in[64][16] (inputs 0-8, column 9 the
+ * bias, 10-15 zero), per layer Ws[64][64], Wn[64][64], b[64], then
+ * w_out[64], b_out, feature means[9], feature scales[9], s_out.
+ * adc_set_predictor uploads them (and builds the predictor on first use);
+ * with ADC_LEARNED_START in the bind mode every later step starts JCG from
+ * the prediction when its initial residual is the smaller one
+ * (adc_warm_start_stats counts the choices).  adc_predictor_train(on, lr)
+ * trains the network on the device after every step's solve on that
+ * step's (features, solved ETAS), Adam on the MSE of the normalised
+ * correction; without ADC_LEARNED_START the steps keep the reference guess,
+ * so the pairs are the plain solver's.  The predictor is not part of the
+ * hotstart file. */
+int adc_predictor_nparams(void);
+int adc_set_predictor(adc_ctx *ctx, const float *params, int nparams);
+int adc_get_predictor(adc_ctx *ctx, float *params, int nparams);
+int adc_predictor_train(adc_ctx *ctx, int on, float lr);
+/* loss: mean squared normalised error of the last training step; adam_steps:
+ * updates so far. */
+int adc_predictor_stats(adc_ctx *ctx, double *loss, long long *adam_steps);
+/* Runs the forward pass on the current device state; guess (NP doubles)
+ * receives the predicted ETAS, hidden3 (optional, NP*64 floats) the last
+ * hidden layer. */
+int adc_predictor_forward(adc_ctx *ctx, double *guess, float *hidden3);
+/* The gradient of the last training step, in the parameter layout. */
+int adc_predictor_gradient(adc_ctx *ctx, float *grad, int nparams);
+/* The gradient of the training loss for the current device state and a
+ * given solved ETAS (NP doubles), without updating the weights (a check of
+ * the backward pass). */
+int adc_predictor_gradient_at(adc_ctx *ctx, const double *target, float *grad, int nparams);
 
 /* Device time of the phases of the last adc_timestep/adc_run (ms). */
 int adc_phase_times(adc_ctx *ctx, double *ms_shift, double *ms_gwce, double *ms_jcg,
