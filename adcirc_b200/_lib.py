@@ -149,6 +149,12 @@ def load():
         "adc_launch_count": (C.c_int64, [vp]),
         "adc_get_scalars": (C.c_int, [vp, C.POINTER(AdcScalars)]),
         "adc_kernel_times": (C.c_int, [vp, dp_, C.c_int]),
+        "adc_set_jcg_blocks": (C.c_int, [vp, C.c_int]),
+        "adc_jcg_layout": (C.c_int, [vp, ip_, ip_]),
+        "adc_ensemble_create": (C.c_int, [C.c_int, C.POINTER(vp), C.POINTER(vp)]),
+        "adc_ensemble_run": (C.c_int, [vp, C.c_int, C.POINTER(AdcStep), ip_, C.POINTER(AdcStepOut)]),
+        "adc_ensemble_last_ms": (C.c_double, [vp]),
+        "adc_ensemble_free": (C.c_int, [vp]),
         "adc_predictor_nparams": (C.c_int, []),
         "adc_set_predictor": (C.c_int, [vp, C.POINTER(C.c_float), C.c_int]),
         "adc_get_predictor": (C.c_int, [vp, C.POINTER(C.c_float), C.c_int]),

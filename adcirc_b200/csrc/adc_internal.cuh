@@ -195,6 +195,8 @@ struct adc_ctx {
   cudaGraphExec_t graph1;   // one timed step (adc_timestep), phase events inside
   int graph1_ok, graph1_launches;
   int graph_launches;    // kernel launches per replayed step
+  int graph_gen;         // bumped whenever the step's captured form changes
+  int jcg_nrb_req;       // requested JCG row blocks (0: the default choice)
   cudaEvent_t run_ev[2];
   double last_run_ms;
 };
@@ -227,6 +229,7 @@ inline void drop_graphs(adc_ctx *c) {
   if (c->graph1_ok) cudaGraphExecDestroy(c->graph1);
   c->graph_ok = 0;
   c->graph1_ok = 0;
+  c->graph_gen++;   // graphs that captured this context's step are stale too
 }
 
 // Programmatic dependent launch.  Step kernels are launched so that the

@@ -1193,7 +1193,8 @@ int jcg_setup_grid(adc_ctx *c, const JcgHostSell *h) {
     return ADC_ERR_ARG;
   }
   // keep at least ~8 slices per block so the barrier cost stays amortised
-  const int nrb0 = std::max(1, std::min(2 * nsm - 1, std::max(1, c->nslices / 8)));
+  int nrb0 = std::max(1, std::min(2 * nsm - 1, std::max(1, c->nslices / 8)));
+  if (c->jcg_nrb_req > 0) nrb0 = std::max(1, std::min({c->jcg_nrb_req, 2 * nsm - 1, c->nslices}));
   c->jcg_res = 0;
   if (h) {
     const int nrb = nrb0;

@@ -935,6 +935,190 @@ int adc_kernel_times(adc_ctx *c, double *ms, int n) {
 
 int64_t adc_launch_count(adc_ctx *c) { return c ? c->launches : -1; }
 
+int adc_set_jcg_blocks(adc_ctx *c, int nrb) {
+  if (!c || nrb < 0) return ADC_ERR_ARG;
+  ADC_CUDA(cudaStreamSynchronize(c->stream));
+  drop_graphs(c);
+  void **old[] = {(void **)&c->jlcol, (void **)&c->jhalo_ptr, (void **)&c->jhalo_ids,
+                  (void **)&c->jexp, (void **)&c->jpart, (void **)&c->jlines};
+  for (void **q : old)
+    if (*q) { cudaFree(*q); *q = nullptr; }
+  const size_t nsl = c->nslices, nnz = c->nnz_pad;
+  std::vector<int> sl_ptr(nsl + 1), sl_w(nsl), col(std::max<size_t>(nnz, 1)), rlen(nsl * kSlice);
+  ADC_CUDA(cudaMemcpy(sl_ptr.data(), c->sl_ptr, (nsl + 1) * sizeof(int), cudaMemcpyDeviceToHost));
+  ADC_CUDA(cudaMemcpy(sl_w.data(), c->sl_w, nsl * sizeof(int), cudaMemcpyDeviceToHost));
+  if (nnz) ADC_CUDA(cudaMemcpy(col.data(), c->col, nnz * sizeof(int), cudaMemcpyDeviceToHost));
+  ADC_CUDA(cudaMemcpy(rlen.data(), c->rlen, nsl * kSlice * sizeof(int), cudaMemcpyDeviceToHost));
+  c->jcg_nrb_req = nrb;
+  const JcgHostSell hs{sl_ptr.data(), sl_w.data(), col.data(), rlen.data()};
+  TRY(jcg_setup_grid(c, &hs));
+  TRY(dalloc(&c->jpart, 4 * (size_t)c->jcg_grid));
+  TRY(dalloc((char **)&c->jlines, 2 * 128 * (size_t)c->jcg_rows_blocks));
+  return ADC_OK;
+}
+
+int adc_jcg_layout(adc_ctx *c, int *row_blocks, int *resident) {
+  if (!c) return ADC_ERR_ARG;
+  if (row_blocks) *row_blocks = c->jcg_rows_blocks;
+  if (resident) *resident = c->jcg_res;
+  return ADC_OK;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------ ensembles
+// Independent bound contexts (ensemble members) stepped together: one
+// captured graph per time step holds every member's whole step on the
+// member's own stream, forked from and joined back into the ensemble's
+// stream, so members' kernels overlap on the GPU.
+struct adc_ensemble {
+  int n;
+  adc_ctx **m;
+  cudaStream_t root;
+  cudaEvent_t fork, t0, t1;
+  cudaEvent_t *join;
+  cudaGraphExec_t graph;
+  int graph_ok;
+  long long gen;   // sum of the members' graph generations at capture
+  double last_ms;
+};
+
+namespace adc {
+
+static long long ens_gen(const adc_ensemble *e) {
+  long long g = 0;
+  for (int k = 0; k < e->n; ++k) g += e->m[k]->graph_gen;
+  return g;
+}
+
+static int ens_capture(adc_ensemble *e) {
+  cudaGraph_t g = nullptr;
+  int rc = ADC_OK;
+  cudaError_t err = cudaStreamBeginCapture(e->root, cudaStreamCaptureModeThreadLocal);
+  if (err != cudaSuccess) return cuda_fail(err, "ensemble capture");
+  cudaEventRecord(e->fork, e->root);
+  for (int k = 0; k < e->n && rc == ADC_OK; ++k) {
+    adc_ctx *c = e->m[k];
+    cudaStreamWaitEvent(c->stream, e->fork, 0);
+    int64_t l0 = c->launches;
+    rc = enqueue_step(c, false);
+    launch_k(k_step_end, 1, 1, c->stream, c->flags, c->numitr_log, c->numitr_cap);
+    c->graph_launches = (int)(c->launches - l0) + 1;
+    c->launches = l0;
+    cudaEventRecord(e->join[k], c->stream);
+    cudaStreamWaitEvent(e->root, e->join[k], 0);
+  }
+  cudaError_t e2 = cudaStreamEndCapture(e->root, &g);
+  if (err == cudaSuccess) err = e2;
+  if (err == cudaSuccess && rc == ADC_OK) err = cudaGraphInstantiate(&e->graph, g, 0);
+  if (g) cudaGraphDestroy(g);
+  cudaGetLastError();
+  if (rc) return rc;
+  if (err != cudaSuccess) return cuda_fail(err, "ensemble graph");
+  e->graph_ok = 1;
+  e->gen = ens_gen(e);
+  return ADC_OK;
+}
+
+}  // namespace adc
+
+extern "C" {
+
+int adc_ensemble_create(int n, adc_ctx *const *ctxs, adc_ensemble **out) {
+  if (n <= 0 || !ctxs || !out) { set_error("adc_ensemble_create: bad arguments"); return ADC_ERR_ARG; }
+  for (int k = 0; k < n; ++k)
+    if (!ctxs[k] || ctxs[k]->met_pending) { set_error("adc_ensemble_create: member %d not usable", k); return ADC_ERR_ARG; }
+  adc_ensemble *e = new adc_ensemble();
+  memset((void *)e, 0, sizeof(*e));
+  e->n = n;
+  e->m = new adc_ctx *[n];
+  e->join = new cudaEvent_t[n];
+  for (int k = 0; k < n; ++k) e->m[k] = ctxs[k];
+  cudaError_t err = cudaStreamCreateWithFlags(&e->root, cudaStreamNonBlocking);
+  if (err == cudaSuccess) err = cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming);
+  if (err == cudaSuccess) err = cudaEventCreate(&e->t0);
+  if (err == cudaSuccess) err = cudaEventCreate(&e->t1);
+  for (int k = 0; k < n && err == cudaSuccess; ++k) err = cudaEventCreateWithFlags(&e->join[k], cudaEventDisableTiming);
+  if (err != cudaSuccess) {
+    adc_ensemble_free(e);
+    return cuda_fail(err, "adc_ensemble_create");
+  }
+  *out = e;
+  return ADC_OK;
+}
+
+int adc_ensemble_free(adc_ensemble *e) {
+  if (!e) return ADC_ERR_ARG;
+  if (e->root) cudaStreamSynchronize(e->root);
+  if (e->graph_ok) cudaGraphExecDestroy(e->graph);
+  for (int k = 0; k < e->n; ++k)
+    if (e->join && e->join[k]) cudaEventDestroy(e->join[k]);
+  if (e->fork) cudaEventDestroy(e->fork);
+  if (e->t0) cudaEventDestroy(e->t0);
+  if (e->t1) cudaEventDestroy(e->t1);
+  if (e->root) cudaStreamDestroy(e->root);
+  delete[] e->join;
+  delete[] e->m;
+  delete e;
+  return ADC_OK;
+}
+
+int adc_ensemble_run(adc_ensemble *e, int nsteps, const adc_step_t *steps, int *numitr,
+                     adc_stepout_t *last) {
+  if (!e || nsteps < 0 || (nsteps > 0 && !steps)) { set_error("bad arguments"); return ADC_ERR_ARG; }
+  if (nsteps == 0) return ADC_OK;
+  for (int k = 0; k < e->n; ++k) {
+    adc_ctx *c = e->m[k];
+    if (nsteps > c->steps_cap) {
+      cudaFree(c->steps);
+      c->steps = nullptr;
+      TRY(dalloc(&c->steps, nsteps));
+      c->steps_cap = nsteps;
+      drop_graphs(c);
+    }
+    if (nsteps > c->numitr_cap) {
+      cudaFree(c->numitr_log);
+      c->numitr_log = nullptr;
+      TRY(dalloc(&c->numitr_log, nsteps));
+      c->numitr_cap = nsteps;
+      drop_graphs(c);
+    }
+    ADC_CUDA(cudaMemcpyAsync(c->steps, steps, nsteps * sizeof(adc_step_t), cudaMemcpyHostToDevice, c->stream));
+    int zero = 0;
+    ADC_CUDA(cudaMemcpyAsync(&c->flags->cursor, &zero, sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    ADC_CUDA(cudaEventRecord(e->join[k], c->stream));
+    ADC_CUDA(cudaStreamWaitEvent(e->root, e->join[k], 0));
+  }
+  if (e->graph_ok && e->gen != ens_gen(e)) {
+    cudaGraphExecDestroy(e->graph);
+    e->graph_ok = 0;
+  }
+  if (!e->graph_ok) TRY(ens_capture(e));
+  ADC_CUDA(cudaEventRecord(e->t0, e->root));
+  for (int s = 0; s < nsteps; ++s) {
+    ADC_CUDA(cudaGraphLaunch(e->graph, e->root));
+    for (int k = 0; k < e->n; ++k) e->m[k]->launches += e->m[k]->graph_launches;
+  }
+  ADC_CUDA(cudaEventRecord(e->t1, e->root));
+  ADC_CUDA(cudaStreamSynchronize(e->root));
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, e->t0, e->t1);
+  e->last_ms = ms;
+  int status = ADC_OK;
+  for (int k = 0; k < e->n; ++k) {
+    adc_ctx *c = e->m[k];
+    Flags f;
+    TRY(read_flags(c, f));
+    if (numitr) ADC_CUDA(cudaMemcpy(numitr + (size_t)k * nsteps, c->numitr_log, nsteps * sizeof(int), cudaMemcpyDeviceToHost));
+    if (last) fill_out(f, last + k);
+    if (f.status && !status) status = f.status;
+  }
+  return status;
+}
+
+double adc_ensemble_last_ms(adc_ensemble *e) { return e ? e->last_ms : -1.0; }
+
+
 double adc_last_run_ms(adc_ctx *c) { return c ? c->last_run_ms : -1.0; }
 
 }  // extern "C"

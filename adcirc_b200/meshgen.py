@@ -205,7 +205,8 @@ def surge_mesh(seed: int = 2024, target_nodes: int = 600_000, lx: float = 1000e3
                shelf_width: float = 100e3, shelf_depth: float = 30.0,
                ocean_depth: float = 4000.0, land_height: float = 6.0,
                grf_sigma: float = 2.0, grf_ell: float = 5e3,
-               land_grading: float = 3.0, beta: float = 0.75, verbose: bool = False) -> RawMesh:
+               land_grading: float = 3.0, beta: float = 0.75, verbose: bool = False,
+               alpha: float | None = None) -> RawMesh:
     """Graded storm-surge mesh (~600k nodes, ~1.2M triangles).
 
     Points: seeded Poisson-disk sampling whose spacing follows the target
@@ -258,9 +259,11 @@ def surge_mesh(seed: int = 2024, target_nodes: int = 600_000, lx: float = 1000e3
 
     # the thinned set keeps a stable fraction of the candidates: calibrate
     # it once, then bisect alpha on the candidate count
+    given = alpha is not None
     lo, hi = 0.005, 0.5
     frac = 0.19
-    for _ in range(40):
+    mid = alpha
+    for _ in range(0 if given else 40):
         mid = np.sqrt(lo * hi)
         cx, _, _ = _quadtree_leaves(lx, ly, make_h(mid), h_max)
         if 2 * cx.size * frac > target_nodes:
@@ -291,7 +294,7 @@ def surge_mesh(seed: int = 2024, target_nodes: int = 600_000, lx: float = 1000e3
         n_kept = int(kept.sum())
         if verbose:
             print(f"surge_mesh: alpha {alpha:.5f} candidates {ax.size} kept {n_kept}")
-        if abs(n_kept - target_nodes) < 0.015 * target_nodes:
+        if given or abs(n_kept - target_nodes) < 0.015 * target_nodes:
             break
         # the node count scales about as alpha^-0.95 for these gradings
         alpha *= (n_kept / target_nodes) ** (1.0 / 0.95)

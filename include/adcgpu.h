@@ -396,6 +396,31 @@ int adc_phase_times(adc_ctx *ctx, double *ms_shift, double *ms_gwce, double *ms_
 #define ADC_NKT 8
 int adc_kernel_times(adc_ctx *ctx, double *ms, int n);
 
+/* JCG launch shape of a bound context (no reference counterpart): the
+ * persistent solver's row blocks (0 restores the default choice) and
+ * whether the resident variant (row vectors in shared memory) is used.
+ * adc_set_jcg_blocks rebuilds the solver's tables; results do not depend
+ * on it beyond the dot products' summation tree. */
+int adc_set_jcg_blocks(adc_ctx *ctx, int row_blocks);
+int adc_jcg_layout(adc_ctx *ctx, int *row_blocks, int *resident);
+
+/* Ensembles (no reference counterpart; the reference runs one mesh per
+ * process, adcirc.F:475-476): n independent bound contexts stepped
+ * together.  Every replayed time step is one captured CUDA graph holding
+ * each member's whole step on the member's own stream, so the members'
+ * kernels overlap on the GPU.  All members take the same step table (same
+ * DT and start time).  numitr (optional) receives NUMITR[member][step],
+ * last (optional) each member's outputs after the final step; the return
+ * is the first nonzero member status.  A member's later per-context calls
+ * (adc_run, adc_timestep, adc_sync_to_host ...) stay valid. */
+typedef struct adc_ensemble adc_ensemble;
+int adc_ensemble_create(int n, adc_ctx *const *members, adc_ensemble **out);
+int adc_ensemble_run(adc_ensemble *ens, int nsteps, const adc_step_t *steps, int *numitr,
+                     adc_stepout_t *last);
+/* Device time of the last adc_ensemble_run (ms, CUDA events). */
+double adc_ensemble_last_ms(adc_ensemble *ens);
+int adc_ensemble_free(adc_ensemble *ens);
+
 /* Number of kernel launches issued by the library since bind. */
 int64_t adc_launch_count(adc_ctx *ctx);
 

@@ -26,6 +26,83 @@
 #include <vector>
 #include <algorithm>
 
+/* Thread-parallel variant for the multi-core CPU baseline only.  The
+ * checker is built without ORC_THREADS: par_for is then a plain loop in
+ * index order and orc_add a plain add, so its arithmetic is unchanged.
+ * The threaded build (liboracle_mt.so) splits the loops into contiguous
+ * chunks over std::thread workers, sums dot products per chunk and
+ * scatters element contributions with atomic adds, so its sums are
+ * ordered differently. */
+#ifdef ORC_THREADS
+#include <atomic>
+#include <functional>
+#include <thread>
+namespace {
+int orc_nthreads() {
+  static int n = [] {
+    const char *e = std::getenv("ORC_THREADS");
+    int v = e ? std::atoi(e) : (int)std::thread::hardware_concurrency();
+    return v > 0 ? v : 1;
+  }();
+  return n;
+}
+// Persistent workers released by a generation counter; the caller runs
+// chunk 0 and waits for the others.
+struct Pool {
+  int T;
+  std::vector<std::thread> th;
+  std::atomic<unsigned> gen{0};
+  std::atomic<int> done{0};
+  std::function<void(int, int)> job;   // (thread, nthreads)
+  explicit Pool(int t) : T(t) {
+    for (int k = 1; k < T; ++k)
+      th.emplace_back([this, k] {
+        unsigned seen = 0;
+        for (;;) {
+          unsigned g;
+          while ((g = gen.load(std::memory_order_acquire)) == seen) std::this_thread::yield();
+          seen = g;
+          job(k, T);
+          done.fetch_add(1, std::memory_order_acq_rel);
+        }
+      });
+    for (auto &x : th) x.detach();
+  }
+  void run(const std::function<void(int, int)> &f) {
+    job = f;
+    done.store(0, std::memory_order_relaxed);
+    gen.fetch_add(1, std::memory_order_acq_rel);
+    f(0, T);
+    while (done.load(std::memory_order_acquire) != T - 1) std::this_thread::yield();
+  }
+};
+Pool &pool() {
+  static Pool *p = new Pool(orc_nthreads());
+  return *p;
+}
+template <class F>
+void par_for(int n, F f) {
+  if (orc_nthreads() <= 1 || n < 4096) {
+    for (int i = 0; i < n; ++i) f(i);
+    return;
+  }
+  pool().run([&](int t, int T) {
+    const int i0 = (int)((long long)n * t / T), i1 = (int)((long long)n * (t + 1) / T);
+    for (int i = i0; i < i1; ++i) f(i);
+  });
+}
+inline void orc_add(double &x, double v) { std::atomic_ref<double>(x).fetch_add(v, std::memory_order_relaxed); }
+}  // namespace
+#else
+namespace {
+template <class F>
+inline void par_for(int n, F f) {
+  for (int i = 0; i < n; ++i) f(i);
+}
+inline void orc_add(double &x, double v) { x = x + v; }
+}  // namespace
+#endif
+
 namespace {
 
 /* ------------------------------------------------------------------ */
@@ -51,6 +128,19 @@ Itpack g_itp; /* process-global, like the Fortran common blocks */
 /* sdot, itpackv.F:2828-2845: plain sequential sum. */
 double sdot(int n, const double *x, const double *y) {
   double d = 0.0;
+#ifdef ORC_THREADS
+  if (orc_nthreads() > 1 && n >= 4096) {
+    std::vector<double> part(orc_nthreads(), 0.0);
+    pool().run([&](int t, int T) {
+      const int i0 = (int)((long long)n * t / T), i1 = (int)((long long)n * (t + 1) / T);
+      double s = 0.0;
+      for (int i = i0; i < i1; ++i) s = s + x[i] * y[i];
+      part[t] = s;
+    });
+    for (double v : part) d = d + v;
+    return d;
+  }
+#endif
   for (int i = 0; i < n; ++i) d = d + x[i] * y[i];
   return d;
 }
@@ -59,8 +149,9 @@ double sdot(int n, const double *x, const double *y) {
 void pjac(int n, int ndim, int maxnz, const int *jcoef, const double *coef,
           const double *u, double *rhs) {
   for (int j = 1; j < maxnz; ++j)
-    for (int i = 0; i < n; ++i)
+    par_for(n, [&](int i) {
       rhs[i] = rhs[i] - coef[i + (size_t)ndim * j] * u[jcoef[i + (size_t)ndim * j] - 1];
+    });
 }
 
 /* pmult, itpackv.F:1970-2005 (c = b - sum_j coef(:,j)*b(jcoef(:,j))). */
@@ -68,8 +159,9 @@ void pmult(int n, int ndim, int maxnz, const int *jcoef, const double *coef,
            const double *b, double *c) {
   for (int i = 0; i < n; ++i) c[i] = b[i];
   for (int j = 1; j < maxnz; ++j)
-    for (int i = 0; i < n; ++i)
+    par_for(n, [&](int i) {
       c[i] = c[i] - coef[i + (size_t)ndim * j] * b[jcoef[i + (size_t)ndim * j] - 1];
+    });
 }
 
 /* determ, itpackv.F:1029-1068: characteristic polynomial of tri at xlmda. */
@@ -282,10 +374,10 @@ void itjcg(int n, int ndim, int maxnz, const int *jcoef, const double *coef,
   pstop_nrms(unorm, dnrm, c.cme, c.q1);
   if (c.halt) return;
   parcon(dtnrm, c1, c2, c3, c4, c.gamold, c.rhoold);
-  for (int i = 0; i < n; ++i) {
+  par_for(n, [&](int i) {
     u1[i] = c1 * d[i] + c2 * u[i] + c3 * u1[i];
     d1[i] = c1 * dtwd[i] + c4 * d[i] + c3 * d1[i];
-  }
+  });
 }
 
 /* scal, itpackv.F:2281-2421. */
@@ -665,7 +757,7 @@ int orc_model_gwce(orc_model *m, const orc_step_t *s, orc_stepout_t *out) {
   if (m->ncchange > 0) {
     m->ncchange = 0;
     for (size_t k = 0; k < (size_t)np * mnei; ++k) Coef[k] = 0.0;
-    for (int ie = 0; ie < ne; ++ie) {
+    par_for(ne, [&](int ie) {
       int n1 = NM(a, ie, 0), n2 = NM(a, ie, 1), n3 = NM(a, ie, 2);
       int NCEle = a->nodecode[n1] * a->nodecode[n2] * a->nodecode[n3] * a->noff[ie];
       double FDX1 = a->fdxe[3 * (size_t)ie], FDX2 = a->fdxe[3 * (size_t)ie + 1], FDX3 = a->fdxe[3 * (size_t)ie + 2];
@@ -687,16 +779,16 @@ int orc_model_gwce(orc_model *m, const orc_step_t *s, orc_stepout_t *out) {
       int J31 = cp[ie + (size_t)ne * (2 + 3 * 0)] - 1;
       int J32 = cp[ie + (size_t)ne * (2 + 3 * 1)] - 1;
       double nc = (double)NCEle;
-      COEF(n1, 0) = COEF(n1, 0) + (MsFacLOnDiag + GA00DPAvgOAreaIE4 * (FDX1 * FDX1 + FDY1 * FDY1)) * nc;
-      COEF(n1, J12) = COEF(n1, J12) + (MsFacLOffDiag + GA00DPAvgOAreaIE4 * (FDX1 * FDX2 + FDY1 * FDY2)) * nc;
-      COEF(n1, J13) = COEF(n1, J13) + (MsFacLOffDiag + GA00DPAvgOAreaIE4 * (FDX1 * FDX3 + FDY1 * FDY3)) * nc;
-      COEF(n2, J21) = COEF(n2, J21) + (MsFacLOffDiag + GA00DPAvgOAreaIE4 * (FDX2 * FDX1 + FDY2 * FDY1)) * nc;
-      COEF(n2, 0) = COEF(n2, 0) + (MsFacLOnDiag + GA00DPAvgOAreaIE4 * (FDX2 * FDX2 + FDY2 * FDY2)) * nc;
-      COEF(n2, J23) = COEF(n2, J23) + (MsFacLOffDiag + GA00DPAvgOAreaIE4 * (FDX2 * FDX3 + FDY2 * FDY3)) * nc;
-      COEF(n3, J31) = COEF(n3, J31) + (MsFacLOffDiag + GA00DPAvgOAreaIE4 * (FDX3 * FDX1 + FDY3 * FDY1)) * nc;
-      COEF(n3, J32) = COEF(n3, J32) + (MsFacLOffDiag + GA00DPAvgOAreaIE4 * (FDX3 * FDX2 + FDY3 * FDY2)) * nc;
-      COEF(n3, 0) = COEF(n3, 0) + (MsFacLOnDiag + GA00DPAvgOAreaIE4 * (FDX3 * FDX3 + FDY3 * FDY3)) * nc;
-    }
+      orc_add(COEF(n1, 0), (MsFacLOnDiag + GA00DPAvgOAreaIE4 * (FDX1 * FDX1 + FDY1 * FDY1)) * nc);
+      orc_add(COEF(n1, J12), (MsFacLOffDiag + GA00DPAvgOAreaIE4 * (FDX1 * FDX2 + FDY1 * FDY2)) * nc);
+      orc_add(COEF(n1, J13), (MsFacLOffDiag + GA00DPAvgOAreaIE4 * (FDX1 * FDX3 + FDY1 * FDY3)) * nc);
+      orc_add(COEF(n2, J21), (MsFacLOffDiag + GA00DPAvgOAreaIE4 * (FDX2 * FDX1 + FDY2 * FDY1)) * nc);
+      orc_add(COEF(n2, 0), (MsFacLOnDiag + GA00DPAvgOAreaIE4 * (FDX2 * FDX2 + FDY2 * FDY2)) * nc);
+      orc_add(COEF(n2, J23), (MsFacLOffDiag + GA00DPAvgOAreaIE4 * (FDX2 * FDX3 + FDY2 * FDY3)) * nc);
+      orc_add(COEF(n3, J31), (MsFacLOffDiag + GA00DPAvgOAreaIE4 * (FDX3 * FDX1 + FDY3 * FDY1)) * nc);
+      orc_add(COEF(n3, J32), (MsFacLOffDiag + GA00DPAvgOAreaIE4 * (FDX3 * FDX2 + FDY3 * FDY2)) * nc);
+      orc_add(COEF(n3, 0), (MsFacLOnDiag + GA00DPAvgOAreaIE4 * (FDX3 * FDX3 + FDY3 * FDY3)) * nc);
+    });
     /* gwce.F:646-650 */
     double EP = 0.0;
     for (int i = 0; i < np; ++i) EP = EP + COEF(i, 0) * COEF(i, 0);
@@ -732,7 +824,7 @@ int orc_model_gwce(orc_model *m, const orc_step_t *s, orc_stepout_t *out) {
 
   /* RHS element loop, gwce.F:1000-1617 (NWS/NRS gate for PR1, WSX1) */
   const bool met = (p.nws != 0);
-  for (int ie = 0; ie < ne; ++ie) {
+  par_for(ne, [&](int ie) {
     int n1 = NM(a, ie, 0), n2 = NM(a, ie, 1), n3 = NM(a, ie, 2);
     int NCEle = a->nodecode[n1] * a->nodecode[n2] * a->nodecode[n3] * a->noff[ie];
     double E0N1 = a->eta1[n1], E0N2 = a->eta1[n2], E0N3 = a->eta1[n3];
@@ -835,11 +927,11 @@ int orc_model_gwce(orc_model *m, const orc_step_t *s, orc_stepout_t *out) {
                 GDPAvgOAreaIE4 * (A00pB00 * (FDX3 * E1XGrad2A + FDY3 * E1YGrad2A)) +
                 (JXAvg * FDX3 + JYAvg * FDY3) * 0.5 + Tau0SpaVar;
     double nc = (double)NCEle;
-    a->gwce_lv[n1] = a->gwce_lv[n1] + T1 * nc;
-    a->gwce_lv[n2] = a->gwce_lv[n2] + T2 * nc;
-    a->gwce_lv[n3] = a->gwce_lv[n3] + T3 * nc;
+    orc_add(a->gwce_lv[n1], T1 * nc);
+    orc_add(a->gwce_lv[n2], T2 * nc);
+    orc_add(a->gwce_lv[n3], T3 * nc);
     (void)AreaIE;
-  }
+  });
 
   /* gwce.F:1622-1631 */
   for (int i = 0; i < np; ++i) {
@@ -1098,7 +1190,7 @@ int orc_model_momentum(orc_model *m, const orc_step_t *s) {
   const double THIRD = 1.0 / 3.0, GO2 = G / 2.0, DTO2 = DT / 2.0;
   const double Cfac1 = 1.0, Cfac2 = 1.0;
   const bool met = (p.nws != 0);
-  for (int ie = 0; ie < ne; ++ie) {
+  par_for(ne, [&](int ie) {
     int n1 = NM(a, ie, 0), n2 = NM(a, ie, 1), n3 = NM(a, ie, 2);
     int NCEle = a->nodecode[n1] * a->nodecode[n2] * a->nodecode[n3] * a->noff[ie];
     double U1N1 = a->uu1[n1], U1N2 = a->uu1[n2], U1N3 = a->uu1[n3];
@@ -1154,13 +1246,13 @@ int orc_model_momentum(orc_model *m, const orc_step_t *s) {
                            (1.5 * (LSYXN2 * FDX2 + LSYYN2 * FDY2)) / H1N2);
     double B3 = nc * DT * (-p.ifnlct * (U1AvgDV1DXA + V1AvgDV1DYA) - GO2 * DBTPDYA - 0.0 -
                            (1.5 * (LSYXN3 * FDX3 + LSYYN3 * FDY3)) / H1N3);
-    a->mom_lv_x[n1] = a->mom_lv_x[n1] + A1;
-    a->mom_lv_x[n2] = a->mom_lv_x[n2] + A2;
-    a->mom_lv_x[n3] = a->mom_lv_x[n3] + A3;
-    a->mom_lv_y[n1] = a->mom_lv_y[n1] + B1;
-    a->mom_lv_y[n2] = a->mom_lv_y[n2] + B2;
-    a->mom_lv_y[n3] = a->mom_lv_y[n3] + B3;
-  }
+    orc_add(a->mom_lv_x[n1], A1);
+    orc_add(a->mom_lv_x[n2], A2);
+    orc_add(a->mom_lv_x[n3], A3);
+    orc_add(a->mom_lv_y[n1], B1);
+    orc_add(a->mom_lv_y[n2], B2);
+    orc_add(a->mom_lv_y[n3], B3);
+  });
   /* nodal part, momentum.F:713-803 */
   std::vector<double> AUV(4 * (size_t)np);
   for (int i = 0; i < np; ++i) {

@@ -16,6 +16,7 @@ import numpy as np
 
 HERE = pathlib.Path(__file__).resolve().parent
 LIB = HERE / "_build" / "liboracle.so"
+LIB_MT = HERE / "_build" / "liboracle_mt.so"   # multi-core timing baseline, not the checker
 
 dp_ = C.POINTER(C.c_double)
 ip_ = C.POINTER(C.c_int)
@@ -82,6 +83,7 @@ class OrcVortex(C.Structure):
 
 
 _lib = None
+_lib_mt = None
 
 
 def build():
@@ -89,13 +91,18 @@ def build():
     return LIB
 
 
-def load():
-    global _lib
-    if _lib is not None:
+def load(omp: bool = False):
+    """The checker (serial) or, with `omp`, the multi-threaded build (its
+    loops split over all host cores) used only as the multi-core CPU
+    baseline."""
+    global _lib, _lib_mt
+    if omp and _lib_mt is not None:
+        return _lib_mt
+    if not omp and _lib is not None:
         return _lib
-    if not LIB.exists():
+    if not (LIB_MT if omp else LIB).exists():
         build()
-    lib = C.CDLL(str(LIB))
+    lib = C.CDLL(str(LIB_MT if omp else LIB))
     lib.orc_jcg.argtypes = [ip_, ip_, ip_, ip_, dp_, dp_, dp_, ip_, ip_, dp_, ip_, dp_, ip_]
     lib.orc_jcg.restype = None
     lib.orc_dfault.argtypes = [ip_, dp_]
@@ -137,7 +144,10 @@ def load():
     for name, args in sig.items():
         getattr(lib, name).argtypes = args
         getattr(lib, name).restype = C.c_int
-    _lib = lib
+    if omp:
+        _lib_mt = lib
+    else:
+        _lib = lib
     return lib
 
 
@@ -148,8 +158,8 @@ def _ptr(a, typ):
 class OracleModel:
     """Serial FP64 oracle stepping a case's arrays in place (its own copy)."""
 
-    def __init__(self, case):
-        self.lib = load()
+    def __init__(self, case, omp: bool = False):
+        self.lib = load(omp)
         self.case = case
         self.p = OrcParams()
         for k, v in case.params.items():
