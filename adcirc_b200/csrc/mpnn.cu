@@ -13,6 +13,7 @@
 //   h_l,i = ReLU(Ws_l h_l-1,i + Wn_l mean_{j in N(i)} h_l-1,j + b_l)   l = 1..3
 //   ETAS_guess_i = ETAS_ref_i + s_out (w_out . h3_i + b_out)
 //
+// with s_out a fixed scale of the corrections (set with the weights).
 // N(i) is the node's NeiTab ring (the GWCE matrix pattern).  Weights are
 // FP32 masters with BF16 copies for the tensor-core passes; activations
 // are stored in BF16, gradients in FP32.  JCG iterates to the unchanged
@@ -20,8 +21,9 @@
 // residual (warm.cu), so the network can cost iterations but not accuracy.
 //
 // Training (adc_predictor_train) runs after each step's solve on the pair
-// (features before the solve, solved ETAS): MSE of the normalised
-// correction over wet interior nodes, exact backpropagation through the
+// (features before the solve, solved ETAS): Huber loss (quadratic within
+// kHuber, linear beyond) of the normalised correction over wet interior
+// nodes, so the few nodes at a moving wet/dry front do not dominate it; exact backpropagation through the
 // head, the three message-passing layers and the input layer, weight
 // gradients as per-CTA partial GEMMs summed in a fixed order, and an Adam
 // update of the FP32 masters.  With ADC_LEARNED_START off the solver keeps
@@ -39,6 +41,8 @@ constexpr int kH = 64;              // hidden width
 constexpr int kL = 3;               // message-passing layers
 constexpr int kTile = 64;           // nodes per CTA tile
 constexpr int kMpThreads = 128;     // 4 warps, 16 nodes each
+constexpr float kHuber = 3.f;       // Huber threshold of the normalised error
+constexpr int kNStats = 2;          // Mpnn::stats entries
 
 // Flat FP32 parameter layout (adc_set_predictor / adc_get_predictor).
 constexpr int kOffWin = 0;                                  // W_in [64][16]
@@ -122,6 +126,131 @@ struct MpArgs {
 constexpr int kSA = 2 * kH + 8;     // A rows of up to 128
 constexpr int kSX = kF + 8;
 
+// Neighbour gathers.  A tile's 64 nodes have contiguous CSR slices, so a
+// CTA stages the tile's ring pointers and (when they fit) its neighbour
+// indices in shared memory with coalesced loads; then 8 lanes share a node,
+// each summing 8 channels of the neighbours' rows with 16-byte loads, the
+// first kRing neighbours' rows requested together.  Every channel sums its
+// neighbours in NeiTab order.
+constexpr int kIdxCap = 1024;       // staged neighbour indices per tile
+constexpr int kRing = 8;            // neighbour rows requested together
+
+template <bool W>
+struct TileRing {
+  int ptr[kTile + 1];
+  int idx[kIdxCap];
+  float w[W ? kIdxCap : 1];         // 1/deg of each neighbour (dz sums)
+};
+
+// Stages the CSR slice of the tile at node0; returns whether its indices
+// fit in shared memory (otherwise they are read from global memory).
+template <bool W>
+__device__ bool stage_ring(const MpArgs &a, int node0, TileRing<W> &s) {
+  const int nt = min(kTile, a.n - node0);
+  for (int t = threadIdx.x; t <= nt; t += blockDim.x) s.ptr[t] = a.nb_ptr[node0 + t];
+  __syncthreads();
+  const int base = s.ptr[0], cnt = s.ptr[nt] - base;
+  const bool fit = cnt <= kIdxCap;
+  if (fit)
+    for (int q = threadIdx.x; q < cnt; q += blockDim.x) {
+      const int j = a.nb_idx[base + q];
+      s.idx[q] = j;
+      if (W) s.w[q] = a.inv_deg[j];
+    }
+  __syncthreads();
+  return fit;
+}
+
+__device__ __forceinline__ void add_bf16x8(float (&acc)[8], const uint4 &v) {
+  const __nv_bfloat162 *b = reinterpret_cast<const __nv_bfloat162 *>(&v);
+#pragma unroll
+  for (int e = 0; e < 4; ++e) {
+    const float2 f = __bfloat1622float2(b[e]);
+    acc[2 * e] += f.x;
+    acc[2 * e + 1] += f.y;
+  }
+}
+
+__device__ __forceinline__ void unpack_bf16x8(float (&o)[8], const uint4 &v) {
+  const __nv_bfloat162 *b = reinterpret_cast<const __nv_bfloat162 *>(&v);
+#pragma unroll
+  for (int e = 0; e < 4; ++e) {
+    const float2 f = __bfloat1622float2(b[e]);
+    o[2 * e] = f.x;
+    o[2 * e + 1] = f.y;
+  }
+}
+
+__device__ __forceinline__ uint4 pack_bf16x8(const float (&v)[8]) {
+  uint4 o;
+  o.x = pack_bf16(v[0], v[1]);
+  o.y = pack_bf16(v[2], v[3]);
+  o.z = pack_bf16(v[4], v[5]);
+  o.w = pack_bf16(v[6], v[7]);
+  return o;
+}
+
+// Row r of the staged tile: sum over its ring of h_j[8 ch .. 8 ch + 7].
+template <bool W>
+__device__ __forceinline__ void ring_chunk_h(const MpArgs &a, const TileRing<W> &s, bool fit,
+                                             const __nv_bfloat16 *h, int r, int ch, float (&acc)[8]) {
+  const int p0 = s.ptr[r], deg = s.ptr[r + 1] - p0, o = p0 - s.ptr[0];
+#pragma unroll
+  for (int e = 0; e < 8; ++e) acc[e] = 0.f;
+  uint4 v[kRing];
+#pragma unroll
+  for (int q = 0; q < kRing; ++q) {
+    v[q] = make_uint4(0u, 0u, 0u, 0u);
+    if (q < deg) {
+      const int j = fit ? s.idx[o + q] : a.nb_idx[p0 + q];
+      v[q] = reinterpret_cast<const uint4 *>(h + (size_t)j * kH)[ch];
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < kRing; ++q)
+    if (q < deg) add_bf16x8(acc, v[q]);
+  for (int q = kRing; q < deg; ++q) {
+    const int j = fit ? s.idx[o + q] : a.nb_idx[p0 + q];
+    add_bf16x8(acc, reinterpret_cast<const uint4 *>(h + (size_t)j * kH)[ch]);
+  }
+}
+
+// Row r of the staged tile: sum over its ring of dz_j[8 ch .. +7] / deg_j.
+__device__ __forceinline__ void ring_chunk_dz(const MpArgs &a, const TileRing<true> &s, bool fit,
+                                              const float *dz, int r, int ch, float (&acc)[8]) {
+  const int p0 = s.ptr[r], deg = s.ptr[r + 1] - p0, o = p0 - s.ptr[0];
+#pragma unroll
+  for (int e = 0; e < 8; ++e) acc[e] = 0.f;
+  for (int q0 = 0; q0 < deg; q0 += kRing / 2) {
+    float4 v[kRing / 2][2];
+    float w[kRing / 2];
+#pragma unroll
+    for (int q = 0; q < kRing / 2; ++q) {
+      v[q][0] = v[q][1] = make_float4(0.f, 0.f, 0.f, 0.f);
+      w[q] = 0.f;
+      if (q0 + q < deg) {
+        const int j = fit ? s.idx[o + q0 + q] : a.nb_idx[p0 + q0 + q];
+        w[q] = fit ? s.w[o + q0 + q] : a.inv_deg[j];
+        const float4 *row = reinterpret_cast<const float4 *>(dz + (size_t)j * kH) + 2 * ch;
+        v[q][0] = row[0];
+        v[q][1] = row[1];
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < kRing / 2; ++q)
+      if (q0 + q < deg) {
+        acc[0] += v[q][0].x * w[q];
+        acc[1] += v[q][0].y * w[q];
+        acc[2] += v[q][0].z * w[q];
+        acc[3] += v[q][0].w * w[q];
+        acc[4] += v[q][1].x * w[q];
+        acc[5] += v[q][1].y * w[q];
+        acc[6] += v[q][1].z * w[q];
+        acc[7] += v[q][1].w * w[q];
+      }
+  }
+}
+
 // ----------------------------------------------------------- the features
 __global__ void k_mp_features(adc_ctx c, Mpnn m) {
   griddep_wait();
@@ -165,17 +294,18 @@ __global__ void __launch_bounds__(kMpThreads) k_mp_dense(MpArgs a, int layer,
   constexpr int SA = MODE == 0 ? kSX : kSA;
   __shared__ __align__(16) __nv_bfloat16 sA[kTile * SA];
   __shared__ __align__(16) __nv_bfloat16 sB[kH * SA];
+  __shared__ TileRing<MODE == 2> ring;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int node0 = blockIdx.x * kTile;
   // B^T[64 x K]
   if (MODE == 0) {
-    for (int q = threadIdx.x; q < kH * kF; q += blockDim.x)
-      sB[(q / kF) * SA + q % kF] = a.wbf[q];
+    for (int q = threadIdx.x; q < kH * kF / 8; q += blockDim.x)
+      reinterpret_cast<uint4 *>(sB + (q / 2) * SA)[q & 1] = reinterpret_cast<const uint4 *>(a.wbf)[q];
   } else {
     const __nv_bfloat16 *w = a.wbf + kH * kF + (size_t)layer * kH * 2 * kH;   // [64][128] = [Ws | Wn]
     if (MODE == 1) {
-      for (int q = threadIdx.x; q < kH * 2 * kH; q += blockDim.x)
-        sB[(q / (2 * kH)) * SA + q % (2 * kH)] = w[q];
+      for (int q = threadIdx.x; q < kH * 2 * kH / 8; q += blockDim.x)
+        reinterpret_cast<uint4 *>(sB + (q / 16) * SA)[q & 15] = reinterpret_cast<const uint4 *>(w)[q];
     } else {
       // dgrad: B[k][o] = Ws[k][o] (k < 64), Wn[k-64][o]; B^T[o][k]
       for (int q = threadIdx.x; q < kH * 2 * kH; q += blockDim.x) {
@@ -184,45 +314,40 @@ __global__ void __launch_bounds__(kMpThreads) k_mp_dense(MpArgs a, int layer,
       }
     }
   }
-  // A rows of this warp's 16 nodes
-  for (int r = 0; r < 16; ++r) {
-    const int row = warp * 16 + r, i = node0 + row;
-    __nv_bfloat16 *ar = sA + row * SA;
-    if (MODE == 0) {
-      if (lane < kF / 2) {
-        __nv_bfloat162 v = __floats2bfloat162_rn(0.f, 0.f);
-        if (i < a.n) v = reinterpret_cast<const __nv_bfloat162 *>(hin + (size_t)i * kF)[lane];
-        reinterpret_cast<__nv_bfloat162 *>(ar)[lane] = v;
-      }
-      continue;
+  // A rows: [x] (mode 0), [h | mean_N h] (mode 1), [dz | sum_N dz_j / deg_j]
+  if constexpr (MODE == 0) {
+    for (int q = threadIdx.x; q < kTile * 2; q += blockDim.x) {
+      const int row = q >> 1, i = node0 + row;
+      uint4 v = make_uint4(0u, 0u, 0u, 0u);
+      if (i < a.n) v = reinterpret_cast<const uint4 *>(hin + (size_t)i * kF)[q & 1];
+      reinterpret_cast<uint4 *>(sA + row * SA)[q & 1] = v;
     }
-    float2 self = make_float2(0.f, 0.f), agg = make_float2(0.f, 0.f);
-    if (i < a.n) {
-      const int p0 = a.nb_ptr[i], p1 = a.nb_ptr[i + 1];
-      if (MODE == 1) {
-        self = __bfloat1622float2(reinterpret_cast<const __nv_bfloat162 *>(hin + (size_t)i * kH)[lane]);
-        for (int p = p0; p < p1; ++p) {
-          const float2 v = __bfloat1622float2(
-              reinterpret_cast<const __nv_bfloat162 *>(hin + (size_t)a.nb_idx[p] * kH)[lane]);
-          agg.x += v.x;
-          agg.y += v.y;
-        }
-        const float s = a.inv_deg[i];
-        agg.x *= s;
-        agg.y *= s;
-      } else {
-        self = reinterpret_cast<const float2 *>(dzin + (size_t)i * kH)[lane];
-        for (int p = p0; p < p1; ++p) {
-          const int j = a.nb_idx[p];
-          const float2 v = reinterpret_cast<const float2 *>(dzin + (size_t)j * kH)[lane];
-          const float s = a.inv_deg[j];
-          agg.x += v.x * s;
-          agg.y += v.y * s;
+  } else {
+    const bool fit = stage_ring<MODE == 2>(a, node0, ring);
+    const int ch = threadIdx.x & 7;
+    for (int row = threadIdx.x >> 3; row < kTile; row += kMpThreads / 8) {
+      const int i = node0 + row;
+      float self[8], agg[8];
+#pragma unroll
+      for (int e = 0; e < 8; ++e) self[e] = agg[e] = 0.f;
+      if (i < a.n) {
+        if constexpr (MODE == 1) {
+          unpack_bf16x8(self, reinterpret_cast<const uint4 *>(hin + (size_t)i * kH)[ch]);
+          ring_chunk_h(a, ring, fit, hin, row, ch, agg);
+          const float sc = a.inv_deg[i];
+#pragma unroll
+          for (int e = 0; e < 8; ++e) agg[e] *= sc;
+        } else {
+          const float4 *d = reinterpret_cast<const float4 *>(dzin + (size_t)i * kH) + 2 * ch;
+          const float4 d0 = d[0], d1 = d[1];
+          self[0] = d0.x; self[1] = d0.y; self[2] = d0.z; self[3] = d0.w;
+          self[4] = d1.x; self[5] = d1.y; self[6] = d1.z; self[7] = d1.w;
+          ring_chunk_dz(a, ring, fit, dzin, row, ch, agg);
         }
       }
+      reinterpret_cast<uint4 *>(sA + row * SA)[ch] = pack_bf16x8(self);
+      reinterpret_cast<uint4 *>(sA + row * SA + kH)[ch] = pack_bf16x8(agg);
     }
-    reinterpret_cast<unsigned *>(ar)[lane] = pack_bf16(self.x, self.y);
-    reinterpret_cast<unsigned *>(ar + kH)[lane] = pack_bf16(agg.x, agg.y);
   }
   __syncthreads();
   float acc[8][4];
@@ -273,41 +398,49 @@ __global__ void __launch_bounds__(kMpThreads) k_mp_wgrad(MpArgs a, const float *
   float acc[NT][4];
 #pragma unroll
   for (int nt = 0; nt < NT; ++nt) acc[nt][0] = acc[nt][1] = acc[nt][2] = acc[nt][3] = 0.f;
-  for (int ch = 0; ch < chunks_per_cta; ++ch) {
-    const int node0 = (blockIdx.x * chunks_per_cta + ch) * kTile;
+  __shared__ TileRing<false> ring;
+  for (int chunk = 0; chunk < chunks_per_cta; ++chunk) {
+    const int node0 = (blockIdx.x * chunks_per_cta + chunk) * kTile;
     if (node0 >= a.n) break;
     __syncthreads();
-    for (int r = warp; r < kTile; r += kMpThreads / 32) {
+    const bool fit = MODE == 1 ? stage_ring<false>(a, node0, ring) : true;
+    const int ch = threadIdx.x & 7;
+    for (int r = threadIdx.x >> 3; r < kTile; r += kMpThreads / 8) {
       const int i = node0 + r;
-      float2 d = make_float2(0.f, 0.f);
-      if (i < a.n) d = reinterpret_cast<const float2 *>(dz + (size_t)i * kH)[lane];
-      sDt[(2 * lane) * SN + r] = __float2bfloat16_rn(d.x);
-      sDt[(2 * lane + 1) * SN + r] = __float2bfloat16_rn(d.y);
+      float d[8], self[8], agg[8];
+#pragma unroll
+      for (int e = 0; e < 8; ++e) d[e] = self[e] = agg[e] = 0.f;
+      if (i < a.n) {
+        const float4 *dr = reinterpret_cast<const float4 *>(dz + (size_t)i * kH) + 2 * ch;
+        const float4 d0 = dr[0], d1 = dr[1];
+        d[0] = d0.x; d[1] = d0.y; d[2] = d0.z; d[3] = d0.w;
+        d[4] = d1.x; d[5] = d1.y; d[6] = d1.z; d[7] = d1.w;
+        if constexpr (MODE == 0) {
+          if (ch < 2) unpack_bf16x8(self, reinterpret_cast<const uint4 *>(hin + (size_t)i * kF)[ch]);
+        } else {
+          unpack_bf16x8(self, reinterpret_cast<const uint4 *>(hin + (size_t)i * kH)[ch]);
+          ring_chunk_h(a, ring, fit, hin, r, ch, agg);
+          const float sc = a.inv_deg[i];
+#pragma unroll
+          for (int e = 0; e < 8; ++e) agg[e] *= sc;
+        }
+      }
+#pragma unroll
+      for (int e = 0; e < 8; ++e) sDt[(8 * ch + e) * SN + r] = __float2bfloat16_rn(d[e]);
       if (MODE == 0) {
-        if (lane < kF) {
-          __nv_bfloat16 v = __float2bfloat16_rn(0.f);
-          if (i < a.n) v = hin[(size_t)i * kF + lane];
-          sAt[lane * SN + r] = v;
-        }
+        if (ch < 2)
+#pragma unroll
+          for (int e = 0; e < 8; ++e) sAt[(8 * ch + e) * SN + r] = __float2bfloat16_rn(self[e]);
       } else {
-        float2 self = make_float2(0.f, 0.f), agg = make_float2(0.f, 0.f);
-        if (i < a.n) {
-          self = __bfloat1622float2(reinterpret_cast<const __nv_bfloat162 *>(hin + (size_t)i * kH)[lane]);
-          const int p0 = a.nb_ptr[i], p1 = a.nb_ptr[i + 1];
-          for (int p = p0; p < p1; ++p) {
-            const float2 v = __bfloat1622float2(
-                reinterpret_cast<const __nv_bfloat162 *>(hin + (size_t)a.nb_idx[p] * kH)[lane]);
-            agg.x += v.x;
-            agg.y += v.y;
-          }
-          agg.x *= a.inv_deg[i];
-          agg.y *= a.inv_deg[i];
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+          sAt[(8 * ch + e) * SN + r] = __float2bfloat16_rn(self[e]);
+          sAt[(kH + 8 * ch + e) * SN + r] = __float2bfloat16_rn(agg[e]);
         }
-        sAt[(2 * lane) * SN + r] = __float2bfloat16_rn(self.x);
-        sAt[(2 * lane + 1) * SN + r] = __float2bfloat16_rn(self.y);
-        sAt[(kH + 2 * lane) * SN + r] = __float2bfloat16_rn(agg.x);
-        sAt[(kH + 2 * lane + 1) * SN + r] = __float2bfloat16_rn(agg.y);
-        if (lane < 16) sAt[(2 * kH + lane) * SN + r] = __float2bfloat16_rn(lane == 0 && i < a.n ? 1.f : 0.f);
+        // the bias column (row 128 of A^T) and its zero padding
+#pragma unroll
+        for (int e = 0; e < 2; ++e)
+          sAt[(2 * kH + 2 * ch + e) * SN + r] = __float2bfloat16_rn(ch == 0 && e == 0 && i < a.n ? 1.f : 0.f);
       }
     }
     __syncthreads();
@@ -360,9 +493,9 @@ __global__ void k_mp_wreduce(const float *part, int nctas, int mode, int layer, 
 
 // ------------------------------------------------------------ the head
 // out_i = w_out . h3_i + b_out; the guess at wet interior nodes, the
-// reference elsewhere.  With `loss`, also dL/dout_i (MSE of the normalised
-// correction over wet interior nodes, target from the solved ETAS) and the
-// block partials of the loss.
+// reference elsewhere.  With `loss`, also dL/dout_i (Huber loss of the
+// normalised correction over wet interior nodes, target from the solved
+// ETAS) and the block partials of the loss.
 __global__ void k_mp_head(adc_ctx c, Mpnn m, int mode) {
   griddep_wait();
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
@@ -374,20 +507,20 @@ __global__ void k_mp_head(adc_ctx c, Mpnn m, int mode) {
     float s = h.x * w[2 * lane] + h.y * w[2 * lane + 1];
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
     const float out = s + m.par[kOffBout];
-    const float s_out = m.par[kOffNorm + 2 * kNF];
+    const double s_out = (double)m.par[kOffNorm + 2 * kNF];
     const bool use = c.nodecode[i] == 1 && c.is_nbd[i] < 0;
     if (mode == 0) {
-      if (lane == 0) m.pred[i] = use ? m.ref[i] + (double)s_out * out : m.ref[i];
+      if (lane == 0) m.pred[i] = use ? m.ref[i] + s_out * out : m.ref[i];
     } else if (lane == 0) {
       float d = 0.f;
       if (use) {
         const double sol = m.tgt ? m.tgt[i] : c.etas[i];
         const float tgt = (float)((sol - m.ref[i]) / s_out);
-        const float e = out - tgt;
-        d = e;
-        l = (double)e * e;
+        const float e = out - tgt, ae = fabsf(e);
+        d = fminf(fmaxf(e, -kHuber), kHuber);
+        l = ae <= kHuber ? (double)e * e : (double)kHuber * (2.0 * ae - kHuber);
       }
-      m.dout[i] = d;   // scaled by 2 / n_used in the backward pass
+      m.dout[i] = d;   // half the loss derivative; scaled by 2 / n in the backward pass
     }
   }
   if (mode == 1) {
@@ -402,9 +535,9 @@ __global__ void k_mp_head(adc_ctx c, Mpnn m, int mode) {
   }
 }
 
-// dz3 = (dL/dout w_out) * (h3 > 0) with dL/dout = 2 e / n (the loss is the
-// mean over all nodes of e^2, e = 0 where the guess is not used); one warp
-// per node, lanes over channel pairs.
+// dz3 = (dL/dout w_out) * (h3 > 0) with dL/dout = 2 clamp(e) / n (the loss
+// is the mean over all nodes of the Huber loss of e, e = 0 where the guess
+// is not used); one warp per node, lanes over channel pairs.
 __global__ void k_mp_head_bwd(Mpnn m) {
   griddep_wait();
   const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
@@ -418,7 +551,7 @@ __global__ void k_mp_head_bwd(Mpnn m) {
 
 // Head gradient partials per CTA (its nodes, warp-strided, lanes over
 // channel pairs): dw_out[k] = sum d_i h3_i[k], db_out = sum d_i, with
-// d_i = 2 e_i / n.  Row b of `part` holds CTA b's 65 sums.
+// d_i = 2 clamp(e_i) / n.  Row b of `part` holds CTA b's 65 sums.
 __global__ void k_mp_head_grad(Mpnn m, int nodes_per_cta) {
   griddep_wait();
   __shared__ float sh[kMpThreads / 32][kH + 1];
@@ -444,7 +577,7 @@ __global__ void k_mp_head_grad(Mpnn m, int nodes_per_cta) {
 }
 
 // Sums the head partials in CTA order, and the loss partials of k_mp_head
-// (fixed tree) into stats[0] (the mean squared normalised error).
+// (fixed tree) into stats[0] (the mean Huber loss of the normalised error).
 __global__ void k_mp_head_reduce(Mpnn m, int nctas, int nloss) {
   griddep_wait();
   __shared__ double sh[32];
@@ -612,7 +745,7 @@ static int mp_alloc(adc_ctx *c) {
   rc |= al(&m->nb_ptr, n + 1); rc |= al(&m->nb_idx, idx.size()); rc |= al(&m->inv_deg, n);
   rc |= al(&m->part, (size_t)m->part_ctas * kH * (2 * kH + 16));
   rc |= al(&m->loss_part, (size_t)((n * 32LL + 255) / 256) + 1);
-  rc |= al(&m->stats, 2);
+  rc |= al(&m->stats, kNStats);
   if (rc) return ADC_ERR_NOMEM;
   ADC_CUDA(cudaMemcpy(m->nb_ptr, ptr.data(), (n + 1) * sizeof(int), cudaMemcpyHostToDevice));
   if (!idx.empty())
@@ -622,7 +755,7 @@ static int mp_alloc(adc_ctx *c) {
   ADC_CUDA(cudaMemset(m->grad, 0, kNParams * sizeof(float)));
   ADC_CUDA(cudaMemset(m->m1, 0, kNParams * sizeof(float)));
   ADC_CUDA(cudaMemset(m->m2, 0, kNParams * sizeof(float)));
-  ADC_CUDA(cudaMemset(m->stats, 0, 2 * sizeof(double)));
+  ADC_CUDA(cudaMemset(m->stats, 0, kNStats * sizeof(double)));
   ADC_CUDA(cudaMemset(m->dz[0], 0, (size_t)n * kH * sizeof(float)));
   ADC_CUDA(cudaMemset(m->dz[1], 0, (size_t)n * kH * sizeof(float)));
   c->mp = m;
@@ -673,7 +806,7 @@ int adc_set_predictor(adc_ctx *c, const float *params, int nparams) {
   ADC_CUDA(cudaMemcpy(c->mp->par, params, kNParams * sizeof(float), cudaMemcpyHostToDevice));
   ADC_CUDA(cudaMemset(c->mp->m1, 0, kNParams * sizeof(float)));
   ADC_CUDA(cudaMemset(c->mp->m2, 0, kNParams * sizeof(float)));
-  ADC_CUDA(cudaMemset(c->mp->stats, 0, 2 * sizeof(double)));
+  ADC_CUDA(cudaMemset(c->mp->stats, 0, kNStats * sizeof(double)));
   k_mp_tobf16<<<(kH * kF + kL * kH * 2 * kH + 255) / 256, 256, 0, c->stream>>>(*c->mp);
   ADC_CUDA(cudaGetLastError());
   ADC_CUDA(cudaStreamSynchronize(c->stream));
@@ -706,7 +839,7 @@ int adc_predictor_train(adc_ctx *c, int on, float lr) {
 
 int adc_predictor_stats(adc_ctx *c, double *loss, long long *adam_steps) {
   if (!c || !c->mp) return ADC_ERR_ARG;
-  double s[2];
+  double s[kNStats];
   ADC_CUDA(cudaStreamSynchronize(c->stream));
   ADC_CUDA(cudaMemcpy(s, c->mp->stats, sizeof(s), cudaMemcpyDeviceToHost));
   if (loss) *loss = s[0];

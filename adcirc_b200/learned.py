@@ -97,19 +97,32 @@ def track(rng, base_case, hours: float = 30.0) -> model.Vortex:
     return v
 
 
-def _stats_from(case, gpu, steps: int = 600):
-    """Feature means/scales and the correction scale from a short plain
-    run: s_out is the RMS change of the solved increment between steps at
-    wet interior nodes."""
-    gpu.run(1, steps)
+def use_mask(arrays) -> np.ndarray:
+    """Nodes where the network predicts: wet and off the elevation boundary."""
+    use = arrays["nodecode"] == 1
+    use[arrays["nbd"] - 1] = False
+    return use
+
+
+def _stats_from(case, gpu, hours: float = 6.0, samples: int = 60):
+    """Feature means/scales and the correction scale s_out from a plain run
+    into the storm: s_out is the RMS, over `samples` consecutive steps and
+    the wet interior nodes, of the change of the solved increment between
+    steps (the correction the network predicts)."""
+    start = int(round(hours * 3600 / case.params["dt"]))
+    gpu.run(1, start)
     gpu.sync_to_host()
     a = case.arrays
     x = features(a, case.params["prbckgrnd_mh2o"])
-    e0 = a["etas"].copy()
-    gpu.run(1 + steps, 1)
-    gpu.sync_to_host()
-    wet = (a["nodecode"] == 1)
-    s_out = float(np.sqrt(np.mean((a["etas"][wet] - e0[wet]) ** 2))) or 1e-6
+    ss, cnt = 0.0, 0
+    for k in range(samples):
+        e0 = a["etas"].copy()
+        use = use_mask(a)
+        gpu.run(1 + start + k, 1)
+        gpu.sync_to_host()
+        ss += float(np.sum((a["etas"][use] - e0[use]) ** 2))
+        cnt += int(use.sum())
+    s_out = math.sqrt(ss / max(cnt, 1)) or 1e-6
     return x.mean(axis=0), x.std(axis=0), s_out
 
 

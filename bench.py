@@ -285,6 +285,9 @@ PATHS = {
                              "dot products, norms, stopping test and state"),
     "mixed": (1, "FP32 GWCE assembly + SpMV matrix + momentum, FP64 reductions and state"),
     "warm": (2, "plain FP64 with the extrapolated JCG initial guess (residual-tested fallback)"),
+    "learned": (32, "plain FP64 with the learned (message-passing, BF16 tensor-core) JCG initial "
+                    "guess, residual-tested against the reference guess"),
+    "learned_spmv32": (32 | 8, "learned initial guess + FP32 SpMV matrix, FP64 elsewhere"),
 }
 
 
@@ -314,8 +317,10 @@ def _sync_dev(dist):
 def run_path(name, case, W, K, dist, ref_snaps, stop_on_fail):
     """Binds `case` in mode PATHS[name] and runs W + K hours.  Returns the
     per-hour records, the timed device ms (max over ranks) and the model."""
-    from adcirc_b200 import model
+    from adcirc_b200 import learned, model
     gpu = model.GpuModel(case, prec=PATHS[name][0])
+    if PATHS[name][0] & 32:
+        gpu.set_predictor(learned.load())
     it = 1
     hours = []
     ms_timed = 0.0
@@ -356,6 +361,39 @@ def run_path(name, case, W, K, dist, ref_snaps, stop_on_fail):
             break
     return {"hours": hours, "ms_timed": ms_timed, "launches": launches, "it": it,
             "failed_at": failed_at, "snaps": snaps if ref_snaps is None else None}, gpu
+
+
+def ensemble_leg(args, world, prec, log):
+    """Config-5 leg: `args.ensemble` members built as the surge mesh with
+    their own seeds and sizes (log-uniform 50k-400k nodes) and perturbed
+    vortices, stepped together (one captured graph per time step), the JCG
+    layout autotuned; aggregate sim-days/wall-hour over --ensemble-steps
+    time steps, beside the same members stepped one after another."""
+    from adcirc_b200 import ensemble
+    t0 = time.perf_counter()
+    specs = ensemble.member_specs(args.ensemble)
+    cases = ensemble.build_members(specs)
+    t_mesh = time.perf_counter() - t0
+    ens = ensemble.Ensemble(cases, prec=prec)
+    dt = cases[0].params["dt"]
+    ens.run(5)
+    best, tune = ensemble.autotune(ens, steps=20, log=log)
+    seq_ms = ensemble.sequential_step_ms(ens, steps=10)
+    n = args.ensemble_steps
+    first = ens.it
+    numitr, ms = ens.run(n)
+    nodes = ens.nodes
+    ens.close()
+    member_days = len(cases) * sim_days_per_hour(n, dt, ms / 1000.0)
+    return {"members": len(cases), "nodes_total": nodes,
+            "member_nodes": [c.sizes["np"] for c in cases],
+            "value": world * member_days, "unit": "member sim-days/wall-hour (aggregate)",
+            "ms_per_step": ms / n, "steps": n, "first_step": first,
+            "sequential_ms_per_step": seq_ms, "speedup_vs_sequential": seq_ms / (ms / n),
+            "autotune": {"chosen": best, "layouts": tune},
+            "jcg_iters_per_step": float(numitr.mean()), "mesh_seconds": t_mesh,
+            "note": "one captured CUDA graph per time step over all members (each member's "
+                    "kernels on its own stream); members keep one persistent JCG kernel each"}
 
 
 def oracle_check(case_fn, nsteps=5):
@@ -415,7 +453,9 @@ def bench_gpu(args, rank, world, dist):
     dt = base.params["dt"]
     npn, ne = base.sizes["np"], base.sizes["ne"]
     W, K = args.warmup, args.steps
-    names = ["plain"] + [p for p in args.paths.split(",") if p and p != "plain"]
+    from adcirc_b200 import learned
+    names = ["plain"] + [p for p in args.paths.split(",") if p and p != "plain"
+                         and (not PATHS[p][0] & 32 or learned.DEFAULT_WEIGHTS.exists())]
     res = {}
     models = {}
     plain_snaps = None
@@ -495,6 +535,7 @@ def bench_gpu(args, rank, world, dist):
         rl[k] = {"ms": kt_sum.get(k, 0.0), "algorithmic_bytes": None,
                  "note": "work varies per step (incremental rebuild, front activity)"}
     ocheck = oracle_check(case_fn) if (rank == 0 and not args.no_oracle) else None
+    ens = ensemble_leg(args, world, mode, lambda *a: None) if args.ensemble > 0 else None
     line = {
         "metric": METRIC, "value": res[chosen]["value"], "unit": UNIT, "n_gpus": world,
         "steps": K, "warmup": W, "ms_per_step": res[chosen]["ms_per_time_step"] * HOUR_STEPS,
@@ -512,6 +553,7 @@ def bench_gpu(args, rank, world, dist):
         "accuracy_bound": {"max_deta_m": BOUND_M, "comparator": "plain FP64 GPU path, hourly outputs"},
         "paths": res,
         "oracle_check": ocheck,
+        "ensemble": ens,
         "jcg_iters_per_step": res[chosen]["jcg_iters_per_step"],
         "kernel_ms": kt_sum,
         "roofline": {"bound": "hbm", "kernel": "jcg_kernel", "achieved": rl["jcg"]["achieved_gbs"],
@@ -552,9 +594,12 @@ def main():
     ap.add_argument("--warmup", type=int, default=4, help="warm-up simulated hours")
     ap.add_argument("--impl", default="adcgpu", choices=["adcgpu", "reference"])
     ap.add_argument("--case", default="surge", choices=["surge", "channel"])
-    ap.add_argument("--paths", default="spmv32,spmv32_mom32",
+    ap.add_argument("--paths", default="spmv32,spmv32_mom32,learned",
                     help="paths compared with plain FP64 (comma list of " + ",".join(PATHS) + ")")
     ap.add_argument("--e2e-hours", type=float, default=1.0)
+    ap.add_argument("--ensemble", type=int, default=48, help="ensemble members (0: no ensemble leg)")
+    ap.add_argument("--ensemble-steps", type=int, default=600,
+                    help="timed ensemble time steps (12 simulated hours: 43200)")
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--ref-seconds", type=float, default=3.0,
                     help="reference arm: host seconds sampled per bench step")

@@ -344,8 +344,8 @@ int adc_get_scalars(adc_ctx *ctx, adc_scalars_t *out);
  * from ETAS as GWCE_New leaves it, gwce.F:1846-1850, 2002-2004).  A
  * message-passing network over each node's NeiTab ring (input layer 9 -> 64,
  * three layers h' = ReLU(Ws h + Wn mean_ring(h) + b) of width 64, a linear
- * head) predicts a correction s_out * out to that guess at wet nodes off the
- * elevation boundary, from the normalised eta^k, ETAS, u, v, depth, wet
+ * head) predicts a correction s_out * out to that guess at wet nodes off
+ * the elevation boundary, from the normalised eta^k, ETAS, u, v, depth, wet
  * flag, p - p_background and wind stress.  BF16 weights and activations,
  * FP32 accumulation on the tensor cores.  Parameters are a flat FP32 array
  * of adc_predictor_nparams() values: W_in[64][16] (inputs 0-8, column 9 the
@@ -356,15 +356,15 @@ int adc_get_scalars(adc_ctx *ctx, adc_scalars_t *out);
  * the prediction when its initial residual is the smaller one
  * (adc_warm_start_stats counts the choices).  adc_predictor_train(on, lr)
  * trains the network on the device after every step's solve on that
- * step's (features, solved ETAS), Adam on the MSE of the normalised
- * correction; without ADC_LEARNED_START the steps keep the reference guess,
+ * step's (features, solved ETAS), Adam on the Huber loss (threshold 3)
+ * of the normalised correction; without ADC_LEARNED_START the steps keep the reference guess,
  * so the pairs are the plain solver's.  The predictor is not part of the
  * hotstart file. */
 int adc_predictor_nparams(void);
 int adc_set_predictor(adc_ctx *ctx, const float *params, int nparams);
 int adc_get_predictor(adc_ctx *ctx, float *params, int nparams);
 int adc_predictor_train(adc_ctx *ctx, int on, float lr);
-/* loss: mean squared normalised error of the last training step; adam_steps:
+/* loss: mean Huber loss of the normalised error of the last training step; adam_steps:
  * updates so far. */
 int adc_predictor_stats(adc_ctx *ctx, double *loss, long long *adam_steps);
 /* Runs the forward pass on the current device state; guess (NP doubles)
