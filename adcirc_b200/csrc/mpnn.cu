@@ -60,6 +60,8 @@ struct Mpnn {
   __nv_bfloat16 *wbf;             // BF16 copies: W_in, then per layer [Ws | Wn] rows of 128
   __nv_bfloat16 *x;               // [n][16]
   __nv_bfloat16 *h[kL + 1];       // [n][64]
+  __nv_bfloat16 *mean[kL];        // ring means of h[0..kL-1], [n][64]
+  __nv_bfloat16 *adz;             // backward messages, [n][64]
   float *dz[2];                   // [n][64]
   double *ref;                    // ETAS_ref, [n]
   double *pred;                   // ETAS guess, [n]
@@ -68,6 +70,7 @@ struct Mpnn {
   float *inv_deg;                 // 1 / |N(i)|
   float *part;                    // per-CTA weight-gradient partials
   int part_ctas;
+  int dense_ctas[3];              // persistent grid of k_mp_dense<0/1/2>
   double *loss_part;              // per-block loss partials
   double *stats;                  // [0] loss of the last step, [1] Adam steps
   const double *tgt;              // training target (the solved ETAS when null)
@@ -197,21 +200,19 @@ __device__ __forceinline__ void ring_chunk_h(const MpArgs &a, const TileRing<W> 
   const int p0 = s.ptr[r], deg = s.ptr[r + 1] - p0, o = p0 - s.ptr[0];
 #pragma unroll
   for (int e = 0; e < 8; ++e) acc[e] = 0.f;
-  uint4 v[kRing];
+  for (int q0 = 0; q0 < deg; q0 += kRing) {
+    uint4 v[kRing];
 #pragma unroll
-  for (int q = 0; q < kRing; ++q) {
-    v[q] = make_uint4(0u, 0u, 0u, 0u);
-    if (q < deg) {
-      const int j = fit ? s.idx[o + q] : a.nb_idx[p0 + q];
-      v[q] = reinterpret_cast<const uint4 *>(h + (size_t)j * kH)[ch];
+    for (int q = 0; q < kRing; ++q) {
+      v[q] = make_uint4(0u, 0u, 0u, 0u);
+      if (q0 + q < deg) {
+        const int j = fit ? s.idx[o + q0 + q] : a.nb_idx[p0 + q0 + q];
+        v[q] = reinterpret_cast<const uint4 *>(h + (size_t)j * kH)[ch];
+      }
     }
-  }
 #pragma unroll
-  for (int q = 0; q < kRing; ++q)
-    if (q < deg) add_bf16x8(acc, v[q]);
-  for (int q = kRing; q < deg; ++q) {
-    const int j = fit ? s.idx[o + q] : a.nb_idx[p0 + q];
-    add_bf16x8(acc, reinterpret_cast<const uint4 *>(h + (size_t)j * kH)[ch]);
+    for (int q = 0; q < kRing; ++q)
+      if (q0 + q < deg) add_bf16x8(acc, v[q]);
   }
 }
 
@@ -280,30 +281,76 @@ __global__ void k_mp_features(adc_ctx c, Mpnn m) {
   m.ref[i] = ref;
 }
 
+// ------------------------------------------------------ ring aggregation
+// The messages of one tile of 64 nodes per CTA (8 lanes per node):
+// mean_i = BF16((1/|N(i)|) sum_{j in N(i)} h_j).
+__global__ void __launch_bounds__(kMpThreads, 8) k_mp_aggr(MpArgs a, const __nv_bfloat16 *h,
+                                                         __nv_bfloat16 *mean) {
+  griddep_wait();
+  __shared__ TileRing<false> ring;
+  const int node0 = blockIdx.x * kTile;
+  const bool fit = stage_ring<false>(a, node0, ring);
+  const int ch = threadIdx.x & 7;
+  for (int row = threadIdx.x >> 3; row < kTile; row += kMpThreads / 8) {
+    const int i = node0 + row;
+    if (i >= a.n) break;
+    float agg[8];
+    ring_chunk_h(a, ring, fit, h, row, ch, agg);
+    const float sc = a.inv_deg[i];
+#pragma unroll
+    for (int e = 0; e < 8; ++e) agg[e] *= sc;
+    reinterpret_cast<uint4 *>(mean + (size_t)i * kH)[ch] = pack_bf16x8(agg);
+  }
+}
+
+// The backward messages: adz_i = BF16(sum_{j in N(i)} dz_j / |N(j)|).
+__global__ void __launch_bounds__(kMpThreads, 8) k_mp_aggr_dz(MpArgs a, const float *dz,
+                                                            __nv_bfloat16 *adz) {
+  griddep_wait();
+  __shared__ TileRing<true> ring;
+  const int node0 = blockIdx.x * kTile;
+  const bool fit = stage_ring<true>(a, node0, ring);
+  const int ch = threadIdx.x & 7;
+  for (int row = threadIdx.x >> 3; row < kTile; row += kMpThreads / 8) {
+    const int i = node0 + row;
+    if (i >= a.n) break;
+    float agg[8];
+    ring_chunk_dz(a, ring, fit, dz, row, ch, agg);
+    reinterpret_cast<uint4 *>(adz + (size_t)i * kH)[ch] = pack_bf16x8(agg);
+  }
+}
+
 // ----------------------------------------------------------- dense passes
-// mode 0: h0 = ReLU(W_in x)                      (K = 16)
-// mode 1: h_l = ReLU([h_l-1 | mean_N h_l-1] [Ws; Wn]^T + b)     (K = 128)
-// mode 2: dz_l-1 = ([dz_l | sum_N dz_j / deg_j] [Ws; Wn]) * (h_l-1 > 0)
+// mode 0: h0 = ReLU(W_in x)                                  (K = 16)
+// mode 1: h_l = ReLU([h_l-1 | mean_l-1] [Ws; Wn]^T + b)        (K = 128)
+// mode 2: dz_l-1 = ([dz_l | adz_l] [Ws; Wn]) * (h_l-1 > 0)
+// Persistent CTAs over tiles of 64 nodes: the weights are staged once per
+// CTA; each thread loads its share of the next tile's rows into registers
+// while the current tile's GEMM and store run.  Mode 0 and 1 stage the
+// output tile in shared memory and write whole rows.
 template <int MODE>
 __global__ void __launch_bounds__(kMpThreads) k_mp_dense(MpArgs a, int layer,
                                                           const __nv_bfloat16 *hin,
+                                                          const __nv_bfloat16 *msg,
                                                           const float *dzin,
-                                                          __nv_bfloat16 *hout, float *dzout) {
+                                                          __nv_bfloat16 *hout, float *dzout,
+                                                          int ntiles) {
   griddep_wait();
   constexpr int K = MODE == 0 ? kF : 2 * kH;
   constexpr int SA = MODE == 0 ? kSX : kSA;
+  constexpr int NR = MODE == 0 ? 1 : 8;          // 16-byte row pieces per thread
+  constexpr int SO = kH + 8;                     // output tile row stride
   __shared__ __align__(16) __nv_bfloat16 sA[kTile * SA];
   __shared__ __align__(16) __nv_bfloat16 sB[kH * SA];
-  __shared__ TileRing<MODE == 2> ring;
+  __shared__ __align__(16) __nv_bfloat16 sO[MODE <= 1 ? kTile * SO : 8];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int node0 = blockIdx.x * kTile;
   // B^T[64 x K]
-  if (MODE == 0) {
+  if constexpr (MODE == 0) {
     for (int q = threadIdx.x; q < kH * kF / 8; q += blockDim.x)
       reinterpret_cast<uint4 *>(sB + (q / 2) * SA)[q & 1] = reinterpret_cast<const uint4 *>(a.wbf)[q];
   } else {
     const __nv_bfloat16 *w = a.wbf + kH * kF + (size_t)layer * kH * 2 * kH;   // [64][128] = [Ws | Wn]
-    if (MODE == 1) {
+    if constexpr (MODE == 1) {
       for (int q = threadIdx.x; q < kH * 2 * kH / 8; q += blockDim.x)
         reinterpret_cast<uint4 *>(sB + (q / 16) * SA)[q & 15] = reinterpret_cast<const uint4 *>(w)[q];
     } else {
@@ -314,79 +361,87 @@ __global__ void __launch_bounds__(kMpThreads) k_mp_dense(MpArgs a, int layer,
       }
     }
   }
-  // A rows: [x] (mode 0), [h | mean_N h] (mode 1), [dz | sum_N dz_j / deg_j]
-  if constexpr (MODE == 0) {
-    for (int q = threadIdx.x; q < kTile * 2; q += blockDim.x) {
-      const int row = q >> 1, i = node0 + row;
-      uint4 v = make_uint4(0u, 0u, 0u, 0u);
-      if (i < a.n) v = reinterpret_cast<const uint4 *>(hin + (size_t)i * kF)[q & 1];
-      reinterpret_cast<uint4 *>(sA + row * SA)[q & 1] = v;
-    }
-  } else {
-    const bool fit = stage_ring<MODE == 2>(a, node0, ring);
-    const int ch = threadIdx.x & 7;
-    for (int row = threadIdx.x >> 3; row < kTile; row += kMpThreads / 8) {
-      const int i = node0 + row;
-      float self[8], agg[8];
+  // Thread's pieces: mode 0, row tid/2, piece tid&1 of the 32-byte x row;
+  // modes 1-2, rows tid/16 + 8k (k < 8), piece tid&15 of [self | message].
+  const int piece = MODE == 0 ? (threadIdx.x & 1) : (threadIdx.x & 15);
+  const int row0 = MODE == 0 ? (threadIdx.x >> 1) : (threadIdx.x >> 4);
+  auto load = [&](int tile, uint4 (&r)[NR]) {
 #pragma unroll
-      for (int e = 0; e < 8; ++e) self[e] = agg[e] = 0.f;
-      if (i < a.n) {
-        if constexpr (MODE == 1) {
-          unpack_bf16x8(self, reinterpret_cast<const uint4 *>(hin + (size_t)i * kH)[ch]);
-          ring_chunk_h(a, ring, fit, hin, row, ch, agg);
-          const float sc = a.inv_deg[i];
-#pragma unroll
-          for (int e = 0; e < 8; ++e) agg[e] *= sc;
-        } else {
-          const float4 *d = reinterpret_cast<const float4 *>(dzin + (size_t)i * kH) + 2 * ch;
-          const float4 d0 = d[0], d1 = d[1];
-          self[0] = d0.x; self[1] = d0.y; self[2] = d0.z; self[3] = d0.w;
-          self[4] = d1.x; self[5] = d1.y; self[6] = d1.z; self[7] = d1.w;
-          ring_chunk_dz(a, ring, fit, dzin, row, ch, agg);
-        }
+    for (int k = 0; k < NR; ++k) {
+      const int i = tile * kTile + row0 + 8 * k;
+      r[k] = make_uint4(0u, 0u, 0u, 0u);
+      if (i >= a.n) continue;
+      if constexpr (MODE == 0) {
+        r[k] = reinterpret_cast<const uint4 *>(hin + (size_t)i * kF)[piece];
+      } else if (piece >= 8) {
+        r[k] = reinterpret_cast<const uint4 *>(msg + (size_t)i * kH)[piece - 8];
+      } else if constexpr (MODE == 1) {
+        r[k] = reinterpret_cast<const uint4 *>(hin + (size_t)i * kH)[piece];
+      } else {
+        const float4 *d = reinterpret_cast<const float4 *>(dzin + (size_t)i * kH) + 2 * piece;
+        const float4 d0 = d[0], d1 = d[1];
+        r[k] = make_uint4(pack_bf16(d0.x, d0.y), pack_bf16(d0.z, d0.w), pack_bf16(d1.x, d1.y),
+                          pack_bf16(d1.z, d1.w));
       }
-      reinterpret_cast<uint4 *>(sA + row * SA)[ch] = pack_bf16x8(self);
-      reinterpret_cast<uint4 *>(sA + row * SA + kH)[ch] = pack_bf16x8(agg);
     }
-  }
-  __syncthreads();
-  float acc[8][4];
-#pragma unroll
-  for (int nt = 0; nt < 8; ++nt) acc[nt][0] = acc[nt][1] = acc[nt][2] = acc[nt][3] = 0.f;
-  warp_gemm_16x64<K>(sA + warp * 16 * SA, SA, sB, SA, acc);
+  };
+  uint4 r[NR];
+  int tile = blockIdx.x;
+  if (tile < ntiles) load(tile, r);
   const int g = lane >> 2, t = lane & 3;
   const float *bias = a.par + kOffLayer + layer * kLayerSz + 2 * kH * kH;
+  for (; tile < ntiles; tile += gridDim.x) {
+    const int node0 = tile * kTile;
+    __syncthreads();                     // the previous tile is done with sA and sO
 #pragma unroll
-  for (int nt = 0; nt < 8; ++nt)
+    for (int k = 0; k < NR; ++k) reinterpret_cast<uint4 *>(sA + (row0 + 8 * k) * SA)[piece] = r[k];
+    __syncthreads();
+    if (tile + (int)gridDim.x < ntiles) load(tile + gridDim.x, r);
+    float acc[8][4];
 #pragma unroll
-    for (int hlf = 0; hlf < 2; ++hlf) {
-      const int row = warp * 16 + g + 8 * hlf, i = node0 + row;
-      const int col = nt * 8 + 2 * t;
-      if (i >= a.n) continue;
-      float v0 = acc[nt][2 * hlf], v1 = acc[nt][2 * hlf + 1];
-      if (MODE == 1) {
-        v0 += bias[col];
-        v1 += bias[col + 1];
+    for (int nt = 0; nt < 8; ++nt) acc[nt][0] = acc[nt][1] = acc[nt][2] = acc[nt][3] = 0.f;
+    warp_gemm_16x64<K>(sA + warp * 16 * SA, SA, sB, SA, acc);
+#pragma unroll
+    for (int nt = 0; nt < 8; ++nt)
+#pragma unroll
+      for (int hlf = 0; hlf < 2; ++hlf) {
+        const int row = warp * 16 + g + 8 * hlf, i = node0 + row;
+        const int col = nt * 8 + 2 * t;
+        float v0 = acc[nt][2 * hlf], v1 = acc[nt][2 * hlf + 1];
+        if constexpr (MODE == 1) {
+          v0 += bias[col];
+          v1 += bias[col + 1];
+        }
+        if constexpr (MODE <= 1) {
+          reinterpret_cast<unsigned *>(sO + row * SO + col)[0] = pack_bf16(fmaxf(v0, 0.f), fmaxf(v1, 0.f));
+        } else {
+          if (i >= a.n) continue;
+          const float2 h = __bfloat1622float2(
+              *reinterpret_cast<const __nv_bfloat162 *>(hin + (size_t)i * kH + col));
+          reinterpret_cast<float2 *>(dzout + (size_t)i * kH + col)[0] =
+              make_float2(h.x > 0.f ? v0 : 0.f, h.y > 0.f ? v1 : 0.f);
+        }
       }
-      if (MODE <= 1) {
-        reinterpret_cast<unsigned *>(hout + (size_t)i * kH + col)[0] =
-            pack_bf16(fmaxf(v0, 0.f), fmaxf(v1, 0.f));
-      } else {
-        const float2 h = __bfloat1622float2(
-            *reinterpret_cast<const __nv_bfloat162 *>(hin + (size_t)i * kH + col));
-        reinterpret_cast<float2 *>(dzout + (size_t)i * kH + col)[0] =
-            make_float2(h.x > 0.f ? v0 : 0.f, h.y > 0.f ? v1 : 0.f);
+    if constexpr (MODE <= 1) {
+      __syncthreads();
+      for (int q = threadIdx.x; q < kTile * 8; q += blockDim.x) {
+        const int row = q >> 3, i = node0 + row;
+        if (i < a.n)
+          reinterpret_cast<uint4 *>(hout + (size_t)i * kH)[q & 7] =
+              reinterpret_cast<const uint4 *>(sO + row * SO)[q & 7];
       }
     }
+  }
 }
 
 // Weight gradient partial of one CTA over its node chunks:
-// P[o][k] = sum_i dz[i][o] A[i][k], A = [h | mean_N h | 1] (K = 144) or
-// [x] (K = 16, whose column 9 is the constant 1).  The mma's M is o (64),
-// its N is k and its reduction runs over nodes.
+// P[o][k] = sum_i dz[i][o] A[i][k], A = [h | mean | 1] (K = 144) or [x]
+// (K = 16, whose column 9 is the constant 1).  The mma's M is o (64), its
+// N is k and its reduction runs over nodes.
 template <int MODE>
 __global__ void __launch_bounds__(kMpThreads) k_mp_wgrad(MpArgs a, const float *dz,
-                                                          const __nv_bfloat16 *hin, float *part,
+                                                          const __nv_bfloat16 *hin,
+                                                          const __nv_bfloat16 *msg, float *part,
                                                           int chunks_per_cta) {
   griddep_wait();
   constexpr int K = MODE == 0 ? kF : 2 * kH + 16;
@@ -398,12 +453,10 @@ __global__ void __launch_bounds__(kMpThreads) k_mp_wgrad(MpArgs a, const float *
   float acc[NT][4];
 #pragma unroll
   for (int nt = 0; nt < NT; ++nt) acc[nt][0] = acc[nt][1] = acc[nt][2] = acc[nt][3] = 0.f;
-  __shared__ TileRing<false> ring;
   for (int chunk = 0; chunk < chunks_per_cta; ++chunk) {
     const int node0 = (blockIdx.x * chunks_per_cta + chunk) * kTile;
     if (node0 >= a.n) break;
     __syncthreads();
-    const bool fit = MODE == 1 ? stage_ring<false>(a, node0, ring) : true;
     const int ch = threadIdx.x & 7;
     for (int r = threadIdx.x >> 3; r < kTile; r += kMpThreads / 8) {
       const int i = node0 + r;
@@ -419,15 +472,12 @@ __global__ void __launch_bounds__(kMpThreads) k_mp_wgrad(MpArgs a, const float *
           if (ch < 2) unpack_bf16x8(self, reinterpret_cast<const uint4 *>(hin + (size_t)i * kF)[ch]);
         } else {
           unpack_bf16x8(self, reinterpret_cast<const uint4 *>(hin + (size_t)i * kH)[ch]);
-          ring_chunk_h(a, ring, fit, hin, r, ch, agg);
-          const float sc = a.inv_deg[i];
-#pragma unroll
-          for (int e = 0; e < 8; ++e) agg[e] *= sc;
+          unpack_bf16x8(agg, reinterpret_cast<const uint4 *>(msg + (size_t)i * kH)[ch]);
         }
       }
 #pragma unroll
       for (int e = 0; e < 8; ++e) sDt[(8 * ch + e) * SN + r] = __float2bfloat16_rn(d[e]);
-      if (MODE == 0) {
+      if constexpr (MODE == 0) {
         if (ch < 2)
 #pragma unroll
           for (int e = 0; e < 8; ++e) sAt[(8 * ch + e) * SN + r] = __float2bfloat16_rn(self[e]);
@@ -495,23 +545,36 @@ __global__ void k_mp_wreduce(const float *part, int nctas, int mode, int layer, 
 // out_i = w_out . h3_i + b_out; the guess at wet interior nodes, the
 // reference elsewhere.  With `loss`, also dL/dout_i (Huber loss of the
 // normalised correction over wet interior nodes, target from the solved
-// ETAS) and the block partials of the loss.
-__global__ void k_mp_head(adc_ctx c, Mpnn m, int mode) {
+// ETAS) and the block partials of the loss.  8 lanes per node, 8 channels
+// each.
+constexpr int kHeadThreads = 256;
+
+__host__ __device__ constexpr int head_blocks(int n) {
+  return (int)(((long long)n * 8 + kHeadThreads - 1) / kHeadThreads);
+}
+
+__global__ void __launch_bounds__(kHeadThreads) k_mp_head(adc_ctx c, Mpnn m, int mode) {
   griddep_wait();
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-  const int i = warp;   // one warp per node: 64 channels as 32 pairs
+  const int q = blockIdx.x * blockDim.x + threadIdx.x, i = q >> 3, ch = q & 7;
+  float hv[8];
+#pragma unroll
+  for (int e = 0; e < 8; ++e) hv[e] = 0.f;
+  if (i < m.n) unpack_bf16x8(hv, reinterpret_cast<const uint4 *>(m.h[kL] + (size_t)i * kH)[ch]);
+  const float *w = m.par + kOffWout + 8 * ch;
+  float s = 0.f;
+#pragma unroll
+  for (int e = 0; e < 8; ++e) s += hv[e] * w[e];
+  s += __shfl_xor_sync(0xffffffffu, s, 4);
+  s += __shfl_xor_sync(0xffffffffu, s, 2);
+  s += __shfl_xor_sync(0xffffffffu, s, 1);
   double l = 0.0;
-  if (i < m.n) {
-    const float2 h = __bfloat1622float2(reinterpret_cast<const __nv_bfloat162 *>(m.h[kL] + (size_t)i * kH)[lane]);
-    const float *w = m.par + kOffWout;
-    float s = h.x * w[2 * lane] + h.y * w[2 * lane + 1];
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if (i < m.n && ch == 0) {
     const float out = s + m.par[kOffBout];
     const double s_out = (double)m.par[kOffNorm + 2 * kNF];
     const bool use = c.nodecode[i] == 1 && c.is_nbd[i] < 0;
     if (mode == 0) {
-      if (lane == 0) m.pred[i] = use ? m.ref[i] + s_out * out : m.ref[i];
-    } else if (lane == 0) {
+      m.pred[i] = use ? m.ref[i] + s_out * out : m.ref[i];
+    } else {
       float d = 0.f;
       if (use) {
         const double sol = m.tgt ? m.tgt[i] : c.etas[i];
@@ -524,12 +587,13 @@ __global__ void k_mp_head(adc_ctx c, Mpnn m, int mode) {
     }
   }
   if (mode == 1) {
-    __shared__ double sh[32];
-    if (lane == 0) sh[threadIdx.x >> 5] = l;
+    __shared__ double sh[kHeadThreads / 32];
+    l = warp_sum(l);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = l;
     __syncthreads();
     if (threadIdx.x == 0) {
       double t = 0.0;
-      for (int k = 0; k < (int)(blockDim.x >> 5); ++k) t += sh[k];
+      for (int k = 0; k < kHeadThreads / 32; ++k) t += sh[k];
       m.loss_part[blockIdx.x] = t;
     }
   }
@@ -537,16 +601,21 @@ __global__ void k_mp_head(adc_ctx c, Mpnn m, int mode) {
 
 // dz3 = (dL/dout w_out) * (h3 > 0) with dL/dout = 2 clamp(e) / n (the loss
 // is the mean over all nodes of the Huber loss of e, e = 0 where the guess
-// is not used); one warp per node, lanes over channel pairs.
-__global__ void k_mp_head_bwd(Mpnn m) {
+// is not used); 8 lanes per node.
+__global__ void __launch_bounds__(kHeadThreads) k_mp_head_bwd(Mpnn m) {
   griddep_wait();
-  const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  const int q = blockIdx.x * blockDim.x + threadIdx.x, i = q >> 3, ch = q & 7;
   if (i >= m.n) return;
   const float d = m.dout[i] * (2.f / (float)m.n);
-  const float2 h = __bfloat1622float2(reinterpret_cast<const __nv_bfloat162 *>(m.h[kL] + (size_t)i * kH)[lane]);
-  const float *w = m.par + kOffWout;
-  reinterpret_cast<float2 *>(m.dz[0] + (size_t)i * kH)[lane] =
-      make_float2(h.x > 0.f ? d * w[2 * lane] : 0.f, h.y > 0.f ? d * w[2 * lane + 1] : 0.f);
+  float hv[8];
+  unpack_bf16x8(hv, reinterpret_cast<const uint4 *>(m.h[kL] + (size_t)i * kH)[ch]);
+  const float *w = m.par + kOffWout + 8 * ch;
+  float o[8];
+#pragma unroll
+  for (int e = 0; e < 8; ++e) o[e] = hv[e] > 0.f ? d * w[e] : 0.f;
+  float4 *dst = reinterpret_cast<float4 *>(m.dz[0] + (size_t)i * kH) + 2 * ch;
+  dst[0] = make_float4(o[0], o[1], o[2], o[3]);
+  dst[1] = make_float4(o[4], o[5], o[6], o[7]);
 }
 
 // Head gradient partials per CTA (its nodes, warp-strided, lanes over
@@ -639,22 +708,26 @@ static MpArgs mp_args(const Mpnn &m) {
   return MpArgs{m.n, m.wbf, m.par, m.nb_ptr, m.nb_idx, m.inv_deg};
 }
 
-// Forward pass: features, input layer, three message-passing layers, head
-// (the guess in m.pred).
+// Forward pass: features, input layer, three message-passing layers (each
+// a ring aggregation and a dense pass), head (the guess in m.pred).
 int launch_predictor_forward(adc_ctx *c) {
   Mpnn *mp = c->mp;
   if (!mp || !(mp->learned || mp->train)) return ADC_OK;
   const Mpnn &m = *mp;
   const MpArgs a = mp_args(m);
   const int tiles = (m.n + kTile - 1) / kTile;
+  const __nv_bfloat16 *none = nullptr;
   launch_k(k_mp_features, nblk(m.n), kThreads, c->stream, *c, m);
-  launch_k(k_mp_dense<0>, tiles, kMpThreads, c->stream, a, 0, (const __nv_bfloat16 *)m.x,
-           (const float *)nullptr, m.h[0], (float *)nullptr);
-  for (int l = 0; l < kL; ++l)
-    launch_k(k_mp_dense<1>, tiles, kMpThreads, c->stream, a, l, (const __nv_bfloat16 *)m.h[l],
-             (const float *)nullptr, m.h[l + 1], (float *)nullptr);
-  launch_k(k_mp_head, (int)(((long long)m.n * 32 + 255) / 256), 256, c->stream, *c, m, 0);
-  c->launches += 3 + kL;
+  launch_k(k_mp_dense<0>, std::min(tiles, m.dense_ctas[0]), kMpThreads, c->stream, a, 0,
+           (const __nv_bfloat16 *)m.x, none, (const float *)nullptr, m.h[0], (float *)nullptr, tiles);
+  for (int l = 0; l < kL; ++l) {
+    launch_k(k_mp_aggr, tiles, kMpThreads, c->stream, a, (const __nv_bfloat16 *)m.h[l], m.mean[l]);
+    launch_k(k_mp_dense<1>, std::min(tiles, m.dense_ctas[1]), kMpThreads, c->stream, a, l,
+             (const __nv_bfloat16 *)m.h[l], (const __nv_bfloat16 *)m.mean[l], (const float *)nullptr,
+             m.h[l + 1], (float *)nullptr, tiles);
+  }
+  launch_k(k_mp_head, head_blocks(m.n), kHeadThreads, c->stream, *c, m, 0);
+  c->launches += 3 + 2 * kL;
   return ADC_OK;
 }
 
@@ -664,9 +737,9 @@ static int launch_predictor_backward(adc_ctx *c) {
   const Mpnn &m = *c->mp;
   const MpArgs a = mp_args(m);
   const int tiles = (m.n + kTile - 1) / kTile;
-  const int hb = (int)(((long long)m.n * 32 + 255) / 256);
-  launch_k(k_mp_head, hb, 256, c->stream, *c, m, 1);
-  launch_k(k_mp_head_bwd, hb, 256, c->stream, m);
+  const int hb = head_blocks(m.n);
+  launch_k(k_mp_head, hb, kHeadThreads, c->stream, *c, m, 1);
+  launch_k(k_mp_head_bwd, hb, kHeadThreads, c->stream, m);
   const int npc = (m.n + m.part_ctas - 1) / m.part_ctas;
   launch_k(k_mp_head_grad, m.part_ctas, kMpThreads, c->stream, m, npc);
   launch_k(k_mp_head_reduce, 1, 1024, c->stream, m, m.part_ctas, hb);
@@ -675,18 +748,21 @@ static int launch_predictor_backward(adc_ctx *c) {
   for (int l = kL - 1; l >= 0; --l) {
     // dz[cur] holds dz of layer l+1 (h_{l+1} = ReLU(z_{l+1}))
     launch_k(k_mp_wgrad<1>, m.part_ctas, kMpThreads, c->stream, a, (const float *)m.dz[cur],
-             (const __nv_bfloat16 *)m.h[l], m.part, chunks);
+             (const __nv_bfloat16 *)m.h[l], (const __nv_bfloat16 *)m.mean[l], m.part, chunks);
     launch_k(k_mp_wreduce, (kH * (2 * kH + 16) + 255) / 256, 256, c->stream,
              (const float *)m.part, m.part_ctas, 1, l, m.grad);
-    launch_k(k_mp_dense<2>, tiles, kMpThreads, c->stream, a, l, (const __nv_bfloat16 *)m.h[l],
-             (const float *)m.dz[cur], (__nv_bfloat16 *)nullptr, m.dz[cur ^ 1]);
+    launch_k(k_mp_aggr_dz, tiles, kMpThreads, c->stream, a, (const float *)m.dz[cur], m.adz);
+    launch_k(k_mp_dense<2>, std::min(tiles, m.dense_ctas[2]), kMpThreads, c->stream, a, l,
+             (const __nv_bfloat16 *)m.h[l], (const __nv_bfloat16 *)m.adz, (const float *)m.dz[cur],
+             (__nv_bfloat16 *)nullptr, m.dz[cur ^ 1], tiles);
     cur ^= 1;
   }
+  const __nv_bfloat16 *none = nullptr;
   launch_k(k_mp_wgrad<0>, m.part_ctas, kMpThreads, c->stream, a, (const float *)m.dz[cur],
-           (const __nv_bfloat16 *)m.x, m.part, chunks);
+           (const __nv_bfloat16 *)m.x, none, m.part, chunks);
   launch_k(k_mp_wreduce, (kH * kF + 255) / 256, 256, c->stream, (const float *)m.part,
            m.part_ctas, 0, 0, m.grad);
-  c->launches += 4 + 3 * kL + 2;
+  c->launches += 4 + 4 * kL + 2;
   return ADC_OK;
 }
 
@@ -729,6 +805,15 @@ static int mp_alloc(adc_ctx *c) {
   m->n = n;
   m->lr = 1e-3f;
   m->part_ctas = 4 * 148;
+  {
+    int dev = 0, sms = 148, per[3] = {1, 1, 1};
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per[0], k_mp_dense<0>, kMpThreads, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per[1], k_mp_dense<1>, kMpThreads, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per[2], k_mp_dense<2>, kMpThreads, 0);
+    for (int k = 0; k < 3; ++k) m->dense_ctas[k] = std::max(1, per[k]) * sms;
+  }
   auto al = [&](auto **p, size_t cnt) -> int {
     cudaError_t e = cudaMalloc((void **)p, std::max<size_t>(cnt, 1) * sizeof(**p));
     if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc (predictor)");
@@ -740,11 +825,13 @@ static int mp_alloc(adc_ctx *c) {
   rc |= al(&m->wbf, (size_t)kH * kF + (size_t)kL * kH * 2 * kH);
   rc |= al(&m->x, (size_t)n * kF);
   for (int l = 0; l <= kL; ++l) rc |= al(&m->h[l], (size_t)n * kH);
+  for (int l = 0; l < kL; ++l) rc |= al(&m->mean[l], (size_t)n * kH);
+  rc |= al(&m->adz, (size_t)n * kH);
   rc |= al(&m->dz[0], (size_t)n * kH); rc |= al(&m->dz[1], (size_t)n * kH);
   rc |= al(&m->ref, n); rc |= al(&m->pred, n); rc |= al(&m->dout, n);
   rc |= al(&m->nb_ptr, n + 1); rc |= al(&m->nb_idx, idx.size()); rc |= al(&m->inv_deg, n);
   rc |= al(&m->part, (size_t)m->part_ctas * kH * (2 * kH + 16));
-  rc |= al(&m->loss_part, (size_t)((n * 32LL + 255) / 256) + 1);
+  rc |= al(&m->loss_part, (size_t)head_blocks(n) + 1);
   rc |= al(&m->stats, kNStats);
   if (rc) return ADC_ERR_NOMEM;
   ADC_CUDA(cudaMemcpy(m->nb_ptr, ptr.data(), (n + 1) * sizeof(int), cudaMemcpyHostToDevice));
@@ -766,7 +853,7 @@ void mp_free(adc_ctx *c) {
   Mpnn *m = c->mp;
   if (!m) return;
   void *ptrs[] = {m->par, m->grad, m->m1, m->m2, m->wbf, m->x, m->h[0], m->h[1], m->h[2], m->h[3],
-                  m->dz[0], m->dz[1], m->ref, m->pred, m->dout, m->nb_ptr, m->nb_idx, m->inv_deg,
+                  m->mean[0], m->mean[1], m->mean[2], m->adz, m->dz[0], m->dz[1], m->ref, m->pred, m->dout, m->nb_ptr, m->nb_idx, m->inv_deg,
                   m->part, m->loss_part, m->stats};
   for (void *p : ptrs)
     if (p) cudaFree(p);
