@@ -94,6 +94,36 @@ class AdcScalars(C.Structure):
                 ("rparm2", C.c_double), ("vortex_wtratio", C.c_double)]
 
 
+class AdcOutputSpec(C.Structure):
+    _fields_ = [("nout", C.c_int), ("nspool", C.c_int), ("touts", C.c_double), ("toutf", C.c_double)]
+
+
+_F15_INTS = ("nfover nabout nscreen ihot ics im nolibf nolifa nolica nolicat nwp ncor ntip nws nramp "
+             "nodedrymin nodewetmin storm_number irefyr irefmo irefday irefhr ntif nbfr nffr nfreq "
+             "nstae nstav nstac nstam nhainc nhase nhasv nhage nhagv nhstar nhsinc ititer isldia "
+             "itmax has_slim has_wind_drag_limit").split()
+_F15_REALS = ("bladj g tau0 tau0_min tau0_max dtdp statim reftim rnday dramp dramp_extflux "
+              "flux_settling_time dramp_intflux dramp_elev dramp_tip dramp_mete dramp_wrad "
+              "dunramp_mete a00 b00 c00 h0 velmin slam0 sfea0 tau cf hbreak ftheta fgamma eslm eslc "
+              "cori anginn thas thaf fmv convcr slim wind_drag_limit").split()
+
+
+class AdcFort15(C.Structure):
+    """adc_fort15_t (include/adcgpu.h)."""
+    _fields_ = ([("rundes", C.c_char * 88), ("runid", C.c_char * 88)] +
+                [(n, C.c_int) for n in _F15_INTS] + [(n, C.c_double) for n in _F15_REALS] +
+                [(n, AdcOutputSpec) for n in ("oute", "outv", "outc", "outm", "outge", "outgv",
+                                              "outgc", "outgw")])
+
+
+class AdcFort15Tables(C.Structure):
+    """adc_fort15_tables_t (include/adcgpu.h)."""
+    _fields_ = ([(n, dp_) for n in ("tpk amigt etrf fft facet amig ff face emo efa famig fff fface "
+                                    "qnam qnph enam enph hafreq haff haface xel yel xev yev xem "
+                                    "yem").split()] +
+                [(n, C.c_char_p) for n in ("tiptag", "bountag", "fbountag", "namefr")])
+
+
 _lib = None
 
 
@@ -135,6 +165,10 @@ def load():
         "adc_set_flux": (C.c_int, [vp, C.POINTER(AdcFlux)]),
         "adc_fort14_dims": (C.c_int, [C.c_char_p, ip_]),
         "adc_fort14_read": (C.c_int, [C.c_char_p, C.c_char_p, dp_, dp_, dp_, ip_, ip_, ip_, ip_, ip_, ip_]),
+        "adc_fort15_read": (C.c_int, [C.c_char_p, C.c_int, C.c_int, ip_, C.POINTER(AdcFort15),
+                                      C.POINTER(AdcFort15Tables)]),
+        "adc_fort15_write": (C.c_int, [C.c_char_p, C.POINTER(AdcFort15), C.c_int, C.c_int, ip_,
+                                       C.POINTER(AdcFort15Tables)]),
         "adc_fort14_write": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int, C.c_int, dp_, dp_, dp_, ip_,
                                        C.c_int, ip_, ip_, C.c_int, ip_, ip_, ip_]),
         "adc_fort6x_header": (C.c_int, [C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p, C.c_int,

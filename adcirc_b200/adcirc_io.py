@@ -1,9 +1,11 @@
 """ADCIRC text files at the edges of the hot path, through libadcgpu's host
-functions: fort.14 meshes (read14, mesh.F:319-581) and the full-domain
-ASCII outputs fort.63/fort.64 (globalio.F:544-643, 802-930, 1005-1085)."""
+functions: fort.14 meshes (read14, mesh.F:319-581), fort.15 model
+parameters (READ_INPUT, read_input.F:949-4566) and the full-domain ASCII
+outputs fort.63/fort.64 (globalio.F:544-643, 802-930, 1005-1085)."""
 from __future__ import annotations
 
 import ctypes as C
+import dataclasses
 import os
 
 import numpy as np
@@ -92,3 +94,109 @@ class Fort6x:
                                           ptr(b, dp_) if b is not None else None,
                                           ptr(nc, ip_) if nc is not None else None,
                                           float(alternate)), "adc_fort6x_append")
+
+
+# ---------------------------------------------------------------- fort.15
+_F15_TABLE_COUNTS = {
+    "ntif": ("tpk", "amigt", "etrf", "fft", "facet"),
+    "nbfr": ("amig", "ff", "face"),
+    "nffr": ("famig", "fff", "fface"),
+    "nfreq": ("hafreq", "haff", "haface"),
+}
+_F15_TAGS = {"ntif": "tiptag", "nbfr": "bountag", "nffr": "fbountag", "nfreq": "namefr"}
+
+
+@dataclasses.dataclass
+class Fort15:
+    """A fort.15 file's values: `p` holds every scalar record (an
+    adc_fort15_t), the other fields the tables, angles in radians where
+    read_input converts them (FACE, EFA, FFACE, QNPH, ENPH, FACET)."""
+    p: object
+    tiptag: list
+    bountag: list
+    fbountag: list
+    namefr: list
+    tables: dict      # name -> array: (NTIF,), (NBFR,), EMO/EFA (NBFR, NETA), QNAM... (NFFR, NVEL)
+
+    def __getattr__(self, name):
+        if name in ("p", "tables"):
+            raise AttributeError(name)
+        if name in self.tables:
+            return self.tables[name]
+        return getattr(self.p, name)
+
+
+def _f15_tables(counts: dict, neta: int, nvel: int):
+    """Zeroed tables for the given counts and the ctypes struct over them."""
+    tabs = {}
+    for cnt, names in _F15_TABLE_COUNTS.items():
+        for nm in names:
+            tabs[nm] = np.zeros(max(counts[cnt], 1))
+    nb, nf = max(counts["nbfr"], 1), max(counts["nffr"], 1)
+    for nm in ("emo", "efa"):
+        tabs[nm] = np.zeros((nb, max(neta, 1)), order="F")
+    for nm in ("qnam", "qnph", "enam", "enph"):
+        tabs[nm] = np.zeros((nf, max(nvel, 1)), order="F")
+    for nm, cnt in (("xel", "nstae"), ("yel", "nstae"), ("xev", "nstav"), ("yev", "nstav"),
+                    ("xem", "nstam"), ("yem", "nstam")):
+        tabs[nm] = np.zeros(max(counts[cnt], 1))
+    tags = {cnt: C.create_string_buffer(16 * max(counts[cnt], 1)) for cnt in _F15_TAGS}
+    t = _lib.AdcFort15Tables()
+    for nm, a in tabs.items():
+        setattr(t, nm, ptr(a, dp_))
+    for cnt, field in _F15_TAGS.items():
+        setattr(t, field, C.cast(tags[cnt], C.c_char_p))
+    return tabs, tags, t
+
+
+def read_fort15(path, neta: int, lbcodei) -> Fort15:
+    """Reads a fort.15 (adc_fort15_read).  neta: NETA of the mesh;
+    lbcodei: LBCODEI of the flux-boundary nodes in the reference's order
+    (a Case's arrays['lbcodei']), which places the flux records."""
+    lib = _lib.load()
+    p = os.fsencode(path)
+    lbc = np.ascontiguousarray(np.asarray(lbcodei, np.int32).ravel())
+    nvel = int(lbc.size)
+    o = _lib.AdcFort15()
+    _check(lib.adc_fort15_read(p, int(neta), nvel, ptr(lbc, ip_), C.byref(o), None), "adc_fort15_read")
+    counts = {k: int(getattr(o, k)) for k in ("ntif", "nbfr", "nffr", "nfreq", "nstae", "nstav", "nstam")}
+    tabs, tags, t = _f15_tables(counts, neta, nvel)
+    o = _lib.AdcFort15()
+    _check(lib.adc_fort15_read(p, int(neta), nvel, ptr(lbc, ip_), C.byref(o), C.byref(t)),
+           "adc_fort15_read")
+
+    def taglist(cnt):
+        raw = tags[cnt].raw
+        return [raw[16 * k:16 * k + 16].split(b"\0", 1)[0].decode(errors="replace")
+                for k in range(counts[cnt])]
+    for cnt, names in _F15_TABLE_COUNTS.items():
+        for nm in names:
+            tabs[nm] = tabs[nm][:counts[cnt]]
+    tabs["emo"], tabs["efa"] = (tabs[k][:counts["nbfr"], :neta] for k in ("emo", "efa"))
+    for k in ("qnam", "qnph", "enam", "enph"):
+        tabs[k] = tabs[k][:counts["nffr"], :nvel]
+    for k, cnt in (("xel", "nstae"), ("yel", "nstae"), ("xev", "nstav"), ("yev", "nstav"),
+                   ("xem", "nstam"), ("yem", "nstam")):
+        tabs[k] = tabs[k][:counts[cnt]]
+    return Fort15(o, taglist("ntif"), taglist("nbfr"), taglist("nffr"), taglist("nfreq"), tabs)
+
+
+def write_fort15(path, f: Fort15, neta: int, lbcodei) -> None:
+    """Writes `f` as a fort.15 (adc_fort15_write): read_fort15 of the file
+    gives back the same values."""
+    lib = _lib.load()
+    lbc = np.ascontiguousarray(np.asarray(lbcodei, np.int32).ravel())
+    nvel = int(lbc.size)
+    counts = {k: int(getattr(f.p, k)) for k in ("ntif", "nbfr", "nffr", "nfreq", "nstae", "nstav",
+                                                   "nstam")}
+    tabs, tags, t = _f15_tables(counts, neta, nvel)
+    for nm, a in f.tables.items():
+        a = np.asarray(a, np.float64)
+        if a.size:
+            tabs[nm][tuple(slice(0, s) for s in a.shape)] = a
+    for cnt, field in _F15_TAGS.items():
+        names = {"ntif": f.tiptag, "nbfr": f.bountag, "nffr": f.fbountag, "nfreq": f.namefr}[cnt]
+        buf = b"".join(n.encode()[:15].ljust(16, b"\0") for n in names)
+        C.memmove(tags[cnt], buf, min(len(buf), C.sizeof(tags[cnt])))
+    _check(lib.adc_fort15_write(os.fsencode(path), C.byref(f.p), int(neta), nvel, ptr(lbc, ip_),
+                                C.byref(t)), "adc_fort15_write")

@@ -346,7 +346,131 @@ def build_case(raw, params: dict, schedule: Schedule, tides, cf: float = 0.0025,
             A[k] = np.asfortranarray(v)
     sizes = dict(np=npn, ne=ne, mnei=mnei, neta=neta, nbfr=nbfr, nvel=nv, nvelme=nme,
                  neimax=neimax.value)
-    return Case(raw.name, dict(params), sizes, A, schedule, dict(raw.meta))
+    meta = dict(raw.meta)
+    meta["build"] = dict(cf=cf, tau0=tau0, eslm=eslm, cori=cori, anginn=anginn)
+    meta["raw"] = raw            # the mesh as built (write it with adcirc_io.write_fort14)
+    return Case(raw.name, dict(params), sizes, A, schedule, meta)
+
+
+# --------------------------------------------------------------------------
+# Cases from ADCIRC input files, and input files from cases
+# --------------------------------------------------------------------------
+
+def _raw_lbcodes(raw) -> np.ndarray:
+    """IBTYPE of every flux-boundary node of a RawMesh in fort.14 order:
+    the flux records of a fort.15 follow it (island closure nodes carry no
+    record)."""
+    if not raw.land_segments:
+        return np.zeros(0, np.int32)
+    return np.concatenate([np.full(len(nodes), t, np.int32) for t, nodes in raw.land_segments])
+
+
+def case_from_files(fort14, fort15, vortex: "Vortex | None" = None,
+                    prep: MeshPrep | None = None) -> Case:
+    """A Case from a fort.14 mesh and a fort.15 parameter file, with the
+    parameter derivations of the reference: IFNLFA/IFNLCT/IFNLCAT from
+    NOLIFA/NOLICA/NOLICAT (adcirc.F:287-290, 376-384), the friction flags
+    and FRIC = CF (or TAU when NOLIBF = 0) (nodalattr.F:1974-2001), the ramps
+    of NRAMP (read_input.F:2893-2955), periodic elevation constituents and,
+    with flux boundaries, the periodic flux constituents.  Runs this path
+    does not cover raise NotImplementedError: ICS = 2, NCOR = 1, tidal
+    potential, hot starts, TAU0 = -5, non-periodic flux (NFFR <= 0) and
+    NWS = 8 without a `vortex` (the fort.22 track is not read)."""
+    from . import adcirc_io
+    raw = adcirc_io.read_fort14(fort14)
+    neta = int(raw.open_nodes.size)
+    f = adcirc_io.read_fort15(fort15, neta, _raw_lbcodes(raw))
+    why = []
+    if f.ics != 1:
+        why.append("ICS = 2 (spherical coordinates)")
+    if f.ncor != 0:
+        why.append("NCOR = 1 (latitude-dependent Coriolis)")
+    if f.ntip != 0:
+        why.append("NTIP > 0 (tidal potential)")
+    if f.ihot != 0:
+        why.append("IHOT > 0 (use adc_hotstart_read)")
+    if f.tau0 == -5.0:
+        why.append("TAU0 = -5 (time-varying TAU0)")
+    if any(t in (2, 12, 22, 52, 32) for t, _ in raw.land_segments) and f.nffr <= 0:
+        why.append("NFFR <= 0 (non-periodic fort.20 flux)")
+    if abs(f.nws) == 8 and vortex is None:
+        why.append("NWS = 8 without a vortex track")
+    if why:
+        raise NotImplementedError(f"{fort15}: " + "; ".join(why))
+    params = default_params(
+        f.dtdp, g=f.g, a00=f.a00, b00=f.b00, c00=f.c00, h0=f.h0, slim=f.slim, convcr=f.convcr,
+        itmax=f.itmax, isldia=f.isldia, nolifa=f.nolifa, ifnlfa=int(f.nolifa != 0),
+        ifnlct=int(f.nolica != 0), ifnlcat=int(f.nolicat != 0),
+        iflinbf=int(f.nolibf == 0), ifnlbf=int(f.nolibf in (1, 3)), ifhybf=int(f.nolibf == 2),
+        nws=int(abs(f.nws)))
+    if f.nolifa == 2:
+        params["velmin"] = f.velmin
+    if f.nolibf in (2, 3):
+        params.update(hbreak=f.hbreak, ftheta=f.ftheta)
+    if f.nolibf == 2:
+        params["fgamma"] = f.fgamma
+    sched = Schedule(dt=f.dtdp, statim=f.statim, reftim=f.reftim, nramp=f.nramp, dramp=f.dramp_elev,
+                     dramp_mete=f.dramp_mete, dunramp_mete=f.dunramp_mete,
+                     dramp_extflux=f.dramp_extflux)
+    tides = [(float(f.amig[k]), float(f.face[k]), float(f.ff[k]), f.emo[k].copy(), f.efa[k].copy())
+             for k in range(f.nbfr)]
+    case = build_case(raw, params, sched, tides, cf=f.tau if f.nolibf == 0 else f.cf, tau0=f.tau0,
+                      eslm=f.eslm, cori=f.cori, anginn=f.anginn, prep=prep)
+    if f.nffr > 0:
+        lbc = case.arrays["lbcodei"][:case.sizes["nvel"]]
+        f = adcirc_io.read_fort15(fort15, neta, lbc)      # flux records on the case's NVEL order
+        fper = np.where(f.famig != 0.0, 2.0 * math.pi / np.where(f.famig != 0.0, f.famig, 1.0), 0.0)
+        case.flux = Flux(f.famig.copy(), fper, f.fff.copy(), f.fface.copy(), f.qnam.copy(),
+                         f.qnph.copy())
+    if abs(f.nws) == 8:
+        case.vortex = vortex
+    case.meta["fort15"] = f
+    return case
+
+
+def fort15_for_case(case: Case, rnday: float = 1.0, rundes: str = "", runid: str = "run"):
+    """The fort.15 values of a Case (the inverse of case_from_files), for
+    adcirc_io.write_fort15: NRAMP 8 carries the case's separate elevation,
+    flux and met ramps; outputs, stations and harmonic analysis are off."""
+    from . import adcirc_io
+    p, b, s = case.params, case.meta.get("build", {}), case.schedule
+    o = _lib.AdcFort15()
+    o.rundes = (rundes or case.name).encode()[:80]
+    o.runid = runid.encode()[:80]
+    o.nfover, o.nabout, o.nscreen, o.ihot, o.ics, o.im = 1, 1, 0, 0, 1, 0
+    o.nolibf = 0 if p["iflinbf"] else (2 if p["ifhybf"] else 1)
+    o.nolifa, o.nolica, o.nolicat = p["nolifa"], p["ifnlct"], p["ifnlcat"]
+    o.ncor, o.ntip, o.nws = 0, 0, p["nws"]
+    o.g, o.tau0, o.dtdp, o.statim, o.reftim, o.rnday = p["g"], b.get("tau0", 0.005), p["dt"], \
+        s.statim, s.reftim, rnday
+    if o.nws:
+        o.irefyr, o.irefmo, o.irefday, o.irefhr, o.storm_number = 2000, 1, 1, 0, 1
+        o.bladj = case.vortex.bladj if case.vortex is not None else 0.9
+    o.nramp = 0 if s.nramp == 0 else 8
+    o.dramp = o.dramp_intflux = o.dramp_elev = o.dramp_tip = o.dramp_wrad = s.dramp
+    o.dramp_extflux = s.dramp if s.dramp_extflux is None else s.dramp_extflux
+    o.dramp_mete, o.dunramp_mete = s.dramp_mete, s.dunramp_mete
+    o.a00, o.b00, o.c00, o.h0, o.velmin = p["a00"], p["b00"], p["c00"], p["h0"], p["velmin"]
+    o.nodedrymin, o.nodewetmin = 0, 0
+    cf = b.get("cf", 0.0025)
+    o.tau, o.cf = cf, cf
+    o.hbreak, o.ftheta, o.fgamma = p["hbreak"], p["ftheta"], p["fgamma"]
+    o.eslm, o.cori, o.anginn = b.get("eslm", 5.0), b.get("cori", 1.0e-4), b.get("anginn", 110.0)
+    o.convcr, o.itmax, o.ititer, o.isldia = p["convcr"], p["itmax"], 1, p["isldia"]
+    o.slim, o.has_slim = p["slim"], int(p["slim"] != 1.0e9)
+    o.wind_drag_limit = case.vortex.drag_limit if case.vortex is not None else 0.0035
+    o.has_wind_drag_limit = int(case.vortex is not None and o.wind_drag_limit != 0.0035)
+    nbfr, neta = case.sizes["nbfr"], case.sizes["neta"]
+    a = case.arrays
+    o.nbfr = nbfr
+    tabs = {"amig": a["amig"][:nbfr], "ff": a["ff"][:nbfr], "face": a["face"][:nbfr],
+            "emo": a["emo"][:nbfr, :neta], "efa": a["efa"][:nbfr, :neta]}
+    if case.flux is not None:
+        o.nffr = case.flux.famig.size
+        tabs.update(famig=case.flux.famig, fff=case.flux.fff, fface=case.flux.fface,
+                    qnam=case.flux.qnam, qnph=case.flux.qnph)
+    return adcirc_io.Fort15(o, [], [f"C{k + 1}" for k in range(nbfr)],
+                            [f"F{k + 1}" for k in range(o.nffr)], [], tabs)
 
 
 # --------------------------------------------------------------------------

@@ -278,6 +278,66 @@ int adc_fort14_write(const char *path, const char *title, int np, int ne, const 
                      const int *nbdv, int nbou, const int *nvell, const int *ibtype,
                      const int *nbvv);
 
+/* fort.15 model parameters of a 2DDI run (READ_INPUT, read_input.F:
+ * 949-4566), positional records in read_input's order plus the namelist
+ * values the path uses (&wetDryControl slim, &metControl WindDragLimit).
+ * Angles read_input converts on reading (FACE, EFA, FFACE, QNPH, ENPH,
+ * FACET) are returned in radians.  IM other than 0/10/111111, NWS other
+ * than 0/+-8, and station lists in external .151 files return
+ * ADC_ERR_UNSUPPORTED; malformed records ADC_ERR_ARG with the record
+ * number in adc_last_error(). */
+typedef struct {
+  int nout, nspool;      /* NOUT*, NSPOOL* */
+  double touts, toutf;   /* TOUTS*, TOUTF* (days) */
+} adc_output_spec_t;
+
+typedef struct {
+  char rundes[88], runid[88];
+  int nfover, nabout, nscreen, ihot, ics, im;
+  int nolibf, nolifa, nolica, nolicat, nwp, ncor;
+  int ntip, nws, nramp, nodedrymin, nodewetmin, storm_number;
+  int irefyr, irefmo, irefday, irefhr;             /* NWS = 8 wind record */
+  int ntif, nbfr, nffr, nfreq;
+  int nstae, nstav, nstac, nstam;
+  int nhainc, nhase, nhasv, nhage, nhagv, nhstar;
+  int nhsinc, ititer, isldia, itmax;
+  int has_slim, has_wind_drag_limit;               /* namelist values found */
+  double bladj, g, tau0, tau0_min, tau0_max, dtdp, statim, reftim, rnday;
+  double dramp, dramp_extflux, flux_settling_time, dramp_intflux, dramp_elev, dramp_tip,
+      dramp_mete, dramp_wrad, dunramp_mete;        /* days */
+  double a00, b00, c00, h0, velmin, slam0, sfea0;
+  double tau, cf, hbreak, ftheta, fgamma, eslm, eslc, cori, anginn;
+  double thas, thaf, fmv, convcr;
+  double slim, wind_drag_limit;                    /* defaults 1e9, 0.0035 */
+  adc_output_spec_t oute, outv, outc, outm, outge, outgv, outgc, outgw;
+} adc_fort15_t;
+
+/* Caller-owned tables adc_fort15_read fills; any pointer may be NULL (a
+ * first call with tables = NULL returns the counts NTIF, NBFR, NFFR, NFREQ
+ * and the station counts).  Tags are 16 bytes per entry, NUL-terminated. */
+typedef struct {
+  double *tpk, *amigt, *etrf, *fft, *facet;     /* (NTIF) */
+  double *amig, *ff, *face;                     /* (NBFR) */
+  double *emo, *efa;                            /* EMO(NBFR,NETA), EFA(NBFR,NETA) */
+  double *famig, *fff, *fface;                  /* (NFFR) */
+  double *qnam, *qnph, *enam, *enph;            /* QNAM(NFFR,NVEL) ...; 0 off flux nodes */
+  double *hafreq, *haff, *haface;               /* (NFREQ); HAFACE in degrees */
+  double *xel, *yel, *xev, *yev, *xem, *yem;    /* station coordinates */
+  char *tiptag, *bountag, *fbountag, *namefr;
+} adc_fort15_tables_t;
+
+/* neta: NETA of the fort.14; lbcodei (NVEL): LBCODEI of every flux-boundary
+ * node in the reference's order (adc_boundary_setup's), which decides
+ * where the flux records are and how many items each holds. */
+int adc_fort15_read(const char *path, int neta, int nvel, const int *lbcodei, adc_fort15_t *out,
+                    const adc_fort15_tables_t *tables);
+/* Writes the same records in the same order (reals to 17 significant
+ * digits, angles in degrees as the file holds them; NWP = 0), so that
+ * adc_fort15_read gives back the same values; the namelists only when
+ * their has_* flag is set. */
+int adc_fort15_write(const char *path, const adc_fort15_t *p, int neta, int nvel,
+                     const int *lbcodei, const adc_fort15_tables_t *tables);
+
 /* Full-domain ASCII output files fort.63 (irtype 1) and fort.64 (irtype 2):
  * the header of header63/64 (globalio.F:1005-1085) and one record per call
  * as writeFullFormat/storeOne/storeTwo write them (globalio.F:544-643,
