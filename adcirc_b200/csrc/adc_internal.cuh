@@ -119,11 +119,13 @@ struct adc_ctx {
   int *me_i;             // per momentum BC entry: its boundary entry (NVEL index)
   // specified normal flux (flux.cu)
   int nfluxf, flux_on, nffr, n_fx;
+  int nfluxrbc;          // radiation (IBTYPE 30) entries present
   double *qn;            // QN0, QN1, QN2 (NVEL each)
   double *qforce;        // per boundary entry: the GWCE line-integral force
   double *fconst, *fqn;  // FAMIG/FPER/FFF/FFACE, then QNAM and QNPH (NFFR x NVEL)
   int *bnv, *blbc;       // boundary entries: node (0-based), LBCODEI
   double *bbl;           // BNDLEN2O3
+  double *bcsii, *bsiii; // CSII, SIII per boundary entry (radiation discharge)
   int *fx_node, *fx_ptr, *fx_ent;   // per boundary node: (segment << 1 | side) in order
   int *me_lbc;
   double *me_csi, *me_sii;

@@ -1,16 +1,20 @@
-// flux.cu -- specified normal flux boundaries (IBTYPE 2, 12, 22).
+// flux.cu -- specified normal flux boundaries (IBTYPE 2, 12, 22) and
+// radiation boundaries (IBTYPE 30).
 //
 // Three pieces of the reference's flux-boundary path:
 //  * QN0 <- QN1 <- QN2 <- 0 (timestep.F:606-613), then QN2 as the sum of the
 //    periodic flux constituents (timestep.F:861-880; ICS = 1, so the normal
-//    flux is not rotated);
+//    flux is not rotated), and at radiation entries QN1 = H2 (UU1 CSII +
+//    VV1 SIII), the discharge of the latest velocity (timestep.F:932-940);
 //  * the GWCE boundary line integral (gwce.F:1737-1834): a force per
-//    boundary entry, then for each pair of consecutive entries a
-//    contribution to both nodes.  The reference adds these in entry order;
+//    boundary entry (specified flux, or the radiation condition
+//    -sqrt(g H1) ETAS / DT - TAU0 QN1), then for each pair of consecutive
+//    entries a contribution to both nodes.  The reference adds these in entry order;
 //    here one thread per boundary node adds its contributions in that same
 //    order (a table built at bind lists them), so GWCE_LV gets the same bits;
 //  * the specified normal velocity -QN2/H2 of the momentum boundary
-//    conditions (momentum.F:815-856), read in k_mom_node.
+//    conditions (momentum.F:815-856), read in k_mom_node; radiation nodes
+//    take no momentum boundary condition.
 #include "adc_internal.cuh"
 
 #include <cstring>
@@ -41,16 +45,28 @@ __global__ void k_flux_forcing(adc_ctx c, const adc_step_t *steps, const Flags *
     }
   }
   qn2[I] = q;
+  if (lb == 30) {
+    const int n = c.bnv[I];
+    const double UN1 = c.uu1[n] * c.bcsii[I] + c.vv1[n] * c.bsiii[I];
+    qn1[I] = c.h2[n] * UN1;
+  }
 }
 
-// The force of each boundary entry (LBCODEI <= 29 types, gwce.F:1783).
+// The force of each boundary entry (gwce.F:1783-1790): LBCODEI <= 29 from
+// the specified flux, 30 the radiation condition with the saved H1.
 __global__ void k_flux_qforce(adc_ctx c) {
   griddep_wait();
   const int J = blockIdx.x * blockDim.x + threadIdx.x;
   if (J >= c.nvel) return;
   const double *qn0 = c.qn, *qn1 = c.qn + c.nvel, *qn2 = c.qn + 2 * c.nvel;
+  const int n = c.bnv[J];
+  if (c.blbc[J] == 30) {
+    const double CELERITY = sqrt(c.p.g * c.h1[n]);
+    c.qforce[J] = -CELERITY * c.etas[n] / c.p.dt - c.tau0[n] * qn1[J];
+    return;
+  }
   const double DT2 = c.p.dt * 2.0;
-  c.qforce[J] = (qn2[J] - qn0[J]) / DT2 + c.tau0[c.bnv[J]] * qn1[J];
+  c.qforce[J] = (qn2[J] - qn0[J]) / DT2 + c.tau0[n] * qn1[J];
 }
 
 // One thread per boundary node: its contributions in entry order.
@@ -72,14 +88,14 @@ __global__ void k_flux_rhs(adc_ctx c) {
 }
 
 int launch_flux_forcing(adc_ctx *c) {
-  if (!c->nfluxf) return ADC_OK;
+  if (!c->nfluxf && !c->nfluxrbc) return ADC_OK;
   launch_k(k_flux_forcing, nblk(c->nvel), kThreads, c->stream, *c, c->steps, c->flags);
   c->launches++;
   return ADC_OK;
 }
 
 int launch_flux_rhs(adc_ctx *c) {
-  if (!c->nfluxf) return ADC_OK;
+  if (!c->nfluxf && !c->nfluxrbc) return ADC_OK;
   launch_k(k_flux_qforce, nblk(c->nvel), kThreads, c->stream, *c);
   launch_k(k_flux_rhs, nblk(c->n_fx), kThreads, c->stream, *c);
   c->launches += 2;
@@ -92,19 +108,20 @@ int flux_tables(adc_ctx *c, const adc_arrays_t *a) {
   const int nv = a->nvel;
   c->nvel = nv;
   c->nfluxf = 0;
+  c->nfluxrbc = 0;
   for (int I = 0; I < nv; ++I) {
     const int lb = a->lbcodei[I];
     if (lb == 2 || lb == 12 || lb == 22) c->nfluxf = 1;
-    if (lb == 30 || lb == 32 || lb == 40 || lb == 41 || lb == 52 || lb == 64) {
-      set_error("boundary code %d (radiation, zero-gradient or river-radiation flux) is not "
-                "implemented", lb);
+    if (lb == 30) c->nfluxrbc = 1;
+    if (lb == 32 || lb == 40 || lb == 41 || lb == 52 || lb == 64) {
+      set_error("boundary code %d (zero-gradient or river-radiation flux) is not implemented", lb);
       return ADC_ERR_UNSUPPORTED;
     }
   }
   const size_t nva = (size_t)(nv > 0 ? nv : 1);
   ADC_CUDA(cudaMalloc((void **)&c->qn, 3 * nva * sizeof(double)));
   ADC_CUDA(cudaMemset(c->qn, 0, 3 * nva * sizeof(double)));
-  if (!c->nfluxf) return ADC_OK;
+  if (!c->nfluxf && !c->nfluxrbc) return ADC_OK;
   std::vector<int> bnv(nv);
   for (int I = 0; I < nv; ++I) bnv[I] = a->nbv[I] - 1;
   std::vector<std::vector<int>> lists(c->np);
@@ -137,6 +154,10 @@ int flux_tables(adc_ctx *c, const adc_arrays_t *a) {
   ADC_CUDA(cudaMalloc((void **)&c->bbl, nva * sizeof(double)));
   ADC_CUDA(cudaMemcpy(c->bbl, a->bndlen2o3, nv * sizeof(double), cudaMemcpyHostToDevice));
   ADC_CUDA(cudaMalloc((void **)&c->qforce, nva * sizeof(double)));
+  ADC_CUDA(cudaMalloc((void **)&c->bcsii, nva * sizeof(double)));
+  ADC_CUDA(cudaMalloc((void **)&c->bsiii, nva * sizeof(double)));
+  ADC_CUDA(cudaMemcpy(c->bcsii, a->csii, nv * sizeof(double), cudaMemcpyHostToDevice));
+  ADC_CUDA(cudaMemcpy(c->bsiii, a->siii, nv * sizeof(double), cudaMemcpyHostToDevice));
   return ADC_OK;
 }
 

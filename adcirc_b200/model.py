@@ -482,22 +482,23 @@ K1_PERIOD = 86164.0
 
 
 def channel_case(dt: float = 5.0, amp: float = 0.5, vortex: bool = False,
-                 river: float | None = None, river_type: int = 2, prep: MeshPrep | None = None,
-                 **kw) -> Case:
+                 river: float | None = None, river_type: int = 2, radiation: bool = False,
+                 prep: MeshPrep | None = None, **kw) -> Case:
     """Tidal channel: 121x41 nodes, 20 m -> 5 m, M2 0.5 m, dt 5 s.  With
     `vortex`, a small Holland vortex (Rmax 8 km) crosses the channel.  With
     `river` [m^2/s per unit width], the closed east end becomes a
     specified-flux boundary (IBTYPE `river_type`, 2 or 22) carrying that
-    steady inflow, ramped in over 0.02 days."""
+    steady inflow, ramped in over 0.02 days.  With `radiation`, the east end
+    is a radiation boundary (IBTYPE 30) the tide leaves through."""
     from .meshgen import channel_mesh
     raw = channel_mesh()
-    if river is not None:
+    if river is not None or radiation:
         nx, ny = 121, 41
         nid = lambda i, j: i * ny + j
         south = np.array([nid(i, 0) for i in range(nx)])
         east = np.array([nid(nx - 1, j) for j in range(ny)])
         north = np.array([nid(i, ny - 1) for i in range(nx - 1, -1, -1)])
-        raw.land_segments = [(0, south), (river_type, east), (0, north)]
+        raw.land_segments = [(0, south), (30 if radiation else river_type, east), (0, north)]
     neta = raw.open_nodes.size
     tides = [(2.0 * math.pi / M2_PERIOD, 0.0, 1.0, np.full(neta, amp), np.zeros(neta))]
     if vortex:

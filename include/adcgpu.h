@@ -371,7 +371,11 @@ int adc_selftest_div_const(long long n, unsigned long long seed, long long *mism
  * the GWCE gains the boundary flux integral (gwce.F:1737-1834) and the
  * momentum equation the specified normal velocity -QN2/H2 (momentum.F:
  * 815-856).  Without a call the fluxes stay zero.  ADC_ERR_ARG if the mesh
- * has no flux boundary or nffr < 1. */
+ * has no flux boundary or nffr < 1.  Radiation boundaries (IBTYPE 30) need
+ * no call: every step takes their discharge from the latest velocity
+ * (timestep.F:932-940) and the GWCE boundary integral the radiation force
+ * (gwce.F:1783-1790); codes 32, 40, 41, 52 and 64 are refused at bind with
+ * ADC_ERR_UNSUPPORTED. */
 int adc_set_flux(adc_ctx *ctx, const adc_flux_t *flux);
 
 /* No reference counterpart (the reference always starts JCG from ETAS as

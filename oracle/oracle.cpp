@@ -584,6 +584,7 @@ struct orc_model {
    * (bestTrackCounter, WTRATIO; nws08.F90:68, 114) */
   /* specified normal flux: NFLUXF, the constituents and QN0/QN1/QN2 (NVEL) */
   int nfluxf = 0, flux_on = 0, nffr = 0;
+  int nfluxrbc = 0;   /* radiation (IBTYPE 30) entries, mesh.F:2045 */
   std::vector<double> famig, fper, fff, fface, qnam, qnph, qn0, qn1, qn2;
   int vortex_on = 0;
   orc_vortex_t vpar;
@@ -640,6 +641,7 @@ orc_model *orc_model_create(const orc_params_t *p, orc_arrays_t *a) {
   for (int I = 0; I < a->nvel; ++I) {
     const int lb = a->lbcodei[I];
     if (lb == 2 || lb == 12 || lb == 22) m->nfluxf = 1;
+    if (lb == 30) m->nfluxrbc = 1;
   }
   m->qn0.assign(std::max(a->nvel, 1), 0.0);
   m->qn1 = m->qn0;
@@ -724,10 +726,19 @@ int orc_model_set_flux(orc_model *m, const orc_flux_t *f) {
   return 0;
 }
 
-/* periodic specified normal flux, timestep.F:861-880 (ICS = 1: no rotation) */
+/* periodic specified normal flux, timestep.F:861-880 (ICS = 1: no rotation),
+ * then the discharge at radiation entries, timestep.F:932-940 */
 static void orc_model_flux(orc_model *m, const orc_step_t *s) {
-  if (!m->nfluxf || !m->flux_on) return;
   orc_arrays_t *a = m->a;
+  if (m->nfluxrbc) {
+    for (int I = 0; I < a->nvel; ++I) {
+      if (a->lbcodei[I] != 30) continue;
+      const int NNBB = a->nbv[I] - 1;
+      const double UN1 = a->uu1[NNBB] * a->csii[I] + a->vv1[NNBB] * a->siii[I];
+      m->qn1[I] = a->h2[NNBB] * UN1;
+    }
+  }
+  if (!m->nfluxf || !m->flux_on) return;
   for (int J = 0; J < m->nffr; ++J) {
     int NCYC = 0;
     if (m->fper[J] != 0.0) NCYC = (int)(s->timeh / m->fper[J]);
@@ -951,16 +962,24 @@ int orc_model_gwce(orc_model *m, const orc_step_t *s, orc_stepout_t *out) {
       a->eta2[b] = a->eta2[b] + a->emo[J + (size_t)a->nbfr * I] * RFF * std::cos(ARG);
     }
   }
-  /* boundary flux integral, gwce.F:1737-1834 (LBCODEI <= 29 types) */
-  if (m->nfluxf) {
+  /* boundary flux integral, gwce.F:1737-1834 (LBCODEI <= 29 types and
+   * radiation, 30, with the H1 saved above) */
+  if (m->nfluxf || m->nfluxrbc) {
     const double DT2 = p.dt * 2.0;
+    auto qforce = [&](int J, int NBDJ) {
+      if (a->lbcodei[J] == 30) {
+        const double CELERITY = std::sqrt(G * a->h1[NBDJ]);
+        return -CELERITY * a->etas[NBDJ] / DT - a->tau0var[NBDJ] * m->qn1[J];
+      }
+      return (m->qn2[J] - m->qn0[J]) / DT2 + a->tau0var[NBDJ] * m->qn1[J];
+    };
     int NBDJ = a->nbv[0] - 1;
-    double QFORCEJ = (m->qn2[0] - m->qn0[0]) / DT2 + a->tau0var[NBDJ] * m->qn1[0];
+    double QFORCEJ = qforce(0, NBDJ);
     for (int J = 1; J < a->nvel; ++J) {
       const int NBDI = NBDJ;
       NBDJ = a->nbv[J] - 1;
       const double QFORCEI = QFORCEJ;
-      QFORCEJ = (m->qn2[J] - m->qn0[J]) / DT2 + a->tau0var[NBDJ] * m->qn1[J];
+      QFORCEJ = qforce(J, NBDJ);
       const int NCI = a->nodecode[NBDI], NCJ = a->nodecode[NBDJ];
       const double B = NCI * NCJ * a->bndlen2o3[J - 1] / 4.0;
       a->gwce_lv[NBDI] = a->gwce_lv[NBDI] + B * (2.0 * QFORCEI + QFORCEJ);

@@ -224,3 +224,17 @@ def test_channel_river_flux(lib, orc, river_type):
     a = c0.arrays
     east = a["x"] > 59.9e3
     assert a["uu2"][east].mean() < -0.02   # the inflow reaches the boundary nodes
+
+
+def test_channel_radiation_boundary(lib, orc):
+    """A radiation boundary (IBTYPE 30) at the channel's east end: the
+    discharge of the latest velocity (timestep.F:932-940) and the radiation
+    force -sqrt(g H1) ETAS / DT - TAU0 QN1 of the GWCE boundary integral
+    (gwce.F:1783-1790), against the oracle over a graph-replayed run long
+    enough for the tide to reach and leave through the boundary."""
+    from adcirc_b200 import model
+    c0, cg, io, ig = _pair(lambda **k: model.channel_case(radiation=True, **k), 1500, use_run=True)
+    _check(c0, cg, io, ig)
+    a = c0.arrays
+    east = a["x"] > 59.9e3
+    assert a["uu2"][east].mean() > 0.02   # the tide leaves through the boundary

@@ -38,3 +38,21 @@ def test_mirror_symmetry(orc):
     om.close()
     asym = K.asymmetry(c)
     assert asym["eta"] <= 1e-12 and asym["u"] <= 1e-12 and asym["v"] <= 1e-9, asym
+
+
+def test_radiation_boundary_passes_the_wave(orc):
+    """A radiation boundary (IBTYPE 30) lets the incoming tide leave: at the
+    boundary the normal velocity follows the outgoing long-wave relation
+    u = eta sqrt(g / H) (the condition gwce.F:1783-1790 imposes), where a
+    closed end holds u = 0 and reflects."""
+    from adcirc_b200 import model
+    c = model.channel_case(radiation=True, prep=orc.mesh_prep())
+    om = orc.OracleModel(c)
+    om.run(1, 1500)
+    om.close()
+    a = c.arrays
+    east = a["x"] > 59.9e3
+    u, eta, h = a["uu2"][east].mean(), a["eta2"][east].mean(), a["h2"][east].mean()
+    assert u > 0.02 and eta > 0.02
+    ratio = u / (eta * np.sqrt(c.params["g"] / h))
+    assert 0.9 <= ratio <= 1.1, ratio

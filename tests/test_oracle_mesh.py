@@ -19,10 +19,11 @@ def _cases(orc):
     yield "beach", model.beach_case
     yield "river2", lambda **k: model.channel_case(river=0.5, river_type=2, **k)
     yield "river22", lambda **k: model.channel_case(river=0.5, river_type=22, **k)
+    yield "radiation", lambda **k: model.channel_case(radiation=True, **k)
     yield "surge30k", lambda **k: model.surge_case(target_nodes=30_000, **k)
 
 
-@pytest.mark.parametrize("name", ["channel", "beach", "river2", "river22", "surge30k"])
+@pytest.mark.parametrize("name", ["channel", "beach", "river2", "river22", "radiation", "surge30k"])
 def test_case_tables_match(lib, orc, name):
     fn = dict(_cases(orc))[name]
     a = fn()
