@@ -78,6 +78,44 @@ def beach_mesh(nx: int = 41, ny: int = 13, lx: float = 4e3, ly: float = 1.2e3,
     return m
 
 
+def quarter_annulus_mesh(nr: int = 21, nth: int = 31, r1: float = 60.96e3, r2: float = 152.4e3,
+                         h1: float = 3.048) -> RawMesh:
+    """Quarter-annular harbour (Lynch and Gray's analytic test): r1 <= r <=
+    r2, 0 <= theta <= 90 degrees, depth h1 (r / r1)^2 (3.048 m to 19.05 m),
+    nr x nth nodes on a polar grid, each cell split along alternating
+    diagonals.  The outer arc is the elevation boundary; the inner arc and
+    the two radial sides are one mainland segment (IBTYPE 0)."""
+    rs = np.linspace(r1, r2, nr)
+    th = np.linspace(0.0, 0.5 * np.pi, nth)
+    R, T = np.meshgrid(rs, th, indexing="ij")          # (nr, nth)
+    x = (R * np.cos(T)).ravel()
+    y = (R * np.sin(T)).ravel()
+    dp = h1 * (R.ravel() / r1) ** 2
+
+    def nid(i, j):
+        return i * nth + j
+
+    tris = []
+    for i in range(nr - 1):
+        for j in range(nth - 1):
+            a, b, c, d = nid(i, j), nid(i + 1, j), nid(i + 1, j + 1), nid(i, j + 1)
+            if (i + j) % 2 == 0:
+                tris += [(a, b, c), (a, c, d)]
+            else:
+                tris += [(a, b, d), (b, c, d)]
+    nm = np.asarray(tris, np.int64)
+    # outer arc, counter-clockwise (theta 0 -> 90 degrees)
+    open_nodes = np.array([nid(nr - 1, j) for j in range(nth)], np.int64)
+    # theta = 90 side inwards, inner arc back to theta = 0, theta = 0 side outwards
+    land = [nid(i, nth - 1) for i in range(nr - 1, -1, -1)]
+    land += [nid(0, j) for j in range(nth - 2, -1, -1)]
+    land += [nid(i, 0) for i in range(1, nr)]
+    return RawMesh("quarter_annulus", x, y, dp, nm, open_nodes,
+                   [(0, np.asarray(land, np.int64))],
+                   {"nr": nr, "nth": nth, "r1": r1, "r2": r2, "h1": h1,
+                    "lx": r2, "ly": r2})
+
+
 # --------------------------------------------------------------------------
 # Graded storm-surge mesh
 # --------------------------------------------------------------------------

@@ -534,6 +534,46 @@ def beach_case(dt: float = 2.0, amp: float = 0.5, period: float = 10800.0,
     return build_case(raw, params, sched, tides, prep=prep)
 
 
+def quarter_annulus_case(dt: float = 100.0, amp: float = 0.3048, tau: float = 1.0e-4,
+                         tau0: float = 1.0e-3, nr: int = 21, nth: int = 31,
+                         prep: MeshPrep | None = None, **kw) -> Case:
+    """Linear tide in the quarter-annular harbour (meshgen.quarter_annulus_mesh):
+    M2 of `amp` on the outer arc, linear bottom friction `tau` (NOLIBF = 0),
+    no advection, no finite-amplitude terms (H = DP), no Coriolis, no
+    lateral viscosity, ramped over half a day.  Its periodic state has the
+    closed-form solution of `quarter_annulus_solution`."""
+    from .meshgen import quarter_annulus_mesh
+    raw = quarter_annulus_mesh(nr, nth)
+    neta = raw.open_nodes.size
+    tides = [(2.0 * math.pi / M2_PERIOD, 0.0, 1.0, np.full(neta, amp), np.zeros(neta))]
+    kw = dict(dict(ifnlfa=0, ifnlct=0, ifnlcat=0, nolifa=0, iflinbf=1, ifnlbf=0, ifhybf=0), **kw)
+    params = default_params(dt, **kw)
+    sched = Schedule(dt=dt, dramp=0.5, dramp_mete=0.5)
+    return build_case(raw, params, sched, tides, cf=tau, tau0=tau0, eslm=0.0, cori=0.0, prep=prep)
+
+
+def quarter_annulus_solution(r, meta: dict, amp: float = 0.3048, tau: float = 1.0e-4,
+                             g: float = G_DEFAULT):
+    """Amplitude and phase (eta = A cos(w t - phase)) of the linear periodic
+    tide in the quarter annulus, depth h = h1 (r / r1)^2, no flow through
+    r = r1 and eta = amp cos(w t) at r = r2 (Lynch and Gray, 1978): with
+    eta = Re(E(r) exp(i w t)), the linear equations with bottom friction tau
+    give h1/r1^2 (r^2 E'' + 3 r E') = (-w^2 + i w tau) / g E, so E = a r^s1 +
+    b r^s2 with s^2 + 2 s - k = 0, k = (-w^2 + i w tau) r1^2 / (g h1)."""
+    w = 2.0 * math.pi / M2_PERIOD
+    r1, r2, h1 = meta["r1"], meta["r2"], meta["h1"]
+    k = (-w * w + 1j * w * tau) * r1 * r1 / (g * h1)
+    q = np.sqrt(1.0 + k + 0j)
+    s1, s2 = -1.0 + q, -1.0 - q
+    # E'(r1) = 0, E(r2) = amp (radii scaled by r1 to keep the powers tame)
+    x2 = r2 / r1
+    M = np.array([[s1, s2], [x2 ** s1, x2 ** s2]], dtype=complex)
+    a, b = np.linalg.solve(M, np.array([0.0, amp], dtype=complex))
+    x = np.asarray(r, np.float64) / r1
+    E = a * x ** s1 + b * x ** s2
+    return np.abs(E), -np.angle(E)
+
+
 def surge_case(seed: int = 2024, target_nodes: int = 600_000, dt: float = 1.0,
                vortex: bool = True, prep: MeshPrep | None = None, raw=None,
                tau0: float = -1.0, tide_scale: float = 1.0, cf: float = 0.0025,

@@ -13,7 +13,11 @@ equations, so both implementations must meet it to solver tolerance:
   1737-1834): once the flux ramp is complete each step adds Q*dt;
 * a channel triangulated mirror-symmetrically about its centreline,
   forced uniformly along the open boundary, without Coriolis: eta and u
-  are even and v is odd under the mirror.
+  are even and v is odd under the mirror;
+* the quarter-annular harbour of Lynch and Gray (depth ~ r^2, linear
+  friction, M2 on the outer arc), whose periodic linear tide has a closed
+  form (model.quarter_annulus_solution): the discrete solution matches it
+  to discretisation error, which falls with refinement.
 """
 from __future__ import annotations
 
@@ -112,3 +116,37 @@ def asymmetry(case) -> dict:
     return {"eta": float(np.abs(e - e[m]).max() / np.abs(e).max()),
             "u": float(np.abs(u - u[m]).max() / np.abs(u).max()),
             "v": float(np.abs(v + v[m]).max() / max(np.abs(v).max(), 1e-30))}
+
+
+def harmonic_m2(step_fn, case, n_spin_days: float = 5.0, cycles: int = 2):
+    """Runs `step_fn(it0, n)` (a model's run method) from cold start for
+    n_spin_days, then samples ETA2 every step over `cycles` M2 periods and
+    returns the least-squares M2 amplitude and phase (eta = A cos(w t -
+    phase)) per node."""
+    from adcirc_b200 import model
+    w = 2.0 * math.pi / model.M2_PERIOD
+    dt = case.params["dt"]
+    n_spin = int(n_spin_days * 86400.0 / dt)
+    per = int(round(model.M2_PERIOD / dt))
+    step_fn(1, n_spin)
+    it = n_spin + 1
+    ts, etas = [], []
+    for _ in range(cycles * per):
+        step_fn(it, 1)
+        ts.append(it * dt)
+        etas.append(case.arrays["eta2"].copy())
+        it += 1
+    ts = np.asarray(ts)
+    A = np.stack([np.cos(w * ts), np.sin(w * ts), np.ones_like(ts)], axis=1)
+    coef, *_ = np.linalg.lstsq(A, np.asarray(etas), rcond=None)
+    return np.hypot(coef[0], coef[1]), np.arctan2(coef[1], coef[0])
+
+
+def annulus_errors(case, amp, phase):
+    """Max relative amplitude error and max phase error [deg] against the
+    closed-form quarter-annulus tide."""
+    from adcirc_b200 import model
+    r = np.hypot(case.arrays["x"], case.arrays["y"])
+    ea, ep = model.quarter_annulus_solution(r, case.meta)
+    dph = np.degrees(np.abs((phase - ep + np.pi) % (2.0 * np.pi) - np.pi))
+    return float((np.abs(amp - ea) / ea).max()), float(dph.max())

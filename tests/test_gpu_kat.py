@@ -1,6 +1,7 @@
 """Known answers on the GPU path: volume conservation, the inflow mass
-balance and mirror symmetry (kat_cases.py), and the slope limiter
-(computeAlpha, wetdry.F:1561-1652) with ALPHAL < 1 against the oracle."""
+balance, mirror symmetry and the quarter-annulus analytic tide
+(kat_cases.py), and the slope limiter (computeAlpha, wetdry.F:1561-1652)
+with ALPHAL < 1 against the oracle."""
 import numpy as np
 import pytest
 
@@ -78,3 +79,26 @@ def test_slope_limiter_alphal(lib, orc):
     assert limited >= 100, limited
     assert c0.arrays["alphal"].min() <= 1.0
     _check(c0, cg, np.asarray(its_o), np.asarray(its_g))
+
+
+def test_gpu_quarter_annulus_matches_the_analytic_tide(lib, orc):
+    """The quarter-annular harbour (kat_cases): the GPU's periodic tide
+    matches the closed-form solution as the oracle's does, and the two
+    runs agree to the parity tolerance after five days."""
+    import oracle
+    from adcirc_b200 import model
+    c0, cg = oracle_and_gpu_cases(lambda **k: model.quarter_annulus_case(**k))
+    g = model.GpuModel(cg)
+
+    def run(it, n):
+        g.run(it, n)
+        g.sync_to_host()
+    amp, ph = K.harmonic_m2(run, cg)
+    g.close()
+    a_err, p_err = K.annulus_errors(cg, amp, ph)
+    assert a_err <= 5e-3 and p_err <= 0.5, (a_err, p_err)
+    om = oracle.OracleModel(c0)
+    it_end = int(5.0 * 86400.0 / c0.params["dt"]) + 2 * int(round(model.M2_PERIOD / c0.params["dt"]))
+    om.run(1, it_end)
+    om.close()
+    assert _rel(cg.arrays["eta2"], c0.arrays["eta2"]) <= 1e-9

@@ -56,3 +56,21 @@ def test_radiation_boundary_passes_the_wave(orc):
     assert u > 0.02 and eta > 0.02
     ratio = u / (eta * np.sqrt(c.params["g"] / h))
     assert 0.9 <= ratio <= 1.1, ratio
+
+
+def test_quarter_annulus_matches_the_analytic_tide(orc):
+    """Lynch and Gray's quarter-annular harbour (the reference test suite's
+    2D case): depth ~ r^2, linear friction, M2 on the outer arc.  The
+    oracle's periodic tide matches the closed-form solution (amplitude
+    0.30-0.57 m, phase 0-36 degrees) and the error falls with refinement."""
+    from adcirc_b200 import model
+    errs = []
+    for nr, nth in ((11, 16), (21, 31)):
+        c = model.quarter_annulus_case(nr=nr, nth=nth, prep=orc.mesh_prep())
+        om = orc.OracleModel(c)
+        amp, ph = K.harmonic_m2(lambda it, n: om.run(it, n), c)
+        om.close()
+        errs.append(K.annulus_errors(c, amp, ph))
+    (a0, p0), (a1, p1) = errs
+    assert a1 <= 5e-3 and p1 <= 0.5, errs
+    assert a1 < a0 and p1 < p0, errs
