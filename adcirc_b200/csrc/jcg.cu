@@ -1179,6 +1179,22 @@ static void jcg_local_tables(int n, int nslices, int nrb, int rows_max, const in
   }
 }
 
+// The dynamic shared memory a kernel may use is a per-function limit that
+// every context in the process shares, so it is set to the most the device
+// allows (its opt-in maximum less the kernel's static shared memory), not to
+// one context's need: contexts with different layouts (the members of an
+// ensemble) then all launch.
+static int jcg_smem_limit(const void *fn) {
+  int dev = 0, optin = 0;
+  ADC_CUDA(cudaGetDevice(&dev));
+  ADC_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  cudaFuncAttributes fa;
+  ADC_CUDA(cudaFuncGetAttributes(&fa, fn));
+  ADC_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                optin - (int)fa.sharedSizeBytes));
+  return ADC_OK;
+}
+
 // Grid of the persistent solver: as many 256-thread row blocks as can be
 // co-resident (2 per SM), plus the scalar block.  The resident variant is
 // used when host copies of the sliced ELL are given and each row block's
@@ -1221,7 +1237,7 @@ int jcg_setup_grid(adc_ctx *c, const JcgHostSell *h) {
     for (; fits && wcap >= std::max(1, wmax - 4); --wcap) {
       smem = jcg_smem_bytes(c->itmax, true, rows_max, halo_max, wcap);
       if (smem > 200 * 1024) continue;
-      ADC_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      if (int rc = jcg_smem_limit(fn)) return rc;
       ADC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kThreads, smem));
       if (per_sm >= 2) break;
     }
@@ -1249,7 +1265,7 @@ int jcg_setup_grid(adc_ctx *c, const JcgHostSell *h) {
   }
   const void *fn = (const void *)jcg_kernel<0, double>;
   size_t smem = jcg_smem_bytes(c->itmax, false, 0, 0, 1);
-  ADC_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  if (int rc = jcg_smem_limit(fn)) return rc;
   int per_sm = 0;
   ADC_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kThreads, smem));
   if (per_sm < 1) {
