@@ -34,7 +34,7 @@ struct Flags {
   int n_w1_events;    // W1 events of the last wet/dry pass
   int timeout;        // nonzero once a bounded wait expired
   int cursor;         // index of the current step in the step table
-  int pad_;
+  int etadisc_done;   // river radiation: ElevDisc taken (EtaDisc_Fill false, timestep.F:183, 906-926)
   double ep;          // EP (gwce.F:646-650), persists between rebuilds
   double zeta;        // RPARM(1) after the last solve
   double cme;         // RPARM(2) after the last solve
@@ -125,6 +125,9 @@ struct adc_ctx {
   // specified normal flux (flux.cu)
   int nfluxf, flux_on, nffr, n_fx;
   int nfluxrbc;          // radiation (IBTYPE 30) entries present
+  int flux_settling_it;  // FluxSettlingIT (river radiation, IBTYPE 52)
+  double *elevdisc;      // ElevDisc per boundary entry (IBTYPE 52)
+  double *etadisc_b;     // EtaDisc at the boundary entries' nodes
   double *qn;            // QN0, QN1, QN2 (NVEL each)
   double *qforce;        // per boundary entry: the GWCE line-integral force
   double *fconst, *fqn;  // FAMIG/FPER/FFF/FFACE, then QNAM and QNPH (NFFR x NVEL)

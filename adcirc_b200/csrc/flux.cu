@@ -1,14 +1,18 @@
-// flux.cu -- specified normal flux boundaries (IBTYPE 2, 12, 22) and
-// radiation boundaries (IBTYPE 30).
+// flux.cu -- specified normal flux boundaries (IBTYPE 2, 12, 22), radiation
+// boundaries (IBTYPE 30) and river-radiation boundaries (IBTYPE 52).
 //
 // Three pieces of the reference's flux-boundary path:
 //  * QN0 <- QN1 <- QN2 <- 0 (timestep.F:606-613), then QN2 as the sum of the
 //    periodic flux constituents (timestep.F:861-880; ICS = 1, so the normal
 //    flux is not rotated), and at radiation entries QN1 = H2 (UU1 CSII +
 //    VV1 SIII), the discharge of the latest velocity (timestep.F:932-940);
+//    river-radiation entries take their discharge elevation ElevDisc at
+//    FluxSettlingIT (or from the cold-start EtaDisc, timestep.F:906-926);
 //  * the GWCE boundary line integral (gwce.F:1737-1834): a force per
-//    boundary entry (specified flux, or the radiation condition
-//    -sqrt(g H1) ETAS / DT - TAU0 QN1), then for each pair of consecutive
+//    boundary entry (specified flux, the radiation condition
+//    -sqrt(g H1) ETAS / DT - TAU0 QN1, or for river radiation the specified
+//    flux less sqrt(g H1) (ETAS / DT + TAU0 (ETA1 - ElevDisc)) after
+//    FluxSettlingIT), then for each pair of consecutive
 //    entries a contribution to both nodes.  The reference adds these in entry order;
 //    here one thread per boundary node adds its contributions in that same
 //    order (a table built at bind lists them), so GWCE_LV gets the same bits;
@@ -31,8 +35,8 @@ __global__ void k_flux_forcing(adc_ctx c, const adc_step_t *steps, const Flags *
   qn1[I] = qn2[I];
   double q = 0.0;
   const int lb = c.blbc[I];
-  if (c.flux_on && (lb == 2 || lb == 12 || lb == 22)) {
-    const adc_step_t st = steps[flags->cursor];
+  const adc_step_t st = steps[flags->cursor];
+  if (c.flux_on && (lb == 2 || lb == 12 || lb == 22 || lb == 52)) {
     const int nf = c.nffr;
     const double *famig = c.fconst, *fper = famig + nf, *fff = fper + nf, *fface = fff + nf;
     const double *qnam = c.fqn, *qnph = c.fqn + (size_t)nf * c.nvel;
@@ -45,6 +49,15 @@ __global__ void k_flux_forcing(adc_ctx c, const adc_step_t *steps, const Flags *
     }
   }
   qn2[I] = q;
+  if (lb == 52) {
+    const int n = c.bnv[I];
+    if (st.it == c.flux_settling_it) {
+      c.etadisc_b[I] = c.eta2[n];
+      c.elevdisc[I] = c.eta2[n];
+    } else if (!flags->etadisc_done && st.it > c.flux_settling_it) {
+      c.elevdisc[I] = c.etadisc_b[I];
+    }
+  }
   if (lb == 30) {
     const int n = c.bnv[I];
     const double UN1 = c.uu1[n] * c.bcsii[I] + c.vv1[n] * c.bsiii[I];
@@ -52,11 +65,16 @@ __global__ void k_flux_forcing(adc_ctx c, const adc_step_t *steps, const Flags *
   }
 }
 
-// The force of each boundary entry (gwce.F:1783-1790): LBCODEI <= 29 from
-// the specified flux, 30 the radiation condition with the saved H1.
-__global__ void k_flux_qforce(adc_ctx c) {
+// The force of each boundary entry (gwce.F:1783-1815): LBCODEI <= 29 from
+// the specified flux, 30 the radiation condition with the saved H1, 52 the
+// specified flux plus, after FluxSettlingIT, the radiation term.
+__global__ void k_flux_qforce(adc_ctx c, const adc_step_t *steps, Flags *flags) {
   griddep_wait();
   const int J = blockIdx.x * blockDim.x + threadIdx.x;
+  const int it = steps[flags->cursor].it;
+  // EtaDisc_Fill ends with the first step at or after FluxSettlingIT; the
+  // forcing kernel of this step has read it already
+  if (J == 0 && it >= c.flux_settling_it) flags->etadisc_done = 1;
   if (J >= c.nvel) return;
   const double *qn0 = c.qn, *qn1 = c.qn + c.nvel, *qn2 = c.qn + 2 * c.nvel;
   const int n = c.bnv[J];
@@ -66,7 +84,12 @@ __global__ void k_flux_qforce(adc_ctx c) {
     return;
   }
   const double DT2 = c.p.dt * 2.0;
-  c.qforce[J] = (qn2[J] - qn0[J]) / DT2 + c.tau0[n] * qn1[J];
+  double q = (qn2[J] - qn0[J]) / DT2 + c.tau0[n] * qn1[J];
+  if (c.blbc[J] == 52 && it > c.flux_settling_it) {
+    const double Celerity = sqrt(c.p.g * c.h1[n]);
+    q = q - Celerity * (c.etas[n] / c.p.dt + c.tau0[n] * (c.eta1[n] - c.elevdisc[J]));
+  }
+  c.qforce[J] = q;
 }
 
 // One thread per boundary node: its contributions in entry order.
@@ -96,7 +119,7 @@ int launch_flux_forcing(adc_ctx *c) {
 
 int launch_flux_rhs(adc_ctx *c) {
   if (!c->nfluxf && !c->nfluxrbc) return ADC_OK;
-  launch_k(k_flux_qforce, nblk(c->nvel), kThreads, c->stream, *c);
+  launch_k(k_flux_qforce, nblk(c->nvel), kThreads, c->stream, *c, c->steps, c->flags);
   launch_k(k_flux_rhs, nblk(c->n_fx), kThreads, c->stream, *c);
   c->launches += 2;
   return ADC_OK;
@@ -111,9 +134,9 @@ int flux_tables(adc_ctx *c, const adc_arrays_t *a) {
   c->nfluxrbc = 0;
   for (int I = 0; I < nv; ++I) {
     const int lb = a->lbcodei[I];
-    if (lb == 2 || lb == 12 || lb == 22) c->nfluxf = 1;
+    if (lb == 2 || lb == 12 || lb == 22 || lb == 52) c->nfluxf = 1;
     if (lb == 30) c->nfluxrbc = 1;
-    if (lb == 32 || lb == 40 || lb == 41 || lb == 52 || lb == 64) {
+    if (lb == 32 || lb == 40 || lb == 41 || lb == 64) {
       set_error("boundary code %d (zero-gradient or river-radiation flux) is not implemented", lb);
       return ADC_ERR_UNSUPPORTED;
     }
@@ -158,6 +181,15 @@ int flux_tables(adc_ctx *c, const adc_arrays_t *a) {
   ADC_CUDA(cudaMalloc((void **)&c->bsiii, nva * sizeof(double)));
   ADC_CUDA(cudaMemcpy(c->bcsii, a->csii, nv * sizeof(double), cudaMemcpyHostToDevice));
   ADC_CUDA(cudaMemcpy(c->bsiii, a->siii, nv * sizeof(double), cudaMemcpyHostToDevice));
+  // EtaDisc at the river-radiation nodes from the bound (cold-start) ETA2,
+  // cstart.F:1186-1191; ElevDisc is set by the steps
+  std::vector<double> ed(nva, 0.0);
+  for (int I = 0; I < nv; ++I)
+    if (a->lbcodei[I] == 52) ed[I] = a->eta2[bnv[I]];
+  ADC_CUDA(cudaMalloc((void **)&c->etadisc_b, nva * sizeof(double)));
+  ADC_CUDA(cudaMemcpy(c->etadisc_b, ed.data(), nva * sizeof(double), cudaMemcpyHostToDevice));
+  ADC_CUDA(cudaMalloc((void **)&c->elevdisc, nva * sizeof(double)));
+  ADC_CUDA(cudaMemset(c->elevdisc, 0, nva * sizeof(double)));
   return ADC_OK;
 }
 
@@ -172,7 +204,7 @@ extern "C" int adc_set_flux(adc_ctx *c, const adc_flux_t *f) {
     return ADC_ERR_ARG;
   }
   if (!c->nfluxf) {
-    set_error("adc_set_flux: the mesh has no specified-flux boundary (IBTYPE 2, 12 or 22)");
+    set_error("adc_set_flux: the mesh has no specified-flux boundary (IBTYPE 2, 12, 22 or 52)");
     return ADC_ERR_ARG;
   }
   const int nf = f->nffr, nv = c->nvel;
@@ -192,6 +224,7 @@ extern "C" int adc_set_flux(adc_ctx *c, const adc_flux_t *f) {
   ADC_CUDA(cudaMemcpy(c->fqn + (size_t)nf * nv, f->qnph, (size_t)nf * nv * sizeof(double),
                       cudaMemcpyHostToDevice));
   c->nffr = nf;
+  c->flux_settling_it = f->flux_settling_it;
   c->flux_on = 1;
   drop_graphs(c);   // replayed steps must see the forcing
   return ADC_OK;

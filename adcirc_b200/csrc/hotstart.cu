@@ -60,7 +60,11 @@ static std::vector<HsRec> hs_records(adc_ctx *c) {
       {"itpack", c->itp, sizeof(Itp)},
   };
   if (c->vortex_on) r.push_back({"vortex", c->vstate, sizeof(VortexState)});
-  if (c->nfluxf || c->nfluxrbc) r.push_back({"flux_qn", c->qn, 3 * (size_t)c->nvel * d});
+  if (c->nfluxf || c->nfluxrbc) {
+    r.push_back({"flux_qn", c->qn, 3 * (size_t)c->nvel * d});
+    r.push_back({"flux_elevdisc", c->elevdisc, (size_t)c->nvel * d});   // river radiation
+    r.push_back({"flux_etadisc", c->etadisc_b, (size_t)c->nvel * d});
+  }
   if (c->prec & ADC_WARM_START) {
     r.push_back({"etas_prev", c->etas_prev, np * d});
     r.push_back({"warm", c->warm, sizeof(WarmState)});

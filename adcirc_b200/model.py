@@ -39,6 +39,12 @@ class Schedule:
     dramp_mete: float = 0.5  # days
     dunramp_mete: float = 0.0
     dramp_extflux: float | None = None   # days; None: the elevation ramp's
+    flux_settling_time: float = 0.0      # days (fort.15 FluxSettlingTime, NRAMP >= 2)
+
+    @property
+    def flux_settling_it(self) -> int:
+        """FluxSettlingIT, timestep.F:243-245."""
+        return int(self.flux_settling_time * 86400.0 / self.dt)
 
     def step(self, it: int) -> AdcStep:
         timeloc = it * self.dt + self.statim * 86400.0
@@ -48,6 +54,17 @@ class Schedule:
         else:
             relev = math.tanh((2.0 * timeloc / 86400.0) / self.dramp)
             rmete = math.tanh((2.0 * (timeloc / 86400.0 - self.dunramp_mete)) / self.dramp_mete)
+        fsit = self.flux_settling_it
+        if self.nramp > 1 and fsit > 0:
+            # every forcing but the river flux waits for the flux to settle,
+            # then ramps from there (timestep.F:314-345)
+            if it < fsit + 10:
+                relev = rmete = 0.0
+            else:
+                tl = (it - fsit - 10) * self.dt + self.statim * 86400.0
+                relev = math.tanh((2.0 * tl / 86400.0) / self.dramp)
+                if self.nramp != 8:
+                    rmete = math.tanh((2.0 * tl / 86400.0) / self.dramp_mete)
         if self.dramp < 1.0e-6:
             relev = 1.0
         if self.dramp_mete < 1.0e-6:
@@ -113,14 +130,16 @@ class Case:
 @dataclasses.dataclass
 class Flux:
     """Periodic specified normal flux on the flux boundaries (IBTYPE 2, 12,
-    22): constituents (rad/s, s, nodal factor, rad) and per boundary entry
-    (NVEL) amplitudes [m^2/s] and phases [rad], zero off flux entries."""
+    22, 52): constituents (rad/s, s, nodal factor, rad) and per boundary
+    entry (NVEL) amplitudes [m^2/s] and phases [rad], zero off flux entries;
+    flux_settling_it is FluxSettlingIT (river radiation, IBTYPE 52)."""
     famig: np.ndarray
     fper: np.ndarray
     fff: np.ndarray
     fface: np.ndarray
     qnam: np.ndarray   # (NFFR, NVEL)
     qnph: np.ndarray   # (NFFR, NVEL)
+    flux_settling_it: int = 0
 
     def struct(self, cls=None):
         """(struct, backing arrays); keep both alive while in use."""
@@ -130,6 +149,7 @@ class Flux:
         keep += [np.asfortranarray(a, np.float64) for a in (self.qnam, self.qnph)]
         f = cls()
         f.nffr = int(keep[0].size)
+        f.flux_settling_it = int(self.flux_settling_it)
         for name, a in zip(("famig", "fper", "fff", "fface", "qnam", "qnph"), keep):
             setattr(f, name, a.ctypes.data_as(dp_))
         return f, keep
@@ -411,7 +431,7 @@ def case_from_files(fort14, fort15, vortex: "Vortex | None" = None,
         params["fgamma"] = f.fgamma
     sched = Schedule(dt=f.dtdp, statim=f.statim, reftim=f.reftim, nramp=f.nramp, dramp=f.dramp_elev,
                      dramp_mete=f.dramp_mete, dunramp_mete=f.dunramp_mete,
-                     dramp_extflux=f.dramp_extflux)
+                     dramp_extflux=f.dramp_extflux, flux_settling_time=f.flux_settling_time)
     tides = [(float(f.amig[k]), float(f.face[k]), float(f.ff[k]), f.emo[k].copy(), f.efa[k].copy())
              for k in range(f.nbfr)]
     case = build_case(raw, params, sched, tides, cf=f.tau if f.nolibf == 0 else f.cf, tau0=f.tau0,
@@ -421,7 +441,7 @@ def case_from_files(fort14, fort15, vortex: "Vortex | None" = None,
         f = adcirc_io.read_fort15(fort15, neta, lbc)      # flux records on the case's NVEL order
         fper = np.where(f.famig != 0.0, 2.0 * math.pi / np.where(f.famig != 0.0, f.famig, 1.0), 0.0)
         case.flux = Flux(f.famig.copy(), fper, f.fff.copy(), f.fface.copy(), f.qnam.copy(),
-                         f.qnph.copy())
+                         f.qnph.copy(), flux_settling_it=sched.flux_settling_it)
     if abs(f.nws) == 8:
         case.vortex = vortex
     case.meta["fort15"] = f
@@ -449,6 +469,7 @@ def fort15_for_case(case: Case, rnday: float = 1.0, rundes: str = "", runid: str
     o.nramp = 0 if s.nramp == 0 else 8
     o.dramp = o.dramp_intflux = o.dramp_elev = o.dramp_tip = o.dramp_wrad = s.dramp
     o.dramp_extflux = s.dramp if s.dramp_extflux is None else s.dramp_extflux
+    o.flux_settling_time = s.flux_settling_time
     o.dramp_mete, o.dunramp_mete = s.dramp_mete, s.dunramp_mete
     o.a00, o.b00, o.c00, o.h0, o.velmin = p["a00"], p["b00"], p["c00"], p["h0"], p["velmin"]
     o.nodedrymin, o.nodewetmin = 0, 0
@@ -483,13 +504,15 @@ K1_PERIOD = 86164.0
 
 def channel_case(dt: float = 5.0, amp: float = 0.5, vortex: bool = False,
                  river: float | None = None, river_type: int = 2, radiation: bool = False,
-                 prep: MeshPrep | None = None, **kw) -> Case:
+                 flux_settling: float = 0.0, prep: MeshPrep | None = None, **kw) -> Case:
     """Tidal channel: 121x41 nodes, 20 m -> 5 m, M2 0.5 m, dt 5 s.  With
     `vortex`, a small Holland vortex (Rmax 8 km) crosses the channel.  With
     `river` [m^2/s per unit width], the closed east end becomes a
     specified-flux boundary (IBTYPE `river_type`, 2 or 22) carrying that
-    steady inflow, ramped in over 0.02 days.  With `radiation`, the east end
-    is a radiation boundary (IBTYPE 30) the tide leaves through."""
+    steady inflow, ramped in over 0.02 days; IBTYPE 52 (river radiation)
+    with `flux_settling` > 0 [days] holds the tide until the river flux has
+    settled (NRAMP 2).  With `radiation`, the east end is a radiation
+    boundary (IBTYPE 30) the tide leaves through."""
     from .meshgen import channel_mesh
     raw = channel_mesh()
     if river is not None or radiation:
@@ -504,14 +527,16 @@ def channel_case(dt: float = 5.0, amp: float = 0.5, vortex: bool = False,
     if vortex:
         kw.setdefault("nws", 8)
     params = default_params(dt, **kw)
-    sched = Schedule(dt=dt, dramp=0.5, dramp_mete=0.02 if vortex else 0.5, dramp_extflux=0.02)
+    sched = Schedule(dt=dt, dramp=0.5, dramp_mete=0.02 if vortex else 0.5, dramp_extflux=0.02,
+                     nramp=2 if flux_settling > 0 else 1, flux_settling_time=flux_settling)
     case = build_case(raw, params, sched, tides, prep=prep)
     if river is not None:
         lbc = case.arrays["lbcodei"]
         nv = lbc.size
         qnam = np.zeros((1, nv))
-        qnam[0, (lbc == 2) | (lbc == 12) | (lbc == 22)] = river
-        case.flux = Flux(np.zeros(1), np.zeros(1), np.ones(1), np.zeros(1), qnam, np.zeros((1, nv)))
+        qnam[0, (lbc == 2) | (lbc == 12) | (lbc == 22) | (lbc == 52)] = river
+        case.flux = Flux(np.zeros(1), np.zeros(1), np.ones(1), np.zeros(1), qnam, np.zeros((1, nv)),
+                         flux_settling_it=sched.flux_settling_it)
     if vortex:
         case.vortex = straight_track(30.3e3, 3.7e3, 80.0, 6.0, 960.0, 8.0, 1.3, hours=12.0,
                                      interval_h=3.0)

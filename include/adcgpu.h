@@ -107,11 +107,14 @@ typedef struct {
   double rampextflux;    /* RampExtFlux, the ramp of specified boundary fluxes */
 } adc_step_t;
 
-/* Periodic specified normal flux on flux boundaries (IBTYPE 2, 12, 22):
+/* Periodic specified normal flux on flux boundaries (IBTYPE 2, 12, 22, 52):
  * the fort.15 flux constituents timestep.F:861-880 sums each step. */
 typedef struct {
   int nffr;              /* NFFR > 0 constituents */
-  int pad_;
+  int flux_settling_it;  /* FluxSettlingIT = INT(FluxSettlingTime*86400/DTDP),
+                            timestep.F:243-245: river-radiation (IBTYPE 52) entries
+                            take their discharge elevation at this step and add
+                            the radiation term after it (gwce.F:1805-1815) */
   const double *famig;   /* FAMIG(NFFR), rad/s */
   const double *fper;    /* FPER(NFFR), s (0: no whole-period removal) */
   const double *fff;     /* FFF(NFFR), nodal factors */
@@ -374,7 +377,11 @@ int adc_selftest_div_const(long long n, unsigned long long seed, long long *mism
  * has no flux boundary or nffr < 1.  Radiation boundaries (IBTYPE 30) need
  * no call: every step takes their discharge from the latest velocity
  * (timestep.F:932-940) and the GWCE boundary integral the radiation force
- * (gwce.F:1783-1790); codes 32, 40, 41, 52 and 64 are refused at bind with
+ * (gwce.F:1783-1790).  River-radiation entries (IBTYPE 52) take the flux
+ * constituents of this call and, after flux_settling_it, the radiation term
+ * against the discharge elevation of that step (gwce.F:1805-1815); the
+ * flux-settling ramps themselves are the caller's adc_step_t values
+ * (timestep.F:314-345).  Codes 32, 40, 41 and 64 are refused at bind with
  * ADC_ERR_UNSUPPORTED. */
 int adc_set_flux(adc_ctx *ctx, const adc_flux_t *flux);
 

@@ -585,6 +585,10 @@ struct orc_model {
   /* specified normal flux: NFLUXF, the constituents and QN0/QN1/QN2 (NVEL) */
   int nfluxf = 0, flux_on = 0, nffr = 0;
   int nfluxrbc = 0;   /* radiation (IBTYPE 30) entries, mesh.F:2045 */
+  /* river radiation (IBTYPE 52): FluxSettlingIT, EtaDisc_Fill and
+   * EtaDisc/ElevDisc at the boundary entries (timestep.F:183, 243-245) */
+  int flux_settling_it = 0, etadisc_fill = 1;
+  std::vector<double> elevdisc, etadisc_b;
   std::vector<double> famig, fper, fff, fface, qnam, qnph, qn0, qn1, qn2;
   int vortex_on = 0;
   orc_vortex_t vpar;
@@ -640,9 +644,14 @@ orc_model *orc_model_create(const orc_params_t *p, orc_arrays_t *a) {
   /* NFLUXF, mesh.F:1907 etc.: any specified-flux segment */
   for (int I = 0; I < a->nvel; ++I) {
     const int lb = a->lbcodei[I];
-    if (lb == 2 || lb == 12 || lb == 22) m->nfluxf = 1;
+    if (lb == 2 || lb == 12 || lb == 22 || lb == 52) m->nfluxf = 1;
     if (lb == 30) m->nfluxrbc = 1;
   }
+  /* EtaDisc at river-radiation nodes from the cold-start ETA2, cstart.F:1186-1191 */
+  m->elevdisc.assign(std::max(a->nvel, 1), 0.0);
+  m->etadisc_b.assign(std::max(a->nvel, 1), 0.0);
+  for (int I = 0; I < a->nvel; ++I)
+    if (a->lbcodei[I] == 52) m->etadisc_b[I] = a->eta2[a->nbv[I] - 1];
   m->qn0.assign(std::max(a->nvel, 1), 0.0);
   m->qn1 = m->qn0;
   m->qn2 = m->qn0;
@@ -722,33 +731,51 @@ int orc_model_set_flux(orc_model *m, const orc_flux_t *f) {
   m->fface.assign(f->fface, f->fface + nf);
   m->qnam.assign(f->qnam, f->qnam + (size_t)nf * nv);
   m->qnph.assign(f->qnph, f->qnph + (size_t)nf * nv);
+  m->flux_settling_it = f->flux_settling_it;
   m->flux_on = 1;
   return 0;
 }
 
 /* periodic specified normal flux, timestep.F:861-880 (ICS = 1: no rotation),
- * then the discharge at radiation entries, timestep.F:932-940 */
+ * the discharge elevation of river-radiation entries, :906-926, then the
+ * discharge at radiation entries, timestep.F:932-940 */
 static void orc_model_flux(orc_model *m, const orc_step_t *s) {
   orc_arrays_t *a = m->a;
+  if (m->nfluxf && m->flux_on) {
+    for (int J = 0; J < m->nffr; ++J) {
+      int NCYC = 0;
+      if (m->fper[J] != 0.0) NCYC = (int)(s->timeh / m->fper[J]);
+      const double ARGJ = m->famig[J] * (s->timeh - NCYC * m->fper[J]) + m->fface[J];
+      const double RFF = m->fff[J] * s->rampextflux;
+      for (int I = 0; I < a->nvel; ++I) {
+        const int lb = a->lbcodei[I];
+        if (lb == 2 || lb == 12 || lb == 22 || lb == 52)
+          m->qn2[I] = m->qn2[I] + m->qnam[J + (size_t)m->nffr * I] * RFF *
+                                      std::cos(ARGJ - m->qnph[J + (size_t)m->nffr * I]);
+      }
+    }
+  }
+  if (m->nfluxf) {
+    if (s->it == m->flux_settling_it) {
+      m->etadisc_fill = 0;
+      for (int I = 0; I < a->nvel; ++I)
+        if (a->lbcodei[I] == 52) {
+          const int NNBB = a->nbv[I] - 1;
+          m->etadisc_b[I] = a->eta2[NNBB];
+          m->elevdisc[I] = a->eta2[NNBB];
+        }
+    } else if (m->etadisc_fill && s->it > m->flux_settling_it) {
+      m->etadisc_fill = 0;
+      for (int I = 0; I < a->nvel; ++I)
+        if (a->lbcodei[I] == 52) m->elevdisc[I] = m->etadisc_b[I];
+    }
+  }
   if (m->nfluxrbc) {
     for (int I = 0; I < a->nvel; ++I) {
       if (a->lbcodei[I] != 30) continue;
       const int NNBB = a->nbv[I] - 1;
       const double UN1 = a->uu1[NNBB] * a->csii[I] + a->vv1[NNBB] * a->siii[I];
       m->qn1[I] = a->h2[NNBB] * UN1;
-    }
-  }
-  if (!m->nfluxf || !m->flux_on) return;
-  for (int J = 0; J < m->nffr; ++J) {
-    int NCYC = 0;
-    if (m->fper[J] != 0.0) NCYC = (int)(s->timeh / m->fper[J]);
-    const double ARGJ = m->famig[J] * (s->timeh - NCYC * m->fper[J]) + m->fface[J];
-    const double RFF = m->fff[J] * s->rampextflux;
-    for (int I = 0; I < a->nvel; ++I) {
-      const int lb = a->lbcodei[I];
-      if (lb == 2 || lb == 12 || lb == 22)
-        m->qn2[I] = m->qn2[I] + m->qnam[J + (size_t)m->nffr * I] * RFF *
-                                    std::cos(ARGJ - m->qnph[J + (size_t)m->nffr * I]);
     }
   }
 }
@@ -962,8 +989,8 @@ int orc_model_gwce(orc_model *m, const orc_step_t *s, orc_stepout_t *out) {
       a->eta2[b] = a->eta2[b] + a->emo[J + (size_t)a->nbfr * I] * RFF * std::cos(ARG);
     }
   }
-  /* boundary flux integral, gwce.F:1737-1834 (LBCODEI <= 29 types and
-   * radiation, 30, with the H1 saved above) */
+  /* boundary flux integral, gwce.F:1737-1834 (LBCODEI <= 29 types,
+   * radiation 30 and river radiation 52, with the H1 saved above) */
   if (m->nfluxf || m->nfluxrbc) {
     const double DT2 = p.dt * 2.0;
     auto qforce = [&](int J, int NBDJ) {
@@ -971,7 +998,13 @@ int orc_model_gwce(orc_model *m, const orc_step_t *s, orc_stepout_t *out) {
         const double CELERITY = std::sqrt(G * a->h1[NBDJ]);
         return -CELERITY * a->etas[NBDJ] / DT - a->tau0var[NBDJ] * m->qn1[J];
       }
-      return (m->qn2[J] - m->qn0[J]) / DT2 + a->tau0var[NBDJ] * m->qn1[J];
+      double QforceJ = (m->qn2[J] - m->qn0[J]) / DT2 + a->tau0var[NBDJ] * m->qn1[J];
+      if (a->lbcodei[J] == 52 && s->it > m->flux_settling_it) {
+        const double Celerity = std::sqrt(G * a->h1[NBDJ]);
+        QforceJ = QforceJ - Celerity * (a->etas[NBDJ] / DT +
+                                        a->tau0var[NBDJ] * (a->eta1[NBDJ] - m->elevdisc[J]));
+      }
+      return QforceJ;
     };
     int NBDJ = a->nbv[0] - 1;
     double QFORCEJ = qforce(0, NBDJ);

@@ -87,7 +87,7 @@ typedef struct {
 
 /* Periodic specified normal flux (same layout as adc_flux_t). */
 typedef struct {
-  int nffr, pad_;
+  int nffr, flux_settling_it;
   const double *famig, *fper, *fff, *fface, *qnam, *qnph;
 } orc_flux_t;
 

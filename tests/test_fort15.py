@@ -200,3 +200,24 @@ def test_case_from_files_refuses_uncovered_runs(lib, tmp_path):
     adcirc_io.write_fort15(tmp_path / "fort.15", f, c.sizes["neta"], c.arrays["lbcodei"][:c.sizes["nvel"]])
     with pytest.raises(NotImplementedError, match="ICS = 2.*NCOR = 1"):
         model.case_from_files(tmp_path / "fort.14", tmp_path / "fort.15")
+
+
+def test_river_radiation_case_through_files(lib, orc, tmp_path):
+    """IBTYPE 52 with a flux settling time: NRAMP, FluxSettlingTime and the
+    river flux records survive the files, and the oracle steps both cases
+    (through the settling and after it) to the same state."""
+    import oracle
+    c = model.channel_case(river=0.5, river_type=52, flux_settling=0.02)
+    adcirc_io.write_fort14(c.meta["raw"], tmp_path / "fort.14")
+    adcirc_io.write_fort15(tmp_path / "fort.15", model.fort15_for_case(c), c.sizes["neta"],
+                           c.arrays["lbcodei"][:c.sizes["nvel"]])
+    c2 = model.case_from_files(tmp_path / "fort.14", tmp_path / "fort.15")
+    assert c2.flux.flux_settling_it == c.flux.flux_settling_it == 345
+    assert c2.schedule.flux_settling_time == c.schedule.flux_settling_time
+    for k, v in c.arrays.items():
+        assert np.array_equal(v, c2.arrays[k]), k
+    for case in (c, c2):
+        om = oracle.OracleModel(case)
+        om.run(1, 500)
+        om.close()
+    assert np.array_equal(c.arrays["eta2"], c2.arrays["eta2"])

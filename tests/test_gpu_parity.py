@@ -238,3 +238,18 @@ def test_channel_radiation_boundary(lib, orc):
     a = c0.arrays
     east = a["x"] > 59.9e3
     assert a["uu2"][east].mean() > 0.02   # the tide leaves through the boundary
+
+
+def test_channel_river_radiation(lib, orc):
+    """A river-radiation boundary (IBTYPE 52) with a flux settling time: the
+    tide waits for the river flux to settle (NRAMP 2, timestep.F:314-345),
+    the discharge elevation is taken at FluxSettlingIT (timestep.F:906-926)
+    and the radiation term joins the specified flux after it (gwce.F:
+    1805-1815), against the oracle over a graph-replayed run."""
+    from adcirc_b200 import model
+    c0, cg, io, ig = _pair(lambda **k: model.channel_case(river=0.5, river_type=52, flux_settling=0.02,
+                                                          **k), 800, use_run=True)
+    _check(c0, cg, io, ig)
+    a = c0.arrays
+    east = a["x"] > 59.9e3
+    assert a["uu2"][east].mean() < -0.02   # the river enters

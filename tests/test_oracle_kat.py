@@ -74,3 +74,24 @@ def test_quarter_annulus_matches_the_analytic_tide(orc):
     (a0, p0), (a1, p1) = errs
     assert a1 <= 5e-3 and p1 <= 0.5, errs
     assert a1 < a0 and p1 < p0, errs
+
+
+def test_river_radiation_settles_and_holds_the_discharge_level(orc):
+    """River radiation (IBTYPE 52): before FluxSettlingIT only the river
+    flux drives the channel (the tide is held at zero), the discharge
+    elevation is then fixed, and afterwards the boundary keeps carrying the
+    river inflow while the tide comes in."""
+    from adcirc_b200 import model
+    c = model.channel_case(river=0.5, river_type=52, flux_settling=0.02, prep=orc.mesh_prep())
+    fsit = c.flux.flux_settling_it
+    a = c.arrays
+    open_nodes = a["nbd"] - 1
+    om = orc.OracleModel(c)
+    om.run(1, fsit)
+    assert np.abs(a["eta2"][open_nodes]).max() == 0.0     # no tide while settling
+    east = a["x"] > 59.9e3
+    assert a["uu2"][east].mean() < -0.02                  # the river flows in
+    om.run(fsit + 1, 800)
+    om.close()
+    assert np.abs(a["eta2"][open_nodes]).max() > 0.01     # the tide has started
+    assert a["uu2"][east].mean() < -0.02 and np.isfinite(a["eta2"]).all()

@@ -20,10 +20,12 @@ def _cases(orc):
     yield "river2", lambda **k: model.channel_case(river=0.5, river_type=2, **k)
     yield "river22", lambda **k: model.channel_case(river=0.5, river_type=22, **k)
     yield "radiation", lambda **k: model.channel_case(radiation=True, **k)
+    yield "river52", lambda **k: model.channel_case(river=0.5, river_type=52, flux_settling=0.02, **k)
     yield "surge30k", lambda **k: model.surge_case(target_nodes=30_000, **k)
 
 
-@pytest.mark.parametrize("name", ["channel", "beach", "river2", "river22", "radiation", "surge30k"])
+@pytest.mark.parametrize("name", ["channel", "beach", "river2", "river22", "radiation", "river52",
+                                  "surge30k"])
 def test_case_tables_match(lib, orc, name):
     fn = dict(_cases(orc))[name]
     a = fn()
