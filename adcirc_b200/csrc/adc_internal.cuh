@@ -125,6 +125,10 @@ struct adc_ctx {
   // specified normal flux (flux.cu)
   int nfluxf, flux_on, nffr, n_fx;
   int nfluxrbc;          // radiation (IBTYPE 30) entries present
+  int nfluxgbc;          // zero-normal-gradient (IBTYPE 40) entries present
+  int n_zng;             // IBTYPE 40 momentum entries, in ME2GW order:
+  int *zng_node, *zng_ele;   //   boundary node, NEleZNG (0-based)
+  double *zng_f;             //   ZNGIF1-3 (3 per entry)
   int flux_settling_it;  // FluxSettlingIT (river radiation, IBTYPE 52)
   double *elevdisc;      // ElevDisc per boundary entry (IBTYPE 52)
   double *etadisc_b;     // EtaDisc at the boundary entries' nodes

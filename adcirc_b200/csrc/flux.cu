@@ -1,11 +1,13 @@
 // flux.cu -- specified normal flux boundaries (IBTYPE 2, 12, 22), radiation
-// boundaries (IBTYPE 30) and river-radiation boundaries (IBTYPE 52).
+// boundaries (IBTYPE 30), zero-normal-gradient boundaries (IBTYPE 40) and
+// river-radiation boundaries (IBTYPE 52).
 //
 // Three pieces of the reference's flux-boundary path:
 //  * QN0 <- QN1 <- QN2 <- 0 (timestep.F:606-613), then QN2 as the sum of the
 //    periodic flux constituents (timestep.F:861-880; ICS = 1, so the normal
 //    flux is not rotated), and at radiation entries QN1 = H2 (UU1 CSII +
-//    VV1 SIII), the discharge of the latest velocity (timestep.F:932-940);
+//    VV1 SIII), the discharge of the latest velocity (timestep.F:932-940),
+//    and the same at zero-normal-gradient entries (:945-952);
 //    river-radiation entries take their discharge elevation ElevDisc at
 //    FluxSettlingIT (or from the cold-start EtaDisc, timestep.F:906-926);
 //  * the GWCE boundary line integral (gwce.F:1737-1834): a force per
@@ -58,7 +60,7 @@ __global__ void k_flux_forcing(adc_ctx c, const adc_step_t *steps, const Flags *
       c.elevdisc[I] = c.etadisc_b[I];
     }
   }
-  if (lb == 30) {
+  if (lb == 30 || lb == 40) {
     const int n = c.bnv[I];
     const double UN1 = c.uu1[n] * c.bcsii[I] + c.vv1[n] * c.bsiii[I];
     qn1[I] = c.h2[n] * UN1;
@@ -78,6 +80,10 @@ __global__ void k_flux_qforce(adc_ctx c, const adc_step_t *steps, Flags *flags) 
   if (J >= c.nvel) return;
   const double *qn0 = c.qn, *qn1 = c.qn + c.nvel, *qn2 = c.qn + 2 * c.nvel;
   const int n = c.bnv[J];
+  if (c.blbc[J] == 40) {   // gwce.F:1804-1805
+    c.qforce[J] = -(qn1[J] - qn0[J]) / c.p.dt - c.tau0[n] * (qn1[J] + qn0[J]) / 2.0;
+    return;
+  }
   if (c.blbc[J] == 30) {
     const double CELERITY = sqrt(c.p.g * c.h1[n]);
     c.qforce[J] = -CELERITY * c.etas[n] / c.p.dt - c.tau0[n] * qn1[J];
@@ -111,14 +117,14 @@ __global__ void k_flux_rhs(adc_ctx c) {
 }
 
 int launch_flux_forcing(adc_ctx *c) {
-  if (!c->nfluxf && !c->nfluxrbc) return ADC_OK;
+  if (!c->nfluxf && !c->nfluxrbc && !c->nfluxgbc) return ADC_OK;
   launch_k(k_flux_forcing, nblk(c->nvel), kThreads, c->stream, *c, c->steps, c->flags);
   c->launches++;
   return ADC_OK;
 }
 
 int launch_flux_rhs(adc_ctx *c) {
-  if (!c->nfluxf && !c->nfluxrbc) return ADC_OK;
+  if (!c->nfluxf && !c->nfluxrbc && !c->nfluxgbc) return ADC_OK;
   launch_k(k_flux_qforce, nblk(c->nvel), kThreads, c->stream, *c, c->steps, c->flags);
   launch_k(k_flux_rhs, nblk(c->n_fx), kThreads, c->stream, *c);
   c->launches += 2;
@@ -132,11 +138,13 @@ int flux_tables(adc_ctx *c, const adc_arrays_t *a) {
   c->nvel = nv;
   c->nfluxf = 0;
   c->nfluxrbc = 0;
+  c->nfluxgbc = 0;
   for (int I = 0; I < nv; ++I) {
     const int lb = a->lbcodei[I];
     if (lb == 2 || lb == 12 || lb == 22 || lb == 52) c->nfluxf = 1;
     if (lb == 30) c->nfluxrbc = 1;
-    if (lb == 32 || lb == 40 || lb == 41 || lb == 64) {
+    if (lb == 40) c->nfluxgbc = 1;
+    if (lb == 32 || lb == 41 || lb == 64) {
       set_error("boundary code %d (zero-gradient or river-radiation flux) is not implemented", lb);
       return ADC_ERR_UNSUPPORTED;
     }
@@ -144,7 +152,7 @@ int flux_tables(adc_ctx *c, const adc_arrays_t *a) {
   const size_t nva = (size_t)(nv > 0 ? nv : 1);
   ADC_CUDA(cudaMalloc((void **)&c->qn, 3 * nva * sizeof(double)));
   ADC_CUDA(cudaMemset(c->qn, 0, 3 * nva * sizeof(double)));
-  if (!c->nfluxf && !c->nfluxrbc) return ADC_OK;
+  if (!c->nfluxf && !c->nfluxrbc && !c->nfluxgbc) return ADC_OK;
   std::vector<int> bnv(nv);
   for (int I = 0; I < nv; ++I) bnv[I] = a->nbv[I] - 1;
   std::vector<std::vector<int>> lists(c->np);
@@ -190,6 +198,28 @@ int flux_tables(adc_ctx *c, const adc_arrays_t *a) {
   ADC_CUDA(cudaMemcpy(c->etadisc_b, ed.data(), nva * sizeof(double), cudaMemcpyHostToDevice));
   ADC_CUDA(cudaMalloc((void **)&c->elevdisc, nva * sizeof(double)));
   ADC_CUDA(cudaMemset(c->elevdisc, 0, nva * sizeof(double)));
+  // zero-normal-gradient entries in ME2GW order (momentum.F:1157-1174)
+  std::vector<int> zn, ze;
+  std::vector<double> zf;
+  for (int J = 0; J < a->nvelme; ++J) {
+    const int I = a->me2gw[J] - 1;
+    if (I < 0 || I >= nv || a->lbcodei[I] != 40) continue;
+    if (!a->nelezng || a->nelezng[I] < 1 || a->nelezng[I] > c->ne) {
+      set_error("NEleZNG of boundary entry %d is missing or out of range", I + 1);
+      return ADC_ERR_MESH;
+    }
+    zn.push_back(bnv[I]);
+    ze.push_back(a->nelezng[I] - 1);
+    zf.push_back(a->zngif1[I]);
+    zf.push_back(a->zngif2[I]);
+    zf.push_back(a->zngif3[I]);
+  }
+  c->n_zng = (int)zn.size();
+  if ((rc = up_i(&c->zng_node, zn))) return rc;
+  if ((rc = up_i(&c->zng_ele, ze))) return rc;
+  ADC_CUDA(cudaMalloc((void **)&c->zng_f, std::max<size_t>(zf.size(), 1) * sizeof(double)));
+  if (!zf.empty())
+    ADC_CUDA(cudaMemcpy(c->zng_f, zf.data(), zf.size() * sizeof(double), cudaMemcpyHostToDevice));
   return ADC_OK;
 }
 

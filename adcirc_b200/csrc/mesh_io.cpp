@@ -7,8 +7,8 @@
 // fort.14 node numbers may be any labels; as read14 does, they are mapped
 // to 1..NP in file order and element and boundary references go through
 // that map.  Boundary segments of the types the 2DDI hot path handles
-// (one node per line: IBTYPE 0, 1, 2, 10, 11, 12, 20, 21, 22, 30, 32, 52,
-// 102, 112, 122, 152) are returned; barrier types (3, 4, 5 families) and
+// (one node per line: IBTYPE 0, 1, 2, 10, 11, 12, 20, 21, 22, 30, 32, 40,
+// 41, 52, 102, 112, 122, 152) are returned; barrier types (3, 4, 5 families) and
 // periodic segments (94) return ADC_ERR_UNSUPPORTED.
 #include <cerrno>
 #include <cmath>
@@ -100,7 +100,7 @@ struct Reader {
 bool simple_flux_type(long long t) {
   switch (t) {
     case 0: case 1: case 2: case 10: case 11: case 12: case 20: case 21: case 22: case 30:
-    case 32: case 52: case 102: case 112: case 122: case 152:
+    case 32: case 40: case 41: case 52: case 102: case 112: case 122: case 152:
       return true;
     default:
       return false;

@@ -12,6 +12,7 @@
  *   adc_mesh_neighb        mesh.F:3089-3318   NeiTab sorted by angle, NNeigh
  *   adc_mesh_csr_positions mesh.F:5261-5282   CSR_POSITION(NE,3,2)
  *   adc_boundary_setup     mesh.F:2100-2800   NBV, LBCODEI, CSII, SIII, ME2GW, BNDLEN2O3
+ *   adc_zng_setup          mesh.F:2434-2512   NEleZNG, ZNGIF1-3 (IBTYPE 40)
  *
  * All arrays use the reference layout: column-major, 1-based node numbers.
  */
@@ -167,8 +168,9 @@ int adc_mesh_csr_positions(int np, int ne, int mnei, const int *nm, const int *n
 
 /*
  * Flow-boundary arrays for external land segments (IBTYPE 0, 10, 20),
- * islands (IBTYPE 1, 11, 21), specified-flow (2, 12, 22), radiation (30)
- * and river-radiation (52) segments, mesh.F:2180-2800.  seg_ptr[k]..seg_ptr[k+1]-1
+ * islands (IBTYPE 1, 11, 21), specified-flow (2, 12, 22), radiation (30),
+ * zero-normal-gradient (40) and river-radiation (52) segments,
+ * mesh.F:2180-2800.  seg_ptr[k]..seg_ptr[k+1]-1
  * index seg_nodes (1-based node numbers, as listed in fort.14).  Outputs are
  * sized by the caller for nvel_max entries (sum of segment lengths plus one
  * per island for closing).  cos_inner = COS(ANGINN*DEG2RAD).
@@ -182,7 +184,7 @@ int adc_boundary_setup(int np, const double *x, const double *y, int nbou,
   /* flow types (specified flow, radiation) take the momentum equation
      where segments overlap (mesh.F:2529-2541, 2555-2566) */
   auto specified_flow = [](int code) {
-    return code == 2 || code == 12 || code == 22 || code == 30 || code == 52;
+    return code == 2 || code == 12 || code == 22 || code == 30 || code == 40 || code == 52;
   };
   for (int k = 0; k < nbou; ++k) {
     int t = ibtype[k];
@@ -278,6 +280,64 @@ int adc_boundary_setup(int np, const double *x, const double *y, int nbou,
   return ADC_OK;
 }
 
+
+/*
+ * Fictitious interior nodes of the zero-normal-velocity-gradient entries
+ * (IBTYPE 40), mesh.F:2434-2512.  For each such boundary entry: a point
+ * inward along the entry's normal (CSII, SIII) at 1.001 times the distance
+ * to its farthest NeiTab neighbour; the element holding it, taken as the
+ * one whose three sub-triangle areas add up closest to its own area (the
+ * first such element in element order); and the point's linear
+ * interpolation factors in that element.  Entries of other types get
+ * NEleZNG = 0.  All node and element numbers are 1-based.
+ */
+int adc_zng_setup(int np, int ne, const double *x, const double *y, const int *nm, int mnei,
+                  const int *nneigh, const int *neitab, const double *areas, int nvel,
+                  const int *nbv, const int *lbcodei, const double *csii, const double *siii,
+                  int *nelezng, double *zngif1, double *zngif2, double *zngif3) {
+  if (np <= 0 || ne <= 0 || nvel < 0) return ADC_ERR_ARG;
+  auto N = [&](int ie, int k) { return nm[ie + (size_t)ne * k] - 1; };
+  for (int j = 0; j < nvel; ++j) {
+    nelezng[j] = 0;
+    zngif1[j] = zngif2[j] = zngif3[j] = 0.0;
+    if (lbcodei[j] != 40) continue;
+    const int i = nbv[j] - 1;
+    if (i < 0 || i >= np) return ADC_ERR_ARG;
+    double dist = 0.0;
+    for (int q = 2; q <= nneigh[i] && q <= mnei; ++q) {
+      const int nb = neitab[i + (size_t)np * (q - 1)] - 1;
+      if (nb < 0 || nb >= np) return ADC_ERR_ARG;
+      const double dx = x[nb] - x[i], dy = y[nb] - y[i];
+      const double d = std::sqrt(dx * dx + dy * dy);
+      if (dist < d) dist = d;
+    }
+    dist = 1.001 * dist;
+    const double x4 = x[i] - dist * csii[j], y4 = y[i] - dist * siii[j];
+    double best = (double)1.0e25f;   /* AEMIN = 1.0E+25, a default-kind REAL */
+    int ele = -1;
+    for (int e = 0; e < ne; ++e) {
+      const int a = N(e, 0), b = N(e, 1), c = N(e, 2);
+      const double x1 = x[a], x2 = x[b], x3 = x[c], y1 = y[a], y2 = y[b], y3 = y[c];
+      const double A1 = (x4 - x3) * (y2 - y3) + (x2 - x3) * (y3 - y4);
+      const double A2 = (x4 - x1) * (y3 - y1) - (y4 - y1) * (x3 - x1);
+      const double A3 = (y4 - y1) * (x2 - x1) - (x4 - x1) * (y2 - y1);
+      const double AA = std::fabs(A1) + std::fabs(A2) + std::fabs(A3);
+      const double AE = std::fabs(AA - areas[e]) / areas[e];
+      if (AE < best) {
+        best = AE;
+        ele = e;
+      }
+    }
+    if (ele < 0) return ADC_ERR_MESH;
+    const int a = N(ele, 0), b = N(ele, 1), c = N(ele, 2);
+    const double x1 = x[a], x2 = x[b], x3 = x[c], y1 = y[a], y2 = y[b], y3 = y[c];
+    nelezng[j] = ele + 1;
+    zngif1[j] = ((x4 - x3) * (y2 - y3) + (x2 - x3) * (y3 - y4)) / areas[ele];
+    zngif2[j] = ((x4 - x1) * (y3 - y1) - (y4 - y1) * (x3 - x1)) / areas[ele];
+    zngif3[j] = (-(x4 - x1) * (y2 - y1) + (y4 - y1) * (x2 - x1)) / areas[ele];
+  }
+  return ADC_OK;
+}
 } /* extern "C" */
 
 extern "C" {

@@ -1,6 +1,7 @@
 // momentum.cu -- Mom_Eqs_New_NC (momentum.F:166-1208): lumped explicit
 // non-conservative 2DDI momentum with IBPV lateral stress and corrected
-// area integration, land boundary codes 0-19, Cartesian coordinates.
+// area integration, land boundary codes 0-19 and the zero normal velocity
+// gradient of code 40, Cartesian coordinates.
 //
 // Two kernels: an element kernel forms the six load-vector contributions
 // (momentum.F:298-699); a node kernel gathers them in element order, forms
@@ -224,6 +225,28 @@ __global__ void k_mom_node(adc_ctx c) {
   c.qy2[i] = v2 * h2;
 }
 
+// Zero normal velocity gradient (IBTYPE 40), momentum.F:1157-1174: after
+// the nodal solve each such boundary node takes the velocity interpolated
+// at its fictitious interior node, then its fluxes (:1179-1182).  The
+// entries go in ME2GW order on one thread, since an entry's element may
+// hold a node an earlier entry has just set.
+__global__ void k_mom_zng(adc_ctx c) {
+  griddep_wait();
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  for (int k = 0; k < c.n_zng; ++k) {
+    const int n = c.zng_node[k], e = c.zng_ele[k];
+    const int NM1 = c.nm[3 * e], NM2 = c.nm[3 * e + 1], NM3 = c.nm[3 * e + 2];
+    const int NCEle = c.nodecode[NM1] * c.nodecode[NM2] * c.nodecode[NM3] * c.noff[e];
+    const double f1 = c.zng_f[3 * k], f2 = c.zng_f[3 * k + 1], f3 = c.zng_f[3 * k + 2];
+    const double u = NCEle * (c.uu2[NM1] * f1 + c.uu2[NM2] * f2 + c.uu2[NM3] * f3);
+    const double v = NCEle * (c.vv2[NM1] * f1 + c.vv2[NM2] * f2 + c.vv2[NM3] * f3);
+    c.uu2[n] = u;
+    c.vv2[n] = v;
+    c.qx2[n] = u * c.h2[n];
+    c.qy2[n] = v * c.h2[n];
+  }
+}
+
 int launch_momentum(adc_ctx *c) {
   kmark(c, KS_MOM_ELEM, 0);
   if (f32_momentum(c)) {   // FP32 element terms and their gather
@@ -236,6 +259,10 @@ int launch_momentum(adc_ctx *c) {
     kmark(c, KS_MOM_ELEM, 1);
     kmark(c, KS_MOM_NODE, 0);
     launch_k(k_mom_node<double>, nblk(c->np), kThreads, c->stream, *c);
+  }
+  if (c->n_zng > 0) {
+    launch_k(k_mom_zng, 1, 32, c->stream, *c);
+    c->launches++;
   }
   kmark(c, KS_MOM_NODE, 1);
   c->launches += 2;

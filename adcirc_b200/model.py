@@ -246,12 +246,14 @@ class MeshPrep:
     csr_positions: object
     boundary_setup: object
     coldstart: object
+    zng_setup: object = None
 
 
 def product_prep() -> MeshPrep:
     lib = _lib.load()
     return MeshPrep(lib.adc_mesh_geometry, lib.adc_mesh_mnei, lib.adc_mesh_neighb,
-                    lib.adc_mesh_csr_positions, lib.adc_boundary_setup, lib.adc_coldstart)
+                    lib.adc_mesh_csr_positions, lib.adc_boundary_setup, lib.adc_coldstart,
+                    lib.adc_zng_setup)
 
 
 def build_case(raw, params: dict, schedule: Schedule, tides, cf: float = 0.0025,
@@ -316,6 +318,19 @@ def build_case(raw, params: dict, schedule: Schedule, tides, cf: float = 0.0025,
     if rc != 0:
         raise RuntimeError(f"adc_boundary_setup failed: {rc}")
     nv, nme = nvel.value, nvelme.value
+    # zero-normal-gradient fictitious nodes (IBTYPE 40), mesh.F:2434-2512
+    nvz = max(nv, 1)
+    nelezng = np.zeros(nvz, np.int32)
+    zngif = [np.zeros(nvz) for _ in range(3)]
+    if (lbc[:nv] == 40).any():
+        if lib.zng_setup is None:
+            raise RuntimeError("the table builders have no zero-normal-gradient setup")
+        rc = lib.zng_setup(npn, ne, ptr(x, dp_), ptr(y, dp_), ptr(nm, ip_), mnei, ptr(nneigh, ip_),
+                           ptr(neitab, ip_), ptr(areas, dp_), nv, ptr(nbv, ip_), ptr(lbc, ip_),
+                           ptr(csii, dp_), ptr(siii, dp_), ptr(nelezng, ip_), ptr(zngif[0], dp_),
+                           ptr(zngif[1], dp_), ptr(zngif[2], dp_))
+        if rc != 0:
+            raise RuntimeError(f"zero-normal-gradient setup failed: {rc}")
     nbfr = len(tides)
     amig = _f([t[0] for t in tides], np.float64)
     face = _f([t[1] for t in tides], np.float64)
@@ -340,6 +355,7 @@ def build_case(raw, params: dict, schedule: Schedule, tides, cf: float = 0.0025,
         csii=_f(csii[:max(nv, 1)], np.float64), siii=_f(siii[:max(nv, 1)], np.float64),
         me2gw=_f(me2gw[:max(nme, 1)], np.int32),
         bndlen2o3=_f(bndlen[:max(nv, 1)], np.float64),
+        nelezng=nelezng, zngif1=zngif[0], zngif2=zngif[1], zngif3=zngif[2],
     )
     for k in STATE_F64:
         A[k] = np.zeros(npn, np.float64)
@@ -504,7 +520,8 @@ K1_PERIOD = 86164.0
 
 def channel_case(dt: float = 5.0, amp: float = 0.5, vortex: bool = False,
                  river: float | None = None, river_type: int = 2, radiation: bool = False,
-                 flux_settling: float = 0.0, prep: MeshPrep | None = None, **kw) -> Case:
+                 zero_gradient: bool = False, flux_settling: float = 0.0,
+                 prep: MeshPrep | None = None, **kw) -> Case:
     """Tidal channel: 121x41 nodes, 20 m -> 5 m, M2 0.5 m, dt 5 s.  With
     `vortex`, a small Holland vortex (Rmax 8 km) crosses the channel.  With
     `river` [m^2/s per unit width], the closed east end becomes a
@@ -512,16 +529,18 @@ def channel_case(dt: float = 5.0, amp: float = 0.5, vortex: bool = False,
     steady inflow, ramped in over 0.02 days; IBTYPE 52 (river radiation)
     with `flux_settling` > 0 [days] holds the tide until the river flux has
     settled (NRAMP 2).  With `radiation`, the east end is a radiation
-    boundary (IBTYPE 30) the tide leaves through."""
+    boundary (IBTYPE 30) the tide leaves through; with `zero_gradient`, a
+    zero-normal-velocity-gradient boundary (IBTYPE 40)."""
     from .meshgen import channel_mesh
     raw = channel_mesh()
-    if river is not None or radiation:
+    if river is not None or radiation or zero_gradient:
         nx, ny = 121, 41
         nid = lambda i, j: i * ny + j
         south = np.array([nid(i, 0) for i in range(nx)])
         east = np.array([nid(nx - 1, j) for j in range(ny)])
         north = np.array([nid(i, ny - 1) for i in range(nx - 1, -1, -1)])
-        raw.land_segments = [(0, south), (30 if radiation else river_type, east), (0, north)]
+        east_type = 30 if radiation else (40 if zero_gradient else river_type)
+        raw.land_segments = [(0, south), (east_type, east), (0, north)]
     neta = raw.open_nodes.size
     tides = [(2.0 * math.pi / M2_PERIOD, 0.0, 1.0, np.full(neta, amp), np.zeros(neta))]
     if vortex:

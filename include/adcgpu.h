@@ -97,6 +97,11 @@ typedef struct {
   double *coef;                  /* COEF(NP,MNEI) */
   double *obccoef;               /* OBCCoef(NETA,MNEI-1) */
   double *gwce_lv, *mom_lv_x, *mom_lv_y;
+  /* zero-normal-gradient entries (IBTYPE 40, mesh.F:2434-2512): the element
+   * holding each entry's fictitious interior node and its interpolation
+   * factors (adc_zng_setup); NEleZNG = 0 off IBTYPE 40 entries */
+  const int *nelezng;            /* NEleZNG(NVEL), 1-based */
+  const double *zngif1, *zngif2, *zngif3;   /* (NVEL) */
 } adc_arrays_t;
 
 /* Per-step scalars TIMESTEP computes before the hot path (timestep.F:257-353). */
@@ -381,8 +386,9 @@ int adc_selftest_div_const(long long n, unsigned long long seed, long long *mism
  * constituents of this call and, after flux_settling_it, the radiation term
  * against the discharge elevation of that step (gwce.F:1805-1815); the
  * flux-settling ramps themselves are the caller's adc_step_t values
- * (timestep.F:314-345).  Codes 32, 40, 41 and 64 are refused at bind with
- * ADC_ERR_UNSUPPORTED. */
+ * (timestep.F:314-345).  Zero-normal-gradient entries (IBTYPE 40) need the
+ * NEleZNG/ZNGIF tables of adc_zng_setup in adc_arrays_t.  Codes 32, 41 and
+ * 64 are refused at bind with ADC_ERR_UNSUPPORTED. */
 int adc_set_flux(adc_ctx *ctx, const adc_flux_t *flux);
 
 /* No reference counterpart (the reference always starts JCG from ETAS as
@@ -517,6 +523,12 @@ int adc_boundary_setup(int np, const double *x, const double *y, int nbou,
                        double cos_inner, int nvel_max, int *nvel, int *nbv,
                        int *lbcodei, double *csii, double *siii, int *nvelme,
                        int *me2gw, double *bndlen2o3);
+/* Zero-normal-gradient (IBTYPE 40) fictitious nodes (mesh.F:2434-2512):
+ * NEleZNG and the interpolation factors ZNGIF1-3 per boundary entry. */
+int adc_zng_setup(int np, int ne, const double *x, const double *y, const int *nm, int mnei,
+                  const int *nneigh, const int *neitab, const double *areas, int nvel,
+                  const int *nbv, const int *lbcodei, const double *csii, const double *siii,
+                  int *nelezng, double *zngif1, double *zngif2, double *zngif3);
 /* Cold-start wet/dry state (cstart.F:1332-1427) and totalAreaCalc
  * (mesh.F:3360-3400). */
 int adc_coldstart(int np, int ne, int nolifa, double h0, const double *dp, const int *nm,

@@ -33,6 +33,7 @@ module adcgpu_iface
       type(c_ptr) :: tk, tkm, nodecode, nnodecode, noff, mju, totalarea, alphal
       type(c_ptr) :: wsx1, wsy1, wsx2, wsy2, pr1, pr2, coef, obccoef
       type(c_ptr) :: gwce_lv, mom_lv_x, mom_lv_y
+      type(c_ptr) :: nelezng, zngif1, zngif2, zngif3
    end type
 
    type, bind(C), public :: adc_step_t
@@ -41,7 +42,7 @@ module adcgpu_iface
    end type
 
    type, bind(C), public :: adc_flux_t
-      integer(c_int) :: nffr, pad_
+      integer(c_int) :: nffr, flux_settling_it
       type(c_ptr) :: famig, fper, fff, fface, qnam, qnph
    end type
 

@@ -585,6 +585,7 @@ struct orc_model {
   /* specified normal flux: NFLUXF, the constituents and QN0/QN1/QN2 (NVEL) */
   int nfluxf = 0, flux_on = 0, nffr = 0;
   int nfluxrbc = 0;   /* radiation (IBTYPE 30) entries, mesh.F:2045 */
+  int nfluxgbc = 0;   /* zero normal velocity gradient (IBTYPE 40) entries, mesh.F:2072 */
   /* river radiation (IBTYPE 52): FluxSettlingIT, EtaDisc_Fill and
    * EtaDisc/ElevDisc at the boundary entries (timestep.F:183, 243-245) */
   int flux_settling_it = 0, etadisc_fill = 1;
@@ -646,6 +647,7 @@ orc_model *orc_model_create(const orc_params_t *p, orc_arrays_t *a) {
     const int lb = a->lbcodei[I];
     if (lb == 2 || lb == 12 || lb == 22 || lb == 52) m->nfluxf = 1;
     if (lb == 30) m->nfluxrbc = 1;
+    if (lb == 40) m->nfluxgbc = 1;
   }
   /* EtaDisc at river-radiation nodes from the cold-start ETA2, cstart.F:1186-1191 */
   m->elevdisc.assign(std::max(a->nvel, 1), 0.0);
@@ -776,6 +778,15 @@ static void orc_model_flux(orc_model *m, const orc_step_t *s) {
       const int NNBB = a->nbv[I] - 1;
       const double UN1 = a->uu1[NNBB] * a->csii[I] + a->vv1[NNBB] * a->siii[I];
       m->qn1[I] = a->h2[NNBB] * UN1;
+    }
+  }
+  /* zero normal velocity gradient entries, timestep.F:945-952 */
+  if (m->nfluxgbc) {
+    for (int J = 0; J < a->nvel; ++J) {
+      if (a->lbcodei[J] != 40) continue;
+      const int NNBB = a->nbv[J] - 1;
+      const double UN1 = a->uu1[NNBB] * a->csii[J] + a->vv1[NNBB] * a->siii[J];
+      m->qn1[J] = a->h2[NNBB] * UN1;
     }
   }
 }
@@ -991,9 +1002,11 @@ int orc_model_gwce(orc_model *m, const orc_step_t *s, orc_stepout_t *out) {
   }
   /* boundary flux integral, gwce.F:1737-1834 (LBCODEI <= 29 types,
    * radiation 30 and river radiation 52, with the H1 saved above) */
-  if (m->nfluxf || m->nfluxrbc) {
+  if (m->nfluxf || m->nfluxrbc || m->nfluxgbc) {
     const double DT2 = p.dt * 2.0;
     auto qforce = [&](int J, int NBDJ) {
+      if (a->lbcodei[J] == 40)   /* gwce.F:1804-1805 */
+        return -(m->qn1[J] - m->qn0[J]) / DT - a->tau0var[NBDJ] * (m->qn1[J] + m->qn0[J]) / 2.0;
       if (a->lbcodei[J] == 30) {
         const double CELERITY = std::sqrt(G * a->h1[NBDJ]);
         return -CELERITY * a->etas[NBDJ] / DT - a->tau0var[NBDJ] * m->qn1[J];
@@ -1374,6 +1387,21 @@ int orc_model_momentum(orc_model *m, const orc_step_t *s) {
     double DDU = auv[0] * auv[1] - auv[2] * auv[3];
     a->uu2[i] = (a->mom_lv_x[i] * auv[1] - a->mom_lv_y[i] * auv[2]) / DDU;
     a->vv2[i] = (a->mom_lv_y[i] * auv[0] - a->mom_lv_x[i] * auv[3]) / DDU;
+  }
+  /* zero normal velocity gradient (IBTYPE 40), momentum.F:1157-1174 */
+  if (m->nfluxgbc) {
+    for (int J = 0; J < a->nvelme; ++J) {
+      const int I = a->me2gw[J] - 1;
+      if (a->lbcodei[I] != 40) continue;
+      const int NBDI = a->nbv[I] - 1, E = a->nelezng[I] - 1;
+      const int NM1 = a->nm[E] - 1, NM2 = a->nm[E + (size_t)a->ne] - 1,
+                NM3 = a->nm[E + 2 * (size_t)a->ne] - 1;
+      const int NCEle = a->nodecode[NM1] * a->nodecode[NM2] * a->nodecode[NM3] * a->noff[E];
+      a->uu2[NBDI] = NCEle * (a->uu2[NM1] * a->zngif1[I] + a->uu2[NM2] * a->zngif2[I] +
+                              a->uu2[NM3] * a->zngif3[I]);
+      a->vv2[NBDI] = NCEle * (a->vv2[NM1] * a->zngif1[I] + a->vv2[NM2] * a->zngif2[I] +
+                              a->vv2[NM3] * a->zngif3[I]);
+    }
   }
   for (int i = 0; i < np; ++i) {
     a->qx2[i] = a->uu2[i] * a->h2[i];

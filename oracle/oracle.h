@@ -76,6 +76,8 @@ typedef struct {
   double *coef;             /* COEF(NP,MNEI) */
   double *obccoef;          /* OBCCoef(NETA,MNEI-1) */
   double *gwce_lv, *mom_lv_x, *mom_lv_y;
+  const int *nelezng;       /* NEleZNG(NVEL), 1-based (IBTYPE 40 entries) */
+  const double *zngif1, *zngif2, *zngif3;
 } orc_arrays_t;
 
 /* Per-step scalars the TIMESTEP driver computes before the hot path. */
@@ -172,6 +174,10 @@ int orc_boundary_setup(int np, const double *x, const double *y, int nbou, const
                        const int *seg_ptr, const int *seg_nodes, double costset, int nvel_max,
                        int *nvel_out, int *nbv, int *lbcodei, double *csii, double *siii,
                        int *nvelme_out, int *me2gw, double *bndlen2o3);
+int orc_zng_setup(int np, int ne, const double *x, const double *y, const int *nm, int mnei,
+                  const int *nneigh, const int *neitab, const double *areas, int nvel,
+                  const int *nbv, const int *lbcodei, const double *csii, const double *siii,
+                  int *nelezng, double *zngif1, double *zngif2, double *zngif3);
 int orc_coldstart_arrays(int np, int ne, int nolifa, double h0, const double *dp, const int *nm,
                          const double *areas, double *eta1, double *eta2, int *nnodecode,
                          int *nodecode, int *noff, int *mju, double *totalarea);

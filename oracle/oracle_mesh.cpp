@@ -18,6 +18,7 @@
  *   orc_mesh_neighb          mesh.F:3089-3318  NEIGHB: NeiTab by clockwise angle
  *   orc_mesh_csr_positions   mesh.F:5261-5282  compute_csr_positions
  *   orc_boundary_setup       mesh.F:2226-2568  NBV, LBCODEI, CSII, SIII, ME2GW, BNDLEN2O3
+ *   orc_zng_setup            mesh.F:2434-2512  NEleZNG, ZNGIF1-3 (IBTYPE 40)
  *   orc_coldstart_arrays     cstart.F:1332-1427 + totalAreaCalc mesh.F:3360-3400
  */
 #include "oracle.h"
@@ -217,7 +218,7 @@ int orc_mesh_csr_positions(int np, int ne, int mnei, const int *nm, const int *n
 
 /* Flow-boundary tables of mesh.F:2226-2568 for the land-segment types of
  * the path (external 0/10/20, island 1/11/21, specified flow 2/12/22,
- * radiation 30, river radiation 52):
+ * radiation 30, zero normal gradient 40, river radiation 52):
  * segment closure (:2226-2244), per node the GWCE entry NBV/LBCODEI with
  * the inner-angle test (:2266-2411), BNDLEN2O3 (:2301-2303), the outward
  * normal CSII/SIII (:2421-2433, including the FLG_IBLEN2 special case of a
@@ -238,7 +239,7 @@ int orc_boundary_setup(int np, const double *x, const double *y, int nbou, const
     const int t = ibtype[k];
     const bool island = (t == 1 || t == 11 || t == 21);
     if (!(island || t == 0 || t == 10 || t == 20 || t == 2 || t == 12 || t == 22 || t == 30 ||
-          t == 52))
+          t == 40 || t == 52))
       return -1;
     int nvell = seg_ptr[k + 1] - seg_ptr[k];
     if (nvell < 2) return -1;
@@ -342,6 +343,62 @@ int orc_boundary_setup(int np, const double *x, const double *y, int nbou, const
   }
   *nvel_out = jgw;
   *nvelme_out = jme;
+  return 0;
+}
+
+/* Zero-normal-gradient fictitious nodes, mesh.F:2434-2512: for each
+ * IBTYPE 40 entry JGW, ZNGFicNodeDist = 1.001 x the largest distance to the
+ * NeiTab neighbours, X4/Y4 that far inward along -(CSII, SIII), NEleZNG the
+ * element minimising |AA - AREAS|/AREAS (strict <, so the first one wins)
+ * and ZNGIF1-3 the interpolation factors. */
+int orc_zng_setup(int np, int ne, const double *x, const double *y, const int *nm, int mnei,
+                  const int *nneigh, const int *neitab, const double *areas, int nvel,
+                  const int *nbv, const int *lbcodei, const double *csii, const double *siii,
+                  int *nelezng, double *zngif1, double *zngif2, double *zngif3) {
+  if (np <= 0 || ne <= 0 || nvel < 0) return -1;
+  CI2 NM{nm, ne}, NeiTab{neitab, np};
+  auto X = [&](int n) { return x[n - 1]; };
+  auto Y = [&](int n) { return y[n - 1]; };
+  for (int JGW = 1; JGW <= nvel; ++JGW) {
+    nelezng[JGW - 1] = 0;
+    zngif1[JGW - 1] = zngif2[JGW - 1] = zngif3[JGW - 1] = 0.0;
+    if (lbcodei[JGW - 1] != 40) continue;
+    const int NBVI = nbv[JGW - 1];
+    if (NBVI < 1 || NBVI > np) return -1;
+    double ZNGFicNodeDist = 0.0;
+    for (int N = 2; N <= nneigh[NBVI - 1] && N <= mnei; ++N) {
+      const int nb = NeiTab(NBVI, N);
+      if (nb < 1 || nb > np) return -1;
+      const double ZNGFicNodeDistTemp = std::sqrt((X(nb) - X(NBVI)) * (X(nb) - X(NBVI)) +
+                                                  (Y(nb) - Y(NBVI)) * (Y(nb) - Y(NBVI)));
+      if (ZNGFicNodeDist < ZNGFicNodeDistTemp) ZNGFicNodeDist = ZNGFicNodeDistTemp;
+    }
+    ZNGFicNodeDist = 1.001 * ZNGFicNodeDist;
+    const double X4 = X(NBVI) - ZNGFicNodeDist * csii[JGW - 1];
+    const double Y4 = Y(NBVI) - ZNGFicNodeDist * siii[JGW - 1];
+    double AEMIN = (double)1.0E+25f;
+    int NEle = 0;
+    for (int N = 1; N <= ne; ++N) {
+      const int N1 = NM(N, 1), N2 = NM(N, 2), N3 = NM(N, 3);
+      const double X1 = X(N1), X2 = X(N2), X3 = X(N3), Y1 = Y(N1), Y2 = Y(N2), Y3 = Y(N3);
+      const double A1 = (X4 - X3) * (Y2 - Y3) + (X2 - X3) * (Y3 - Y4);
+      const double A2 = (X4 - X1) * (Y3 - Y1) - (Y4 - Y1) * (X3 - X1);
+      const double A3 = (Y4 - Y1) * (X2 - X1) - (X4 - X1) * (Y2 - Y1);
+      const double AA = std::fabs(A1) + std::fabs(A2) + std::fabs(A3);
+      const double AE = std::fabs(AA - areas[N - 1]) / areas[N - 1];
+      if (AE < AEMIN) {
+        AEMIN = AE;
+        NEle = N;
+      }
+    }
+    if (NEle == 0) return -1;
+    const int N1 = NM(NEle, 1), N2 = NM(NEle, 2), N3 = NM(NEle, 3);
+    const double X1 = X(N1), X2 = X(N2), X3 = X(N3), Y1 = Y(N1), Y2 = Y(N2), Y3 = Y(N3);
+    nelezng[JGW - 1] = NEle;
+    zngif1[JGW - 1] = ((X4 - X3) * (Y2 - Y3) + (X2 - X3) * (Y3 - Y4)) / areas[NEle - 1];
+    zngif2[JGW - 1] = ((X4 - X1) * (Y3 - Y1) - (Y4 - Y1) * (X3 - X1)) / areas[NEle - 1];
+    zngif3[JGW - 1] = (-(X4 - X1) * (Y2 - Y1) + (Y4 - Y1) * (X2 - X1)) / areas[NEle - 1];
+  }
   return 0;
 }
 

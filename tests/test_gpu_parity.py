@@ -253,3 +253,17 @@ def test_channel_river_radiation(lib, orc):
     a = c0.arrays
     east = a["x"] > 59.9e3
     assert a["uu2"][east].mean() < -0.02   # the river enters
+
+
+def test_channel_zero_gradient_boundary(lib, orc):
+    """A zero-normal-velocity-gradient boundary (IBTYPE 40) at the east end:
+    the discharge of the latest velocity (timestep.F:945-952), its force in
+    the GWCE boundary integral (gwce.F:1804-1805) and the interpolated
+    boundary velocity of the momentum step (momentum.F:1157-1174), against
+    the oracle over a graph-replayed run."""
+    from adcirc_b200 import model
+    c0, cg, io, ig = _pair(lambda **k: model.channel_case(zero_gradient=True, **k), 1500, use_run=True)
+    _check(c0, cg, io, ig)
+    a = c0.arrays
+    east = a["x"] > 59.9e3
+    assert a["uu2"][east].mean() > 0.02

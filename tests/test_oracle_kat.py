@@ -95,3 +95,29 @@ def test_river_radiation_settles_and_holds_the_discharge_level(orc):
     om.close()
     assert np.abs(a["eta2"][open_nodes]).max() > 0.01     # the tide has started
     assert a["uu2"][east].mean() < -0.02 and np.isfinite(a["eta2"]).all()
+
+
+def test_zero_gradient_boundary_takes_the_interior_velocity(orc):
+    """Zero normal velocity gradient (IBTYPE 40): each boundary node's
+    velocity is the one interpolated at its fictitious interior node
+    (mesh.F:2434-2512, momentum.F:1157-1174), the fictitious node lies in
+    its element (interpolation factors in [0, 1], summing to 1), and the
+    tide flows out through the boundary."""
+    from adcirc_b200 import model
+    c = model.channel_case(zero_gradient=True, prep=orc.mesh_prep())
+    a = c.arrays
+    nv = c.sizes["nvel"]
+    j = np.where(a["lbcodei"][:nv] == 40)[0]
+    f = np.stack([a["zngif1"][j], a["zngif2"][j], a["zngif3"][j]])
+    assert j.size == 41 and (f >= -1e-12).all() and np.allclose(f.sum(axis=0), 1.0, atol=1e-12)
+    om = orc.OracleModel(c)
+    om.run(1, 1500)
+    om.close()
+    e = a["nelezng"][j] - 1
+    nm = a["nm"] - 1
+    for comp in ("uu2", "vv2"):
+        v = a[comp]
+        interp = sum(v[nm[e, k]] * f[k] for k in range(3))
+        assert np.allclose(v[a["nbv"][j] - 1], interp, rtol=0, atol=1e-15)
+    east = a["x"] > 59.9e3
+    assert a["uu2"][east].mean() > 0.02

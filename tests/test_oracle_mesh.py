@@ -21,11 +21,12 @@ def _cases(orc):
     yield "river22", lambda **k: model.channel_case(river=0.5, river_type=22, **k)
     yield "radiation", lambda **k: model.channel_case(radiation=True, **k)
     yield "river52", lambda **k: model.channel_case(river=0.5, river_type=52, flux_settling=0.02, **k)
+    yield "zerograd", lambda **k: model.channel_case(zero_gradient=True, **k)
     yield "surge30k", lambda **k: model.surge_case(target_nodes=30_000, **k)
 
 
 @pytest.mark.parametrize("name", ["channel", "beach", "river2", "river22", "radiation", "river52",
-                                  "surge30k"])
+                                  "zerograd", "surge30k"])
 def test_case_tables_match(lib, orc, name):
     fn = dict(_cases(orc))[name]
     a = fn()
