@@ -328,46 +328,29 @@ __device__ __forceinline__ double rhs_field(const adc_ctx &c, int f, int n) {
   }
 }
 
-template <class R>
-__global__ void __launch_bounds__(256, sizeof(R) == 4 ? 3 : 2) k_rhs_elem(adc_ctx c) {
-  griddep_wait();
-  __shared__ R sh[kThreads / 32][32 * 3];
-  __shared__ double sv[RF_N][kTileNodes];
-  __shared__ int snc[kTileNodes];
-  const int t0 = c.et_ptr[blockIdx.x], nu = c.et_ptr[blockIdx.x + 1] - t0;
-  const bool staged = nu <= kTileNodes;
-  const bool met = c.p.nws != 0;
-  if (staged) {   // block-uniform
-    const int nf = met ? RF_N : RF_PR1;
-    for (int q = threadIdx.x; q < nf * nu; q += blockDim.x) {
-      const int f = q / nu, k = q - f * nu;
-      sv[f][k] = rhs_field(c, f, c.et_node[t0 + k]);
-    }
-    for (int k = threadIdx.x; k < nu; k += blockDim.x) snc[k] = c.nodecode[c.et_node[t0 + k]];
-    __syncthreads();
-  }
-  const int e0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31);
-  if (e0 >= c.ne) return;
-  const int nvalid = min(32, c.ne - e0);
-  int e = blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= c.ne) e = c.ne - 1;   // idle lanes recompute the last element; not stored
-  int n1 = c.nm[3 * e], n2 = c.nm[3 * e + 1], n3 = c.nm[3 * e + 2];
+// One element's three contributions; nodal fields from the staged tile
+// (STAGED) or from global memory.
+template <class R, bool STAGED>
+__device__ __forceinline__ void rhs_elem_body(const adc_ctx &c, int e, const double (*sv)[kTileNodes],
+                                              const int *snc, R (&o)[3]) {
+  const int n1 = c.nm[3 * e], n2 = c.nm[3 * e + 1], n3 = c.nm[3 * e + 2];
   int l1 = 0, l2 = 0, l3 = 0;
-  if (staged) {
+  if constexpr (STAGED) {
     l1 = c.e_loc[3 * e];
     l2 = c.e_loc[3 * e + 1];
     l3 = c.e_loc[3 * e + 2];
   }
   // the value of field f at the element's vertex k (0, 1, 2)
   auto V = [&](int f, int k) -> double {
-    if (staged) return sv[f][k == 0 ? l1 : (k == 1 ? l2 : l3)];
-    return rhs_field(c, f, k == 0 ? n1 : (k == 1 ? n2 : n3));
+    if constexpr (STAGED) return sv[f][k == 0 ? l1 : (k == 1 ? l2 : l3)];
+    else return rhs_field(c, f, k == 0 ? n1 : (k == 1 ? n2 : n3));
   };
   auto NC = [&](int k) -> int {
-    if (staged) return snc[k == 0 ? l1 : (k == 1 ? l2 : l3)];
-    return c.nodecode[k == 0 ? n1 : (k == 1 ? n2 : n3)];
+    if constexpr (STAGED) return snc[k == 0 ? l1 : (k == 1 ? l2 : l3)];
+    else return c.nodecode[k == 0 ? n1 : (k == 1 ? n2 : n3)];
   };
   const adc_params_t &p = c.p;
+  const bool met = p.nws != 0;
   const R DT = R(p.dt), G = R(p.g), A00 = R(p.a00), B00 = R(p.b00), C00 = R(p.c00);
   // x / DT: with a power-of-two DT, the product with its exact reciprocal
   // gives the same bits
@@ -494,7 +477,48 @@ __global__ void __launch_bounds__(256, sizeof(R) == 4 ? 3 : 2) k_rhs_elem(adc_ct
               c1 * (A00pB00 * (FDX3 * E1XGrad2A + FDY3 * E1YGrad2A)) +
               (JXAvg * FDX3 + JYAvg * FDY3) * R(0.5) + Tau0SpaVar;
   R nc = (R)NCEle;
-  const R o[3] = {T1 * nc, T2 * nc, T3 * nc};
+  o[0] = T1 * nc;
+  o[1] = T2 * nc;
+  o[2] = T3 * nc;
+}
+
+template <class R>
+__global__ void __launch_bounds__(256, sizeof(R) == 4 ? 3 : 2) k_rhs_elem(adc_ctx c) {
+  griddep_wait();
+  __shared__ R sh[kThreads / 32][32 * 3];
+  __shared__ double sv[RF_N][kTileNodes];
+  __shared__ int snc[kTileNodes];
+  const int t0 = c.et_ptr[blockIdx.x], nu = c.et_ptr[blockIdx.x + 1] - t0;
+  const bool staged = nu <= kTileNodes;   // block-uniform
+  if (staged) {
+    // every field of one node per thread: all loads of a thread in flight together
+    const double *base[RF_N] = {c.eta1, c.eta2, c.etas, c.uu1, c.vv1, c.qx1, c.qy1, c.h2, c.evm,
+                                c.tau0, c.corif, c.dp, c.tkm, c.tkm + 1, c.tkm + 2, c.pr1, c.wsx1,
+                                c.wsy1};
+    const bool met = c.p.nws != 0;
+    for (int k = threadIdx.x; k < nu; k += blockDim.x) {
+      const int n = c.et_node[t0 + k];
+      double v[RF_N];
+#pragma unroll
+      for (int f = 0; f < RF_N; ++f) {
+        const size_t at = (f == RF_TK0 || f == RF_TK1 || f == RF_TK2) ? 3 * (size_t)n : (size_t)n;
+        v[f] = (f < RF_PR1 || met) ? base[f][at] : 0.0;
+      }
+      const int nc = c.nodecode[n];
+#pragma unroll
+      for (int f = 0; f < RF_N; ++f) sv[f][k] = v[f];
+      snc[k] = nc;
+    }
+    __syncthreads();
+  }
+  const int e0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31);
+  if (e0 >= c.ne) return;
+  const int nvalid = min(32, c.ne - e0);
+  int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= c.ne) e = c.ne - 1;   // idle lanes recompute the last element; not stored
+  R o[3];
+  if (staged) rhs_elem_body<R, true>(c, e, sv, snc, o);
+  else rhs_elem_body<R, false>(c, e, sv, snc, o);
   warp_store_k<3>(reinterpret_cast<R *>(c.ebuf) + 3 * (size_t)e0, o, nvalid, sh[threadIdx.x >> 5]);
 }
 
