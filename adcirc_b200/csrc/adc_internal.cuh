@@ -22,7 +22,6 @@ namespace adc {
 constexpr int kSlice = 32;            // rows per SELL slice (one warp)
 constexpr int kGatherChunk = 8;       // per-node gathers issued together
 constexpr int kThreads = 256;
-constexpr int kTileNodes = 256;        // distinct nodes an element tile stages in shared memory
 constexpr long long kSpinCycles = 4000000000LL;  // ~2 s at 1.9 GHz
 
 // Device-visible scalar state of the step and of ITPACK.
@@ -105,10 +104,6 @@ struct adc_ctx {
   int *nm;
   double *fdx, *fdy, *areas;
   int *n2e_ptr, *n2e;
-  // element tiles of kThreads elements: their distinct nodes (sorted) and,
-  // per element vertex, its position in the tile's list
-  int *et_ptr, *et_node;
-  unsigned short *e_loc;
   // matrix structure (SELL)
   int *sl_ptr, *sl_w, *col, *rlen;
   int *lhs_src;          // 2 per padded slot: index 6*e+q of the element off-diagonal value, or -1

@@ -293,99 +293,54 @@ __global__ void k_lhs_bc(adc_ctx c, const int *rebuild) {
 
 // --------------------------------------------------------------- RHS
 // gwce.F:1000-1617, one element, IM=0 branches.
-//
-// The nodal fields an element reads (NF of them) are staged per block: the
-// block's 256 elements share about 160 distinct nodes, whose fields are
-// loaded once into shared memory (all threads, every field, the node list
-// built at bind), instead of 3 x NF scattered loads per element.  A tile with
-// more than kTileNodes distinct nodes reads global memory directly.  Both
-// paths evaluate the same expressions on the same doubles.
-enum RhsField {
-  RF_ETA1, RF_ETA2, RF_ETAS, RF_UU1, RF_VV1, RF_QX1, RF_QY1, RF_H2, RF_EVM, RF_TAU0, RF_CORIF,
-  RF_DP, RF_TK0, RF_TK1, RF_TK2, RF_PR1, RF_WSX1, RF_WSY1, RF_N
-};
-
-__device__ __forceinline__ double rhs_field(const adc_ctx &c, int f, int n) {
-  switch (f) {
-    case RF_ETA1: return c.eta1[n];
-    case RF_ETA2: return c.eta2[n];
-    case RF_ETAS: return c.etas[n];
-    case RF_UU1: return c.uu1[n];
-    case RF_VV1: return c.vv1[n];
-    case RF_QX1: return c.qx1[n];
-    case RF_QY1: return c.qy1[n];
-    case RF_H2: return c.h2[n];
-    case RF_EVM: return c.evm[n];
-    case RF_TAU0: return c.tau0[n];
-    case RF_CORIF: return c.corif[n];
-    case RF_DP: return c.dp[n];
-    case RF_TK0: return c.tkm[3 * (size_t)n];
-    case RF_TK1: return c.tkm[3 * (size_t)n + 1];
-    case RF_TK2: return c.tkm[3 * (size_t)n + 2];
-    case RF_PR1: return c.pr1[n];
-    case RF_WSX1: return c.wsx1[n];
-    default: return c.wsy1[n];
-  }
-}
-
-// One element's three contributions; nodal fields from the staged tile
-// (STAGED) or from global memory.
-template <class R, bool STAGED>
-__device__ __forceinline__ void rhs_elem_body(const adc_ctx &c, int e, const double (*sv)[kTileNodes],
-                                              const int *snc, R (&o)[3]) {
-  const int n1 = c.nm[3 * e], n2 = c.nm[3 * e + 1], n3 = c.nm[3 * e + 2];
-  int l1 = 0, l2 = 0, l3 = 0;
-  if constexpr (STAGED) {
-    l1 = c.e_loc[3 * e];
-    l2 = c.e_loc[3 * e + 1];
-    l3 = c.e_loc[3 * e + 2];
-  }
-  // the value of field f at the element's vertex k (0, 1, 2)
-  auto V = [&](int f, int k) -> double {
-    if constexpr (STAGED) return sv[f][k == 0 ? l1 : (k == 1 ? l2 : l3)];
-    else return rhs_field(c, f, k == 0 ? n1 : (k == 1 ? n2 : n3));
-  };
-  auto NC = [&](int k) -> int {
-    if constexpr (STAGED) return snc[k == 0 ? l1 : (k == 1 ? l2 : l3)];
-    else return c.nodecode[k == 0 ? n1 : (k == 1 ? n2 : n3)];
-  };
+template <class R>
+__global__ void __launch_bounds__(256, sizeof(R) == 4 ? 3 : 2) k_rhs_elem(adc_ctx c) {
+  griddep_wait();
+  __shared__ R sh[kThreads / 32][32 * 3];
+  const int e0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31);
+  if (e0 >= c.ne) return;
+  const int nvalid = min(32, c.ne - e0);
+  int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= c.ne) e = c.ne - 1;   // idle lanes recompute the last element; not stored
   const adc_params_t &p = c.p;
-  const bool met = p.nws != 0;
   const R DT = R(p.dt), G = R(p.g), A00 = R(p.a00), B00 = R(p.b00), C00 = R(p.c00);
   // x / DT: with a power-of-two DT, the product with its exact reciprocal
   // gives the same bits
   const bool dt2 = c.dt_pow2 != 0;
   const R IDT = R(c.inv_dt);
   auto odt = [&](R x) { return dt2 ? x * IDT : x / DT; };
-  int NCEle = NC(0) * NC(1) * NC(2) * c.noff[e];
-  R E0N1 = V(RF_ETA1, 0), E0N2 = V(RF_ETA1, 1), E0N3 = V(RF_ETA1, 2);
-  R E1N1 = V(RF_ETA2, 0), E1N2 = V(RF_ETA2, 1), E1N3 = V(RF_ETA2, 2);
+  int n1 = c.nm[3 * e], n2 = c.nm[3 * e + 1], n3 = c.nm[3 * e + 2];
+  int NCEle = c.nodecode[n1] * c.nodecode[n2] * c.nodecode[n3] * c.noff[e];
+  R E0N1 = c.eta1[n1], E0N2 = c.eta1[n2], E0N3 = c.eta1[n3];
+  R E1N1 = c.eta2[n1], E1N2 = c.eta2[n2], E1N3 = c.eta2[n3];
   R E1N1SQ = E1N1 * E1N1, E1N2SQ = E1N2 * E1N2, E1N3SQ = E1N3 * E1N3;
-  R ESN1 = V(RF_ETAS, 0), ESN2 = V(RF_ETAS, 1), ESN3 = V(RF_ETAS, 2);
-  R U1N1 = V(RF_UU1, 0), U1N2 = V(RF_UU1, 1), U1N3 = V(RF_UU1, 2);
-  R V1N1 = V(RF_VV1, 0), V1N2 = V(RF_VV1, 1), V1N3 = V(RF_VV1, 2);
-  R QX1N1 = V(RF_QX1, 0), QX1N2 = V(RF_QX1, 1), QX1N3 = V(RF_QX1, 2);
-  R QY1N1 = V(RF_QY1, 0), QY1N2 = V(RF_QY1, 1), QY1N3 = V(RF_QY1, 2);
-  R H1N1 = V(RF_H2, 0), H1N2 = V(RF_H2, 1), H1N3 = V(RF_H2, 2);
-  R EVMN1 = V(RF_EVM, 0), EVMN2 = V(RF_EVM, 1), EVMN3 = V(RF_EVM, 2);
-  R T0N1 = V(RF_TAU0, 0), T0N2 = V(RF_TAU0, 1), T0N3 = V(RF_TAU0, 2);
+  R ESN1 = c.etas[n1], ESN2 = c.etas[n2], ESN3 = c.etas[n3];
+  R U1N1 = c.uu1[n1], U1N2 = c.uu1[n2], U1N3 = c.uu1[n3];
+  R V1N1 = c.vv1[n1], V1N2 = c.vv1[n2], V1N3 = c.vv1[n3];
+  R QX1N1 = c.qx1[n1], QX1N2 = c.qx1[n2], QX1N3 = c.qx1[n3];
+  R QY1N1 = c.qy1[n1], QY1N2 = c.qy1[n2], QY1N3 = c.qy1[n3];
+  R H1N1 = c.h2[n1], H1N2 = c.h2[n2], H1N3 = c.h2[n3];
+  R EVMN1 = c.evm[n1], EVMN2 = c.evm[n2], EVMN3 = c.evm[n3];
+  R T0N1 = c.tau0[n1], T0N2 = c.tau0[n2], T0N3 = c.tau0[n3];
+  const bool met = p.nws != 0;
   R Pr1N1 = R(0.0), Pr1N2 = R(0.0), Pr1N3 = R(0.0);
   if (met) {
     if constexpr (sizeof(R) == 4) {
       // only the gradient of PR1 is used: FP32 carries its deviation from
       // the background pressure, not the ~10 m total
       const double pb = p.prbckgrnd_mh2o;
-      Pr1N1 = R(V(RF_PR1, 0) - pb); Pr1N2 = R(V(RF_PR1, 1) - pb); Pr1N3 = R(V(RF_PR1, 2) - pb);
+      Pr1N1 = R(c.pr1[n1] - pb); Pr1N2 = R(c.pr1[n2] - pb); Pr1N3 = R(c.pr1[n3] - pb);
     } else {
-      Pr1N1 = V(RF_PR1, 0); Pr1N2 = V(RF_PR1, 1); Pr1N3 = V(RF_PR1, 2);
+      Pr1N1 = c.pr1[n1]; Pr1N2 = c.pr1[n2]; Pr1N3 = c.pr1[n3];
     }
   }
-  R BSXN1 = R(V(RF_TK0, 0)) * QX1N1 + R(V(RF_TK2, 0)) * QY1N1;
-  R BSYN1 = R(V(RF_TK2, 0)) * QX1N1 + R(V(RF_TK1, 0)) * QY1N1;
-  R BSXN2 = R(V(RF_TK0, 1)) * QX1N2 + R(V(RF_TK2, 1)) * QY1N2;
-  R BSYN2 = R(V(RF_TK2, 1)) * QX1N2 + R(V(RF_TK1, 1)) * QY1N2;
-  R BSXN3 = R(V(RF_TK0, 2)) * QX1N3 + R(V(RF_TK2, 2)) * QY1N3;
-  R BSYN3 = R(V(RF_TK2, 2)) * QX1N3 + R(V(RF_TK1, 2)) * QY1N3;
+  const double *tk1 = c.tkm + 3 * n1, *tk2 = c.tkm + 3 * n2, *tk3 = c.tkm + 3 * n3;
+  R BSXN1 = R(tk1[0]) * QX1N1 + R(tk1[2]) * QY1N1;
+  R BSYN1 = R(tk1[2]) * QX1N1 + R(tk1[1]) * QY1N1;
+  R BSXN2 = R(tk2[0]) * QX1N2 + R(tk2[2]) * QY1N2;
+  R BSYN2 = R(tk2[2]) * QX1N2 + R(tk2[1]) * QY1N2;
+  R BSXN3 = R(tk3[0]) * QX1N3 + R(tk3[2]) * QY1N3;
+  R BSYN3 = R(tk3[2]) * QX1N3 + R(tk3[1]) * QY1N3;
   R AreaIE2 = c.areas[e];
   R AreaIE = AreaIE2 / R(2.0);
   R AreaIE4 = R(2.0) * AreaIE2;
@@ -396,8 +351,8 @@ __device__ __forceinline__ void rhs_elem_body(const adc_ctx &c, int e, const dou
     // Elevation gradients cancel metre-sized nodal values down to
     // centimetres: they are formed in FP64 and only then narrowed.
     const double *fx = c.fdx + 3 * e, *fy = c.fdy + 3 * e;
-    const double a1 = V(RF_ETA1, 0), a2 = V(RF_ETA1, 1), a3 = V(RF_ETA1, 2);
-    const double b1 = V(RF_ETA2, 0), b2 = V(RF_ETA2, 1), b3 = V(RF_ETA2, 2);
+    const double a1 = c.eta1[n1], a2 = c.eta1[n2], a3 = c.eta1[n3];
+    const double b1 = c.eta2[n1], b2 = c.eta2[n2], b3 = c.eta2[n3];
     E0XGrad2A = R(a1 * fx[0] + a2 * fx[1] + a3 * fx[2]);
     E0YGrad2A = R(a1 * fy[0] + a2 * fy[1] + a3 * fy[2]);
     E1XGrad2A = R(b1 * fx[0] + b2 * fx[1] + b3 * fx[2]);
@@ -423,7 +378,7 @@ __device__ __forceinline__ void rhs_elem_body(const adc_ctx &c, int e, const dou
   R MY = (EVMXGrad * (QX1N1 * FDY1 + QX1N2 * FDY2 + QX1N3 * FDY3) +
                EVMYGrad * (QY1N1 * FDY1 + QY1N2 * FDY2 + QY1N3 * FDY3) -
                EVMAvgODT * (ESN1 * FDY1 + ESN2 * FDY2 + ESN3 * FDY3)) / AreaIE2;
-  R CorifAvg = div3(V(RF_CORIF, 0) + V(RF_CORIF, 1) + V(RF_CORIF, 2));
+  R CorifAvg = div3(c.corif[n1] + c.corif[n2] + c.corif[n3]);
   R Tau0Avg = div3(T0N1 + T0N2 + T0N3);
   R Tau0QXAvg = div3(T0N1 * QX1N1 + T0N2 * QX1N2 + T0N3 * QX1N3);
   R Tau0QYAvg = div3(T0N1 * QY1N1 + T0N2 * QY1N2 + T0N3 * QY1N3);
@@ -432,7 +387,7 @@ __device__ __forceinline__ void rhs_elem_body(const adc_ctx &c, int e, const dou
   R QX1Avg = div3(QX1N1 + QX1N2 + QX1N3);
   R QY1Avg = div3(QY1N1 + QY1N2 + QY1N3);
   R ESAvg = div3(ESN1 + ESN2 + ESN3);
-  R DPAvg = div3(V(RF_DP, 0) + V(RF_DP, 1) + V(RF_DP, 2));
+  R DPAvg = div3(c.dp[n1] + c.dp[n2] + c.dp[n3]);
   R al = c.alphal[e];
   R GDPAvgOAreaIE4 = al * G * DPAvg / AreaIE4;
   R GDPAvgOAreaIE4_S0 = GDPAvgOAreaIE4;   // DPAvgS0 == DPAvg when IFNL_HDP = 0
@@ -443,8 +398,8 @@ __device__ __forceinline__ void rhs_elem_body(const adc_ctx &c, int e, const dou
   R BSYAvg = div3(BSYN1 + BSYN2 + BSYN3);
   R WSXAvg = R(0.0), WSYAvg = R(0.0);
   if (met) {
-    WSXAvg = div3(V(RF_WSX1, 0) + V(RF_WSX1, 1) + V(RF_WSX1, 2));
-    WSYAvg = div3(V(RF_WSY1, 0) + V(RF_WSY1, 1) + V(RF_WSY1, 2));
+    WSXAvg = div3(c.wsx1[n1] + c.wsx1[n2] + c.wsx1[n3]);
+    WSYAvg = div3(c.wsy1[n1] + c.wsy1[n2] + c.wsy1[n3]);
   }
   R MsFacR = div12(odt(AreaIE * ((dt2 ? IDT : R(1.0) / DT) - Tau0Avg / R(2.0))));
   R GOAreaIE4 = al * G / AreaIE4;
@@ -477,48 +432,7 @@ __device__ __forceinline__ void rhs_elem_body(const adc_ctx &c, int e, const dou
               c1 * (A00pB00 * (FDX3 * E1XGrad2A + FDY3 * E1YGrad2A)) +
               (JXAvg * FDX3 + JYAvg * FDY3) * R(0.5) + Tau0SpaVar;
   R nc = (R)NCEle;
-  o[0] = T1 * nc;
-  o[1] = T2 * nc;
-  o[2] = T3 * nc;
-}
-
-template <class R>
-__global__ void __launch_bounds__(256, sizeof(R) == 4 ? 3 : 2) k_rhs_elem(adc_ctx c) {
-  griddep_wait();
-  __shared__ R sh[kThreads / 32][32 * 3];
-  __shared__ double sv[RF_N][kTileNodes];
-  __shared__ int snc[kTileNodes];
-  const int t0 = c.et_ptr[blockIdx.x], nu = c.et_ptr[blockIdx.x + 1] - t0;
-  const bool staged = nu <= kTileNodes;   // block-uniform
-  if (staged) {
-    // every field of one node per thread: all loads of a thread in flight together
-    const double *base[RF_N] = {c.eta1, c.eta2, c.etas, c.uu1, c.vv1, c.qx1, c.qy1, c.h2, c.evm,
-                                c.tau0, c.corif, c.dp, c.tkm, c.tkm + 1, c.tkm + 2, c.pr1, c.wsx1,
-                                c.wsy1};
-    const bool met = c.p.nws != 0;
-    for (int k = threadIdx.x; k < nu; k += blockDim.x) {
-      const int n = c.et_node[t0 + k];
-      double v[RF_N];
-#pragma unroll
-      for (int f = 0; f < RF_N; ++f) {
-        const size_t at = (f == RF_TK0 || f == RF_TK1 || f == RF_TK2) ? 3 * (size_t)n : (size_t)n;
-        v[f] = (f < RF_PR1 || met) ? base[f][at] : 0.0;
-      }
-      const int nc = c.nodecode[n];
-#pragma unroll
-      for (int f = 0; f < RF_N; ++f) sv[f][k] = v[f];
-      snc[k] = nc;
-    }
-    __syncthreads();
-  }
-  const int e0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31);
-  if (e0 >= c.ne) return;
-  const int nvalid = min(32, c.ne - e0);
-  int e = blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= c.ne) e = c.ne - 1;   // idle lanes recompute the last element; not stored
-  R o[3];
-  if (staged) rhs_elem_body<R, true>(c, e, sv, snc, o);
-  else rhs_elem_body<R, false>(c, e, sv, snc, o);
+  const R o[3] = {T1 * nc, T2 * nc, T3 * nc};
   warp_store_k<3>(reinterpret_cast<R *>(c.ebuf) + 3 * (size_t)e0, o, nvalid, sh[threadIdx.x >> 5]);
 }
 

@@ -189,8 +189,6 @@ struct HostTables {
       obc_rhs_b, me_of_node, me_lbc, me_i;
   std::vector<double> me_csi, me_sii;
   std::vector<int> sell_of_ell;   // ELL (i + np*j), j >= 1 -> SELL idx or -1
-  std::vector<int> et_ptr, et_node;
-  std::vector<unsigned short> e_loc;
 };
 
 static int build_tables(const adc_arrays_t *a, HostTables &T, int &nslices, int &nnz_pad) {
@@ -211,26 +209,6 @@ static int build_tables(const adc_arrays_t *a, HostTables &T, int &nslices, int 
     std::vector<int> fill(T.n2e_ptr.begin(), T.n2e_ptr.end() - 1);
     for (int e = 0; e < ne; ++e)
       for (int k = 0; k < 3; ++k) T.n2e[fill[T.nm[3 * (size_t)e + k]]++] = 3 * e + k;
-  }
-  // element tiles (one block of an element kernel each): distinct nodes and
-  // each vertex's position among them; the positions are only used for
-  // tiles with at most kTileNodes distinct nodes
-  {
-    const int ntile = (ne + kThreads - 1) / kThreads;
-    T.et_ptr.assign(ntile + 1, 0);
-    T.e_loc.assign(3 * (size_t)ne, 0);
-    std::vector<int> u;
-    for (int t = 0; t < ntile; ++t) {
-      const int e0 = t * kThreads, e1 = std::min(ne, e0 + kThreads);
-      u.assign(T.nm.begin() + 3 * (size_t)e0, T.nm.begin() + 3 * (size_t)e1);
-      std::sort(u.begin(), u.end());
-      u.erase(std::unique(u.begin(), u.end()), u.end());
-      if ((int)u.size() <= kTileNodes)
-        for (size_t q = 3 * (size_t)e0; q < 3 * (size_t)e1; ++q)
-          T.e_loc[q] = (unsigned short)(std::lower_bound(u.begin(), u.end(), T.nm[q]) - u.begin());
-      T.et_node.insert(T.et_node.end(), u.begin(), u.end());
-      T.et_ptr[t + 1] = (int)T.et_node.size();
-    }
   }
   // sliced ELL of the off-diagonal NeiTab slots
   nslices = (np + kSlice - 1) / kSlice;
@@ -451,7 +429,7 @@ static void free_ctx(adc_ctx *c) {
       (void **)&c->x, (void **)&c->y, (void **)&c->dp, (void **)&c->tau0, (void **)&c->evm,
       (void **)&c->fric, (void **)&c->corif, (void **)&c->nneigh, (void **)&c->nm,
       (void **)&c->fdx, (void **)&c->fdy, (void **)&c->areas, (void **)&c->n2e_ptr,
-      (void **)&c->n2e, (void **)&c->et_ptr, (void **)&c->et_node, (void **)&c->e_loc, (void **)&c->sl_ptr, (void **)&c->sl_w, (void **)&c->col,
+      (void **)&c->n2e, (void **)&c->sl_ptr, (void **)&c->sl_w, (void **)&c->col,
       (void **)&c->rlen, (void **)&c->lhs_src, (void **)&c->nbd, (void **)&c->is_nbd,
       (void **)&c->amig, (void **)&c->per, (void **)&c->face, (void **)&c->ff,
       (void **)&c->emo, (void **)&c->efa, (void **)&c->obc_slot, (void **)&c->obc_zero,
@@ -550,9 +528,6 @@ static int bind_impl(const adc_params_t *p, const adc_arrays_t *a, int prec, adc
   B(dalloc(&c->areas, ne)); B(up(c->areas, a->areas, ne));
   B(dalloc(&c->n2e_ptr, np + 1)); B(up(c->n2e_ptr, T.n2e_ptr.data(), np + 1));
   B(dalloc(&c->n2e, 3 * (size_t)ne)); B(up(c->n2e, T.n2e.data(), T.n2e.size()));
-  B(dalloc(&c->et_ptr, T.et_ptr.size())); B(up(c->et_ptr, T.et_ptr.data(), T.et_ptr.size()));
-  B(dalloc(&c->et_node, T.et_node.size())); B(up(c->et_node, T.et_node.data(), T.et_node.size()));
-  B(dalloc(&c->e_loc, T.e_loc.size())); B(up(c->e_loc, T.e_loc.data(), T.e_loc.size()));
   B(dalloc(&c->sl_ptr, nslices + 1)); B(up(c->sl_ptr, T.sl_ptr.data(), nslices + 1));
   B(dalloc(&c->sl_w, nslices)); B(up(c->sl_w, T.sl_w.data(), nslices));
   B(dalloc(&c->col, std::max(nnz_pad, 1))); B(up(c->col, T.col.data(), T.col.size()));
