@@ -428,6 +428,9 @@ def profile_run(args):
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
     case = make_case(args.case)
     gpu = model.GpuModel(case, prec=PATHS[args.profile_path][0])
+    if PATHS[args.profile_path][0] & 32:
+        from adcirc_b200 import learned
+        gpu.set_predictor(learned.load())
     numitr, last = gpu.run(1, args.profile_steps)
     torch.cuda.synchronize()
     print(f"profile run: {args.profile_steps} steps, status {last.status}, "
