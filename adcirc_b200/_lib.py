@@ -69,7 +69,7 @@ class AdcStep(C.Structure):
 
 class AdcFlux(C.Structure):
     _fields_ = [("nffr", C.c_int), ("flux_settling_it", C.c_int)] + [
-        (n, dp_) for n in ("famig", "fper", "fff", "fface", "qnam", "qnph")]
+        (n, dp_) for n in ("famig", "fper", "fff", "fface", "qnam", "qnph", "enam", "enph")]
 
 
 class AdcVortexFix(C.Structure):

@@ -126,6 +126,8 @@ struct adc_ctx {
   double *zng_f;             //   ZNGIF1-3 (3 per entry)
   int flux_settling_it;  // FluxSettlingIT (river radiation, IBTYPE 52)
   double *elevdisc;      // ElevDisc per boundary entry (IBTYPE 52)
+  double *en;            // EN0, EN1, EN2 (NVEL each): specified elevation of IBTYPE 32
+  int fen;               // ENAM/ENPH follow QNAM/QNPH in fqn
   double *etadisc_b;     // EtaDisc at the boundary entries' nodes
   double *qn;            // QN0, QN1, QN2 (NVEL each)
   double *qforce;        // per boundary entry: the GWCE line-integral force

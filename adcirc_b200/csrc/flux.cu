@@ -1,18 +1,21 @@
 // flux.cu -- specified normal flux boundaries (IBTYPE 2, 12, 22), radiation
-// boundaries (IBTYPE 30), zero-normal-gradient boundaries (IBTYPE 40) and
-// river-radiation boundaries (IBTYPE 52).
+// boundaries (IBTYPE 30), coupled flux/radiation boundaries (IBTYPE 32),
+// zero-normal-gradient boundaries (IBTYPE 40) and river-radiation
+// boundaries (IBTYPE 52).
 //
 // Three pieces of the reference's flux-boundary path:
-//  * QN0 <- QN1 <- QN2 <- 0 (timestep.F:606-613), then QN2 as the sum of the
-//    periodic flux constituents (timestep.F:861-880; ICS = 1, so the normal
-//    flux is not rotated), and at radiation entries QN1 = H2 (UU1 CSII +
+//  * QN0 <- QN1 <- QN2 <- 0 and EN0 <- EN1 <- EN2 <- 0 (timestep.F:606-613),
+//    then QN2 (and at IBTYPE 32 entries EN2) as the sum of the periodic
+//    constituents (timestep.F:861-880; ICS = 1, so the normal flux is not
+//    rotated), and at radiation entries QN1 = H2 (UU1 CSII +
 //    VV1 SIII), the discharge of the latest velocity (timestep.F:932-940),
 //    and the same at zero-normal-gradient entries (:945-952);
 //    river-radiation entries take their discharge elevation ElevDisc at
 //    FluxSettlingIT (or from the cold-start EtaDisc, timestep.F:906-926);
 //  * the GWCE boundary line integral (gwce.F:1737-1834): a force per
 //    boundary entry (specified flux, the radiation condition
-//    -sqrt(g H1) ETAS / DT - TAU0 QN1, or for river radiation the specified
+//    -sqrt(g H1) ETAS / DT - TAU0 QN1, the coupled condition of IBTYPE 32
+//    against the specified elevation EN, or for river radiation the specified
 //    flux less sqrt(g H1) (ETAS / DT + TAU0 (ETA1 - ElevDisc)) after
 //    FluxSettlingIT), then for each pair of consecutive
 //    entries a contribution to both nodes.  The reference adds these in entry order;
@@ -33,24 +36,31 @@ __global__ void k_flux_forcing(adc_ctx c, const adc_step_t *steps, const Flags *
   const int I = blockIdx.x * blockDim.x + threadIdx.x;
   if (I >= c.nvel) return;
   double *qn0 = c.qn, *qn1 = c.qn + c.nvel, *qn2 = c.qn + 2 * c.nvel;
+  double *en0 = c.en, *en1 = c.en + c.nvel, *en2 = c.en + 2 * c.nvel;
   qn0[I] = qn1[I];
   qn1[I] = qn2[I];
-  double q = 0.0;
+  en0[I] = en1[I];
+  en1[I] = en2[I];
+  double q = 0.0, el = 0.0;
   const int lb = c.blbc[I];
   const adc_step_t st = steps[flags->cursor];
-  if (c.flux_on && (lb == 2 || lb == 12 || lb == 22 || lb == 52)) {
+  if (c.flux_on && (lb == 2 || lb == 12 || lb == 22 || lb == 32 || lb == 52)) {
     const int nf = c.nffr;
+    const size_t nfv = (size_t)nf * c.nvel;
     const double *famig = c.fconst, *fper = famig + nf, *fff = fper + nf, *fface = fff + nf;
-    const double *qnam = c.fqn, *qnph = c.fqn + (size_t)nf * c.nvel;
+    const double *qnam = c.fqn, *qnph = c.fqn + nfv, *enam = qnph + nfv, *enph = enam + nfv;
+    const bool coupled = lb == 32 && c.fen;
     for (int J = 0; J < nf; ++J) {
       int NCYC = 0;
       if (fper[J] != 0.0) NCYC = (int)(st.timeh / fper[J]);
       const double ARGJ = famig[J] * (st.timeh - NCYC * fper[J]) + fface[J];
       const double RFF = fff[J] * st.rampextflux;
       q = q + qnam[J + (size_t)nf * I] * RFF * cos(ARGJ - qnph[J + (size_t)nf * I]);
+      if (coupled) el = el + enam[J + (size_t)nf * I] * RFF * cos(ARGJ - enph[J + (size_t)nf * I]);
     }
   }
   qn2[I] = q;
+  en2[I] = el;
   if (lb == 52) {
     const int n = c.bnv[I];
     if (st.it == c.flux_settling_it) {
@@ -80,6 +90,14 @@ __global__ void k_flux_qforce(adc_ctx c, const adc_step_t *steps, Flags *flags) 
   if (J >= c.nvel) return;
   const double *qn0 = c.qn, *qn1 = c.qn + c.nvel, *qn2 = c.qn + 2 * c.nvel;
   const int n = c.bnv[J];
+  if (c.blbc[J] == 32) {   // gwce.F:1792-1797
+    const double *en0 = c.en, *en1 = c.en + c.nvel, *en2 = c.en + 2 * c.nvel;
+    const double CELERITY = sqrt(c.p.g * c.h1[n]);
+    const double DT2 = c.p.dt * 2.0;
+    c.qforce[J] = (qn2[J] - qn0[J]) / DT2 - CELERITY * (2.0 * c.etas[n] - (en2[J] - en0[J])) / DT2 +
+                  c.tau0[n] * (qn1[J] - CELERITY * (c.eta1[n] - en1[J]));
+    return;
+  }
   if (c.blbc[J] == 40) {   // gwce.F:1804-1805
     c.qforce[J] = -(qn1[J] - qn0[J]) / c.p.dt - c.tau0[n] * (qn1[J] + qn0[J]) / 2.0;
     return;
@@ -141,10 +159,10 @@ int flux_tables(adc_ctx *c, const adc_arrays_t *a) {
   c->nfluxgbc = 0;
   for (int I = 0; I < nv; ++I) {
     const int lb = a->lbcodei[I];
-    if (lb == 2 || lb == 12 || lb == 22 || lb == 52) c->nfluxf = 1;
-    if (lb == 30) c->nfluxrbc = 1;
+    if (lb == 2 || lb == 12 || lb == 22 || lb == 32 || lb == 52) c->nfluxf = 1;
+    if (lb == 30 || lb == 32) c->nfluxrbc = 1;
     if (lb == 40) c->nfluxgbc = 1;
-    if (lb == 32 || lb == 41 || lb == 64) {
+    if (lb == 41 || lb == 64) {
       set_error("boundary code %d (zero-gradient or river-radiation flux) is not implemented", lb);
       return ADC_ERR_UNSUPPORTED;
     }
@@ -152,6 +170,8 @@ int flux_tables(adc_ctx *c, const adc_arrays_t *a) {
   const size_t nva = (size_t)(nv > 0 ? nv : 1);
   ADC_CUDA(cudaMalloc((void **)&c->qn, 3 * nva * sizeof(double)));
   ADC_CUDA(cudaMemset(c->qn, 0, 3 * nva * sizeof(double)));
+  ADC_CUDA(cudaMalloc((void **)&c->en, 3 * nva * sizeof(double)));
+  ADC_CUDA(cudaMemset(c->en, 0, 3 * nva * sizeof(double)));
   if (!c->nfluxf && !c->nfluxrbc && !c->nfluxgbc) return ADC_OK;
   std::vector<int> bnv(nv);
   for (int I = 0; I < nv; ++I) bnv[I] = a->nbv[I] - 1;
@@ -234,7 +254,7 @@ extern "C" int adc_set_flux(adc_ctx *c, const adc_flux_t *f) {
     return ADC_ERR_ARG;
   }
   if (!c->nfluxf) {
-    set_error("adc_set_flux: the mesh has no specified-flux boundary (IBTYPE 2, 12, 22 or 52)");
+    set_error("adc_set_flux: the mesh has no specified-flux boundary (IBTYPE 2, 12, 22, 32 or 52)");
     return ADC_ERR_ARG;
   }
   const int nf = f->nffr, nv = c->nvel;
@@ -249,10 +269,16 @@ extern "C" int adc_set_flux(adc_ctx *c, const adc_flux_t *f) {
   c->fqn = nullptr;
   ADC_CUDA(cudaMalloc((void **)&c->fconst, cst.size() * sizeof(double)));
   ADC_CUDA(cudaMemcpy(c->fconst, cst.data(), cst.size() * sizeof(double), cudaMemcpyHostToDevice));
-  ADC_CUDA(cudaMalloc((void **)&c->fqn, 2 * (size_t)nf * nv * sizeof(double)));
-  ADC_CUDA(cudaMemcpy(c->fqn, f->qnam, (size_t)nf * nv * sizeof(double), cudaMemcpyHostToDevice));
-  ADC_CUDA(cudaMemcpy(c->fqn + (size_t)nf * nv, f->qnph, (size_t)nf * nv * sizeof(double),
-                      cudaMemcpyHostToDevice));
+  const size_t nfv = (size_t)nf * nv;
+  const int fen = (f->enam && f->enph) ? 1 : 0;
+  ADC_CUDA(cudaMalloc((void **)&c->fqn, (fen ? 4 : 2) * nfv * sizeof(double)));
+  ADC_CUDA(cudaMemcpy(c->fqn, f->qnam, nfv * sizeof(double), cudaMemcpyHostToDevice));
+  ADC_CUDA(cudaMemcpy(c->fqn + nfv, f->qnph, nfv * sizeof(double), cudaMemcpyHostToDevice));
+  if (fen) {
+    ADC_CUDA(cudaMemcpy(c->fqn + 2 * nfv, f->enam, nfv * sizeof(double), cudaMemcpyHostToDevice));
+    ADC_CUDA(cudaMemcpy(c->fqn + 3 * nfv, f->enph, nfv * sizeof(double), cudaMemcpyHostToDevice));
+  }
+  c->fen = fen;
   c->nffr = nf;
   c->flux_settling_it = f->flux_settling_it;
   c->flux_on = 1;

@@ -62,6 +62,7 @@ static std::vector<HsRec> hs_records(adc_ctx *c) {
   if (c->vortex_on) r.push_back({"vortex", c->vstate, sizeof(VortexState)});
   if (c->nfluxf || c->nfluxrbc) {
     r.push_back({"flux_qn", c->qn, 3 * (size_t)c->nvel * d});
+    r.push_back({"flux_en", c->en, 3 * (size_t)c->nvel * d});
     r.push_back({"flux_elevdisc", c->elevdisc, (size_t)c->nvel * d});   // river radiation
     r.push_back({"flux_etadisc", c->etadisc_b, (size_t)c->nvel * d});
   }

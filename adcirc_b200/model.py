@@ -130,7 +130,7 @@ class Case:
 @dataclasses.dataclass
 class Flux:
     """Periodic specified normal flux on the flux boundaries (IBTYPE 2, 12,
-    22, 52): constituents (rad/s, s, nodal factor, rad) and per boundary
+    22, 32, 52): constituents (rad/s, s, nodal factor, rad) and per boundary
     entry (NVEL) amplitudes [m^2/s] and phases [rad], zero off flux entries;
     flux_settling_it is FluxSettlingIT (river radiation, IBTYPE 52)."""
     famig: np.ndarray
@@ -140,6 +140,8 @@ class Flux:
     qnam: np.ndarray   # (NFFR, NVEL)
     qnph: np.ndarray   # (NFFR, NVEL)
     flux_settling_it: int = 0
+    enam: "np.ndarray | None" = None   # (NFFR, NVEL) elevation constituents (IBTYPE 32)
+    enph: "np.ndarray | None" = None
 
     def struct(self, cls=None):
         """(struct, backing arrays); keep both alive while in use."""
@@ -147,10 +149,14 @@ class Flux:
         keep = [np.ascontiguousarray(a, np.float64) for a in (self.famig, self.fper, self.fff,
                                                                 self.fface)]
         keep += [np.asfortranarray(a, np.float64) for a in (self.qnam, self.qnph)]
+        names = ["famig", "fper", "fff", "fface", "qnam", "qnph"]
+        if self.enam is not None:
+            keep += [np.asfortranarray(a, np.float64) for a in (self.enam, self.enph)]
+            names += ["enam", "enph"]
         f = cls()
         f.nffr = int(keep[0].size)
         f.flux_settling_it = int(self.flux_settling_it)
-        for name, a in zip(("famig", "fper", "fff", "fface", "qnam", "qnph"), keep):
+        for name, a in zip(names, keep):
             setattr(f, name, a.ctypes.data_as(dp_))
         return f, keep
 
@@ -456,8 +462,10 @@ def case_from_files(fort14, fort15, vortex: "Vortex | None" = None,
         lbc = case.arrays["lbcodei"][:case.sizes["nvel"]]
         f = adcirc_io.read_fort15(fort15, neta, lbc)      # flux records on the case's NVEL order
         fper = np.where(f.famig != 0.0, 2.0 * math.pi / np.where(f.famig != 0.0, f.famig, 1.0), 0.0)
+        has32 = (lbc == 32).any()
         case.flux = Flux(f.famig.copy(), fper, f.fff.copy(), f.fface.copy(), f.qnam.copy(),
-                         f.qnph.copy(), flux_settling_it=sched.flux_settling_it)
+                         f.qnph.copy(), flux_settling_it=sched.flux_settling_it,
+                         enam=f.enam.copy() if has32 else None, enph=f.enph.copy() if has32 else None)
     if abs(f.nws) == 8:
         case.vortex = vortex
     case.meta["fort15"] = f
@@ -506,6 +514,8 @@ def fort15_for_case(case: Case, rnday: float = 1.0, rundes: str = "", runid: str
         o.nffr = case.flux.famig.size
         tabs.update(famig=case.flux.famig, fff=case.flux.fff, fface=case.flux.fface,
                     qnam=case.flux.qnam, qnph=case.flux.qnph)
+        if case.flux.enam is not None:
+            tabs.update(enam=case.flux.enam, enph=case.flux.enph)
     return adcirc_io.Fort15(o, [], [f"C{k + 1}" for k in range(nbfr)],
                             [f"F{k + 1}" for k in range(o.nffr)], [], tabs)
 
@@ -520,7 +530,7 @@ K1_PERIOD = 86164.0
 
 def channel_case(dt: float = 5.0, amp: float = 0.5, vortex: bool = False,
                  river: float | None = None, river_type: int = 2, radiation: bool = False,
-                 zero_gradient: bool = False, flux_settling: float = 0.0,
+                 zero_gradient: bool = False, flux_settling: float = 0.0, river_eta: float = 0.05,
                  prep: MeshPrep | None = None, **kw) -> Case:
     """Tidal channel: 121x41 nodes, 20 m -> 5 m, M2 0.5 m, dt 5 s.  With
     `vortex`, a small Holland vortex (Rmax 8 km) crosses the channel.  With
@@ -528,7 +538,8 @@ def channel_case(dt: float = 5.0, amp: float = 0.5, vortex: bool = False,
     specified-flux boundary (IBTYPE `river_type`, 2 or 22) carrying that
     steady inflow, ramped in over 0.02 days; IBTYPE 52 (river radiation)
     with `flux_settling` > 0 [days] holds the tide until the river flux has
-    settled (NRAMP 2).  With `radiation`, the east end is a radiation
+    settled (NRAMP 2); IBTYPE 32 (coupled flux and radiation) also takes
+    the steady elevation `river_eta` [m].  With `radiation`, the east end is a radiation
     boundary (IBTYPE 30) the tide leaves through; with `zero_gradient`, a
     zero-normal-velocity-gradient boundary (IBTYPE 40)."""
     from .meshgen import channel_mesh
@@ -553,9 +564,11 @@ def channel_case(dt: float = 5.0, amp: float = 0.5, vortex: bool = False,
         lbc = case.arrays["lbcodei"]
         nv = lbc.size
         qnam = np.zeros((1, nv))
-        qnam[0, (lbc == 2) | (lbc == 12) | (lbc == 22) | (lbc == 52)] = river
+        qnam[0, (lbc == 2) | (lbc == 12) | (lbc == 22) | (lbc == 32) | (lbc == 52)] = river
+        enam = np.where(lbc == 32, river_eta, 0.0)[None, :] if (lbc == 32).any() else None
         case.flux = Flux(np.zeros(1), np.zeros(1), np.ones(1), np.zeros(1), qnam, np.zeros((1, nv)),
-                         flux_settling_it=sched.flux_settling_it)
+                         flux_settling_it=sched.flux_settling_it, enam=enam,
+                         enph=None if enam is None else np.zeros((1, nv)))
     if vortex:
         case.vortex = straight_track(30.3e3, 3.7e3, 80.0, 6.0, 960.0, 8.0, 1.3, hours=12.0,
                                      interval_h=3.0)

@@ -112,7 +112,7 @@ typedef struct {
   double rampextflux;    /* RampExtFlux, the ramp of specified boundary fluxes */
 } adc_step_t;
 
-/* Periodic specified normal flux on flux boundaries (IBTYPE 2, 12, 22, 52):
+/* Periodic specified normal flux on flux boundaries (IBTYPE 2, 12, 22, 32, 52):
  * the fort.15 flux constituents timestep.F:861-880 sums each step. */
 typedef struct {
   int nffr;              /* NFFR > 0 constituents */
@@ -126,6 +126,9 @@ typedef struct {
   const double *fface;   /* FFACE(NFFR), rad */
   const double *qnam;    /* QNAM(NFFR,NVEL), normal flux per unit width, m^2/s */
   const double *qnph;    /* QNPH(NFFR,NVEL), rad */
+  const double *enam;    /* ENAM(NFFR,NVEL), m: elevation constituents of coupled
+                            flux/radiation entries (IBTYPE 32); NULL when there are none */
+  const double *enph;    /* ENPH(NFFR,NVEL), rad */
 } adc_flux_t;
 
 /* One fix of a parametric-vortex track: the fields of a fort.22 best-track
@@ -387,8 +390,10 @@ int adc_selftest_div_const(long long n, unsigned long long seed, long long *mism
  * against the discharge elevation of that step (gwce.F:1805-1815); the
  * flux-settling ramps themselves are the caller's adc_step_t values
  * (timestep.F:314-345).  Zero-normal-gradient entries (IBTYPE 40) need the
- * NEleZNG/ZNGIF tables of adc_zng_setup in adc_arrays_t.  Codes 32, 41 and
- * 64 are refused at bind with ADC_ERR_UNSUPPORTED. */
+ * NEleZNG/ZNGIF tables of adc_zng_setup in adc_arrays_t.  Coupled
+ * flux/radiation entries (IBTYPE 32) take their elevation constituents from
+ * enam/enph (gwce.F:1792-1797).  Codes 41 and 64 are refused at bind with
+ * ADC_ERR_UNSUPPORTED. */
 int adc_set_flux(adc_ctx *ctx, const adc_flux_t *flux);
 
 /* No reference counterpart (the reference always starts JCG from ETAS as

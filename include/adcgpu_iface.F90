@@ -43,7 +43,7 @@ module adcgpu_iface
 
    type, bind(C), public :: adc_flux_t
       integer(c_int) :: nffr, flux_settling_it
-      type(c_ptr) :: famig, fper, fff, fface, qnam, qnph
+      type(c_ptr) :: famig, fper, fff, fface, qnam, qnph, enam, enph
    end type
 
    type, bind(C), public :: adc_stepout_t

@@ -591,6 +591,8 @@ struct orc_model {
   int flux_settling_it = 0, etadisc_fill = 1;
   std::vector<double> elevdisc, etadisc_b;
   std::vector<double> famig, fper, fff, fface, qnam, qnph, qn0, qn1, qn2;
+  /* coupled flux/radiation (IBTYPE 32): ENAM/ENPH and EN0/EN1/EN2 (NVEL) */
+  std::vector<double> enam, enph, en0, en1, en2;
   int vortex_on = 0;
   orc_vortex_t vpar;
   std::vector<orc_vortex_fix_t> vfix;
@@ -645,8 +647,8 @@ orc_model *orc_model_create(const orc_params_t *p, orc_arrays_t *a) {
   /* NFLUXF, mesh.F:1907 etc.: any specified-flux segment */
   for (int I = 0; I < a->nvel; ++I) {
     const int lb = a->lbcodei[I];
-    if (lb == 2 || lb == 12 || lb == 22 || lb == 52) m->nfluxf = 1;
-    if (lb == 30) m->nfluxrbc = 1;
+    if (lb == 2 || lb == 12 || lb == 22 || lb == 32 || lb == 52) m->nfluxf = 1;
+    if (lb == 30 || lb == 32) m->nfluxrbc = 1;   /* mesh.F:2044-2045, 2056-2058 */
     if (lb == 40) m->nfluxgbc = 1;
   }
   /* EtaDisc at river-radiation nodes from the cold-start ETA2, cstart.F:1186-1191 */
@@ -657,6 +659,9 @@ orc_model *orc_model_create(const orc_params_t *p, orc_arrays_t *a) {
   m->qn0.assign(std::max(a->nvel, 1), 0.0);
   m->qn1 = m->qn0;
   m->qn2 = m->qn0;
+  m->en0 = m->qn0;
+  m->en1 = m->qn0;
+  m->en2 = m->qn0;
   m->wksp.assign((size_t)4 * a->np + 400 + 4 * (size_t)p->itmax, 0.0);
   m->tk_tmp.assign(a->np, 0.0);
   m->ncchange = 1; /* adcirc.F:404 */
@@ -719,6 +724,9 @@ int orc_model_shift_friction(orc_model *m, const orc_step_t *s) {
     m->qn0[I] = m->qn1[I];
     m->qn1[I] = m->qn2[I];
     m->qn2[I] = 0.0;
+    m->en0[I] = m->en1[I];
+    m->en1[I] = m->en2[I];
+    m->en2[I] = 0.0;
   }
   return 0;
 }
@@ -733,6 +741,13 @@ int orc_model_set_flux(orc_model *m, const orc_flux_t *f) {
   m->fface.assign(f->fface, f->fface + nf);
   m->qnam.assign(f->qnam, f->qnam + (size_t)nf * nv);
   m->qnph.assign(f->qnph, f->qnph + (size_t)nf * nv);
+  if (f->enam && f->enph) {
+    m->enam.assign(f->enam, f->enam + (size_t)nf * nv);
+    m->enph.assign(f->enph, f->enph + (size_t)nf * nv);
+  } else {
+    m->enam.assign((size_t)nf * nv, 0.0);
+    m->enph.assign((size_t)nf * nv, 0.0);
+  }
   m->flux_settling_it = f->flux_settling_it;
   m->flux_on = 1;
   return 0;
@@ -751,9 +766,12 @@ static void orc_model_flux(orc_model *m, const orc_step_t *s) {
       const double RFF = m->fff[J] * s->rampextflux;
       for (int I = 0; I < a->nvel; ++I) {
         const int lb = a->lbcodei[I];
-        if (lb == 2 || lb == 12 || lb == 22 || lb == 52)
+        if (lb == 2 || lb == 12 || lb == 22 || lb == 52 || lb == 32)
           m->qn2[I] = m->qn2[I] + m->qnam[J + (size_t)m->nffr * I] * RFF *
                                       std::cos(ARGJ - m->qnph[J + (size_t)m->nffr * I]);
+        if (lb == 32)
+          m->en2[I] = m->en2[I] + m->enam[J + (size_t)m->nffr * I] * RFF *
+                                      std::cos(ARGJ - m->enph[J + (size_t)m->nffr * I]);
       }
     }
   }
@@ -1005,6 +1023,12 @@ int orc_model_gwce(orc_model *m, const orc_step_t *s, orc_stepout_t *out) {
   if (m->nfluxf || m->nfluxrbc || m->nfluxgbc) {
     const double DT2 = p.dt * 2.0;
     auto qforce = [&](int J, int NBDJ) {
+      if (a->lbcodei[J] == 32) {   /* gwce.F:1792-1797 */
+        const double CELERITY = std::sqrt(G * a->h1[NBDJ]);
+        return (m->qn2[J] - m->qn0[J]) / DT2 -
+               CELERITY * (2.0 * a->etas[NBDJ] - (m->en2[J] - m->en0[J])) / DT2 +
+               a->tau0var[NBDJ] * (m->qn1[J] - CELERITY * (a->eta1[NBDJ] - m->en1[J]));
+      }
       if (a->lbcodei[J] == 40)   /* gwce.F:1804-1805 */
         return -(m->qn1[J] - m->qn0[J]) / DT - a->tau0var[NBDJ] * (m->qn1[J] + m->qn0[J]) / 2.0;
       if (a->lbcodei[J] == 30) {

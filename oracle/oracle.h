@@ -90,7 +90,7 @@ typedef struct {
 /* Periodic specified normal flux (same layout as adc_flux_t). */
 typedef struct {
   int nffr, flux_settling_it;
-  const double *famig, *fper, *fff, *fface, *qnam, *qnph;
+  const double *famig, *fper, *fff, *fface, *qnam, *qnph, *enam, *enph;
 } orc_flux_t;
 
 /* Parametric-vortex track (fort.22 fields HollandGet consumes,

@@ -63,7 +63,7 @@ class OrcStep(C.Structure):
 
 class OrcFlux(C.Structure):
     _fields_ = [("nffr", C.c_int), ("flux_settling_it", C.c_int)] + [
-        (n, dp_) for n in ("famig", "fper", "fff", "fface", "qnam", "qnph")]
+        (n, dp_) for n in ("famig", "fper", "fff", "fface", "qnam", "qnph", "enam", "enph")]
 
 
 class OrcStepOut(C.Structure):

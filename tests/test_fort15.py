@@ -221,3 +221,22 @@ def test_river_radiation_case_through_files(lib, orc, tmp_path):
         om.run(1, 500)
         om.close()
     assert np.array_equal(c.arrays["eta2"], c2.arrays["eta2"])
+
+
+def test_coupled_flux_radiation_case_through_files(lib, orc, tmp_path):
+    """IBTYPE 32: the four-item flux records (QNAM, QNPH, ENAM, ENPH)
+    survive the files, and the oracle steps both cases to the same state."""
+    import oracle
+    c = model.channel_case(river=0.5, river_type=32, river_eta=0.07)
+    adcirc_io.write_fort14(c.meta["raw"], tmp_path / "fort.14")
+    adcirc_io.write_fort15(tmp_path / "fort.15", model.fort15_for_case(c), c.sizes["neta"],
+                           c.arrays["lbcodei"][:c.sizes["nvel"]])
+    c2 = model.case_from_files(tmp_path / "fort.14", tmp_path / "fort.15")
+    assert np.array_equal(c.flux.enam, c2.flux.enam) and np.array_equal(c.flux.qnam, c2.flux.qnam)
+    for k, v in c.arrays.items():
+        assert np.array_equal(v, c2.arrays[k]), k
+    for case in (c, c2):
+        om = oracle.OracleModel(case)
+        om.run(1, 300)
+        om.close()
+    assert np.array_equal(c.arrays["eta2"], c2.arrays["eta2"])

@@ -267,3 +267,17 @@ def test_channel_zero_gradient_boundary(lib, orc):
     a = c0.arrays
     east = a["x"] > 59.9e3
     assert a["uu2"][east].mean() > 0.02
+
+
+def test_channel_coupled_flux_radiation(lib, orc):
+    """A coupled flux/radiation boundary (IBTYPE 32): flux and elevation
+    constituents (timestep.F:861-880) and the radiation condition against
+    the specified elevation in the GWCE boundary integral (gwce.F:
+    1792-1797), against the oracle over a graph-replayed run."""
+    from adcirc_b200 import model
+    c0, cg, io, ig = _pair(lambda **k: model.channel_case(river=0.5, river_type=32, **k), 1000,
+                           use_run=True)
+    _check(c0, cg, io, ig)
+    a = c0.arrays
+    east = a["x"] > 59.9e3
+    assert a["uu2"][east].mean() < -0.02

@@ -22,11 +22,12 @@ def _cases(orc):
     yield "radiation", lambda **k: model.channel_case(radiation=True, **k)
     yield "river52", lambda **k: model.channel_case(river=0.5, river_type=52, flux_settling=0.02, **k)
     yield "zerograd", lambda **k: model.channel_case(zero_gradient=True, **k)
+    yield "river32", lambda **k: model.channel_case(river=0.5, river_type=32, **k)
     yield "surge30k", lambda **k: model.surge_case(target_nodes=30_000, **k)
 
 
 @pytest.mark.parametrize("name", ["channel", "beach", "river2", "river22", "radiation", "river52",
-                                  "zerograd", "surge30k"])
+                                  "zerograd", "river32", "surge30k"])
 def test_case_tables_match(lib, orc, name):
     fn = dict(_cases(orc))[name]
     a = fn()
