@@ -15,8 +15,10 @@
 
 namespace adc {
 
+// Four 256-thread blocks per SM (64 registers): measured 0.057 ms per
+// launch on the surge mesh against 0.062 ms at the compiler's choice (68).
 template <class R>
-__global__ void k_mom_elem(adc_ctx c) {
+__global__ void __launch_bounds__(256, 4) k_mom_elem(adc_ctx c) {
   griddep_wait();
   __shared__ R sh[kThreads / 32][32 * 6];
   const int e0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31);
