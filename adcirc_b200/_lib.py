@@ -52,7 +52,7 @@ ARRAY_FIELDS = [
     ("wsx1", dp_), ("wsy1", dp_), ("wsx2", dp_), ("wsy2", dp_), ("pr1", dp_), ("pr2", dp_),
     ("coef", dp_), ("obccoef", dp_),
     ("gwce_lv", dp_), ("mom_lv_x", dp_), ("mom_lv_y", dp_),
-    ("nelezng", ip_), ("zngif1", dp_), ("zngif2", dp_), ("zngif3", dp_),
+    ("nelezng", ip_), ("zngif1", dp_), ("zngif2", dp_), ("zngif3", dp_), ("neitabele", ip_),
 ]
 
 
@@ -144,6 +144,7 @@ def load():
         "adc_mesh_csr_positions": (C.c_int, [C.c_int, C.c_int, C.c_int, ip_, ip_, C.c_int, ip_]),
         "adc_boundary_setup": (C.c_int, [C.c_int, dp_, dp_, C.c_int, ip_, ip_, ip_, C.c_double,
                                           C.c_int, ip_, ip_, ip_, dp_, dp_, ip_, ip_, dp_]),
+        "adc_mesh_neitabele": (C.c_int, [C.c_int, C.c_int, C.c_int, ip_, ip_, ip_, ip_]),
         "adc_zng_setup": (C.c_int, [C.c_int, C.c_int, dp_, dp_, ip_, C.c_int, ip_, ip_, dp_, C.c_int, ip_, ip_, dp_, dp_, ip_, dp_, dp_, dp_]),
         "adc_coldstart": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_double, dp_, ip_, dp_, dp_,
                                      dp_, ip_, ip_, ip_, ip_, dp_]),

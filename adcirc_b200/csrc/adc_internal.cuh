@@ -117,6 +117,8 @@ struct adc_ctx {
   int *obc_rhs_b;
   int *me_of_node;       // momentum BC entry per node or -1
   int *me_i;             // per momentum BC entry: its boundary entry (NVEL index)
+  int *me41_ptr;         // per momentum BC entry: its IBTYPE 41 triples [ptr, ptr+1)
+  int *me41_tri;         // (NM2, NM3, NeiTabEle element) triples, 0-based, element -1 = none
   // specified normal flux (flux.cu)
   int nfluxf, flux_on, nffr, n_fx;
   int nfluxrbc;          // radiation (IBTYPE 30) entries present

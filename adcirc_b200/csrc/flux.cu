@@ -70,7 +70,7 @@ __global__ void k_flux_forcing(adc_ctx c, const adc_step_t *steps, const Flags *
       c.elevdisc[I] = c.etadisc_b[I];
     }
   }
-  if (lb == 30 || lb == 40) {
+  if (lb == 30 || lb == 40 || lb == 41) {
     const int n = c.bnv[I];
     const double UN1 = c.uu1[n] * c.bcsii[I] + c.vv1[n] * c.bsiii[I];
     qn1[I] = c.h2[n] * UN1;
@@ -98,7 +98,7 @@ __global__ void k_flux_qforce(adc_ctx c, const adc_step_t *steps, Flags *flags) 
                   c.tau0[n] * (qn1[J] - CELERITY * (c.eta1[n] - en1[J]));
     return;
   }
-  if (c.blbc[J] == 40) {   // gwce.F:1804-1805
+  if (c.blbc[J] == 40 || c.blbc[J] == 41) {   // gwce.F:1804-1805
     c.qforce[J] = -(qn1[J] - qn0[J]) / c.p.dt - c.tau0[n] * (qn1[J] + qn0[J]) / 2.0;
     return;
   }
@@ -161,9 +161,9 @@ int flux_tables(adc_ctx *c, const adc_arrays_t *a) {
     const int lb = a->lbcodei[I];
     if (lb == 2 || lb == 12 || lb == 22 || lb == 32 || lb == 52) c->nfluxf = 1;
     if (lb == 30 || lb == 32) c->nfluxrbc = 1;
-    if (lb == 40) c->nfluxgbc = 1;
-    if (lb == 41 || lb == 64) {
-      set_error("boundary code %d (zero-gradient or river-radiation flux) is not implemented", lb);
+    if (lb == 40 || lb == 41) c->nfluxgbc = 1;
+    if (lb == 64) {
+      set_error("boundary code %d (condensed nodes) is not implemented", lb);
       return ADC_ERR_UNSUPPORTED;
     }
   }

@@ -13,6 +13,7 @@
  *   adc_mesh_csr_positions mesh.F:5261-5282   CSR_POSITION(NE,3,2)
  *   adc_boundary_setup     mesh.F:2100-2800   NBV, LBCODEI, CSII, SIII, ME2GW, BNDLEN2O3
  *   adc_zng_setup          mesh.F:2434-2512   NEleZNG, ZNGIF1-3 (IBTYPE 40)
+ *   adc_mesh_neitabele     mesh.F:3110-3131, 3248-3283   NeiTabEle
  *
  * All arrays use the reference layout: column-major, 1-based node numbers.
  */
@@ -169,7 +170,7 @@ int adc_mesh_csr_positions(int np, int ne, int mnei, const int *nm, const int *n
 /*
  * Flow-boundary arrays for external land segments (IBTYPE 0, 10, 20),
  * islands (IBTYPE 1, 11, 21), specified-flow (2, 12, 22), radiation (30),
- * coupled flux/radiation (32), zero-normal-gradient (40) and
+ * coupled flux/radiation (32), zero-normal-gradient (40, 41) and
  * river-radiation (52) segments,
  * mesh.F:2180-2800.  seg_ptr[k]..seg_ptr[k+1]-1
  * index seg_nodes (1-based node numbers, as listed in fort.14).  Outputs are
@@ -186,7 +187,7 @@ int adc_boundary_setup(int np, const double *x, const double *y, int nbou,
      where segments overlap (mesh.F:2529-2541, 2555-2566) */
   auto specified_flow = [](int code) {
     return code == 2 || code == 12 || code == 22 || code == 30 || code == 32 || code == 40 ||
-           code == 52;
+           code == 41 || code == 52;
   };
   for (int k = 0; k < nbou; ++k) {
     int t = ibtype[k];
@@ -282,6 +283,53 @@ int adc_boundary_setup(int np, const double *x, const double *y, int nbou,
   return ADC_OK;
 }
 
+
+/*
+ * NeiTabEle (NEIGHB, mesh.F:3110-3131, 3248-3283): for each node, its
+ * elements in the order of its NeiTab ring: going round the ring, the
+ * element with vertices (node, next neighbour, this neighbour) in
+ * counter-clockwise order, first match in element-number order; entries
+ * without such an element are skipped, so the list is packed from the
+ * front (zeros after it).  neitabele is NeiTabEle(NP,MNEI), 1-based.
+ */
+int adc_mesh_neitabele(int np, int ne, int mnei, const int *nm, const int *nneigh,
+                       const int *neitab, int *neitabele) {
+  if (np <= 0 || ne <= 0 || mnei < 3) return ADC_ERR_ARG;
+  std::vector<std::vector<int>> around(np);
+  for (int e = 0; e < ne; ++e)
+    for (int k = 0; k < 3; ++k) {
+      const int v = nm[e + (size_t)ne * k] - 1;
+      if (v < 0 || v >= np) return ADC_ERR_ARG;
+      around[v].push_back(e + 1);
+    }
+  std::memset(neitabele, 0, sizeof(int) * (size_t)np * mnei);
+  for (int i = 0; i < np; ++i) {
+    std::vector<int> cand = around[i];
+    const int nn = nneigh[i];
+    if (nn > mnei) return ADC_ERR_ARG;
+    int found = 0;
+    for (int j = 2; j <= nn; ++j) {
+      const int nn1 = i + 1;
+      const int nn3 = neitab[i + (size_t)np * (j - 1)];
+      const int nn2 = j != nn ? neitab[i + (size_t)np * j] : neitab[i + (size_t)np * 1];
+      for (int &e : cand) {
+        if (e == 0) continue;
+        const int a = nm[e - 1], b = nm[e - 1 + (size_t)ne], c = nm[e - 1 + 2 * (size_t)ne];
+        // the element's vertices rotated to start at the node
+        const int r2 = a == nn1 ? b : (b == nn1 ? c : a);
+        const int r3 = a == nn1 ? c : (b == nn1 ? a : b);
+        if (r2 == nn2 && r3 == nn3) {
+          if (found >= mnei) return ADC_ERR_MESH;
+          neitabele[i + (size_t)np * found] = e;
+          ++found;
+          e = 0;
+          break;
+        }
+      }
+    }
+  }
+  return ADC_OK;
+}
 
 /*
  * Fictitious interior nodes of the zero-normal-velocity-gradient entries

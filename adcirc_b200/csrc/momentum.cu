@@ -214,6 +214,33 @@ __global__ void k_mom_node(adc_ctx c) {
       a4 = csi;
       a2 = sii;
     }
+    if (lb == 41) {
+      // zero normal velocity gradient by a Galerkin normal derivative over
+      // the ring's elements (momentum.F:864-933), from the old velocities
+      double r1 = 0.0, r2 = 0.0, lhs = 0.0;
+      for (int q = c.me41_ptr[me]; q < c.me41_ptr[me + 1]; ++q) {
+        const int nm2 = c.me41_tri[3 * q], nm3 = c.me41_tri[3 * q + 1], e = c.me41_tri[3 * q + 2];
+        if (e < 0) continue;
+        const int NCEle = NCI * c.nodecode[nm2] * c.nodecode[nm3] * c.noff[e];
+        if (NCEle == 0) continue;
+        const double FDX1 = c.fdx[3 * e] * 1.0, FDX2 = c.fdx[3 * e + 1] * 1.0, FDX3 = c.fdx[3 * e + 2] * 1.0;
+        const double FDY1 = c.fdy[3 * e] * 1.0, FDY2 = c.fdy[3 * e + 1] * 1.0, FDY3 = c.fdy[3 * e + 2] * 1.0;
+        r1 = r1 - (csi * FDX2 + sii * FDY2) * c.uu1[nm2] - (csi * FDX3 + sii * FDY3) * c.uu1[nm3];
+        r2 = r2 - (csi * FDX2 + sii * FDY2) * c.vv1[nm2] - (csi * FDX3 + sii * FDY3) * c.vv1[nm3];
+        lhs = lhs + csi * FDX1 + sii * FDY1;
+      }
+      if (NCI == 0) {
+        mx = 0.0;
+        my = 0.0;
+      } else {
+        mx = r1 / lhs;
+        my = r2 / lhs;
+      }
+      a1 = 1.0;
+      a2 = 1.0;
+      a3 = 0.0;
+      a4 = 0.0;
+    }
   }
   c.mom_x[i] = mx;
   c.mom_y[i] = my;

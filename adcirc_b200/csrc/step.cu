@@ -188,6 +188,7 @@ struct HostTables {
   std::vector<int> is_nbd, nbd, obc_slot, obc_zero, obc_rhs_ptr, obc_rhs_node, obc_rhs_ent,
       obc_rhs_b, me_of_node, me_lbc, me_i;
   std::vector<double> me_csi, me_sii;
+  std::vector<int> me41_ptr, me41_tri;   // Galerkin zero-gradient (IBTYPE 41) neighbour triples
   std::vector<int> sell_of_ell;   // ELL (i + np*j), j >= 1 -> SELL idx or -1
 };
 
@@ -309,6 +310,28 @@ static int build_tables(const adc_arrays_t *a, HostTables &T, int &nslices, int 
     T.me_i.push_back(I);
     T.me_csi.push_back(a->csii[I]);
     T.me_sii.push_back(a->siii[I]);
+  }
+  // IBTYPE 41 (momentum.F:864-933): per momentum entry, the ring's
+  // (NM2, NM3, NeiTabEle) triples in the order the reference visits them,
+  // the wrap-around pair last; NeiTabEle is used positionally as there
+  T.me41_ptr.assign(1, 0);
+  for (int J = 0; J < a->nvelme; ++J) {
+    const int I = a->me2gw[J] - 1;
+    if (a->lbcodei[I] == 41) {
+      if (!a->neitabele) { set_error("IBTYPE 41 needs NeiTabEle"); return ADC_ERR_MESH; }
+      const int node = a->nbv[I] - 1, nn = a->nneigh[node];
+      auto NT = [&](int k) { return a->neitab[node + (size_t)np * (k - 1)] - 1; };
+      auto TE = [&](int k) { return a->neitabele[node + (size_t)np * (k - 1)] - 1; };
+      int nm2 = NT(2);
+      const int first = nm2;
+      for (int q = 3; q <= nn; ++q) {
+        const int nm3 = nm2;
+        nm2 = NT(q);
+        T.me41_tri.insert(T.me41_tri.end(), {nm2, nm3, TE(q - 2)});
+      }
+      T.me41_tri.insert(T.me41_tri.end(), {first, nm2, TE(nn - 1)});
+    }
+    T.me41_ptr.push_back((int)(T.me41_tri.size() / 3));
   }
   return ADC_OK;
 }
@@ -435,7 +458,8 @@ static void free_ctx(adc_ctx *c) {
       (void **)&c->emo, (void **)&c->efa, (void **)&c->obc_slot, (void **)&c->obc_zero,
       (void **)&c->obc_rhs_ptr, (void **)&c->obc_rhs_node, (void **)&c->obc_rhs_ent,
       (void **)&c->obc_rhs_b, (void **)&c->me_of_node, (void **)&c->me_lbc,
-      (void **)&c->me_csi, (void **)&c->me_sii, (void **)&c->me_i, (void **)&c->qn,
+      (void **)&c->me_csi, (void **)&c->me_sii, (void **)&c->me_i, (void **)&c->me41_ptr,
+      (void **)&c->me41_tri, (void **)&c->qn,
       (void **)&c->qforce, (void **)&c->fconst, (void **)&c->fqn, (void **)&c->bnv, (void **)&c->blbc,
       (void **)&c->bbl, (void **)&c->bcsii, (void **)&c->bsiii, (void **)&c->elevdisc, (void **)&c->etadisc_b, (void **)&c->en, (void **)&c->zng_node, (void **)&c->zng_ele, (void **)&c->zng_f, (void **)&c->fx_node, (void **)&c->fx_ptr, (void **)&c->fx_ent, (void **)&c->eta1, (void **)&c->eta2,
       (void **)&c->etas, (void **)&c->uu1, (void **)&c->vv1, (void **)&c->uu2, (void **)&c->vv2,
@@ -578,6 +602,9 @@ static int bind_impl(const adc_params_t *p, const adc_arrays_t *a, int prec, adc
   B(dalloc(&c->me_lbc, std::max<size_t>(T.me_lbc.size(), 1))); B(up(c->me_lbc, T.me_lbc.data(), T.me_lbc.size()));
   B(dalloc(&c->me_csi, std::max<size_t>(T.me_csi.size(), 1))); B(up(c->me_csi, T.me_csi.data(), T.me_csi.size()));
   B(dalloc(&c->me_sii, std::max<size_t>(T.me_sii.size(), 1))); B(up(c->me_sii, T.me_sii.data(), T.me_sii.size()));
+  B(dalloc(&c->me41_ptr, T.me41_ptr.size())); B(up(c->me41_ptr, T.me41_ptr.data(), T.me41_ptr.size()));
+  B(dalloc(&c->me41_tri, std::max<size_t>(T.me41_tri.size(), 1)));
+  if (!T.me41_tri.empty()) B(up(c->me41_tri, T.me41_tri.data(), T.me41_tri.size()));
   double **node_f64[] = {&c->eta1, &c->eta2, &c->etas, &c->uu1, &c->vv1, &c->uu2, &c->vv2, &c->qx1,
                          &c->qy1, &c->qx2, &c->qy2, &c->h1, &c->h2, &c->tk, &c->totalarea,
                          &c->wsx1, &c->wsy1, &c->wsx2, &c->wsy2, &c->pr1, &c->pr2, &c->gwce_lv,

@@ -253,13 +253,14 @@ class MeshPrep:
     boundary_setup: object
     coldstart: object
     zng_setup: object = None
+    neitabele: object = None
 
 
 def product_prep() -> MeshPrep:
     lib = _lib.load()
     return MeshPrep(lib.adc_mesh_geometry, lib.adc_mesh_mnei, lib.adc_mesh_neighb,
                     lib.adc_mesh_csr_positions, lib.adc_boundary_setup, lib.adc_coldstart,
-                    lib.adc_zng_setup)
+                    lib.adc_zng_setup, lib.adc_mesh_neitabele)
 
 
 def build_case(raw, params: dict, schedule: Schedule, tides, cf: float = 0.0025,
@@ -324,6 +325,13 @@ def build_case(raw, params: dict, schedule: Schedule, tides, cf: float = 0.0025,
     if rc != 0:
         raise RuntimeError(f"adc_boundary_setup failed: {rc}")
     nv, nme = nvel.value, nvelme.value
+    # NeiTabEle (used by the Galerkin zero-gradient entries, IBTYPE 41)
+    neitabele = np.zeros((npn, mnei), np.int32, order="F")
+    if lib.neitabele is not None:
+        rc = lib.neitabele(npn, ne, mnei, ptr(nm, ip_), ptr(nneigh, ip_), ptr(neitab, ip_),
+                           ptr(neitabele, ip_))
+        if rc != 0:
+            raise RuntimeError(f"NeiTabEle failed: {rc}")
     # zero-normal-gradient fictitious nodes (IBTYPE 40), mesh.F:2434-2512
     nvz = max(nv, 1)
     nelezng = np.zeros(nvz, np.int32)
@@ -361,7 +369,7 @@ def build_case(raw, params: dict, schedule: Schedule, tides, cf: float = 0.0025,
         csii=_f(csii[:max(nv, 1)], np.float64), siii=_f(siii[:max(nv, 1)], np.float64),
         me2gw=_f(me2gw[:max(nme, 1)], np.int32),
         bndlen2o3=_f(bndlen[:max(nv, 1)], np.float64),
-        nelezng=nelezng, zngif1=zngif[0], zngif2=zngif[1], zngif3=zngif[2],
+        nelezng=nelezng, zngif1=zngif[0], zngif2=zngif[1], zngif3=zngif[2], neitabele=neitabele,
     )
     for k in STATE_F64:
         A[k] = np.zeros(npn, np.float64)
@@ -530,7 +538,7 @@ K1_PERIOD = 86164.0
 
 def channel_case(dt: float = 5.0, amp: float = 0.5, vortex: bool = False,
                  river: float | None = None, river_type: int = 2, radiation: bool = False,
-                 zero_gradient: bool = False, flux_settling: float = 0.0, river_eta: float = 0.05,
+                 zero_gradient: int = 0, flux_settling: float = 0.0, river_eta: float = 0.05,
                  prep: MeshPrep | None = None, **kw) -> Case:
     """Tidal channel: 121x41 nodes, 20 m -> 5 m, M2 0.5 m, dt 5 s.  With
     `vortex`, a small Holland vortex (Rmax 8 km) crosses the channel.  With
@@ -540,8 +548,8 @@ def channel_case(dt: float = 5.0, amp: float = 0.5, vortex: bool = False,
     with `flux_settling` > 0 [days] holds the tide until the river flux has
     settled (NRAMP 2); IBTYPE 32 (coupled flux and radiation) also takes
     the steady elevation `river_eta` [m].  With `radiation`, the east end is a radiation
-    boundary (IBTYPE 30) the tide leaves through; with `zero_gradient`, a
-    zero-normal-velocity-gradient boundary (IBTYPE 40)."""
+    boundary (IBTYPE 30) the tide leaves through; with `zero_gradient` 40
+    (or True) or 41, a zero-normal-velocity-gradient boundary of that type."""
     from .meshgen import channel_mesh
     raw = channel_mesh()
     if river is not None or radiation or zero_gradient:
@@ -550,7 +558,8 @@ def channel_case(dt: float = 5.0, amp: float = 0.5, vortex: bool = False,
         south = np.array([nid(i, 0) for i in range(nx)])
         east = np.array([nid(nx - 1, j) for j in range(ny)])
         north = np.array([nid(i, ny - 1) for i in range(nx - 1, -1, -1)])
-        east_type = 30 if radiation else (40 if zero_gradient else river_type)
+        zg = 40 if zero_gradient is True else int(zero_gradient)
+        east_type = 30 if radiation else (zg if zg else river_type)
         raw.land_segments = [(0, south), (east_type, east), (0, north)]
     neta = raw.open_nodes.size
     tides = [(2.0 * math.pi / M2_PERIOD, 0.0, 1.0, np.full(neta, amp), np.zeros(neta))]

@@ -102,6 +102,7 @@ typedef struct {
    * factors (adc_zng_setup); NEleZNG = 0 off IBTYPE 40 entries */
   const int *nelezng;            /* NEleZNG(NVEL), 1-based */
   const double *zngif1, *zngif2, *zngif3;   /* (NVEL) */
+  const int *neitabele;          /* NeiTabEle(NP,MNEI), 1-based, 0 = none (IBTYPE 41) */
 } adc_arrays_t;
 
 /* Per-step scalars TIMESTEP computes before the hot path (timestep.F:257-353). */
@@ -392,8 +393,9 @@ int adc_selftest_div_const(long long n, unsigned long long seed, long long *mism
  * (timestep.F:314-345).  Zero-normal-gradient entries (IBTYPE 40) need the
  * NEleZNG/ZNGIF tables of adc_zng_setup in adc_arrays_t.  Coupled
  * flux/radiation entries (IBTYPE 32) take their elevation constituents from
- * enam/enph (gwce.F:1792-1797).  Codes 41 and 64 are refused at bind with
- * ADC_ERR_UNSUPPORTED. */
+ * enam/enph (gwce.F:1792-1797); Galerkin zero-gradient entries (IBTYPE 41)
+ * need NeiTabEle (adc_mesh_neitabele) in adc_arrays_t.  Code 64 is refused
+ * at bind with ADC_ERR_UNSUPPORTED. */
 int adc_set_flux(adc_ctx *ctx, const adc_flux_t *flux);
 
 /* No reference counterpart (the reference always starts JCG from ETAS as
@@ -528,6 +530,10 @@ int adc_boundary_setup(int np, const double *x, const double *y, int nbou,
                        double cos_inner, int nvel_max, int *nvel, int *nbv,
                        int *lbcodei, double *csii, double *siii, int *nvelme,
                        int *me2gw, double *bndlen2o3);
+/* NeiTabEle (NEIGHB, mesh.F:3110-3131, 3248-3283): each node's elements in
+ * the order of its NeiTab ring, packed from the front. */
+int adc_mesh_neitabele(int np, int ne, int mnei, const int *nm, const int *nneigh,
+                       const int *neitab, int *neitabele);
 /* Zero-normal-gradient (IBTYPE 40) fictitious nodes (mesh.F:2434-2512):
  * NEleZNG and the interpolation factors ZNGIF1-3 per boundary entry. */
 int adc_zng_setup(int np, int ne, const double *x, const double *y, const int *nm, int mnei,

@@ -33,7 +33,7 @@ module adcgpu_iface
       type(c_ptr) :: tk, tkm, nodecode, nnodecode, noff, mju, totalarea, alphal
       type(c_ptr) :: wsx1, wsy1, wsx2, wsy2, pr1, pr2, coef, obccoef
       type(c_ptr) :: gwce_lv, mom_lv_x, mom_lv_y
-      type(c_ptr) :: nelezng, zngif1, zngif2, zngif3
+      type(c_ptr) :: nelezng, zngif1, zngif2, zngif3, neitabele
    end type
 
    type, bind(C), public :: adc_step_t

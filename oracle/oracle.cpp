@@ -649,7 +649,7 @@ orc_model *orc_model_create(const orc_params_t *p, orc_arrays_t *a) {
     const int lb = a->lbcodei[I];
     if (lb == 2 || lb == 12 || lb == 22 || lb == 32 || lb == 52) m->nfluxf = 1;
     if (lb == 30 || lb == 32) m->nfluxrbc = 1;   /* mesh.F:2044-2045, 2056-2058 */
-    if (lb == 40) m->nfluxgbc = 1;
+    if (lb == 40 || lb == 41) m->nfluxgbc = 1;
   }
   /* EtaDisc at river-radiation nodes from the cold-start ETA2, cstart.F:1186-1191 */
   m->elevdisc.assign(std::max(a->nvel, 1), 0.0);
@@ -801,7 +801,7 @@ static void orc_model_flux(orc_model *m, const orc_step_t *s) {
   /* zero normal velocity gradient entries, timestep.F:945-952 */
   if (m->nfluxgbc) {
     for (int J = 0; J < a->nvel; ++J) {
-      if (a->lbcodei[J] != 40) continue;
+      if (a->lbcodei[J] != 40 && a->lbcodei[J] != 41) continue;
       const int NNBB = a->nbv[J] - 1;
       const double UN1 = a->uu1[NNBB] * a->csii[J] + a->vv1[NNBB] * a->siii[J];
       m->qn1[J] = a->h2[NNBB] * UN1;
@@ -1029,7 +1029,7 @@ int orc_model_gwce(orc_model *m, const orc_step_t *s, orc_stepout_t *out) {
                CELERITY * (2.0 * a->etas[NBDJ] - (m->en2[J] - m->en0[J])) / DT2 +
                a->tau0var[NBDJ] * (m->qn1[J] - CELERITY * (a->eta1[NBDJ] - m->en1[J]));
       }
-      if (a->lbcodei[J] == 40)   /* gwce.F:1804-1805 */
+      if (a->lbcodei[J] == 40 || a->lbcodei[J] == 41)   /* gwce.F:1804-1805 */
         return -(m->qn1[J] - m->qn0[J]) / DT - a->tau0var[NBDJ] * (m->qn1[J] + m->qn0[J]) / 2.0;
       if (a->lbcodei[J] == 30) {
         const double CELERITY = std::sqrt(G * a->h1[NBDJ]);
@@ -1367,7 +1367,7 @@ int orc_model_momentum(orc_model *m, const orc_step_t *s) {
     AUV[4 * (size_t)i + 2] = VCOEFXY * NCI;
     AUV[4 * (size_t)i + 3] = VCOEFYX * NCI;
   }
-  /* velocity BCs, momentum.F:810-862 (LBCODEI 0-9 and 10-19) */
+  /* velocity BCs, momentum.F:810-933 (LBCODEI 0-9, 10-19 and 41) */
   const double sqrt2 = std::sqrt(2.0);
   for (int J = 0; J < a->nvelme; ++J) {
     int I = a->me2gw[J] - 1;
@@ -1403,6 +1403,52 @@ int orc_model_momentum(orc_model *m, const orc_step_t *s) {
       auv[2] = -csi;
       auv[3] = csi;
       auv[1] = sii;
+    }
+    /* Galerkin zero normal velocity gradient, momentum.F:864-933 */
+    if (lb == 41) {
+      const int np_ = a->np;
+      auto NeiTab = [&](int k) { return a->neitab[NBDI + (size_t)np_ * (k - 1)]; };
+      auto NeiTabEle = [&](int k) { return a->neitabele[NBDI + (size_t)np_ * (k - 1)]; };
+      auto FDXE = [&](int k, int e) { return a->fdxe[(k - 1) + 3 * (size_t)(e - 1)]; };
+      auto FDYE = [&](int k, int e) { return a->fdye[(k - 1) + 3 * (size_t)(e - 1)]; };
+      double ZNGRHS1 = 0.0, ZNGRHS2 = 0.0, ZNGLHS = 0.0;
+      auto contribution = [&](int NM2, int NM3, int NEle) {
+        if (NEle == 0) return;
+        const int NCEle = NCI * a->nodecode[NM2 - 1] * a->nodecode[NM3 - 1] * a->noff[NEle - 1];
+        if (NCEle == 0) return;
+        const double sfdxfac = 1.0, sfdyfac = 1.0;   /* SFacEle = SFMXEle = SFMYEle = 1, IFSFM = 0 */
+        const double FDX1 = FDXE(1, NEle) * sfdxfac, FDX2 = FDXE(2, NEle) * sfdxfac,
+                     FDX3 = FDXE(3, NEle) * sfdxfac;
+        const double FDY1 = FDYE(1, NEle) * sfdyfac, FDY2 = FDYE(2, NEle) * sfdyfac,
+                     FDY3 = FDYE(3, NEle) * sfdyfac;
+        ZNGRHS1 = ZNGRHS1 - (csi * FDX2 + sii * FDY2) * a->uu1[NM2 - 1] -
+                  (csi * FDX3 + sii * FDY3) * a->uu1[NM3 - 1];
+        ZNGRHS2 = ZNGRHS2 - (csi * FDX2 + sii * FDY2) * a->vv1[NM2 - 1] -
+                  (csi * FDX3 + sii * FDY3) * a->vv1[NM3 - 1];
+        ZNGLHS = ZNGLHS + csi * FDX1 + sii * FDY1;
+      };
+      int NM2 = NeiTab(2), NM3 = 0;
+      const int NNFirst = NM2;
+      const int nn = a->nneigh[NBDI];
+      for (int N = 3; N <= nn; ++N) {
+        NM3 = NM2;
+        NM2 = NeiTab(N);
+        contribution(NM2, NM3, NeiTabEle(N - 2));
+      }
+      NM3 = NM2;
+      NM2 = NNFirst;
+      contribution(NM2, NM3, NeiTabEle(nn - 1));
+      if (NCI == 0) {
+        a->mom_lv_x[NBDI] = 0.0;
+        a->mom_lv_y[NBDI] = 0.0;
+      } else {
+        a->mom_lv_x[NBDI] = ZNGRHS1 / ZNGLHS;
+        a->mom_lv_y[NBDI] = ZNGRHS2 / ZNGLHS;
+      }
+      auv[0] = 1.0;
+      auv[1] = 1.0;
+      auv[2] = 0.0;
+      auv[3] = 0.0;
     }
   }
   /* 2x2 solve, momentum.F:1128-1138; fluxes :1179-1182 */

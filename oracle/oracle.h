@@ -78,6 +78,7 @@ typedef struct {
   double *gwce_lv, *mom_lv_x, *mom_lv_y;
   const int *nelezng;       /* NEleZNG(NVEL), 1-based (IBTYPE 40 entries) */
   const double *zngif1, *zngif2, *zngif3;
+  const int *neitabele;     /* NeiTabEle(NP,MNEI), 1-based, 0 = none */
 } orc_arrays_t;
 
 /* Per-step scalars the TIMESTEP driver computes before the hot path. */
@@ -174,6 +175,8 @@ int orc_boundary_setup(int np, const double *x, const double *y, int nbou, const
                        const int *seg_ptr, const int *seg_nodes, double costset, int nvel_max,
                        int *nvel_out, int *nbv, int *lbcodei, double *csii, double *siii,
                        int *nvelme_out, int *me2gw, double *bndlen2o3);
+int orc_mesh_neitabele(int np, int ne, int mnei, const int *nm, const int *nneigh,
+                       const int *neitab, int *neitabele);
 int orc_zng_setup(int np, int ne, const double *x, const double *y, const int *nm, int mnei,
                   const int *nneigh, const int *neitab, const double *areas, int nvel,
                   const int *nbv, const int *lbcodei, const double *csii, const double *siii,

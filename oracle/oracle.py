@@ -46,7 +46,7 @@ _ARR = [
     ("wsx1", dp_), ("wsy1", dp_), ("wsx2", dp_), ("wsy2", dp_), ("pr1", dp_), ("pr2", dp_),
     ("coef", dp_), ("obccoef", dp_),
     ("gwce_lv", dp_), ("mom_lv_x", dp_), ("mom_lv_y", dp_),
-    ("nelezng", ip_), ("zngif1", dp_), ("zngif2", dp_), ("zngif3", dp_),
+    ("nelezng", ip_), ("zngif1", dp_), ("zngif2", dp_), ("zngif3", dp_), ("neitabele", ip_),
 ]
 
 
@@ -139,6 +139,7 @@ def load(omp: bool = False):
         "orc_mesh_csr_positions": [C.c_int, C.c_int, C.c_int, ip_, ip_, C.c_int, ip_],
         "orc_boundary_setup": [C.c_int, dp_, dp_, C.c_int, ip_, ip_, ip_, C.c_double, C.c_int,
                                ip_, ip_, ip_, dp_, dp_, ip_, ip_, dp_],
+        "orc_mesh_neitabele": [C.c_int, C.c_int, C.c_int, ip_, ip_, ip_, ip_],
         "orc_zng_setup": [C.c_int, C.c_int, dp_, dp_, ip_, C.c_int, ip_, ip_, dp_, C.c_int, ip_, ip_, dp_, dp_, ip_, dp_, dp_, dp_],
         "orc_coldstart_arrays": [C.c_int, C.c_int, C.c_int, C.c_double, dp_, ip_, dp_, dp_, dp_,
                                  ip_, ip_, ip_, ip_, dp_],
@@ -282,7 +283,8 @@ def mesh_prep():
     return types.SimpleNamespace(
         geometry=lib.orc_mesh_geometry, mnei=lib.orc_mesh_mnei, neighb=lib.orc_mesh_neighb,
         csr_positions=lib.orc_mesh_csr_positions, boundary_setup=lib.orc_boundary_setup,
-        coldstart=lib.orc_coldstart_arrays, zng_setup=lib.orc_zng_setup)
+        coldstart=lib.orc_coldstart_arrays, zng_setup=lib.orc_zng_setup,
+        neitabele=lib.orc_mesh_neitabele)
 
 
 def dfault():

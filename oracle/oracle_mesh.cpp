@@ -19,6 +19,7 @@
  *   orc_mesh_csr_positions   mesh.F:5261-5282  compute_csr_positions
  *   orc_boundary_setup       mesh.F:2226-2568  NBV, LBCODEI, CSII, SIII, ME2GW, BNDLEN2O3
  *   orc_zng_setup            mesh.F:2434-2512  NEleZNG, ZNGIF1-3 (IBTYPE 40)
+ *   orc_mesh_neitabele       mesh.F:3110-3131, 3248-3283  NeiTabEle
  *   orc_coldstart_arrays     cstart.F:1332-1427 + totalAreaCalc mesh.F:3360-3400
  */
 #include "oracle.h"
@@ -218,8 +219,8 @@ int orc_mesh_csr_positions(int np, int ne, int mnei, const int *nm, const int *n
 
 /* Flow-boundary tables of mesh.F:2226-2568 for the land-segment types of
  * the path (external 0/10/20, island 1/11/21, specified flow 2/12/22,
- * radiation 30, coupled flux/radiation 32, zero normal gradient 40, river
- * radiation 52):
+ * radiation 30, coupled flux/radiation 32, zero normal gradient 40/41,
+ * river radiation 52):
  * segment closure (:2226-2244), per node the GWCE entry NBV/LBCODEI with
  * the inner-angle test (:2266-2411), BNDLEN2O3 (:2301-2303), the outward
  * normal CSII/SIII (:2421-2433, including the FLG_IBLEN2 special case of a
@@ -240,7 +241,7 @@ int orc_boundary_setup(int np, const double *x, const double *y, int nbou, const
     const int t = ibtype[k];
     const bool island = (t == 1 || t == 11 || t == 21);
     if (!(island || t == 0 || t == 10 || t == 20 || t == 2 || t == 12 || t == 22 || t == 30 ||
-          t == 32 || t == 40 || t == 52))
+          t == 32 || t == 40 || t == 41 || t == 52))
       return -1;
     int nvell = seg_ptr[k + 1] - seg_ptr[k];
     if (nvell < 2) return -1;
@@ -344,6 +345,56 @@ int orc_boundary_setup(int np, const double *x, const double *y, int nbou, const
   }
   *nvel_out = jgw;
   *nvelme_out = jme;
+  return 0;
+}
+
+/* NeiTabEle, NEIGHB mesh.F:3110-3131 (each element appended to its three
+ * nodes' lists in element order) and :3248-3283 (for J = 2..NNeigh, the
+ * element (NN1, NN2, NN3) = (I, NeiTab(I,J+1) or NeiTab(I,2) at the end,
+ * NeiTab(I,J)) in counter-clockwise order, packed as NN = NN + 1). */
+int orc_mesh_neitabele(int np, int ne, int mnei, const int *nm, const int *nneigh,
+                       const int *neitab, int *neitabele) {
+  if (np <= 0 || ne <= 0 || mnei < 3) return -1;
+  CI2 NM{nm, ne}, NeiTab{neitab, np};
+  I2 NeiTabEle{neitabele, np};
+  std::vector<int> NNeighEle(np + 1, 0);
+  std::vector<int> lists((size_t)np * mnei * 2, 0);   /* elements around each node */
+  const int cap = mnei * 2;
+  for (int i = 1; i <= np; ++i)
+    for (int k = 1; k <= mnei; ++k) NeiTabEle(i, k) = 0;
+  for (int N = 1; N <= ne; ++N)
+    for (int k = 1; k <= 3; ++k) {
+      const int v = NM(N, k);
+      if (v < 1 || v > np || NNeighEle[v] >= cap) return -1;
+      lists[(size_t)(v - 1) * cap + NNeighEle[v]] = N;
+      NNeighEle[v] = NNeighEle[v] + 1;
+    }
+  for (int I = 1; I <= np; ++I) {
+    std::vector<int> NEITEM(lists.begin() + (size_t)(I - 1) * cap,
+                            lists.begin() + (size_t)(I - 1) * cap + NNeighEle[I]);
+    int NN = 0;
+    for (int J = 2; J <= nneigh[I - 1]; ++J) {
+      const int NN1 = NeiTab(I, 1);
+      const int NN3 = NeiTab(I, J);
+      const int NN2 = J != nneigh[I - 1] ? NeiTab(I, J + 1) : NeiTab(I, 2);
+      int NE1 = 0, NE2 = 0, NE3 = 0;
+      for (int K = 0; K < (int)NEITEM.size(); ++K) {
+        if (NEITEM[K] == 0) continue;
+        const int e = NEITEM[K];
+        if (NM(e, 1) == NN1) { NE1 = NM(e, 1); NE2 = NM(e, 2); NE3 = NM(e, 3); }
+        if (NM(e, 2) == NN1) { NE1 = NM(e, 2); NE2 = NM(e, 3); NE3 = NM(e, 1); }
+        if (NM(e, 3) == NN1) { NE1 = NM(e, 3); NE2 = NM(e, 1); NE3 = NM(e, 2); }
+        if (NE2 == NN2 && NE3 == NN3) {
+          NN = NN + 1;
+          if (NN > mnei) return -1;
+          NeiTabEle(I, NN) = e;
+          NEITEM[K] = 0;
+          break;
+        }
+      }
+      (void)NE1;
+    }
+  }
   return 0;
 }
 

@@ -281,3 +281,16 @@ def test_channel_coupled_flux_radiation(lib, orc):
     a = c0.arrays
     east = a["x"] > 59.9e3
     assert a["uu2"][east].mean() < -0.02
+
+
+def test_channel_galerkin_zero_gradient_boundary(lib, orc):
+    """The Galerkin zero-normal-velocity-gradient boundary (IBTYPE 41): the
+    momentum equations of its nodes replaced by the normal derivative over
+    the ring's elements (momentum.F:864-933, NeiTabEle used positionally as
+    there), against the oracle over a graph-replayed run."""
+    from adcirc_b200 import model
+    c0, cg, io, ig = _pair(lambda **k: model.channel_case(zero_gradient=41, **k), 1500, use_run=True)
+    _check(c0, cg, io, ig)
+    a = c0.arrays
+    east = a["x"] > 59.9e3
+    assert a["uu2"][east].mean() > 0.02

@@ -23,11 +23,12 @@ def _cases(orc):
     yield "river52", lambda **k: model.channel_case(river=0.5, river_type=52, flux_settling=0.02, **k)
     yield "zerograd", lambda **k: model.channel_case(zero_gradient=True, **k)
     yield "river32", lambda **k: model.channel_case(river=0.5, river_type=32, **k)
+    yield "zerograd41", lambda **k: model.channel_case(zero_gradient=41, **k)
     yield "surge30k", lambda **k: model.surge_case(target_nodes=30_000, **k)
 
 
 @pytest.mark.parametrize("name", ["channel", "beach", "river2", "river22", "radiation", "river52",
-                                  "zerograd", "river32", "surge30k"])
+                                  "zerograd", "river32", "zerograd41", "surge30k"])
 def test_case_tables_match(lib, orc, name):
     fn = dict(_cases(orc))[name]
     a = fn()
@@ -95,3 +96,23 @@ def test_neighb_rejects_coincident_nodes(orc):
     rc = orc.load().orc_mesh_neighb(4, 2, 6, ptr(x, dp_), ptr(y, dp_), ptr(nm, ip_),
                                     ptr(nneigh, ip_), ptr(neitab, ip_), C.byref(mx))
     assert rc == -4
+
+
+def test_neitabele_packs_each_ring(lib, orc):
+    """NeiTabEle (mesh.F:3248-3283): every interior node lists one element
+    per neighbour pair of its ring, every boundary node one fewer, each
+    element holding the node."""
+    from adcirc_b200 import model
+    c = model.channel_case(prep=orc.mesh_prep())
+    a = c.arrays
+    te, nn, nm = a["neitabele"], a["nneigh"], a["nm"] - 1
+    nv = c.sizes["nvel"]
+    boundary = np.zeros(c.sizes["np"], bool)
+    boundary[a["nbv"][:nv] - 1] = True
+    boundary[a["nbd"] - 1] = True
+    cnt = (te > 0).sum(axis=1)
+    assert np.array_equal(cnt[~boundary], nn[~boundary] - 1)
+    assert np.array_equal(cnt[boundary], nn[boundary] - 2)
+    for i in range(0, c.sizes["np"], 97):
+        for e in te[i][te[i] > 0] - 1:
+            assert i in nm[e]
