@@ -72,6 +72,11 @@ class AdcFlux(C.Structure):
         (n, dp_) for n in ("famig", "fper", "fff", "fface", "qnam", "qnph", "enam", "enph")]
 
 
+class AdcSeries(C.Structure):
+    _fields_ = [("nrec", C.c_int), ("flux_settling_it", C.c_int), ("interval", C.c_double),
+                ("start_time", C.c_double), ("values", dp_), ("values2", dp_)]
+
+
 class AdcVortexFix(C.Structure):
     _fields_ = [(n, C.c_double) for n in ("time", "x", "y", "cpress", "vmax", "rmw", "tvx", "tvy")]
 
@@ -166,6 +171,10 @@ def load():
         "adc_set_met": (C.c_int, [vp, dp_, dp_, dp_]),
         "adc_set_vortex": (C.c_int, [vp, C.POINTER(AdcVortex)]),
         "adc_set_flux": (C.c_int, [vp, C.POINTER(AdcFlux)]),
+        "adc_set_elev_series": (C.c_int, [vp, C.POINTER(AdcSeries)]),
+        "adc_set_flux_series": (C.c_int, [vp, C.POINTER(AdcSeries)]),
+        "adc_fort19_read": (C.c_int, [C.c_char_p, C.c_int, ip_, dp_, dp_]),
+        "adc_fort20_read": (C.c_int, [C.c_char_p, C.c_int, ip_, ip_, dp_, dp_, dp_]),
         "adc_fort14_dims": (C.c_int, [C.c_char_p, ip_]),
         "adc_fort14_read": (C.c_int, [C.c_char_p, C.c_char_p, dp_, dp_, dp_, ip_, ip_, ip_, ip_, ip_, ip_]),
         "adc_fort15_read": (C.c_int, [C.c_char_p, C.c_int, C.c_int, ip_, C.POINTER(AdcFort15),

@@ -200,3 +200,63 @@ def write_fort15(path, f: Fort15, neta: int, lbcodei) -> None:
         C.memmove(tags[cnt], buf, min(len(buf), C.sizeof(tags[cnt])))
     _check(lib.adc_fort15_write(os.fsencode(path), C.byref(f.p), int(neta), nvel, ptr(lbc, ip_),
                                 C.byref(t)), "adc_fort15_write")
+
+
+def read_fort19(path, neta: int, start_time: float = 0.0):
+    """Reads a fort.19 non-periodic elevation boundary file
+    (adc_fort19_read) into a model.Series of (nrec, NETA) records."""
+    from .model import Series
+    lib = _lib.load()
+    p = os.fsencode(path)
+    n, inc = C.c_int(0), C.c_double(0.0)
+    _check(lib.adc_fort19_read(p, int(neta), C.byref(n), C.byref(inc), None), "adc_fort19_read")
+    vals = np.zeros((n.value, int(neta)))
+    _check(lib.adc_fort19_read(p, int(neta), C.byref(n), C.byref(inc), ptr(vals, dp_)),
+           "adc_fort19_read")
+    return Series(inc.value, vals, start_time=start_time)
+
+
+def read_fort20(path, lbcodei, start_time: float = 0.0, flux_settling_it: int = 0):
+    """Reads a fort.20 non-periodic normal-flux file (adc_fort20_read) into a
+    model.Series of (nrec, NVEL) fluxes, with the elevations of code-32
+    entries as values2 when there are any.  lbcodei: LBCODEI of the
+    flux-boundary nodes (a Case's arrays['lbcodei'])."""
+    from .model import Series
+    lib = _lib.load()
+    p = os.fsencode(path)
+    lbc = np.ascontiguousarray(np.asarray(lbcodei, np.int32).ravel())
+    nv = int(lbc.size)
+    n, inc = C.c_int(0), C.c_double(0.0)
+    _check(lib.adc_fort20_read(p, nv, ptr(lbc, ip_), C.byref(n), C.byref(inc), None, None),
+           "adc_fort20_read")
+    q = np.zeros((n.value, nv))
+    e = np.zeros((n.value, nv))
+    _check(lib.adc_fort20_read(p, nv, ptr(lbc, ip_), C.byref(n), C.byref(inc), ptr(q, dp_),
+                               ptr(e, dp_)), "adc_fort20_read")
+    return Series(inc.value, q, e if (lbc == 32).any() else None, start_time=start_time,
+                  flux_settling_it=flux_settling_it)
+
+
+def write_fort19(path, series) -> None:
+    """Writes a model.Series as a fort.19: the interval, then one value per
+    line, record after record (17 significant digits)."""
+    with open(path, "w") as f:
+        f.write(f"{series.interval!r}\n")
+        for rec in np.asarray(series.values):
+            f.writelines(f"{float(v)!r}\n" for v in rec)
+
+
+def write_fort20(path, series, lbcodei) -> None:
+    """Writes a model.Series as a fort.20: the interval, then per record one
+    line per entry of code 2/12/22 (its flux) or 32 (flux and elevation)."""
+    lbc = np.asarray(lbcodei).ravel()
+    e = series.values2
+    with open(path, "w") as f:
+        f.write(f"{series.interval!r}\n")
+        for k, rec in enumerate(np.asarray(series.values)):
+            for j, lb in enumerate(lbc):
+                if lb in (2, 12, 22):
+                    f.write(f"{float(rec[j])!r}\n")
+                elif lb == 32:
+                    ev = 0.0 if e is None else float(e[k, j])
+                    f.write(f"{float(rec[j])!r} {ev!r}\n")

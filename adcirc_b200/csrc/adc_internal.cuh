@@ -81,6 +81,15 @@ struct VortexState {
   double x, y, cpress, dpdef, spd, b, rmw, tvx, tvy;
 };
 
+// Position in a non-periodic boundary series (fort.19 / fort.20): the two
+// record times the reference holds (ETIME1/ETIME2, QTIME1/QTIME2), the index
+// of the earlier record and this step's interpolation ratio.
+struct SeriesState {
+  double t1, t2, ratio;
+  int k;
+  int err;       // set when the run passes the last record
+};
+
 // Choice and statistics of the extrapolated JCG initial guess.
 struct WarmState {
   int use;         // this step starts from the extrapolated guess
@@ -131,6 +140,13 @@ struct adc_ctx {
   double *en;            // EN0, EN1, EN2 (NVEL each): specified elevation of IBTYPE 32
   int fen;               // ENAM/ENPH follow QNAM/QNPH in fqn
   double *etadisc_b;     // EtaDisc at the boundary entries' nodes
+  // non-periodic boundary series: fort.19 elevations (NETA per record) and
+  // fort.20 fluxes and elevations (NVEL per record); sstate[0] elevation,
+  // sstate[1] flux
+  int eser_on, fser_on, eser_nrec, fser_nrec;
+  double eser_interval, fser_interval;
+  double *eser, *fser_q, *fser_e;
+  SeriesState *sstate;
   double *qn;            // QN0, QN1, QN2 (NVEL each)
   double *qforce;        // per boundary entry: the GWCE line-integral force
   double *fconst, *fqn;  // FAMIG/FPER/FFF/FFACE, then QNAM and QNPH (NFFR x NVEL)

@@ -24,12 +24,43 @@
 //  * the specified normal velocity -QN2/H2 of the momentum boundary
 //    conditions (momentum.F:815-856), read in k_mom_node; radiation nodes
 //    take no momentum boundary condition.
+// It also holds the non-periodic boundary series: fort.20 fluxes in place of
+// the periodic constituents (NFFR <= 0, timestep.F:882-903) and fort.19
+// elevations added to the periodic boundary elevation in k_eta_bc
+// (gwce.F:1659-1674).  Both files sit whole in HBM; k_series_state moves
+// the pair of record times as the reference's reads do.
 #include "adc_internal.cuh"
 
+#include <cmath>
 #include <cstring>
 #include <vector>
 
 namespace adc {
+
+// One thread: per active series, the record pair and ratio of this step.
+// The reference reads the next record when TimeLoc passes the later record
+// time, at most once per step (gwce.F:1660-1668, timestep.F:882-900).
+__global__ void k_series_state(adc_ctx c, const adc_step_t *steps, Flags *flags) {
+  griddep_wait();
+  const double timeloc = steps[flags->cursor].timeloc;
+  for (int s = 0; s < 2; ++s) {
+    if (!(s == 0 ? c.eser_on : c.fser_on)) continue;
+    SeriesState &st = c.sstate[s];
+    const int nrec = s == 0 ? c.eser_nrec : c.fser_nrec;
+    const double inc = s == 0 ? c.eser_interval : c.fser_interval;
+    if (timeloc > st.t2) {
+      st.t1 = st.t2;
+      st.t2 = st.t1 + inc;
+      st.k = st.k + 1;
+      if (st.k + 1 >= nrec) {   // the file has no further record
+        st.err = 1;
+        flags->status = ADC_ERR_ARG;
+        st.k = nrec - 2;
+      }
+    }
+    st.ratio = (timeloc - st.t1) / inc;
+  }
+}
 
 __global__ void k_flux_forcing(adc_ctx c, const adc_step_t *steps, const Flags *flags) {
   griddep_wait();
@@ -58,6 +89,11 @@ __global__ void k_flux_forcing(adc_ctx c, const adc_step_t *steps, const Flags *
       q = q + qnam[J + (size_t)nf * I] * RFF * cos(ARGJ - qnph[J + (size_t)nf * I]);
       if (coupled) el = el + enam[J + (size_t)nf * I] * RFF * cos(ARGJ - enph[J + (size_t)nf * I]);
     }
+  } else if (c.fser_on) {   // timestep.F:900-902, every entry
+    const SeriesState &ss = c.sstate[1];
+    const size_t r1 = (size_t)ss.k * c.nvel, r2 = r1 + c.nvel;
+    q = st.rampextflux * (c.fser_q[r1 + I] + ss.ratio * (c.fser_q[r2 + I] - c.fser_q[r1 + I]));
+    el = st.rampextflux * (c.fser_e[r1 + I] + ss.ratio * (c.fser_e[r2 + I] - c.fser_e[r1 + I]));
   }
   qn2[I] = q;
   en2[I] = el;
@@ -135,6 +171,10 @@ __global__ void k_flux_rhs(adc_ctx c) {
 }
 
 int launch_flux_forcing(adc_ctx *c) {
+  if (c->eser_on || c->fser_on) {
+    launch_k(k_series_state, 1, 1, c->stream, *c, c->steps, c->flags);
+    c->launches++;
+  }
   if (!c->nfluxf && !c->nfluxrbc && !c->nfluxgbc) return ADC_OK;
   launch_k(k_flux_forcing, nblk(c->nvel), kThreads, c->stream, *c, c->steps, c->flags);
   c->launches++;
@@ -282,6 +322,79 @@ extern "C" int adc_set_flux(adc_ctx *c, const adc_flux_t *f) {
   c->nffr = nf;
   c->flux_settling_it = f->flux_settling_it;
   c->flux_on = 1;
+  c->fser_on = 0;
   drop_graphs(c);   // replayed steps must see the forcing
   return ADC_OK;
+}
+
+// Checks a series and uploads its records (width values per record; a
+// second table of the same shape when values2 is given, zeros otherwise).
+static int series_upload(adc_ctx *c, const adc_series_t *s, int width, const char *what,
+                         double **v1, double **v2) {
+  if (!s || s->nrec < 2 || !s->values || !(s->interval > 0.0) || !std::isfinite(s->start_time)) {
+    set_error("%s: at least two records, a positive interval and a finite start time are required",
+              what);
+    return ADC_ERR_ARG;
+  }
+  if (!c->sstate) {
+    ADC_CUDA(cudaMalloc((void **)&c->sstate, 2 * sizeof(SeriesState)));
+    ADC_CUDA(cudaMemset(c->sstate, 0, 2 * sizeof(SeriesState)));
+  }
+  const size_t n = (size_t)s->nrec * width;
+  for (double **p : {v1, v2})
+    if (p && *p) {
+      cudaFree(*p);
+      *p = nullptr;
+    }
+  ADC_CUDA(cudaMalloc((void **)v1, n * sizeof(double)));
+  ADC_CUDA(cudaMemcpy(*v1, s->values, n * sizeof(double), cudaMemcpyHostToDevice));
+  if (v2) {
+    ADC_CUDA(cudaMalloc((void **)v2, n * sizeof(double)));
+    if (s->values2)
+      ADC_CUDA(cudaMemcpy(*v2, s->values2, n * sizeof(double), cudaMemcpyHostToDevice));
+    else
+      ADC_CUDA(cudaMemset(*v2, 0, n * sizeof(double)));
+  }
+  return ADC_OK;
+}
+
+// cstart.F:207-216 / 227-256: the first two records, ETIME1 = STATIM*86400.
+static int series_start(adc_ctx *c, int which, const adc_series_t *s) {
+  SeriesState st;
+  std::memset(&st, 0, sizeof(st));
+  st.t1 = s->start_time;
+  st.t2 = st.t1 + s->interval;
+  ADC_CUDA(cudaMemcpy(c->sstate + which, &st, sizeof(st), cudaMemcpyHostToDevice));
+  drop_graphs(c);
+  return ADC_OK;
+}
+
+extern "C" int adc_set_elev_series(adc_ctx *c, const adc_series_t *s) {
+  if (!c) return ADC_ERR_ARG;
+  if (c->neta < 1) {
+    set_error("adc_set_elev_series: the mesh has no elevation boundary nodes");
+    return ADC_ERR_ARG;
+  }
+  int rc = series_upload(c, s, c->neta, "adc_set_elev_series", &c->eser, nullptr);
+  if (rc) return rc;
+  c->eser_nrec = s->nrec;
+  c->eser_interval = s->interval;
+  c->eser_on = 1;
+  return series_start(c, 0, s);
+}
+
+extern "C" int adc_set_flux_series(adc_ctx *c, const adc_series_t *s) {
+  if (!c) return ADC_ERR_ARG;
+  if (!c->nfluxf) {
+    set_error("adc_set_flux_series: the mesh has no specified-flux boundary (IBTYPE 2, 12, 22, 32 or 52)");
+    return ADC_ERR_ARG;
+  }
+  int rc = series_upload(c, s, c->nvel, "adc_set_flux_series", &c->fser_q, &c->fser_e);
+  if (rc) return rc;
+  c->fser_nrec = s->nrec;
+  c->fser_interval = s->interval;
+  c->flux_settling_it = s->flux_settling_it;
+  c->fser_on = 1;
+  c->flux_on = 0;
+  return series_start(c, 1, s);
 }

@@ -645,3 +645,122 @@ extern "C" int adc_fort15_write(const char *path, const adc_fort15_t *o, int net
   }
   return ADC_OK;
 }
+
+// ---------------------------------------------------------------------------
+// fort.19 / fort.20: non-periodic elevation and normal-flux boundary series.
+// The interval, then records as the reference's READ(19,*)/READ(20,*) take
+// them (cstart.F:207-216, 227-256; gwce.F:1664-1666; timestep.F:886-897).
+
+namespace {
+
+// Reads the interval line and every full record of `per` values; a record
+// takes `items(j)` values for its j-th READ.  Returns the record count or a
+// negative status.
+template <class ItemsOf, class Store>
+int read_series(const char *path, const char *which, int nreads, ItemsOf items, Store store,
+                double *interval) {
+  Records r;
+  if (!r.open(path)) {
+    set_error("%s %s: cannot open", which, path);
+    return ADC_ERR_ARG;
+  }
+  std::vector<std::string> tok;
+  double inc = 0.0;
+  if (!r.items(1, tok) || !to_real(tok[0], inc) || !(inc > 0.0)) {
+    set_error("%s %s: the first record must hold a positive time increment", which, path);
+    return ADC_ERR_ARG;
+  }
+  *interval = inc;
+  int nrec = 0;
+  for (;;) {
+    // the end of the file (blank records aside) ends the series
+    size_t q0 = r.next;
+    while (q0 < r.rec.size() && r.rec[q0].find_first_not_of(" \t") == std::string::npos) ++q0;
+    if (q0 >= r.rec.size()) break;
+    std::vector<double> vals;
+    for (int j = 0; j < nreads; ++j) {
+      const int k = items(j);
+      if (k == 0) continue;
+      if (!r.items((size_t)k, tok)) {
+        set_error("%s %s: record %d is incomplete", which, path, nrec + 1);
+        return ADC_ERR_ARG;
+      }
+      for (int q = 0; q < k; ++q) {
+        double v;
+        if (!to_real(tok[q], v)) {
+          set_error("%s %s: '%s' is not a number (line %d)", which, path, tok[q].c_str(), r.line());
+          return ADC_ERR_ARG;
+        }
+        vals.push_back(v);
+      }
+    }
+    store(nrec, vals);
+    ++nrec;
+  }
+  return nrec;
+}
+
+}  // namespace
+
+extern "C" int adc_fort19_read(const char *path, int neta, int *nrec, double *interval,
+                               double *esbin) {
+  if (!path || neta < 1 || !nrec || !interval) {
+    set_error("adc_fort19_read: a path, NETA >= 1 and the count outputs are required");
+    return ADC_ERR_ARG;
+  }
+  const int cap = esbin ? *nrec : 0;
+  int n = read_series(
+      path, "fort.19", neta, [](int) { return 1; },
+      [&](int k, const std::vector<double> &v) {
+        if (esbin && k < cap)
+          for (int j = 0; j < neta; ++j) esbin[(size_t)k * neta + j] = v[j];
+      },
+      interval);
+  if (n < 0) return n;
+  if (n < 2) {
+    set_error("adc_fort19_read %s: fewer than two records of %d values", path, neta);
+    return ADC_ERR_ARG;
+  }
+  *nrec = esbin ? (n < cap ? n : cap) : n;
+  return ADC_OK;
+}
+
+extern "C" int adc_fort20_read(const char *path, int nvel, const int *lbcodei, int *nrec,
+                               double *interval, double *qnin, double *enin) {
+  if (!path || nvel < 1 || !lbcodei || !nrec || !interval) {
+    set_error("adc_fort20_read: a path, NVEL >= 1, LBCODEI and the count outputs are required");
+    return ADC_ERR_ARG;
+  }
+  auto items = [&](int j) {
+    const int lb = lbcodei[j];
+    return (lb == 2 || lb == 12 || lb == 22) ? 1 : lb == 32 ? 2 : 0;
+  };
+  int any = 0;
+  for (int j = 0; j < nvel; ++j) any |= items(j);
+  if (!any) {
+    set_error("adc_fort20_read: no boundary entry of code 2, 12, 22 or 32 takes a fort.20 record");
+    return ADC_ERR_ARG;
+  }
+  const int cap = qnin ? *nrec : 0;
+  int n = read_series(
+      path, "fort.20", nvel, items,
+      [&](int k, const std::vector<double> &v) {
+        if (!qnin || k >= cap) return;
+        size_t q = 0;
+        for (int j = 0; j < nvel; ++j) {
+          const size_t o = (size_t)k * nvel + j;
+          const int m = items(j);
+          qnin[o] = m ? v[q] : 0.0;   // ICS = 1: the flux is not rotated
+          if (enin) enin[o] = m == 2 ? v[q + 1] : 0.0;
+          q += m;
+        }
+      },
+      interval);
+  if (n < 0) return n;
+  if (n < 2) {
+    set_error("adc_fort20_read %s: fewer than two records", path);
+    return ADC_ERR_ARG;
+  }
+  *nrec = qnin ? (n < cap ? n : cap) : n;
+  return ADC_OK;
+}

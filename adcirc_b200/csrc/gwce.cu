@@ -477,6 +477,11 @@ __global__ void k_eta_bc(adc_ctx c, const adc_step_t *steps, const Flags *flags)
     double ARG = ARGJ - c.efa[J + (size_t)c.nbfr * I];
     e2 = e2 + c.emo[J + (size_t)c.nbfr * I] * RFF * cos(ARG);
   }
+  if (c.eser_on) {   // non-periodic elevations, gwce.F:1668-1673
+    const SeriesState &ss = c.sstate[0];
+    const size_t r1 = (size_t)ss.k * c.neta, r2 = r1 + c.neta;
+    e2 = e2 + st.rampelev * (c.eser[r1 + I] + ss.ratio * (c.eser[r2 + I] - c.eser[r1 + I]));
+  }
   c.eta2[b] = e2;
   double es = e2 - c.eta1[b];
   c.etas[b] = es;

@@ -6,8 +6,8 @@
 // this library's own: it holds every array and scalar the device step
 // carries from one step to the next (state fields, the GWCE matrix and EP,
 // ITPACK's persistent scalars, the pending unscal drift, the vortex track
-// state, the specified boundary fluxes of the last two steps and the
-// warm-start history), so N steps equal N/2 steps, a dump, a
+// state, the specified boundary fluxes of the last two steps, the position
+// in non-periodic boundary series and the warm-start history), so N steps equal N/2 steps, a dump, a
 // load into a freshly bound context of the same mesh and mode, and N/2
 // more steps, bit for bit.
 //
@@ -60,12 +60,14 @@ static std::vector<HsRec> hs_records(adc_ctx *c) {
       {"itpack", c->itp, sizeof(Itp)},
   };
   if (c->vortex_on) r.push_back({"vortex", c->vstate, sizeof(VortexState)});
-  if (c->nfluxf || c->nfluxrbc) {
+  if (c->nfluxf || c->nfluxrbc || c->nfluxgbc) {
     r.push_back({"flux_qn", c->qn, 3 * (size_t)c->nvel * d});
     r.push_back({"flux_en", c->en, 3 * (size_t)c->nvel * d});
     r.push_back({"flux_elevdisc", c->elevdisc, (size_t)c->nvel * d});   // river radiation
     r.push_back({"flux_etadisc", c->etadisc_b, (size_t)c->nvel * d});
   }
+  // fort.19 / fort.20 record pair, read-ahead times and ratio
+  if (c->eser_on || c->fser_on) r.push_back({"series", c->sstate, 2 * sizeof(SeriesState)});
   if (c->prec & ADC_WARM_START) {
     r.push_back({"etas_prev", c->etas_prev, np * d});
     r.push_back({"warm", c->warm, sizeof(WarmState)});

@@ -478,7 +478,8 @@ static void free_ctx(adc_ctx *c) {
       (void **)&c->jhalo_ptr, (void **)&c->jhalo_ids, (void **)&c->soff32, (void **)&c->etas_prev, (void **)&c->warm, (void **)&c->soff, (void **)&c->jpart, (void **)&c->jtri,
       (void **)&c->itp, (void **)&c->bar, (void **)&c->jlines, (void **)&c->flags, (void **)&c->steps,
       (void **)&c->numitr_log, (void **)&c->met_wsx, (void **)&c->met_wsy,
-      (void **)&c->met_pr, (void **)&c->vfix, (void **)&c->vstate};
+      (void **)&c->met_pr, (void **)&c->vfix, (void **)&c->vstate, (void **)&c->eser,
+      (void **)&c->fser_q, (void **)&c->fser_e, (void **)&c->sstate};
   for (void **p : ptrs)
     if (*p) { cudaFree(*p); *p = nullptr; }
   drop_graphs(c);

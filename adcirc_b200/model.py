@@ -99,6 +99,8 @@ class Case:
     meta: dict = dataclasses.field(default_factory=dict)
     vortex: "Vortex | None" = None   # NWS = 8 parametric-vortex track
     flux: "Flux | None" = None       # specified normal flux (IBTYPE 2/12/22)
+    elev_series: "Series | None" = None   # non-periodic boundary elevations (fort.19)
+    flux_series: "Series | None" = None   # non-periodic normal fluxes (fort.20, NFFR <= 0)
 
     def clone(self) -> "Case":
         c = copy.copy(self)
@@ -159,6 +161,38 @@ class Flux:
         for name, a in zip(names, keep):
             setattr(f, name, a.ctypes.data_as(dp_))
         return f, keep
+
+
+@dataclasses.dataclass
+class Series:
+    """A non-periodic boundary time series: the records of a fort.19
+    (`values` (nrec, NETA) boundary elevations [m]) or of a fort.20
+    (`values` (nrec, NVEL) normal fluxes [m^2/s], zero off the entries of
+    code 2/12/22/32, and `values2` the elevations of code-32 entries), one
+    record every `interval` seconds from `start_time` (STATIM*86400).
+    `flux_settling_it` is FluxSettlingIT for a fort.20 with river-radiation
+    entries."""
+    interval: float
+    values: np.ndarray
+    values2: "np.ndarray | None" = None
+    start_time: float = 0.0
+    flux_settling_it: int = 0
+
+    def struct(self, cls=None):
+        """(struct, backing arrays); keep both alive while in use."""
+        cls = cls or _lib.AdcSeries
+        keep = [np.ascontiguousarray(self.values, np.float64)]
+        if self.values2 is not None:
+            keep.append(np.ascontiguousarray(self.values2, np.float64))
+            assert keep[1].shape == keep[0].shape
+        s = cls()
+        s.nrec = int(keep[0].shape[0])
+        s.flux_settling_it = int(self.flux_settling_it)
+        s.interval, s.start_time = float(self.interval), float(self.start_time)
+        s.values = keep[0].ctypes.data_as(dp_)
+        if len(keep) > 1:
+            s.values2 = keep[1].ctypes.data_as(dp_)
+        return s, keep
 
 
 @dataclasses.dataclass
@@ -539,6 +573,7 @@ K1_PERIOD = 86164.0
 def channel_case(dt: float = 5.0, amp: float = 0.5, vortex: bool = False,
                  river: float | None = None, river_type: int = 2, radiation: bool = False,
                  zero_gradient: int = 0, flux_settling: float = 0.0, river_eta: float = 0.05,
+                 elev_series: float = 0.0, flux_series: float = 0.0, series_hours: float = 6.0,
                  prep: MeshPrep | None = None, **kw) -> Case:
     """Tidal channel: 121x41 nodes, 20 m -> 5 m, M2 0.5 m, dt 5 s.  With
     `vortex`, a small Holland vortex (Rmax 8 km) crosses the channel.  With
@@ -549,7 +584,14 @@ def channel_case(dt: float = 5.0, amp: float = 0.5, vortex: bool = False,
     settled (NRAMP 2); IBTYPE 32 (coupled flux and radiation) also takes
     the steady elevation `river_eta` [m].  With `radiation`, the east end is a radiation
     boundary (IBTYPE 30) the tide leaves through; with `zero_gradient` 40
-    (or True) or 41, a zero-normal-velocity-gradient boundary of that type."""
+    (or True) or 41, a zero-normal-velocity-gradient boundary of that type.
+    With `elev_series` [s], the open boundary takes no periodic tide (NBFR
+    0) but a fort.19 series of that record interval: the M2 sampled at the
+    record times with a phase that varies along the boundary, plus a
+    set-up of 0.1 m per hour.  With `flux_series` [s] (and `river`), the
+    river flux comes from a fort.20 series of that interval (NFFR 0):
+    the steady inflow modulated by 50 % with a one-hour period.  Series
+    cover `series_hours` of simulated time."""
     from .meshgen import channel_mesh
     raw = channel_mesh()
     if river is not None or radiation or zero_gradient:
@@ -563,6 +605,8 @@ def channel_case(dt: float = 5.0, amp: float = 0.5, vortex: bool = False,
         raw.land_segments = [(0, south), (east_type, east), (0, north)]
     neta = raw.open_nodes.size
     tides = [(2.0 * math.pi / M2_PERIOD, 0.0, 1.0, np.full(neta, amp), np.zeros(neta))]
+    if elev_series > 0:
+        tides = []
     if vortex:
         kw.setdefault("nws", 8)
     params = default_params(dt, **kw)
@@ -578,6 +622,26 @@ def channel_case(dt: float = 5.0, amp: float = 0.5, vortex: bool = False,
         case.flux = Flux(np.zeros(1), np.zeros(1), np.ones(1), np.zeros(1), qnam, np.zeros((1, nv)),
                          flux_settling_it=sched.flux_settling_it, enam=enam,
                          enph=None if enam is None else np.zeros((1, nv)))
+    if elev_series > 0:
+        nrec = int(math.ceil(series_hours * 3600.0 / elev_series)) + 2
+        t = np.arange(nrec)[:, None] * elev_series
+        phase = np.linspace(0.0, 0.3, neta)[None, :]
+        vals = amp * np.cos(2.0 * math.pi / M2_PERIOD * t - phase) + 0.1 * t / 3600.0
+        case.elev_series = Series(float(elev_series), vals)
+    if flux_series > 0 and case.flux is not None:
+        f = case.flux
+        nrec = int(math.ceil(series_hours * 3600.0 / flux_series)) + 2
+        t = np.arange(nrec)[:, None] * flux_series
+        mod = 1.0 + 0.5 * np.sin(2.0 * math.pi * t / 3600.0)
+        lbc = case.arrays["lbcodei"]
+        on = ((lbc == 2) | (lbc == 12) | (lbc == 22) | (lbc == 32))[None, :]
+        q = np.where(on, f.qnam[0][None, :] * mod, 0.0)
+        e = None
+        if f.enam is not None:
+            e = np.where((lbc == 32)[None, :], f.enam[0][None, :] * mod, 0.0)
+        case.flux = None
+        case.flux_series = Series(float(flux_series), q, e,
+                                  flux_settling_it=sched.flux_settling_it)
     if vortex:
         case.vortex = straight_track(30.3e3, 3.7e3, 80.0, 6.0, 960.0, 8.0, 1.3, hours=12.0,
                                      interval_h=3.0)
@@ -712,6 +776,12 @@ class GpuModel:
         if case.flux is not None:
             f, keep = case.flux.struct()
             _check(self.lib.adc_set_flux(self.h, C.byref(f)), "adc_set_flux")
+        for attr in ("elev_series", "flux_series"):
+            ser = getattr(case, attr)
+            if ser is not None:
+                sv, keep = ser.struct()
+                fn = "adc_set_" + attr
+                _check(getattr(self.lib, fn)(self.h, C.byref(sv)), fn)
 
     def close(self):
         if self.h:

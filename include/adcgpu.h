@@ -398,6 +398,46 @@ int adc_selftest_div_const(long long n, unsigned long long seed, long long *mism
  * at bind with ADC_ERR_UNSUPPORTED. */
 int adc_set_flux(adc_ctx *ctx, const adc_flux_t *flux);
 
+/* A non-periodic boundary time series: the records of a fort.19 (elevations)
+ * or fort.20 (normal fluxes) after its interval line, one record every
+ * `interval` seconds from `start_time`.  The reference reads one record
+ * ahead as the run passes each record time and interpolates linearly
+ * between the two it holds; here the whole file is in HBM and one device
+ * thread per step advances the same pair of record times. */
+typedef struct {
+  int nrec;               /* records (>= 2) */
+  int flux_settling_it;   /* fort.20 series only: FluxSettlingIT (IBTYPE 52) */
+  double interval;        /* ETIMINC / FTIMINC, s */
+  double start_time;      /* STATIM*86400: ETIME1 / QTIME1 at cold start */
+  const double *values;   /* fort.19: ESBIN, NETA per record; fort.20: QNIN,
+                             NVEL per record, 0 at entries without a flux record */
+  const double *values2;  /* fort.20: ENIN at IBTYPE 32 entries, NVEL per record,
+                             NULL when there are none; unused for fort.19 */
+} adc_series_t;
+
+/* Non-periodic elevation boundary (NPEBC, a fort.19 beside the fort.15;
+ * read_input.F:1893-1898, cstart.F:198-217): every step adds
+ * RampElev*(ESBIN1 + ETRATIO*(ESBIN2 - ESBIN1)) to the periodic boundary
+ * elevation (gwce.F:1659-1674).  ADC_ERR_ARG without elevation boundary
+ * nodes; a run past the last record sets ADC_ERR_ARG in the step status
+ * (the reference stops at the end of fort.19). */
+int adc_set_elev_series(adc_ctx *ctx, const adc_series_t *series);
+/* Non-periodic normal flux (NFFR = 0 or -1, fort.20; cstart.F:227-258): QN2
+ * = RampExtFlux*(QNIN1 + QTRATIO*(QNIN2 - QNIN1)) and EN2 likewise at every
+ * entry (timestep.F:882-903) in place of the periodic constituents of
+ * adc_set_flux.  ADC_ERR_ARG without flux boundaries. */
+int adc_set_flux_series(adc_ctx *ctx, const adc_series_t *series);
+
+/* fort.19 / fort.20 readers: the interval line, then records as the
+ * reference's list-directed READs take them (one READ per value of ESBIN;
+ * per entry of code 2/12/22 one value of QNIN, per entry of code 32 QNIN and
+ * ENIN).  With values == NULL only *nrec and *interval are set (the full
+ * records in the file); otherwise the first *nrec records are stored,
+ * entries of other codes at 0.  Negative on a missing or malformed file. */
+int adc_fort19_read(const char *path, int neta, int *nrec, double *interval, double *esbin);
+int adc_fort20_read(const char *path, int nvel, const int *lbcodei, int *nrec, double *interval,
+                    double *qnin, double *enin);
+
 /* No reference counterpart (the reference always starts JCG from ETAS as
  * GWCE_New leaves it, gwce.F:2002-2004).  With ADC_WARM_START in the bind
  * mode, counts of the steps that started from the extrapolated guess and of

@@ -46,6 +46,13 @@ module adcgpu_iface
       type(c_ptr) :: famig, fper, fff, fface, qnam, qnph, enam, enph
    end type
 
+   ! non-periodic boundary series (fort.19 elevations, fort.20 fluxes)
+   type, bind(C), public :: adc_series_t
+      integer(c_int) :: nrec, flux_settling_it
+      real(c_double) :: interval, start_time
+      type(c_ptr) :: values, values2
+   end type
+
    type, bind(C), public :: adc_stepout_t
       integer(c_int) :: numitr, ier, ncchange, status
       real(c_double) :: ep, zeta, cme
@@ -74,7 +81,7 @@ module adcgpu_iface
    public :: adc_jcg, adc_dfault, adc_gpu_bind, adc_gpu_free, adc_shift_friction, &
              adc_gwce_new, adc_wetdry, adc_momentum, adc_timestep, adc_sync_to_host, &
              adc_sync_from_host, adc_set_met, adc_set_vortex, adc_hotstart_write, &
-             adc_hotstart_read, adc_set_flux
+             adc_hotstart_read, adc_set_flux, adc_set_elev_series, adc_set_flux_series
 
    interface
       ! drop-in for ITPACK jcg (itpackv.F:63): identical argument list
@@ -166,6 +173,20 @@ module adcgpu_iface
          import :: c_int, c_ptr, adc_flux_t
          type(c_ptr), value :: ctx
          type(adc_flux_t), intent(in) :: f
+      end function
+
+      ! fort.19 (NPEBC, gwce.F:1659-1674) and fort.20 (NFFR <= 0,
+      ! timestep.F:882-903) records, uploaded once after bind
+      integer(c_int) function adc_set_elev_series(ctx, s) bind(C, name="adc_set_elev_series")
+         import :: c_int, c_ptr, adc_series_t
+         type(c_ptr), value :: ctx
+         type(adc_series_t), intent(in) :: s
+      end function
+
+      integer(c_int) function adc_set_flux_series(ctx, s) bind(C, name="adc_set_flux_series")
+         import :: c_int, c_ptr, adc_series_t
+         type(c_ptr), value :: ctx
+         type(adc_series_t), intent(in) :: s
       end function
 
       ! hotstart dump/load (write_output.F:4429-5582, hstart.F:47-2048);

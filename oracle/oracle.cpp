@@ -593,6 +593,14 @@ struct orc_model {
   std::vector<double> famig, fper, fff, fface, qnam, qnph, qn0, qn1, qn2;
   /* coupled flux/radiation (IBTYPE 32): ENAM/ENPH and EN0/EN1/EN2 (NVEL) */
   std::vector<double> enam, enph, en0, en1, en2;
+  /* fort.19 (NPEBC) and fort.20 (NFFR <= 0) series as the reference holds
+   * them: the two records in use (ESBIN1/ESBIN2, QNIN1/QNIN2, ENIN1/ENIN2),
+   * their times, and the next record of the file to read */
+  int npebc = 0, fser_on = 0, series_err = 0;
+  double etiminc = 0, etime1 = 0, etime2 = 0, ftiminc = 0, qtime1 = 0, qtime2 = 0;
+  std::vector<double> e19, q20, e20;   /* the files' records */
+  int e19_nrec = 0, q20_nrec = 0, e19_next = 0, q20_next = 0;
+  std::vector<double> esbin1, esbin2, qnin1, qnin2, enin1, enin2;
   int vortex_on = 0;
   orc_vortex_t vpar;
   std::vector<orc_vortex_fix_t> vfix;
@@ -753,6 +761,58 @@ int orc_model_set_flux(orc_model *m, const orc_flux_t *f) {
   return 0;
 }
 
+int orc_model_set_elev_series(orc_model *m, const orc_series_t *s) {
+  const int neta = m->a->neta;
+  if (!s || s->nrec < 2 || !s->values || !(s->interval > 0.0) || neta < 1) return 1;
+  m->e19.assign(s->values, s->values + (size_t)s->nrec * neta);
+  m->e19_nrec = s->nrec;
+  /* cstart.F:207-216: ETIMINC, two records, ETIME1 = STATIM*86400 */
+  m->etiminc = s->interval;
+  m->esbin1.assign(m->e19.begin(), m->e19.begin() + neta);
+  m->esbin2.assign(m->e19.begin() + neta, m->e19.begin() + 2 * (size_t)neta);
+  m->e19_next = 2;
+  m->etime1 = s->start_time;
+  m->etime2 = m->etime1 + m->etiminc;
+  m->npebc = 1;
+  return 0;
+}
+
+int orc_model_set_flux_series(orc_model *m, const orc_series_t *s) {
+  const int nv = m->a->nvel;
+  if (!s || s->nrec < 2 || !s->values || !(s->interval > 0.0) || !m->nfluxf) return 1;
+  m->q20.assign(s->values, s->values + (size_t)s->nrec * nv);
+  if (s->values2)
+    m->e20.assign(s->values2, s->values2 + (size_t)s->nrec * nv);
+  else
+    m->e20.assign((size_t)s->nrec * nv, 0.0);
+  m->q20_nrec = s->nrec;
+  /* cstart.F:227-256: QNIN1 = QNIN2 = 0, then two records at the flux entries */
+  m->ftiminc = s->interval;
+  m->qnin1.assign(nv, 0.0);
+  m->qnin2.assign(nv, 0.0);
+  m->enin1.assign(nv, 0.0);
+  m->enin2.assign(nv, 0.0);
+  const orc_arrays_t *a = m->a;
+  for (int J = 0; J < nv; ++J) {
+    const int lb = a->lbcodei[J];
+    if (lb == 2 || lb == 12 || lb == 22 || lb == 32) {
+      m->qnin1[J] = m->q20[J];
+      m->qnin2[J] = m->q20[(size_t)nv + J];
+    }
+    if (lb == 32) {
+      m->enin1[J] = m->e20[J];
+      m->enin2[J] = m->e20[(size_t)nv + J];
+    }
+  }
+  m->q20_next = 2;
+  m->qtime1 = s->start_time;
+  m->qtime2 = m->qtime1 + m->ftiminc;
+  m->flux_settling_it = s->flux_settling_it;
+  m->fser_on = 1;
+  m->flux_on = 0;
+  return 0;
+}
+
 /* periodic specified normal flux, timestep.F:861-880 (ICS = 1: no rotation),
  * the discharge elevation of river-radiation entries, :906-926, then the
  * discharge at radiation entries, timestep.F:932-940 */
@@ -773,6 +833,34 @@ static void orc_model_flux(orc_model *m, const orc_step_t *s) {
           m->en2[I] = m->en2[I] + m->enam[J + (size_t)m->nffr * I] * RFF *
                                       std::cos(ARGJ - m->enph[J + (size_t)m->nffr * I]);
       }
+    }
+  } else if (m->nfluxf && m->fser_on) {
+    /* non-periodic flux, timestep.F:882-903 */
+    if (s->timeloc > m->qtime2) {
+      m->qtime1 = m->qtime2;
+      m->qtime2 = m->qtime2 + m->ftiminc;
+      if (m->q20_next >= m->q20_nrec) {   /* the reference's READ hits the end of fort.20 */
+        m->series_err = 1;
+      } else {
+        const size_t r = (size_t)m->q20_next++ * a->nvel;
+        for (int J = 0; J < a->nvel; ++J) {
+          const int lb = a->lbcodei[J];
+          if (lb == 2 || lb == 12 || lb == 22) {
+            m->qnin1[J] = m->qnin2[J];
+            m->qnin2[J] = m->q20[r + J];
+          } else if (lb == 32) {
+            m->qnin1[J] = m->qnin2[J];
+            m->enin1[J] = m->enin2[J];
+            m->qnin2[J] = m->q20[r + J];
+            m->enin2[J] = m->e20[r + J];
+          }
+        }
+      }
+    }
+    const double QTRATIO = (s->timeloc - m->qtime1) / m->ftiminc;
+    for (int I = 0; I < a->nvel; ++I) {
+      m->qn2[I] = s->rampextflux * (m->qnin1[I] + QTRATIO * (m->qnin2[I] - m->qnin1[I]));
+      m->en2[I] = s->rampextflux * (m->enin1[I] + QTRATIO * (m->enin2[I] - m->enin1[I]));
     }
   }
   if (m->nfluxf) {
@@ -1016,6 +1104,27 @@ int orc_model_gwce(orc_model *m, const orc_step_t *s, orc_stepout_t *out) {
       double ARG = ARGJ - a->efa[J + (size_t)a->nbfr * I];
       int b = a->nbd[I] - 1;
       a->eta2[b] = a->eta2[b] + a->emo[J + (size_t)a->nbfr * I] * RFF * std::cos(ARG);
+    }
+  }
+  /* non-periodic elevation BC, gwce.F:1659-1674 */
+  if (m->npebc) {
+    if (s->timeloc > m->etime2) {
+      m->etime1 = m->etime2;
+      m->etime2 = m->etime1 + m->etiminc;
+      if (m->e19_next >= m->e19_nrec) {   /* the reference's READ hits the end of fort.19 */
+        m->series_err = 1;
+      } else {
+        const size_t r = (size_t)m->e19_next++ * a->neta;
+        for (int J = 0; J < a->neta; ++J) {
+          m->esbin1[J] = m->esbin2[J];
+          m->esbin2[J] = m->e19[r + J];
+        }
+      }
+    }
+    const double ETRATIO = (s->timeloc - m->etime1) / m->etiminc;
+    for (int I = 0; I < a->neta; ++I) {
+      const int NBDI = a->nbd[I] - 1;
+      a->eta2[NBDI] = a->eta2[NBDI] + s->rampelev * (m->esbin1[I] + ETRATIO * (m->esbin2[I] - m->esbin1[I]));
     }
   }
   /* boundary flux integral, gwce.F:1737-1834 (LBCODEI <= 29 types,
@@ -1595,6 +1704,7 @@ int orc_model_step(orc_model *m, const orc_step_t *s, orc_stepout_t *out) {
   for (int i = 0; i < a->np; ++i) a->h2[i] = a->dp[i] + m->p.ifnlfa * a->eta2[i];
   orc_model_momentum(m, s);
   out->ncchange = m->ncchange;
+  if (m->series_err) { out->status = -1; return -1; }   /* past the end of fort.19/fort.20 */
   return 0;
 }
 

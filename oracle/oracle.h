@@ -94,6 +94,14 @@ typedef struct {
   const double *famig, *fper, *fff, *fface, *qnam, *qnph, *enam, *enph;
 } orc_flux_t;
 
+/* Non-periodic boundary series, a fort.19 or fort.20 (same layout as
+ * adc_series_t): nrec records of NETA (fort.19) or NVEL (fort.20) values. */
+typedef struct {
+  int nrec, flux_settling_it;
+  double interval, start_time;
+  const double *values, *values2;
+} orc_series_t;
+
 /* Parametric-vortex track (fort.22 fields HollandGet consumes,
  * nws08.F90:827-878) in mesh units; same layout as adc_vortex_fix_t /
  * adc_vortex_t in include/adcgpu.h. */
@@ -148,6 +156,11 @@ int orc_model_set_vortex(orc_model *m, const orc_vortex_t *v);
 int orc_model_met(orc_model *m, const orc_step_t *s);
 /* Specified normal flux (timestep.F:861-880); nonzero without flux boundaries. */
 int orc_model_set_flux(orc_model *m, const orc_flux_t *f);
+/* fort.19 elevations (NPEBC, gwce.F:1659-1674) and fort.20 fluxes (NFFR <= 0,
+ * timestep.F:882-903); nonzero without elevation / flux boundaries.  A run
+ * past the last record makes the step return nonzero. */
+int orc_model_set_elev_series(orc_model *m, const orc_series_t *s);
+int orc_model_set_flux_series(orc_model *m, const orc_series_t *s);
 void orc_model_set_ncchange(orc_model *m, int ncchange);
 int orc_model_get_ncchange(const orc_model *m);
 double orc_model_get_zeta(const orc_model *m);

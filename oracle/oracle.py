@@ -66,6 +66,11 @@ class OrcFlux(C.Structure):
         (n, dp_) for n in ("famig", "fper", "fff", "fface", "qnam", "qnph", "enam", "enph")]
 
 
+class OrcSeries(C.Structure):
+    _fields_ = [("nrec", C.c_int), ("flux_settling_it", C.c_int), ("interval", C.c_double),
+                ("start_time", C.c_double), ("values", dp_), ("values2", dp_)]
+
+
 class OrcStepOut(C.Structure):
     _fields_ = [("numitr", C.c_int), ("ier", C.c_int), ("ncchange", C.c_int),
                 ("status", C.c_int), ("ep", C.c_double), ("zeta", C.c_double),
@@ -119,6 +124,9 @@ def load(omp: bool = False):
         getattr(lib, f).restype = C.c_int
     lib.orc_model_set_flux.argtypes = [C.c_void_p, C.POINTER(OrcFlux)]
     lib.orc_model_set_flux.restype = C.c_int
+    for f in ("orc_model_set_elev_series", "orc_model_set_flux_series"):
+        getattr(lib, f).argtypes = [C.c_void_p, C.POINTER(OrcSeries)]
+        getattr(lib, f).restype = C.c_int
     lib.orc_model_set_vortex.argtypes = [C.c_void_p, C.POINTER(OrcVortex)]
     lib.orc_model_set_vortex.restype = C.c_int
     lib.orc_model_met.argtypes = [C.c_void_p, C.POINTER(OrcStep)]
@@ -183,6 +191,13 @@ class OracleModel:
             f, keep = flux.struct(OrcFlux)
             if self.lib.orc_model_set_flux(self.h, C.byref(f)) != 0:
                 raise ValueError("invalid flux forcing")
+        for attr, fn in (("elev_series", "orc_model_set_elev_series"),
+                         ("flux_series", "orc_model_set_flux_series")):
+            ser = getattr(case, attr, None)
+            if ser is not None:
+                sv, self._series_keep = ser.struct(OrcSeries)
+                if getattr(self.lib, fn)(self.h, C.byref(sv)) != 0:
+                    raise ValueError(f"invalid {attr}")
 
     def set_vortex(self, vortex):
         """vortex: an object with the adcirc_b200.model.Vortex fields."""

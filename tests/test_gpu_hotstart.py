@@ -84,3 +84,17 @@ def test_hotstart_rejects_other_mesh_or_mode(lib, tmp_path):
 def test_resume_channel_river(lib, tmp_path):
     from adcirc_b200 import model
     _resume_equal(lambda: model.channel_case(river=0.5), 80, 0, tmp_path, use_run=True)
+
+
+def test_resume_series(lib, tmp_path):
+    """fort.19 and fort.20 series: the record pair, its times and the ratio
+    travel in the hotstart file."""
+    from adcirc_b200 import model
+    _resume_equal(lambda: model.channel_case(river=0.5, elev_series=150.0, flux_series=300.0,
+                                             series_hours=1.0), 240, 0, tmp_path, use_run=True)
+
+
+def test_resume_zero_gradient(lib, tmp_path):
+    """Zero-normal-gradient entries keep QN0 from the step before the dump."""
+    from adcirc_b200 import model
+    _resume_equal(lambda: model.channel_case(zero_gradient=True), 80, 0, tmp_path, use_run=True)

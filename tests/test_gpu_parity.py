@@ -294,3 +294,29 @@ def test_channel_galerkin_zero_gradient_boundary(lib, orc):
     a = c0.arrays
     east = a["x"] > 59.9e3
     assert a["uu2"][east].mean() > 0.02
+
+
+def test_channel_elevation_series(lib, orc):
+    """A non-periodic elevation boundary (fort.19, NBFR 0): the record pair
+    the run holds moves on as TimeLoc passes each record time and the
+    boundary elevation is their interpolation (gwce.F:1659-1674), against
+    the oracle over a graph-replayed run through twenty record changes."""
+    from adcirc_b200 import model
+    c0, cg, io, ig = _pair(lambda **k: model.channel_case(elev_series=150.0, series_hours=1.0, **k),
+                           600, use_run=True)
+    _check(c0, cg, io, ig)
+
+
+@pytest.mark.parametrize("river_type", [2, 32])
+def test_channel_flux_series(lib, orc, river_type):
+    """A river boundary driven by a fort.20 series (NFFR 0): QN2 (and EN2 at
+    IBTYPE 32) interpolated between the records the run holds (timestep.F:
+    882-903), against the oracle over a graph-replayed run."""
+    from adcirc_b200 import model
+    c0, cg, io, ig = _pair(lambda **k: model.channel_case(river=0.5, river_type=river_type,
+                                                          flux_series=300.0, series_hours=1.0, **k),
+                           600, use_run=True)
+    _check(c0, cg, io, ig)
+    a = c0.arrays
+    east = a["x"] > 59.9e3
+    assert a["uu2"][east].mean() < -0.02
