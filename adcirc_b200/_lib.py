@@ -81,6 +81,12 @@ class AdcVortexFix(C.Structure):
     _fields_ = [(n, C.c_double) for n in ("time", "x", "y", "cpress", "vmax", "rmw", "tvx", "tvy")]
 
 
+class AdcFort22Opts(C.Structure):
+    _fields_ = [("irefyr", C.c_int), ("irefmo", C.c_int), ("irefday", C.c_int),
+                ("irefhr", C.c_int), ("slam0", C.c_double), ("sfea0", C.c_double),
+                ("rnday", C.c_double)]
+
+
 class AdcVortex(C.Structure):
     _fields_ = [("nfix", C.c_int), ("avg_minute", C.c_int), ("hemisphere", C.c_int),
                 ("pad_", C.c_int)] + [(n, C.c_double) for n in (
@@ -170,6 +176,8 @@ def load():
         "adc_sync_from_host": (C.c_int, [vp]),
         "adc_set_met": (C.c_int, [vp, dp_, dp_, dp_]),
         "adc_set_vortex": (C.c_int, [vp, C.POINTER(AdcVortex)]),
+        "adc_fort22_read": (C.c_int, [C.c_char_p, C.POINTER(AdcFort22Opts), ip_,
+                                      C.POINTER(AdcVortexFix)]),
         "adc_set_flux": (C.c_int, [vp, C.POINTER(AdcFlux)]),
         "adc_set_elev_series": (C.c_int, [vp, C.POINTER(AdcSeries)]),
         "adc_set_flux_series": (C.c_int, [vp, C.POINTER(AdcSeries)]),

@@ -260,3 +260,25 @@ def write_fort20(path, series, lbcodei) -> None:
                 elif lb == 32:
                     ev = 0.0 if e is None else float(e[k, j])
                     f.write(f"{float(rec[j])!r} {ev!r}\n")
+
+
+def read_fort22(path, irefyr: int, irefmo: int, irefday: int, irefhr: int, slam0: float = 0.0,
+                sfea0: float = 0.0, rnday: float = 0.0, **vortex_kw):
+    """Reads an NWS = 8 fort.22 (ATCF best-track lines; adc_fort22_read) into
+    a model.Vortex: times since the wind reference time IREFYR/IREFMO/
+    IREFDAY/IREFHR, centres projected about (SLAM0, SFEA0) [degrees] into mesh
+    metres.  `rnday` > 0 requires the track to reach RNDAY days.  vortex_kw
+    (bladj, start_time, ...) go to the Vortex."""
+    from .model import Vortex
+    lib = _lib.load()
+    p = os.fsencode(path)
+    o = _lib.AdcFort22Opts(int(irefyr), int(irefmo), int(irefday), int(irefhr), float(slam0),
+                           float(sfea0), float(rnday))
+    n = C.c_int(0)
+    _check(lib.adc_fort22_read(p, C.byref(o), C.byref(n), None), "adc_fort22_read")
+    arr = (_lib.AdcVortexFix * n.value)()
+    _check(lib.adc_fort22_read(p, C.byref(o), C.byref(n), arr), "adc_fort22_read")
+    rows = np.array([[getattr(arr[k], f) for f, _ in _lib.AdcVortexFix._fields_]
+                     for k in range(n.value)])
+    vortex_kw.setdefault("hemisphere", -1 if rows[0, 2] < 0.0 else 1)   # sign(1, lat)
+    return Vortex(rows, **vortex_kw)

@@ -79,6 +79,8 @@ struct VortexState {
   int err;       // set when the run passes the last fix
   double wtratio;
   double x, y, cpress, dpdef, spd, b, rmw, tvx, tvy;
+  int calm;      // a CALM fix brackets the time: no wind, background pressure
+  int pad_;
 };
 
 // Position in a non-periodic boundary series (fort.19 / fort.20): the two

@@ -44,6 +44,15 @@ __global__ void k_vortex_state(adc_ctx c, const adc_step_t *steps, Flags *flags)
   }
   const double lon = f[i - 1].x + v.wtratio * (f[i].x - f[i - 1].x);
   const double lat = f[i - 1].y + v.wtratio * (f[i].y - f[i - 1].y);
+  v.counter = i;
+  if (f[i].cpress < 0.0 || f[i - 1].cpress < 0.0) {
+    // a CALM line on either side (nws08.F90:858-872): no storm, WTRATIO kept
+    v.calm = 1;
+    v.x = lon;
+    v.y = lat;
+    return;
+  }
+  v.calm = 0;
   const double wt = (timeloc - f[i - 1].time) / (f[i].time - f[i - 1].time);
   v.wtratio = wt;
   const double cpress = f[i - 1].cpress + wt * (f[i].cpress - f[i - 1].cpress);
@@ -51,7 +60,6 @@ __global__ void k_vortex_state(adc_ctx c, const adc_step_t *steps, Flags *flags)
   const double rmw = f[i - 1].rmw + wt * (f[i].rmw - f[i - 1].rmw);
   const double tvx = f[i - 1].tvx + wt * (f[i].tvx - f[i - 1].tvx);
   const double tvy = f[i - 1].tvy + wt * (f[i].tvy - f[i - 1].tvy);
-  v.counter = i;
   // HollandGet: pressure deficit floor, translation removal, BL adjustment,
   // the limited Holland B (backgroundWindFac = 1 for the radial-velocity-
   // weighted background model, nws08.F90:480-485)
@@ -83,34 +91,41 @@ __global__ void k_vortex_nodes(adc_ctx c, const adc_step_t *steps, const Flags *
   if (i >= c.np) return;
   const VortexState &v = *c.vstate;
   const double rampmete = steps[flags->cursor].rampmete;
-  const double hemi = c.vpar.hemisphere >= 0 ? 1.0 : -1.0;   // sign(1, lat)
-  const double dx = c.x[i] - v.x;
-  const double dy = c.y[i] - v.y;
-  const double theta = atan2(dy, dx);
-  const double rad = sqrt(dx * dx + dy * dy);
-  const double f = c.corif[i];
-  const double alpha = pow(v.rmw / rad, v.b);
-  double press = v.cpress + v.dpdef * exp(-alpha);
-  double vr = sqrt(alpha * exp(1.0 - alpha) * v.spd * (v.spd + 0.0) + 0.25 * (rad * rad) * (f * f)) -
-              0.5 * rad * fabs(f);
-  vr = vr * c.vpar.wind_mult;
-  vr = vr * c.vpar.bladj;
-  // inflow angle 0 (useInflow = .false.): theta + sign(1,lat)*0 == theta
-  double wx = (-hemi) * vr * sin(theta + hemi * 0.0);
-  double wy = hemi * vr * cos(theta + hemi * 0.0);
-  // calcTranslationSpeed, radial-velocity-weighted (nws08.F90:746-749)
-  const double tsx = (fabs(vr) / v.spd) * v.tvx;
-  const double tsy = (fabs(vr) / v.spd) * v.tvy;
-  wx = wx + tsx;
-  wy = wy + tsy;
-  if (c.vpar.avg_minute == 1) {
-    wx = wx * kOne2Ten;
-    wy = wy * kOne2Ten;
+  double wx, wy, prn2;
+  if (v.calm) {   // HollandGet's CALM return (nws08.F90:588-601)
+    wx = 0.0;
+    wy = 0.0;
+    prn2 = kPrBckgrndMb * 100.0 / (kRhoWat0 * c.p.g);
+  } else {
+    const double hemi = c.vpar.hemisphere >= 0 ? 1.0 : -1.0;   // sign(1, lat)
+    const double dx = c.x[i] - v.x;
+    const double dy = c.y[i] - v.y;
+    const double theta = atan2(dy, dx);
+    const double rad = sqrt(dx * dx + dy * dy);
+    const double f = c.corif[i];
+    const double alpha = pow(v.rmw / rad, v.b);
+    double press = v.cpress + v.dpdef * exp(-alpha);
+    double vr = sqrt(alpha * exp(1.0 - alpha) * v.spd * (v.spd + 0.0) + 0.25 * (rad * rad) * (f * f)) -
+                0.5 * rad * fabs(f);
+    vr = vr * c.vpar.wind_mult;
+    vr = vr * c.vpar.bladj;
+    // inflow angle 0 (useInflow = .false.): theta + sign(1,lat)*0 == theta
+    wx = (-hemi) * vr * sin(theta + hemi * 0.0);
+    wy = hemi * vr * cos(theta + hemi * 0.0);
+    // calcTranslationSpeed, radial-velocity-weighted (nws08.F90:746-749)
+    const double tsx = (fabs(vr) / v.spd) * v.tvx;
+    const double tsy = (fabs(vr) / v.spd) * v.tvy;
+    wx = wx + tsx;
+    wy = wy + tsy;
+    if (c.vpar.avg_minute == 1) {
+      wx = wx * kOne2Ten;
+      wy = wy * kOne2Ten;
+    }
+    press = fmax(0.85e5, fmin(1.1e5, press));
+    wx = fmax(-200.0, fmin(200.0, wx));
+    wy = fmax(-200.0, fmin(200.0, wy));
+    prn2 = press / (kRhoWat0 * c.p.g);
   }
-  press = fmax(0.85e5, fmin(1.1e5, press));
-  wx = fmax(-200.0, fmin(200.0, wx));
-  wy = fmax(-200.0, fmin(200.0, wy));
-  const double prn2 = press / (kRhoWat0 * c.p.g);
   // wind.F:1174-1193
   const double mag = sqrt(wx * wx + wy * wy);
   double drag = 0.001 * (0.75 + 0.067 * mag);

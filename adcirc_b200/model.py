@@ -450,17 +450,23 @@ def _raw_lbcodes(raw) -> np.ndarray:
 
 
 def case_from_files(fort14, fort15, vortex: "Vortex | None" = None,
-                    prep: MeshPrep | None = None) -> Case:
+                    prep: MeshPrep | None = None, fort19=None, fort20=None, fort22=None) -> Case:
     """A Case from a fort.14 mesh and a fort.15 parameter file, with the
     parameter derivations of the reference: IFNLFA/IFNLCT/IFNLCAT from
     NOLIFA/NOLICA/NOLICAT (adcirc.F:287-290, 376-384), the friction flags
     and FRIC = CF (or TAU when NOLIBF = 0) (nodalattr.F:1974-2001), the ramps
     of NRAMP (read_input.F:2893-2955), periodic elevation constituents and,
-    with flux boundaries, the periodic flux constituents.  Runs this path
+    with flux boundaries, the periodic flux constituents.  As the reference
+    does, a fort.19 beside the fort.15 adds non-periodic boundary
+    elevations (read_input.F:1893-1898), NFFR <= 0 reads the fluxes from
+    the fort.20 and NWS = 8 the track from the fort.22 (unless `vortex` is
+    given); `fort19`/`fort20`/`fort22` name other paths.  Runs this path
     does not cover raise NotImplementedError: ICS = 2, NCOR = 1, tidal
-    potential, hot starts, TAU0 = -5, non-periodic flux (NFFR <= 0) and
-    NWS = 8 without a `vortex` (the fort.22 track is not read)."""
+    potential, hot starts and TAU0 = -5."""
+    import pathlib
     from . import adcirc_io
+    here = pathlib.Path(fort15).parent
+    side = lambda given, name: pathlib.Path(given) if given is not None else here / name
     raw = adcirc_io.read_fort14(fort14)
     neta = int(raw.open_nodes.size)
     f = adcirc_io.read_fort15(fort15, neta, _raw_lbcodes(raw))
@@ -475,10 +481,11 @@ def case_from_files(fort14, fort15, vortex: "Vortex | None" = None,
         why.append("IHOT > 0 (use adc_hotstart_read)")
     if f.tau0 == -5.0:
         why.append("TAU0 = -5 (time-varying TAU0)")
-    if any(t in (2, 12, 22, 52, 32) for t, _ in raw.land_segments) and f.nffr <= 0:
-        why.append("NFFR <= 0 (non-periodic fort.20 flux)")
-    if abs(f.nws) == 8 and vortex is None:
-        why.append("NWS = 8 without a vortex track")
+    has_flux = any(t in (2, 12, 22, 52, 32) for t, _ in raw.land_segments)
+    if has_flux and f.nffr <= 0 and not side(fort20, "fort.20").exists():
+        why.append("NFFR <= 0 without a fort.20")
+    if abs(f.nws) == 8 and vortex is None and not side(fort22, "fort.22").exists():
+        why.append("NWS = 8 without a fort.22 track")
     if why:
         raise NotImplementedError(f"{fort15}: " + "; ".join(why))
     params = default_params(
@@ -508,7 +515,19 @@ def case_from_files(fort14, fort15, vortex: "Vortex | None" = None,
         case.flux = Flux(f.famig.copy(), fper, f.fff.copy(), f.fface.copy(), f.qnam.copy(),
                          f.qnph.copy(), flux_settling_it=sched.flux_settling_it,
                          enam=f.enam.copy() if has32 else None, enph=f.enph.copy() if has32 else None)
+    lbc = case.arrays["lbcodei"][:case.sizes["nvel"]]
+    start = f.statim * 86400.0
+    p19 = side(fort19, "fort.19")
+    if neta > 0 and p19.exists():
+        case.elev_series = adcirc_io.read_fort19(p19, neta, start_time=start)
+    if has_flux and f.nffr <= 0:
+        case.flux_series = adcirc_io.read_fort20(side(fort20, "fort.20"), lbc, start_time=start,
+                                                 flux_settling_it=sched.flux_settling_it)
     if abs(f.nws) == 8:
+        if vortex is None:
+            vortex = adcirc_io.read_fort22(side(fort22, "fort.22"), f.irefyr, f.irefmo, f.irefday,
+                                           f.irefhr, f.slam0, f.sfea0, f.rnday, bladj=f.bladj,
+                                           start_time=start)
         case.vortex = vortex
     case.meta["fort15"] = f
     return case

@@ -163,6 +163,28 @@ typedef struct {
   const adc_vortex_fix_t *fix;
 } adc_vortex_t;
 
+/* fort.22 reader for NWS = 8 (readBestTrackData, nws08.F90:884-1098): the
+ * ATCF best-track lines (BEST, OFCL, CALM) as track fixes.  Times are
+ * seconds since the wind reference time of the fort.15 NWS = 8 record
+ * (TIMECONV, global.F:1556-1583); the centre is projected to mesh
+ * coordinates with the CPP projection about (SLAM0, SFEA0) that ICS = 1
+ * meshes use (mesh.F:3409-3418); pressure, wind and radius units and the
+ * translation velocity (uvtrans, wind/vortex.F:1174-1200) are the
+ * reference's.  A CALM line gives a fix with a negative cpress. */
+typedef struct {
+  int irefyr, irefmo, irefday, irefhr;   /* wind reference time (fort.15) */
+  double slam0, sfea0;                   /* CPP projection centre, degrees (fort.15) */
+  double rnday;                          /* the track must reach RNDAY days; <= 0: no check */
+} adc_fort22_opts_t;
+
+/* With fix == NULL sets *nfix to the number of track times; otherwise fills
+ * up to *nfix fixes (ADC_ERR_ARG if the track has more) and sets *nfix.
+ * ADC_ERR_ARG on a missing or malformed file, an unknown line type, a
+ * forecast line without central pressure or Rmax, or a track that ends
+ * before RNDAY (the reference's fatal errors, nws08.F90:1017-1094). */
+int adc_fort22_read(const char *path, const adc_fort22_opts_t *opts, int *nfix,
+                    adc_vortex_fix_t *fix);
+
 /* Host-visible results of a step or phase. */
 typedef struct {
   int numitr;       /* NUMITR = IPARM(1) after JCG (gwce.F:2005) */

@@ -1633,6 +1633,24 @@ int orc_model_met(orc_model *m, const orc_step_t *s) {
   }
   const double lon = f[i - 1].x + m->vwtratio * (f[i].x - f[i - 1].x);
   const double lat = f[i - 1].y + m->vwtratio * (f[i].y - f[i - 1].y);
+  /* a CALM line on either side (castType, nws08.F90:858-872; a negative
+   * central pressure marks it): HollandGet returns zero wind and the
+   * background pressure in metres of water (nws08.F90:588-601); WTRATIO is
+   * not updated */
+  if (f[i].cpress < 0.0 || f[i - 1].cpress < 0.0) {
+    m->vcounter = i;
+    const double prn2 = PRB * 100.0 / (RHOW * p.g);
+    const double awr = vp.rho_air / RHOW;
+    for (int n = 0; n < a->np; ++n) {
+      const double wx = 0.0, wy = 0.0;
+      const double mag = std::sqrt(wx * wx + wy * wy);
+      const double drag = std::min(0.001 * (0.75 + 0.067 * mag), vp.drag_limit);
+      a->wsx2[n] = s->rampmete * awr * drag * wx * mag;
+      a->wsy2[n] = s->rampmete * awr * drag * wy * mag;
+      a->pr2[n] = p.prbckgrnd_mh2o + s->rampmete * (prn2 - p.prbckgrnd_mh2o);
+    }
+    return err;
+  }
   const double wt = (s->timeloc - f[i - 1].time) / (f[i].time - f[i - 1].time);
   m->vwtratio = wt;
   const double cpress = f[i - 1].cpress + wt * (f[i].cpress - f[i - 1].cpress);

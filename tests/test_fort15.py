@@ -240,3 +240,53 @@ def test_coupled_flux_radiation_case_through_files(lib, orc, tmp_path):
         om.run(1, 300)
         om.close()
     assert np.array_equal(c.arrays["eta2"], c2.arrays["eta2"])
+
+
+def test_series_case_through_files(lib, orc, tmp_path):
+    """NBFR 0 with a fort.19 beside the fort.15, and NFFR 0 with a fort.20:
+    case_from_files finds both as the reference does (read_input.F:1893-1898,
+    cstart.F:198-256), the records survive the files, and the oracle steps
+    both cases to the same state."""
+    import oracle
+    c = model.channel_case(river=0.5, elev_series=150.0, flux_series=300.0, series_hours=1.0)
+    lbc = c.arrays["lbcodei"][:c.sizes["nvel"]]
+    adcirc_io.write_fort14(c.meta["raw"], tmp_path / "fort.14")
+    adcirc_io.write_fort15(tmp_path / "fort.15", model.fort15_for_case(c), c.sizes["neta"], lbc)
+    adcirc_io.write_fort19(tmp_path / "fort.19", c.elev_series)
+    adcirc_io.write_fort20(tmp_path / "fort.20", c.flux_series, lbc)
+    c2 = model.case_from_files(tmp_path / "fort.14", tmp_path / "fort.15")
+    assert c2.flux is None and c2.sizes["nbfr"] == 0
+    assert np.array_equal(c2.elev_series.values, c.elev_series.values)
+    assert np.array_equal(c2.flux_series.values, c.flux_series.values)
+    assert c2.elev_series.interval == 150.0 and c2.flux_series.interval == 300.0
+    for case in (c, c2):
+        om = oracle.OracleModel(case)
+        om.run(1, 200)
+        om.close()
+    assert np.array_equal(c.arrays["eta2"], c2.arrays["eta2"])
+    assert np.array_equal(c.arrays["uu2"], c2.arrays["uu2"])
+
+
+def test_vortex_case_through_files(lib, orc, tmp_path):
+    """NWS = 8: the track comes from the fort.22 beside the fort.15, read
+    against the fort.15's wind reference time and projection centre."""
+    import oracle
+    from test_fort22 import atcf
+    c = model.channel_case(vortex=True)
+    lbc = c.arrays["lbcodei"][:c.sizes["nvel"]]
+    adcirc_io.write_fort14(c.meta["raw"], tmp_path / "fort.14")
+    adcirc_io.write_fort15(tmp_path / "fort.15", model.fort15_for_case(c), c.sizes["neta"], lbc)
+    lines = [atcf(2000, 1, 1, 0, "BEST", 0, 0, 0, 60, 970, 200, 8, ew="E"),
+             atcf(2000, 1, 1, 6, "BEST", 0, 2, 3, 60, 968, 200, 8, ew="E"),
+             atcf(2000, 1, 2, 0, "BEST", 0, 5, 6, 55, 975, 200, 9, ew="E")]
+    (tmp_path / "fort.22").write_text("\n".join(lines) + "\n")
+    with pytest.raises(NotImplementedError, match="fort.22"):
+        model.case_from_files(tmp_path / "fort.14", tmp_path / "fort.15", fort22=tmp_path / "none")
+    c2 = model.case_from_files(tmp_path / "fort.14", tmp_path / "fort.15")
+    want = adcirc_io.read_fort22(tmp_path / "fort.22", 2000, 1, 1, 0)
+    assert np.array_equal(c2.vortex.fixes, want.fixes)
+    assert c2.vortex.bladj == c.vortex.bladj
+    om = oracle.OracleModel(c2)
+    om.run(1, 20)
+    om.close()
+    assert np.abs(c2.arrays["wsx2"]).max() > 0.0

@@ -77,3 +77,14 @@ def test_set_vortex_rejects_bad_tracks(lib):
     v, arr = case.vortex.struct()
     assert lib.adc_set_vortex(g.h, C.byref(v)) != 0
     g.close()
+
+
+def test_vortex_calm_period(lib, orc):
+    """A track with a CALM line: no wind and the background pressure while it
+    brackets the time (nws08.F90:588-601, 858-872), the storm after it,
+    against the oracle over a graph-replayed run."""
+    from test_oracle_met import calm_track_case
+    c0, cg, io, ig = _pair(calm_track_case, 120, use_run=True)
+    _check(c0, cg, io, ig)
+    for f in ("wsx2", "wsy2", "pr2"):
+        assert _rel(cg.arrays[f], c0.arrays[f]) < 1e-13, f

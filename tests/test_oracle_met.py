@@ -133,6 +133,41 @@ def test_vortex_track_bookkeeping(orc):
     m.close()
 
 
+def calm_track_case(**kw):
+    """The channel with a vortex track of fixes every 100 s whose third fix
+    (t = 200 s) is a CALM line: steps with 100 s < TimeLoc <= 300 s have a
+    CALM fix on one side of them."""
+    from adcirc_b200 import model
+    case = model.channel_case(vortex=True, **kw)
+    case.vortex = model.straight_track(30.3e3, 3.7e3, 80.0, 6.0, 960.0, 8.0, 1.3, hours=1.0,
+                                       interval_h=100.0 / 3600.0)
+    case.vortex.fixes[2, 3] = -99999.0
+    return case
+
+
+def test_vortex_calm_period(orc):
+    """While a CALM line brackets the time, HollandGet returns no wind and
+    the background pressure in metres of water (nws08.F90:588-601), so the
+    stress is zero and PR2 the ramped background; the storm is back after
+    it."""
+    case = calm_track_case()
+    m = orc.OracleModel(case)
+    a = case.arrays
+    pb = case.params["prbckgrnd_mh2o"]
+    g = case.params["g"]
+    for it in range(1, 80):
+        m.step(it)
+        st = case.schedule.step(it)
+        calm = 100.0 < st.timeloc <= 300.0
+        if calm:
+            assert not np.any(a["wsx2"]) and not np.any(a["wsy2"]), it
+            want = pb + st.rampmete * (1013.0 * 100.0 / (1000.0 * g) - pb)
+            assert np.all(a["pr2"] == want), it
+        elif st.timeloc > 300.0:
+            assert np.abs(a["wsx2"]).max() > 0.0, it
+    m.close()
+
+
 def test_surge_track_makes_landfall():
     """The surge case's track (pc 940 hPa, Rmax 40 km, B 1.3, 5 m/s) starts
     offshore and crosses the coast (y ~ 640 km) within the simulated day."""
