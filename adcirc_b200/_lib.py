@@ -53,6 +53,7 @@ ARRAY_FIELDS = [
     ("coef", dp_), ("obccoef", dp_),
     ("gwce_lv", dp_), ("mom_lv_x", dp_), ("mom_lv_y", dp_),
     ("nelezng", ip_), ("zngif1", dp_), ("zngif2", dp_), ("zngif3", dp_), ("neitabele", ip_),
+    ("barlanht", dp_), ("barlancfsp", dp_),
 ]
 
 
@@ -64,7 +65,7 @@ class AdcArrays(C.Structure):
 class AdcStep(C.Structure):
     _fields_ = [("it", C.c_int), ("pad_", C.c_int), ("timeloc", C.c_double),
                 ("timeh", C.c_double), ("rampelev", C.c_double), ("rampmete", C.c_double),
-                ("rampextflux", C.c_double)]
+                ("rampextflux", C.c_double), ("rampintflux", C.c_double)]
 
 
 class AdcFlux(C.Structure):
@@ -191,6 +192,10 @@ def load():
                                        C.POINTER(AdcFort15Tables)]),
         "adc_fort14_write": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int, C.c_int, dp_, dp_, dp_, ip_,
                                        C.c_int, ip_, ip_, C.c_int, ip_, ip_, ip_]),
+        "adc_fort14_write_barriers": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int, C.c_int, dp_, dp_,
+                                                dp_, ip_, C.c_int, ip_, ip_, C.c_int, ip_, ip_, ip_,
+                                                dp_, dp_]),
+        "adc_fort14_barriers": (C.c_int, [C.c_char_p, dp_, dp_]),
         "adc_fort6x_header": (C.c_int, [C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p, C.c_int,
                                         C.c_int, C.c_double, C.c_int, C.c_int]),
         "adc_fort6x_append": (C.c_int, [C.c_char_p, C.c_double, C.c_int, C.c_int, dp_, dp_, ip_,

@@ -41,15 +41,20 @@ def read_fort14(path) -> RawMesh:
     _check(lib.adc_fort14_read(p, title, ptr(x, dp_), ptr(y, dp_), ptr(dp, dp_), ptr(nm, ip_),
                                ptr(nvdll, ip_), ptr(nbdv, ip_), ptr(nvell, ip_), ptr(ibtype, ip_),
                                ptr(nbvv, ip_)), "adc_fort14_read")
-    segs, q = [], 0
+    bht, bcf = np.zeros(max(nvel, 1)), np.zeros(max(nvel, 1))
+    if any(int(t) in (3, 13, 23) for t in ibtype[:nbou]):
+        _check(lib.adc_fort14_barriers(p, ptr(bht, dp_), ptr(bcf, dp_)), "adc_fort14_barriers")
+    segs, barriers, q = [], {}, 0
     for k in range(nbou):
         segs.append((int(ibtype[k]), nbvv[q:q + nvell[k]].astype(np.int64) - 1))
+        if int(ibtype[k]) in (3, 13, 23):
+            barriers[k] = (bht[q:q + nvell[k]].copy(), bcf[q:q + nvell[k]].copy())
         q += int(nvell[k])
     name = title.value.decode(errors="replace").strip() or os.path.basename(os.fsdecode(path))
     meta = {"lx": float(x.max() - x.min()), "ly": float(y.max() - y.min()),
             "open_segments": [int(v) for v in nvdll[:nope]], "source": os.fsdecode(path)}
     return RawMesh(name, x, y, dp, np.asarray(nm, np.int64) - 1,
-                   nbdv[:neta].astype(np.int64) - 1, segs, meta)
+                   nbdv[:neta].astype(np.int64) - 1, segs, meta, barriers)
 
 
 def write_fort14(raw: RawMesh, path, title: str | None = None) -> None:
@@ -66,11 +71,18 @@ def write_fort14(raw: RawMesh, path, title: str | None = None) -> None:
     nbvv = (np.concatenate([np.asarray(s, np.int32) + 1 for _, s in raw.land_segments])
             if raw.land_segments else np.zeros(1, np.int32))
     nbvv = np.ascontiguousarray(nbvv, np.int32)
-    _check(lib.adc_fort14_write(os.fsencode(path), (title or raw.name).encode()[:80],
-                                int(x.size), int(nm.shape[0]), ptr(x, dp_), ptr(y, dp_),
-                                ptr(dp, dp_), ptr(nm, ip_), len(lens), ptr(nvdll, ip_),
-                                ptr(nbdv, ip_), len(raw.land_segments), ptr(nvell, ip_),
-                                ptr(ibtype, ip_), ptr(nbvv, ip_)), "adc_fort14_write")
+    bht, bcf = np.zeros(max(nbvv.size, 1)), np.zeros(max(nbvv.size, 1))
+    q = 0
+    for k, (t, nodes) in enumerate(raw.land_segments):
+        if t in (3, 13, 23):
+            bht[q:q + len(nodes)], bcf[q:q + len(nodes)] = raw.barriers[k]
+        q += len(nodes)
+    _check(lib.adc_fort14_write_barriers(os.fsencode(path), (title or raw.name).encode()[:80],
+                                         int(x.size), int(nm.shape[0]), ptr(x, dp_), ptr(y, dp_),
+                                         ptr(dp, dp_), ptr(nm, ip_), len(lens), ptr(nvdll, ip_),
+                                         ptr(nbdv, ip_), len(raw.land_segments), ptr(nvell, ip_),
+                                         ptr(ibtype, ip_), ptr(nbvv, ip_), ptr(bht, dp_),
+                                         ptr(bcf, dp_)), "adc_fort14_write_barriers")
 
 
 class Fort6x:

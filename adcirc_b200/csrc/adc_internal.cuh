@@ -134,6 +134,8 @@ struct adc_ctx {
   int nfluxf, flux_on, nffr, n_fx;
   int nfluxrbc;          // radiation (IBTYPE 30) entries present
   int nfluxgbc;          // zero-normal-gradient (IBTYPE 40) entries present
+  int nfluxb;            // external barrier (IBTYPE 3/13/23) entries present
+  double *barht, *barcf; // BARLANHT, BARLANCFSP per boundary entry
   int n_zng;             // IBTYPE 40 momentum entries, in ME2GW order:
   int *zng_node, *zng_ele;   //   boundary node, NEleZNG (0-based)
   double *zng_f;             //   ZNGIF1-3 (3 per entry)

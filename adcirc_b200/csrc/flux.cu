@@ -24,6 +24,11 @@
 //  * the specified normal velocity -QN2/H2 of the momentum boundary
 //    conditions (momentum.F:815-856), read in k_mom_node; radiation nodes
 //    take no momentum boundary condition.
+// External barriers (IBTYPE 3/13/23) take as QN2 the free-surface
+// supercritical outflow over the crest once the water stands BARMIN above it
+// (COMPUTE_EXTERNAL_BOUNDARY_FLUX, weir_boundary.F90:1727-1763, called from
+// timestep.F:967-975 after the other fluxes); the GWCE integral and the
+// momentum equations then treat them like specified-flux entries.
 // It also holds the non-periodic boundary series: fort.20 fluxes in place of
 // the periodic constituents (NFFR <= 0, timestep.F:882-903) and fort.19
 // elevations added to the periodic boundary elevation in k_eta_bc
@@ -94,6 +99,12 @@ __global__ void k_flux_forcing(adc_ctx c, const adc_step_t *steps, const Flags *
     const size_t r1 = (size_t)ss.k * c.nvel, r2 = r1 + c.nvel;
     q = st.rampextflux * (c.fser_q[r1 + I] + ss.ratio * (c.fser_q[r2 + I] - c.fser_q[r1 + I]));
     el = st.rampextflux * (c.fser_e[r1 + I] + ss.ratio * (c.fser_e[r2 + I] - c.fser_e[r1 + I]));
+  }
+  if (lb == 3 || lb == 13 || lb == 23) {
+    // the weir formula with g and BARMIN = 0.04 m (weir_boundary.F90:51);
+    // (RBARWL g)^0.5 as a square root
+    const double RBARWL = 2.0 * (c.eta2[c.bnv[I]] - c.barht[I]) / 3.0;
+    q = RBARWL > 0.04 ? -st.rampintflux * c.barcf[I] * RBARWL * sqrt(RBARWL * c.p.g) : 0.0;
   }
   qn2[I] = q;
   en2[I] = el;
@@ -175,14 +186,14 @@ int launch_flux_forcing(adc_ctx *c) {
     launch_k(k_series_state, 1, 1, c->stream, *c, c->steps, c->flags);
     c->launches++;
   }
-  if (!c->nfluxf && !c->nfluxrbc && !c->nfluxgbc) return ADC_OK;
+  if (!c->nfluxf && !c->nfluxrbc && !c->nfluxgbc && !c->nfluxb) return ADC_OK;
   launch_k(k_flux_forcing, nblk(c->nvel), kThreads, c->stream, *c, c->steps, c->flags);
   c->launches++;
   return ADC_OK;
 }
 
 int launch_flux_rhs(adc_ctx *c) {
-  if (!c->nfluxf && !c->nfluxrbc && !c->nfluxgbc) return ADC_OK;
+  if (!c->nfluxf && !c->nfluxrbc && !c->nfluxgbc && !c->nfluxb) return ADC_OK;
   launch_k(k_flux_qforce, nblk(c->nvel), kThreads, c->stream, *c, c->steps, c->flags);
   launch_k(k_flux_rhs, nblk(c->n_fx), kThreads, c->stream, *c);
   c->launches += 2;
@@ -197,8 +208,10 @@ int flux_tables(adc_ctx *c, const adc_arrays_t *a) {
   c->nfluxf = 0;
   c->nfluxrbc = 0;
   c->nfluxgbc = 0;
+  c->nfluxb = 0;
   for (int I = 0; I < nv; ++I) {
     const int lb = a->lbcodei[I];
+    if (lb == 3 || lb == 13 || lb == 23) c->nfluxb = 1;
     if (lb == 2 || lb == 12 || lb == 22 || lb == 32 || lb == 52) c->nfluxf = 1;
     if (lb == 30 || lb == 32) c->nfluxrbc = 1;
     if (lb == 40 || lb == 41) c->nfluxgbc = 1;
@@ -212,7 +225,11 @@ int flux_tables(adc_ctx *c, const adc_arrays_t *a) {
   ADC_CUDA(cudaMemset(c->qn, 0, 3 * nva * sizeof(double)));
   ADC_CUDA(cudaMalloc((void **)&c->en, 3 * nva * sizeof(double)));
   ADC_CUDA(cudaMemset(c->en, 0, 3 * nva * sizeof(double)));
-  if (!c->nfluxf && !c->nfluxrbc && !c->nfluxgbc) return ADC_OK;
+  if (!c->nfluxf && !c->nfluxrbc && !c->nfluxgbc && !c->nfluxb) return ADC_OK;
+  if (c->nfluxb && (!a->barlanht || !a->barlancfsp)) {
+    set_error("the mesh has external barriers (IBTYPE 3/13/23) but no BARLANHT/BARLANCFSP");
+    return ADC_ERR_MESH;
+  }
   std::vector<int> bnv(nv);
   for (int I = 0; I < nv; ++I) bnv[I] = a->nbv[I] - 1;
   std::vector<std::vector<int>> lists(c->np);
@@ -249,6 +266,14 @@ int flux_tables(adc_ctx *c, const adc_arrays_t *a) {
   ADC_CUDA(cudaMalloc((void **)&c->bsiii, nva * sizeof(double)));
   ADC_CUDA(cudaMemcpy(c->bcsii, a->csii, nv * sizeof(double), cudaMemcpyHostToDevice));
   ADC_CUDA(cudaMemcpy(c->bsiii, a->siii, nv * sizeof(double), cudaMemcpyHostToDevice));
+  ADC_CUDA(cudaMalloc((void **)&c->barht, nva * sizeof(double)));
+  ADC_CUDA(cudaMalloc((void **)&c->barcf, nva * sizeof(double)));
+  ADC_CUDA(cudaMemset(c->barht, 0, nva * sizeof(double)));
+  ADC_CUDA(cudaMemset(c->barcf, 0, nva * sizeof(double)));
+  if (c->nfluxb) {
+    ADC_CUDA(cudaMemcpy(c->barht, a->barlanht, nv * sizeof(double), cudaMemcpyHostToDevice));
+    ADC_CUDA(cudaMemcpy(c->barcf, a->barlancfsp, nv * sizeof(double), cudaMemcpyHostToDevice));
+  }
   // EtaDisc at the river-radiation nodes from the bound (cold-start) ETA2,
   // cstart.F:1186-1191; ElevDisc is set by the steps
   std::vector<double> ed(nva, 0.0);

@@ -8,7 +8,9 @@
 // to 1..NP in file order and element and boundary references go through
 // that map.  Boundary segments of the types the 2DDI hot path handles
 // (one node per line: IBTYPE 0, 1, 2, 10, 11, 12, 20, 21, 22, 30, 32, 40,
-// 41, 52, 102, 112, 122, 152) are returned; barrier types (3, 4, 5 families) and
+// 41, 52, 102, 112, 122, 152; external barriers 3, 13, 23 with the crest
+// height BARLANHT and discharge coefficient BARLANCFSP after the node,
+// mesh.F:460-473) are returned; internal barriers (4, 5 families) and
 // periodic segments (94) return ADC_ERR_UNSUPPORTED.
 #include <cerrno>
 #include <cmath>
@@ -101,6 +103,7 @@ bool simple_flux_type(long long t) {
   switch (t) {
     case 0: case 1: case 2: case 10: case 11: case 12: case 20: case 21: case 22: case 30:
     case 32: case 40: case 41: case 52: case 102: case 112: case 122: case 152:
+    case 3: case 13: case 23:
       return true;
     default:
       return false;
@@ -112,7 +115,10 @@ struct Mesh14 {
   std::vector<double> x, y, dp;
   std::vector<int> nm;                 // NM(NE,3), 1-based
   std::vector<int> nvdll, nbdv, nvell, ibtype, nbvv;
+  std::vector<double> barlanht, barlancfsp;   // per nbvv entry, 0 off external barriers
 };
+
+bool external_barrier(long long t) { return t == 3 || t == 13 || t == 23; }
 
 int parse14(const char *path, Mesh14 &m) {
   Reader r;
@@ -189,8 +195,13 @@ int parse14(const char *path, Mesh14 &m) {
       long long lab;
       int id;
       if (!r.inum(lab) || !find(lab, id)) return bad("flux boundary node");
+      double ht = 0.0, cf = 0.0;
+      if (external_barrier(t) && (!r.num(ht) || !r.num(cf)))
+        return bad("external barrier node (NBVV BARLANHT BARLANCFSP)");
       r.end_line();
       m.nbvv.push_back(id);
+      m.barlanht.push_back(ht);
+      m.barlancfsp.push_back(cf);
     }
   }
   if ((long long)m.nbvv.size() != nvel) return bad("NVEL does not match the segment lengths");
@@ -275,10 +286,35 @@ extern "C" int adc_fort14_read(const char *path, char *title, double *x, double 
   return ADC_OK;
 }
 
+extern "C" int adc_fort14_barriers(const char *path, double *barlanht, double *barlancfsp) {
+  if (!path || !barlanht || !barlancfsp) {
+    set_error("adc_fort14_barriers: null argument");
+    return ADC_ERR_ARG;
+  }
+  Mesh14 m;
+  int rc = parse14(path, m);
+  if (rc) return rc;
+  if (!m.barlanht.empty()) {
+    std::memcpy(barlanht, m.barlanht.data(), m.barlanht.size() * sizeof(double));
+    std::memcpy(barlancfsp, m.barlancfsp.data(), m.barlancfsp.size() * sizeof(double));
+  }
+  return ADC_OK;
+}
+
 extern "C" int adc_fort14_write(const char *path, const char *title, int np, int ne, const double *x,
                                 const double *y, const double *dp, const int *nm, int nope,
                                 const int *nvdll, const int *nbdv, int nbou, const int *nvell,
                                 const int *ibtype, const int *nbvv) {
+  return adc_fort14_write_barriers(path, title, np, ne, x, y, dp, nm, nope, nvdll, nbdv, nbou,
+                                   nvell, ibtype, nbvv, nullptr, nullptr);
+}
+
+extern "C" int adc_fort14_write_barriers(const char *path, const char *title, int np, int ne,
+                                         const double *x, const double *y, const double *dp,
+                                         const int *nm, int nope, const int *nvdll,
+                                         const int *nbdv, int nbou, const int *nvell,
+                                         const int *ibtype, const int *nbvv,
+                                         const double *barlanht, const double *barlancfsp) {
   if (!path || !x || !y || !dp || !nm || np < 3 || ne < 1 || nope < 0 || nbou < 0) {
     set_error("adc_fort14_write: bad arguments");
     return ADC_ERR_ARG;
@@ -305,7 +341,19 @@ extern "C" int adc_fort14_write(const char *path, const char *title, int np, int
   q = 0;
   for (int k = 0; k < nbou; ++k) {
     std::fprintf(f, "%d %d\n", nvell[k], ibtype[k]);
-    for (int j = 0; j < nvell[k]; ++j) std::fprintf(f, "%d\n", nbvv[q++]);
+    const bool bar = external_barrier(ibtype[k]);
+    if (bar && (!barlanht || !barlancfsp)) {
+      std::fclose(f);
+      set_error("adc_fort14_write: segment %d is an external barrier; its heights and "
+                "coefficients are required", k + 1);
+      return ADC_ERR_ARG;
+    }
+    for (int j = 0; j < nvell[k]; ++j, ++q) {
+      if (bar)
+        std::fprintf(f, "%d %.17g %.17g\n", nbvv[q], barlanht[q], barlancfsp[q]);
+      else
+        std::fprintf(f, "%d\n", nbvv[q]);
+    }
   }
   if (std::fclose(f) != 0) { set_error("adc_fort14_write: write to %s failed", path); return ADC_ERR_ARG; }
   return ADC_OK;

@@ -170,8 +170,8 @@ int adc_mesh_csr_positions(int np, int ne, int mnei, const int *nm, const int *n
 /*
  * Flow-boundary arrays for external land segments (IBTYPE 0, 10, 20),
  * islands (IBTYPE 1, 11, 21), specified-flow (2, 12, 22), radiation (30),
- * coupled flux/radiation (32), zero-normal-gradient (40, 41) and
- * river-radiation (52) segments,
+ * coupled flux/radiation (32), zero-normal-gradient (40, 41),
+ * river-radiation (52) and external barrier (3, 13, 23) segments,
  * mesh.F:2180-2800.  seg_ptr[k]..seg_ptr[k+1]-1
  * index seg_nodes (1-based node numbers, as listed in fort.14).  Outputs are
  * sized by the caller for nvel_max entries (sum of segment lengths plus one
@@ -186,8 +186,8 @@ int adc_boundary_setup(int np, const double *x, const double *y, int nbou,
   /* flow types (specified flow, radiation) take the momentum equation
      where segments overlap (mesh.F:2529-2541, 2555-2566) */
   auto specified_flow = [](int code) {
-    return code == 2 || code == 12 || code == 22 || code == 30 || code == 32 || code == 40 ||
-           code == 41 || code == 52;
+    return code == 2 || code == 12 || code == 22 || code == 3 || code == 13 || code == 23 ||
+           code == 30 || code == 32 || code == 40 || code == 41 || code == 52;
   };
   for (int k = 0; k < nbou; ++k) {
     int t = ibtype[k];
@@ -252,6 +252,7 @@ int adc_boundary_setup(int np, const double *x, const double *y, int nbou,
         if (t == 0) lbcodei[jgw - 1] = 10;
         if (t == 1) lbcodei[jgw - 1] = 11;
         if (t == 2) lbcodei[jgw - 1] = 12;
+        if (t == 3) lbcodei[jgw - 1] = 13;
       }
       /* 2/3 of the segment to the next node, mesh.F:2301-2303 (zero after
          the last node of an unclosed segment) */

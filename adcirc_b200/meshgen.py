@@ -25,6 +25,9 @@ class RawMesh:
     open_nodes: np.ndarray  # elevation boundary node ids (0-based), in order
     land_segments: list    # list of (ibtype, node id array (0-based))
     meta: dict
+    # external barrier segments (IBTYPE 3/13/23): segment index ->
+    # (BARLANHT crest heights [m above datum], BARLANCFSP coefficients), per node
+    barriers: dict = dataclasses.field(default_factory=dict)
 
 
 def channel_mesh(nx: int = 121, ny: int = 41, lx: float = 60e3, ly: float = 20e3,

@@ -39,6 +39,7 @@ class Schedule:
     dramp_mete: float = 0.5  # days
     dunramp_mete: float = 0.0
     dramp_extflux: float | None = None   # days; None: the elevation ramp's
+    dramp_intflux: float | None = None   # days (barrier overflow); None: the elevation ramp's
     flux_settling_time: float = 0.0      # days (fort.15 FluxSettlingTime, NRAMP >= 2)
 
     @property
@@ -54,21 +55,29 @@ class Schedule:
         else:
             relev = math.tanh((2.0 * timeloc / 86400.0) / self.dramp)
             rmete = math.tanh((2.0 * (timeloc / 86400.0 - self.dunramp_mete)) / self.dramp_mete)
+        dix = self.dramp if self.dramp_intflux is None else self.dramp_intflux
+        if self.nramp == 0:
+            rint = 1.0
+        else:
+            rint = math.tanh((2.0 * timeloc / 86400.0) / dix)
         fsit = self.flux_settling_it
         if self.nramp > 1 and fsit > 0:
             # every forcing but the river flux waits for the flux to settle,
             # then ramps from there (timestep.F:314-345)
             if it < fsit + 10:
-                relev = rmete = 0.0
+                relev = rmete = rint = 0.0
             else:
                 tl = (it - fsit - 10) * self.dt + self.statim * 86400.0
                 relev = math.tanh((2.0 * tl / 86400.0) / self.dramp)
+                rint = math.tanh((2.0 * tl / 86400.0) / dix)
                 if self.nramp != 8:
                     rmete = math.tanh((2.0 * tl / 86400.0) / self.dramp_mete)
         if self.dramp < 1.0e-6:
             relev = 1.0
         if self.dramp_mete < 1.0e-6:
             rmete = 1.0
+        if dix < 1.0e-6:
+            rint = 1.0
         s = AdcStep()
         s.it = it
         s.timeloc = timeloc
@@ -80,6 +89,7 @@ class Schedule:
             s.rampextflux = 1.0
         else:
             s.rampextflux = math.tanh((2.0 * timeloc / 86400.0) / dfx)
+        s.rampintflux = rint
         return s
 
     def steps(self, it0: int, n: int):
@@ -379,6 +389,19 @@ def build_case(raw, params: dict, schedule: Schedule, tides, cf: float = 0.0025,
                            ptr(zngif[1], dp_), ptr(zngif[2], dp_))
         if rc != 0:
             raise RuntimeError(f"zero-normal-gradient setup failed: {rc}")
+    # external barriers (IBTYPE 3/13/23): crest and coefficient per entry, in
+    # the entry order of the boundary setup (islands gain a closing node)
+    barlanht, barlancfsp = np.zeros(max(nv, 1)), np.zeros(max(nv, 1))
+    j = 0
+    for k, (t, nodes) in enumerate(raw.land_segments):
+        n = len(nodes)
+        if t in (1, 11, 21) and nodes[0] != nodes[-1]:
+            n += 1
+        if t in (3, 13, 23):
+            barlanht[j:j + n], barlancfsp[j:j + n] = raw.barriers[k]
+        j += n
+    if j != nv:
+        raise RuntimeError(f"boundary entries {j} != NVEL {nv}")
     nbfr = len(tides)
     amig = _f([t[0] for t in tides], np.float64)
     face = _f([t[1] for t in tides], np.float64)
@@ -404,6 +427,7 @@ def build_case(raw, params: dict, schedule: Schedule, tides, cf: float = 0.0025,
         me2gw=_f(me2gw[:max(nme, 1)], np.int32),
         bndlen2o3=_f(bndlen[:max(nv, 1)], np.float64),
         nelezng=nelezng, zngif1=zngif[0], zngif2=zngif[1], zngif3=zngif[2], neitabele=neitabele,
+        barlanht=barlanht, barlancfsp=barlancfsp,
     )
     for k in STATE_F64:
         A[k] = np.zeros(npn, np.float64)
@@ -502,7 +526,8 @@ def case_from_files(fort14, fort15, vortex: "Vortex | None" = None,
         params["fgamma"] = f.fgamma
     sched = Schedule(dt=f.dtdp, statim=f.statim, reftim=f.reftim, nramp=f.nramp, dramp=f.dramp_elev,
                      dramp_mete=f.dramp_mete, dunramp_mete=f.dunramp_mete,
-                     dramp_extflux=f.dramp_extflux, flux_settling_time=f.flux_settling_time)
+                     dramp_extflux=f.dramp_extflux, dramp_intflux=f.dramp_intflux,
+                     flux_settling_time=f.flux_settling_time)
     tides = [(float(f.amig[k]), float(f.face[k]), float(f.ff[k]), f.emo[k].copy(), f.efa[k].copy())
              for k in range(f.nbfr)]
     case = build_case(raw, params, sched, tides, cf=f.tau if f.nolibf == 0 else f.cf, tau0=f.tau0,
@@ -552,7 +577,8 @@ def fort15_for_case(case: Case, rnday: float = 1.0, rundes: str = "", runid: str
         o.irefyr, o.irefmo, o.irefday, o.irefhr, o.storm_number = 2000, 1, 1, 0, 1
         o.bladj = case.vortex.bladj if case.vortex is not None else 0.9
     o.nramp = 0 if s.nramp == 0 else 8
-    o.dramp = o.dramp_intflux = o.dramp_elev = o.dramp_tip = o.dramp_wrad = s.dramp
+    o.dramp = o.dramp_elev = o.dramp_tip = o.dramp_wrad = s.dramp
+    o.dramp_intflux = s.dramp if s.dramp_intflux is None else s.dramp_intflux
     o.dramp_extflux = s.dramp if s.dramp_extflux is None else s.dramp_extflux
     o.flux_settling_time = s.flux_settling_time
     o.dramp_mete, o.dunramp_mete = s.dramp_mete, s.dunramp_mete
@@ -593,6 +619,7 @@ def channel_case(dt: float = 5.0, amp: float = 0.5, vortex: bool = False,
                  river: float | None = None, river_type: int = 2, radiation: bool = False,
                  zero_gradient: int = 0, flux_settling: float = 0.0, river_eta: float = 0.05,
                  elev_series: float = 0.0, flux_series: float = 0.0, series_hours: float = 6.0,
+                 barrier: float | None = None, barrier_type: int = 3,
                  prep: MeshPrep | None = None, **kw) -> Case:
     """Tidal channel: 121x41 nodes, 20 m -> 5 m, M2 0.5 m, dt 5 s.  With
     `vortex`, a small Holland vortex (Rmax 8 km) crosses the channel.  With
@@ -610,10 +637,13 @@ def channel_case(dt: float = 5.0, amp: float = 0.5, vortex: bool = False,
     set-up of 0.1 m per hour.  With `flux_series` [s] (and `river`), the
     river flux comes from a fort.20 series of that interval (NFFR 0):
     the steady inflow modulated by 50 % with a one-hour period.  Series
-    cover `series_hours` of simulated time."""
+    cover `series_hours` of simulated time.  With `barrier` [m above datum],
+    the east end is an external barrier (IBTYPE `barrier_type`, 3, 13 or
+    23) with that crest height and a discharge coefficient of 1: water
+    leaves over it once it stands 6 cm above the crest."""
     from .meshgen import channel_mesh
     raw = channel_mesh()
-    if river is not None or radiation or zero_gradient:
+    if river is not None or radiation or zero_gradient or barrier is not None:
         nx, ny = 121, 41
         nid = lambda i, j: i * ny + j
         south = np.array([nid(i, 0) for i in range(nx)])
@@ -621,6 +651,9 @@ def channel_case(dt: float = 5.0, amp: float = 0.5, vortex: bool = False,
         north = np.array([nid(i, ny - 1) for i in range(nx - 1, -1, -1)])
         zg = 40 if zero_gradient is True else int(zero_gradient)
         east_type = 30 if radiation else (zg if zg else river_type)
+        if barrier is not None:
+            east_type = barrier_type
+            raw.barriers = {1: (np.full(east.size, float(barrier)), np.ones(east.size))}
         raw.land_segments = [(0, south), (east_type, east), (0, north)]
     neta = raw.open_nodes.size
     tides = [(2.0 * math.pi / M2_PERIOD, 0.0, 1.0, np.full(neta, amp), np.zeros(neta))]

@@ -103,6 +103,10 @@ typedef struct {
   const int *nelezng;            /* NEleZNG(NVEL), 1-based */
   const double *zngif1, *zngif2, *zngif3;   /* (NVEL) */
   const int *neitabele;          /* NeiTabEle(NP,MNEI), 1-based, 0 = none (IBTYPE 41) */
+  /* external barriers (IBTYPE 3/13/23, mesh.F:2570-2574): crest height above
+   * datum and the supercritical discharge coefficient per boundary entry;
+   * NULL when the mesh has none */
+  const double *barlanht, *barlancfsp;   /* (NVEL) */
 } adc_arrays_t;
 
 /* Per-step scalars TIMESTEP computes before the hot path (timestep.F:257-353). */
@@ -111,6 +115,7 @@ typedef struct {
   int pad_;
   double timeloc, timeh, rampelev, rampmete;
   double rampextflux;    /* RampExtFlux, the ramp of specified boundary fluxes */
+  double rampintflux;    /* RampIntFlux, the ramp of barrier overflow (IBTYPE 3/13/23) */
 } adc_step_t;
 
 /* Periodic specified normal flux on flux boundaries (IBTYPE 2, 12, 22, 32, 52):
@@ -311,6 +316,16 @@ int adc_fort14_write(const char *path, const char *title, int np, int ne, const 
                      const double *y, const double *dp, const int *nm, int nope, const int *nvdll,
                      const int *nbdv, int nbou, const int *nvell, const int *ibtype,
                      const int *nbvv);
+/* External barrier segments (IBTYPE 3/13/23) carry BARLANHT and BARLANCFSP
+ * on each node line (mesh.F:460-473): adc_fort14_barriers returns them per
+ * flux-boundary node (NVEL, in file order, 0 elsewhere), and
+ * adc_fort14_write_barriers writes a mesh that has such segments. */
+int adc_fort14_barriers(const char *path, double *barlanht, double *barlancfsp);
+int adc_fort14_write_barriers(const char *path, const char *title, int np, int ne,
+                              const double *x, const double *y, const double *dp, const int *nm,
+                              int nope, const int *nvdll, const int *nbdv, int nbou,
+                              const int *nvell, const int *ibtype, const int *nbvv,
+                              const double *barlanht, const double *barlancfsp);
 
 /* fort.15 model parameters of a 2DDI run (READ_INPUT, read_input.F:
  * 949-4566), positional records in read_input's order plus the namelist

@@ -34,11 +34,12 @@ module adcgpu_iface
       type(c_ptr) :: wsx1, wsy1, wsx2, wsy2, pr1, pr2, coef, obccoef
       type(c_ptr) :: gwce_lv, mom_lv_x, mom_lv_y
       type(c_ptr) :: nelezng, zngif1, zngif2, zngif3, neitabele
+      type(c_ptr) :: barlanht, barlancfsp
    end type
 
    type, bind(C), public :: adc_step_t
       integer(c_int) :: it, pad_
-      real(c_double) :: timeloc, timeh, rampelev, rampmete, rampextflux
+      real(c_double) :: timeloc, timeh, rampelev, rampmete, rampextflux, rampintflux
    end type
 
    type, bind(C), public :: adc_flux_t

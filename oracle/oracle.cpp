@@ -586,6 +586,7 @@ struct orc_model {
   int nfluxf = 0, flux_on = 0, nffr = 0;
   int nfluxrbc = 0;   /* radiation (IBTYPE 30) entries, mesh.F:2045 */
   int nfluxgbc = 0;   /* zero normal velocity gradient (IBTYPE 40) entries, mesh.F:2072 */
+  int nfluxb = 0;     /* external barrier (IBTYPE 3/13/23) entries, mesh.F:1913 */
   /* river radiation (IBTYPE 52): FluxSettlingIT, EtaDisc_Fill and
    * EtaDisc/ElevDisc at the boundary entries (timestep.F:183, 243-245) */
   int flux_settling_it = 0, etadisc_fill = 1;
@@ -658,6 +659,7 @@ orc_model *orc_model_create(const orc_params_t *p, orc_arrays_t *a) {
     if (lb == 2 || lb == 12 || lb == 22 || lb == 32 || lb == 52) m->nfluxf = 1;
     if (lb == 30 || lb == 32) m->nfluxrbc = 1;   /* mesh.F:2044-2045, 2056-2058 */
     if (lb == 40 || lb == 41) m->nfluxgbc = 1;
+    if (lb == 3 || lb == 13 || lb == 23) m->nfluxb = 1;
   }
   /* EtaDisc at river-radiation nodes from the cold-start ETA2, cstart.F:1186-1191 */
   m->elevdisc.assign(std::max(a->nvel, 1), 0.0);
@@ -818,6 +820,7 @@ int orc_model_set_flux_series(orc_model *m, const orc_series_t *s) {
  * discharge at radiation entries, timestep.F:932-940 */
 static void orc_model_flux(orc_model *m, const orc_step_t *s) {
   orc_arrays_t *a = m->a;
+  const double G = m->p.g;
   if (m->nfluxf && m->flux_on) {
     for (int J = 0; J < m->nffr; ++J) {
       int NCYC = 0;
@@ -884,6 +887,21 @@ static void orc_model_flux(orc_model *m, const orc_step_t *s) {
       const int NNBB = a->nbv[I] - 1;
       const double UN1 = a->uu1[NNBB] * a->csii[I] + a->vv1[NNBB] * a->siii[I];
       m->qn1[I] = a->h2[NNBB] * UN1;
+    }
+  }
+  /* supercritical outflow over external barriers, timestep.F:967-975 and
+   * COMPUTE_EXTERNAL_BOUNDARY_FLUX (weir_boundary.F90:1727-1763; BARMIN
+   * 0.04 m, no time-varying crest) */
+  if (m->nfluxb) {
+    for (int I = 0; I < a->nvel; ++I) {
+      const int lb = a->lbcodei[I];
+      if (lb != 3 && lb != 13 && lb != 23) continue;
+      const int NNBB = a->nbv[I] - 1;
+      const double RBARWL = 2.0 * (a->eta2[NNBB] - a->barlanht[I]) / 3.0;
+      if (RBARWL > 0.04)
+        m->qn2[I] = -s->rampintflux * a->barlancfsp[I] * RBARWL * std::sqrt(RBARWL * G);
+      else
+        m->qn2[I] = 0.0;
     }
   }
   /* zero normal velocity gradient entries, timestep.F:945-952 */
@@ -1129,7 +1147,7 @@ int orc_model_gwce(orc_model *m, const orc_step_t *s, orc_stepout_t *out) {
   }
   /* boundary flux integral, gwce.F:1737-1834 (LBCODEI <= 29 types,
    * radiation 30 and river radiation 52, with the H1 saved above) */
-  if (m->nfluxf || m->nfluxrbc || m->nfluxgbc) {
+  if (m->nfluxf || m->nfluxrbc || m->nfluxgbc || m->nfluxb) {
     const double DT2 = p.dt * 2.0;
     auto qforce = [&](int J, int NBDJ) {
       if (a->lbcodei[J] == 32) {   /* gwce.F:1792-1797 */

@@ -79,13 +79,14 @@ typedef struct {
   const int *nelezng;       /* NEleZNG(NVEL), 1-based (IBTYPE 40 entries) */
   const double *zngif1, *zngif2, *zngif3;
   const int *neitabele;     /* NeiTabEle(NP,MNEI), 1-based, 0 = none */
+  const double *barlanht, *barlancfsp;   /* (NVEL) external barriers (IBTYPE 3/13/23) */
 } orc_arrays_t;
 
 /* Per-step scalars the TIMESTEP driver computes before the hot path. */
 typedef struct {
   int it;
   int pad_;
-  double timeloc, timeh, rampelev, rampmete, rampextflux;
+  double timeloc, timeh, rampelev, rampmete, rampextflux, rampintflux;
 } orc_step_t;
 
 /* Periodic specified normal flux (same layout as adc_flux_t). */

@@ -47,6 +47,7 @@ _ARR = [
     ("coef", dp_), ("obccoef", dp_),
     ("gwce_lv", dp_), ("mom_lv_x", dp_), ("mom_lv_y", dp_),
     ("nelezng", ip_), ("zngif1", dp_), ("zngif2", dp_), ("zngif3", dp_), ("neitabele", ip_),
+    ("barlanht", dp_), ("barlancfsp", dp_),
 ]
 
 
@@ -58,7 +59,7 @@ class OrcArrays(C.Structure):
 class OrcStep(C.Structure):
     _fields_ = [("it", C.c_int), ("pad_", C.c_int), ("timeloc", C.c_double),
                 ("timeh", C.c_double), ("rampelev", C.c_double), ("rampmete", C.c_double),
-                ("rampextflux", C.c_double)]
+                ("rampextflux", C.c_double), ("rampintflux", C.c_double)]
 
 
 class OrcFlux(C.Structure):
@@ -240,7 +241,7 @@ class OracleModel:
         s = self.case.schedule.step(it)
         o = OrcStep()
         o.it, o.timeloc, o.timeh, o.rampelev, o.rampmete = s.it, s.timeloc, s.timeh, s.rampelev, s.rampmete
-        o.rampextflux = s.rampextflux
+        o.rampextflux, o.rampintflux = s.rampextflux, s.rampintflux
         return o
 
     def step(self, it) -> OrcStepOut:

@@ -290,3 +290,24 @@ def test_vortex_case_through_files(lib, orc, tmp_path):
     om.run(1, 20)
     om.close()
     assert np.abs(c2.arrays["wsx2"]).max() > 0.0
+
+
+def test_external_barrier_case_through_files(lib, orc, tmp_path):
+    """An external barrier segment (crest heights and coefficients in the
+    fort.14) and DRampIntFlux (NRAMP 8 in the fort.15) survive the files,
+    and the oracle steps both cases to the same state."""
+    import oracle
+    c = model.channel_case(barrier=-0.5, barrier_type=13)
+    c.schedule.dramp_intflux = 0.2
+    adcirc_io.write_fort14(c.meta["raw"], tmp_path / "fort.14")
+    adcirc_io.write_fort15(tmp_path / "fort.15", model.fort15_for_case(c), c.sizes["neta"],
+                           c.arrays["lbcodei"][:c.sizes["nvel"]])
+    c2 = model.case_from_files(tmp_path / "fort.14", tmp_path / "fort.15")
+    assert c2.schedule.dramp_intflux == 0.2
+    for k, v in c.arrays.items():
+        assert np.array_equal(v, c2.arrays[k]), k
+    for case in (c, c2):
+        om = oracle.OracleModel(case)
+        om.run(1, 200)
+        om.close()
+    assert np.array_equal(c.arrays["eta2"], c2.arrays["eta2"])

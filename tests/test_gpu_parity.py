@@ -320,3 +320,19 @@ def test_channel_flux_series(lib, orc, river_type):
     a = c0.arrays
     east = a["x"] > 59.9e3
     assert a["uu2"][east].mean() < -0.02
+
+
+@pytest.mark.parametrize("btype,crest,nsteps", [(3, -0.05, 1500), (13, -0.5, 400), (23, -0.5, 400)])
+def test_channel_external_barrier(lib, orc, btype, crest, nsteps):
+    """An external barrier (IBTYPE 3/13/23) at the east end: the weir outflow
+    over the crest as QN2 (weir_boundary.F90:1727-1763), its GWCE boundary
+    integral and, for 3 and 13, the normal velocity of the momentum step,
+    against the oracle over a graph-replayed run.  With the crest at -0.05 m
+    the run passes from no outflow to outflow when the tide arrives."""
+    from adcirc_b200 import model
+    c0, cg, io, ig = _pair(lambda **k: model.channel_case(barrier=crest, barrier_type=btype, **k),
+                           nsteps, use_run=True)
+    _check(c0, cg, io, ig)
+    a = c0.arrays
+    east = a["x"] > 59.9e3
+    assert a["uu2"][east].mean() > 0.001   # water leaves over the barrier

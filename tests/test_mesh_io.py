@@ -82,6 +82,29 @@ def test_fort14_barrier_unsupported(lib, tmp_path):
         adcirc_io.read_fort14(p)
 
 
+def test_fort14_external_barrier(lib, tmp_path):
+    """IBTYPE 3/13/23 node lines carry BARLANHT and BARLANCFSP (read14,
+    mesh.F:460-473); they survive a write and a read."""
+    from adcirc_b200 import adcirc_io
+    text = ("t\n1 3\n1 0 0 1\n2 1 0 1\n3 0 1 1\n1 3 1 2 3\n0\n0\n2\n5\n"
+            "2 3\n1 0.5 1.0\n2 0.6D0 0.9\n3 0\n2\n3\n1\n")
+    p = tmp_path / "fort.14"
+    p.write_text(text)
+    m = adcirc_io.read_fort14(p)
+    assert [t for t, _ in m.land_segments] == [3, 0]
+    assert np.array_equal(m.barriers[0][0], [0.5, 0.6]) and np.array_equal(m.barriers[0][1], [1.0, 0.9])
+    assert 1 not in m.barriers
+    q = tmp_path / "back.14"
+    adcirc_io.write_fort14(m, q)
+    m2 = adcirc_io.read_fort14(q)
+    assert np.array_equal(m2.barriers[0][0], m.barriers[0][0])
+    assert np.array_equal(m2.barriers[0][1], m.barriers[0][1])
+    bad = tmp_path / "bad.14"
+    bad.write_text(text.replace("2 0.6D0 0.9", "2"))
+    with pytest.raises(OSError, match="external barrier"):
+        adcirc_io.read_fort14(bad)
+
+
 def test_fort63_64_format(lib, tmp_path):
     from adcirc_b200 import adcirc_io
     p = tmp_path / "fort.63"

@@ -121,3 +121,35 @@ def test_zero_gradient_boundary_takes_the_interior_velocity(orc):
         assert np.allclose(v[a["nbv"][j] - 1], interp, rtol=0, atol=1e-15)
     east = a["x"] > 59.9e3
     assert a["uu2"][east].mean() > 0.02
+
+
+def test_external_barrier_outflow_follows_the_weir_formula(orc):
+    """IBTYPE 13 (external barrier, no tangential slip): the normal velocity
+    at each boundary node is QN2/H2 with QN2 the supercritical weir outflow
+    RampIntFlux * BARLANCFSP * R * sqrt(R g), R = 2/3 of the head over the
+    crest at the start of the step, once R exceeds BARMIN = 0.04 m
+    (weir_boundary.F90:1751-1759, momentum.F:846-856); below it, none."""
+    from adcirc_b200 import model
+    case = model.channel_case(barrier=-0.05, barrier_type=13)
+    a = case.arrays
+    lbc = a["lbcodei"]
+    ent = np.nonzero(lbc == 13)[0]
+    assert ent.size > 30
+    nodes = a["nbv"][ent] - 1
+    g = case.params["g"]
+    om = orc.OracleModel(case)
+    flowing = dry_steps = 0
+    for it in range(1, 1401):
+        head = a["eta2"][nodes].copy()          # ETA2 when the step starts
+        om.step(it)
+        st = case.schedule.step(it)
+        R = 2.0 * (head - a["barlanht"][ent]) / 3.0
+        q = np.where(R > 0.04, -st.rampintflux * a["barlancfsp"][ent] * R * np.sqrt(np.maximum(R, 0) * g),
+                     0.0)
+        wet = a["nodecode"][nodes] == 1
+        want = -q / a["h2"][nodes]
+        assert np.array_equal(a["uu2"][nodes][wet], want[wet]), it
+        flowing += int((R > 0.04).any())
+        dry_steps += int((R <= 0.04).all())
+    om.close()
+    assert flowing > 100 and dry_steps > 100
