@@ -44,12 +44,21 @@ def read_fort14(path) -> RawMesh:
     bht, bcf = np.zeros(max(nvel, 1)), np.zeros(max(nvel, 1))
     if any(int(t) in (3, 13, 23) for t in ibtype[:nbou]):
         _check(lib.adc_fort14_barriers(p, ptr(bht, dp_), ptr(bcf, dp_)), "adc_fort14_barriers")
+    ibc = np.zeros(max(nvel, 1), np.int32)
+    iht, icb, icp = (np.zeros(max(nvel, 1)) for _ in range(3))
+    if any(int(t) in (4, 24) for t in ibtype[:nbou]):
+        _check(lib.adc_fort14_internal_barriers(p, ptr(ibc, ip_), ptr(iht, dp_), ptr(icb, dp_),
+                                                ptr(icp, dp_)), "adc_fort14_internal_barriers")
     segs, barriers, q = [], {}, 0
     for k in range(nbou):
-        segs.append((int(ibtype[k]), nbvv[q:q + nvell[k]].astype(np.int64) - 1))
+        n = int(nvell[k])
+        segs.append((int(ibtype[k]), nbvv[q:q + n].astype(np.int64) - 1))
         if int(ibtype[k]) in (3, 13, 23):
-            barriers[k] = (bht[q:q + nvell[k]].copy(), bcf[q:q + nvell[k]].copy())
-        q += int(nvell[k])
+            barriers[k] = (bht[q:q + n].copy(), bcf[q:q + n].copy())
+        if int(ibtype[k]) in (4, 24):
+            barriers[k] = (iht[q:q + n].copy(), icb[q:q + n].copy(), icp[q:q + n].copy(),
+                           ibc[q:q + n].astype(np.int64) - 1)
+        q += n
     name = title.value.decode(errors="replace").strip() or os.path.basename(os.fsdecode(path))
     meta = {"lx": float(x.max() - x.min()), "ly": float(y.max() - y.min()),
             "open_segments": [int(v) for v in nvdll[:nope]], "source": os.fsdecode(path)}
@@ -72,17 +81,24 @@ def write_fort14(raw: RawMesh, path, title: str | None = None) -> None:
             if raw.land_segments else np.zeros(1, np.int32))
     nbvv = np.ascontiguousarray(nbvv, np.int32)
     bht, bcf = np.zeros(max(nbvv.size, 1)), np.zeros(max(nbvv.size, 1))
+    ibc = np.zeros(max(nbvv.size, 1), np.int32)
+    iht, icb, icp = (np.zeros(max(nbvv.size, 1)) for _ in range(3))
     q = 0
     for k, (t, nodes) in enumerate(raw.land_segments):
+        n = len(nodes)
         if t in (3, 13, 23):
-            bht[q:q + len(nodes)], bcf[q:q + len(nodes)] = raw.barriers[k]
-        q += len(nodes)
+            bht[q:q + n], bcf[q:q + n] = raw.barriers[k]
+        if t in (4, 24):
+            iht[q:q + n], icb[q:q + n], icp[q:q + n], across = raw.barriers[k]
+            ibc[q:q + n] = np.asarray(across) + 1
+        q += n
     _check(lib.adc_fort14_write_barriers(os.fsencode(path), (title or raw.name).encode()[:80],
                                          int(x.size), int(nm.shape[0]), ptr(x, dp_), ptr(y, dp_),
                                          ptr(dp, dp_), ptr(nm, ip_), len(lens), ptr(nvdll, ip_),
                                          ptr(nbdv, ip_), len(raw.land_segments), ptr(nvell, ip_),
                                          ptr(ibtype, ip_), ptr(nbvv, ip_), ptr(bht, dp_),
-                                         ptr(bcf, dp_)), "adc_fort14_write_barriers")
+                                         ptr(bcf, dp_), ptr(ibc, ip_), ptr(iht, dp_),
+                                         ptr(icb, dp_), ptr(icp, dp_)), "adc_fort14_write_barriers")
 
 
 class Fort6x:

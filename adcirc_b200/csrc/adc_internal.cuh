@@ -136,6 +136,12 @@ struct adc_ctx {
   int nfluxgbc;          // zero-normal-gradient (IBTYPE 40) entries present
   int nfluxb;            // external barrier (IBTYPE 3/13/23) entries present
   double *barht, *barcf; // BARLANHT, BARLANCFSP per boundary entry
+  int nfluxib;           // internal barrier (IBTYPE 4/24) entries present
+  int *ibconn;           // per boundary entry: the node across the barrier (0-based)
+  int *ibkind;           // per entry: 0 first, 1 last, 2 inner node of its face; -1 none
+  double *binht, *bincfsb, *bincfsp;   // BARINHT, BARINCFSB, BARINCFSP per entry
+  int *nib;              // NIBNODECODE (NP): receives barrier overflow this step
+  int *nibcnt;           // NIBCNT (NP), wetdry.F:813-816
   int n_zng;             // IBTYPE 40 momentum entries, in ME2GW order:
   int *zng_node, *zng_ele;   //   boundary node, NEleZNG (0-based)
   double *zng_f;             //   ZNGIF1-3 (3 per entry)

@@ -29,6 +29,13 @@
 // (COMPUTE_EXTERNAL_BOUNDARY_FLUX, weir_boundary.F90:1727-1763, called from
 // timestep.F:967-975 after the other fluxes); the GWCE integral and the
 // momentum equations then treat them like specified-flux entries.
+// Internal barriers (IBTYPE 4/24) pass water between the paired nodes of
+// their two faces (COMPUTE_INTERNAL_BOUNDARY_FLUX, weir_boundary.F90:
+// 1775-1942, called per entry from timestep.F:1003-1026): sub- or
+// supercritical weir flow from the higher side once it stands BARMIN over
+// the crest, none while the source node or all its neighbours along the
+// barrier are dry; a receiving node is flagged in NIBNODECODE, which the
+// wet/dry step uses (wetdry.F:813-816, 1086-1090, 1114).
 // It also holds the non-periodic boundary series: fort.20 fluxes in place of
 // the periodic constituents (NFFR <= 0, timestep.F:882-903) and fort.19
 // elevations added to the periodic boundary elevation in k_eta_bc
@@ -65,6 +72,49 @@ __global__ void k_series_state(adc_ctx c, const adc_step_t *steps, Flags *flags)
     }
     st.ratio = (timeloc - st.t1) / inc;
   }
+}
+
+// COMPUTE_INTERNAL_BOUNDARY_FLUX (weir_boundary.F90:1775-1942, the default
+// wet-edge formulation without averaging); the square roots stand for the
+// reference's **0.5.
+__device__ double internal_barrier_flux(const adc_ctx &c, int I, double ramp) {
+  const int n1 = c.bnv[I], n2 = c.ibconn[I], kind = c.ibkind[I];
+  const int *nc = c.nodecode;
+  int wn1 = 0, wn2 = 0;   // wet neighbours along the barrier on each side
+  if (kind == 0) {
+    wn1 = wn1 + nc[c.bnv[I + 1]];
+    wn2 = wn2 + nc[c.ibconn[I + 1]];
+  } else if (kind == 1) {
+    wn1 = wn1 + nc[c.bnv[I - 1]];
+    wn2 = wn2 + nc[c.ibconn[I - 1]];
+  } else {
+    wn1 = wn1 + nc[c.bnv[I - 1]];
+    wn1 = wn1 + nc[c.bnv[I + 1]];
+    wn2 = wn2 + nc[c.ibconn[I + 1]];
+    wn2 = wn2 + nc[c.ibconn[I - 1]];
+  }
+  const double R1 = c.eta2[n1] - c.binht[I], R2 = c.eta2[n2] - c.binht[I];
+  const double R1F = 2.0 * R1 / 3.0, R2F = 2.0 * R2 / 3.0;
+  const double G = c.p.g, BARMIN = 0.04;
+  double flux = 0.0;
+  if ((R1 < 0.0) && (R2 < 0.0)) {
+    flux = 0.0;
+  } else if (fabs(R1 - R2) < 0.01) {
+    flux = 0.0;
+  } else if ((R1 > R2) && (R1 > BARMIN)) {   // this side is the source
+    if (nc[n1] == 0 || wn1 == 0) flux = 0.0;
+    else if (R2 > R1F) flux = -ramp * R2 * c.bincfsb[I] * sqrt(2.0 * G * (R1 - R2));
+    else flux = -ramp * c.bincfsp[I] * R1F * sqrt(R1F * G);
+  } else if ((R2 > R1) && (R2 > BARMIN)) {   // this side receives
+    if (nc[n2] == 0 || wn2 == 0) {
+      flux = 0.0;
+    } else {
+      if (R1 > R2F) flux = ramp * R1 * c.bincfsb[I] * sqrt(2.0 * G * (R2 - R1));
+      else flux = ramp * c.bincfsp[I] * R2F * sqrt(R2F * G);
+      c.nib[n1] = 1;
+    }
+  }
+  return flux;
 }
 
 __global__ void k_flux_forcing(adc_ctx c, const adc_step_t *steps, const Flags *flags) {
@@ -106,6 +156,7 @@ __global__ void k_flux_forcing(adc_ctx c, const adc_step_t *steps, const Flags *
     const double RBARWL = 2.0 * (c.eta2[c.bnv[I]] - c.barht[I]) / 3.0;
     q = RBARWL > 0.04 ? -st.rampintflux * c.barcf[I] * RBARWL * sqrt(RBARWL * c.p.g) : 0.0;
   }
+  if (lb == 4 || lb == 24) q = internal_barrier_flux(c, I, st.rampintflux);
   qn2[I] = q;
   en2[I] = el;
   if (lb == 52) {
@@ -186,14 +237,14 @@ int launch_flux_forcing(adc_ctx *c) {
     launch_k(k_series_state, 1, 1, c->stream, *c, c->steps, c->flags);
     c->launches++;
   }
-  if (!c->nfluxf && !c->nfluxrbc && !c->nfluxgbc && !c->nfluxb) return ADC_OK;
+  if (!c->nfluxf && !c->nfluxrbc && !c->nfluxgbc && !c->nfluxb && !c->nfluxib) return ADC_OK;
   launch_k(k_flux_forcing, nblk(c->nvel), kThreads, c->stream, *c, c->steps, c->flags);
   c->launches++;
   return ADC_OK;
 }
 
 int launch_flux_rhs(adc_ctx *c) {
-  if (!c->nfluxf && !c->nfluxrbc && !c->nfluxgbc && !c->nfluxb) return ADC_OK;
+  if (!c->nfluxf && !c->nfluxrbc && !c->nfluxgbc && !c->nfluxb && !c->nfluxib) return ADC_OK;
   launch_k(k_flux_qforce, nblk(c->nvel), kThreads, c->stream, *c, c->steps, c->flags);
   launch_k(k_flux_rhs, nblk(c->n_fx), kThreads, c->stream, *c);
   c->launches += 2;
@@ -209,9 +260,11 @@ int flux_tables(adc_ctx *c, const adc_arrays_t *a) {
   c->nfluxrbc = 0;
   c->nfluxgbc = 0;
   c->nfluxb = 0;
+  c->nfluxib = 0;
   for (int I = 0; I < nv; ++I) {
     const int lb = a->lbcodei[I];
     if (lb == 3 || lb == 13 || lb == 23) c->nfluxb = 1;
+    if (lb == 4 || lb == 24) c->nfluxib = 1;
     if (lb == 2 || lb == 12 || lb == 22 || lb == 32 || lb == 52) c->nfluxf = 1;
     if (lb == 30 || lb == 32) c->nfluxrbc = 1;
     if (lb == 40 || lb == 41) c->nfluxgbc = 1;
@@ -225,7 +278,7 @@ int flux_tables(adc_ctx *c, const adc_arrays_t *a) {
   ADC_CUDA(cudaMemset(c->qn, 0, 3 * nva * sizeof(double)));
   ADC_CUDA(cudaMalloc((void **)&c->en, 3 * nva * sizeof(double)));
   ADC_CUDA(cudaMemset(c->en, 0, 3 * nva * sizeof(double)));
-  if (!c->nfluxf && !c->nfluxrbc && !c->nfluxgbc && !c->nfluxb) return ADC_OK;
+  if (!c->nfluxf && !c->nfluxrbc && !c->nfluxgbc && !c->nfluxb && !c->nfluxib) return ADC_OK;
   if (c->nfluxb && (!a->barlanht || !a->barlancfsp)) {
     set_error("the mesh has external barriers (IBTYPE 3/13/23) but no BARLANHT/BARLANCFSP");
     return ADC_ERR_MESH;
@@ -266,6 +319,61 @@ int flux_tables(adc_ctx *c, const adc_arrays_t *a) {
   ADC_CUDA(cudaMalloc((void **)&c->bsiii, nva * sizeof(double)));
   ADC_CUDA(cudaMemcpy(c->bcsii, a->csii, nv * sizeof(double), cudaMemcpyHostToDevice));
   ADC_CUDA(cudaMemcpy(c->bsiii, a->siii, nv * sizeof(double), cudaMemcpyHostToDevice));
+  // internal barriers: the entry's place on its face, as the loop of
+  // timestep.F:1003-1026 walks the segments (J = 1..2 NVELL per barrier)
+  std::vector<int> ibk(nva, -1), ibc(nva, 0);
+  if (c->nfluxib) {
+    if (!a->ibconn || !a->barinht || !a->barincfsb || !a->barincfsp || !a->nvell || a->nbou < 1) {
+      set_error("the mesh has internal barriers (IBTYPE 4/24) but no IBCONN/BARINHT/BARINCFSB/"
+                "BARINCFSP/NVELL");
+      return ADC_ERR_MESH;
+    }
+    int I = 0;
+    for (int K = 0; K < a->nbou; ++K) {
+      if (I >= nv) {
+        set_error("NVELL overruns NVEL at boundary segment %d", K + 1);
+        return ADC_ERR_MESH;
+      }
+      const int lb = a->lbcodei[I], n = a->nvell[K];
+      if (lb == 4 || lb == 24) {
+        if (I + 2 * n > nv || n < 2) {
+          set_error("internal barrier segment %d does not fit NVEL", K + 1);
+          return ADC_ERR_MESH;
+        }
+        for (int J = 1; J <= 2 * n; ++J, ++I) {
+          ibk[I] = (J == 1 || J == n + 1) ? 0 : (J == n || J == 2 * n) ? 1 : 2;
+          const int across = a->ibconn[I];
+          if (across < 1 || across > c->np) {
+            set_error("IBCONN of boundary entry %d is out of range", I + 1);
+            return ADC_ERR_MESH;
+          }
+          ibc[I] = across - 1;
+        }
+      } else {
+        I += n;
+      }
+    }
+    if (I != nv) {
+      set_error("NVELL adds up to %d boundary entries, NVEL is %d", I, nv);
+      return ADC_ERR_MESH;
+    }
+  }
+  if ((rc = up_i(&c->ibkind, ibk))) return rc;
+  if ((rc = up_i(&c->ibconn, ibc))) return rc;
+  for (double **d : {&c->binht, &c->bincfsb, &c->bincfsp}) {
+    ADC_CUDA(cudaMalloc((void **)d, nva * sizeof(double)));
+    ADC_CUDA(cudaMemset(*d, 0, nva * sizeof(double)));
+  }
+  if (c->nfluxib) {
+    ADC_CUDA(cudaMemcpy(c->binht, a->barinht, nv * sizeof(double), cudaMemcpyHostToDevice));
+    ADC_CUDA(cudaMemcpy(c->bincfsb, a->barincfsb, nv * sizeof(double), cudaMemcpyHostToDevice));
+    ADC_CUDA(cudaMemcpy(c->bincfsp, a->barincfsp, nv * sizeof(double), cudaMemcpyHostToDevice));
+  }
+  const size_t npa = (size_t)c->np;
+  ADC_CUDA(cudaMalloc((void **)&c->nib, npa * sizeof(int)));
+  ADC_CUDA(cudaMemset(c->nib, 0, npa * sizeof(int)));
+  ADC_CUDA(cudaMalloc((void **)&c->nibcnt, npa * sizeof(int)));
+  ADC_CUDA(cudaMemset(c->nibcnt, 0, npa * sizeof(int)));
   ADC_CUDA(cudaMalloc((void **)&c->barht, nva * sizeof(double)));
   ADC_CUDA(cudaMalloc((void **)&c->barcf, nva * sizeof(double)));
   ADC_CUDA(cudaMemset(c->barht, 0, nva * sizeof(double)));

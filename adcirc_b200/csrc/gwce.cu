@@ -53,6 +53,7 @@ __global__ void k_shift_friction(adc_ctx c, const adc_step_t *steps, const Flags
   c.tkm[3 * i + 0] = tk;
   c.tkm[3 * i + 1] = tk;
   c.tkm[3 * i + 2] = 0.0;
+  if (c.nfluxib) c.nib[i] = 0;   // NIBNODECODE(:) = 0, timestep.F:1004
 }
 
 // Met forcing supplied by the host for this step (WSX2, WSY2, PR2).

@@ -60,7 +60,7 @@ static std::vector<HsRec> hs_records(adc_ctx *c) {
       {"itpack", c->itp, sizeof(Itp)},
   };
   if (c->vortex_on) r.push_back({"vortex", c->vstate, sizeof(VortexState)});
-  if (c->nfluxf || c->nfluxrbc || c->nfluxgbc || c->nfluxb) {
+  if (c->nfluxf || c->nfluxrbc || c->nfluxgbc || c->nfluxb || c->nfluxib) {
     r.push_back({"flux_qn", c->qn, 3 * (size_t)c->nvel * d});
     r.push_back({"flux_en", c->en, 3 * (size_t)c->nvel * d});
     r.push_back({"flux_elevdisc", c->elevdisc, (size_t)c->nvel * d});   // river radiation

@@ -10,7 +10,9 @@
 // (one node per line: IBTYPE 0, 1, 2, 10, 11, 12, 20, 21, 22, 30, 32, 40,
 // 41, 52, 102, 112, 122, 152; external barriers 3, 13, 23 with the crest
 // height BARLANHT and discharge coefficient BARLANCFSP after the node,
-// mesh.F:460-473) are returned; internal barriers (4, 5 families) and
+// mesh.F:460-473; internal barriers 4, 24 with the paired node IBCONN,
+// BARINHT, BARINCFSB and BARINCFSP, mesh.F:479-495, whose pairs count twice
+// in NVEL, mesh.F:260-265) are returned; barriers with pipes (5, 25) and
 // periodic segments (94) return ADC_ERR_UNSUPPORTED.
 #include <cerrno>
 #include <cmath>
@@ -103,7 +105,7 @@ bool simple_flux_type(long long t) {
   switch (t) {
     case 0: case 1: case 2: case 10: case 11: case 12: case 20: case 21: case 22: case 30:
     case 32: case 40: case 41: case 52: case 102: case 112: case 122: case 152:
-    case 3: case 13: case 23:
+    case 3: case 13: case 23: case 4: case 24:
       return true;
     default:
       return false;
@@ -116,9 +118,12 @@ struct Mesh14 {
   std::vector<int> nm;                 // NM(NE,3), 1-based
   std::vector<int> nvdll, nbdv, nvell, ibtype, nbvv;
   std::vector<double> barlanht, barlancfsp;   // per nbvv entry, 0 off external barriers
+  std::vector<int> ibconn;                     // per nbvv entry, 0 off internal barriers
+  std::vector<double> barinht, barincfsb, barincfsp;
 };
 
 bool external_barrier(long long t) { return t == 3 || t == 13 || t == 23; }
+bool internal_barrier(long long t) { return t == 4 || t == 24; }
 
 int parse14(const char *path, Mesh14 &m) {
   Reader r;
@@ -175,7 +180,7 @@ int parse14(const char *path, Mesh14 &m) {
     }
   }
   if ((long long)m.nbdv.size() != neta) return bad("NETA does not match the segment lengths");
-  long long nbou, nvel;
+  long long nbou, nvel, nvel_count = 0;
   if (!r.inum(nbou)) return bad("NBOU");
   r.end_line();
   if (!r.inum(nvel)) return bad("NVEL");
@@ -195,16 +200,27 @@ int parse14(const char *path, Mesh14 &m) {
       long long lab;
       int id;
       if (!r.inum(lab) || !find(lab, id)) return bad("flux boundary node");
-      double ht = 0.0, cf = 0.0;
+      double ht = 0.0, cf = 0.0, iht = 0.0, icb = 0.0, icp = 0.0;
+      int across = 0;
       if (external_barrier(t) && (!r.num(ht) || !r.num(cf)))
         return bad("external barrier node (NBVV BARLANHT BARLANCFSP)");
+      if (internal_barrier(t)) {
+        long long lab2;
+        if (!r.inum(lab2) || !find(lab2, across) || !r.num(iht) || !r.num(icb) || !r.num(icp))
+          return bad("internal barrier node (NBVV IBCONN BARINHT BARINCFSB BARINCFSP)");
+      }
       r.end_line();
       m.nbvv.push_back(id);
       m.barlanht.push_back(ht);
       m.barlancfsp.push_back(cf);
+      m.ibconn.push_back(across);
+      m.barinht.push_back(iht);
+      m.barincfsb.push_back(icb);
+      m.barincfsp.push_back(icp);
+      nvel_count += internal_barrier(t) ? 2 : 1;
     }
   }
-  if ((long long)m.nbvv.size() != nvel) return bad("NVEL does not match the segment lengths");
+  if (nvel_count != nvel) return bad("NVEL does not match the segment lengths");
   return ADC_OK;
 }
 
@@ -301,12 +317,32 @@ extern "C" int adc_fort14_barriers(const char *path, double *barlanht, double *b
   return ADC_OK;
 }
 
+extern "C" int adc_fort14_internal_barriers(const char *path, int *ibconn, double *barinht,
+                                            double *barincfsb, double *barincfsp) {
+  if (!path || !ibconn || !barinht || !barincfsb || !barincfsp) {
+    set_error("adc_fort14_internal_barriers: null argument");
+    return ADC_ERR_ARG;
+  }
+  Mesh14 m;
+  int rc = parse14(path, m);
+  if (rc) return rc;
+  const size_t n = m.nbvv.size();
+  if (n) {
+    std::memcpy(ibconn, m.ibconn.data(), n * sizeof(int));
+    std::memcpy(barinht, m.barinht.data(), n * sizeof(double));
+    std::memcpy(barincfsb, m.barincfsb.data(), n * sizeof(double));
+    std::memcpy(barincfsp, m.barincfsp.data(), n * sizeof(double));
+  }
+  return ADC_OK;
+}
+
 extern "C" int adc_fort14_write(const char *path, const char *title, int np, int ne, const double *x,
                                 const double *y, const double *dp, const int *nm, int nope,
                                 const int *nvdll, const int *nbdv, int nbou, const int *nvell,
                                 const int *ibtype, const int *nbvv) {
   return adc_fort14_write_barriers(path, title, np, ne, x, y, dp, nm, nope, nvdll, nbdv, nbou,
-                                   nvell, ibtype, nbvv, nullptr, nullptr);
+                                   nvell, ibtype, nbvv, nullptr, nullptr, nullptr, nullptr, nullptr,
+                                   nullptr);
 }
 
 extern "C" int adc_fort14_write_barriers(const char *path, const char *title, int np, int ne,
@@ -314,7 +350,9 @@ extern "C" int adc_fort14_write_barriers(const char *path, const char *title, in
                                          const int *nm, int nope, const int *nvdll,
                                          const int *nbdv, int nbou, const int *nvell,
                                          const int *ibtype, const int *nbvv,
-                                         const double *barlanht, const double *barlancfsp) {
+                                         const double *barlanht, const double *barlancfsp,
+                                         const int *ibconn, const double *barinht,
+                                         const double *barincfsb, const double *barincfsp) {
   if (!path || !x || !y || !dp || !nm || np < 3 || ne < 1 || nope < 0 || nbou < 0) {
     set_error("adc_fort14_write: bad arguments");
     return ADC_ERR_ARG;
@@ -336,21 +374,25 @@ extern "C" int adc_fort14_write_barriers(const char *path, const char *title, in
     for (int j = 0; j < nvdll[k]; ++j) std::fprintf(f, "%d\n", nbdv[q++]);
   }
   long long nvel = 0;
-  for (int k = 0; k < nbou; ++k) nvel += nvell[k];
+  for (int k = 0; k < nbou; ++k) nvel += internal_barrier(ibtype[k]) ? 2 * nvell[k] : nvell[k];
   std::fprintf(f, "%d\n%lld\n", nbou, nvel);
   q = 0;
   for (int k = 0; k < nbou; ++k) {
     std::fprintf(f, "%d %d\n", nvell[k], ibtype[k]);
-    const bool bar = external_barrier(ibtype[k]);
-    if (bar && (!barlanht || !barlancfsp)) {
+    const bool bar = external_barrier(ibtype[k]), ibar = internal_barrier(ibtype[k]);
+    if ((bar && (!barlanht || !barlancfsp)) ||
+        (ibar && (!ibconn || !barinht || !barincfsb || !barincfsp))) {
       std::fclose(f);
-      set_error("adc_fort14_write: segment %d is an external barrier; its heights and "
+      set_error("adc_fort14_write: segment %d is a barrier; its pairs, heights and "
                 "coefficients are required", k + 1);
       return ADC_ERR_ARG;
     }
     for (int j = 0; j < nvell[k]; ++j, ++q) {
       if (bar)
         std::fprintf(f, "%d %.17g %.17g\n", nbvv[q], barlanht[q], barlancfsp[q]);
+      else if (ibar)
+        std::fprintf(f, "%d %d %.17g %.17g %.17g\n", nbvv[q], ibconn[q], barinht[q], barincfsb[q],
+                     barincfsp[q]);
       else
         std::fprintf(f, "%d\n", nbvv[q]);
     }

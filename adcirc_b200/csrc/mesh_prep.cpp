@@ -171,7 +171,11 @@ int adc_mesh_csr_positions(int np, int ne, int mnei, const int *nm, const int *n
  * Flow-boundary arrays for external land segments (IBTYPE 0, 10, 20),
  * islands (IBTYPE 1, 11, 21), specified-flow (2, 12, 22), radiation (30),
  * coupled flux/radiation (32), zero-normal-gradient (40, 41),
- * river-radiation (52) and external barrier (3, 13, 23) segments,
+ * river-radiation (52) and external barrier (3, 13, 23) segments, and the
+ * faces of internal barriers (4, 24): mesh.F processes a barrier segment as
+ * its front face and then its back face, each an unclosed segment
+ * (mesh.F:2158-2192), so the caller lists the two faces as two segments of
+ * the barrier's type, the back face in the reversed order mesh.F gives it,
  * mesh.F:2180-2800.  seg_ptr[k]..seg_ptr[k+1]-1
  * index seg_nodes (1-based node numbers, as listed in fort.14).  Outputs are
  * sized by the caller for nvel_max entries (sum of segment lengths plus one
@@ -194,7 +198,8 @@ int adc_boundary_setup(int np, const double *x, const double *y, int nbou,
     bool island = (t == 1 || t == 11 || t == 21);
     bool mainland = (t == 0 || t == 10 || t == 20);
     bool flux = specified_flow(t);   /* external boundaries with normal flow or radiation */
-    if (!island && !mainland && !flux) return ADC_ERR_ARG;
+    bool barrier_face = (t == 4 || t == 24);
+    if (!island && !mainland && !flux && !barrier_face) return ADC_ERR_ARG;
     std::vector<int> nbvv;
     int nvell = seg_ptr[k + 1] - seg_ptr[k];
     if (nvell < 2) return ADC_ERR_ARG;

@@ -1,6 +1,8 @@
 // wetdry.cu -- computeWettingAndDrying (wetdry.F:140-1470) and computeAlpha
-// (wetdry.F:1561-1652): non-subgrid 2DDI, no weirs or barriers
-// (NIBNODECODE = 0, so W2a/W2b never fire), NDDT = 0, default NOFF rules.
+// (wetdry.F:1561-1652): non-subgrid 2DDI, NDDT = 0, default NOFF rules.
+// With internal barriers the nodes that receive overflow (NIBNODECODE, set
+// by the flux step) wet their elements' nodes through NIBCNT (W2a/W2b,
+// wetdry.F:813-816, 1086-1090) and exempt those elements from DE1 (:1114).
 //
 // Flags are integers and every pass except one is order independent, so
 // node and element passes run one thread per item.  The exception is the
@@ -395,6 +397,23 @@ __global__ void __launch_bounds__(1024) k_wd_chain(adc_ctx c) {
   }
 }
 
+// W2a/W2b with internal barriers: NIBCNT(i) sums NIBNODECODE over the nodes
+// of every element around node i (wetdry.F:813-816, an integer sum, so its
+// element order does not matter), and a node with NIBCNT > 0 is wet
+// (:1086-1090).
+__global__ void k_wd_w2b(adc_ctx c) {
+  griddep_wait();
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= c.np) return;
+  int cnt = 0;
+  for (int q = c.n2e_ptr[i]; q < c.n2e_ptr[i + 1]; ++q) {
+    const int e = c.n2e[q] / 3;
+    cnt += c.nib[c.nm[3 * e]] + c.nib[c.nm[3 * e + 1]] + c.nib[c.nm[3 * e + 2]];
+  }
+  c.nibcnt[i] = cnt;
+  if (cnt > 0 && c.nnodecode[i] == 0) c.nnodecode[i] = 1;
+}
+
 // DE1 (wetdry.F:1110-1162), then NCEle for D2 and the NOFF change count
 // (:1428-1430).
 __global__ void k_wd_de1(adc_ctx c) {
@@ -406,12 +425,16 @@ __global__ void k_wd_de1(adc_ctx c) {
   double E1 = c.eta2[NM1], E2 = c.eta2[NM2], E3 = c.eta2[NM3];
   double H1 = c.dp[NM1] + E1, H2 = c.dp[NM2] + E2, H3 = c.dp[NM3] + E3;
   int noff = c.noff[e];
-  if ((E1 >= E2) && (E2 > E3)) if ((H1 < HOFF) || (H2 < HOFF)) noff = 0;
-  if ((E2 >= E3) && (E3 > E1)) if ((H2 < HOFF) || (H3 < HOFF)) noff = 0;
-  if ((E3 >= E1) && (E1 > E2)) if ((H3 < HOFF) || (H1 < HOFF)) noff = 0;
-  if ((E1 >= E3) && (E3 > E2)) if ((H1 < HOFF) || (H3 < HOFF)) noff = 0;
-  if ((E2 >= E1) && (E1 > E3)) if ((H2 < HOFF) || (H1 < HOFF)) noff = 0;
-  if ((E3 >= E2) && (E2 > E1)) if ((H3 < HOFF) || (H2 < HOFF)) noff = 0;
+  // elements with a barrier-receiving node at every vertex keep NOFF (:1114)
+  const bool receiving = c.nfluxib && c.nibcnt[NM1] * c.nibcnt[NM2] * c.nibcnt[NM3] != 0;
+  if (!receiving) {
+    if ((E1 >= E2) && (E2 > E3)) if ((H1 < HOFF) || (H2 < HOFF)) noff = 0;
+    if ((E2 >= E3) && (E3 > E1)) if ((H2 < HOFF) || (H3 < HOFF)) noff = 0;
+    if ((E3 >= E1) && (E1 > E2)) if ((H3 < HOFF) || (H1 < HOFF)) noff = 0;
+    if ((E1 >= E3) && (E3 > E2)) if ((H1 < HOFF) || (H3 < HOFF)) noff = 0;
+    if ((E2 >= E1) && (E1 > E3)) if ((H2 < HOFF) || (H1 < HOFF)) noff = 0;
+    if ((E3 >= E2) && (E2 > E1)) if ((H3 < HOFF) || (H2 < HOFF)) noff = 0;
+  }
   c.noff[e] = noff;
   c.ncele[e] = c.nnodecode[NM1] * c.nnodecode[NM2] * c.nnodecode[NM3] * noff;
   if (noff != c.noffold[e]) atomicAdd(&c.flags->ncchange, 1);
@@ -514,6 +537,10 @@ int launch_wetdry(adc_ctx *c) {
   launch_k(k_wd_d1, nblk(c->np), kThreads, c->stream, cv);
   launch_k(k_wd_w1, c->ev_blocks, kW1Block, c->stream, cv);
   launch_k(k_wd_chain, 1, 1024, c->stream, cv);
+  if (c->nfluxib) {
+    launch_k(k_wd_w2b, nblk(c->np), kThreads, c->stream, cv);
+    c->launches++;
+  }
   launch_k(k_wd_de1, nblk(c->ne), kThreads, c->stream, cv);
   launch_k(k_wd_d2, nblk(c->np), kThreads, c->stream, cv);
   launch_k(k_wd_alpha, nblk(c->ne), kThreads, c->stream, cv);

@@ -66,6 +66,46 @@ def channel_mesh(nx: int = 121, ny: int = 41, lx: float = 60e3, ly: float = 20e3
                    {"nx": nx, "ny": ny, "lx": lx, "ly": ly})
 
 
+def levee_channel_mesh(crest: float, btype: int = 4, ib: int = 60, polder_depth: float = 0.0,
+                       cfsb: float = 1.0, cfsp: float = 1.0, gap: float = 50.0, **kw) -> RawMesh:
+    """The channel with an internal barrier (IBTYPE `btype`, 4 or 24) along
+    the column x = ib * dx: the column's inner nodes (all but the wall
+    corners) are duplicated, the elements east of the column use the copies,
+    and the two lines of nodes are the barrier's front (west) and back (east,
+    `gap` metres further east) faces, paired in order, with crest height `crest` [m above datum] and
+    discharge coefficients `cfsb` (subcritical) and `cfsp` (supercritical).
+    East of the barrier the bed is flat at depth `polder_depth` (0: the
+    datum, so the polder starts dry); the outer walls are one land segment
+    as in `channel_mesh`."""
+    m = channel_mesh(**kw)
+    nx, ny = m.meta["nx"], m.meta["ny"]
+    nid = lambda i, j: i * ny + j
+    npn = m.x.size
+    front = np.array([nid(ib, j) for j in range(1, ny - 1)], dtype=np.int64)
+    back = np.arange(npn, npn + front.size, dtype=np.int64)
+    # the back face stands `gap` east of the front face: NEIGHB sorts a
+    # node's neighbours by angle and cannot hold two at one place
+    # (mesh.F:3223-3235), which a shared wall-corner node would have
+    x = np.concatenate([m.x, m.x[front] + gap])
+    y = np.concatenate([m.y, m.y[front]])
+    dp = np.concatenate([m.dp, m.dp[front]])
+    east = x > m.x[nid(ib, 0)]
+    dp[east] = polder_depth
+    dp[back] = polder_depth
+    remap = np.arange(npn, dtype=np.int64)
+    remap[front] = back
+    nm = m.nm.copy()
+    # elements of the columns east of the barrier line take the copies
+    cx = m.x[m.nm].mean(axis=1)
+    east_el = cx > m.x[nid(ib, 0)]
+    nm[east_el] = remap[nm[east_el]]
+    n = front.size
+    barriers = {1: (np.full(n, float(crest)), np.full(n, float(cfsb)), np.full(n, float(cfsp)), back)}
+    meta = dict(m.meta, barrier_column=ib)
+    return RawMesh("levee_channel", x, y, dp, nm, m.open_nodes,
+                   [m.land_segments[0], (int(btype), front)], meta, barriers)
+
+
 def beach_mesh(nx: int = 41, ny: int = 13, lx: float = 4e3, ly: float = 1.2e3,
                depth0: float = 3.0, depth1: float = -1.5) -> RawMesh:
     """Small sloping-beach channel whose closed end rises above the datum.

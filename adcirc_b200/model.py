@@ -126,7 +126,7 @@ class Case:
 
     def arrays_struct(self) -> AdcArrays:
         a = AdcArrays()
-        for k in ("np", "ne", "mnei", "neta", "nbfr", "nvel", "nvelme"):
+        for k in ("np", "ne", "mnei", "neta", "nbfr", "nvel", "nvelme", "nbou"):
             setattr(a, k, int(self.sizes[k]))
         for name, typ in _lib.ARRAY_FIELDS:
             arr = self.arrays[name]
@@ -347,8 +347,17 @@ def build_case(raw, params: dict, schedule: Schedule, tides, cf: float = 0.0025,
     # boundaries
     nbd = _f(raw.open_nodes + 1, np.int32)
     neta = int(nbd.size)
-    ibtype = np.array([t for t, _ in raw.land_segments], np.int32)
-    segs = [np.asarray(s, np.int64) + 1 for _, s in raw.land_segments]
+    # an internal barrier (IBTYPE 4/24) is set up as its front face and then
+    # its back face, reversed (mesh.F:2158-2192)
+    faces = []
+    for k, (t, s) in enumerate(raw.land_segments):
+        if t in (4, 24):
+            back = np.asarray(raw.barriers[k][3], np.int64)
+            faces += [(t, np.asarray(s, np.int64)), (t, back[::-1])]
+        else:
+            faces.append((t, np.asarray(s, np.int64)))
+    ibtype = np.array([t for t, _ in faces], np.int32)
+    segs = [s + 1 for _, s in faces]
     seg_ptr = np.zeros(len(segs) + 1, np.int32)
     seg_ptr[1:] = np.cumsum([s.size for s in segs])
     seg_nodes = np.concatenate(segs).astype(np.int32)
@@ -389,16 +398,30 @@ def build_case(raw, params: dict, schedule: Schedule, tides, cf: float = 0.0025,
                            ptr(zngif[1], dp_), ptr(zngif[2], dp_))
         if rc != 0:
             raise RuntimeError(f"zero-normal-gradient setup failed: {rc}")
-    # external barriers (IBTYPE 3/13/23): crest and coefficient per entry, in
-    # the entry order of the boundary setup (islands gain a closing node)
+    # barriers per entry, in the entry order of the boundary setup (islands
+    # gain a closing node; internal barriers give two faces), and NVELL as
+    # mesh.F leaves it (closed islands, barrier pairs)
     barlanht, barlancfsp = np.zeros(max(nv, 1)), np.zeros(max(nv, 1))
+    ibconn = np.zeros(max(nv, 1), np.int32)
+    barin = [np.zeros(max(nv, 1)) for _ in range(3)]
+    nvell = np.zeros(max(len(raw.land_segments), 1), np.int32)
     j = 0
     for k, (t, nodes) in enumerate(raw.land_segments):
         n = len(nodes)
         if t in (1, 11, 21) and nodes[0] != nodes[-1]:
             n += 1
+        nvell[k] = n
         if t in (3, 13, 23):
             barlanht[j:j + n], barlancfsp[j:j + n] = raw.barriers[k]
+        if t in (4, 24):
+            ht, cfsb, cfsp, back = (np.asarray(v) for v in raw.barriers[k])
+            front = np.asarray(nodes, np.int64)
+            ibconn[j:j + n] = back + 1
+            ibconn[j + n:j + 2 * n] = front[::-1] + 1
+            for arr, v in zip(barin, (ht, cfsb, cfsp)):
+                arr[j:j + n] = v
+                arr[j + n:j + 2 * n] = v[::-1]
+            n *= 2
         j += n
     if j != nv:
         raise RuntimeError(f"boundary entries {j} != NVEL {nv}")
@@ -427,7 +450,8 @@ def build_case(raw, params: dict, schedule: Schedule, tides, cf: float = 0.0025,
         me2gw=_f(me2gw[:max(nme, 1)], np.int32),
         bndlen2o3=_f(bndlen[:max(nv, 1)], np.float64),
         nelezng=nelezng, zngif1=zngif[0], zngif2=zngif[1], zngif3=zngif[2], neitabele=neitabele,
-        barlanht=barlanht, barlancfsp=barlancfsp,
+        barlanht=barlanht, barlancfsp=barlancfsp, ibconn=ibconn, barinht=barin[0],
+        barincfsb=barin[1], barincfsp=barin[2], nvell=nvell,
     )
     for k in STATE_F64:
         A[k] = np.zeros(npn, np.float64)
@@ -453,7 +477,7 @@ def build_case(raw, params: dict, schedule: Schedule, tides, cf: float = 0.0025,
         if not v.flags.f_contiguous:
             A[k] = np.asfortranarray(v)
     sizes = dict(np=npn, ne=ne, mnei=mnei, neta=neta, nbfr=nbfr, nvel=nv, nvelme=nme,
-                 neimax=neimax.value)
+                 nbou=len(raw.land_segments), neimax=neimax.value)
     meta = dict(raw.meta)
     meta["build"] = dict(cf=cf, tau0=tau0, eslm=eslm, cori=cori, anginn=anginn)
     meta["raw"] = raw            # the mesh as built (write it with adcirc_io.write_fort14)
@@ -620,6 +644,7 @@ def channel_case(dt: float = 5.0, amp: float = 0.5, vortex: bool = False,
                  zero_gradient: int = 0, flux_settling: float = 0.0, river_eta: float = 0.05,
                  elev_series: float = 0.0, flux_series: float = 0.0, series_hours: float = 6.0,
                  barrier: float | None = None, barrier_type: int = 3,
+                 levee: float | None = None, levee_type: int = 4,
                  prep: MeshPrep | None = None, **kw) -> Case:
     """Tidal channel: 121x41 nodes, 20 m -> 5 m, M2 0.5 m, dt 5 s.  With
     `vortex`, a small Holland vortex (Rmax 8 km) crosses the channel.  With
@@ -640,9 +665,12 @@ def channel_case(dt: float = 5.0, amp: float = 0.5, vortex: bool = False,
     cover `series_hours` of simulated time.  With `barrier` [m above datum],
     the east end is an external barrier (IBTYPE `barrier_type`, 3, 13 or
     23) with that crest height and a discharge coefficient of 1: water
-    leaves over it once it stands 6 cm above the crest."""
-    from .meshgen import channel_mesh
-    raw = channel_mesh()
+    leaves over it once it stands 6 cm above the crest.  With `levee` [m
+    above datum], an internal barrier (IBTYPE `levee_type`, 4 or 24) with
+    that crest crosses the channel at x = 30 km and a dry polder at datum
+    level lies east of it (meshgen.levee_channel_mesh)."""
+    from .meshgen import channel_mesh, levee_channel_mesh
+    raw = channel_mesh() if levee is None else levee_channel_mesh(levee, levee_type)
     if river is not None or radiation or zero_gradient or barrier is not None:
         nx, ny = 121, 41
         nid = lambda i, j: i * ny + j

@@ -72,7 +72,8 @@ typedef struct {
  * NodalAttributes.  adc_gpu_bind copies them to the device; state arrays
  * are written back only by adc_sync_to_host. */
 typedef struct {
-  int np, ne, mnei, neta, nbfr, nvel, nvelme, pad_;
+  int np, ne, mnei, neta, nbfr, nvel, nvelme;
+  int nbou;                      /* NBOU; with nvell below, needed only for internal barriers */
   const double *x, *y, *dp;      /* (NP) */
   const int *nm;                 /* NM(NE,3) */
   const int *nneigh;             /* NNeigh(NP) */
@@ -107,6 +108,15 @@ typedef struct {
    * datum and the supercritical discharge coefficient per boundary entry;
    * NULL when the mesh has none */
   const double *barlanht, *barlancfsp;   /* (NVEL) */
+  /* internal barriers (IBTYPE 4/24, mesh.F:2140-2240, 2577-2584): the node
+   * across the barrier (IBCONN, 1-based), crest height and the subcritical
+   * and supercritical discharge coefficients per boundary entry, front face
+   * then back face of each barrier segment; NVELL(NBOU) as mesh.F leaves it
+   * (islands closed, barrier segments in pairs).  NULL without internal
+   * barriers. */
+  const int *ibconn;
+  const double *barinht, *barincfsb, *barincfsp;   /* (NVEL) */
+  const int *nvell;                                 /* (NBOU) */
 } adc_arrays_t;
 
 /* Per-step scalars TIMESTEP computes before the hot path (timestep.F:257-353). */
@@ -321,11 +331,20 @@ int adc_fort14_write(const char *path, const char *title, int np, int ne, const 
  * flux-boundary node (NVEL, in file order, 0 elsewhere), and
  * adc_fort14_write_barriers writes a mesh that has such segments. */
 int adc_fort14_barriers(const char *path, double *barlanht, double *barlancfsp);
+/* Internal barrier segments (IBTYPE 4/24) list pairs: the node, the node
+ * across the barrier and BARINHT, BARINCFSB, BARINCFSP (mesh.F:479-495); a
+ * pair counts twice in the file's NVEL.  adc_fort14_read's nbvv holds the
+ * front nodes (nvell counts pairs); adc_fort14_internal_barriers returns
+ * IBCONN (1-based) and the three values per nbvv entry, 0 elsewhere. */
+int adc_fort14_internal_barriers(const char *path, int *ibconn, double *barinht,
+                                 double *barincfsb, double *barincfsp);
 int adc_fort14_write_barriers(const char *path, const char *title, int np, int ne,
                               const double *x, const double *y, const double *dp, const int *nm,
                               int nope, const int *nvdll, const int *nbdv, int nbou,
                               const int *nvell, const int *ibtype, const int *nbvv,
-                              const double *barlanht, const double *barlancfsp);
+                              const double *barlanht, const double *barlancfsp,
+                              const int *ibconn, const double *barinht,
+                              const double *barincfsb, const double *barincfsp);
 
 /* fort.15 model parameters of a 2DDI run (READ_INPUT, read_input.F:
  * 949-4566), positional records in read_input's order plus the namelist

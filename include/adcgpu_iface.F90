@@ -24,7 +24,7 @@ module adcgpu_iface
    end type
 
    type, bind(C), public :: adc_arrays_t
-      integer(c_int) :: np, ne, mnei, neta, nbfr, nvel, nvelme, pad_
+      integer(c_int) :: np, ne, mnei, neta, nbfr, nvel, nvelme, nbou
       type(c_ptr) :: x, y, dp, nm, nneigh, neitab, fdxe, fdye, areas, csr_position
       type(c_ptr) :: tau0var, evm, fric, corif
       type(c_ptr) :: nbd, amig, per, face, ff, emo, efa, nbv, lbcodei, csii, siii, me2gw
@@ -35,6 +35,7 @@ module adcgpu_iface
       type(c_ptr) :: gwce_lv, mom_lv_x, mom_lv_y
       type(c_ptr) :: nelezng, zngif1, zngif2, zngif3, neitabele
       type(c_ptr) :: barlanht, barlancfsp
+      type(c_ptr) :: ibconn, barinht, barincfsb, barincfsp, nvell
    end type
 
    type, bind(C), public :: adc_step_t

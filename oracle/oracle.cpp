@@ -587,6 +587,8 @@ struct orc_model {
   int nfluxrbc = 0;   /* radiation (IBTYPE 30) entries, mesh.F:2045 */
   int nfluxgbc = 0;   /* zero normal velocity gradient (IBTYPE 40) entries, mesh.F:2072 */
   int nfluxb = 0;     /* external barrier (IBTYPE 3/13/23) entries, mesh.F:1913 */
+  int nfluxib = 0;    /* internal barrier (IBTYPE 4/24) entries, mesh.F:1919 */
+  std::vector<int> nib, nibcnt;   /* NIBNODECODE, NIBCNT (NP) */
   /* river radiation (IBTYPE 52): FluxSettlingIT, EtaDisc_Fill and
    * EtaDisc/ElevDisc at the boundary entries (timestep.F:183, 243-245) */
   int flux_settling_it = 0, etadisc_fill = 1;
@@ -660,7 +662,10 @@ orc_model *orc_model_create(const orc_params_t *p, orc_arrays_t *a) {
     if (lb == 30 || lb == 32) m->nfluxrbc = 1;   /* mesh.F:2044-2045, 2056-2058 */
     if (lb == 40 || lb == 41) m->nfluxgbc = 1;
     if (lb == 3 || lb == 13 || lb == 23) m->nfluxb = 1;
+    if (lb == 4 || lb == 24) m->nfluxib = 1;
   }
+  m->nib.assign(a->np, 0);
+  m->nibcnt.assign(a->np, 0);
   /* EtaDisc at river-radiation nodes from the cold-start ETA2, cstart.F:1186-1191 */
   m->elevdisc.assign(std::max(a->nvel, 1), 0.0);
   m->etadisc_b.assign(std::max(a->nvel, 1), 0.0);
@@ -902,6 +907,80 @@ static void orc_model_flux(orc_model *m, const orc_step_t *s) {
         m->qn2[I] = -s->rampintflux * a->barlancfsp[I] * RBARWL * std::sqrt(RBARWL * G);
       else
         m->qn2[I] = 0.0;
+    }
+  }
+  /* flow between the faces of internal barriers, timestep.F:1003-1026 and
+   * COMPUTE_INTERNAL_BOUNDARY_FLUX (weir_boundary.F90:1775-1942; default
+   * wet-edge form, no averaging, no time-varying crest) */
+  if (m->nfluxib) {
+    std::fill(m->nib.begin(), m->nib.end(), 0);
+    const double BARMIN = 0.04;
+    const int *NODECODE = a->nodecode;
+    auto NBV = [&](int I) { return a->nbv[I - 1] - 1; };        /* 1-based entry -> node */
+    auto IBCONN = [&](int I) { return a->ibconn[I - 1] - 1; };
+    int I = 0;
+    for (int K = 0; K < a->nbou; ++K) {
+      const int lb = a->lbcodei[I], NV = a->nvell[K];
+      if (lb != 4 && lb != 24) {
+        I = I + NV;
+        continue;
+      }
+      for (int J = 1; J <= NV * 2; ++J) {
+        I = I + 1;
+        const int NNBB1 = NBV(I), NNBB2 = IBCONN(I);
+        int NNBB1WN = 0, NNBB2WN = 0;
+        if (J == 1 || J == NV + 1) {
+          NNBB1WN = NNBB1WN + NODECODE[NBV(I + 1)];
+          NNBB2WN = NNBB2WN + NODECODE[IBCONN(I + 1)];
+        } else if (J == NV || J == NV * 2) {
+          NNBB1WN = NNBB1WN + NODECODE[NBV(I - 1)];
+          NNBB2WN = NNBB2WN + NODECODE[IBCONN(I - 1)];
+        } else {
+          NNBB1WN = NNBB1WN + NODECODE[NBV(I - 1)];
+          NNBB1WN = NNBB1WN + NODECODE[NBV(I + 1)];
+          NNBB2WN = NNBB2WN + NODECODE[IBCONN(I + 1)];
+          NNBB2WN = NNBB2WN + NODECODE[IBCONN(I - 1)];
+        }
+        const double RBARWL1 = a->eta2[NNBB1] - a->barinht[I - 1];
+        const double RBARWL2 = a->eta2[NNBB2] - a->barinht[I - 1];
+        const double RBARWL1F = 2.0 * RBARWL1 / 3.0, RBARWL2F = 2.0 * RBARWL2 / 3.0;
+        const double CFSB = a->barincfsb[I - 1], CFSP = a->barincfsp[I - 1];
+        double FLUX = 0.0;
+        if ((RBARWL1 < 0.0) && (RBARWL2 < 0.0)) {
+          FLUX = 0.0;
+        } else if (std::fabs(RBARWL1 - RBARWL2) < 0.01) {
+          FLUX = 0.0;
+        } else if ((RBARWL1 > RBARWL2) && (RBARWL1 > BARMIN)) {
+          if (RBARWL2 > RBARWL1F) {
+            if (NODECODE[NNBB1] == 0 || NNBB1WN == 0)
+              FLUX = 0.0;
+            else
+              FLUX = -s->rampintflux * RBARWL2 * CFSB * std::sqrt(2.0 * G * (RBARWL1 - RBARWL2));
+          } else {
+            if (NODECODE[NNBB1] == 0 || NNBB1WN == 0)
+              FLUX = 0.0;
+            else
+              FLUX = -s->rampintflux * CFSP * RBARWL1F * std::sqrt(RBARWL1F * G);
+          }
+        } else if ((RBARWL2 > RBARWL1) && (RBARWL2 > BARMIN)) {
+          if (RBARWL1 > RBARWL2F) {
+            if (NODECODE[NNBB2] == 0 || NNBB2WN == 0) {
+              FLUX = 0.0;
+            } else {
+              FLUX = s->rampintflux * RBARWL1 * CFSB * std::sqrt(2.0 * G * (RBARWL2 - RBARWL1));
+              m->nib[NNBB1] = 1;
+            }
+          } else {
+            if (NODECODE[NNBB2] == 0 || NNBB2WN == 0) {
+              FLUX = 0.0;
+            } else {
+              FLUX = s->rampintflux * CFSP * RBARWL2F * std::sqrt(RBARWL2F * G);
+              m->nib[NNBB1] = 1;
+            }
+          }
+        }
+        m->qn2[I - 1] = FLUX;
+      }
     }
   }
   /* zero normal velocity gradient entries, timestep.F:945-952 */
@@ -1147,7 +1226,7 @@ int orc_model_gwce(orc_model *m, const orc_step_t *s, orc_stepout_t *out) {
   }
   /* boundary flux integral, gwce.F:1737-1834 (LBCODEI <= 29 types,
    * radiation 30 and river radiation 52, with the H1 saved above) */
-  if (m->nfluxf || m->nfluxrbc || m->nfluxgbc || m->nfluxb) {
+  if (m->nfluxf || m->nfluxrbc || m->nfluxgbc || m->nfluxb || m->nfluxib) {
     const double DT2 = p.dt * 2.0;
     auto qforce = [&](int J, int NBDJ) {
       if (a->lbcodei[J] == 32) {   /* gwce.F:1792-1797 */
@@ -1297,10 +1376,27 @@ int orc_model_wetdry(orc_model *m, const orc_step_t *s, orc_stepout_t *out) {
       }
     }
   }
-  /* W2a/W2b: NIBNODECODE = 0, so NIBCNT = 0 and W2b never fires. */
+  /* W2a, wetdry.F:813-816: the reference adds each element's NIBNODECODE
+   * sum to its nodes' NIBCNT at the end of every W1 iteration; W1 does not
+   * touch NIBNODECODE, so the same sums are taken in a loop of their own */
+  std::vector<int> &NIBCNT = m->nibcnt;
+  std::fill(NIBCNT.begin(), NIBCNT.end(), 0);
+  if (m->nfluxib) {
+    for (int ie = 0; ie < ne; ++ie) {
+      int NM1 = NM(a, ie, 0), NM2 = NM(a, ie, 1), NM3 = NM(a, ie, 2);
+      const int NBNCTOT = m->nib[NM1] + m->nib[NM2] + m->nib[NM3];
+      NIBCNT[NM1] = NIBCNT[NM1] + NBNCTOT;
+      NIBCNT[NM2] = NIBCNT[NM2] + NBNCTOT;
+      NIBCNT[NM3] = NIBCNT[NM3] + NBNCTOT;
+    }
+    /* W2b, wetdry.F:1086-1090 */
+    for (int i = 0; i < np; ++i)
+      if (NIBCNT[i] > 0 && NNODECODE[i] == 0) NNODECODE[i] = 1;
+  }
   /* DE1, wetdry.F:1110-1162 */
   for (int ie = 0; ie < ne; ++ie) {
     int NM1 = NM(a, ie, 0), NM2 = NM(a, ie, 1), NM3 = NM(a, ie, 2);
+    if (NIBCNT[NM1] * NIBCNT[NM2] * NIBCNT[NM3] != 0) continue;   /* receiving barrier nodes */
     double ETAN1 = ETA2[NM1], ETAN2 = ETA2[NM2], ETAN3 = ETA2[NM3];
     double HTOTN1 = a->dp[NM1] + ETA2[NM1];
     double HTOTN2 = a->dp[NM2] + ETA2[NM2];

@@ -47,7 +47,7 @@ typedef struct {
 } orc_params_t;
 
 typedef struct {
-  int np, ne, mnei, neta, nbfr, nvel, nvelme, pad_;
+  int np, ne, mnei, neta, nbfr, nvel, nvelme, nbou;
   /* mesh.F */
   const double *x, *y, *dp;
   const int *nm;            /* NM(NE,3) */
@@ -80,6 +80,9 @@ typedef struct {
   const double *zngif1, *zngif2, *zngif3;
   const int *neitabele;     /* NeiTabEle(NP,MNEI), 1-based, 0 = none */
   const double *barlanht, *barlancfsp;   /* (NVEL) external barriers (IBTYPE 3/13/23) */
+  const int *ibconn;        /* (NVEL) internal barriers (IBTYPE 4/24): node across, 1-based */
+  const double *barinht, *barincfsb, *barincfsp;   /* (NVEL) */
+  const int *nvell;         /* NVELL(NBOU) after closure, barrier segments in pairs */
 } orc_arrays_t;
 
 /* Per-step scalars the TIMESTEP driver computes before the hot path. */

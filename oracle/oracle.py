@@ -48,12 +48,13 @@ _ARR = [
     ("gwce_lv", dp_), ("mom_lv_x", dp_), ("mom_lv_y", dp_),
     ("nelezng", ip_), ("zngif1", dp_), ("zngif2", dp_), ("zngif3", dp_), ("neitabele", ip_),
     ("barlanht", dp_), ("barlancfsp", dp_),
+    ("ibconn", ip_), ("barinht", dp_), ("barincfsb", dp_), ("barincfsp", dp_), ("nvell", ip_),
 ]
 
 
 class OrcArrays(C.Structure):
     _fields_ = [(n, C.c_int) for n in ("np", "ne", "mnei", "neta", "nbfr", "nvel", "nvelme",
-                                        "pad_")] + _ARR
+                                        "nbou")] + _ARR
 
 
 class OrcStep(C.Structure):
@@ -177,7 +178,7 @@ class OracleModel:
         for k, v in case.params.items():
             setattr(self.p, k, v)
         self.a = OrcArrays()
-        for k in ("np", "ne", "mnei", "neta", "nbfr", "nvel", "nvelme"):
+        for k in ("np", "ne", "mnei", "neta", "nbfr", "nvel", "nvelme", "nbou"):
             setattr(self.a, k, int(case.sizes[k]))
         for name, typ in _ARR:
             arr = case.arrays[name]

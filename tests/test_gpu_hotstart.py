@@ -98,3 +98,10 @@ def test_resume_zero_gradient(lib, tmp_path):
     """Zero-normal-gradient entries keep QN0 from the step before the dump."""
     from adcirc_b200 import model
     _resume_equal(lambda: model.channel_case(zero_gradient=True), 80, 0, tmp_path, use_run=True)
+
+
+def test_resume_levee(lib, tmp_path):
+    """An internal barrier between channel and polder: the run resumed while
+    the polder floods continues bit for bit."""
+    from adcirc_b200 import model
+    _resume_equal(lambda: model.channel_case(levee=0.0, amp=2.0), 800, 0, tmp_path, use_run=True)

@@ -336,3 +336,19 @@ def test_channel_external_barrier(lib, orc, btype, crest, nsteps):
     a = c0.arrays
     east = a["x"] > 59.9e3
     assert a["uu2"][east].mean() > 0.001   # water leaves over the barrier
+
+
+@pytest.mark.parametrize("ltype", [4, 24])
+def test_channel_internal_barrier(lib, orc, ltype):
+    """An internal barrier (IBTYPE 4/24) between the tidal channel and a dry
+    polder: the paired flow over the crest (weir_boundary.F90:1775-1942,
+    the wet-edge rules included), the receiving-node flags and the polder's
+    wetting through NIBCNT (wetdry.F:813-816, 1086-1090, 1114), against the
+    oracle over a graph-replayed run."""
+    from adcirc_b200 import model
+    c0, cg, io, ig = _pair(lambda **k: model.channel_case(levee=0.0, levee_type=ltype, amp=2.0, **k),
+                           1000, use_run=True)
+    _check(c0, cg, io, ig)
+    a = c0.arrays
+    east = a["x"] > 30.0e3 + 1.0
+    assert a["nodecode"][east].sum() > 100   # the polder has begun to flood

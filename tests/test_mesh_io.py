@@ -70,9 +70,11 @@ def test_fort14_labels_and_fortran_numbers(lib, tmp_path):
     assert m.land_segments[0][0] == 0 and np.array_equal(m.land_segments[0][1], [1, 2, 3])
 
 
-def test_fort14_barrier_unsupported(lib, tmp_path):
+def test_fort14_barrier_with_pipes_unsupported(lib, tmp_path):
+    """Internal barriers with cross-barrier pipes (IBTYPE 5/25) are refused."""
     from adcirc_b200 import _lib, adcirc_io
-    text = "t\n1 3\n1 0 0 1\n2 1 0 1\n3 0 1 1\n1 3 1 2 3\n0\n0\n1\n2\n2 4\n1 2 0.5 1.0 1.0\n3 1 0.5 1.0 1.0\n"
+    text = ("t\n1 3\n1 0 0 1\n2 1 0 1\n3 0 1 1\n1 3 1 2 3\n0\n0\n1\n4\n2 5\n"
+            "1 2 0.5 1.0 1.0 0.1 1.0 0.5\n3 1 0.5 1.0 1.0 0.1 1.0 0.5\n")
     p = tmp_path / "fort.14"
     p.write_text(text)
     dims = np.zeros(6, np.int32)
@@ -103,6 +105,38 @@ def test_fort14_external_barrier(lib, tmp_path):
     bad.write_text(text.replace("2 0.6D0 0.9", "2"))
     with pytest.raises(OSError, match="external barrier"):
         adcirc_io.read_fort14(bad)
+
+
+def test_fort14_internal_barrier(lib, tmp_path):
+    """IBTYPE 4/24 node lines hold the pair, the crest and both discharge
+    coefficients (read14, mesh.F:479-495); the pairs count twice in NVEL,
+    and a mesh written and read back builds the same bound arrays."""
+    from adcirc_b200 import adcirc_io, meshgen, model
+    raw = meshgen.levee_channel_mesh(0.25, 24, cfsb=0.9, cfsp=0.8)
+    p = tmp_path / "fort.14"
+    adcirc_io.write_fort14(raw, p)
+    text = p.read_text().splitlines()
+    nbou_line = len(text) - 2 - sum(len(s) + 1 for _, s in raw.land_segments)
+    assert int(text[nbou_line].split()[0]) == 2                   # NBOU
+    assert int(text[nbou_line + 1].split()[0]) == 281 + 2 * 39   # NVEL
+    back = adcirc_io.read_fort14(p)
+    assert [t for t, _ in back.land_segments] == [0, 24]
+    b0, b1 = raw.barriers[1], back.barriers[1]
+    for u, v in zip(b0, b1):
+        assert np.array_equal(np.asarray(u), np.asarray(v))
+    sched = model.Schedule(dt=5.0)
+    tides = [(1e-4, 0.0, 1.0, np.full(raw.open_nodes.size, 0.5), np.zeros(raw.open_nodes.size))]
+    a = model.build_case(raw, model.default_params(5.0), sched, tides).arrays
+    b = model.build_case(back, model.default_params(5.0), sched, tides).arrays
+    for k in a:
+        assert np.array_equal(a[k], b[k]), k
+    assert np.array_equal(a["nvell"], [281, 39])
+    lbc = a["lbcodei"]
+    assert (lbc == 24).sum() == 78
+    # front face pairs with the back face, the back face runs backwards
+    front = np.nonzero(lbc == 24)[0][:39]
+    assert np.array_equal(a["ibconn"][front] - 1, b1[3])
+    assert np.array_equal(a["nbv"][front[-1] + 1:front[-1] + 40] - 1, b1[3][::-1])
 
 
 def test_fort63_64_format(lib, tmp_path):

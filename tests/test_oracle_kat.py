@@ -153,3 +153,30 @@ def test_external_barrier_outflow_follows_the_weir_formula(orc):
         dry_steps += int((R <= 0.04).all())
     om.close()
     assert flowing > 100 and dry_steps > 100
+
+
+def test_levee_overtopping_floods_the_polder(orc):
+    """An internal barrier (IBTYPE 4) with its crest at datum between the
+    tidal channel and a dry polder: once the tide stands BARMIN over the
+    crest, water crosses the barrier (weir_boundary.F90:1775-1942) and the
+    receiving nodes wet the polder through NIBCNT (wetdry.F:813-816,
+    1086-1090); the polder wets from the barrier outward.  With a crest
+    10 m high nothing crosses."""
+    from adcirc_b200 import model
+    wet = {}
+    for crest in (0.0, 10.0):
+        case = model.channel_case(levee=crest, amp=2.0)
+        a = case.arrays
+        east = a["x"] > 30.0e3 + 1.0
+        om = orc.OracleModel(case)
+        first = None
+        for k in range(10):
+            om.run(1 + 100 * k, 100)
+            if first is None and a["nodecode"][east].any():
+                first = a["x"][east & (a["nodecode"] == 1)].max()
+        om.close()
+        wet[crest] = int(a["nodecode"][east].sum())
+        if crest == 0.0:
+            # within two element columns (0.5 km each) of the barrier
+            assert first is not None and first <= 31.0e3 + 1.0
+    assert wet[0.0] > 100 and wet[10.0] == 0
