@@ -55,6 +55,7 @@ ARRAY_FIELDS = [
     ("nelezng", ip_), ("zngif1", dp_), ("zngif2", dp_), ("zngif3", dp_), ("neitabele", ip_),
     ("barlanht", dp_), ("barlancfsp", dp_),
     ("ibconn", ip_), ("barinht", dp_), ("barincfsb", dp_), ("barincfsp", dp_), ("nvell", ip_),
+    ("pipeht", dp_), ("pipecoef", dp_), ("pipediam", dp_),
 ]
 
 
@@ -195,8 +196,8 @@ def load():
                                        C.c_int, ip_, ip_, C.c_int, ip_, ip_, ip_]),
         "adc_fort14_write_barriers": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int, C.c_int, dp_, dp_,
                                                 dp_, ip_, C.c_int, ip_, ip_, C.c_int, ip_, ip_, ip_,
-                                                dp_, dp_, ip_, dp_, dp_, dp_]),
-        "adc_fort14_internal_barriers": (C.c_int, [C.c_char_p, ip_, dp_, dp_, dp_]),
+                                                dp_, dp_, ip_, dp_, dp_, dp_, dp_, dp_, dp_]),
+        "adc_fort14_internal_barriers": (C.c_int, [C.c_char_p, ip_, dp_, dp_, dp_, dp_, dp_, dp_]),
         "adc_fort14_barriers": (C.c_int, [C.c_char_p, dp_, dp_]),
         "adc_fort6x_header": (C.c_int, [C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p, C.c_int,
                                         C.c_int, C.c_double, C.c_int, C.c_int]),

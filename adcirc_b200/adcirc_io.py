@@ -45,19 +45,22 @@ def read_fort14(path) -> RawMesh:
     if any(int(t) in (3, 13, 23) for t in ibtype[:nbou]):
         _check(lib.adc_fort14_barriers(p, ptr(bht, dp_), ptr(bcf, dp_)), "adc_fort14_barriers")
     ibc = np.zeros(max(nvel, 1), np.int32)
-    iht, icb, icp = (np.zeros(max(nvel, 1)) for _ in range(3))
-    if any(int(t) in (4, 24) for t in ibtype[:nbou]):
+    iht, icb, icp, pht, pcf, pdm = (np.zeros(max(nvel, 1)) for _ in range(6))
+    if any(int(t) in (4, 24, 5, 25) for t in ibtype[:nbou]):
         _check(lib.adc_fort14_internal_barriers(p, ptr(ibc, ip_), ptr(iht, dp_), ptr(icb, dp_),
-                                                ptr(icp, dp_)), "adc_fort14_internal_barriers")
+                                                ptr(icp, dp_), ptr(pht, dp_), ptr(pcf, dp_),
+                                                ptr(pdm, dp_)), "adc_fort14_internal_barriers")
     segs, barriers, q = [], {}, 0
     for k in range(nbou):
         n = int(nvell[k])
         segs.append((int(ibtype[k]), nbvv[q:q + n].astype(np.int64) - 1))
         if int(ibtype[k]) in (3, 13, 23):
             barriers[k] = (bht[q:q + n].copy(), bcf[q:q + n].copy())
-        if int(ibtype[k]) in (4, 24):
+        if int(ibtype[k]) in (4, 24, 5, 25):
             barriers[k] = (iht[q:q + n].copy(), icb[q:q + n].copy(), icp[q:q + n].copy(),
                            ibc[q:q + n].astype(np.int64) - 1)
+        if int(ibtype[k]) in (5, 25):
+            barriers[k] += (pht[q:q + n].copy(), pcf[q:q + n].copy(), pdm[q:q + n].copy())
         q += n
     name = title.value.decode(errors="replace").strip() or os.path.basename(os.fsdecode(path))
     meta = {"lx": float(x.max() - x.min()), "ly": float(y.max() - y.min()),
@@ -82,15 +85,17 @@ def write_fort14(raw: RawMesh, path, title: str | None = None) -> None:
     nbvv = np.ascontiguousarray(nbvv, np.int32)
     bht, bcf = np.zeros(max(nbvv.size, 1)), np.zeros(max(nbvv.size, 1))
     ibc = np.zeros(max(nbvv.size, 1), np.int32)
-    iht, icb, icp = (np.zeros(max(nbvv.size, 1)) for _ in range(3))
+    iht, icb, icp, pht, pcf, pdm = (np.zeros(max(nbvv.size, 1)) for _ in range(6))
     q = 0
     for k, (t, nodes) in enumerate(raw.land_segments):
         n = len(nodes)
         if t in (3, 13, 23):
             bht[q:q + n], bcf[q:q + n] = raw.barriers[k]
-        if t in (4, 24):
-            iht[q:q + n], icb[q:q + n], icp[q:q + n], across = raw.barriers[k]
+        if t in (4, 24, 5, 25):
+            iht[q:q + n], icb[q:q + n], icp[q:q + n], across = raw.barriers[k][:4]
             ibc[q:q + n] = np.asarray(across) + 1
+        if t in (5, 25):
+            pht[q:q + n], pcf[q:q + n], pdm[q:q + n] = raw.barriers[k][4:7]
         q += n
     _check(lib.adc_fort14_write_barriers(os.fsencode(path), (title or raw.name).encode()[:80],
                                          int(x.size), int(nm.shape[0]), ptr(x, dp_), ptr(y, dp_),
@@ -98,7 +103,8 @@ def write_fort14(raw: RawMesh, path, title: str | None = None) -> None:
                                          ptr(nbdv, ip_), len(raw.land_segments), ptr(nvell, ip_),
                                          ptr(ibtype, ip_), ptr(nbvv, ip_), ptr(bht, dp_),
                                          ptr(bcf, dp_), ptr(ibc, ip_), ptr(iht, dp_),
-                                         ptr(icb, dp_), ptr(icp, dp_)), "adc_fort14_write_barriers")
+                                         ptr(icb, dp_), ptr(icp, dp_), ptr(pht, dp_), ptr(pcf, dp_),
+                                         ptr(pdm, dp_)), "adc_fort14_write_barriers")
 
 
 class Fort6x:

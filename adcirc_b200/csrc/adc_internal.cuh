@@ -136,7 +136,9 @@ struct adc_ctx {
   int nfluxgbc;          // zero-normal-gradient (IBTYPE 40) entries present
   int nfluxb;            // external barrier (IBTYPE 3/13/23) entries present
   double *barht, *barcf; // BARLANHT, BARLANCFSP per boundary entry
-  int nfluxib;           // internal barrier (IBTYPE 4/24) entries present
+  int nfluxib;           // internal barrier (IBTYPE 4/24/5/25) entries present
+  int nfluxibp;          // barriers with cross-barrier pipes (IBTYPE 5/25) present
+  double *pipe;          // PIPEHT, PIPECOEF, PIPEDIAM per entry (3 x NVEL)
   int *ibconn;           // per boundary entry: the node across the barrier (0-based)
   int *ibkind;           // per entry: 0 first, 1 last, 2 inner node of its face; -1 none
   double *binht, *bincfsb, *bincfsp;   // BARINHT, BARINCFSB, BARINCFSP per entry

@@ -35,7 +35,10 @@
 // supercritical weir flow from the higher side once it stands BARMIN over
 // the crest, none while the source node or all its neighbours along the
 // barrier are dry; a receiving node is flagged in NIBNODECODE, which the
-// wet/dry step uses (wetdry.F:813-816, 1086-1090, 1114).
+// wet/dry step uses (wetdry.F:813-816, 1086-1090, 1114).  Barriers with
+// pipes (IBTYPE 5/25) add the free or submerged discharge through the pipe
+// under the crown (COMPUTE_CROSS_BARRIER_PIPE_FLUX, weir_boundary.F90:
+// 2469-2579, timestep.F:1034-1044).
 // It also holds the non-periodic boundary series: fort.20 fluxes in place of
 // the periodic constituents (NFFR <= 0, timestep.F:882-903) and fort.19
 // elevations added to the periodic boundary elevation in k_eta_bc
@@ -117,6 +120,35 @@ __device__ double internal_barrier_flux(const adc_ctx &c, int I, double ramp) {
   return flux;
 }
 
+// COMPUTE_CROSS_BARRIER_PIPE_FLUX (weir_boundary.F90:2469-2579); the
+// reference's **0.5 as square roots and PIPEDIAM**2 as a product.
+__device__ double pipe_flux(const adc_ctx &c, int I, double ramp) {
+  const int n1 = c.bnv[I], n2 = c.ibconn[I];
+  const double *pp = c.pipe;
+  const double ht = pp[I], coef = pp[c.nvel + I], diam = pp[2 * c.nvel + I];
+  const double G = c.p.g, BARMIN = 0.04, PI = 3.141592653589793;
+  const double R1 = c.eta2[n1] - ht, R2 = c.eta2[n2] - ht;
+  if ((R1 < 0.0) && (R2 < 0.0)) return 0.0;
+  if (fabs(R1 - R2) < BARMIN) return 0.0;
+  double flux = 0.0;
+  if ((R1 > R2) && (R1 > BARMIN)) {   // outward
+    if (R2 <= 0.0) {
+      flux = c.nodecode[n1] == 0 ? 0.0
+                                 : -ramp * 0.25 * PI * (diam * diam) * sqrt(2.0 * G * R1 / (1.0 + coef));
+    } else {
+      return c.nodecode[n1] == 0 ? 0.0
+                                 : -ramp * 0.25 * PI * (diam * diam) * sqrt(2.0 * G * (R1 - R2) / coef);
+    }
+  }
+  if ((R2 > R1) && (R2 > BARMIN)) {   // inward
+    if (c.nodecode[n2] == 0) return 0.0;
+    if (R1 <= 0.0) flux = ramp * 0.25 * PI * (diam * diam) * sqrt(2.0 * G * R2 / (1.0 + coef));
+    else flux = ramp * 0.25 * PI * (diam * diam) * sqrt(2.0 * G * (R2 - R1) / coef);
+    c.nib[n1] = 1;
+  }
+  return flux;
+}
+
 __global__ void k_flux_forcing(adc_ctx c, const adc_step_t *steps, const Flags *flags) {
   griddep_wait();
   const int I = blockIdx.x * blockDim.x + threadIdx.x;
@@ -156,7 +188,8 @@ __global__ void k_flux_forcing(adc_ctx c, const adc_step_t *steps, const Flags *
     const double RBARWL = 2.0 * (c.eta2[c.bnv[I]] - c.barht[I]) / 3.0;
     q = RBARWL > 0.04 ? -st.rampintflux * c.barcf[I] * RBARWL * sqrt(RBARWL * c.p.g) : 0.0;
   }
-  if (lb == 4 || lb == 24) q = internal_barrier_flux(c, I, st.rampintflux);
+  if (lb == 4 || lb == 24 || lb == 5 || lb == 25) q = internal_barrier_flux(c, I, st.rampintflux);
+  if (lb == 5 || lb == 25) q = q + pipe_flux(c, I, st.rampintflux);   // timestep.F:1034-1044
   qn2[I] = q;
   en2[I] = el;
   if (lb == 52) {
@@ -261,10 +294,12 @@ int flux_tables(adc_ctx *c, const adc_arrays_t *a) {
   c->nfluxgbc = 0;
   c->nfluxb = 0;
   c->nfluxib = 0;
+  c->nfluxibp = 0;
   for (int I = 0; I < nv; ++I) {
     const int lb = a->lbcodei[I];
     if (lb == 3 || lb == 13 || lb == 23) c->nfluxb = 1;
-    if (lb == 4 || lb == 24) c->nfluxib = 1;
+    if (lb == 4 || lb == 24 || lb == 5 || lb == 25) c->nfluxib = 1;
+    if (lb == 5 || lb == 25) c->nfluxibp = 1;
     if (lb == 2 || lb == 12 || lb == 22 || lb == 32 || lb == 52) c->nfluxf = 1;
     if (lb == 30 || lb == 32) c->nfluxrbc = 1;
     if (lb == 40 || lb == 41) c->nfluxgbc = 1;
@@ -335,7 +370,7 @@ int flux_tables(adc_ctx *c, const adc_arrays_t *a) {
         return ADC_ERR_MESH;
       }
       const int lb = a->lbcodei[I], n = a->nvell[K];
-      if (lb == 4 || lb == 24) {
+      if (lb == 4 || lb == 24 || lb == 5 || lb == 25) {
         if (I + 2 * n > nv || n < 2) {
           set_error("internal barrier segment %d does not fit NVEL", K + 1);
           return ADC_ERR_MESH;
@@ -363,6 +398,17 @@ int flux_tables(adc_ctx *c, const adc_arrays_t *a) {
   for (double **d : {&c->binht, &c->bincfsb, &c->bincfsp}) {
     ADC_CUDA(cudaMalloc((void **)d, nva * sizeof(double)));
     ADC_CUDA(cudaMemset(*d, 0, nva * sizeof(double)));
+  }
+  ADC_CUDA(cudaMalloc((void **)&c->pipe, 3 * nva * sizeof(double)));
+  ADC_CUDA(cudaMemset(c->pipe, 0, 3 * nva * sizeof(double)));
+  if (c->nfluxibp) {
+    if (!a->pipeht || !a->pipecoef || !a->pipediam) {
+      set_error("the mesh has barrier pipes (IBTYPE 5/25) but no PIPEHT/PIPECOEF/PIPEDIAM");
+      return ADC_ERR_MESH;
+    }
+    ADC_CUDA(cudaMemcpy(c->pipe, a->pipeht, nv * sizeof(double), cudaMemcpyHostToDevice));
+    ADC_CUDA(cudaMemcpy(c->pipe + nva, a->pipecoef, nv * sizeof(double), cudaMemcpyHostToDevice));
+    ADC_CUDA(cudaMemcpy(c->pipe + 2 * nva, a->pipediam, nv * sizeof(double), cudaMemcpyHostToDevice));
   }
   if (c->nfluxib) {
     ADC_CUDA(cudaMemcpy(c->binht, a->barinht, nv * sizeof(double), cudaMemcpyHostToDevice));

@@ -11,9 +11,10 @@
 // 41, 52, 102, 112, 122, 152; external barriers 3, 13, 23 with the crest
 // height BARLANHT and discharge coefficient BARLANCFSP after the node,
 // mesh.F:460-473; internal barriers 4, 24 with the paired node IBCONN,
-// BARINHT, BARINCFSB and BARINCFSP, mesh.F:479-495, whose pairs count twice
-// in NVEL, mesh.F:260-265) are returned; barriers with pipes (5, 25) and
-// periodic segments (94) return ADC_ERR_UNSUPPORTED.
+// BARINHT, BARINCFSB and BARINCFSP, mesh.F:479-495, and 5, 25 with the
+// pipe's PIPEHT, PIPECOEF and PIPEDIAM after them, mesh.F:506-524; their
+// pairs count twice in NVEL, mesh.F:260-268) are returned; periodic
+// segments (94) return ADC_ERR_UNSUPPORTED.
 #include <cerrno>
 #include <cmath>
 #include <cstdarg>
@@ -105,7 +106,7 @@ bool simple_flux_type(long long t) {
   switch (t) {
     case 0: case 1: case 2: case 10: case 11: case 12: case 20: case 21: case 22: case 30:
     case 32: case 40: case 41: case 52: case 102: case 112: case 122: case 152:
-    case 3: case 13: case 23: case 4: case 24:
+    case 3: case 13: case 23: case 4: case 24: case 5: case 25:
       return true;
     default:
       return false;
@@ -120,10 +121,12 @@ struct Mesh14 {
   std::vector<double> barlanht, barlancfsp;   // per nbvv entry, 0 off external barriers
   std::vector<int> ibconn;                     // per nbvv entry, 0 off internal barriers
   std::vector<double> barinht, barincfsb, barincfsp;
+  std::vector<double> pipeht, pipecoef, pipediam;
 };
 
 bool external_barrier(long long t) { return t == 3 || t == 13 || t == 23; }
-bool internal_barrier(long long t) { return t == 4 || t == 24; }
+bool pipe_barrier(long long t) { return t == 5 || t == 25; }
+bool internal_barrier(long long t) { return t == 4 || t == 24 || pipe_barrier(t); }
 
 int parse14(const char *path, Mesh14 &m) {
   Reader r;
@@ -200,7 +203,7 @@ int parse14(const char *path, Mesh14 &m) {
       long long lab;
       int id;
       if (!r.inum(lab) || !find(lab, id)) return bad("flux boundary node");
-      double ht = 0.0, cf = 0.0, iht = 0.0, icb = 0.0, icp = 0.0;
+      double ht = 0.0, cf = 0.0, iht = 0.0, icb = 0.0, icp = 0.0, pht = 0.0, pcf = 0.0, pdm = 0.0;
       int across = 0;
       if (external_barrier(t) && (!r.num(ht) || !r.num(cf)))
         return bad("external barrier node (NBVV BARLANHT BARLANCFSP)");
@@ -208,6 +211,8 @@ int parse14(const char *path, Mesh14 &m) {
         long long lab2;
         if (!r.inum(lab2) || !find(lab2, across) || !r.num(iht) || !r.num(icb) || !r.num(icp))
           return bad("internal barrier node (NBVV IBCONN BARINHT BARINCFSB BARINCFSP)");
+        if (pipe_barrier(t) && (!r.num(pht) || !r.num(pcf) || !r.num(pdm)))
+          return bad("barrier pipe (PIPEHT PIPECOEF PIPEDIAM)");
       }
       r.end_line();
       m.nbvv.push_back(id);
@@ -217,6 +222,9 @@ int parse14(const char *path, Mesh14 &m) {
       m.barinht.push_back(iht);
       m.barincfsb.push_back(icb);
       m.barincfsp.push_back(icp);
+      m.pipeht.push_back(pht);
+      m.pipecoef.push_back(pcf);
+      m.pipediam.push_back(pdm);
       nvel_count += internal_barrier(t) ? 2 : 1;
     }
   }
@@ -318,7 +326,8 @@ extern "C" int adc_fort14_barriers(const char *path, double *barlanht, double *b
 }
 
 extern "C" int adc_fort14_internal_barriers(const char *path, int *ibconn, double *barinht,
-                                            double *barincfsb, double *barincfsp) {
+                                            double *barincfsb, double *barincfsp, double *pipeht,
+                                            double *pipecoef, double *pipediam) {
   if (!path || !ibconn || !barinht || !barincfsb || !barincfsp) {
     set_error("adc_fort14_internal_barriers: null argument");
     return ADC_ERR_ARG;
@@ -332,6 +341,9 @@ extern "C" int adc_fort14_internal_barriers(const char *path, int *ibconn, doubl
     std::memcpy(barinht, m.barinht.data(), n * sizeof(double));
     std::memcpy(barincfsb, m.barincfsb.data(), n * sizeof(double));
     std::memcpy(barincfsp, m.barincfsp.data(), n * sizeof(double));
+    if (pipeht) std::memcpy(pipeht, m.pipeht.data(), n * sizeof(double));
+    if (pipecoef) std::memcpy(pipecoef, m.pipecoef.data(), n * sizeof(double));
+    if (pipediam) std::memcpy(pipediam, m.pipediam.data(), n * sizeof(double));
   }
   return ADC_OK;
 }
@@ -342,7 +354,7 @@ extern "C" int adc_fort14_write(const char *path, const char *title, int np, int
                                 const int *ibtype, const int *nbvv) {
   return adc_fort14_write_barriers(path, title, np, ne, x, y, dp, nm, nope, nvdll, nbdv, nbou,
                                    nvell, ibtype, nbvv, nullptr, nullptr, nullptr, nullptr, nullptr,
-                                   nullptr);
+                                   nullptr, nullptr, nullptr, nullptr);
 }
 
 extern "C" int adc_fort14_write_barriers(const char *path, const char *title, int np, int ne,
@@ -352,7 +364,9 @@ extern "C" int adc_fort14_write_barriers(const char *path, const char *title, in
                                          const int *ibtype, const int *nbvv,
                                          const double *barlanht, const double *barlancfsp,
                                          const int *ibconn, const double *barinht,
-                                         const double *barincfsb, const double *barincfsp) {
+                                         const double *barincfsb, const double *barincfsp,
+                                         const double *pipeht, const double *pipecoef,
+                                         const double *pipediam) {
   if (!path || !x || !y || !dp || !nm || np < 3 || ne < 1 || nope < 0 || nbou < 0) {
     set_error("adc_fort14_write: bad arguments");
     return ADC_ERR_ARG;
@@ -380,8 +394,10 @@ extern "C" int adc_fort14_write_barriers(const char *path, const char *title, in
   for (int k = 0; k < nbou; ++k) {
     std::fprintf(f, "%d %d\n", nvell[k], ibtype[k]);
     const bool bar = external_barrier(ibtype[k]), ibar = internal_barrier(ibtype[k]);
+    const bool pipe = pipe_barrier(ibtype[k]);
     if ((bar && (!barlanht || !barlancfsp)) ||
-        (ibar && (!ibconn || !barinht || !barincfsb || !barincfsp))) {
+        (ibar && (!ibconn || !barinht || !barincfsb || !barincfsp)) ||
+        (pipe && (!pipeht || !pipecoef || !pipediam))) {
       std::fclose(f);
       set_error("adc_fort14_write: segment %d is a barrier; its pairs, heights and "
                 "coefficients are required", k + 1);
@@ -390,6 +406,9 @@ extern "C" int adc_fort14_write_barriers(const char *path, const char *title, in
     for (int j = 0; j < nvell[k]; ++j, ++q) {
       if (bar)
         std::fprintf(f, "%d %.17g %.17g\n", nbvv[q], barlanht[q], barlancfsp[q]);
+      else if (pipe)
+        std::fprintf(f, "%d %d %.17g %.17g %.17g %.17g %.17g %.17g\n", nbvv[q], ibconn[q], barinht[q],
+                     barincfsb[q], barincfsp[q], pipeht[q], pipecoef[q], pipediam[q]);
       else if (ibar)
         std::fprintf(f, "%d %d %.17g %.17g %.17g\n", nbvv[q], ibconn[q], barinht[q], barincfsb[q],
                      barincfsp[q]);

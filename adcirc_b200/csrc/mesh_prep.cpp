@@ -172,7 +172,7 @@ int adc_mesh_csr_positions(int np, int ne, int mnei, const int *nm, const int *n
  * islands (IBTYPE 1, 11, 21), specified-flow (2, 12, 22), radiation (30),
  * coupled flux/radiation (32), zero-normal-gradient (40, 41),
  * river-radiation (52) and external barrier (3, 13, 23) segments, and the
- * faces of internal barriers (4, 24): mesh.F processes a barrier segment as
+ * faces of internal barriers (4, 24; 5, 25 with pipes): mesh.F processes a barrier segment as
  * its front face and then its back face, each an unclosed segment
  * (mesh.F:2158-2192), so the caller lists the two faces as two segments of
  * the barrier's type, the back face in the reversed order mesh.F gives it,
@@ -198,7 +198,7 @@ int adc_boundary_setup(int np, const double *x, const double *y, int nbou,
     bool island = (t == 1 || t == 11 || t == 21);
     bool mainland = (t == 0 || t == 10 || t == 20);
     bool flux = specified_flow(t);   /* external boundaries with normal flow or radiation */
-    bool barrier_face = (t == 4 || t == 24);
+    bool barrier_face = (t == 4 || t == 24 || t == 5 || t == 25);
     if (!island && !mainland && !flux && !barrier_face) return ADC_ERR_ARG;
     std::vector<int> nbvv;
     int nvell = seg_ptr[k + 1] - seg_ptr[k];

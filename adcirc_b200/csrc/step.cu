@@ -463,7 +463,7 @@ static void free_ctx(adc_ctx *c) {
       (void **)&c->qforce, (void **)&c->fconst, (void **)&c->fqn, (void **)&c->bnv, (void **)&c->blbc,
       (void **)&c->bbl, (void **)&c->bcsii, (void **)&c->bsiii, (void **)&c->barht, (void **)&c->barcf, (void **)&c->ibconn,
       (void **)&c->ibkind, (void **)&c->binht, (void **)&c->bincfsb, (void **)&c->bincfsp,
-      (void **)&c->nib, (void **)&c->nibcnt, (void **)&c->elevdisc, (void **)&c->etadisc_b, (void **)&c->en, (void **)&c->zng_node, (void **)&c->zng_ele, (void **)&c->zng_f, (void **)&c->fx_node, (void **)&c->fx_ptr, (void **)&c->fx_ent, (void **)&c->eta1, (void **)&c->eta2,
+      (void **)&c->nib, (void **)&c->nibcnt, (void **)&c->pipe, (void **)&c->elevdisc, (void **)&c->etadisc_b, (void **)&c->en, (void **)&c->zng_node, (void **)&c->zng_ele, (void **)&c->zng_f, (void **)&c->fx_node, (void **)&c->fx_ptr, (void **)&c->fx_ent, (void **)&c->eta1, (void **)&c->eta2,
       (void **)&c->etas, (void **)&c->uu1, (void **)&c->vv1, (void **)&c->uu2, (void **)&c->vv2,
       (void **)&c->qx1, (void **)&c->qy1, (void **)&c->qx2, (void **)&c->qy2, (void **)&c->h1,
       (void **)&c->h2, (void **)&c->tk, (void **)&c->tkm, (void **)&c->totalarea,

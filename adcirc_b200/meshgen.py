@@ -25,8 +25,10 @@ class RawMesh:
     open_nodes: np.ndarray  # elevation boundary node ids (0-based), in order
     land_segments: list    # list of (ibtype, node id array (0-based))
     meta: dict
-    # external barrier segments (IBTYPE 3/13/23): segment index ->
-    # (BARLANHT crest heights [m above datum], BARLANCFSP coefficients), per node
+    # barrier segments, by segment index, per node: IBTYPE 3/13/23 (BARLANHT
+    # crest heights [m above datum], BARLANCFSP); 4/24 (BARINHT, BARINCFSB,
+    # BARINCFSP, the paired back-face nodes, 0-based); 5/25 those and
+    # (PIPEHT, PIPECOEF, PIPEDIAM)
     barriers: dict = dataclasses.field(default_factory=dict)
 
 
@@ -67,7 +69,8 @@ def channel_mesh(nx: int = 121, ny: int = 41, lx: float = 60e3, ly: float = 20e3
 
 
 def levee_channel_mesh(crest: float, btype: int = 4, ib: int = 60, polder_depth: float = 0.0,
-                       cfsb: float = 1.0, cfsp: float = 1.0, gap: float = 50.0, **kw) -> RawMesh:
+                       cfsb: float = 1.0, cfsp: float = 1.0, gap: float = 50.0, pipe=None,
+                       **kw) -> RawMesh:
     """The channel with an internal barrier (IBTYPE `btype`, 4 or 24) along
     the column x = ib * dx: the column's inner nodes (all but the wall
     corners) are duplicated, the elements east of the column use the copies,
@@ -76,7 +79,8 @@ def levee_channel_mesh(crest: float, btype: int = 4, ib: int = 60, polder_depth:
     discharge coefficients `cfsb` (subcritical) and `cfsp` (supercritical).
     East of the barrier the bed is flat at depth `polder_depth` (0: the
     datum, so the polder starts dry); the outer walls are one land segment
-    as in `channel_mesh`."""
+    as in `channel_mesh`.  For btype 5/25, `pipe` = (PIPEHT, PIPECOEF,
+    PIPEDIAM) is the same pipe under every pair."""
     m = channel_mesh(**kw)
     nx, ny = m.meta["nx"], m.meta["ny"]
     nid = lambda i, j: i * ny + j
@@ -100,7 +104,10 @@ def levee_channel_mesh(crest: float, btype: int = 4, ib: int = 60, polder_depth:
     east_el = cx > m.x[nid(ib, 0)]
     nm[east_el] = remap[nm[east_el]]
     n = front.size
-    barriers = {1: (np.full(n, float(crest)), np.full(n, float(cfsb)), np.full(n, float(cfsp)), back)}
+    bar = (np.full(n, float(crest)), np.full(n, float(cfsb)), np.full(n, float(cfsp)), back)
+    if btype in (5, 25):
+        bar += tuple(np.full(n, float(v)) for v in pipe)
+    barriers = {1: bar}
     meta = dict(m.meta, barrier_column=ib)
     return RawMesh("levee_channel", x, y, dp, nm, m.open_nodes,
                    [m.land_segments[0], (int(btype), front)], meta, barriers)

@@ -351,7 +351,7 @@ def build_case(raw, params: dict, schedule: Schedule, tides, cf: float = 0.0025,
     # its back face, reversed (mesh.F:2158-2192)
     faces = []
     for k, (t, s) in enumerate(raw.land_segments):
-        if t in (4, 24):
+        if t in (4, 24, 5, 25):
             back = np.asarray(raw.barriers[k][3], np.int64)
             faces += [(t, np.asarray(s, np.int64)), (t, back[::-1])]
         else:
@@ -404,6 +404,7 @@ def build_case(raw, params: dict, schedule: Schedule, tides, cf: float = 0.0025,
     barlanht, barlancfsp = np.zeros(max(nv, 1)), np.zeros(max(nv, 1))
     ibconn = np.zeros(max(nv, 1), np.int32)
     barin = [np.zeros(max(nv, 1)) for _ in range(3)]
+    pipes = [np.zeros(max(nv, 1)) for _ in range(3)]
     nvell = np.zeros(max(len(raw.land_segments), 1), np.int32)
     j = 0
     for k, (t, nodes) in enumerate(raw.land_segments):
@@ -413,12 +414,16 @@ def build_case(raw, params: dict, schedule: Schedule, tides, cf: float = 0.0025,
         nvell[k] = n
         if t in (3, 13, 23):
             barlanht[j:j + n], barlancfsp[j:j + n] = raw.barriers[k]
-        if t in (4, 24):
-            ht, cfsb, cfsp, back = (np.asarray(v) for v in raw.barriers[k])
+        if t in (4, 24, 5, 25):
+            vals = [np.asarray(v) for v in raw.barriers[k]]
+            back = vals[3]
             front = np.asarray(nodes, np.int64)
             ibconn[j:j + n] = back + 1
             ibconn[j + n:j + 2 * n] = front[::-1] + 1
-            for arr, v in zip(barin, (ht, cfsb, cfsp)):
+            per_entry = list(zip(barin, vals[:3]))
+            if t in (5, 25):
+                per_entry += list(zip(pipes, vals[4:7]))
+            for arr, v in per_entry:
                 arr[j:j + n] = v
                 arr[j + n:j + 2 * n] = v[::-1]
             n *= 2
@@ -452,6 +457,7 @@ def build_case(raw, params: dict, schedule: Schedule, tides, cf: float = 0.0025,
         nelezng=nelezng, zngif1=zngif[0], zngif2=zngif[1], zngif3=zngif[2], neitabele=neitabele,
         barlanht=barlanht, barlancfsp=barlancfsp, ibconn=ibconn, barinht=barin[0],
         barincfsb=barin[1], barincfsp=barin[2], nvell=nvell,
+        pipeht=pipes[0], pipecoef=pipes[1], pipediam=pipes[2],
     )
     for k in STATE_F64:
         A[k] = np.zeros(npn, np.float64)
@@ -644,7 +650,7 @@ def channel_case(dt: float = 5.0, amp: float = 0.5, vortex: bool = False,
                  zero_gradient: int = 0, flux_settling: float = 0.0, river_eta: float = 0.05,
                  elev_series: float = 0.0, flux_series: float = 0.0, series_hours: float = 6.0,
                  barrier: float | None = None, barrier_type: int = 3,
-                 levee: float | None = None, levee_type: int = 4,
+                 levee: float | None = None, levee_type: int = 4, pipe=None,
                  prep: MeshPrep | None = None, **kw) -> Case:
     """Tidal channel: 121x41 nodes, 20 m -> 5 m, M2 0.5 m, dt 5 s.  With
     `vortex`, a small Holland vortex (Rmax 8 km) crosses the channel.  With
@@ -668,9 +674,11 @@ def channel_case(dt: float = 5.0, amp: float = 0.5, vortex: bool = False,
     leaves over it once it stands 6 cm above the crest.  With `levee` [m
     above datum], an internal barrier (IBTYPE `levee_type`, 4 or 24) with
     that crest crosses the channel at x = 30 km and a dry polder at datum
-    level lies east of it (meshgen.levee_channel_mesh)."""
+    level lies east of it (meshgen.levee_channel_mesh); for levee_type 5 or
+    25, `pipe` = (crown height [m above datum], friction coefficient,
+    diameter [m]) gives every pair a pipe under the crest."""
     from .meshgen import channel_mesh, levee_channel_mesh
-    raw = channel_mesh() if levee is None else levee_channel_mesh(levee, levee_type)
+    raw = channel_mesh() if levee is None else levee_channel_mesh(levee, levee_type, pipe=pipe)
     if river is not None or radiation or zero_gradient or barrier is not None:
         nx, ny = 121, 41
         nid = lambda i, j: i * ny + j

@@ -108,7 +108,7 @@ typedef struct {
    * datum and the supercritical discharge coefficient per boundary entry;
    * NULL when the mesh has none */
   const double *barlanht, *barlancfsp;   /* (NVEL) */
-  /* internal barriers (IBTYPE 4/24, mesh.F:2140-2240, 2577-2584): the node
+  /* internal barriers (IBTYPE 4/24 and 5/25, mesh.F:2140-2240, 2577-2594): the node
    * across the barrier (IBCONN, 1-based), crest height and the subcritical
    * and supercritical discharge coefficients per boundary entry, front face
    * then back face of each barrier segment; NVELL(NBOU) as mesh.F leaves it
@@ -117,6 +117,9 @@ typedef struct {
   const int *ibconn;
   const double *barinht, *barincfsb, *barincfsp;   /* (NVEL) */
   const int *nvell;                                 /* (NBOU) */
+  /* cross-barrier pipes of IBTYPE 5/25 barriers (mesh.F:2586-2594): crown
+   * height, friction coefficient and diameter per entry; NULL without them */
+  const double *pipeht, *pipecoef, *pipediam;      /* (NVEL) */
 } adc_arrays_t;
 
 /* Per-step scalars TIMESTEP computes before the hot path (timestep.F:257-353). */
@@ -331,20 +334,24 @@ int adc_fort14_write(const char *path, const char *title, int np, int ne, const 
  * flux-boundary node (NVEL, in file order, 0 elsewhere), and
  * adc_fort14_write_barriers writes a mesh that has such segments. */
 int adc_fort14_barriers(const char *path, double *barlanht, double *barlancfsp);
-/* Internal barrier segments (IBTYPE 4/24) list pairs: the node, the node
- * across the barrier and BARINHT, BARINCFSB, BARINCFSP (mesh.F:479-495); a
- * pair counts twice in the file's NVEL.  adc_fort14_read's nbvv holds the
- * front nodes (nvell counts pairs); adc_fort14_internal_barriers returns
- * IBCONN (1-based) and the three values per nbvv entry, 0 elsewhere. */
+/* Internal barrier segments (IBTYPE 4/24, and 5/25 with pipes) list pairs:
+ * the node, the node across the barrier, BARINHT, BARINCFSB, BARINCFSP and
+ * for 5/25 PIPEHT, PIPECOEF, PIPEDIAM (mesh.F:479-524); a pair counts twice
+ * in the file's NVEL.  adc_fort14_read's nbvv holds the front nodes (nvell
+ * counts pairs); adc_fort14_internal_barriers returns IBCONN (1-based) and
+ * the values per nbvv entry, 0 elsewhere (the pipe arrays may be NULL). */
 int adc_fort14_internal_barriers(const char *path, int *ibconn, double *barinht,
-                                 double *barincfsb, double *barincfsp);
+                                 double *barincfsb, double *barincfsp, double *pipeht,
+                                 double *pipecoef, double *pipediam);
 int adc_fort14_write_barriers(const char *path, const char *title, int np, int ne,
                               const double *x, const double *y, const double *dp, const int *nm,
                               int nope, const int *nvdll, const int *nbdv, int nbou,
                               const int *nvell, const int *ibtype, const int *nbvv,
                               const double *barlanht, const double *barlancfsp,
                               const int *ibconn, const double *barinht,
-                              const double *barincfsb, const double *barincfsp);
+                              const double *barincfsb, const double *barincfsp,
+                              const double *pipeht, const double *pipecoef,
+                              const double *pipediam);
 
 /* fort.15 model parameters of a 2DDI run (READ_INPUT, read_input.F:
  * 949-4566), positional records in read_input's order plus the namelist

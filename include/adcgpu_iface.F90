@@ -36,6 +36,7 @@ module adcgpu_iface
       type(c_ptr) :: nelezng, zngif1, zngif2, zngif3, neitabele
       type(c_ptr) :: barlanht, barlancfsp
       type(c_ptr) :: ibconn, barinht, barincfsb, barincfsp, nvell
+      type(c_ptr) :: pipeht, pipecoef, pipediam
    end type
 
    type, bind(C), public :: adc_step_t

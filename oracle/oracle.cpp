@@ -587,7 +587,8 @@ struct orc_model {
   int nfluxrbc = 0;   /* radiation (IBTYPE 30) entries, mesh.F:2045 */
   int nfluxgbc = 0;   /* zero normal velocity gradient (IBTYPE 40) entries, mesh.F:2072 */
   int nfluxb = 0;     /* external barrier (IBTYPE 3/13/23) entries, mesh.F:1913 */
-  int nfluxib = 0;    /* internal barrier (IBTYPE 4/24) entries, mesh.F:1919 */
+  int nfluxib = 0;    /* internal barrier (IBTYPE 4/24/5/25) entries, mesh.F:1919, 1924 */
+  int nfluxibp = 0;   /* barriers with pipes (IBTYPE 5/25), mesh.F:1925 */
   std::vector<int> nib, nibcnt;   /* NIBNODECODE, NIBCNT (NP) */
   /* river radiation (IBTYPE 52): FluxSettlingIT, EtaDisc_Fill and
    * EtaDisc/ElevDisc at the boundary entries (timestep.F:183, 243-245) */
@@ -662,7 +663,8 @@ orc_model *orc_model_create(const orc_params_t *p, orc_arrays_t *a) {
     if (lb == 30 || lb == 32) m->nfluxrbc = 1;   /* mesh.F:2044-2045, 2056-2058 */
     if (lb == 40 || lb == 41) m->nfluxgbc = 1;
     if (lb == 3 || lb == 13 || lb == 23) m->nfluxb = 1;
-    if (lb == 4 || lb == 24) m->nfluxib = 1;
+    if (lb == 4 || lb == 24 || lb == 5 || lb == 25) m->nfluxib = 1;
+    if (lb == 5 || lb == 25) m->nfluxibp = 1;
   }
   m->nib.assign(a->np, 0);
   m->nibcnt.assign(a->np, 0);
@@ -921,7 +923,7 @@ static void orc_model_flux(orc_model *m, const orc_step_t *s) {
     int I = 0;
     for (int K = 0; K < a->nbou; ++K) {
       const int lb = a->lbcodei[I], NV = a->nvell[K];
-      if (lb != 4 && lb != 24) {
+      if (lb != 4 && lb != 24 && lb != 5 && lb != 25) {
         I = I + NV;
         continue;
       }
@@ -981,6 +983,59 @@ static void orc_model_flux(orc_model *m, const orc_step_t *s) {
         }
         m->qn2[I - 1] = FLUX;
       }
+    }
+  }
+  /* discharge through cross-barrier pipes, timestep.F:1034-1044 and
+   * COMPUTE_CROSS_BARRIER_PIPE_FLUX (weir_boundary.F90:2469-2579) */
+  if (m->nfluxibp) {
+    const double BARMIN = 0.04, PI = 3.141592653589793;
+    const int *NODECODE = a->nodecode;
+    for (int I = 0; I < a->nvel; ++I) {
+      if (a->lbcodei[I] != 5 && a->lbcodei[I] != 25) continue;
+      const int NNBB1 = a->nbv[I] - 1, NNBB2 = a->ibconn[I] - 1;
+      const double PIPEHT = a->pipeht[I], PIPECOEF = a->pipecoef[I], PIPEDIAM = a->pipediam[I];
+      const double RBARWL1 = a->eta2[NNBB1] - PIPEHT, RBARWL2 = a->eta2[NNBB2] - PIPEHT;
+      double FLUX = 0.0;
+      [&] {
+        if ((RBARWL1 < 0.0) && (RBARWL2 < 0.0)) return;
+        if (std::fabs(RBARWL1 - RBARWL2) < BARMIN) return;
+        if ((RBARWL1 > RBARWL2) && (RBARWL1 > BARMIN)) {
+          if (RBARWL2 <= 0.0) {
+            if (NODECODE[NNBB1] == 0)
+              FLUX = 0.0;
+            else
+              FLUX = -s->rampintflux * 0.25 * PI * (PIPEDIAM * PIPEDIAM) *
+                     std::sqrt(2.0 * G * RBARWL1 / (1.0 + PIPECOEF));
+          } else {
+            if (NODECODE[NNBB1] == 0)
+              FLUX = 0.0;
+            else
+              FLUX = -s->rampintflux * 0.25 * PI * (PIPEDIAM * PIPEDIAM) *
+                     std::sqrt(2.0 * G * (RBARWL1 - RBARWL2) / PIPECOEF);
+            return;
+          }
+        }
+        if ((RBARWL2 > RBARWL1) && (RBARWL2 > BARMIN)) {
+          if (RBARWL1 <= 0.0) {
+            if (NODECODE[NNBB2] == 0) {
+              FLUX = 0.0;
+            } else {
+              FLUX = s->rampintflux * 0.25 * PI * (PIPEDIAM * PIPEDIAM) *
+                     std::sqrt(2.0 * G * RBARWL2 / (1.0 + PIPECOEF));
+              m->nib[NNBB1] = 1;
+            }
+          } else {
+            if (NODECODE[NNBB2] == 0) {
+              FLUX = 0.0;
+            } else {
+              FLUX = s->rampintflux * 0.25 * PI * (PIPEDIAM * PIPEDIAM) *
+                     std::sqrt(2.0 * G * (RBARWL2 - RBARWL1) / PIPECOEF);
+              m->nib[NNBB1] = 1;
+            }
+          }
+        }
+      }();
+      m->qn2[I] = m->qn2[I] + FLUX;
     }
   }
   /* zero normal velocity gradient entries, timestep.F:945-952 */

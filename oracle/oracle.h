@@ -83,6 +83,7 @@ typedef struct {
   const int *ibconn;        /* (NVEL) internal barriers (IBTYPE 4/24): node across, 1-based */
   const double *barinht, *barincfsb, *barincfsp;   /* (NVEL) */
   const int *nvell;         /* NVELL(NBOU) after closure, barrier segments in pairs */
+  const double *pipeht, *pipecoef, *pipediam;   /* (NVEL) pipes of IBTYPE 5/25 barriers */
 } orc_arrays_t;
 
 /* Per-step scalars the TIMESTEP driver computes before the hot path. */

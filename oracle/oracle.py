@@ -49,6 +49,7 @@ _ARR = [
     ("nelezng", ip_), ("zngif1", dp_), ("zngif2", dp_), ("zngif3", dp_), ("neitabele", ip_),
     ("barlanht", dp_), ("barlancfsp", dp_),
     ("ibconn", ip_), ("barinht", dp_), ("barincfsb", dp_), ("barincfsp", dp_), ("nvell", ip_),
+    ("pipeht", dp_), ("pipecoef", dp_), ("pipediam", dp_),
 ]
 
 

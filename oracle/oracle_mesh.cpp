@@ -221,7 +221,7 @@ int orc_mesh_csr_positions(int np, int ne, int mnei, const int *nm, const int *n
  * the path (external 0/10/20, island 1/11/21, specified flow 2/12/22,
  * radiation 30, coupled flux/radiation 32, zero normal gradient 40/41,
  * river radiation 52, external barrier 3/13/23, and each face of an
- * internal barrier 4/24 as its own unclosed segment, the back face reversed
+ * internal barrier 4/24 or 5/25 as its own unclosed segment, the back face reversed
  * as mesh.F:2158-2192 loads it):
  * segment closure (:2226-2244), per node the GWCE entry NBV/LBCODEI with
  * the inner-angle test (:2266-2411), BNDLEN2O3 (:2301-2303), the outward
@@ -244,7 +244,7 @@ int orc_boundary_setup(int np, const double *x, const double *y, int nbou, const
     const bool island = (t == 1 || t == 11 || t == 21);
     if (!(island || t == 0 || t == 10 || t == 20 || t == 2 || t == 12 || t == 22 || t == 30 ||
           t == 32 || t == 40 || t == 41 || t == 52 || t == 3 || t == 13 || t == 23 || t == 4 ||
-          t == 24))
+          t == 24 || t == 5 || t == 25))
       return -1;
     int nvell = seg_ptr[k + 1] - seg_ptr[k];
     if (nvell < 2) return -1;

@@ -352,3 +352,18 @@ def test_channel_internal_barrier(lib, orc, ltype):
     a = c0.arrays
     east = a["x"] > 30.0e3 + 1.0
     assert a["nodecode"][east].sum() > 100   # the polder has begun to flood
+
+
+@pytest.mark.parametrize("ltype", [5, 25])
+def test_channel_barrier_pipes(lib, orc, ltype):
+    """A barrier too high to overtop with a pipe under every pair (IBTYPE
+    5/25): the pipe discharge added to the barrier flux (weir_boundary.F90:
+    2469-2579, timestep.F:1034-1044) floods the polder, against the oracle
+    over a graph-replayed run."""
+    from adcirc_b200 import model
+    c0, cg, io, ig = _pair(lambda **k: model.channel_case(levee=10.0, levee_type=ltype,
+                                                          pipe=(-0.5, 1.0, 1.0), amp=2.0, **k),
+                           1000, use_run=True)
+    _check(c0, cg, io, ig)
+    a = c0.arrays
+    assert a["nodecode"][a["x"] > 30.0e3 + 1.0].sum() > 100

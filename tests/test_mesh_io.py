@@ -70,11 +70,10 @@ def test_fort14_labels_and_fortran_numbers(lib, tmp_path):
     assert m.land_segments[0][0] == 0 and np.array_equal(m.land_segments[0][1], [1, 2, 3])
 
 
-def test_fort14_barrier_with_pipes_unsupported(lib, tmp_path):
-    """Internal barriers with cross-barrier pipes (IBTYPE 5/25) are refused."""
+def test_fort14_periodic_unsupported(lib, tmp_path):
+    """Periodic boundary segments (IBTYPE 94) are refused."""
     from adcirc_b200 import _lib, adcirc_io
-    text = ("t\n1 3\n1 0 0 1\n2 1 0 1\n3 0 1 1\n1 3 1 2 3\n0\n0\n1\n4\n2 5\n"
-            "1 2 0.5 1.0 1.0 0.1 1.0 0.5\n3 1 0.5 1.0 1.0 0.1 1.0 0.5\n")
+    text = "t\n1 3\n1 0 0 1\n2 1 0 1\n3 0 1 1\n1 3 1 2 3\n0\n0\n1\n2\n2 94\n1 2\n3 1\n"
     p = tmp_path / "fort.14"
     p.write_text(text)
     dims = np.zeros(6, np.int32)
@@ -137,6 +136,27 @@ def test_fort14_internal_barrier(lib, tmp_path):
     front = np.nonzero(lbc == 24)[0][:39]
     assert np.array_equal(a["ibconn"][front] - 1, b1[3])
     assert np.array_equal(a["nbv"][front[-1] + 1:front[-1] + 40] - 1, b1[3][::-1])
+
+
+def test_fort14_barrier_pipes(lib, tmp_path):
+    """IBTYPE 5/25 pairs also carry the pipe's crown height, coefficient and
+    diameter (mesh.F:506-524); they survive the file and reach the bound
+    arrays in face order."""
+    from adcirc_b200 import adcirc_io, meshgen, model
+    raw = meshgen.levee_channel_mesh(2.0, 25, pipe=(0.3, 1.5, 0.8))
+    p = tmp_path / "fort.14"
+    adcirc_io.write_fort14(raw, p)
+    back = adcirc_io.read_fort14(p)
+    assert [t for t, _ in back.land_segments] == [0, 25]
+    for u, v in zip(raw.barriers[1], back.barriers[1]):
+        assert np.array_equal(np.asarray(u), np.asarray(v))
+    sched = model.Schedule(dt=5.0)
+    tides = [(1e-4, 0.0, 1.0, np.full(raw.open_nodes.size, 0.5), np.zeros(raw.open_nodes.size))]
+    a = model.build_case(back, model.default_params(5.0), sched, tides).arrays
+    on = a["lbcodei"] == 25
+    assert on.sum() == 78
+    assert np.all(a["pipeht"][on] == 0.3) and np.all(a["pipecoef"][on] == 1.5)
+    assert np.all(a["pipediam"][on] == 0.8) and not np.any(a["pipediam"][~on])
 
 
 def test_fort63_64_format(lib, tmp_path):

@@ -180,3 +180,19 @@ def test_levee_overtopping_floods_the_polder(orc):
             # within two element columns (0.5 km each) of the barrier
             assert first is not None and first <= 31.0e3 + 1.0
     assert wet[0.0] > 100 and wet[10.0] == 0
+
+
+def test_barrier_pipe_floods_the_polder(orc):
+    """A barrier too high to overtop (10 m) with a 1 m pipe under it (IBTYPE
+    5, crown 0.5 m below datum): the pipe's discharge (weir_boundary.F90:
+    2469-2579) floods the polder; with the crown 10 m up nothing crosses."""
+    from adcirc_b200 import model
+    wet = {}
+    for crown in (-0.5, 10.0):
+        case = model.channel_case(levee=10.0, levee_type=5, pipe=(crown, 1.0, 1.0), amp=2.0)
+        a = case.arrays
+        om = orc.OracleModel(case)
+        om.run(1, 1000)
+        om.close()
+        wet[crown] = int(a["nodecode"][a["x"] > 30.0e3 + 1.0].sum())
+    assert wet[-0.5] > 100 and wet[10.0] == 0
