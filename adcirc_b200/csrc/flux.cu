@@ -1,7 +1,8 @@
-// flux.cu -- specified normal flux boundaries (IBTYPE 2, 12, 22), radiation
-// boundaries (IBTYPE 30), coupled flux/radiation boundaries (IBTYPE 32),
-// zero-normal-gradient boundaries (IBTYPE 40) and river-radiation
-// boundaries (IBTYPE 52).
+// flux.cu -- specified normal flux boundaries (IBTYPE 2, 12, 22), external
+// barriers (3, 13, 23), internal barriers (4, 24) and barriers with pipes
+// (5, 25), radiation boundaries (30), coupled flux/radiation boundaries
+// (32), zero-normal-gradient boundaries (40, 41) and river-radiation
+// boundaries (52).
 //
 // Three pieces of the reference's flux-boundary path:
 //  * QN0 <- QN1 <- QN2 <- 0 and EN0 <- EN1 <- EN2 <- 0 (timestep.F:606-613),
