@@ -140,8 +140,8 @@ extern "C" int adc_hotstart_read(adc_ctx *c, const char *path) {
   const std::vector<HsRec> recs = hs_records(c);
   if (h.nrec != (int64_t)recs.size()) {
     std::fclose(f);
-    set_error("adc_hotstart_read: %s has %lld records, the context needs %zu (vortex or warm-start "
-              "state differs)", path, (long long)h.nrec, recs.size());
+    set_error("adc_hotstart_read: %s has %lld records, the context needs %zu (vortex, flux, "
+              "boundary-series or warm-start state differs)", path, (long long)h.nrec, recs.size());
     return ADC_ERR_ARG;
   }
   ADC_CUDA(cudaStreamSynchronize(c->stream));
