@@ -128,7 +128,9 @@ class AdcFort15(C.Structure):
     _fields_ = ([("rundes", C.c_char * 88), ("runid", C.c_char * 88)] +
                 [(n, C.c_int) for n in _F15_INTS] + [(n, C.c_double) for n in _F15_REALS] +
                 [(n, AdcOutputSpec) for n in ("oute", "outv", "outc", "outm", "outge", "outgv",
-                                              "outgc", "outgw")])
+                                              "outgc", "outgw")] +
+                [("has_nws08", C.c_int), ("windspeed_averaging_minute", C.c_int),
+                 ("wind_multiplier", C.c_double)])
 
 
 class AdcFort15Tables(C.Structure):

@@ -204,6 +204,52 @@ bool namelist_real(const Records &r, const char *grp, const char *name, double &
   }
 }
 
+// the raw text of `name` = value inside namelist group `grp` (quotes and
+// surrounding blanks removed), lower-cased
+bool namelist_text(const Records &r, const char *grp, const char *name, std::string &out) {
+  std::string all;
+  for (const std::string &s : r.rec) {
+    all += s;
+    all += '\n';
+  }
+  for (char &c : all) c = (char)std::tolower((unsigned char)c);
+  std::string g = std::string("&") + grp, nm = name;
+  for (char &c : g) c = (char)std::tolower((unsigned char)c);
+  for (char &c : nm) c = (char)std::tolower((unsigned char)c);
+  size_t at = all.find(g);
+  if (at == std::string::npos) return false;
+  size_t end = all.find('/', at);
+  if (end == std::string::npos) end = all.size();
+  for (size_t p = all.find(nm, at + g.size()); p != std::string::npos && p < end;
+       p = all.find(nm, p + nm.size())) {
+    if (std::isalnum((unsigned char)all[p - 1]) || all[p - 1] == '_') continue;
+    size_t q = p + nm.size();
+    while (q < end && std::isspace((unsigned char)all[q])) ++q;
+    if (q >= end || all[q] != '=') continue;
+    ++q;
+    while (q < end && std::isspace((unsigned char)all[q])) ++q;
+    size_t e = q;
+    if (q < end && (all[q] == '\'' || all[q] == '"')) {
+      const char quote = all[q];
+      e = all.find(quote, q + 1);
+      if (e == std::string::npos || e > end) return false;
+      out = all.substr(q + 1, e - q - 1);
+      return true;
+    }
+    while (e < end && !std::isspace((unsigned char)all[e]) && all[e] != ',') ++e;
+    out = all.substr(q, e - q);
+    return true;
+  }
+  return false;
+}
+
+// a Fortran logical value: .true./.false./t/f
+bool fortran_true(const std::string &v) {
+  size_t k = 0;
+  while (k < v.size() && v[k] == '.') ++k;
+  return k < v.size() && v[k] == 't';
+}
+
 bool flux_code(int c) { return c == 2 || c == 12 || c == 22 || c == 52; }
 
 }  // namespace
@@ -446,6 +492,39 @@ extern "C" int adc_fort15_read(const char *path, int neta, int nvel, const int *
     o->wind_drag_limit = v;
     o->has_wind_drag_limit = 1;
   }
+  // &nws08Control (nws08.F90:318-413): defaults, then what the group sets
+  o->windspeed_averaging_minute = 1;
+  o->wind_multiplier = 1.0;
+  {
+    std::string t;
+    const bool any = namelist_text(P.r, "nws08Control", "vortexModel", t) |
+                     namelist_text(P.r, "nws08Control", "backgroundWindModel", t) |
+                     namelist_text(P.r, "nws08Control", "BCalc", t) |
+                     namelist_text(P.r, "nws08Control", "windspeed_averaging_minute", t) |
+                     namelist_text(P.r, "nws08Control", "WindMultiplier", t) |
+                     namelist_text(P.r, "nws08Control", "useInflow", t) |
+                     namelist_text(P.r, "nws08Control", "thetaLatDep", t);
+    o->has_nws08 = any ? 1 : 0;
+    struct Want {
+      const char *name, *value;
+    };
+    for (const Want &w : {Want{"vortexModel", "holland"},
+                          Want{"backgroundWindModel", "radialvelocityweighted"},
+                          Want{"BCalc", "limited"}})
+      if (namelist_text(P.r, "nws08Control", w.name, t) && t != w.value) {
+        set_error("fort.15 %s: &nws08Control %s = '%s' is not implemented (only '%s')", path,
+                  w.name, t.c_str(), w.value);
+        return ADC_ERR_UNSUPPORTED;
+      }
+    for (const char *flag : {"useInflow", "thetaLatDep"})
+      if (namelist_text(P.r, "nws08Control", flag, t) && fortran_true(t)) {
+        set_error("fort.15 %s: &nws08Control %s = .true. is not implemented", path, flag);
+        return ADC_ERR_UNSUPPORTED;
+      }
+    if (namelist_real(P.r, "nws08Control", "WindMultiplier", v)) o->wind_multiplier = v;
+    if (namelist_real(P.r, "nws08Control", "windspeed_averaging_minute", v))
+      o->windspeed_averaging_minute = (int)v;
+  }
   return ADC_OK;
 }
 
@@ -637,6 +716,9 @@ extern "C" int adc_fort15_write(const char *path, const adc_fort15_t *o, int net
                                           {'r', (void *)&o->convcr}, {'i', (void *)&o->itmax}});
   if (o->has_slim) std::fprintf(f, "&wetDryControl slim=%.17g /\n", o->slim);
   if (o->has_wind_drag_limit) std::fprintf(f, "&metControl WindDragLimit=%.17g /\n", o->wind_drag_limit);
+  if (o->has_nws08)
+    std::fprintf(f, "&nws08Control windspeed_averaging_minute=%d, WindMultiplier=%.17g /\n",
+                 o->windspeed_averaging_minute, o->wind_multiplier);
   const bool ok = std::ferror(f) == 0;
   std::fclose(f);
   if (!ok) {

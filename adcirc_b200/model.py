@@ -582,7 +582,9 @@ def case_from_files(fort14, fort15, vortex: "Vortex | None" = None,
         if vortex is None:
             vortex = adcirc_io.read_fort22(side(fort22, "fort.22"), f.irefyr, f.irefmo, f.irefday,
                                            f.irefhr, f.slam0, f.sfea0, f.rnday, bladj=f.bladj,
-                                           start_time=start)
+                                           start_time=start, drag_limit=f.wind_drag_limit,
+                                           avg_minute=f.windspeed_averaging_minute,
+                                           wind_mult=f.wind_multiplier)
         case.vortex = vortex
     case.meta["fort15"] = f
     return case
@@ -622,6 +624,11 @@ def fort15_for_case(case: Case, rnday: float = 1.0, rundes: str = "", runid: str
     o.slim, o.has_slim = p["slim"], int(p["slim"] != 1.0e9)
     o.wind_drag_limit = case.vortex.drag_limit if case.vortex is not None else 0.0035
     o.has_wind_drag_limit = int(case.vortex is not None and o.wind_drag_limit != 0.0035)
+    o.windspeed_averaging_minute, o.wind_multiplier = 1, 1.0
+    if case.vortex is not None:
+        o.windspeed_averaging_minute = case.vortex.avg_minute
+        o.wind_multiplier = case.vortex.wind_mult
+        o.has_nws08 = int(case.vortex.avg_minute != 1 or case.vortex.wind_mult != 1.0)
     nbfr, neta = case.sizes["nbfr"], case.sizes["neta"]
     a = case.arrays
     o.nbfr = nbfr

@@ -355,7 +355,8 @@ int adc_fort14_write_barriers(const char *path, const char *title, int np, int n
 
 /* fort.15 model parameters of a 2DDI run (READ_INPUT, read_input.F:
  * 949-4566), positional records in read_input's order plus the namelist
- * values the path uses (&wetDryControl slim, &metControl WindDragLimit).
+ * values the path uses (&wetDryControl slim, &metControl WindDragLimit,
+ * &nws08Control).
  * Angles read_input converts on reading (FACE, EFA, FFACE, QNPH, ENPH,
  * FACET) are returned in radians.  IM other than 0/10/111111, NWS other
  * than 0/+-8, and station lists in external .151 files return
@@ -385,6 +386,12 @@ typedef struct {
   double thas, thaf, fmv, convcr;
   double slim, wind_drag_limit;                    /* defaults 1e9, 0.0035 */
   adc_output_spec_t oute, outv, outc, outm, outge, outgv, outgc, outgw;
+  /* &nws08Control (readNws08Namelist, nws08.F90:318-413): the values the
+   * Holland path uses; a namelist that selects another vortex model,
+   * background wind, B calculation, inflow angle or latitude-dependent
+   * angle returns ADC_ERR_UNSUPPORTED */
+  int has_nws08, windspeed_averaging_minute;       /* default 1 */
+  double wind_multiplier;                          /* default 1 */
 } adc_fort15_t;
 
 /* Caller-owned tables adc_fort15_read fills; any pointer may be NULL (a

@@ -311,3 +311,32 @@ def test_external_barrier_case_through_files(lib, orc, tmp_path):
         om.run(1, 200)
         om.close()
     assert np.array_equal(c.arrays["eta2"], c2.arrays["eta2"])
+
+
+def test_nws08_namelist(lib, tmp_path):
+    """&nws08Control (nws08.F90:318-413): WindMultiplier and the averaging
+    minute reach the vortex; other vortex models, background winds, B
+    calculations and inflow angles are refused."""
+    from test_fort22 import atcf
+    c = model.channel_case(vortex=True)
+    c.vortex.wind_mult, c.vortex.avg_minute = 1.25, 10
+    lbc = c.arrays["lbcodei"][:c.sizes["nvel"]]
+    adcirc_io.write_fort14(c.meta["raw"], tmp_path / "fort.14")
+    f15 = tmp_path / "fort.15"
+    adcirc_io.write_fort15(f15, model.fort15_for_case(c), c.sizes["neta"], lbc)
+    assert "&nws08Control" in f15.read_text()
+    lines = [atcf(2000, 1, 1, 0, "BEST", 0, 0, 0, 60, 970, 200, 8, ew="E"),
+             atcf(2000, 1, 2, 0, "BEST", 0, 5, 6, 55, 975, 200, 9, ew="E")]
+    (tmp_path / "fort.22").write_text("\n".join(lines) + "\n")
+    c2 = model.case_from_files(tmp_path / "fort.14", f15)
+    assert c2.vortex.wind_mult == 1.25 and c2.vortex.avg_minute == 10
+    text = f15.read_text()
+    for bad in ("vortexModel='CLE15'", "backgroundWindModel = 'LC12'", "BCalc='exact'",
+                "useInflow=.true.", "thetaLatDep = T"):
+        g = tmp_path / "bad.15"
+        g.write_text(text.replace("&nws08Control ", f"&nws08Control {bad}, "))
+        o = _lib.AdcFort15()
+        rc = lib.adc_fort15_read(str(g).encode(), c.sizes["neta"], int(lbc.size),
+                                 lbc.ctypes.data_as(_lib.ip_), o, None)
+        assert rc == _lib.ADC_ERR_UNSUPPORTED, bad
+        assert bad.split("=")[0].strip() in _lib.last_error()
