@@ -25,10 +25,16 @@ def _cases(orc):
     yield "river32", lambda **k: model.channel_case(river=0.5, river_type=32, **k)
     yield "zerograd41", lambda **k: model.channel_case(zero_gradient=41, **k)
     yield "surge30k", lambda **k: model.surge_case(target_nodes=30_000, **k)
+    yield "barrier13", lambda **k: model.channel_case(barrier=-0.5, barrier_type=13, **k)
+    yield "levee24", lambda **k: model.channel_case(levee=0.0, levee_type=24, **k)
+    yield "pipes5", lambda **k: model.channel_case(levee=1.0, levee_type=5, pipe=(0.0, 1.0, 1.0), **k)
+    yield "series", lambda **k: model.channel_case(river=0.5, elev_series=150.0, flux_series=300.0,
+                                                   series_hours=1.0, **k)
 
 
 @pytest.mark.parametrize("name", ["channel", "beach", "river2", "river22", "radiation", "river52",
-                                  "zerograd", "river32", "zerograd41", "surge30k"])
+                                  "zerograd", "river32", "zerograd41", "surge30k", "barrier13",
+                                  "levee24", "pipes5", "series"])
 def test_case_tables_match(lib, orc, name):
     fn = dict(_cases(orc))[name]
     a = fn()
@@ -116,3 +122,47 @@ def test_neitabele_packs_each_ring(lib, orc):
     for i in range(0, c.sizes["np"], 97):
         for e in te[i][te[i] > 0] - 1:
             assert i in nm[e]
+
+
+@pytest.mark.parametrize("seed", [1, 2, 3])
+def test_random_meshes_tables_match(lib, orc, seed):
+    """Scattered-point Delaunay meshes (half the elements listed clockwise,
+    irregular valence, an open segment and a land segment around the hull):
+    the library's and the oracle's table builders agree bit for bit."""
+    from scipy.spatial import Delaunay
+    from adcirc_b200 import model
+    from adcirc_b200.meshgen import RawMesh
+    rng = np.random.default_rng(seed)
+    n = 400
+    pts = rng.uniform(0.0, 1.0e4, size=(n, 2))
+    tri = Delaunay(pts)
+    nm = tri.simplices.astype(np.int64)
+    flip = rng.random(nm.shape[0]) < 0.5            # half the elements clockwise
+    nm[flip] = nm[flip][:, [0, 2, 1]]
+    hull = tri.convex_hull                           # edges of the outer boundary
+    # walk the hull as one ordered loop
+    nxt = {}
+    for a_, b_ in hull:
+        nxt.setdefault(a_, []).append(b_)
+        nxt.setdefault(b_, []).append(a_)
+    loop = [hull[0][0]]
+    prev = None
+    while True:
+        cur = loop[-1]
+        cand = [v for v in nxt[cur] if v != prev]
+        prev, nx_ = cur, cand[0]
+        if nx_ == loop[0]:
+            break
+        loop.append(nx_)
+    loop = np.asarray(loop, np.int64)
+    open_nodes = loop[:6]
+    land = loop[5:]
+    raw = RawMesh(f"random{seed}", pts[:, 0].copy(), pts[:, 1].copy(),
+                  rng.uniform(2.0, 10.0, n), nm, open_nodes, [(0, land)], {"lx": 1e4, "ly": 1e4})
+    sched = model.Schedule(dt=2.0)
+    tides = [(1.4e-4, 0.0, 1.0, np.full(open_nodes.size, 0.3), np.zeros(open_nodes.size))]
+    a = model.build_case(raw, model.default_params(2.0), sched, tides)
+    b = model.build_case(raw, model.default_params(2.0), sched, tides, prep=orc.mesh_prep())
+    assert a.sizes == b.sizes
+    bad = [k for k in a.arrays if not np.array_equal(a.arrays[k], b.arrays[k])]
+    assert not bad, f"tables differ: {bad}"
