@@ -10,8 +10,10 @@
  * ISO_C_BINDING (include/adcgpu_iface.F90) and Python through ctypes.
  *
  * Entry points that allocate device memory: adc_gpu_bind (device mirrors),
- * adc_set_vortex and adc_set_flux (forcing tables), adc_jcg (staging for one
- * solve) and the self-check; adc_jcg_noalloc allocates nothing.  Errors are
+ * adc_set_vortex, adc_set_flux, adc_set_elev_series and adc_set_flux_series
+ * (forcing tables), adc_set_predictor and the ensemble calls, adc_jcg
+ * (staging for one solve) and the self-check; adc_jcg_noalloc allocates
+ * nothing.  Errors are
  * returned as status codes; the library never calls exit().
  */
 #ifndef ADCGPU_H
