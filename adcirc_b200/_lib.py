@@ -90,6 +90,13 @@ class AdcFort22Opts(C.Structure):
                 ("rnday", C.c_double)]
 
 
+class AdcFort67(C.Structure):
+    _fields_ = [("im", C.c_int), ("it", C.c_int), ("np", C.c_int), ("ne", C.c_int),
+                ("timeloc", C.c_double)] + [(n, dp_) for n in ("eta1", "eta2", "etadisc", "uu2",
+                                                               "vv2", "ch1")] + [
+                ("nodecode", ip_), ("noff", ip_)]
+
+
 class AdcVortex(C.Structure):
     _fields_ = [("nfix", C.c_int), ("avg_minute", C.c_int), ("hemisphere", C.c_int),
                 ("pad_", C.c_int)] + [(n, C.c_double) for n in (
@@ -181,6 +188,8 @@ def load():
         "adc_sync_from_host": (C.c_int, [vp]),
         "adc_set_met": (C.c_int, [vp, dp_, dp_, dp_]),
         "adc_set_vortex": (C.c_int, [vp, C.POINTER(AdcVortex)]),
+        "adc_fort67_write": (C.c_int, [C.c_char_p, C.POINTER(AdcFort67)]),
+        "adc_fort67_read": (C.c_int, [C.c_char_p, C.POINTER(AdcFort67)]),
         "adc_fort22_read": (C.c_int, [C.c_char_p, C.POINTER(AdcFort22Opts), ip_,
                                       C.POINTER(AdcVortexFix)]),
         "adc_set_flux": (C.c_int, [vp, C.POINTER(AdcFlux)]),

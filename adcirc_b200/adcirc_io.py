@@ -316,3 +316,44 @@ def read_fort22(path, irefyr: int, irefmo: int, irefday: int, irefhr: int, slam0
                      for k in range(n.value)])
     vortex_kw.setdefault("hemisphere", -1 if rows[0, 2] < 0.0 else 1)   # sign(1, lat)
     return Vortex(rows, **vortex_kw)
+
+
+def write_fort67(path, case, it: int, timeloc: float, im: int = 0, etadisc=None) -> None:
+    """Writes a case's state (as adc_sync_to_host leaves it) as the
+    reference's binary hotstart file (adc_fort67_write), for a reference run
+    to continue from."""
+    lib = _lib.load()
+    a = case.arrays
+    npn, ne = case.sizes["np"], case.sizes["ne"]
+    keep = {k: np.ascontiguousarray(a[k], np.float64) for k in ("eta1", "eta2", "uu2", "vv2")}
+    nc = np.ascontiguousarray(a["nodecode"], np.int32)
+    noff = np.ascontiguousarray(a["noff"], np.int32)
+    ed = np.ascontiguousarray(np.zeros(npn) if etadisc is None else etadisc, np.float64)
+    h = _lib.AdcFort67(int(im), int(it), npn, ne, float(timeloc), keep["eta1"].ctypes.data_as(dp_),
+                       keep["eta2"].ctypes.data_as(dp_), ed.ctypes.data_as(dp_),
+                       keep["uu2"].ctypes.data_as(dp_), keep["vv2"].ctypes.data_as(dp_), None,
+                       nc.ctypes.data_as(ip_), noff.ctypes.data_as(ip_))
+    _check(lib.adc_fort67_write(os.fsencode(path), C.byref(h)), "adc_fort67_write")
+
+
+def read_fort67(path) -> dict:
+    """Reads the reference's binary hotstart file (adc_fort67_read): a dict
+    of im, it, timeloc and the arrays eta1, eta2, etadisc, uu2, vv2,
+    nodecode, noff (ch1 when IM = 10)."""
+    lib = _lib.load()
+    p = os.fsencode(path)
+    h = _lib.AdcFort67()
+    _check(lib.adc_fort67_read(p, C.byref(h)), "adc_fort67_read")
+    npn, ne = h.np, h.ne
+    out = {k: np.zeros(npn) for k in ("eta1", "eta2", "etadisc", "uu2", "vv2", "ch1")}
+    out["nodecode"] = np.zeros(npn, np.int32)
+    out["noff"] = np.zeros(ne, np.int32)
+    for k in ("eta1", "eta2", "etadisc", "uu2", "vv2", "ch1"):
+        setattr(h, k, out[k].ctypes.data_as(dp_))
+    h.nodecode = out["nodecode"].ctypes.data_as(ip_)
+    h.noff = out["noff"].ctypes.data_as(ip_)
+    _check(lib.adc_fort67_read(p, C.byref(h)), "adc_fort67_read")
+    out.update(im=h.im, it=h.it, timeloc=h.timeloc)
+    if h.im != 10:
+        del out["ch1"]
+    return out

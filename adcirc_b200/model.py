@@ -590,6 +590,65 @@ def case_from_files(fort14, fort15, vortex: "Vortex | None" = None,
     return case
 
 
+def apply_hotstart(case: Case, hs: dict) -> int:
+    """Loads a reference hotstart (adcirc_io.read_fort67) into a case's
+    arrays as hstart.F does (:511-533, 764-768): ETA1, ETA2, UU2, VV2, NOFF,
+    NNODECODE and NODECODE from the file, then H1 = DP + IFNLFA ETA1,
+    H2 = DP + IFNLFA ETA2, ETAS = ETA2 - ETA1, QX2 = UU2 H2, QY2 = VV2 H2.
+    A vortex track is repositioned to the file's time (NWS08INIT picks the
+    fix pair from TimeLoc) and non-periodic series are advanced as
+    hstart.F:857-883 advances them.  Returns ITHS; the run continues with
+    step ITHS + 1.  Not carried over, because the reference recomputes them
+    at start-up rather than reading them: the met fields at ITHS
+    (hotstartMeteorologicalForcing, hstart.F:1442) and the flux history QN1,
+    QN2 of fort.20 boundaries (hstart.F:949-971); the first step after the
+    load starts them from the background pressure, no wind and zero flux."""
+    a = case.arrays
+    if hs["eta1"].size != case.sizes["np"] or hs["noff"].size != case.sizes["ne"]:
+        raise ValueError("the hotstart file holds another mesh")
+    ifnlfa = case.params["ifnlfa"]
+    for k in ("eta1", "eta2", "uu2", "vv2"):
+        a[k][:] = hs[k]
+    a["noff"][:] = hs["noff"]
+    a["nnodecode"][:] = hs["nodecode"]
+    a["nodecode"][:] = hs["nodecode"]
+    a["h1"][:] = a["dp"] + ifnlfa * a["eta1"]
+    a["h2"][:] = a["dp"] + ifnlfa * a["eta2"]
+    a["etas"][:] = a["eta2"] - a["eta1"]
+    a["qx2"][:] = a["uu2"] * a["h2"]
+    a["qy2"][:] = a["vv2"] * a["h2"]
+    iths, timeloc = int(hs["it"]), float(hs["timeloc"])
+    if case.vortex is not None:
+        case.vortex = dataclasses.replace(case.vortex, start_time=timeloc)
+    for attr in ("elev_series", "flux_series"):
+        ser = getattr(case, attr)
+        if ser is not None:
+            setattr(case, attr, series_at_hotstart(ser, iths, timeloc, case.schedule))
+    return iths
+
+
+def series_at_hotstart(ser: Series, iths: int, timeloc: float, sched: Schedule) -> Series:
+    """The record pair a reference run holds after a hotstart at step ITHS
+    (hstart.F:857-883: the read-ahead replayed over steps 1 .. ITHS-1, then
+    once more for TimeLoc), as a series that starts there."""
+    t1 = ser.start_time
+    t2 = t1 + ser.interval
+    k = 0
+    for it in range(1, iths):
+        timeit = it * sched.dt + sched.statim * 86400.0
+        if timeit > t2:
+            t1 = t2
+            t2 = t1 + ser.interval
+            k += 1
+    if timeloc > t2:
+        t1 = t2
+        k += 1
+    if k + 2 > ser.values.shape[0]:
+        raise ValueError("the series ends before the hotstart time")
+    v2 = None if ser.values2 is None else ser.values2[k:]
+    return dataclasses.replace(ser, values=ser.values[k:], values2=v2, start_time=t1)
+
+
 def fort15_for_case(case: Case, rnday: float = 1.0, rundes: str = "", runid: str = "run"):
     """The fort.15 values of a Case (the inverse of case_from_files), for
     adcirc_io.write_fort15: NRAMP 8 carries the case's separate elevation,

@@ -432,6 +432,24 @@ int adc_fort6x_header(const char *path, const char *rundes, const char *runid, c
 int adc_fort6x_append(const char *path, double timeloc, int it, int np, const double *v1,
                       const double *v2, const int *nodecode, double alternate);
 
+/* The reference's own binary hotstart file (fort.67/fort.68, writeHotstart
+ * write_output.F:4900-5154, read by hstart.F:500-560) for a serial 2DDI run
+ * without harmonic analysis or wave radiation stress: 8-byte direct-access
+ * records (header, ETA1, ETA2, EtaDisc, UU2, VV2, CH1 when IM = 10,
+ * NODECODE, NOFF, the zero pads and output counters).  adc_fort67_read with
+ * np = ne = 0 only fills the header fields; otherwise np and ne must match
+ * the file and the arrays are filled (etadisc and ch1 may be NULL).  A host
+ * derives H1, H2, ETAS, QX2 and QY2 from them as hstart.F:529-533, 764-768
+ * does, then binds or calls adc_sync_from_host. */
+typedef struct {
+  int im, it, np, ne;
+  double timeloc;
+  double *eta1, *eta2, *etadisc, *uu2, *vv2, *ch1;   /* (NP) */
+  int *nodecode, *noff;                               /* (NP), (NE) */
+} adc_fort67_t;
+int adc_fort67_write(const char *path, const adc_fort67_t *h);
+int adc_fort67_read(const char *path, adc_fort67_t *h);
+
 /* Hotstart: the counterparts of the reference's fort.67/68 dump
  * (write_output.F:4429-5582) and load (hstart.F:47-2048), in this
  * library's own binary format.  The file holds every array and scalar the
