@@ -317,8 +317,10 @@ int adc_set_vortex(adc_ctx *ctx, const adc_vortex_t *vortex);
 /* ------------------------------------------------------------------ */
 
 /* fort.14 mesh (read14, mesh.F:319-581).  dims = {NP, NE, NOPE, NETA,
- * NBOU, NVEL}.  Node labels map to 1..NP in file order, as read14 does.
- * Barrier (IBTYPE 3/4/5 families) and periodic (94) land segments return
+ * NBOU, NVEL}, NVEL counting one line per node (one per pair for internal
+ * barriers).  Node labels map to 1..NP in file order, as read14 does.  The
+ * barrier records (IBTYPE 3/4/5 families) come from adc_fort14_barriers and
+ * adc_fort14_internal_barriers; periodic (94) and VEW (64) segments return
  * ADC_ERR_UNSUPPORTED. */
 int adc_fort14_dims(const char *path, int dims[6]);
 /* title receives up to 80 characters plus NUL; nm is NM(NE,3); nbdv (NETA)
